@@ -1,0 +1,163 @@
+// common.cuh -- device-side types and exact-arithmetic helpers shared by the
+// kernels of libdynamap_b200.
+//
+// The whole library is compiled with -fmad=false and IEEE division/sqrt, so
+// each float expression below rounds once per operation in source order --
+// the rounding of the reference's own expressions (include/utils/utils.h,
+// include/math/cuda_math.h, include/math/utils_matrix.h) and of the CPU
+// oracle.  That is what makes allocation, integration and raycast
+// bit-identical to the oracle.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/dynamap.h"
+
+namespace dyn {
+
+constexpr int kBlockSize = 8;  // voxels per block edge (tsdfParams blockSize)
+constexpr int kBlockVox = kBlockSize * kBlockSize * kBlockSize;
+constexpr unsigned long long kEmptyKey = ~0ull;
+constexpr int kLevels = 4;     // pyramid levels kept (scales 1, 2, 4, 8)
+
+struct DSensor {
+  int rows, cols;
+  float fx, fy, cx, cy;
+};
+
+struct DTsdf {
+  float vs;          // voxelSize
+  float bsm;         // blockSize * voxelSize (metres), tsdf.cu:437-438
+  float trunc;
+  float dmin, dmax;  // min/maxSensorDepth
+  int num_buckets;
+  int bucket_size;
+  int num_blocks;
+  int max_w;
+  int dda_cap;       // DDA step bound (3*ceil((dmax+trunc)/bsm)+8)
+  int rc_cap;        // raycast step bound (ceil(dmax/min(vs,trunc))+4)
+};
+
+// Hash entry: 16 bytes, one vector load per slot.  key packs the block
+// coordinate (21 bits per axis); ptr is the block's heap index (-1: none);
+// stamp is the last frame whose allocation rays touched the block.
+struct __align__(16) Entry {
+  unsigned long long key;
+  int ptr;
+  int stamp;
+};
+
+// Device counters of a session (one per session, zeroed per frame except
+// nalloc).
+struct Counters {
+  int nalloc;          // heap top == allocated blocks (may exceed num_blocks)
+  int new_blocks;
+  int bucket_full;
+  int heap_exhausted;
+  int dda_overruns;
+  int raycast_overruns;
+  int visible;
+  int unique_probed;
+};
+
+struct F3 {
+  float x, y, z;
+};
+__host__ __device__ inline F3 f3(float x, float y, float z) {
+  F3 r;
+  r.x = x;
+  r.y = y;
+  r.z = z;
+  return r;
+}
+__device__ inline F3 operator+(F3 a, F3 b) { return f3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ inline F3 operator-(F3 a, F3 b) { return f3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ inline F3 operator*(F3 a, float s) { return f3(a.x * s, a.y * s, a.z * s); }
+// utils.h:19-22
+__device__ inline float dot3(F3 a, F3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+// cuda_math.h:397-400
+__device__ inline F3 cross3(F3 a, F3 b) {
+  return f3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+// cuda_math.h:409-413 (IEEE sqrt)
+__device__ inline float norm3(F3 v) { return sqrtf(v.x * v.x + v.y * v.y + v.z * v.z); }
+// cuda_math.h:415-419 with an exact reciprocal square root (1/sqrt): the
+// oracle's host form; the device rsqrtf approximation is not used.
+__device__ inline F3 normalize3(F3 v) {
+  float inv = 1.0f / sqrtf(dot3(v, v));
+  return v * inv;
+}
+
+struct M4f {
+  float m[16];  // row-major, float4x4 layout (utils_matrix.h:816-839)
+};
+// float4x4::operator*(float3) with w = 1, utils_matrix.h:923-930
+__device__ inline F3 xform(const M4f& T, F3 v) {
+  return f3(T.m[0] * v.x + T.m[1] * v.y + T.m[2] * v.z + T.m[3] * 1.0f,
+            T.m[4] * v.x + T.m[5] * v.y + T.m[6] * v.z + T.m[7] * 1.0f,
+            T.m[8] * v.x + T.m[9] * v.y + T.m[10] * v.z + T.m[11] * 1.0f);
+}
+
+// getPoint3d, utils.h:104-112 (scale 1)
+__device__ inline F3 point3d(int i, float depth, const DSensor& s) {
+  int v = i / s.cols;
+  int u = i - s.cols * v;
+  F3 p;
+  p.z = depth;
+  p.x = ((float)u - s.cx) * p.z / s.fx;
+  p.y = ((float)v - s.cy) * p.z / s.fy;
+  return p;
+}
+// Project, utils.h:114-119; non-finite coordinates are rejected (the
+// reference converts them to int unchecked).
+__device__ inline bool project(F3 p, const DSensor& s, int* px, int* py) {
+  float x = ((s.fx * p.x) / p.z) + s.cx;
+  float y = ((s.fy * p.y) / p.z) + s.cy;
+  float rx = roundf(x), ry = roundf(y);
+  if (!(fabsf(rx) < 2e9f) || !(fabsf(ry) < 2e9f)) return false;
+  *px = (int)rx;
+  *py = (int)ry;
+  return true;
+}
+
+// HashTable::Hash, hashTable.cu:152-163: wrapping int32 products.
+__host__ __device__ inline int hash_slot(int x, int y, int z, int nb, int bsz) {
+  int h = (int)(((unsigned)x * 73856093u) ^ ((unsigned)y * 19349669u) ^
+                ((unsigned)z * 83492791u));
+  int r = h % nb;
+  if (r < 0) r += nb;
+  return r * bsz;
+}
+
+__host__ __device__ inline unsigned long long pack_key(int x, int y, int z) {
+  const unsigned long long m = (1ull << 21) - 1;
+  return (((unsigned long long)x & m) << 42) | (((unsigned long long)y & m) << 21) |
+         ((unsigned long long)z & m);
+}
+__host__ __device__ inline int key_x(unsigned long long k) {
+  return (int)(((long long)((k >> 42) & 0x1FFFFF) << 43) >> 43);
+}
+__host__ __device__ inline int key_y(unsigned long long k) {
+  return (int)(((long long)((k >> 21) & 0x1FFFFF) << 43) >> 43);
+}
+__host__ __device__ inline int key_z(unsigned long long k) {
+  return (int)(((long long)(k & 0x1FFFFF) << 43) >> 43);
+}
+
+// Bucket scan, HashTable::FindHashEntry (hashTable.cu:136-150): heap index
+// of the block or -1.
+__device__ inline int find_block(const Entry* __restrict__ entries, const DTsdf& t,
+                                 int x, int y, int z) {
+  int b = hash_slot(x, y, z, t.num_buckets, t.bucket_size);
+  unsigned long long k = pack_key(x, y, z);
+  for (int i = 0; i < t.bucket_size; ++i) {
+    int4 e = __ldg(reinterpret_cast<const int4*>(entries + b + i));
+    unsigned long long ek = ((unsigned long long)(unsigned)e.y << 32) | (unsigned)e.x;
+    if (ek == k) return e.z;
+    if (ek == kEmptyKey) return -1;  // slots fill in order; none after this
+  }
+  return -1;
+}
+
+}  // namespace dyn

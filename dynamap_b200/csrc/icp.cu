@@ -1,0 +1,462 @@
+// icp.cu -- normal equations of projective point-to-plane (+photometric) ICP
+// and the Gauss-Newton step, on the device.
+//
+// Reference: buildNLSKernel (include/solver/gnSolver/gnSolver.cu:26-196) and
+// gnSolver::solve (:317-438).  The reference adds 42 FP32 atomics per
+// correspondence into one 6x6 system and round-trips to the host (Eigen LDLT)
+// every iteration.  Here each thread accumulates its pixels' 21 upper-
+// triangle JtJ terms, 6 Jtr terms, r^2 and a count in registers, the block
+// reduces them with warp shuffles, and the last block to finish (ticket
+// counter) sums the block partials in FP64 in block order -- a fixed
+// reduction order, so results are run-to-run deterministic -- and then runs
+// the GN update (scale by 1/max(A), damping, 6x6 LDL^T, convergence test) and
+// the SE(3) exponential for the next iteration, in FP64, with no host
+// round trip.
+#include "icp.cuh"
+
+namespace dyn {
+
+namespace {
+
+__device__ inline bool normal_ok(float4 n) {
+  if (isnan(n.x) || isnan(n.y) || isnan(n.z)) return false;
+  return !(n.x == 0.0f && n.y == 0.0f && n.z == 0.0f);
+}
+
+struct Acc {
+  float v[kIcpVals];
+  float c[kIcpVals];  // Kahan compensation (used when kahan != 0)
+};
+
+template <bool KAHAN>
+__device__ inline void acc_add(Acc& a, int k, float x) {
+  if (KAHAN) {
+    float y = __fsub_rn(x, a.c[k]);
+    float t = __fadd_rn(a.v[k], y);
+    a.c[k] = __fsub_rn(__fsub_rn(t, a.v[k]), y);
+    a.v[k] = t;
+  } else {
+    a.v[k] += x;
+  }
+}
+
+// Per-pixel terms of buildNLSKernel (gnSolver.cu:55-194) for source pixel
+// idx; the reference's unchecked projection is bounded (z > 0, inside the
+// image) and photometric gradient taps outside the image read the centre.
+template <bool KAHAN>
+__device__ inline void pixel_terms(const IcpLevel& L, const IcpParams& P, const M4f& T,
+                                   int idx, Acc& a) {
+  const DSensor& s = L.s;
+  float d = L.sd[idx];
+  if (d < P.dmin || d > P.dmax) return;
+  float4 sn4 = L.sn[idx];
+  if (!normal_ok(sn4)) return;
+  F3 p = xform(T, point3d(idx, d, s));
+  if (!(p.z > 0.0f)) return;
+  int px, py;
+  if (!project(p, s, &px, &py)) return;
+  if (px < 0 || py < 0 || px >= s.cols || py >= s.rows) return;
+  int index = py * s.cols + px;
+  float td = L.td[index];
+  if (td < P.dmin || td > P.dmax) return;
+  float4 n4 = L.tn[index];
+  if (!normal_ok(n4)) return;
+  F3 n = f3(n4.x, n4.y, n4.z);
+  float cosT = dot3(n, f3(sn4.x, sn4.y, sn4.z));
+  F3 q = point3d(index, td, s);
+  if (!(fabsf(cosT) > P.cos_thr)) return;
+  F3 c = cross3(p, n);
+  float cn[6] = {c.x, c.y, c.z, n.x, n.y, n.z};
+  F3 pq = p - q;
+  float b[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k)
+    b[k] = pq.x * (cn[k] * n.x) + pq.y * (cn[k] * n.y) + pq.z * (cn[k] * n.z);
+  float r = dot3(pq, n);
+  if (P.cw != 0.0f) {
+    // gnSolver.cu:137-190: J_c = grad(I_t)(1x3) * [-p^ | I](3x6)
+    int il = px >= 1 ? index - 1 : index;
+    int iu = py >= 1 ? index - s.cols : index;
+    float ic = L.ti[index];
+    float gx = (ic - L.ti[il]) / 2.0f;
+    float gy = (ic - L.ti[iu]) / 2.0f;
+    float Jc[6] = {gx * 0.0f + gy * (-p.z), gx * p.z + gy * 0.0f, gx * (-p.y) + gy * p.x,
+                   gx, gy, 0.0f};
+    float e = ic - L.si[idx];
+    float w1 = 1.0f - P.cw;
+    int u = 0;
+#pragma unroll
+    for (int i = 0; i < 6; ++i)
+#pragma unroll
+      for (int j = i; j < 6; ++j) acc_add<KAHAN>(a, u++, w1 * (cn[i] * cn[j]) + (P.cw * Jc[i]) * Jc[j]);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) acc_add<KAHAN>(a, 21 + k, -(w1 * b[k] + (P.cw * Jc[k]) * e));
+  } else {
+    int u = 0;
+#pragma unroll
+    for (int i = 0; i < 6; ++i)
+#pragma unroll
+      for (int j = i; j < 6; ++j) acc_add<KAHAN>(a, u++, cn[i] * cn[j]);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) acc_add<KAHAN>(a, 21 + k, -b[k]);
+  }
+  acc_add<KAHAN>(a, 27, r * r);
+  acc_add<KAHAN>(a, 28, 1.0f);
+}
+
+// Block sum of the 29 accumulators in double, fixed order; result in
+// red[0..28] (shared) after the call.
+__device__ inline void block_reduce(const Acc& a, bool kahan, double* red /*[8][29]*/) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < kIcpVals; ++k) {
+    double v = (double)a.v[k];
+    if (kahan) v -= (double)a.c[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) red[warp * kIcpVals + k] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < kIcpVals) {
+    double s = 0.0;
+    for (int w = 0; w < kIcpThreads / 32; ++w) s += red[w * kIcpVals + threadIdx.x];
+    red[threadIdx.x] = s;  // row 0 reused: each thread rewrites its own column
+  }
+  __syncthreads();
+}
+
+// Sum of the per-block partials in FP64 (block order fixed per lane, then a
+// fixed shuffle tree).  out[29] in shared memory.
+__device__ inline void final_reduce(const double* __restrict__ partials, int nblocks,
+                                    double* out) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int k = warp; k < kIcpVals; k += kIcpThreads / 32) {
+    double s = 0.0;
+    for (int b = lane; b < nblocks; b += 32) s += __ldcg(partials + (size_t)b * kIcpVals + k);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) out[k] = s;
+  }
+  __syncthreads();
+}
+
+// ---- FP64 6x6 algebra (one thread) --------------------------------------
+// LDL^T of a symmetric positive definite 6x6 (stands in for Eigen's
+// A.ldlt().solve(b), gnSolver.cu:439-442).  Returns false on a zero pivot.
+__device__ bool ldlt6(const double* A, const double* b, double* x) {
+  double L[36], D[6];
+  for (int k = 0; k < 36; ++k) L[k] = 0.0;
+  for (int j = 0; j < 6; ++j) {
+    double s = A[j * 6 + j];
+    for (int k = 0; k < j; ++k) s -= L[j * 6 + k] * L[j * 6 + k] * D[k];
+    D[j] = s;
+    if (!(fabs(s) > 0.0)) return false;
+    L[j * 6 + j] = 1.0;
+    for (int i = j + 1; i < 6; ++i) {
+      double t = A[i * 6 + j];
+      for (int k = 0; k < j; ++k) t -= L[i * 6 + k] * L[j * 6 + k] * D[k];
+      L[i * 6 + j] = t / D[j];
+    }
+  }
+  double y[6];
+  for (int i = 0; i < 6; ++i) {
+    double t = b[i];
+    for (int k = 0; k < i; ++k) t -= L[i * 6 + k] * y[k];
+    y[i] = t;
+  }
+  for (int i = 0; i < 6; ++i) y[i] /= D[i];
+  for (int i = 5; i >= 0; --i) {
+    double t = y[i];
+    for (int k = i + 1; k < 6; ++k) t -= L[k * 6 + i] * x[k];
+    x[i] = t;
+  }
+  return true;
+}
+
+// exp of the twist matrix v2t(xi) (gnSolver.cu:443-455): rotation by
+// Rodrigues' formula and translation through the SE(3) left Jacobian,
+// R = I + a W + b W^2, t = (I + b W + c W^2) v, with a = sin t / t,
+// b = (1 - cos t)/t^2, c = (t - sin t)/t^3 (Taylor below t = 1e-4).
+__device__ void se3_exp(const double* xi, double* T) {
+  double w0 = xi[0], w1 = xi[1], w2 = xi[2];
+  double th2 = w0 * w0 + w1 * w1 + w2 * w2, th = sqrt(th2);
+  double a, b, c;
+  if (th < 1e-4) {
+    a = 1.0 - th2 / 6.0;
+    b = 0.5 - th2 / 24.0;
+    c = 1.0 / 6.0 - th2 / 120.0;
+  } else {
+    double sn, cs;
+    sincos(th, &sn, &cs);
+    a = sn / th;
+    b = (1.0 - cs) / th2;
+    c = (th - sn) / (th2 * th);
+  }
+  double W[9] = {0, -w2, w1, w2, 0, -w0, -w1, w0, 0};
+  double W2[9];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double s = 0;
+      for (int k = 0; k < 3; ++k) s += W[i * 3 + k] * W[k * 3 + j];
+      W2[i * 3 + j] = s;
+    }
+  for (int i = 0; i < 3; ++i) {
+    for (int j = 0; j < 3; ++j) {
+      double I = (i == j) ? 1.0 : 0.0;
+      T[i * 4 + j] = I + a * W[i * 3 + j] + b * W2[i * 3 + j];
+    }
+    double V0 = (i == 0 ? 1.0 : 0.0) + b * W[i * 3 + 0] + c * W2[i * 3 + 0];
+    double V1 = (i == 1 ? 1.0 : 0.0) + b * W[i * 3 + 1] + c * W2[i * 3 + 1];
+    double V2 = (i == 2 ? 1.0 : 0.0) + b * W[i * 3 + 2] + c * W2[i * 3 + 2];
+    T[i * 4 + 3] = V0 * xi[3] + V1 * xi[4] + V2 * xi[5];
+  }
+  T[12] = T[13] = T[14] = 0.0;
+  T[15] = 1.0;
+}
+
+__device__ void matmul4d(const double* A, const double* B, double* C) {
+  double t[16];
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) {
+      double s = 0;
+      for (int k = 0; k < 4; ++k) s += A[i * 4 + k] * B[k * 4 + j];
+      t[i * 4 + j] = s;
+    }
+  for (int k = 0; k < 16; ++k) C[k] = t[k];
+}
+
+// float4x4::getInverse, utils_matrix.h:970-1086: cofactors summed in the
+// reference's order, determinant from row 0, times 1/det.
+__device__ void inverse4f(const float* e, float* out) {
+  float inv[16];
+  inv[0] = e[5] * e[10] * e[15] - e[5] * e[11] * e[14] - e[9] * e[6] * e[15] +
+           e[9] * e[7] * e[14] + e[13] * e[6] * e[11] - e[13] * e[7] * e[10];
+  inv[4] = -e[4] * e[10] * e[15] + e[4] * e[11] * e[14] + e[8] * e[6] * e[15] -
+           e[8] * e[7] * e[14] - e[12] * e[6] * e[11] + e[12] * e[7] * e[10];
+  inv[8] = e[4] * e[9] * e[15] - e[4] * e[11] * e[13] - e[8] * e[5] * e[15] +
+           e[8] * e[7] * e[13] + e[12] * e[5] * e[11] - e[12] * e[7] * e[9];
+  inv[12] = -e[4] * e[9] * e[14] + e[4] * e[10] * e[13] + e[8] * e[5] * e[14] -
+            e[8] * e[6] * e[13] - e[12] * e[5] * e[10] + e[12] * e[6] * e[9];
+  inv[1] = -e[1] * e[10] * e[15] + e[1] * e[11] * e[14] + e[9] * e[2] * e[15] -
+           e[9] * e[3] * e[14] - e[13] * e[2] * e[11] + e[13] * e[3] * e[10];
+  inv[5] = e[0] * e[10] * e[15] - e[0] * e[11] * e[14] - e[8] * e[2] * e[15] +
+           e[8] * e[3] * e[14] + e[12] * e[2] * e[11] - e[12] * e[3] * e[10];
+  inv[9] = -e[0] * e[9] * e[15] + e[0] * e[11] * e[13] + e[8] * e[1] * e[15] -
+           e[8] * e[3] * e[13] - e[12] * e[1] * e[11] + e[12] * e[3] * e[9];
+  inv[13] = e[0] * e[9] * e[14] - e[0] * e[10] * e[13] - e[8] * e[1] * e[14] +
+            e[8] * e[2] * e[13] + e[12] * e[1] * e[10] - e[12] * e[2] * e[9];
+  inv[2] = e[1] * e[6] * e[15] - e[1] * e[7] * e[14] - e[5] * e[2] * e[15] +
+           e[5] * e[3] * e[14] + e[13] * e[2] * e[7] - e[13] * e[3] * e[6];
+  inv[6] = -e[0] * e[6] * e[15] + e[0] * e[7] * e[14] + e[4] * e[2] * e[15] -
+           e[4] * e[3] * e[14] - e[12] * e[2] * e[7] + e[12] * e[3] * e[6];
+  inv[10] = e[0] * e[5] * e[15] - e[0] * e[7] * e[13] - e[4] * e[1] * e[15] +
+            e[4] * e[3] * e[13] + e[12] * e[1] * e[7] - e[12] * e[3] * e[5];
+  inv[14] = -e[0] * e[5] * e[14] + e[0] * e[6] * e[13] + e[4] * e[1] * e[14] -
+            e[4] * e[2] * e[13] - e[12] * e[1] * e[6] + e[12] * e[2] * e[5];
+  inv[3] = -e[1] * e[6] * e[11] + e[1] * e[7] * e[10] + e[5] * e[2] * e[11] -
+           e[5] * e[3] * e[10] - e[9] * e[2] * e[7] + e[9] * e[3] * e[6];
+  inv[7] = e[0] * e[6] * e[11] - e[0] * e[7] * e[10] - e[4] * e[2] * e[11] +
+           e[4] * e[3] * e[10] + e[8] * e[2] * e[7] - e[8] * e[3] * e[6];
+  inv[11] = -e[0] * e[5] * e[11] + e[0] * e[7] * e[9] + e[4] * e[1] * e[11] -
+            e[4] * e[3] * e[9] - e[8] * e[1] * e[7] + e[8] * e[3] * e[5];
+  inv[15] = e[0] * e[5] * e[10] - e[0] * e[6] * e[9] - e[4] * e[1] * e[10] +
+            e[4] * e[2] * e[9] + e[8] * e[1] * e[6] - e[8] * e[2] * e[5];
+  float det = e[0] * inv[0] + e[1] * inv[4] + e[2] * inv[8] + e[3] * inv[12];
+  float detr = 1.0f / det;
+  for (int i = 0; i < 16; ++i) out[i] = inv[i] * detr;
+}
+
+// gnSolver::solve's per-iteration host block (gnSolver.cu:389-415) for the
+// summed system 'acc'.  Updates inc/prev; returns true when converged.
+__device__ bool gn_update(const double* acc, const IcpParams& P, int it, IcpState* st) {
+  double A[36], b[6];
+  int u = 0;
+  for (int i = 0; i < 6; ++i)
+    for (int j = i; j < 6; ++j) {
+      A[i * 6 + j] = acc[u];
+      A[j * 6 + i] = acc[u];
+      ++u;
+    }
+  for (int k = 0; k < 6; ++k) b[k] = acc[21 + k];
+  double mx = A[0];
+  for (int k = 1; k < 36; ++k) mx = fmax(mx, A[k]);
+  double scaling = 1.0 / mx;
+  for (int k = 0; k < 6; ++k) b[k] *= scaling;
+  for (int k = 0; k < 36; ++k) A[k] *= scaling;
+  double mx2 = A[0];
+  for (int k = 1; k < 36; ++k) mx2 = fmax(mx2, A[k]);
+  double alpha = (double)P.reg * mx2;
+  for (int k = 0; k < 6; ++k) A[k * 6 + k] += alpha / (double)it;
+  double d[6] = {0, 0, 0, 0, 0, 0};
+  if (!ldlt6(A, b, d))
+    for (int k = 0; k < 6; ++k) d[k] = __longlong_as_double(0x7ff8000000000000LL);
+  double ch = 0.0;
+  for (int k = 0; k < 6; ++k) {
+    st->inc[k] += d[k];
+    double c = st->inc[k] - st->prev[k];
+    ch += c * c;
+  }
+  bool conv = fabs(sqrt(ch)) <= (double)P.min_inc;
+  if (!conv)
+    for (int k = 0; k < 6; ++k) st->prev[k] = st->inc[k];
+  return conv;
+}
+
+template <bool KAHAN>
+__global__ void __launch_bounds__(kIcpThreads)
+    icp_iteration_kernel(IcpLevel L, IcpParams P, int pl, int it, IcpState* st,
+                         double* __restrict__ partials) {
+  __shared__ double red[(kIcpThreads / 32) * kIcpVals];
+  __shared__ M4f Ts;
+  __shared__ int skip;
+  if (threadIdx.x == 0) {
+    int sk = (st->have_target == 0) || (it > 1 && st->converged);
+    skip = sk;
+  }
+  if (threadIdx.x < 16) Ts.m[threadIdx.x] = st->T[threadIdx.x];
+  __syncthreads();
+  if (skip) return;
+  const M4f T = Ts;
+  Acc a;
+#pragma unroll
+  for (int k = 0; k < kIcpVals; ++k) a.v[k] = a.c[k] = 0.0f;
+  const int n = L.s.rows * L.s.cols;
+  for (int idx = blockIdx.x * kIcpThreads + threadIdx.x; idx < n;
+       idx += gridDim.x * kIcpThreads)
+    pixel_terms<KAHAN>(L, P, T, idx, a);
+  block_reduce(a, KAHAN, red);
+  if (threadIdx.x < kIcpVals) partials[(size_t)blockIdx.x * kIcpVals + threadIdx.x] = red[threadIdx.x];
+  __threadfence();
+  __shared__ unsigned int ticket;
+  if (threadIdx.x == 0) ticket = atomicAdd(&st->ticket, 1u);
+  __syncthreads();
+  if (ticket != gridDim.x - 1) return;
+  __threadfence();
+  __shared__ double tot[kIcpVals];
+  final_reduce(partials, gridDim.x, tot);
+  if (threadIdx.x == 0) {
+    st->ticket = 0;
+    st->iters[pl] = it;
+    st->inliers[pl] = (int)tot[28];
+    st->rms[pl] = tot[28] > 0 ? (float)sqrt(tot[27] / tot[28]) : 0.0f;
+    bool conv = gn_update(tot, P, it, st);
+    st->converged = conv ? 1 : 0;
+    double Td[16];
+    se3_exp(st->inc, Td);
+    for (int k = 0; k < 16; ++k) st->T[k] = (float)Td[k];
+  }
+}
+
+// Normal equations only (stage entry point): no solver state.
+__global__ void __launch_bounds__(kIcpThreads)
+    icp_reduce_kernel(IcpLevel L, IcpParams P, const float* __restrict__ Tdev,
+                      double* __restrict__ partials, unsigned int* ticket_ctr,
+                      double* __restrict__ out) {
+  __shared__ double red[(kIcpThreads / 32) * kIcpVals];
+  __shared__ M4f Ts;
+  if (threadIdx.x < 16) Ts.m[threadIdx.x] = Tdev[threadIdx.x];
+  __syncthreads();
+  const M4f T = Ts;
+  Acc a;
+#pragma unroll
+  for (int k = 0; k < kIcpVals; ++k) a.v[k] = a.c[k] = 0.0f;
+  const int n = L.s.rows * L.s.cols;
+  for (int idx = blockIdx.x * kIcpThreads + threadIdx.x; idx < n;
+       idx += gridDim.x * kIcpThreads) {
+    if (P.kahan) pixel_terms<true>(L, P, T, idx, a);
+    else pixel_terms<false>(L, P, T, idx, a);
+  }
+  block_reduce(a, P.kahan != 0, red);
+  if (threadIdx.x < kIcpVals) partials[(size_t)blockIdx.x * kIcpVals + threadIdx.x] = red[threadIdx.x];
+  __threadfence();
+  __shared__ unsigned int ticket;
+  if (threadIdx.x == 0) ticket = atomicAdd(ticket_ctr, 1u);
+  __syncthreads();
+  if (ticket != gridDim.x - 1) return;
+  __threadfence();
+  __shared__ double tot[kIcpVals];
+  final_reduce(partials, gridDim.x, tot);
+  if (threadIdx.x < kIcpVals) out[threadIdx.x] = tot[threadIdx.x];
+  if (threadIdx.x == 0) *ticket_ctr = 0;
+}
+
+__device__ void finish_pose(PoseState* ps) {
+  for (int k = 0; k < 16; ++k) ps->posef[k] = (float)ps->pose[k];
+  inverse4f(ps->posef, ps->invf);
+}
+
+// gnSolver.cu:426-430 + builder pose bookkeeping.
+__global__ void pose_finalize_kernel(IcpParams P, IcpState* st, PoseState* ps) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  ps->reset = 0;
+  if (st->have_target) {
+    double s = 0.0;
+    for (int k = 0; k < 6; ++k) s += st->inc[k];
+    bool reset = isnan(s) || isinf(s) || s >= (double)P.max_inc;
+    if (reset)
+      for (int k = 0; k < 6; ++k) st->inc[k] = 0.0;
+    double E[16];
+    se3_exp(st->inc, E);
+    if (P.compose_left) matmul4d(E, ps->pose, ps->pose);
+    else matmul4d(ps->pose, E, ps->pose);
+    ps->reset = reset ? 1 : 0;
+  } else {
+    for (int k = 0; k < 3; ++k) {
+      st->iters[k] = 0;
+      st->inliers[k] = 0;
+      st->rms[k] = 0.0f;
+    }
+  }
+  for (int k = 0; k < 6; ++k) {
+    ps->last_inc[k] = st->inc[k];
+    st->inc[k] = 0.0;
+    st->prev[k] = 0.0;
+  }
+  for (int k = 0; k < 16; ++k) st->T[k] = (k % 5 == 0) ? 1.0f : 0.0f;
+  st->converged = 0;
+  st->ticket = 0;
+  finish_pose(ps);
+}
+
+__global__ void pose_set_kernel(PoseState* ps, const double* pose) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  for (int k = 0; k < 16; ++k) ps->pose[k] = pose[k];
+  finish_pose(ps);
+}
+
+inline int icp_grid(int n) {
+  int g = (n + kIcpThreads - 1) / kIcpThreads;
+  if (g > kIcpMaxBlocks) g = kIcpMaxBlocks;
+  if (g < 1) g = 1;
+  return g;
+}
+
+}  // namespace
+
+size_t icp_scratch_bytes() { return sizeof(double) * (size_t)kIcpMaxBlocks * kIcpVals; }
+
+void launch_icp_iteration(const IcpLevel& L, const IcpParams& P, int pl, int it, IcpState* st,
+                          double* partials, cudaStream_t stream) {
+  int g = icp_grid(L.s.rows * L.s.cols);
+  if (P.kahan)
+    icp_iteration_kernel<true><<<g, kIcpThreads, 0, stream>>>(L, P, pl, it, st, partials);
+  else
+    icp_iteration_kernel<false><<<g, kIcpThreads, 0, stream>>>(L, P, pl, it, st, partials);
+}
+
+void launch_pose_finalize(const IcpParams& P, IcpState* st, PoseState* ps, cudaStream_t stream) {
+  pose_finalize_kernel<<<1, 32, 0, stream>>>(P, st, ps);
+}
+
+void launch_pose_set(PoseState* ps, const double* pose_dev, cudaStream_t stream) {
+  pose_set_kernel<<<1, 32, 0, stream>>>(ps, pose_dev);
+}
+
+void launch_icp_reduce_only(const IcpLevel& L, const IcpParams& P, const float* T_dev,
+                            double* partials, unsigned int* ticket, double* out_dev,
+                            cudaStream_t stream) {
+  int g = icp_grid(L.s.rows * L.s.cols);
+  icp_reduce_kernel<<<g, kIcpThreads, 0, stream>>>(L, P, T_dev, partials, ticket, out_dev);
+}
+
+}  // namespace dyn

@@ -1,0 +1,72 @@
+// icp.cuh -- projective point-to-plane (+photometric) ICP normal equations
+// and the on-device Gauss-Newton step.
+#pragma once
+#include "common.cuh"
+
+namespace dyn {
+
+// Per-session solver state, device resident.
+struct IcpState {
+  double inc[6];      // xi accumulated over the frame's levels (gnSolver.cu:345)
+  double prev[6];     // prev_increment (gnSolver.cu:347,415)
+  float T[16];        // float exp(v2t(inc)) used by the next reduction
+  int converged;      // current level stopped (|delta| <= minIncrement)
+  int have_target;    // 0 until a target exists (first frame: no tracking)
+  unsigned int ticket;  // last-block-done counter
+  int iters[3];
+  int inliers[3];
+  float rms[3];
+};
+
+// Pose of the session, device resident.
+struct PoseState {
+  double pose[16];    // camera-to-world (row-major, double)
+  float posef[16];    // float copy used by the kernels
+  float invf[16];     // float4x4::getInverse of posef (utils_matrix.h:970-1086)
+  double last_inc[6];
+  int reset;          // NaN / maxIncrement guard fired this frame
+  int frame;
+};
+
+struct IcpLevel {
+  const float* sd;     // source depth
+  const float4* sn;    // source normals
+  const float* si;     // source intensity (may be null if cw == 0)
+  const float* td;     // target depth
+  const float4* tn;    // target normals
+  const float* ti;     // target intensity (may be null if cw == 0)
+  DSensor s;
+};
+
+struct IcpParams {
+  float dmin, dmax;    // icp depth window
+  float cos_thr;
+  float cw;            // color weight
+  float min_inc, max_inc, reg;
+  int compose_left;
+  int kahan;           // compensated FP32 per-thread sums (mixed precision)
+};
+
+constexpr int kIcpThreads = 256;
+constexpr int kIcpMaxBlocks = 148 * 8;
+constexpr int kIcpVals = 29;
+
+// Scratch a reduction needs: per-block partial sums (kIcpMaxBlocks*29 doubles).
+size_t icp_scratch_bytes();
+
+// One GN iteration of level slot 'pl' (iteration 'it', 1-based): reduce the
+// normal equations into 'partials', the last block solves and updates 'st'.
+void launch_icp_iteration(const IcpLevel& L, const IcpParams& P, int pl, int it,
+                          IcpState* st, double* partials, cudaStream_t stream);
+// After the last level: guards, pose composition, float pose + inverse, reset
+// of the solver state.  Runs with one thread.
+void launch_pose_finalize(const IcpParams& P, IcpState* st, PoseState* ps,
+                          cudaStream_t stream);
+// Set the pose from the host (double[16]); recomputes posef/invf.
+void launch_pose_set(PoseState* ps, const double* pose_dev, cudaStream_t stream);
+// Normal equations only (no solve): out[29] doubles on the device.
+void launch_icp_reduce_only(const IcpLevel& L, const IcpParams& P, const float* T_dev,
+                            double* partials, unsigned int* ticket, double* out_dev,
+                            cudaStream_t stream);
+
+}  // namespace dyn

@@ -1,0 +1,217 @@
+// image.cu -- depth ingest, bilateral filter, 2x pyramid and normal maps.
+//
+// Reference: include/image/pyramid/pyramid.cu (bilateral :208-252, pyramid
+// :49-143), include/image/sensor/rgbdImage.cu (vertex map :23-38, normals
+// :126-157), include/solver/gnSolver/gnSolver.cu:457-465 (intensity).
+#include "image.cuh"
+
+namespace dyn {
+
+namespace {
+
+// gnSolver::Intensity(ColorToFloat(c)), gnSolver.cu:457-459 + utils.h:98-102:
+// channel/255 in float, weighted sum in double, result rounded to float.
+__device__ inline float intensity_u8(const uint8_t* c) {
+  float r = (float)c[0] / 255.0f, g = (float)c[1] / 255.0f, b = (float)c[2] / 255.0f;
+  return (float)(0.2126 * (double)r + 0.7152 * (double)g + 0.0722 * (double)b);
+}
+
+// u16 sensor units -> metres (builder.cu:111, utils_Dataset.cpp:233-235)
+__global__ void ingest_kernel(const uint16_t* __restrict__ raw,
+                              const uint8_t* __restrict__ rgb, int n, float scaler,
+                              float* __restrict__ depth, float* __restrict__ inten) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  depth[i] = (float)raw[i] / scaler;
+  if (inten) inten[i] = rgb ? intensity_u8(rgb + 3 * (size_t)i) : 0.0f;
+}
+
+constexpr int BTX = 32, BTY = 8;
+
+// pyramid::gaussian, pyramid.cu:208-211 (double)
+__device__ inline double gaussian_d(double x, double sigma) {
+  return exp(-(x * x) / (2.0 * sigma * sigma)) / (2.0 * 3.14159265358979323846 * sigma * sigma);
+}
+
+// pyramid::applyBilateralFilter, pyramid.cu:213-233, one thread per pixel,
+// window rows x-(r)..x+r-1, cols y-r..y+r-1, summed row-major.  The depth
+// tile plus halo is staged in shared memory; the spatial weights (a pure
+// function of the tap offset) are built once per CTA in double and rounded
+// to float as the reference does per tap.  Taps outside the image or with
+// depth <= 0 are skipped and invalid centres stay 0.
+__global__ void bilateral_kernel(const float* __restrict__ src, float* __restrict__ dst,
+                                 int rows, int cols, int r, float sigma_i, float sigma_s) {
+  extern __shared__ float sm[];
+  const int D = 2 * r, half = r;
+  float* gs = sm;                        // D*D
+  const int TW = BTX + D - 1, TH = BTY + D - 1;
+  float* tile = sm + D * D;              // TH*TW (rows x cols)
+  const int tid = threadIdx.y * BTX + threadIdx.x;
+  for (int k = tid; k < D * D; k += BTX * BTY) {
+    int i = k / D, j = k - (k / D) * D;
+    float dx = (float)(half - i), dy = (float)(half - j);
+    float dd = sqrtf(dx * dx + dy * dy + 0.0f * 0.0f);
+    gs[k] = (float)gaussian_d((double)dd, (double)sigma_s);
+  }
+  const int row0 = blockIdx.y * BTY - half, col0 = blockIdx.x * BTX - half;
+  for (int k = tid; k < TW * TH; k += BTX * BTY) {
+    int tr = k / TW, tc = k - (k / TW) * TW;
+    int gr = row0 + tr, gc = col0 + tc;
+    tile[k] = (gr >= 0 && gr < rows && gc >= 0 && gc < cols) ? src[gr * cols + gc] : 0.0f;
+  }
+  __syncthreads();
+  const int x = blockIdx.y * BTY + threadIdx.y;  // row (the reference's x)
+  const int y = blockIdx.x * BTX + threadIdx.x;  // column
+  if (x >= rows || y >= cols) return;
+  const float c = tile[(threadIdx.y + half) * TW + threadIdx.x + half];
+  if (!(c > 0.0f)) {
+    dst[x * cols + y] = 0.0f;
+    return;
+  }
+  const float k_norm = (float)(1.0 / (2.0 * 3.14159265358979323846 * (double)sigma_i *
+                                      (double)sigma_i));
+  const float k_exp = 2.0f * sigma_i * sigma_i;
+  float acc = 0.0f, wp = 0.0f;
+  for (int i = 0; i < D; ++i) {
+    int nx = x - (half - i);
+    if (nx < 0 || nx >= rows) continue;
+    const float* trow = tile + (threadIdx.y + i) * TW + threadIdx.x;
+    const float* grow = gs + i * D;
+    for (int j = 0; j < D; ++j) {
+      int ny = y - (half - j);
+      if (ny < 0 || ny >= cols) continue;
+      float nv = trow[j];
+      if (!(nv > 0.0f)) continue;
+      float dv = nv - c;
+      float gi = expf(-(dv * dv) / k_exp) * k_norm;
+      float w = gi * grow[j];
+      acc += nv * w;
+      wp += w;
+    }
+  }
+  dst[x * cols + y] = acc / wp;
+}
+
+// One 2x pyramid step: mean of the valid depths of each 2x2 cell (fix of
+// pyramid.cu:49-82, which scatters into a fixed 640x480 window).
+__global__ void downsample_depth_kernel(const float* __restrict__ src, int rows, int cols,
+                                        float* __restrict__ dst) {
+  int c2 = cols / 2, r2 = rows / 2;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= r2 * c2) return;
+  int y = i / c2, x = i - (i / c2) * c2;
+  const float* a = src + (2 * y) * cols + 2 * x;
+  float v[4] = {a[0], a[1], a[cols], a[cols + 1]};
+  float s = 0.0f;
+  int n = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    if (v[k] > 0.0f) {
+      s += v[k];
+      n++;
+    }
+  dst[i] = n ? s / (float)n : 0.0f;
+}
+
+__global__ void downsample_intensity_kernel(const float* __restrict__ src, int rows, int cols,
+                                            float* __restrict__ dst) {
+  int c2 = cols / 2, r2 = rows / 2;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= r2 * c2) return;
+  int y = i / c2, x = i - (i / c2) * c2;
+  const float* a = src + (2 * y) * cols + 2 * x;
+  dst[i] = (((a[0] + a[1]) + a[cols]) + a[cols + 1]) * 0.25f;
+}
+
+// creatPointCloudKernel (rgbdImage.cu:23-38) and vertextoNormal
+// (rgbdImage.cu:126-145): n = normalize(cross(V(u+2)-V(u-2), V(v+1)-V(v-1))),
+// all pyramid levels in one launch.  Vertices are recomputed from depth, so
+// neighbours need no vertex map.  A normal is 0 when the centre or a
+// neighbour is invalid or outside the row/image.
+__global__ void maps_kernel(MapsArgs a) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= a.total) return;
+  int l = 0;
+#pragma unroll
+  for (int k = 1; k < kLevels; ++k)
+    if (k < a.nlev && g >= a.lv[k].offset) l = k;
+  const LevelMaps& L = a.lv[l];
+  int i = g - L.offset;
+  const DSensor s = L.s;
+  int y = i / s.cols, x = i - (i / s.cols) * s.cols;
+  float d = L.depth[i];
+  float4 nrm = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (!(d > 0.0f)) {
+    L.normal[i] = nrm;
+    if (L.vertex) L.vertex[i] = nrm;
+    return;
+  }
+  F3 p = point3d(i, d, s);
+  if (L.vertex) L.vertex[i] = make_float4(p.x, p.y, p.z, 1.0f);
+  if (x - 2 >= 0 && x + 2 < s.cols && y - 1 >= 0 && y + 1 < s.rows) {
+    int il = i - 2, ir = i + 2, iu = i - s.cols, id = i + s.cols;
+    float dl = L.depth[il], dr = L.depth[ir], du = L.depth[iu], dd = L.depth[id];
+    if (dl > 0.0f && dr > 0.0f && du > 0.0f && dd > 0.0f) {
+      F3 left = point3d(il, dl, s), right = point3d(ir, dr, s);
+      F3 up = point3d(iu, du, s), down = point3d(id, dd, s);
+      F3 c = cross3(right - left, down - up);
+      float dd2 = dot3(c, c);
+      if (dd2 > 0.0f) {
+        F3 n = c * (1.0f / sqrtf(dd2));
+        nrm = make_float4(n.x, n.y, n.z, 0.0f);
+      }
+    }
+  }
+  L.normal[i] = nrm;
+}
+
+__global__ void target_prepare_kernel(const float* __restrict__ ray, float* __restrict__ d0,
+                                      float dmax, const uint8_t* __restrict__ rgb,
+                                      float* __restrict__ inten, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float d = ray[i];
+  d0[i] = (d < dmax) ? d : 0.0f;
+  if (inten) inten[i] = rgb ? intensity_u8(rgb + 3 * (size_t)i) : 0.0f;
+}
+
+inline int nblk(long long n, int t) { return (int)((n + t - 1) / t); }
+
+}  // namespace
+
+void launch_ingest(const uint16_t* raw, const uint8_t* rgb, int n, float scaler,
+                   float* depth_out, float* intensity_out, cudaStream_t st) {
+  ingest_kernel<<<nblk(n, 256), 256, 0, st>>>(raw, rgb, n, scaler, depth_out, intensity_out);
+}
+
+void launch_bilateral(const float* src, float* dst, int rows, int cols, int radius,
+                      float sigma_i, float sigma_s, cudaStream_t st) {
+  int D = 2 * radius;
+  size_t smem = sizeof(float) * ((size_t)D * D + (size_t)(BTX + D - 1) * (BTY + D - 1));
+  dim3 grid(nblk(cols, BTX), nblk(rows, BTY));
+  bilateral_kernel<<<grid, dim3(BTX, BTY), smem, st>>>(src, dst, rows, cols, radius, sigma_i,
+                                                       sigma_s);
+}
+
+void launch_downsample_depth(const float* src, int rows, int cols, float* dst, cudaStream_t st) {
+  int n = (rows / 2) * (cols / 2);
+  if (n > 0) downsample_depth_kernel<<<nblk(n, 256), 256, 0, st>>>(src, rows, cols, dst);
+}
+void launch_downsample_intensity(const float* src, int rows, int cols, float* dst,
+                                 cudaStream_t st) {
+  int n = (rows / 2) * (cols / 2);
+  if (n > 0) downsample_intensity_kernel<<<nblk(n, 256), 256, 0, st>>>(src, rows, cols, dst);
+}
+void launch_maps(const MapsArgs& a, cudaStream_t st) {
+  if (a.total > 0) maps_kernel<<<nblk(a.total, 256), 256, 0, st>>>(a);
+}
+void launch_target_prepare(const float* ray_depth, float* depth0, float dmax, const uint8_t* rgb,
+                           float* intensity0, int n, cudaStream_t st) {
+  target_prepare_kernel<<<nblk(n, 256), 256, 0, st>>>(ray_depth, depth0, dmax, rgb, intensity0,
+                                                      n);
+}
+void launch_copy_f(const float* src, float* dst, size_t n, cudaStream_t st) {
+  if (n) cudaMemcpyAsync(dst, src, n * sizeof(float), cudaMemcpyDeviceToDevice, st);
+}
+
+}  // namespace dyn

@@ -1,0 +1,845 @@
+// session.cu -- the C ABI of include/dynamap.h: sessions (the reference's
+// builder, include/builder/builder.cu), the per-frame pipeline and the stage
+// entry points.
+//
+// One session = one RGB-D stream.  All of its device memory (hash entries,
+// voxel blocks, image pyramids, solver state) is allocated once in
+// dyn_session_create and sized from its parameters; frames allocate nothing.
+// The per-frame kernel sequence is captured once into a CUDA graph and
+// replayed per frame on the session's own stream; tracking state, pose and
+// counters stay on the device, so a frame needs no host synchronisation
+// between stages (the reference synchronises after every launch and solves
+// each GN iteration on the host).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <vector>
+
+#include "common.cuh"
+#include "icp.cuh"
+#include "image.cuh"
+#include "tsdf.cuh"
+
+using namespace dyn;
+
+namespace {
+
+struct ResultBlock {
+  PoseState pose;
+  IcpState icp;
+  Counters cnt;
+};
+
+int level_of_scale(int scale) {
+  int l = 0;
+  while ((1 << l) < scale && l < kLevels - 1) ++l;
+  return l;
+}
+
+DSensor dsensor(const dyn_sensor& s) {
+  DSensor d;
+  d.rows = (int)s.rows;
+  d.cols = (int)s.cols;
+  d.fx = s.fx;
+  d.fy = s.fy;
+  d.cx = s.cx;
+  d.cy = s.cy;
+  return d;
+}
+
+// Level sensor for scale 2^l: f/s, (c+0.5)/s-0.5, dims floor(dim/s).
+dyn_sensor level_sensor(const dyn_sensor& s, int scale) {
+  dyn_sensor o = s;
+  o.rows = s.rows / (uint32_t)scale;
+  o.cols = s.cols / (uint32_t)scale;
+  o.fx = s.fx / (float)scale;
+  o.fy = s.fy / (float)scale;
+  o.cx = (s.cx + 0.5f) / (float)scale - 0.5f;
+  o.cy = (s.cy + 0.5f) / (float)scale - 0.5f;
+  return o;
+}
+
+DTsdf dtsdf(const dyn_tsdf_params& p) {
+  DTsdf t;
+  t.vs = p.voxel_size;
+  t.bsm = (float)p.block_size * p.voxel_size;  // tsdf.cu:437-438
+  t.trunc = p.truncation_distance;
+  t.dmin = p.min_sensor_depth;
+  t.dmax = p.max_sensor_depth;
+  t.num_buckets = p.num_buckets;
+  t.bucket_size = p.bucket_size;
+  t.num_blocks = p.num_blocks;
+  t.max_w = p.max_sdf_weight;
+  double bs = (double)p.block_size * (double)p.voxel_size;
+  t.dda_cap = 3 * (int)std::ceil(((double)p.max_sensor_depth + (double)p.truncation_distance) / bs) + 8;
+  double step = std::min((double)p.voxel_size, (double)p.truncation_distance);
+  t.rc_cap = (int)std::ceil((double)p.max_sensor_depth / step) + 4;
+  return t;
+}
+
+#define DYN_CUDA(x)                                  \
+  do {                                               \
+    cudaError_t e_ = (x);                            \
+    if (e_ != cudaSuccess) {                         \
+      if (e_ == cudaErrorMemoryAllocation) return DYN_ERR_OOM; \
+      return DYN_ERR_CUDA;                           \
+    }                                                \
+  } while (0)
+
+bool valid_sensor(const dyn_sensor* s) {
+  return s && s->rows > 0 && s->cols > 0 && s->rows <= 8192 && s->cols <= 8192 &&
+         s->fx > 0 && s->fy > 0 && s->depth_scaler > 0;
+}
+
+}  // namespace
+
+struct dyn_session {
+  int device = 0;
+  dyn_tsdf_params tp;
+  dyn_gn_params gp;
+  dyn_bilateral_params bp;
+  dyn_sensor sensor;
+  int precision = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t h2d_done = nullptr;
+  DSensor ls[kLevels];
+  int nlev = 1;
+  size_t npx = 0;
+  // device buffers
+  std::vector<void*> allocs;
+  uint16_t* d_u16 = nullptr;
+  uint8_t* d_rgb = nullptr;
+  float* d_raw = nullptr;
+  float* d_filt = nullptr;
+  float* d_sdep[kLevels] = {};
+  float4* d_snrm[kLevels] = {};
+  float4* d_svtx[kLevels] = {};
+  float* d_sint[kLevels] = {};
+  float* d_tdep[kLevels] = {};
+  float4* d_tnrm[kLevels] = {};
+  float4* d_tvtx[kLevels] = {};
+  float* d_tint[kLevels] = {};
+  float* d_ray = nullptr;
+  uint8_t* d_trgb = nullptr;
+  float* d_pose_override = nullptr;
+  double* d_pose_in = nullptr;
+  double* d_partials = nullptr;
+  IcpState* d_icp = nullptr;
+  PoseState* d_pose = nullptr;
+  VolumeDev vol;
+  // host
+  uint16_t* h_depth = nullptr;
+  uint8_t* h_rgb = nullptr;
+  ResultBlock* h_res = nullptr;
+  // graphs: [has_rgb]
+  cudaGraphExec_t exec[2] = {nullptr, nullptr};
+  bool debug_maps = false;
+  int frames = 0;
+  bool pending = false;
+
+  template <class T>
+  dyn_status dalloc(T** p, size_t bytes) {
+    void* q = nullptr;
+    bytes = (bytes + 255) / 256 * 256;  // whole 16-byte vectors at the tail
+    cudaError_t e = cudaMalloc(&q, bytes < 256 ? 256 : bytes);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return e == cudaErrorMemoryAllocation ? DYN_ERR_OOM : DYN_ERR_CUDA;
+    }
+    allocs.push_back(q);
+    *p = (T*)q;
+    return DYN_OK;
+  }
+  bool use_color() const { return gp.color_weight != 0.0f; }
+  IcpParams icp_params() const {
+    IcpParams P;
+    P.dmin = gp.icp_min_depth;
+    P.dmax = gp.icp_max_depth;
+    P.cos_thr = gp.normal_cos_thresh;
+    P.cw = gp.color_weight;
+    P.min_inc = gp.min_increment;
+    P.max_inc = gp.max_increment;
+    P.reg = gp.regularization;
+    P.compose_left = gp.compose_left;
+    P.kahan = precision == DYN_PRECISION_MIXED ? 1 : 0;
+    return P;
+  }
+};
+
+namespace {
+
+void release(dyn_session* s) {
+  if (!s) return;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(s->device);
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  for (int k = 0; k < 2; ++k)
+    if (s->exec[k]) cudaGraphExecDestroy(s->exec[k]);
+  for (void* p : s->allocs) cudaFree(p);
+  if (s->h_depth) cudaFreeHost(s->h_depth);
+  if (s->h_rgb) cudaFreeHost(s->h_rgb);
+  if (s->h_res) cudaFreeHost(s->h_res);
+  if (s->h2d_done) cudaEventDestroy(s->h2d_done);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  cudaSetDevice(prev);
+  delete s;
+}
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+void reset_frame_counters(dyn_session* s) {
+  // every counter but nalloc (the heap top persists)
+  cudaMemsetAsync(reinterpret_cast<char*>(s->vol.cnt) + sizeof(int), 0,
+                  sizeof(Counters) - sizeof(int), s->stream);
+}
+
+MapsArgs maps_args(dyn_session* s, bool target) {
+  MapsArgs a;
+  int off = 0;
+  for (int l = 0; l < s->nlev; ++l) {
+    a.lv[l].depth = target ? s->d_tdep[l] : s->d_sdep[l];
+    a.lv[l].normal = target ? s->d_tnrm[l] : s->d_snrm[l];
+    a.lv[l].vertex = s->debug_maps ? (target ? s->d_tvtx[l] : s->d_svtx[l]) : nullptr;
+    a.lv[l].s = s->ls[l];
+    a.lv[l].offset = off;
+    off += s->ls[l].rows * s->ls[l].cols;
+  }
+  a.nlev = s->nlev;
+  a.total = off;
+  return a;
+}
+
+__global__ void mark_target_kernel(IcpState* st) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) st->have_target = 1;
+}
+__global__ void bump_frame_kernel(PoseState* ps) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) ps->frame += 1;
+}
+
+// Source side of a frame: ingest, bilateral filter, pyramid, normal maps.
+void enqueue_source(dyn_session* s, bool has_rgb) {
+  cudaStream_t st = s->stream;
+  const int n = (int)s->npx;
+  const bool col = s->use_color();
+  launch_ingest(s->d_u16, has_rgb ? s->d_rgb : nullptr, n, s->sensor.depth_scaler, s->d_raw,
+                col ? s->d_sint[0] : nullptr, st);
+  if (s->bp.enabled)
+    launch_bilateral(s->d_raw, s->d_filt, (int)s->sensor.rows, (int)s->sensor.cols,
+                     s->bp.diameter, s->bp.sigma_i, s->bp.sigma_s, st);
+  else
+    launch_copy_f(s->d_raw, s->d_filt, s->npx, st);
+  for (int l = 1; l < s->nlev; ++l) {
+    launch_downsample_depth(s->d_sdep[l - 1], s->ls[l - 1].rows, s->ls[l - 1].cols, s->d_sdep[l], st);
+    if (col)
+      launch_downsample_intensity(s->d_sint[l - 1], s->ls[l - 1].rows, s->ls[l - 1].cols,
+                                  s->d_sint[l], st);
+  }
+  launch_maps(maps_args(s, false), st);
+}
+
+// Integration at the session pose, then the next frame's target.
+void enqueue_map_update(dyn_session* s, bool has_rgb) {
+  cudaStream_t st = s->stream;
+  launch_allocate(s->vol, s->d_raw, s->ls[0], s->d_pose, st);
+  launch_visible(s->vol, s->ls[0], s->d_pose, st);
+  launch_integrate(s->vol, s->d_raw, has_rgb ? s->d_rgb : nullptr, s->ls[0], s->d_pose, st);
+  const bool col = s->use_color();
+  if (s->gp.mode == 1) {
+    launch_raycast(s->vol, s->ls[0], s->d_pose, nullptr, s->d_ray, col ? s->d_trgb : nullptr, st);
+    launch_target_prepare(s->d_ray, s->d_tdep[0], s->tp.max_sensor_depth,
+                          col ? s->d_trgb : nullptr, col ? s->d_tint[0] : nullptr, (int)s->npx, st);
+    for (int l = 1; l < s->nlev; ++l) {
+      launch_downsample_depth(s->d_tdep[l - 1], s->ls[l - 1].rows, s->ls[l - 1].cols,
+                              s->d_tdep[l], st);
+      if (col)
+        launch_downsample_intensity(s->d_tint[l - 1], s->ls[l - 1].rows, s->ls[l - 1].cols,
+                                    s->d_tint[l], st);
+    }
+    launch_maps(maps_args(s, true), st);
+  } else {
+    for (int l = 0; l < s->nlev; ++l) {
+      size_t n = (size_t)s->ls[l].rows * s->ls[l].cols;
+      launch_copy_f(s->d_sdep[l], s->d_tdep[l], n, st);
+      launch_copy_f(reinterpret_cast<const float*>(s->d_snrm[l]),
+                    reinterpret_cast<float*>(s->d_tnrm[l]), 4 * n, st);
+      if (col) launch_copy_f(s->d_sint[l], s->d_tint[l], n, st);
+    }
+  }
+  mark_target_kernel<<<1, 32, 0, st>>>(s->d_icp);
+}
+
+// builder::buildModelLS with the intended order: track frame k against the
+// target of frame k-1, integrate frame k at the new pose, raycast the target
+// for frame k+1.
+void enqueue_frame(dyn_session* s, bool has_rgb) {
+  cudaStream_t st = s->stream;
+  reset_frame_counters(s);
+  enqueue_source(s, has_rgb);
+  IcpParams P = s->icp_params();
+  for (int pl = 0; pl < 3; ++pl) {
+    int l = level_of_scale(s->gp.lvl_scale[pl]);
+    IcpLevel L;
+    L.sd = s->d_sdep[l];
+    L.sn = s->d_snrm[l];
+    L.si = s->d_sint[l];
+    L.td = s->d_tdep[l];
+    L.tn = s->d_tnrm[l];
+    L.ti = s->d_tint[l];
+    L.s = s->ls[l];
+    for (int it = 1; it < s->gp.lvl_iteration_num[pl]; ++it)
+      launch_icp_iteration(L, P, pl, it, s->d_icp, s->d_partials, st);
+  }
+  launch_pose_finalize(P, s->d_icp, s->d_pose, st);
+  bump_frame_kernel<<<1, 32, 0, st>>>(s->d_pose);
+  enqueue_map_update(s, has_rgb);
+}
+
+dyn_status build_graph(dyn_session* s, bool has_rgb) {
+  cudaGraph_t g = nullptr;
+  DYN_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+  enqueue_frame(s, has_rgb);
+  cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+  if (e != cudaSuccess) return DYN_ERR_CUDA;
+  cudaGraphExec_t ex = nullptr;
+  e = cudaGraphInstantiate(&ex, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return DYN_ERR_CUDA;
+  s->exec[has_rgb ? 1 : 0] = ex;
+  return DYN_OK;
+}
+
+bool is_pinned(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+dyn_status upload_frame(dyn_session* s, const uint16_t* depth, const uint8_t* rgb) {
+  size_t nd = s->npx * sizeof(uint16_t), nc = s->npx * 3;
+  // the staging buffers may still feed the previous frame's copies
+  DYN_CUDA(cudaEventSynchronize(s->h2d_done));
+  if (is_pinned(depth)) {
+    DYN_CUDA(cudaMemcpyAsync(s->d_u16, depth, nd, cudaMemcpyHostToDevice, s->stream));
+  } else {
+    std::memcpy(s->h_depth, depth, nd);
+    DYN_CUDA(cudaMemcpyAsync(s->d_u16, s->h_depth, nd, cudaMemcpyHostToDevice, s->stream));
+  }
+  if (rgb) {
+    if (is_pinned(rgb)) {
+      DYN_CUDA(cudaMemcpyAsync(s->d_rgb, rgb, nc, cudaMemcpyHostToDevice, s->stream));
+    } else {
+      std::memcpy(s->h_rgb, rgb, nc);
+      DYN_CUDA(cudaMemcpyAsync(s->d_rgb, s->h_rgb, nc, cudaMemcpyHostToDevice, s->stream));
+    }
+  }
+  DYN_CUDA(cudaEventRecord(s->h2d_done, s->stream));
+  return DYN_OK;
+}
+
+dyn_status launch_frame(dyn_session* s, bool has_rgb) {
+  int k = has_rgb ? 1 : 0;
+  if (!s->exec[k]) {
+    dyn_status r = build_graph(s, has_rgb);
+    if (r != DYN_OK) return r;
+  }
+  DYN_CUDA(cudaGraphLaunch(s->exec[k], s->stream));
+  DYN_CUDA(cudaMemcpyAsync(s->h_res, s->d_pose, sizeof(PoseState), cudaMemcpyDeviceToHost, s->stream));
+  DYN_CUDA(cudaMemcpyAsync(&s->h_res->icp, s->d_icp, sizeof(IcpState), cudaMemcpyDeviceToHost, s->stream));
+  DYN_CUDA(cudaMemcpyAsync(&s->h_res->cnt, s->vol.cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s->stream));
+  s->pending = true;
+  s->frames++;
+  return DYN_OK;
+}
+
+void fill_stats(const dyn_session* s, const ResultBlock& r, dyn_frame_stats* st) {
+  std::memset(st, 0, sizeof(*st));
+  st->frame_index = r.pose.frame - 1;
+  for (int k = 0; k < 3; ++k) {
+    st->icp_iterations[k] = r.icp.iters[k];
+    st->icp_inliers[k] = r.icp.inliers[k];
+    st->icp_rms[k] = r.icp.rms[k];
+  }
+  st->icp_reset = r.pose.reset;
+  st->blocks_total = std::min(r.cnt.nalloc, s->tp.num_blocks);
+  st->blocks_new = r.cnt.new_blocks;
+  st->blocks_visible = r.cnt.visible;
+  st->unique_blocks_probed = r.cnt.unique_probed;
+  st->bucket_full = r.cnt.bucket_full;
+  st->heap_exhausted = r.cnt.heap_exhausted;
+  st->dda_overruns = r.cnt.dda_overruns;
+  st->raycast_overruns = r.cnt.raycast_overruns;
+  for (int k = 0; k < 6; ++k) st->pose_increment[k] = r.pose.last_inc[k];
+}
+
+dyn_status reset_state(dyn_session* s) {
+  cudaStream_t st = s->stream;
+  launch_volume_clear(s->vol, st);
+  IcpState z;
+  std::memset(&z, 0, sizeof(z));
+  for (int k = 0; k < 16; ++k) z.T[k] = (k % 5 == 0) ? 1.0f : 0.0f;
+  DYN_CUDA(cudaMemcpyAsync(s->d_icp, &z, sizeof(z), cudaMemcpyHostToDevice, st));
+  PoseState p;
+  std::memset(&p, 0, sizeof(p));
+  DYN_CUDA(cudaMemcpyAsync(s->d_pose, &p, sizeof(p), cudaMemcpyHostToDevice, st));
+  double I[16];
+  for (int k = 0; k < 16; ++k) I[k] = (k % 5 == 0) ? 1.0 : 0.0;
+  DYN_CUDA(cudaMemcpyAsync(s->d_pose_in, I, sizeof(I), cudaMemcpyHostToDevice, st));
+  launch_pose_set(s->d_pose, s->d_pose_in, st);
+  DYN_CUDA(cudaStreamSynchronize(st));
+  s->frames = 0;
+  s->pending = false;
+  return DYN_OK;
+}
+
+size_t session_bytes(const dyn_tsdf_params& t, const dyn_sensor& s) {
+  size_t n = (size_t)s.rows * s.cols;
+  size_t b = 0;
+  b += sizeof(Entry) * (size_t)t.num_buckets * t.bucket_size;
+  b += sizeof(unsigned long long) * (size_t)t.num_blocks;
+  b += sizeof(dyn_voxel) * (size_t)t.num_blocks * kBlockVox;
+  b += sizeof(int) * (size_t)t.num_blocks;
+  b += n * (2 + 3 + 4 + 4 + 4 + 3);  // inputs, raw, filtered, ray depth, target rgb
+  b += 2 * n * (4 + 16 + 16 + 4) * 4 / 3;  // source + target pyramids
+  b += icp_scratch_bytes() + 4096;
+  return b;
+}
+
+// Per-device scratch of the stage entry points (allocated on first use).
+struct StageScratch {
+  double* partials = nullptr;
+  unsigned int* ticket = nullptr;
+  double* out = nullptr;
+  float* T = nullptr;
+};
+std::mutex g_stage_mu;
+StageScratch g_stage[64];
+
+}  // namespace
+
+extern "C" {
+
+int32_t dyn_abi_version(void) { return DYN_ABI_VERSION; }
+
+const char* dyn_status_string(dyn_status s) {
+  switch (s) {
+    case DYN_OK: return "ok";
+    case DYN_ERR_INVALID_ARG: return "invalid argument";
+    case DYN_ERR_OOM: return "out of device memory";
+    case DYN_ERR_BUDGET_EXCEEDED: return "memory budget exceeded";
+    case DYN_ERR_HASH_FULL: return "hash bucket full";
+    case DYN_ERR_HEAP_EXHAUSTED: return "voxel block heap exhausted";
+    case DYN_ERR_ICP_DIVERGED: return "icp diverged";
+    case DYN_ERR_TIMEOUT: return "timeout";
+    case DYN_ERR_CUDA: return "cuda error";
+    case DYN_ERR_NOT_READY: return "not ready";
+    case DYN_ERR_NO_DEVICE: return "no cuda device";
+  }
+  return "unknown";
+}
+
+dyn_status dyn_session_bytes(const dyn_tsdf_params* tsdf, const dyn_sensor* sensor,
+                             int32_t precision, size_t* bytes_out) {
+  (void)precision;
+  if (!tsdf || !valid_sensor(sensor) || !bytes_out) return DYN_ERR_INVALID_ARG;
+  *bytes_out = session_bytes(*tsdf, *sensor);
+  return DYN_OK;
+}
+
+dyn_status dyn_session_create(const dyn_tsdf_params* tsdf, const dyn_gn_params* gn,
+                              const dyn_bilateral_params* bil, const dyn_sensor* sensor,
+                              int32_t precision, int32_t device, dyn_session** out) {
+  if (!out) return DYN_ERR_INVALID_ARG;
+  *out = nullptr;
+  if (!tsdf || !gn || !bil || !valid_sensor(sensor)) return DYN_ERR_INVALID_ARG;
+  if (tsdf->block_size != kBlockSize || tsdf->bucket_size < 1 || tsdf->num_buckets < 1 ||
+      tsdf->num_blocks < 1 || tsdf->max_sdf_weight < 1 || tsdf->max_sdf_weight > 255 ||
+      !(tsdf->voxel_size > 0) || !(tsdf->truncation_distance > 0) ||
+      !(tsdf->max_sensor_depth > 0))
+    return DYN_ERR_INVALID_ARG;
+  if ((int64_t)tsdf->num_buckets * tsdf->bucket_size > (int64_t)1 << 30) return DYN_ERR_INVALID_ARG;
+  for (int k = 0; k < 3; ++k) {
+    int sc = gn->lvl_scale[k];
+    if (sc != 1 && sc != 2 && sc != 4 && sc != 8) return DYN_ERR_INVALID_ARG;
+    if (gn->lvl_iteration_num[k] < 0 || gn->lvl_iteration_num[k] > 1000) return DYN_ERR_INVALID_ARG;
+    if ((int)(sensor->rows / sc) < 3 || (int)(sensor->cols / sc) < 5) return DYN_ERR_INVALID_ARG;
+  }
+  if (bil->enabled && (bil->diameter < 1 || bil->diameter > 16 || !(bil->sigma_s > 0) ||
+                       !(bil->sigma_i > 0)))
+    return DYN_ERR_INVALID_ARG;
+  if (gn->mode != 0 && gn->mode != 1) return DYN_ERR_INVALID_ARG;
+  if (precision != DYN_PRECISION_FP32 && precision != DYN_PRECISION_MIXED) return DYN_ERR_INVALID_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return DYN_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= ndev) return DYN_ERR_INVALID_ARG;
+  DeviceGuard dg(device);
+  dyn_session* s = new (std::nothrow) dyn_session();
+  if (!s) return DYN_ERR_OOM;
+  s->device = device;
+  s->tp = *tsdf;
+  s->gp = *gn;
+  s->bp = *bil;
+  s->sensor = *sensor;
+  s->precision = precision;
+  s->npx = (size_t)sensor->rows * sensor->cols;
+  int maxl = 0;
+  for (int k = 0; k < 3; ++k) maxl = std::max(maxl, level_of_scale(gn->lvl_scale[k]));
+  s->nlev = maxl + 1;
+  for (int l = 0; l < kLevels; ++l) s->ls[l] = dsensor(level_sensor(*sensor, 1 << l));
+  dyn_status r = DYN_OK;
+#define TRY(x)               \
+  do {                       \
+    r = (x);                 \
+    if (r != DYN_OK) {       \
+      release(s);            \
+      return r;              \
+    }                        \
+  } while (0)
+  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&s->h2d_done, cudaEventDisableTiming) != cudaSuccess) {
+    release(s);
+    return DYN_ERR_CUDA;
+  }
+  size_t n = s->npx;
+  TRY(s->dalloc(&s->d_u16, n * 2));
+  TRY(s->dalloc(&s->d_rgb, n * 3));
+  TRY(s->dalloc(&s->d_raw, n * 4));
+  TRY(s->dalloc(&s->d_filt, n * 4));
+  TRY(s->dalloc(&s->d_ray, n * 4));
+  TRY(s->dalloc(&s->d_trgb, n * 3));
+  for (int l = 0; l < s->nlev; ++l) {
+    size_t m = (size_t)s->ls[l].rows * s->ls[l].cols;
+    size_t m4 = (m + 3) / 4 * 4;
+    if (l == 0) s->d_sdep[0] = s->d_filt;
+    else TRY(s->dalloc(&s->d_sdep[l], m4 * 4));
+    TRY(s->dalloc(&s->d_snrm[l], m * 16));
+    TRY(s->dalloc(&s->d_svtx[l], m * 16));
+    TRY(s->dalloc(&s->d_sint[l], m4 * 4));
+    TRY(s->dalloc(&s->d_tdep[l], m4 * 4));
+    TRY(s->dalloc(&s->d_tnrm[l], m * 16));
+    TRY(s->dalloc(&s->d_tvtx[l], m * 16));
+    TRY(s->dalloc(&s->d_tint[l], m4 * 4));
+  }
+  TRY(s->dalloc(&s->d_pose_override, 64));
+  TRY(s->dalloc(&s->d_pose_in, 128));
+  TRY(s->dalloc(&s->d_partials, icp_scratch_bytes()));
+  TRY(s->dalloc(&s->d_icp, sizeof(IcpState)));
+  TRY(s->dalloc(&s->d_pose, sizeof(PoseState)));
+  s->vol.t = dtsdf(*tsdf);
+  TRY(s->dalloc(&s->vol.entries, sizeof(Entry) * (size_t)tsdf->num_buckets * tsdf->bucket_size));
+  TRY(s->dalloc(&s->vol.block_keys, sizeof(unsigned long long) * (size_t)tsdf->num_blocks));
+  TRY(s->dalloc(&s->vol.voxels, sizeof(dyn_voxel) * (size_t)tsdf->num_blocks * kBlockVox));
+  TRY(s->dalloc(&s->vol.visible, sizeof(int) * (size_t)tsdf->num_blocks));
+  TRY(s->dalloc(&s->vol.cnt, sizeof(Counters)));
+  if (cudaMallocHost(&s->h_depth, n * 2) != cudaSuccess ||
+      cudaMallocHost(&s->h_rgb, n * 3) != cudaSuccess ||
+      cudaMallocHost(&s->h_res, sizeof(ResultBlock)) != cudaSuccess) {
+    cudaGetLastError();
+    release(s);
+    return DYN_ERR_OOM;
+  }
+  // zero the images so unused levels and borders read as invalid
+  for (int l = 0; l < s->nlev; ++l) {
+    size_t m = (size_t)s->ls[l].rows * s->ls[l].cols;
+    cudaMemsetAsync(s->d_tdep[l], 0, m * 4, s->stream);
+    cudaMemsetAsync(s->d_tnrm[l], 0, m * 16, s->stream);
+    cudaMemsetAsync(s->d_tint[l], 0, m * 4, s->stream);
+    cudaMemsetAsync(s->d_sint[l], 0, m * 4, s->stream);
+  }
+  cudaEventRecord(s->h2d_done, s->stream);
+  TRY(reset_state(s));
+#undef TRY
+  *out = s;
+  return DYN_OK;
+}
+
+dyn_status dyn_session_destroy(dyn_session* s) {
+  if (!s) return DYN_ERR_INVALID_ARG;
+  release(s);
+  return DYN_OK;
+}
+
+dyn_status dyn_session_reset(dyn_session* s) {
+  if (!s) return DYN_ERR_INVALID_ARG;
+  DeviceGuard dg(s->device);
+  DYN_CUDA(cudaStreamSynchronize(s->stream));
+  return reset_state(s);
+}
+
+dyn_status dyn_session_get_pose(dyn_session* s, float pose_out[16]) {
+  if (!s || !pose_out) return DYN_ERR_INVALID_ARG;
+  DeviceGuard dg(s->device);
+  PoseState p;
+  DYN_CUDA(cudaMemcpyAsync(&p, s->d_pose, sizeof(p), cudaMemcpyDeviceToHost, s->stream));
+  DYN_CUDA(cudaStreamSynchronize(s->stream));
+  for (int k = 0; k < 16; ++k) pose_out[k] = (float)p.pose[k];
+  return DYN_OK;
+}
+
+dyn_status dyn_session_set_pose(dyn_session* s, const float pose[16]) {
+  if (!s || !pose) return DYN_ERR_INVALID_ARG;
+  DeviceGuard dg(s->device);
+  double P[16];
+  for (int k = 0; k < 16; ++k) P[k] = (double)pose[k];
+  DYN_CUDA(cudaMemcpyAsync(s->d_pose_in, P, sizeof(P), cudaMemcpyHostToDevice, s->stream));
+  launch_pose_set(s->d_pose, s->d_pose_in, s->stream);
+  DYN_CUDA(cudaStreamSynchronize(s->stream));
+  return DYN_OK;
+}
+
+dyn_status dyn_frame_submit(dyn_session* s, const uint16_t* depth_host, const uint8_t* rgb_host) {
+  if (!s || !depth_host) return DYN_ERR_INVALID_ARG;
+  DeviceGuard dg(s->device);
+  dyn_status r = upload_frame(s, depth_host, rgb_host);
+  if (r != DYN_OK) return r;
+  return launch_frame(s, rgb_host != nullptr);
+}
+
+dyn_status dyn_frame_submit_device(dyn_session* s, const uint16_t* depth_dev, const uint8_t* rgb_dev) {
+  if (!s || !depth_dev) return DYN_ERR_INVALID_ARG;
+  DeviceGuard dg(s->device);
+  DYN_CUDA(cudaMemcpyAsync(s->d_u16, depth_dev, s->npx * 2, cudaMemcpyDeviceToDevice, s->stream));
+  if (rgb_dev)
+    DYN_CUDA(cudaMemcpyAsync(s->d_rgb, rgb_dev, s->npx * 3, cudaMemcpyDeviceToDevice, s->stream));
+  return launch_frame(s, rgb_dev != nullptr);
+}
+
+dyn_status dyn_frame_result(dyn_session* s, float pose_out[16], dyn_frame_stats* stats) {
+  if (!s) return DYN_ERR_INVALID_ARG;
+  if (!s->pending) return DYN_ERR_NOT_READY;
+  DeviceGuard dg(s->device);
+  DYN_CUDA(cudaStreamSynchronize(s->stream));
+  s->pending = false;
+  if (pose_out)
+    for (int k = 0; k < 16; ++k) pose_out[k] = (float)s->h_res->pose.pose[k];
+  if (stats) fill_stats(s, *s->h_res, stats);
+  const Counters& c = s->h_res->cnt;
+  if (c.heap_exhausted) return DYN_ERR_HEAP_EXHAUSTED;
+  if (c.bucket_full) return DYN_ERR_HASH_FULL;
+  return DYN_OK;
+}
+
+dyn_status dyn_integrate_with_pose(dyn_session* s, const uint16_t* depth_host,
+                                   const uint8_t* rgb_host, const float pose[16]) {
+  if (!s || !depth_host || !pose) return DYN_ERR_INVALID_ARG;
+  DeviceGuard dg(s->device);
+  dyn_status r = dyn_session_set_pose(s, pose);
+  if (r != DYN_OK) return r;
+  r = upload_frame(s, depth_host, rgb_host);
+  if (r != DYN_OK) return r;
+  reset_frame_counters(s);
+  enqueue_source(s, rgb_host != nullptr);
+  bump_frame_kernel<<<1, 32, 0, s->stream>>>(s->d_pose);
+  enqueue_map_update(s, rgb_host != nullptr);
+  DYN_CUDA(cudaMemcpyAsync(s->h_res, s->d_pose, sizeof(PoseState), cudaMemcpyDeviceToHost, s->stream));
+  DYN_CUDA(cudaMemcpyAsync(&s->h_res->cnt, s->vol.cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s->stream));
+  DYN_CUDA(cudaStreamSynchronize(s->stream));
+  DYN_CUDA(cudaGetLastError());
+  s->frames++;
+  const Counters& c = s->h_res->cnt;
+  if (c.heap_exhausted) return DYN_ERR_HEAP_EXHAUSTED;
+  if (c.bucket_full) return DYN_ERR_HASH_FULL;
+  return DYN_OK;
+}
+
+dyn_status dyn_raycast(dyn_session* s, const float pose[16], const dyn_sensor* virt,
+                       float* depth_host, uint8_t* rgb_host) {
+  if (!s || !pose || !depth_host) return DYN_ERR_INVALID_ARG;
+  dyn_sensor vs = virt ? *virt : s->sensor;
+  if (!valid_sensor(&vs) || (size_t)vs.rows * vs.cols > s->npx) return DYN_ERR_INVALID_ARG;
+  DeviceGuard dg(s->device);
+  DYN_CUDA(cudaMemcpyAsync(s->d_pose_override, pose, 64, cudaMemcpyHostToDevice, s->stream));
+  size_t n = (size_t)vs.rows * vs.cols;
+  launch_raycast(s->vol, dsensor(vs), s->d_pose, s->d_pose_override, s->d_ray,
+                 rgb_host ? s->d_trgb : nullptr, s->stream);
+  DYN_CUDA(cudaGetLastError());
+  DYN_CUDA(cudaMemcpyAsync(depth_host, s->d_ray, n * 4, cudaMemcpyDeviceToHost, s->stream));
+  if (rgb_host)
+    DYN_CUDA(cudaMemcpyAsync(rgb_host, s->d_trgb, n * 3, cudaMemcpyDeviceToHost, s->stream));
+  DYN_CUDA(cudaStreamSynchronize(s->stream));
+  return DYN_OK;
+}
+
+dyn_status dyn_num_blocks(dyn_session* s, int64_t* n_out) {
+  if (!s || !n_out) return DYN_ERR_INVALID_ARG;
+  DeviceGuard dg(s->device);
+  int n = 0;
+  DYN_CUDA(cudaMemcpyAsync(&n, &s->vol.cnt->nalloc, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  DYN_CUDA(cudaStreamSynchronize(s->stream));
+  *n_out = std::min(n, s->tp.num_blocks);
+  return DYN_OK;
+}
+
+dyn_status dyn_download_blocks(dyn_session* s, int32_t* coords_out, dyn_voxel* voxels_out,
+                               int64_t capacity, int64_t* n_out) {
+  if (!s || !n_out || capacity < 0) return DYN_ERR_INVALID_ARG;
+  int64_t n = 0;
+  dyn_status r = dyn_num_blocks(s, &n);
+  if (r != DYN_OK) return r;
+  *n_out = n;
+  int64_t m = std::min(n, capacity);
+  if (m == 0) return DYN_OK;
+  DeviceGuard dg(s->device);
+  if (coords_out) {
+    std::vector<unsigned long long> keys((size_t)m);
+    DYN_CUDA(cudaMemcpyAsync(keys.data(), s->vol.block_keys, sizeof(unsigned long long) * m,
+                             cudaMemcpyDeviceToHost, s->stream));
+    DYN_CUDA(cudaStreamSynchronize(s->stream));
+    for (int64_t i = 0; i < m; ++i) {
+      coords_out[3 * i] = key_x(keys[i]);
+      coords_out[3 * i + 1] = key_y(keys[i]);
+      coords_out[3 * i + 2] = key_z(keys[i]);
+    }
+  }
+  if (voxels_out) {
+    DYN_CUDA(cudaMemcpyAsync(voxels_out, s->vol.voxels, sizeof(dyn_voxel) * kBlockVox * m,
+                             cudaMemcpyDeviceToHost, s->stream));
+    DYN_CUDA(cudaStreamSynchronize(s->stream));
+  }
+  return DYN_OK;
+}
+
+dyn_status dyn_debug_image(dyn_session* s, int32_t which, int32_t level, void* host_out,
+                           size_t bytes) {
+  if (!s || !host_out || level < 0 || level >= s->nlev) return DYN_ERR_INVALID_ARG;
+  DeviceGuard dg(s->device);
+  size_t m = (size_t)s->ls[level].rows * s->ls[level].cols;
+  const void* src = nullptr;
+  size_t nb = 0;
+  switch (which) {
+    case 0: src = s->d_raw; nb = s->npx * 4; break;
+    case 1: src = s->d_filt; nb = s->npx * 4; break;
+    case 2: src = s->d_sdep[level]; nb = m * 4; break;
+    case 3: src = s->d_svtx[level]; nb = m * 16; break;
+    case 4: src = s->d_snrm[level]; nb = m * 16; break;
+    case 5: src = s->d_tdep[level]; nb = m * 4; break;
+    case 6: src = s->d_tvtx[level]; nb = m * 16; break;
+    case 7: src = s->d_tnrm[level]; nb = m * 16; break;
+    case 8: src = s->d_trgb; nb = s->npx * 3; break;
+    case 9: src = s->d_sint[level]; nb = m * 4; break;
+    case 10: src = s->d_tint[level]; nb = m * 4; break;
+    default: return DYN_ERR_INVALID_ARG;
+  }
+  if (bytes < nb) return DYN_ERR_INVALID_ARG;
+  if ((which == 3 || which == 6) && !s->debug_maps) {
+    // vertex maps are only written in debug mode: recompute them now
+    s->debug_maps = true;
+    launch_maps(maps_args(s, which == 6), s->stream);
+    s->debug_maps = false;
+  }
+  DYN_CUDA(cudaMemcpyAsync(host_out, src, nb, cudaMemcpyDeviceToHost, s->stream));
+  DYN_CUDA(cudaStreamSynchronize(s->stream));
+  return DYN_OK;
+}
+
+dyn_status dyn_bilateral_filter(const float* depth_dev, float* out_dev, uint32_t rows, uint32_t cols,
+                                const dyn_bilateral_params* p, void* stream) {
+  if (!depth_dev || !out_dev || !p || rows == 0 || cols == 0 || p->diameter < 1 ||
+      p->diameter > 16 || !(p->sigma_i > 0) || !(p->sigma_s > 0))
+    return DYN_ERR_INVALID_ARG;
+  launch_bilateral(depth_dev, out_dev, (int)rows, (int)cols, p->diameter, p->sigma_i, p->sigma_s,
+                   (cudaStream_t)stream);
+  DYN_CUDA(cudaGetLastError());
+  return DYN_OK;
+}
+
+dyn_status dyn_depth_to_maps(const float* depth_dev, const dyn_sensor* level, float* vertex4_dev,
+                             float* normal4_dev, void* stream) {
+  if (!depth_dev || !valid_sensor(level) || !normal4_dev) return DYN_ERR_INVALID_ARG;
+  MapsArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.lv[0].depth = depth_dev;
+  a.lv[0].normal = reinterpret_cast<float4*>(normal4_dev);
+  a.lv[0].vertex = reinterpret_cast<float4*>(vertex4_dev);
+  a.lv[0].s = dsensor(*level);
+  a.lv[0].offset = 0;
+  a.nlev = 1;
+  a.total = (int)(level->rows * level->cols);
+  launch_maps(a, (cudaStream_t)stream);
+  DYN_CUDA(cudaGetLastError());
+  return DYN_OK;
+}
+
+dyn_status dyn_icp_normal_equations(const float* src_depth_dev, const float* src_normal4_dev,
+                                    const float* src_intensity_dev, const float* tgt_depth_dev,
+                                    const float* tgt_normal4_dev, const float* tgt_intensity_dev,
+                                    const dyn_sensor* level, const dyn_gn_params* gn,
+                                    const float T[16], double out_host[29], void* stream) {
+  if (!src_depth_dev || !src_normal4_dev || !tgt_depth_dev || !tgt_normal4_dev ||
+      !valid_sensor(level) || !gn || !T || !out_host)
+    return DYN_ERR_INVALID_ARG;
+  if (gn->color_weight != 0.0f && (!src_intensity_dev || !tgt_intensity_dev))
+    return DYN_ERR_INVALID_ARG;
+  int dev = 0;
+  DYN_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return DYN_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(g_stage_mu);
+  StageScratch& sc = g_stage[dev];
+  if (!sc.partials) {
+    DYN_CUDA(cudaMalloc(&sc.partials, icp_scratch_bytes()));
+    DYN_CUDA(cudaMalloc(&sc.ticket, 256));
+    DYN_CUDA(cudaMemset(sc.ticket, 0, 256));
+    DYN_CUDA(cudaMalloc(&sc.out, 256));
+    DYN_CUDA(cudaMalloc(&sc.T, 64));
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  IcpLevel L;
+  L.sd = src_depth_dev;
+  L.sn = reinterpret_cast<const float4*>(src_normal4_dev);
+  L.si = src_intensity_dev;
+  L.td = tgt_depth_dev;
+  L.tn = reinterpret_cast<const float4*>(tgt_normal4_dev);
+  L.ti = tgt_intensity_dev;
+  L.s = dsensor(*level);
+  IcpParams P;
+  P.dmin = gn->icp_min_depth;
+  P.dmax = gn->icp_max_depth;
+  P.cos_thr = gn->normal_cos_thresh;
+  P.cw = gn->color_weight;
+  P.min_inc = gn->min_increment;
+  P.max_inc = gn->max_increment;
+  P.reg = gn->regularization;
+  P.compose_left = gn->compose_left;
+  P.kahan = 0;
+  DYN_CUDA(cudaMemcpyAsync(sc.T, T, 64, cudaMemcpyHostToDevice, st));
+  launch_icp_reduce_only(L, P, sc.T, sc.partials, sc.ticket, sc.out, st);
+  DYN_CUDA(cudaGetLastError());
+  DYN_CUDA(cudaMemcpyAsync(out_host, sc.out, sizeof(double) * kIcpVals, cudaMemcpyDeviceToHost, st));
+  DYN_CUDA(cudaStreamSynchronize(st));
+  return DYN_OK;
+}
+
+dyn_status dyn_sessions_submit(dyn_session* const* sessions, int32_t n,
+                               const uint16_t* const* depth_host,
+                               const uint8_t* const* rgb_host) {
+  if (!sessions || n < 0 || !depth_host) return DYN_ERR_INVALID_ARG;
+  for (int i = 0; i < n; ++i) {
+    dyn_status r = dyn_frame_submit(sessions[i], depth_host[i], rgb_host ? rgb_host[i] : nullptr);
+    if (r != DYN_OK) return r;
+  }
+  return DYN_OK;
+}
+
+}  // extern "C"

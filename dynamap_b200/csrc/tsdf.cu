@@ -1,0 +1,519 @@
+// tsdf.cu -- voxel-hashed TSDF kernels.
+//
+// Reference: include/geometry/tsdf/tsdf.cu (integration :268-344, allocation
+// :346-453, raycast :471-526, voxel addressing :47-239),
+// include/dataStructure/hashTable/hashTable.cu (:80-163),
+// include/geometry/geom_Types.h (Voxel merge :79-103).
+//
+// Layout in HBM (per session): a bucketed hash of 16-byte entries
+// {u64 packed block key, i32 heap index, i32 frame stamp}; a heap-index ->
+// key array; voxels as 8-byte {r,g,b,w,f32 sdf} (the reference's Voxel),
+// 512 per block in x-major order, so one block is 4 KB contiguous.
+#include "tsdf.cuh"
+
+namespace dyn {
+
+namespace {
+
+// ------------------------------------------------------------ allocation
+constexpr int kAllocT = 16;          // 16x16 pixel tile per CTA
+constexpr int kSetSlots = 2048;      // CTA-local dedup set (16 KB)
+constexpr int kSetProbes = 32;
+
+__device__ inline unsigned set_hash(unsigned long long k) {
+  return (unsigned)((k * 0x9E3779B97F4A7C15ull) >> 53) & (kSetSlots - 1);
+}
+
+struct AllocSmem {
+  unsigned long long set[kSetSlots];
+  int claim_entry[kSetSlots];
+  int nclaims;
+  int base;
+  int new_blocks, bucket_full, heap_exhausted, unique, overruns;
+};
+
+// Lock-free unique insert into the key's bucket (the set semantics of
+// HashTable::AllocateBlock, hashTable.cu:80-110, without its duplicate-
+// insert race): scan the bucket in slot order, claim the first empty slot by
+// CAS on the key; a lost CAS re-reads the slot.  Slots are claimed in order
+// and never freed, so occupied slots form a prefix of the bucket.  Returns
+// the entry index if this call claimed it (heap index assigned later), -1
+// if the key was present, -2 if the bucket is full.
+__device__ inline int bucket_insert(Entry* entries, const DTsdf& t, unsigned long long key,
+                                    int stamp, int* unique) {
+  int b = hash_slot(key_x(key), key_y(key), key_z(key), t.num_buckets, t.bucket_size);
+  for (int i = 0; i < t.bucket_size; ++i) {
+    Entry* e = entries + b + i;
+    unsigned long long cur = *(volatile unsigned long long*)&e->key;
+    if (cur == kEmptyKey) {
+      cur = atomicCAS(&e->key, kEmptyKey, key);
+      if (cur == kEmptyKey) {
+        atomicExch(&e->stamp, stamp);
+        atomicAdd(unique, 1);
+        return b + i;
+      }
+    }
+    if (cur == key) {
+      if (atomicExch(&e->stamp, stamp) != stamp) atomicAdd(unique, 1);
+      return -1;
+    }
+  }
+  return -2;
+}
+
+// AllocateFromDepthKernel (tsdf.cu:346-453) for one pixel: the reference's
+// DDA over blocks, exact FP32 (this file is built with -fmad=false), with
+// the 'diff' pre-step for negative directions and the step cap.
+template <class F>
+__device__ inline bool dda_ray(F3 start_pt, F3 point, float trunc, float block_size, int cap,
+                               F&& visit) {
+  F3 dir = normalize3(point - start_pt);
+  float surface_distance = norm3(start_pt - point);
+  F3 ray_start = start_pt;
+  F3 ray_end = start_pt + dir * (surface_distance + trunc);
+  int bpx = (int)floorf(ray_start.x / block_size);
+  int bpy = (int)floorf(ray_start.y / block_size);
+  int bpz = (int)floorf(ray_start.z / block_size);
+  int ebx = (int)floorf(ray_end.x / block_size);
+  int eby = (int)floorf(ray_end.y / block_size);
+  int ebz = (int)floorf(ray_end.z / block_size);
+  int sx = (dir.x > 0) - (dir.x < 0), sy = (dir.y > 0) - (dir.y < 0),
+      sz = (dir.z > 0) - (dir.z < 0);
+  const float FMAX = 3.402823466e+38f;
+  float dtx = dir.x != 0 ? fabsf(block_size / dir.x) : FMAX;
+  float dty = dir.y != 0 ? fabsf(block_size / dir.y) : FMAX;
+  float dtz = dir.z != 0 ? fabsf(block_size / dir.z) : FMAX;
+  float bdx = ((float)bpx + (float)sx) * block_size;
+  float bdy = ((float)bpy + (float)sy) * block_size;
+  float bdz = ((float)bpz + (float)sz) * block_size;
+  float mx = dir.x != 0 ? (bdx - ray_start.x) / dir.x : FMAX;
+  float my = dir.y != 0 ? (bdy - ray_start.y) / dir.y : FMAX;
+  float mz = dir.z != 0 ? (bdz - ray_start.z) / dir.z : FMAX;
+  int dx = 0, dy = 0, dz = 0;
+  bool neg = false;
+  if (bpx != ebx && dir.x < 0) { dx--; neg = true; }
+  if (bpy != eby && dir.y < 0) { dy--; neg = true; }
+  if (bpz != ebz && dir.z < 0) { dz--; neg = true; }
+  visit(bpx, bpy, bpz);
+  if (neg) {
+    bpx += dx;
+    bpy += dy;
+    bpz += dz;
+    visit(bpx, bpy, bpz);
+  }
+  int steps = 0;
+  while (bpx != ebx || bpy != eby || bpz != ebz) {
+    if (steps++ >= cap) return false;
+    if (mx < my) {
+      if (mx < mz) { bpx += sx; mx += dtx; }
+      else { bpz += sz; mz += dtz; }
+    } else {
+      if (my < mz) { bpy += sy; my += dty; }
+      else { bpz += sz; mz += dtz; }
+    }
+    visit(bpx, bpy, bpz);
+  }
+  return true;
+}
+
+__global__ void __launch_bounds__(kAllocT* kAllocT)
+    allocate_kernel(const float* __restrict__ depth, DSensor s, VolumeDev v,
+                    const PoseState* __restrict__ ps) {
+  __shared__ AllocSmem sm;
+  __shared__ M4f T;
+  __shared__ int stamp_s;
+  const int tid = threadIdx.y * kAllocT + threadIdx.x;
+  for (int k = tid; k < kSetSlots; k += kAllocT * kAllocT) sm.set[k] = kEmptyKey;
+  if (tid < 16) T.m[tid] = ps->posef[tid];
+  if (tid == 0) {
+    sm.nclaims = 0;
+    sm.new_blocks = sm.bucket_full = sm.heap_exhausted = sm.unique = sm.overruns = 0;
+    stamp_s = ps->frame;
+  }
+  __syncthreads();
+  const int stamp = stamp_s;
+  const DTsdf& t = v.t;
+  const int x = blockIdx.x * kAllocT + threadIdx.x;
+  const int y = blockIdx.y * kAllocT + threadIdx.y;
+  if (x < s.cols && y < s.rows) {
+    const int i = y * s.cols + x;
+    const float d = depth[i];
+    if (!(d < t.dmin || d > t.dmax)) {  // tsdf.cu:442-444
+      F3 point = xform(T, point3d(i, d, s));
+      if (!(point.x == 0 && point.y == 0 && point.z == 0)) {
+        F3 start_pt = f3(T.m[3], T.m[7], T.m[11]);
+        bool ok = dda_ray(start_pt, point, t.trunc, t.bsm, t.dda_cap, [&](int bx, int by, int bz) {
+          unsigned long long key = pack_key(bx, by, bz);
+          unsigned h = set_hash(key);
+          for (int p = 0; p < kSetProbes; ++p) {
+            unsigned slot = (h + p) & (kSetSlots - 1);
+            unsigned long long old = atomicCAS(&sm.set[slot], kEmptyKey, key);
+            if (old == kEmptyKey || old == key) return;
+          }
+          // set saturated: insert directly
+          int r = bucket_insert(v.entries, t, key, stamp, &sm.unique);
+          if (r >= 0) {
+            int ptr = atomicAdd(&v.cnt->nalloc, 1);
+            if (ptr < t.num_blocks) {
+              v.entries[r].ptr = ptr;
+              v.block_keys[ptr] = key;
+              atomicAdd(&sm.new_blocks, 1);
+            } else {
+              atomicAdd(&sm.heap_exhausted, 1);
+            }
+          } else if (r == -2) {
+            atomicAdd(&sm.bucket_full, 1);
+          }
+        });
+        if (!ok) atomicAdd(&sm.overruns, 1);
+      }
+    }
+  }
+  __syncthreads();
+  // drain the set into the global table
+  for (int k = tid; k < kSetSlots; k += kAllocT * kAllocT) {
+    unsigned long long key = sm.set[k];
+    if (key == kEmptyKey) continue;
+    int r = bucket_insert(v.entries, t, key, stamp, &sm.unique);
+    if (r >= 0) {
+      int c = atomicAdd(&sm.nclaims, 1);
+      sm.claim_entry[c] = r;
+    } else if (r == -2) {
+      atomicAdd(&sm.bucket_full, 1);
+    }
+  }
+  __syncthreads();
+  if (tid == 0 && sm.nclaims > 0) sm.base = atomicAdd(&v.cnt->nalloc, sm.nclaims);
+  __syncthreads();
+  for (int c = tid; c < sm.nclaims; c += kAllocT * kAllocT) {
+    int ptr = sm.base + c;
+    int e = sm.claim_entry[c];
+    if (ptr < t.num_blocks) {
+      v.entries[e].ptr = ptr;
+      v.block_keys[ptr] = v.entries[e].key;
+      atomicAdd(&sm.new_blocks, 1);
+    } else {
+      atomicAdd(&sm.heap_exhausted, 1);
+    }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    if (sm.new_blocks) atomicAdd(&v.cnt->new_blocks, sm.new_blocks);
+    if (sm.bucket_full) atomicAdd(&v.cnt->bucket_full, sm.bucket_full);
+    if (sm.heap_exhausted) atomicAdd(&v.cnt->heap_exhausted, sm.heap_exhausted);
+    if (sm.unique) atomicAdd(&v.cnt->unique_probed, sm.unique);
+    if (sm.overruns) atomicAdd(&v.cnt->dda_overruns, sm.overruns);
+  }
+}
+
+// ------------------------------------------------------------ visibility
+// IntegrateScanKernel's block test (tsdf.cu:283-300): block origin to the
+// camera, z < 0 rejected, the origin plus half a block (in camera axes,
+// computed in double) projected into the image.
+__device__ inline bool block_visible(unsigned long long key, const DTsdf& t, const DSensor& s,
+                                     const M4f& invT) {
+  const float vs = t.vs;
+  const int bs = kBlockSize;
+  F3 position = f3((float)key_x(key) * vs * (float)bs, (float)key_y(key) * vs * (float)bs,
+                   (float)key_z(key) * vs * (float)bs);
+  F3 pc = xform(invT, position);
+  if (pc.z < 0) return false;
+  double half = 0.5 * (double)vs * (double)bs;
+  F3 bc = f3((float)((double)pc.x + half), (float)((double)pc.y + half),
+             (float)((double)pc.z + half));
+  int ix, iy;
+  if (!project(bc, s, &ix, &iy)) return false;
+  return ix >= 0 && iy >= 0 && ix < s.cols && iy < s.rows;
+}
+
+__global__ void visible_kernel(VolumeDev v, DSensor s, const PoseState* __restrict__ ps) {
+  __shared__ M4f invT;
+  if (threadIdx.x < 16) invT.m[threadIdx.x] = ps->invf[threadIdx.x];
+  __syncthreads();
+  int n = v.cnt->nalloc;
+  if (n > v.t.num_blocks) n = v.t.num_blocks;
+  const int lane = threadIdx.x & 31;
+  for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    int i = base + threadIdx.x;
+    bool vis = i < n && block_visible(v.block_keys[i], v.t, s, invT);
+    unsigned m = __ballot_sync(0xffffffffu, vis);
+    int off = 0;
+    if (lane == 0 && m) off = atomicAdd(&v.cnt->visible, __popc(m));
+    off = __shfl_sync(0xffffffffu, off, 0);
+    if (vis) v.visible[off + __popc(m & ((1u << lane) - 1))] = i;
+  }
+}
+
+// ------------------------------------------------------------ integration
+// IntegrateScanKernel voxel loop (tsdf.cu:301-341) + Voxel::mergeVoxel
+// (geom_Types.h:79-103), one thread per voxel of a visible block.  The
+// voxel updated is the thread's own: the reference's camera->world round
+// trip through UpdateVoxel lands on the same voxel (the oracle checks this).
+__global__ void __launch_bounds__(kBlockVox)
+    integrate_kernel(VolumeDev v, const float* __restrict__ depth,
+                     const uint8_t* __restrict__ rgb, DSensor s,
+                     const PoseState* __restrict__ ps) {
+  __shared__ M4f invT;
+  if (threadIdx.x < 16) invT.m[threadIdx.x] = ps->invf[threadIdx.x];
+  __syncthreads();
+  const int nvis = v.cnt->visible;
+  const DTsdf& t = v.t;
+  const float vs = t.vs;
+  const int lin = threadIdx.x;
+  const int bx = lin >> 6, by = (lin >> 3) & 7, bz = lin & 7;
+  for (int b = blockIdx.x; b < nvis; b += gridDim.x) {
+    const int ptr = v.visible[b];
+    const unsigned long long key = v.block_keys[ptr];
+    F3 position = f3((float)key_x(key) * vs * (float)kBlockSize,
+                     (float)key_y(key) * vs * (float)kBlockSize,
+                     (float)key_z(key) * vs * (float)kBlockSize);
+    F3 vp = f3(position.x + (float)bx * vs, position.y + (float)by * vs,
+               position.z + (float)bz * vs);
+    vp = xform(invT, vp);
+    int px, py;
+    if (!project(vp, s, &px, &py)) continue;
+    if (!(px >= 0 && py >= 0 && px < s.cols && py < s.rows)) continue;
+    const int idx = py * s.cols + px;
+    const float d = __ldg(depth + idx);
+    if (d < t.dmin) continue;
+    if (d > t.dmax) continue;
+    F3 p3 = point3d(idx, d, s);
+    float sd = norm3(p3);
+    float vd = norm3(vp);
+    float sdf;
+    if (vd > sd - t.trunc && vd < sd + t.trunc && d < t.dmax) sdf = sd - vd;
+    else if (vd < sd - t.trunc) sdf = t.trunc;
+    else continue;
+    uint8_t c0 = 0, c1 = 0, c2 = 0;
+    if (rgb) {
+      c0 = __ldg(rgb + 3 * (size_t)idx);
+      c1 = __ldg(rgb + 3 * (size_t)idx + 1);
+      c2 = __ldg(rgb + 3 * (size_t)idx + 2);
+    }
+    dyn_voxel* vox = v.voxels + (size_t)ptr * kBlockVox + lin;
+    uint2 raw = *reinterpret_cast<const uint2*>(vox);
+    uint8_t r0 = raw.x & 0xff, r1 = (raw.x >> 8) & 0xff, r2 = (raw.x >> 16) & 0xff,
+            w = raw.x >> 24;
+    float osdf = __uint_as_float(raw.y);
+    float fw = (float)w;
+    float nsdf = (osdf * fw + sdf * 1.0f) / (fw + 1.0f);
+    r0 = (uint8_t)(((float)r0 * fw + (float)c0 * 1.0f) / (fw + 1.0f));
+    r1 = (uint8_t)(((float)r1 * fw + (float)c1 * 1.0f) / (fw + 1.0f));
+    r2 = (uint8_t)(((float)r2 * fw + (float)c2 * 1.0f) / (fw + 1.0f));
+    int nw = (uint8_t)(w + 1);
+    if (nw > t.max_w) nw = t.max_w;
+    uint2 out;
+    out.x = (unsigned)r0 | ((unsigned)r1 << 8) | ((unsigned)r2 << 16) | ((unsigned)nw << 24);
+    out.y = __float_as_uint(nsdf);
+    *reinterpret_cast<uint2*>(vox) = out;
+  }
+}
+
+// ------------------------------------------------------------ raycast
+struct VoxelSample {
+  float sdf;
+  float r, g, b;
+  int w;
+};
+
+struct BlockCache {
+  unsigned long long key;
+  int ptr;
+};
+
+// tsdf.cu:189-225: global voxel index by round-half-away of pos/voxelSize,
+// block by floor division, local index by non-negative remainder.
+__device__ inline void world_to_voxel(F3 pos, float vs, int* bx, int* by, int* bz, int* lin) {
+  int g[3];
+  float pv[3] = {pos.x, pos.y, pos.z};
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    float sg = (float)((pv[k] > 0.0f) - (pv[k] < 0.0f));
+    g[k] = (int)(pv[k] / vs + sg * 0.5f);
+  }
+  int b[3], l[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    b[k] = g[k] < 0 ? (g[k] - kBlockSize + 1) / kBlockSize : g[k] / kBlockSize;
+    l[k] = g[k] % kBlockSize;
+    if (l[k] < 0) l[k] += kBlockSize;
+  }
+  *bx = b[0];
+  *by = b[1];
+  *bz = b[2];
+  *lin = l[0] * kBlockSize * kBlockSize + l[1] * kBlockSize + l[2];
+}
+
+// tsdfVolume::GetVoxel, tsdf.cu:227-239, with a one-block lookup cache.
+__device__ inline uint2 get_voxel(const VolumeDev& v, F3 pos, BlockCache& bc) {
+  int bx, by, bz, lin;
+  world_to_voxel(pos, v.t.vs, &bx, &by, &bz, &lin);
+  unsigned long long key = pack_key(bx, by, bz);
+  if (key != bc.key) {
+    bc.key = key;
+    bc.ptr = find_block(v.entries, v.t, bx, by, bz);
+  }
+  if (bc.ptr < 0) return make_uint2(0u, 0u);
+  return __ldg(reinterpret_cast<const uint2*>(v.voxels + (size_t)bc.ptr * kBlockVox + lin));
+}
+
+__device__ inline int vw(uint2 r) { return (int)(r.x >> 24); }
+__device__ inline float vsdf(uint2 r) { return __uint_as_float(r.y); }
+
+// tsdfVolume::GetInterpolatedVoxel, tsdf.cu:47-175.
+__device__ inline VoxelSample get_interpolated(const VolumeDev& v, F3 position, BlockCache& bc) {
+  VoxelSample out;
+  uint2 v0 = get_voxel(v, position, bc);
+  out.w = vw(v0);
+  if (out.w == 0) {
+    out.sdf = vsdf(v0);
+    out.r = (float)(v0.x & 0xff);
+    out.g = (float)((v0.x >> 8) & 0xff);
+    out.b = (float)((v0.x >> 16) & 0xff);
+    return out;
+  }
+  const float vs = v.t.vs;
+  F3 pos_dual = position - f3(vs / 2.0f, vs / 2.0f, vs / 2.0f);
+  const float inv = 1.0f / vs;
+  F3 vp = position * inv;
+  F3 wt = f3(vp.x - floorf(vp.x), vp.y - floorf(vp.y), vp.z - floorf(vp.z));
+  float dist = 0.0f;
+  float cr = 0.0f, cg = 0.0f, cb = 0.0f;
+  const int off[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1},
+                         {1, 1, 0}, {0, 1, 1}, {1, 0, 1}, {1, 1, 1}};
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    F3 q = pos_dual + f3(off[k][0] ? vs : 0.0f, off[k][1] ? vs : 0.0f, off[k][2] ? vs : 0.0f);
+    uint2 vv = get_voxel(v, q, bc);
+    uint2 src = (vw(vv) == 0) ? v0 : vv;
+    float a = off[k][0] ? wt.x : 1.0f - wt.x;
+    float b = off[k][1] ? wt.y : 1.0f - wt.y;
+    float c = off[k][2] ? wt.z : 1.0f - wt.z;
+    float coef = a * b * c;
+    dist += coef * vsdf(src);
+    cr = cr + (float)(src.x & 0xff) * coef;
+    cg = cg + (float)((src.x >> 8) & 0xff) * coef;
+    cb = cb + (float)((src.x >> 16) & 0xff) * coef;
+  }
+  out.sdf = dist;
+  out.r = cr;
+  out.g = cg;
+  out.b = cb;
+  return out;
+}
+
+constexpr int kRayTX = 16, kRayTY = 16;
+
+__global__ void __launch_bounds__(kRayTX* kRayTY)
+    raycast_kernel(VolumeDev v, DSensor s, const PoseState* __restrict__ ps,
+                   const float* __restrict__ pose_override, float* __restrict__ depth_out,
+                   uint8_t* __restrict__ rgb_out) {
+  __shared__ M4f T;
+  __shared__ int over;
+  const int tid = threadIdx.y * kRayTX + threadIdx.x;
+  if (tid < 16) T.m[tid] = pose_override ? pose_override[tid] : ps->posef[tid];
+  if (tid == 0) over = 0;
+  __syncthreads();
+  // warps cover 8x4 pixel sub-tiles for coherent rays
+  const int warp = tid >> 5, lane = tid & 31;
+  const int lx = (warp & 1) * 8 + (lane & 7);
+  const int ly = (warp >> 1) * 4 + (lane >> 3);
+  const int x = blockIdx.x * kRayTX + lx, y = blockIdx.y * kRayTY + ly;
+  if (x < s.cols && y < s.rows) {
+    const int i = y * s.cols + x;
+    const DTsdf& t = v.t;
+    BlockCache bc;
+    bc.key = kEmptyKey;
+    bc.ptr = -1;
+    float cur = 0.0f;
+    int steps = 0;
+    while (cur < t.dmax) {
+      if (steps++ >= t.rc_cap) {
+        atomicAdd(&over, 1);
+        break;
+      }
+      F3 point = xform(T, point3d(i, cur, s));
+      VoxelSample vx = get_interpolated(v, point, bc);
+      if (vx.w == 0) cur += t.trunc;
+      else cur += vx.sdf;
+      if (vx.w != 0 && vx.sdf < t.vs) break;
+    }
+    depth_out[i] = cur;
+    if (rgb_out) {
+      uint8_t r = 0, g = 0, b = 0;
+      if (cur < t.dmax) {
+        F3 point = xform(T, point3d(i, cur, s));
+        VoxelSample vx = get_interpolated(v, point, bc);
+        r = (uint8_t)vx.r;
+        g = (uint8_t)vx.g;
+        b = (uint8_t)vx.b;
+      }
+      rgb_out[3 * (size_t)i] = r;
+      rgb_out[3 * (size_t)i + 1] = g;
+      rgb_out[3 * (size_t)i + 2] = b;
+    }
+  }
+  __syncthreads();
+  if (tid == 0 && over) atomicAdd(&v.cnt->raycast_overruns, over);
+}
+
+__global__ void clear_entries_kernel(Entry* e, size_t n) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  Entry z;
+  z.key = kEmptyKey;
+  z.ptr = -1;
+  z.stamp = -1;
+  e[i] = z;
+}
+
+__global__ void block_coords_kernel(VolumeDev v, int n, int* coords) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  unsigned long long k = v.block_keys[i];
+  coords[3 * i] = key_x(k);
+  coords[3 * i + 1] = key_y(k);
+  coords[3 * i + 2] = key_z(k);
+}
+
+inline int nblk(long long n, int t) { return (int)((n + t - 1) / t); }
+
+}  // namespace
+
+void launch_volume_clear(const VolumeDev& v, cudaStream_t st) {
+  size_t ne = (size_t)v.t.num_buckets * v.t.bucket_size;
+  clear_entries_kernel<<<nblk((long long)ne, 256), 256, 0, st>>>(v.entries, ne);
+  cudaMemsetAsync(v.voxels, 0, sizeof(dyn_voxel) * (size_t)v.t.num_blocks * kBlockVox, st);
+  cudaMemsetAsync(v.cnt, 0, sizeof(Counters), st);
+}
+
+void launch_allocate(const VolumeDev& v, const float* depth, const DSensor& s,
+                     const PoseState* ps, cudaStream_t st) {
+  dim3 grid(nblk(s.cols, kAllocT), nblk(s.rows, kAllocT));
+  allocate_kernel<<<grid, dim3(kAllocT, kAllocT), 0, st>>>(depth, s, v, ps);
+}
+
+void launch_visible(const VolumeDev& v, const DSensor& s, const PoseState* ps, cudaStream_t st) {
+  int g = nblk(v.t.num_blocks, 256);
+  if (g > 148 * 16) g = 148 * 16;
+  visible_kernel<<<g, 256, 0, st>>>(v, s, ps);
+}
+
+void launch_integrate(const VolumeDev& v, const float* depth, const uint8_t* rgb, const DSensor& s,
+                      const PoseState* ps, cudaStream_t st) {
+  integrate_kernel<<<148 * 4, kBlockVox, 0, st>>>(v, depth, rgb, s, ps);
+}
+
+void launch_raycast(const VolumeDev& v, const DSensor& s, const PoseState* ps,
+                    const float* pose_override, float* depth_out, uint8_t* rgb_out,
+                    cudaStream_t st) {
+  dim3 grid(nblk(s.cols, kRayTX), nblk(s.rows, kRayTY));
+  raycast_kernel<<<grid, dim3(kRayTX, kRayTY), 0, st>>>(v, s, ps, pose_override, depth_out,
+                                                        rgb_out);
+}
+
+void launch_block_coords(const VolumeDev& v, int n, int* coords, cudaStream_t st) {
+  if (n > 0) block_coords_kernel<<<nblk(n, 256), 256, 0, st>>>(v, n, coords);
+}
+
+}  // namespace dyn

@@ -1,0 +1,128 @@
+"""Python wrapper of a libdynamap_b200 session (the reference's builder,
+include/builder/builder.h:49-117), over the C ABI.
+
+    t, g, b, s = configs.structs(configs.preset("cfg1"))
+    with Session(t, g, b, s) as m:
+        m.set_pose(pose0)
+        for depth in frames:
+            pose, stats = m.process(depth)        # buildModelLS
+        coords, voxels = m.download_blocks()
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+
+_vp = C.c_void_p
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(_vp)
+
+
+def _f16(pose) -> C.Array:
+    p = np.ascontiguousarray(pose, np.float32).reshape(16)
+    return (C.c_float * 16)(*p.tolist())
+
+
+class Session:
+    def __init__(self, tsdf, gn, bil, sensor, precision: int = abi.PRECISION_FP32,
+                 device: int = 0):
+        self.lib = abi.load()
+        self.sensor = sensor
+        self.tsdf = tsdf
+        self.h = _vp()
+        abi.check("dyn_session_create",
+                  self.lib.dyn_session_create(C.byref(tsdf), C.byref(gn), C.byref(bil),
+                                              C.byref(sensor), precision, device,
+                                              C.byref(self.h)))
+
+    def close(self) -> None:
+        if self.h:
+            self.lib.dyn_session_destroy(self.h)
+            self.h = _vp()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- pose
+    def set_pose(self, pose) -> None:
+        abi.check("dyn_session_set_pose", self.lib.dyn_session_set_pose(self.h, _f16(pose)))
+
+    def pose(self) -> np.ndarray:
+        out = (C.c_float * 16)()
+        abi.check("dyn_session_get_pose", self.lib.dyn_session_get_pose(self.h, out))
+        return np.array(out, np.float32).reshape(4, 4)
+
+    # ---- frames
+    def submit(self, depth: np.ndarray, rgb: np.ndarray | None = None) -> None:
+        d = np.ascontiguousarray(depth, np.uint16)
+        r = None if rgb is None else np.ascontiguousarray(rgb, np.uint8)
+        self._keep = (d, r)
+        abi.check("dyn_frame_submit", self.lib.dyn_frame_submit(self.h, _ptr(d), _ptr(r)))
+
+    def submit_device(self, depth_ptr: int, rgb_ptr: int | None = None) -> None:
+        abi.check("dyn_frame_submit_device",
+                  self.lib.dyn_frame_submit_device(self.h, depth_ptr, rgb_ptr))
+
+    def result(self, strict: bool = True):
+        pose = (C.c_float * 16)()
+        st = abi.FrameStats()
+        r = self.lib.dyn_frame_result(self.h, pose, C.byref(st))
+        if strict or r not in (abi.DYN_ERR_HASH_FULL, abi.DYN_ERR_HEAP_EXHAUSTED):
+            abi.check("dyn_frame_result", r)
+        return np.array(pose, np.float32).reshape(4, 4), st
+
+    def process(self, depth, rgb=None, strict: bool = True):
+        self.submit(depth, rgb)
+        return self.result(strict)
+
+    def integrate_with_pose(self, depth, rgb, pose) -> None:
+        d = np.ascontiguousarray(depth, np.uint16)
+        r = None if rgb is None else np.ascontiguousarray(rgb, np.uint8)
+        abi.check("dyn_integrate_with_pose",
+                  self.lib.dyn_integrate_with_pose(self.h, _ptr(d), _ptr(r), _f16(pose)))
+
+    def raycast(self, pose, sensor=None, rgb: bool = False):
+        s = sensor if sensor is not None else self.sensor
+        d = np.empty((s.rows, s.cols), np.float32)
+        c = np.empty((s.rows, s.cols, 3), np.uint8) if rgb else None
+        abi.check("dyn_raycast", self.lib.dyn_raycast(
+            self.h, _f16(pose), C.byref(s) if sensor is not None else None, _ptr(d), _ptr(c)))
+        return d, c
+
+    # ---- map access
+    def num_blocks(self) -> int:
+        n = C.c_int64()
+        abi.check("dyn_num_blocks", self.lib.dyn_num_blocks(self.h, C.byref(n)))
+        return n.value
+
+    def download_blocks(self):
+        """(coords (n,3) int32, rgbw (n,512,4) uint8, sdf (n,512) float32)."""
+        n = self.num_blocks()
+        coords = np.empty((n, 3), np.int32)
+        vox = np.empty((n, 512, 2), np.uint32)  # {rgbw, sdf bits} per voxel
+        got = C.c_int64()
+        abi.check("dyn_download_blocks", self.lib.dyn_download_blocks(
+            self.h, _ptr(coords), _ptr(vox), n, C.byref(got)))
+        rgbw = vox[..., 0].copy().view(np.uint8).reshape(n, 512, 4)
+        sdf = vox[..., 1].copy().view(np.float32)
+        return coords, rgbw, sdf
+
+    def image(self, which: int, level: int, shape, dtype) -> np.ndarray:
+        out = np.empty(shape, dtype)
+        abi.check("dyn_debug_image",
+                  self.lib.dyn_debug_image(self.h, which, level, _ptr(out), out.nbytes))
+        return out

@@ -1,0 +1,289 @@
+/*
+ * dynamap.h -- C ABI of the B200 rigid-mapping library (libdynamap_b200.so).
+ *
+ * This is the drop-in boundary for DynaMap's per-frame rigid mapping path:
+ * depth ingest -> bilateral filter -> vertex/normal pyramids -> projective
+ * point-to-plane (+photometric) Gauss-Newton ICP -> voxel-hashed TSDF
+ * allocation + integration -> raycast of the model for the next frame.
+ *
+ * Every entry point takes plain pointers and sizes, returns a dyn_status and
+ * never throws.  Citations name the reference interface each item replaces
+ * (paths are relative to the alirezaahmadi/dynamap source tree).
+ *
+ * Conventions
+ *   - Poses are camera-to-world rigid transforms stored as 16 floats in
+ *     ROW-major order (m11 m12 m13 m14 m21 ...), the layout of the
+ *     reference's device-side float4x4 (include/math/utils_matrix.h:816-839,
+ *     built from Eigen at include/builder/builder.cu:102).
+ *   - Depth frames are uint16 raw sensor units, row-major rows*cols;
+ *     metres = raw / depth_scaler.  0 = invalid.
+ *   - RGB frames are uint8 R,G,B interleaved, row-major rows*cols*3.
+ *   - "_host" buffers are caller-owned host memory (pageable or pinned);
+ *     "_dev" buffers are device pointers on the session's device.
+ *   - All calls on one session must be serialised by the caller; different
+ *     sessions may be driven from different host threads.
+ */
+#ifndef DYNAMAP_B200_H
+#define DYNAMAP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DYN_ABI_VERSION 1
+
+/* Status codes.  The reference reports failures with printf + return
+ * (include/solver/gnSolver/gnSolver.cu:329-343) or silent -1 returns
+ * (include/dataStructure/hashTable/hashTable.cu:109); here every call
+ * returns one of these. */
+typedef enum dyn_status {
+  DYN_OK = 0,
+  DYN_ERR_INVALID_ARG = 1,
+  DYN_ERR_OOM = 2,
+  DYN_ERR_BUDGET_EXCEEDED = 3,
+  DYN_ERR_HASH_FULL = 4,       /* a bucket overflowed (block not stored) */
+  DYN_ERR_HEAP_EXHAUSTED = 5,  /* more blocks requested than num_blocks */
+  DYN_ERR_ICP_DIVERGED = 6,
+  DYN_ERR_TIMEOUT = 7,
+  DYN_ERR_CUDA = 8,
+  DYN_ERR_NOT_READY = 9,
+  DYN_ERR_NO_DEVICE = 10
+} dyn_status;
+
+/* Pinhole sensor.  Replaces DynaMap::rgbdSensor
+ * (include/image/sensor/rgbdSensor.h:13-19: rows, cols, f, c, depthScaler). */
+typedef struct dyn_sensor {
+  uint32_t rows;
+  uint32_t cols;
+  float fx, fy;          /* rgbdSensor::f */
+  float cx, cy;          /* rgbdSensor::c */
+  float depth_scaler;    /* raw units per metre (TUM 5000, millimetres 1000) */
+} dyn_sensor;
+
+/* TSDF / voxel-hash configuration.  Replaces tsdf::tsdfProperties
+ * (include/geometry/tsdf/tsdf.h:19-35) and the keys of
+ * config/tsdfParams.yaml (voxelSize, numBuckets, bucketSize, numBlocks,
+ * blockSize, maxSDFWeight, truncationDistance, maxSensorDepth,
+ * minSensorDepth). */
+typedef struct dyn_tsdf_params {
+  float voxel_size;           /* metres */
+  int32_t num_buckets;
+  int32_t bucket_size;        /* slots per bucket, no overflow list */
+  int32_t num_blocks;         /* voxel-block pool size (heap) */
+  int32_t block_size;         /* voxels per block edge; must be 8 */
+  int32_t max_sdf_weight;     /* weight cap, <= 255 (uint8 weight) */
+  float truncation_distance;  /* metres */
+  float max_sensor_depth;     /* metres */
+  float min_sensor_depth;     /* metres */
+} dyn_tsdf_params;
+
+/* Gauss-Newton ICP configuration.  Replaces solver::Properties
+ * (include/solver/gnSolver/gnSolver.h:47-55) and config/gnOptimParams.yaml
+ * (lvlIterationNum[i], lvlScale[i], minIncrement, maxIncrement,
+ * regularization, huberConstant).  The fields after huber_constant are
+ * additive: the reference hard-codes them at the cited lines. */
+typedef struct dyn_gn_params {
+  int32_t lvl_iteration_num[3]; /* level i runs lvl_iteration_num[i]-1
+                                   iterations (gnSolver.cu:370) */
+  int32_t lvl_scale[3];         /* 1, 2, 4 or 8; level order as given */
+  int32_t max_iteration;        /* unused by the reference; kept */
+  float min_increment;          /* stop when |delta xi| <= this */
+  float max_increment;          /* zero the increment if sum(xi) >= this */
+  float regularization;         /* damping: A += (reg*max(A)/it) I */
+  float huber_constant;         /* parsed, unused (gnSolver.cu:116-119) */
+  float color_weight;           /* photometric blend, gnSolver.cu:180 (0) */
+  float icp_min_depth;          /* DEPTH_MIN, pyramid.h:16 (0.15) */
+  float icp_max_depth;          /* DEPTH_MAX, pyramid.h:15 (2.0) */
+  float normal_cos_thresh;      /* |n.ns| gate, gnSolver.cu:108 cos(pi/10) */
+  int32_t mode;                 /* builder Mode: 0 frame-to-frame,
+                                   1 frame-to-model (raycast target) */
+  int32_t compose_left;         /* 1: pose = exp(xi) * pose as at
+                                   gnSolver.cu:429; 0: pose = pose * exp(xi) */
+} dyn_gn_params;
+
+/* Bilateral filter.  Replaces DynaMap::gaussianKernal
+ * (include/image/kernel2D/kernel2D.h:20-43) and config/bilateralFParams.yaml
+ * (diameter, sigmaI, sigmaS).  The window is 2*diameter taps per axis
+ * (pyramid.cu:250). */
+typedef struct dyn_bilateral_params {
+  int32_t diameter;
+  float sigma_i;   /* range sigma (metres) */
+  float sigma_s;   /* spatial sigma (pixels) */
+  int32_t enabled; /* 0: ICP uses the unfiltered depth */
+} dyn_bilateral_params;
+
+typedef enum dyn_precision {
+  DYN_PRECISION_FP32 = 0,   /* 8-byte voxels {r,g,b,w,f32 sdf}: the drop-in */
+  DYN_PRECISION_MIXED = 1   /* f16 sdf + u16 weight, Kahan-f32 normal eqns */
+} dyn_precision;
+
+/* One voxel as downloaded.  Same 8-byte layout as geometry::Voxel
+ * (include/geometry/geom_Types.h:72-76: uchar3 color, uchar weight,
+ * float sdf). */
+typedef struct dyn_voxel {
+  uint8_t r, g, b;
+  uint8_t weight;
+  float sdf;
+} dyn_voxel;
+
+/* Per-frame counters, read back with dyn_frame_result. */
+typedef struct dyn_frame_stats {
+  int32_t frame_index;
+  int32_t icp_iterations[3];    /* executed iterations per level */
+  int32_t icp_inliers[3];       /* correspondences, last iteration per level */
+  float icp_rms[3];             /* point-to-plane RMS residual (m) */
+  int32_t icp_reset;            /* 1 if the NaN / max_increment guard fired */
+  int32_t blocks_total;         /* allocated blocks after this frame */
+  int32_t blocks_new;           /* blocks allocated by this frame */
+  int32_t blocks_visible;       /* blocks integrated this frame */
+  int32_t unique_blocks_probed; /* distinct blocks the rays touched */
+  int32_t bucket_full;          /* inserts refused: bucket full */
+  int32_t heap_exhausted;       /* inserts refused: no free block */
+  int32_t dda_overruns;         /* rays cut at the step limit */
+  int32_t raycast_overruns;     /* raycast pixels cut at the step limit */
+  double pose_increment[6];     /* final xi = [w; t] of this frame */
+} dyn_frame_stats;
+
+typedef struct dyn_session dyn_session;
+
+/* ---- library ---------------------------------------------------------- */
+int32_t dyn_abi_version(void);
+const char* dyn_status_string(dyn_status s);
+/* Fills the defaults of the reference config files (tsdfParams.yaml,
+ * gnOptimParams.yaml, bilateralFParams.yaml, cameraParams.yaml) and of
+ * include/image/pyramid/pyramid.h. */
+dyn_status dyn_default_params(dyn_tsdf_params* tsdf, dyn_gn_params* gn,
+                              dyn_bilateral_params* bil, dyn_sensor* sensor);
+/* Parses the reference's flat "- key: value" YAML files
+ * (config/tsdfParams.yaml, gnOptimParams.yaml, bilateralFParams.yaml,
+ * cameraParams.yaml).  Any pointer may be NULL; unknown keys are ignored,
+ * missing keys keep the value already in the struct. */
+dyn_status dyn_load_yaml(const char* path, dyn_tsdf_params* tsdf,
+                         dyn_gn_params* gn, dyn_bilateral_params* bil,
+                         dyn_sensor* sensor);
+/* Bytes of device memory a session with these parameters holds. */
+dyn_status dyn_session_bytes(const dyn_tsdf_params* tsdf,
+                             const dyn_sensor* sensor, int32_t precision,
+                             size_t* bytes_out);
+
+/* ---- session (builder, include/builder/builder.h:49-117) -------------- */
+/* builder::init (builder.cu:11-49) + tsdfVolume::init (tsdf.cu:18) +
+ * HashTable::Init (hashTable.cu:41-70).  All device memory is allocated
+ * here, once; no call below allocates. */
+dyn_status dyn_session_create(const dyn_tsdf_params* tsdf,
+                              const dyn_gn_params* gn,
+                              const dyn_bilateral_params* bil,
+                              const dyn_sensor* sensor, int32_t precision,
+                              int32_t device, dyn_session** out);
+/* builder::~builder (builder.cu:50-65). */
+dyn_status dyn_session_destroy(dyn_session* s);
+/* Clears the map and the pose (HashTable::Init semantics, no realloc). */
+dyn_status dyn_session_reset(dyn_session* s);
+
+/* Pose of the last processed frame (builder::getCurrentPose, builder.cu:284)
+ * and an explicit initial pose (builder::setInitialPose, builder.cu:263). */
+dyn_status dyn_session_get_pose(dyn_session* s, float pose_out[16]);
+dyn_status dyn_session_set_pose(dyn_session* s, const float pose[16]);
+
+/* builder::buildModelLS (builder.cu:70-139) for one frame: track against
+ * the model (or the previous frame in mode 0), integrate, raycast the
+ * target for the next frame.  Enqueued on the session's stream; returns
+ * before the GPU finishes.  Host buffers are copied before return
+ * (they may be reused immediately). */
+dyn_status dyn_frame_submit(dyn_session* s, const uint16_t* depth_host,
+                            const uint8_t* rgb_host /* nullable */);
+/* Same, with the frame already resident on the device. */
+dyn_status dyn_frame_submit_device(dyn_session* s, const uint16_t* depth_dev,
+                                   const uint8_t* rgb_dev /* nullable */);
+/* Waits for the last submitted frame; returns its pose and counters. */
+dyn_status dyn_frame_result(dyn_session* s, float pose_out[16],
+                            dyn_frame_stats* stats /* nullable */);
+
+/* builder::buildModelGT (builder.cu:140-160): integrate a frame at a given
+ * pose (no tracking), then raycast the target at that pose.  Synchronous. */
+dyn_status dyn_integrate_with_pose(dyn_session* s, const uint16_t* depth_host,
+                                   const uint8_t* rgb_host /* nullable */,
+                                   const float pose[16]);
+
+/* tsdfVolume::GenerateDepth / GenerateRgb (tsdf.cu:527-550; kernels
+ * tsdf.cu:471-526) into caller buffers.  'virt' may be NULL for the session
+ * sensor; otherwise its rows*cols must not exceed the session sensor's.
+ * Synchronous. */
+dyn_status dyn_raycast(dyn_session* s, const float pose[16],
+                       const dyn_sensor* virt, float* depth_host,
+                       uint8_t* rgb_host /* nullable */);
+
+/* Number of allocated blocks (HashTable::GetNumAllocatedBlocks,
+ * hashTable.cu:165). */
+dyn_status dyn_num_blocks(dyn_session* s, int64_t* n_out);
+/* Copies every allocated block: coords_out[3*i..] = block coordinate
+ * (HashEntry::position, hashTable.h:22), voxels_out[512*i..] = its voxels in
+ * the reference's x-major order (VoxelBlock::at, geom_Types.h:116-119).
+ * Order of blocks is unspecified.  voxels_out may be NULL. */
+dyn_status dyn_download_blocks(dyn_session* s, int32_t* coords_out,
+                               dyn_voxel* voxels_out, int64_t capacity,
+                               int64_t* n_out);
+
+/* Internal images of the last frame, for inspection and parity tests.
+ * which: 0 raw depth (f32, level 0), 1 filtered depth (f32, level 0),
+ *        2 source depth pyramid level L (f32), 3 source vertices level L
+ *        (float4), 4 source normals level L (float4), 5 target depth level L,
+ *        6 target vertices L, 7 target normals L, 8 target rgb (u8x3, level 0),
+ *        9 source intensity level L (f32), 10 target intensity level L (f32).
+ * 'level' is the pyramid level (0 = full resolution). */
+dyn_status dyn_debug_image(dyn_session* s, int32_t which, int32_t level,
+                           void* host_out, size_t bytes);
+
+/* ---- stage entry points on caller device buffers ----------------------
+ * These run one stage of the path on caller-owned device memory, on
+ * 'stream' (a cudaStream_t, NULL = legacy default stream), and return once
+ * the work is enqueued (no host synchronisation) unless noted. */
+
+/* pyramid::bilateralFilter (pyramid.cu:253-282 -> applyBilateralFilter
+ * :213-233).  Out-of-image and invalid (<= 0) taps are skipped; an invalid
+ * centre stays 0. */
+dyn_status dyn_bilateral_filter(const float* depth_dev, float* out_dev,
+                                uint32_t rows, uint32_t cols,
+                                const dyn_bilateral_params* p, void* stream);
+
+/* rgbdImage::getPointCloudXYZ + getNormalsfromVertices (rgbdImage.cu:23-49,
+ * :126-167) for one level: vertex (x,y,z,1 | 0 if invalid) and normal
+ * (nx,ny,nz,0 | 0 if invalid) as float4 per pixel. */
+dyn_status dyn_depth_to_maps(const float* depth_dev, const dyn_sensor* level,
+                             float* vertex4_dev, float* normal4_dev,
+                             void* stream);
+
+/* The 6x6 normal equations of one ICP iteration (buildNLSKernel,
+ * gnSolver.cu:26-196): for source pixels (depth, normals, intensity) and a
+ * target (depth, normals, intensity, all on the same level sensor), under
+ * the transform T (row-major float[16]) computes
+ *   out[0..20]  upper triangle of A = sum J^T J (row-major, i<=j)
+ *   out[21..26] -sum J r   (the reference's acc_b)
+ *   out[27]     sum r^2 (point-to-plane residuals)
+ *   out[28]     number of correspondences
+ * in a fixed-order reduction (FP32 per pixel, FP64 across thread blocks).
+ * intensity pointers may be NULL when gn->color_weight == 0.
+ * Synchronous: out_host is filled on return. */
+dyn_status dyn_icp_normal_equations(
+    const float* src_depth_dev, const float* src_normal4_dev,
+    const float* src_intensity_dev, const float* tgt_depth_dev,
+    const float* tgt_normal4_dev, const float* tgt_intensity_dev,
+    const dyn_sensor* level, const dyn_gn_params* gn, const float T[16],
+    double out_host[29], void* stream);
+
+/* ---- batched multi-session stepping ------------------------------------
+ * Process one frame for each of n sessions with as few launches as the
+ * sessions' shapes allow.  Frames are given as host pointers (copied
+ * before return).  Results are read with dyn_frame_result per session. */
+dyn_status dyn_sessions_submit(dyn_session* const* sessions, int32_t n,
+                               const uint16_t* const* depth_host,
+                               const uint8_t* const* rgb_host /* nullable */);
+
+#ifdef __cplusplus
+}  /* extern "C" */
+#endif
+
+#endif /* DYNAMAP_B200_H */

@@ -1,0 +1,30 @@
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and libdynamap_b200.so")
+
+
+@pytest.fixture(scope="session")
+def oracle():
+    from oracle import pyoracle
+    pyoracle.lib()
+    pyoracle.set_threads(min(8, os.cpu_count() or 1))
+    return pyoracle
+
+
+@pytest.fixture(scope="session")
+def gpu_lib():
+    from dynamap_b200 import abi
+    lib = abi.load()  # raises if the CUDA library is missing: no fallback
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("CUDA device required for gpu tests")
+    return lib
