@@ -1,0 +1,450 @@
+#!/usr/bin/env python
+"""Benchmark of the rigid mapping path (one frame = one step).
+
+Workload (default): the 640x480 depth + RGB configuration -- 5 mm voxels,
+2^20 hash buckets, 3-level geometric + photometric (weight 0.1) ICP, FP32
+TSDF -- on a seeded synthetic sequence (analytic scene, 1 cm / 1 deg per
+frame).  Each step tracks one frame against the model, integrates it and
+raycasts the next target.
+
+Passes (each on a fresh session replaying the same frames; W warm-up frames
+then K timed frames):
+  A  device throughput: frames resident in HBM, submitted back to back;
+     CUDA events on the session's stream around the K frames -> value.
+  B  latency + stages: per-frame submit/result; per-stage CUDA events
+     captured inside the frame graph -> p50/p99 and the roofline of the
+     dominant kernel.
+  C  end to end: frames in pinned host memory through dyn_frame_submit
+     (H2D inside) and dyn_frame_result (D2H of pose + counters) -> e2e.
+--impl reference times the CPU implementation instead (rank 0 only).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "agg frames/s + p50/p99 frame latency vs plain FP32 path; ATE/SDF err vs FP64"
+
+
+def _render_chunk(args):
+    from dynamap_b200 import configs, scene
+    name, seed, n_frames, idx = args
+    p = configs.preset(name)
+    s, q = p["sensor"], p["seq"]
+    sc = scene.make_scene(seed, q["kind"])
+    poses = scene.trajectory(sc, n_frames, seed, q["trans"], q["rot"])
+    import numpy as np
+    out_d, out_c = [], []
+    for i in idx:
+        rng = np.random.default_rng(seed * 1000003 + i)
+        d, c = scene.render(sc, poses[i], s["rows"], s["cols"], s["fx"], s["fy"], s["cx"],
+                            s["cy"], rng, depth_scaler=s["depth_scaler"], with_rgb=q["rgb"])
+        out_d.append(d)
+        out_c.append(c)
+    return idx, out_d, out_c, poses
+
+
+def make_frames(name: str, seed: int, n_frames: int, workers: int):
+    """Render the sequence with a spawn process pool (started before CUDA)."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    import numpy as np
+    chunks = [list(range(i, min(i + 8, n_frames))) for i in range(0, n_frames, 8)]
+    depth, rgb, poses = [None] * n_frames, [None] * n_frames, None
+    with cf.ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+        for idx, ds, cs, ps in ex.map(_render_chunk, [(name, seed, n_frames, c) for c in chunks]):
+            poses = ps
+            for i, d, c in zip(idx, ds, cs):
+                depth[i], rgb[i] = d, c
+    depth = np.stack(depth)
+    rgb = np.stack(rgb) if rgb[0] is not None else None
+    return depth, rgb, poses
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during a timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def algorithmic_bytes(stage: str, st_avg: dict, P: int, bsz: int, levels_iters, rgb: bool):
+    """Bytes a kernel must move per launch (the per-unit figures of the
+    design's measurement section), from the run's own counters."""
+    Sv = 8
+    if stage == "integrate":
+        return st_avg["blocks_visible"] * (16 + 2 * 512 * Sv) + 4 * P + (3 * P if rgb else 0)
+    if stage == "raycast":
+        return st_avg["blocks_visible"] * 512 * Sv + 4 * P + 32 * P + (3 * P if rgb else 0)
+    if stage == "allocate":
+        return 4 * P + st_avg["unique_blocks_probed"] * 16 * bsz + 16 * st_avg["blocks_new"]
+    if stage == "icp":
+        tot = 0
+        for Pl, I in levels_iters:
+            tot += I * Pl * (32 + 32 + (6 if rgb else 0))
+        return tot
+    if stage == "bilateral":
+        return 2 * P + 4 * P
+    if stage == "source_maps" or stage == "target_maps":
+        return sum(4 * (P >> (2 * l)) + 16 * (P >> (2 * l)) for l in range(3))
+    return None
+
+
+def read_profile_traffic(kernel: str):
+    """dram bytes per launch of 'kernel' recorded from an ncu capture in
+    profiles/ (a line 'traffic_bytes_per_launch: N'), or None."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_kernel.md")
+    if not os.path.exists(path):
+        return None
+    for ln in open(path):
+        if ln.strip().startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(ln.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_baseline(name, depth, rgb, poses, seconds: float = 15.0):
+    """The oracle (FP32 restatement, OpenMP on all host threads) on the
+    first frames of the same sequence until ~seconds of CPU work."""
+    from dynamap_b200 import configs
+    from oracle import pyoracle as po
+    p = configs.preset(name)
+    t, g, b, s = configs.structs(p)
+    cores = os.cpu_count() or 1
+    po.set_threads(cores)
+    S = po.Session(t, g, b, s)
+    S.set_pose(poses[0])
+    n, t0 = 0, time.perf_counter()
+    while n < len(depth):
+        S.frame(depth[n], None if rgb is None else rgb[n])
+        n += 1
+        if time.perf_counter() - t0 > seconds and n >= 2:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": n / dt, "unit": "frames/s", "cores": cores, "kind": "port",
+            "sample": f"first {n} frames of the timed sequence ({s.cols}x{s.rows}), "
+                      f"oracle FP32 restatement with OpenMP, {dt:.1f} s"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    depth, rgb, poses = make_frames(args.config, args.seed, args.warmup + args.steps,
+                                    max(1, (os.cpu_count() or 2) - 1))
+    from dynamap_b200 import configs
+    from oracle import pyoracle as po
+    p = configs.preset(args.config)
+    t, g, b, s = configs.structs(p)
+    cores = os.cpu_count() or 1
+    po.set_threads(cores)
+    S = po.Session(t, g, b, s)
+    S.set_pose(poses[0])
+    budget = args.ref_seconds
+    for k in range(min(args.warmup, 2)):
+        S.frame(depth[k], None if rgb is None else rgb[k])
+    n, t0 = 0, time.perf_counter()
+    k = min(args.warmup, 2)
+    while n < args.steps and k < len(depth):
+        S.frame(depth[k], None if rgb is None else rgb[k])
+        n += 1
+        k += 1
+        if time.perf_counter() - t0 > budget:
+            break
+    dt = time.perf_counter() - t0
+    v = n / dt
+    line = {"metric": METRIC, "value": v, "unit": "frames/s", "n_gpus": args.gpus,
+            "steps": n, "warmup": min(args.warmup, 2), "ms_per_step": 1e3 * dt / max(n, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "impl": "reference",
+            "config": config_block(args, p),
+            "cpu_baseline": {"value": v, "unit": "frames/s", "cores": cores, "kind": "port",
+                             "sample": f"{n} consecutive frames of the workload after "
+                                       f"{min(args.warmup, 2)} warm-up frames (bounded to "
+                                       f"~{budget:.0f} s), oracle FP32 restatement, OpenMP"},
+            "e2e": {"value": v, "unit": "frames/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def config_block(args, p):
+    s, t = p["sensor"], p["tsdf"]
+    return {"workload": f"{args.config}: {s['cols']}x{s['rows']} uint16 depth"
+                        f"{' + RGB' if p['seq']['rgb'] else ''}, {t['voxel_size']*1e3:g} mm voxels, "
+                        f"2^{int(math.log2(t['num_buckets']))} buckets x {t['bucket_size']}, "
+                        f"ICP iters {p['gn']['lvl_iteration_num']} at scales {p['gn']['lvl_scale']}, "
+                        f"photometric weight {p['gn']['color_weight']}, FP32 TSDF, frame-to-model",
+            "sessions_per_gpu": 1, "precision": "fp32", "seed": args.seed,
+            "l2": "inputs larger than L2: the TSDF working set (voxel pool "
+                  f"{t['num_blocks'] * 4096 / 2**30:.1f} GiB, hash "
+                  f"{t['num_buckets'] * t['bucket_size'] * 16 / 2**20:.0f} MiB) exceeds the 126 MB L2"}
+
+
+def run_ours(args):
+    import numpy as np
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    nframes = args.warmup + args.steps
+    workers = max(1, min(32, ((os.cpu_count() or 2) - 1) // max(world, 1)))
+    depth, rgb, poses = make_frames(args.config, args.seed + rank, nframes, workers)
+
+    import torch
+    from dynamap_b200 import abi, configs
+    from dynamap_b200.session import Session
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    p = configs.preset(args.config)
+    t, g, b, s = configs.structs(p)
+    lib = abi.load()
+    P = s.rows * s.cols
+    has_rgb = rgb is not None
+    d_dev = torch.from_numpy(depth).cuda()
+    c_dev = torch.from_numpy(rgb).cuda() if has_rgb else None
+    fbytes_d, fbytes_c = P * 2, P * 3
+
+    def fptr(tensor, i, nb):
+        return tensor.data_ptr() + i * nb
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        v = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(v, op=dist.ReduceOp.MAX)
+        return float(v.item())
+
+    import ctypes as C
+
+    def session_stream(m):
+        ptr = C.c_void_p()
+        abi.check("stream", lib.dyn_session_stream(m.h, C.byref(ptr)))
+        return torch.cuda.ExternalStream(ptr.value, device=torch.device("cuda", local))
+
+    # ---- pass A: device throughput --------------------------------------
+    with Session(t, g, b, s, device=local) as m:
+        m.set_pose(poses[0])
+        stream = session_stream(m)
+        for i in range(args.warmup):
+            m.submit_device(fptr(d_dev, i, fbytes_d), fptr(c_dev, i, fbytes_c) if has_rgb else None)
+            m.result()
+        kpf = C.c_int32()
+        abi.check("kpf", lib.dyn_session_kernels_per_frame(m.h, C.byref(kpf)))
+        barrier()
+        clk = ClockSampler(local)
+        clk.start()
+        time.sleep(0.3)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for i in range(args.warmup, nframes):
+            m.submit_device(fptr(d_dev, i, fbytes_d), fptr(c_dev, i, fbytes_c) if has_rgb else None)
+        e1.record(stream)
+        m.result(strict=False)
+        torch.cuda.synchronize()
+        elapsed_a = e0.elapsed_time(e1) / 1e3
+        clocks = clk.stop()
+        final_pose_a = m.pose()
+    elapsed_a = max_over_ranks(elapsed_a)
+    barrier()
+
+    # ---- pass B: per-frame latency and stage times ------------------------
+    lat_dev, lat_host, stats = [], [], []
+    with Session(t, g, b, s, device=local) as m:
+        m.set_pose(poses[0])
+        abi.check("profile", lib.dyn_session_profile(m.h, 1))
+        for i in range(args.warmup):
+            m.submit_device(fptr(d_dev, i, fbytes_d), fptr(c_dev, i, fbytes_c) if has_rgb else None)
+            m.result()
+        ms = (C.c_double * abi.STAGES.__len__())()
+        nfr = C.c_int64()
+        abi.check("stages", lib.dyn_session_stage_times(m.h, ms, C.byref(nfr), 1))
+        barrier()
+        track = []
+        for i in range(args.warmup, nframes):
+            h0 = time.perf_counter()
+            m.submit_device(fptr(d_dev, i, fbytes_d), fptr(c_dev, i, fbytes_c) if has_rgb else None)
+            pose, st = m.result(strict=False)
+            lat_host.append(time.perf_counter() - h0)
+            stats.append(st.as_dict())
+            track.append(pose.astype(np.float64))
+        abi.check("stages", lib.dyn_session_stage_times(m.h, ms, C.byref(nfr), 0))
+        stage_ms = {abi.STAGES[k]: ms[k] / max(nfr.value, 1) for k in range(len(abi.STAGES))}
+    barrier()
+
+    # ---- pass C: end to end through the host API ---------------------------
+    pin_d = torch.from_numpy(depth).pin_memory()
+    pin_c = torch.from_numpy(rgb).pin_memory() if has_rgb else None
+    d_np = pin_d.numpy()
+    c_np = pin_c.numpy() if has_rgb else None
+    with Session(t, g, b, s, device=local) as m:
+        m.set_pose(poses[0])
+        stream = session_stream(m)
+        for i in range(args.warmup):
+            m.process(d_np[i], c_np[i] if has_rgb else None, strict=False)
+        barrier()
+        torch.cuda.synchronize()
+        h0 = time.perf_counter()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(args.warmup, nframes):
+            m.process(d_np[i], c_np[i] if has_rgb else None, strict=False)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        elapsed_c_host = time.perf_counter() - h0
+    elapsed_c = max_over_ranks(elapsed_c_host)
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    K = args.steps
+    value = world * K / elapsed_a
+    lat = sorted(x * 1e3 for x in lat_host)
+    p50 = lat[len(lat) // 2]
+    p99 = lat[min(len(lat) - 1, int(math.ceil(0.99 * len(lat))) - 1)]
+    st_avg = {k: float(np.mean([d[k] for d in stats])) for k in
+              ("blocks_visible", "unique_blocks_probed", "blocks_new", "blocks_total")}
+    iters = np.mean([d["icp_iterations"] for d in stats], axis=0)
+    lv = [(P >> (2 * {1: 0, 2: 1, 4: 2, 8: 3}[p["gn"]["lvl_scale"][k]]), iters[k]) for k in range(3)]
+    kernel_stages = [k for k in abi.STAGES if k != "frame"]
+    dom = max(kernel_stages, key=lambda k: stage_ms[k])
+    alg = algorithmic_bytes(dom, st_avg, P, t.bucket_size, lv, has_rgb)
+    hbm, peak_kind = peaks()
+    roof = None
+    if alg is not None and stage_ms[dom] > 0:
+        ach = alg / (stage_ms[dom] / 1e3) / 1e9
+        traffic = read_profile_traffic(dom)
+        roof = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": hbm, "unit": "GB/s",
+                "frac": ach / hbm, "peak_source": f"{peak_kind} hbm_gbs",
+                "algorithmic_bytes_per_launch": alg, "launch_ms": stage_ms[dom],
+                "traffic": traffic}
+    # tracking accuracy against the ground truth
+    gt = poses[args.warmup:nframes]
+    ate = float(np.sqrt(np.mean([np.sum((a[:3, 3] - b_[:3, 3]) ** 2) for a, b_ in zip(track, gt)])))
+    cpu = cpu_baseline(args.config, depth, rgb, poses, seconds=args.cpu_seconds) \
+        if not args.no_cpu else None
+    line = {
+        "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": K,
+        "warmup": args.warmup, "ms_per_step": 1e3 * elapsed_a / K, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: seeded analytic scene (floor, box, 3 spheres), ray-cast depth with "
+                "sigma(z)=0.0012+0.0019(z-0.4)^2 noise, Perlin albedo RGB",
+        "config": config_block(args, p),
+        "latency_ms": {"p50": p50, "p99": p99, "what": "host submit->result per frame, pass B"},
+        "stages_ms": stage_ms,
+        "e2e": {"value": world * K / elapsed_c, "unit": "frames/s",
+                "h2d_bytes_per_step": fbytes_d + (fbytes_c if has_rgb else 0),
+                "d2h_bytes_per_step": int(lib.dyn_frame_d2h_bytes())},
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+        "gpu_launches": int(kpf.value) * K,
+        "kernels_per_frame": int(kpf.value),
+        "ate_gt_mm": ate * 1e3,
+        "map": {"blocks_total": st_avg["blocks_total"], "visible_per_frame": st_avg["blocks_visible"],
+                "load_factor": st_avg["blocks_total"] / (t.num_buckets * t.bucket_size)},
+    }
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="cfg2")
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--ref-seconds", type=float, default=90.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

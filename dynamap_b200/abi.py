@@ -18,6 +18,8 @@ STATUS = {0: "ok", 1: "invalid argument", 2: "out of device memory",
           8: "cuda error", 9: "not ready", 10: "no cuda device"}
 DYN_ERR_HASH_FULL = 4
 DYN_ERR_HEAP_EXHAUSTED = 5
+STAGES = ["ingest", "bilateral", "source_maps", "icp", "allocate", "visible", "integrate",
+          "raycast", "target_maps", "frame"]
 PRECISION_FP32 = 0
 PRECISION_MIXED = 1
 
@@ -108,6 +110,11 @@ SIGNATURES = {
     "dyn_icp_normal_equations": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, P(Sensor), P(GnParams),
                                            P(C.c_float), P(C.c_double), _vp]),
     "dyn_sessions_submit": (C.c_int, [P(_vp), C.c_int32, P(_vp), P(_vp)]),
+    "dyn_session_stream": (C.c_int, [_vp, P(_vp)]),
+    "dyn_session_profile": (C.c_int, [_vp, C.c_int32]),
+    "dyn_session_stage_times": (C.c_int, [_vp, P(C.c_double), P(C.c_int64), C.c_int32]),
+    "dyn_session_kernels_per_frame": (C.c_int, [_vp, P(C.c_int32)]),
+    "dyn_frame_d2h_bytes": (C.c_size_t, []),
 }
 
 _lib = None

@@ -20,7 +20,7 @@ LIB = os.path.join(HERE, "libdynamap_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 SOURCES = ["image.cu", "icp.cu", "tsdf.cu", "session.cu", "config.cpp"]
-HEADERS = ["common.cuh", "image.cuh", "icp.cuh", "tsdf.cuh"]
+HEADERS = ["common.cuh", "image.cuh", "icp.cuh", "tsdf.cuh", "dyn_exp.h"]
 
 # -fmad=false: no FMA contraction, IEEE div/sqrt: every float operation
 # rounds once, in source order (the bit-exact parity with the oracle relies

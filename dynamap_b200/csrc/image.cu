@@ -5,6 +5,11 @@
 // :126-157), include/solver/gnSolver/gnSolver.cu:457-465 (intensity).
 #include "image.cuh"
 
+#include <cmath>
+#include <cstring>
+
+#include "dyn_exp.h"
+
 namespace dyn {
 
 namespace {
@@ -28,31 +33,21 @@ __global__ void ingest_kernel(const uint16_t* __restrict__ raw,
 
 constexpr int BTX = 32, BTY = 8;
 
-// pyramid::gaussian, pyramid.cu:208-211 (double)
-__device__ inline double gaussian_d(double x, double sigma) {
-  return exp(-(x * x) / (2.0 * sigma * sigma)) / (2.0 * 3.14159265358979323846 * sigma * sigma);
-}
-
 // pyramid::applyBilateralFilter, pyramid.cu:213-233, one thread per pixel,
-// window rows x-(r)..x+r-1, cols y-r..y+r-1, summed row-major.  The depth
-// tile plus halo is staged in shared memory; the spatial weights (a pure
-// function of the tap offset) are built once per CTA in double and rounded
-// to float as the reference does per tap.  Taps outside the image or with
-// depth <= 0 are skipped and invalid centres stay 0.
+// window rows x-r..x+r-1, cols y-r..y+r-1, summed row-major.  The depth tile
+// plus halo is staged in shared memory; the spatial weights, a pure function
+// of the tap offset, come precomputed on the host in double and rounded to
+// float exactly as the reference rounds them per tap (kernel parameter,
+// read as warp-uniform constants).  The range weight uses dyn_expf, the
+// same operation sequence the oracle runs, so the filtered depth is
+// bit-identical to the oracle's.  Taps outside the image or with depth <= 0
+// are skipped and invalid centres stay 0.
 __global__ void bilateral_kernel(const float* __restrict__ src, float* __restrict__ dst,
-                                 int rows, int cols, int r, float sigma_i, float sigma_s) {
-  extern __shared__ float sm[];
-  const int D = 2 * r, half = r;
-  float* gs = sm;                        // D*D
+                                 int rows, int cols, const __grid_constant__ BilateralTable tb) {
+  extern __shared__ float tile[];
+  const int D = 2 * tb.radius, half = tb.radius;
   const int TW = BTX + D - 1, TH = BTY + D - 1;
-  float* tile = sm + D * D;              // TH*TW (rows x cols)
   const int tid = threadIdx.y * BTX + threadIdx.x;
-  for (int k = tid; k < D * D; k += BTX * BTY) {
-    int i = k / D, j = k - (k / D) * D;
-    float dx = (float)(half - i), dy = (float)(half - j);
-    float dd = sqrtf(dx * dx + dy * dy + 0.0f * 0.0f);
-    gs[k] = (float)gaussian_d((double)dd, (double)sigma_s);
-  }
   const int row0 = blockIdx.y * BTY - half, col0 = blockIdx.x * BTX - half;
   for (int k = tid; k < TW * TH; k += BTX * BTY) {
     int tr = k / TW, tc = k - (k / TW) * TW;
@@ -68,23 +63,18 @@ __global__ void bilateral_kernel(const float* __restrict__ src, float* __restric
     dst[x * cols + y] = 0.0f;
     return;
   }
-  const float k_norm = (float)(1.0 / (2.0 * 3.14159265358979323846 * (double)sigma_i *
-                                      (double)sigma_i));
-  const float k_exp = 2.0f * sigma_i * sigma_i;
   float acc = 0.0f, wp = 0.0f;
   for (int i = 0; i < D; ++i) {
     int nx = x - (half - i);
     if (nx < 0 || nx >= rows) continue;
     const float* trow = tile + (threadIdx.y + i) * TW + threadIdx.x;
-    const float* grow = gs + i * D;
     for (int j = 0; j < D; ++j) {
       int ny = y - (half - j);
       if (ny < 0 || ny >= cols) continue;
       float nv = trow[j];
       if (!(nv > 0.0f)) continue;
-      float dv = nv - c;
-      float gi = expf(-(dv * dv) / k_exp) * k_norm;
-      float w = gi * grow[j];
+      float gi = range_weight(nv - c, tb.inv2s2, tb.norm);
+      float w = gi * tb.gs[i * D + j];
       acc += nv * w;
       wp += w;
     }
@@ -184,13 +174,36 @@ void launch_ingest(const uint16_t* raw, const uint8_t* rgb, int n, float scaler,
   ingest_kernel<<<nblk(n, 256), 256, 0, st>>>(raw, rgb, n, scaler, depth_out, intensity_out);
 }
 
-void launch_bilateral(const float* src, float* dst, int rows, int cols, int radius,
-                      float sigma_i, float sigma_s, cudaStream_t st) {
-  int D = 2 * radius;
-  size_t smem = sizeof(float) * ((size_t)D * D + (size_t)(BTX + D - 1) * (BTY + D - 1));
+// pyramid::gaussian, pyramid.cu:208-211, in double.
+static double gaussian_d(double x, double sigma) {
+  return std::exp(-(std::pow(x, 2)) / (2 * std::pow(sigma, 2))) /
+         (2 * 3.14159265358979323846 * std::pow(sigma, 2));
+}
+
+BilateralTable make_bilateral_table(int radius, float sigma_i, float sigma_s) {
+  BilateralTable tb;
+  std::memset(&tb, 0, sizeof(tb));
+  tb.radius = radius;
+  const int D = 2 * radius, half = radius;
+  for (int i = 0; i < D; ++i)
+    for (int j = 0; j < D; ++j) {
+      // vertexDistance (pyramid.cu:201-206) in float, gaussian in double
+      float dx = (float)(half - i), dy = (float)(half - j);
+      float dd = std::sqrt(dx * dx + dy * dy + 0.0f * 0.0f);
+      tb.gs[i * D + j] = (float)gaussian_d((double)dd, (double)sigma_s);
+    }
+  double si = (double)sigma_i;
+  tb.inv2s2 = (float)(1.0 / (2.0 * si * si));
+  tb.norm = (float)(1.0 / (2.0 * 3.14159265358979323846 * si * si));
+  return tb;
+}
+
+void launch_bilateral(const float* src, float* dst, int rows, int cols, const BilateralTable& tb,
+                      cudaStream_t st) {
+  int D = 2 * tb.radius;
+  size_t smem = sizeof(float) * ((size_t)(BTX + D - 1) * (BTY + D - 1));
   dim3 grid(nblk(cols, BTX), nblk(rows, BTY));
-  bilateral_kernel<<<grid, dim3(BTX, BTY), smem, st>>>(src, dst, rows, cols, radius, sigma_i,
-                                                       sigma_s);
+  bilateral_kernel<<<grid, dim3(BTX, BTY), smem, st>>>(src, dst, rows, cols, tb);
 }
 
 void launch_downsample_depth(const float* src, int rows, int cols, float* dst, cudaStream_t st) {

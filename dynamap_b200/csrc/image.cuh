@@ -17,11 +17,21 @@ struct MapsArgs {
   int total;
 };
 
+// Bilateral filter constants: spatial weights per tap offset (row-major
+// 2r x 2r, r <= 16) and the range-weight constants.
+struct BilateralTable {
+  float gs[32 * 32];
+  int radius;
+  float inv2s2;  // 1 / (2 sigma_i^2)
+  float norm;    // 1 / (2 pi sigma_i^2)
+};
+BilateralTable make_bilateral_table(int radius, float sigma_i, float sigma_s);
+
 // Launchers (all asynchronous on 'st').
 void launch_ingest(const uint16_t* raw, const uint8_t* rgb, int n, float scaler,
                    float* depth_out, float* intensity_out, cudaStream_t st);
 void launch_bilateral(const float* src, float* dst, int rows, int cols,
-                      int radius, float sigma_i, float sigma_s, cudaStream_t st);
+                      const BilateralTable& tb, cudaStream_t st);
 void launch_downsample_depth(const float* src, int rows, int cols, float* dst,
                              cudaStream_t st);
 void launch_downsample_intensity(const float* src, int rows, int cols, float* dst,

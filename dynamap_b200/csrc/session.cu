@@ -138,6 +138,13 @@ struct dyn_session {
   ResultBlock* h_res = nullptr;
   // graphs: [has_rgb]
   cudaGraphExec_t exec[2] = {nullptr, nullptr};
+  BilateralTable btab;
+  // profiling: ev[i] ends stage i (DYN_STAGE_*), ev[DYN_STAGE_FRAME] starts the frame
+  bool profile = false;
+  cudaEvent_t ev[DYN_NUM_STAGES] = {};
+  double stage_ms[DYN_NUM_STAGES] = {};
+  int64_t prof_frames = 0;
+  int kernels_per_frame[2] = {0, 0};
   bool debug_maps = false;
   int frames = 0;
   bool pending = false;
@@ -186,6 +193,8 @@ void release(dyn_session* s) {
   if (s->h_rgb) cudaFreeHost(s->h_rgb);
   if (s->h_res) cudaFreeHost(s->h_res);
   if (s->h2d_done) cudaEventDestroy(s->h2d_done);
+  for (int k = 0; k < DYN_NUM_STAGES; ++k)
+    if (s->ev[k]) cudaEventDestroy(s->ev[k]);
   if (s->stream) cudaStreamDestroy(s->stream);
   cudaSetDevice(prev);
   delete s;
@@ -226,6 +235,11 @@ MapsArgs maps_args(dyn_session* s, bool target) {
   return a;
 }
 
+// Stage boundary event (profiling only; captured into the frame graph).
+void mark(dyn_session* s, int stage) {
+  if (s->profile) cudaEventRecord(s->ev[stage], s->stream);
+}
+
 __global__ void mark_target_kernel(IcpState* st) {
   if (threadIdx.x == 0 && blockIdx.x == 0) st->have_target = 1;
 }
@@ -238,13 +252,15 @@ void enqueue_source(dyn_session* s, bool has_rgb) {
   cudaStream_t st = s->stream;
   const int n = (int)s->npx;
   const bool col = s->use_color();
+  mark(s, DYN_STAGE_FRAME);
   launch_ingest(s->d_u16, has_rgb ? s->d_rgb : nullptr, n, s->sensor.depth_scaler, s->d_raw,
                 col ? s->d_sint[0] : nullptr, st);
+  mark(s, DYN_STAGE_INGEST);
   if (s->bp.enabled)
-    launch_bilateral(s->d_raw, s->d_filt, (int)s->sensor.rows, (int)s->sensor.cols,
-                     s->bp.diameter, s->bp.sigma_i, s->bp.sigma_s, st);
+    launch_bilateral(s->d_raw, s->d_filt, (int)s->sensor.rows, (int)s->sensor.cols, s->btab, st);
   else
     launch_copy_f(s->d_raw, s->d_filt, s->npx, st);
+  mark(s, DYN_STAGE_BILATERAL);
   for (int l = 1; l < s->nlev; ++l) {
     launch_downsample_depth(s->d_sdep[l - 1], s->ls[l - 1].rows, s->ls[l - 1].cols, s->d_sdep[l], st);
     if (col)
@@ -252,17 +268,22 @@ void enqueue_source(dyn_session* s, bool has_rgb) {
                                   s->d_sint[l], st);
   }
   launch_maps(maps_args(s, false), st);
+  mark(s, DYN_STAGE_SOURCE_MAPS);
 }
 
 // Integration at the session pose, then the next frame's target.
 void enqueue_map_update(dyn_session* s, bool has_rgb) {
   cudaStream_t st = s->stream;
   launch_allocate(s->vol, s->d_raw, s->ls[0], s->d_pose, st);
+  mark(s, DYN_STAGE_ALLOCATE);
   launch_visible(s->vol, s->ls[0], s->d_pose, st);
+  mark(s, DYN_STAGE_VISIBLE);
   launch_integrate(s->vol, s->d_raw, has_rgb ? s->d_rgb : nullptr, s->ls[0], s->d_pose, st);
+  mark(s, DYN_STAGE_INTEGRATE);
   const bool col = s->use_color();
   if (s->gp.mode == 1) {
     launch_raycast(s->vol, s->ls[0], s->d_pose, nullptr, s->d_ray, col ? s->d_trgb : nullptr, st);
+    mark(s, DYN_STAGE_RAYCAST);
     launch_target_prepare(s->d_ray, s->d_tdep[0], s->tp.max_sensor_depth,
                           col ? s->d_trgb : nullptr, col ? s->d_tint[0] : nullptr, (int)s->npx, st);
     for (int l = 1; l < s->nlev; ++l) {
@@ -281,8 +302,10 @@ void enqueue_map_update(dyn_session* s, bool has_rgb) {
                     reinterpret_cast<float*>(s->d_tnrm[l]), 4 * n, st);
       if (col) launch_copy_f(s->d_sint[l], s->d_tint[l], n, st);
     }
+    mark(s, DYN_STAGE_RAYCAST);
   }
   mark_target_kernel<<<1, 32, 0, st>>>(s->d_icp);
+  mark(s, DYN_STAGE_TARGET_MAPS);
 }
 
 // builder::buildModelLS with the intended order: track frame k against the
@@ -308,6 +331,7 @@ void enqueue_frame(dyn_session* s, bool has_rgb) {
   }
   launch_pose_finalize(P, s->d_icp, s->d_pose, st);
   bump_frame_kernel<<<1, 32, 0, st>>>(s->d_pose);
+  mark(s, DYN_STAGE_ICP);
   enqueue_map_update(s, has_rgb);
 }
 
@@ -317,6 +341,16 @@ dyn_status build_graph(dyn_session* s, bool has_rgb) {
   enqueue_frame(s, has_rgb);
   cudaError_t e = cudaStreamEndCapture(s->stream, &g);
   if (e != cudaSuccess) return DYN_ERR_CUDA;
+  size_t nn = 0;
+  cudaGraphGetNodes(g, nullptr, &nn);
+  std::vector<cudaGraphNode_t> nodes(nn);
+  if (nn) cudaGraphGetNodes(g, nodes.data(), &nn);
+  int nk = 0;
+  for (size_t i = 0; i < nn; ++i) {
+    cudaGraphNodeType ty;
+    if (cudaGraphNodeGetType(nodes[i], &ty) == cudaSuccess && ty == cudaGraphNodeTypeKernel) ++nk;
+  }
+  s->kernels_per_frame[has_rgb ? 1 : 0] = nk;
   cudaGraphExec_t ex = nullptr;
   e = cudaGraphInstantiate(&ex, g, 0);
   cudaGraphDestroy(g);
@@ -508,6 +542,7 @@ dyn_status dyn_session_create(const dyn_tsdf_params* tsdf, const dyn_gn_params* 
   for (int k = 0; k < 3; ++k) maxl = std::max(maxl, level_of_scale(gn->lvl_scale[k]));
   s->nlev = maxl + 1;
   for (int l = 0; l < kLevels; ++l) s->ls[l] = dsensor(level_sensor(*sensor, 1 << l));
+  if (bil->enabled) s->btab = make_bilateral_table(bil->diameter, bil->sigma_i, bil->sigma_s);
   dyn_status r = DYN_OK;
 #define TRY(x)               \
   do {                       \
@@ -632,6 +667,19 @@ dyn_status dyn_frame_result(dyn_session* s, float pose_out[16], dyn_frame_stats*
   DeviceGuard dg(s->device);
   DYN_CUDA(cudaStreamSynchronize(s->stream));
   s->pending = false;
+  if (s->profile) {
+    float ms = 0.0f;
+    int prev = DYN_STAGE_FRAME;
+    for (int k = 0; k <= DYN_STAGE_TARGET_MAPS; ++k) {
+      if (cudaEventElapsedTime(&ms, s->ev[prev], s->ev[k]) == cudaSuccess) s->stage_ms[k] += ms;
+      prev = k;
+    }
+    if (cudaEventElapsedTime(&ms, s->ev[DYN_STAGE_FRAME], s->ev[DYN_STAGE_TARGET_MAPS]) ==
+        cudaSuccess)
+      s->stage_ms[DYN_STAGE_FRAME] += ms;
+    cudaGetLastError();
+    s->prof_frames++;
+  }
   if (pose_out)
     for (int k = 0; k < 16; ++k) pose_out[k] = (float)s->h_res->pose.pose[k];
   if (stats) fill_stats(s, *s->h_res, stats);
@@ -754,13 +802,58 @@ dyn_status dyn_debug_image(dyn_session* s, int32_t which, int32_t level, void* h
   return DYN_OK;
 }
 
+dyn_status dyn_session_stream(dyn_session* s, void** stream_out) {
+  if (!s || !stream_out) return DYN_ERR_INVALID_ARG;
+  *stream_out = (void*)s->stream;
+  return DYN_OK;
+}
+
+dyn_status dyn_session_profile(dyn_session* s, int32_t enable) {
+  if (!s) return DYN_ERR_INVALID_ARG;
+  DeviceGuard dg(s->device);
+  DYN_CUDA(cudaStreamSynchronize(s->stream));
+  bool en = enable != 0;
+  if (en && !s->ev[0])
+    for (int k = 0; k < DYN_NUM_STAGES; ++k) DYN_CUDA(cudaEventCreate(&s->ev[k]));
+  if (en != s->profile) {
+    for (int k = 0; k < 2; ++k)
+      if (s->exec[k]) {
+        cudaGraphExecDestroy(s->exec[k]);
+        s->exec[k] = nullptr;
+      }
+    s->profile = en;
+  }
+  return DYN_OK;
+}
+
+dyn_status dyn_session_stage_times(dyn_session* s, double ms_out[DYN_NUM_STAGES],
+                                   int64_t* frames_out, int32_t reset) {
+  if (!s) return DYN_ERR_INVALID_ARG;
+  if (ms_out)
+    for (int k = 0; k < DYN_NUM_STAGES; ++k) ms_out[k] = s->stage_ms[k];
+  if (frames_out) *frames_out = s->prof_frames;
+  if (reset) {
+    for (int k = 0; k < DYN_NUM_STAGES; ++k) s->stage_ms[k] = 0.0;
+    s->prof_frames = 0;
+  }
+  return DYN_OK;
+}
+
+size_t dyn_frame_d2h_bytes(void) { return sizeof(PoseState) + sizeof(IcpState) + sizeof(Counters); }
+
+dyn_status dyn_session_kernels_per_frame(dyn_session* s, int32_t* n_out) {
+  if (!s || !n_out) return DYN_ERR_INVALID_ARG;
+  *n_out = std::max(s->kernels_per_frame[0], s->kernels_per_frame[1]);
+  return DYN_OK;
+}
+
 dyn_status dyn_bilateral_filter(const float* depth_dev, float* out_dev, uint32_t rows, uint32_t cols,
                                 const dyn_bilateral_params* p, void* stream) {
   if (!depth_dev || !out_dev || !p || rows == 0 || cols == 0 || p->diameter < 1 ||
       p->diameter > 16 || !(p->sigma_i > 0) || !(p->sigma_s > 0))
     return DYN_ERR_INVALID_ARG;
-  launch_bilateral(depth_dev, out_dev, (int)rows, (int)cols, p->diameter, p->sigma_i, p->sigma_s,
-                   (cudaStream_t)stream);
+  BilateralTable tb = make_bilateral_table(p->diameter, p->sigma_i, p->sigma_s);
+  launch_bilateral(depth_dev, out_dev, (int)rows, (int)cols, tb, (cudaStream_t)stream);
   DYN_CUDA(cudaGetLastError());
   return DYN_OK;
 }

@@ -237,6 +237,39 @@ dyn_status dyn_download_blocks(dyn_session* s, int32_t* coords_out,
 dyn_status dyn_debug_image(dyn_session* s, int32_t which, int32_t level,
                            void* host_out, size_t bytes);
 
+/* ---- measurement --------------------------------------------------------
+ * The reference times frames with gettimeofday around the whole loop
+ * (src/dynaMap.cpp:220,295-299, include/utils/utils_Timer.h:15-33); these
+ * expose device-side timing of each stage instead. */
+enum {
+  DYN_STAGE_INGEST = 0,     /* u16 -> metres (+ intensity) */
+  DYN_STAGE_BILATERAL = 1,
+  DYN_STAGE_SOURCE_MAPS = 2, /* pyramid + normal maps of the new frame */
+  DYN_STAGE_ICP = 3,         /* all GN iterations + pose update */
+  DYN_STAGE_ALLOCATE = 4,
+  DYN_STAGE_VISIBLE = 5,
+  DYN_STAGE_INTEGRATE = 6,
+  DYN_STAGE_RAYCAST = 7,
+  DYN_STAGE_TARGET_MAPS = 8, /* pyramid + normal maps of the raycast */
+  DYN_STAGE_FRAME = 9,       /* whole frame, first to last kernel */
+  DYN_NUM_STAGES = 10
+};
+/* The session's CUDA stream (a cudaStream_t), for callers that record their
+ * own events around dyn_frame_submit. */
+dyn_status dyn_session_stream(dyn_session* s, void** stream_out);
+/* enable != 0: every frame records a CUDA event between stages (inside the
+ * frame's graph); dyn_frame_result accumulates the stage times. */
+dyn_status dyn_session_profile(dyn_session* s, int32_t enable);
+/* Accumulated device milliseconds per stage since the last reset and the
+ * number of frames they cover; reset != 0 clears the accumulators. */
+dyn_status dyn_session_stage_times(dyn_session* s, double ms_out[DYN_NUM_STAGES],
+                                   int64_t* frames_out, int32_t reset);
+/* Kernels one frame launches (nodes of the frame graph). */
+dyn_status dyn_session_kernels_per_frame(dyn_session* s, int32_t* n_out);
+/* Bytes each submitted frame copies device -> host (pose, solver state and
+ * counters read back by dyn_frame_result). */
+size_t dyn_frame_d2h_bytes(void);
+
 /* ---- stage entry points on caller device buffers ----------------------
  * These run one stage of the path on caller-owned device memory, on
  * 'stream' (a cudaStream_t, NULL = legacy default stream), and return once

@@ -29,6 +29,9 @@
 #include "dynoracle.h"
 
 #include <algorithm>
+#include <cmath>
+
+#include "../dynamap_b200/csrc/dyn_exp.h"
 #include <cfloat>
 #include <cmath>
 #include <cstdint>
@@ -634,6 +637,11 @@ void bilateral(const R* src, R* dst, int rows, int cols, int r, double sI,
       float dd = std::sqrt(dx * dx + dy * dy + 0.0f * 0.0f);
       gs[(size_t)i * diameter + j] = (R)(float)gaussian_d((double)dd, sS);
     }
+  // range weight: FP32 through dyn_expf (dynamap_b200/csrc/dyn_exp.h), the
+  // operation sequence the CUDA kernel runs; FP64 through exp, as
+  // pyramid.cu:208-211 computes it.
+  const float inv2s2 = (float)(1.0 / (2.0 * sI * sI));
+  const float norm = (float)(1.0 / (2.0 * M_PI * sI * sI));
   int nt = std::max(1, g_threads);
 #pragma omp parallel for num_threads(nt) schedule(static)
   for (int x = 0; x < rows; ++x) {
@@ -653,8 +661,9 @@ void bilateral(const R* src, R* dst, int rows, int cols, int r, double sI,
           if (ny < 0 || ny >= cols) continue;
           R nv = src[nx * cols + ny];
           if (!(nv > 0)) continue;
-          R gi = (R)(float)gaussian_d((double)(float)(nv - c), sI);
+          R gi;
           if (sizeof(R) == 8) gi = (R)gaussian_d((double)(nv - c), sI);
+          else gi = (R)dyn::range_weight((float)(nv - c), inv2s2, norm);
           R w = gi * gs[(size_t)i * diameter + j];
           acc += nv * w;
           wp += w;

@@ -207,8 +207,9 @@ def rot_angle(R):
     return float(np.arccos(np.clip((np.trace(R) - 1) / 2, -1, 1)))
 
 
-def test_tracking_matches_oracle(gpu_lib, oracle, seq_cfg1):
-    p = small_cfg1()
+@pytest.mark.parametrize("bilateral", [1, 0])
+def test_tracking_matches_oracle(gpu_lib, oracle, seq_cfg1, bilateral):
+    p = small_cfg1(bilateral=dict(enabled=bilateral))
     t, g, b, s = configs.structs(p)
     os_ = oracle.Session(t, g, b, s)
     os_.set_pose(seq_cfg1.poses[0])
