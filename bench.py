@@ -267,6 +267,8 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
     p = configs.preset(args.config)
+    if args.max_blocks:
+        p["tsdf"]["num_blocks"] = min(p["tsdf"]["num_blocks"], args.max_blocks)
     t, g, b, s = configs.structs(p)
     lib = abi.load()
     P = s.rows * s.cols
@@ -438,6 +440,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--ref-seconds", type=float, default=90.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--max-blocks", type=int, default=0,
+                    help="cap the voxel-block pool (small profiling runs)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

@@ -115,6 +115,8 @@ SIGNATURES = {
     "dyn_session_stage_times": (C.c_int, [_vp, P(C.c_double), P(C.c_int64), C.c_int32]),
     "dyn_session_kernels_per_frame": (C.c_int, [_vp, P(C.c_int32)]),
     "dyn_frame_d2h_bytes": (C.c_size_t, []),
+    "dyn_solver_solve": (C.c_int, [_vp, _vp, _vp, _vp, _vp, P(C.c_float), P(C.c_double),
+                                   P(FrameStats)]),
 }
 
 _lib = None

@@ -237,7 +237,8 @@ MapsArgs maps_args(dyn_session* s, bool target) {
 
 // Stage boundary event (profiling only; captured into the frame graph).
 void mark(dyn_session* s, int stage) {
-  if (s->profile) cudaEventRecord(s->ev[stage], s->stream);
+  // External: during capture this becomes an event-record node of the graph
+  if (s->profile) cudaEventRecordWithFlags(s->ev[stage], s->stream, cudaEventRecordExternal);
 }
 
 __global__ void mark_target_kernel(IcpState* st) {
@@ -311,10 +312,8 @@ void enqueue_map_update(dyn_session* s, bool has_rgb) {
 // builder::buildModelLS with the intended order: track frame k against the
 // target of frame k-1, integrate frame k at the new pose, raycast the target
 // for frame k+1.
-void enqueue_frame(dyn_session* s, bool has_rgb) {
+void enqueue_icp(dyn_session* s) {
   cudaStream_t st = s->stream;
-  reset_frame_counters(s);
-  enqueue_source(s, has_rgb);
   IcpParams P = s->icp_params();
   for (int pl = 0; pl < 3; ++pl) {
     int l = level_of_scale(s->gp.lvl_scale[pl]);
@@ -330,7 +329,13 @@ void enqueue_frame(dyn_session* s, bool has_rgb) {
       launch_icp_iteration(L, P, pl, it, s->d_icp, s->d_partials, st);
   }
   launch_pose_finalize(P, s->d_icp, s->d_pose, st);
-  bump_frame_kernel<<<1, 32, 0, st>>>(s->d_pose);
+}
+
+void enqueue_frame(dyn_session* s, bool has_rgb) {
+  reset_frame_counters(s);
+  enqueue_source(s, has_rgb);
+  enqueue_icp(s);
+  bump_frame_kernel<<<1, 32, 0, s->stream>>>(s->d_pose);
   mark(s, DYN_STAGE_ICP);
   enqueue_map_update(s, has_rgb);
 }
@@ -709,6 +714,57 @@ dyn_status dyn_integrate_with_pose(dyn_session* s, const uint16_t* depth_host,
   const Counters& c = s->h_res->cnt;
   if (c.heap_exhausted) return DYN_ERR_HEAP_EXHAUSTED;
   if (c.bucket_full) return DYN_ERR_HASH_FULL;
+  return DYN_OK;
+}
+
+dyn_status dyn_solver_solve(dyn_session* s, const float* target_depth_host,
+                            const uint8_t* target_rgb_host, const float* source_depth_host,
+                            const uint8_t* source_rgb_host, float pose_inout[16],
+                            double increment_out[6], dyn_frame_stats* stats) {
+  if (!s || !target_depth_host || !source_depth_host || !pose_inout) return DYN_ERR_INVALID_ARG;
+  DeviceGuard dg(s->device);
+  cudaStream_t st = s->stream;
+  const size_t n = s->npx;
+  const bool col = s->use_color();
+  const float inf = 3.402823466e+38f;
+  dyn_status r = dyn_session_set_pose(s, pose_inout);
+  if (r != DYN_OK) return r;
+  // target: images as given (the reference solves on raw images,
+  // builder.cu:91-99), pyramid + normals
+  DYN_CUDA(cudaMemcpyAsync(s->d_ray, target_depth_host, n * 4, cudaMemcpyHostToDevice, st));
+  if (col && target_rgb_host)
+    DYN_CUDA(cudaMemcpyAsync(s->d_trgb, target_rgb_host, n * 3, cudaMemcpyHostToDevice, st));
+  launch_target_prepare(s->d_ray, s->d_tdep[0], inf, (col && target_rgb_host) ? s->d_trgb : nullptr,
+                        col ? s->d_tint[0] : nullptr, (int)n, st);
+  // source
+  DYN_CUDA(cudaMemcpyAsync(s->d_raw, source_depth_host, n * 4, cudaMemcpyHostToDevice, st));
+  if (col && source_rgb_host)
+    DYN_CUDA(cudaMemcpyAsync(s->d_rgb, source_rgb_host, n * 3, cudaMemcpyHostToDevice, st));
+  launch_target_prepare(s->d_raw, s->d_sdep[0], inf, (col && source_rgb_host) ? s->d_rgb : nullptr,
+                        col ? s->d_sint[0] : nullptr, (int)n, st);
+  for (int l = 1; l < s->nlev; ++l) {
+    launch_downsample_depth(s->d_tdep[l - 1], s->ls[l - 1].rows, s->ls[l - 1].cols, s->d_tdep[l], st);
+    launch_downsample_depth(s->d_sdep[l - 1], s->ls[l - 1].rows, s->ls[l - 1].cols, s->d_sdep[l], st);
+    if (col) {
+      launch_downsample_intensity(s->d_tint[l - 1], s->ls[l - 1].rows, s->ls[l - 1].cols,
+                                  s->d_tint[l], st);
+      launch_downsample_intensity(s->d_sint[l - 1], s->ls[l - 1].rows, s->ls[l - 1].cols,
+                                  s->d_sint[l], st);
+    }
+  }
+  launch_maps(maps_args(s, true), st);
+  launch_maps(maps_args(s, false), st);
+  mark_target_kernel<<<1, 32, 0, st>>>(s->d_icp);
+  enqueue_icp(s);
+  DYN_CUDA(cudaMemcpyAsync(s->h_res, s->d_pose, sizeof(PoseState), cudaMemcpyDeviceToHost, st));
+  DYN_CUDA(cudaMemcpyAsync(&s->h_res->icp, s->d_icp, sizeof(IcpState), cudaMemcpyDeviceToHost, st));
+  DYN_CUDA(cudaMemcpyAsync(&s->h_res->cnt, s->vol.cnt, sizeof(Counters), cudaMemcpyDeviceToHost, st));
+  DYN_CUDA(cudaStreamSynchronize(st));
+  DYN_CUDA(cudaGetLastError());
+  for (int k = 0; k < 16; ++k) pose_inout[k] = (float)s->h_res->pose.pose[k];
+  if (increment_out)
+    for (int k = 0; k < 6; ++k) increment_out[k] = s->h_res->pose.last_inc[k];
+  if (stats) fill_stats(s, *s->h_res, stats);
   return DYN_OK;
 }
 

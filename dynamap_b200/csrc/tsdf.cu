@@ -321,33 +321,22 @@ struct BlockCache {
   int ptr;
 };
 
-// tsdf.cu:189-225: global voxel index by round-half-away of pos/voxelSize,
-// block by floor division, local index by non-negative remainder.
-__device__ inline void world_to_voxel(F3 pos, float vs, int* bx, int* by, int* bz, int* lin) {
-  int g[3];
-  float pv[3] = {pos.x, pos.y, pos.z};
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    float sg = (float)((pv[k] > 0.0f) - (pv[k] < 0.0f));
-    g[k] = (int)(pv[k] / vs + sg * 0.5f);
-  }
-  int b[3], l[3];
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    b[k] = g[k] < 0 ? (g[k] - kBlockSize + 1) / kBlockSize : g[k] / kBlockSize;
-    l[k] = g[k] % kBlockSize;
-    if (l[k] < 0) l[k] += kBlockSize;
-  }
-  *bx = b[0];
-  *by = b[1];
-  *bz = b[2];
-  *lin = l[0] * kBlockSize * kBlockSize + l[1] * kBlockSize + l[2];
+// tsdf.cu:189-225 for one axis: global voxel index by round-half-away of
+// p / voxelSize (IEEE division), block by floor division, local index by
+// non-negative remainder.
+__device__ inline void axis_voxel(float p, float vs, int* blk, int* loc) {
+  float sg = (float)((p > 0.0f) - (p < 0.0f));
+  int g = (int)(p / vs + sg * 0.5f);
+  *blk = g < 0 ? (g - kBlockSize + 1) / kBlockSize : g / kBlockSize;
+  int r = g % kBlockSize;
+  *loc = r < 0 ? r + kBlockSize : r;
 }
 
-// tsdfVolume::GetVoxel, tsdf.cu:227-239, with a one-block lookup cache.
-__device__ inline uint2 get_voxel(const VolumeDev& v, F3 pos, BlockCache& bc) {
-  int bx, by, bz, lin;
-  world_to_voxel(pos, v.t.vs, &bx, &by, &bz, &lin);
+// tsdfVolume::GetVoxel, tsdf.cu:227-239, for a voxel already resolved to
+// (block, local index); a one-block lookup cache skips repeated bucket
+// scans of the same block.
+__device__ inline uint2 fetch_voxel(const VolumeDev& v, int bx, int by, int bz, int lin,
+                                    BlockCache& bc) {
   unsigned long long key = pack_key(bx, by, bz);
   if (key != bc.key) {
     bc.key = key;
@@ -357,10 +346,24 @@ __device__ inline uint2 get_voxel(const VolumeDev& v, F3 pos, BlockCache& bc) {
   return __ldg(reinterpret_cast<const uint2*>(v.voxels + (size_t)bc.ptr * kBlockVox + lin));
 }
 
+__device__ inline uint2 get_voxel(const VolumeDev& v, F3 pos, BlockCache& bc) {
+  int bx, by, bz, lx, ly, lz;
+  axis_voxel(pos.x, v.t.vs, &bx, &lx);
+  axis_voxel(pos.y, v.t.vs, &by, &ly);
+  axis_voxel(pos.z, v.t.vs, &bz, &lz);
+  return fetch_voxel(v, bx, by, bz, (lx * kBlockSize + ly) * kBlockSize + lz, bc);
+}
+
 __device__ inline int vw(uint2 r) { return (int)(r.x >> 24); }
 __device__ inline float vsdf(uint2 r) { return __uint_as_float(r.y); }
 
-// tsdfVolume::GetInterpolatedVoxel, tsdf.cu:47-175.
+// tsdfVolume::GetInterpolatedVoxel, tsdf.cu:47-175.  The eight corners are
+// pos_dual + {0, vs} per axis, so each axis has two coordinate values: they
+// are resolved once (six index computations instead of twenty-four) and
+// combined per corner; every corner still gets exactly the reference's
+// float coordinate.  Corners are summed in the reference's order.  COLOR
+// false skips the colour sums (the marching loop only reads sdf/weight).
+template <bool COLOR>
 __device__ inline VoxelSample get_interpolated(const VolumeDev& v, F3 position, BlockCache& bc) {
   VoxelSample out;
   uint2 v0 = get_voxel(v, position, bc);
@@ -377,23 +380,33 @@ __device__ inline VoxelSample get_interpolated(const VolumeDev& v, F3 position, 
   const float inv = 1.0f / vs;
   F3 vp = position * inv;
   F3 wt = f3(vp.x - floorf(vp.x), vp.y - floorf(vp.y), vp.z - floorf(vp.z));
+  int bxv[2], lxv[2], byv[2], lyv[2], bzv[2], lzv[2];
+  axis_voxel(pos_dual.x + 0.0f, vs, &bxv[0], &lxv[0]);
+  axis_voxel(pos_dual.x + vs, vs, &bxv[1], &lxv[1]);
+  axis_voxel(pos_dual.y + 0.0f, vs, &byv[0], &lyv[0]);
+  axis_voxel(pos_dual.y + vs, vs, &byv[1], &lyv[1]);
+  axis_voxel(pos_dual.z + 0.0f, vs, &bzv[0], &lzv[0]);
+  axis_voxel(pos_dual.z + vs, vs, &bzv[1], &lzv[1]);
   float dist = 0.0f;
   float cr = 0.0f, cg = 0.0f, cb = 0.0f;
   const int off[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1},
                          {1, 1, 0}, {0, 1, 1}, {1, 0, 1}, {1, 1, 1}};
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
-    F3 q = pos_dual + f3(off[k][0] ? vs : 0.0f, off[k][1] ? vs : 0.0f, off[k][2] ? vs : 0.0f);
-    uint2 vv = get_voxel(v, q, bc);
+    const int ox = off[k][0], oy = off[k][1], oz = off[k][2];
+    uint2 vv = fetch_voxel(v, bxv[ox], byv[oy], bzv[oz],
+                           (lxv[ox] * kBlockSize + lyv[oy]) * kBlockSize + lzv[oz], bc);
     uint2 src = (vw(vv) == 0) ? v0 : vv;
-    float a = off[k][0] ? wt.x : 1.0f - wt.x;
-    float b = off[k][1] ? wt.y : 1.0f - wt.y;
-    float c = off[k][2] ? wt.z : 1.0f - wt.z;
+    float a = ox ? wt.x : 1.0f - wt.x;
+    float b = oy ? wt.y : 1.0f - wt.y;
+    float c = oz ? wt.z : 1.0f - wt.z;
     float coef = a * b * c;
     dist += coef * vsdf(src);
-    cr = cr + (float)(src.x & 0xff) * coef;
-    cg = cg + (float)((src.x >> 8) & 0xff) * coef;
-    cb = cb + (float)((src.x >> 16) & 0xff) * coef;
+    if (COLOR) {
+      cr = cr + (float)(src.x & 0xff) * coef;
+      cg = cg + (float)((src.x >> 8) & 0xff) * coef;
+      cb = cb + (float)((src.x >> 16) & 0xff) * coef;
+    }
   }
   out.sdf = dist;
   out.r = cr;
@@ -433,7 +446,7 @@ __global__ void __launch_bounds__(kRayTX* kRayTY)
         break;
       }
       F3 point = xform(T, point3d(i, cur, s));
-      VoxelSample vx = get_interpolated(v, point, bc);
+      VoxelSample vx = get_interpolated<false>(v, point, bc);
       if (vx.w == 0) cur += t.trunc;
       else cur += vx.sdf;
       if (vx.w != 0 && vx.sdf < t.vs) break;
@@ -443,7 +456,7 @@ __global__ void __launch_bounds__(kRayTX* kRayTY)
       uint8_t r = 0, g = 0, b = 0;
       if (cur < t.dmax) {
         F3 point = xform(T, point3d(i, cur, s));
-        VoxelSample vx = get_interpolated(v, point, bc);
+        VoxelSample vx = get_interpolated<true>(v, point, bc);
         r = (uint8_t)vx.r;
         g = (uint8_t)vx.g;
         b = (uint8_t)vx.b;

@@ -1,0 +1,133 @@
+// builder/builder.h -- C++ drop-in for DynaMap::builder (reference
+// include/builder/builder.h:49-117, builder.cu), header-only over the C ABI
+// of dynamap.h: one session = one RGB-D stream with its own map.
+//
+// buildModelLS runs the per-frame path in the intended order (track the
+// frame against the previous target, integrate it at the new pose, raycast
+// the next target); Mode 0 tracks frame to frame, Mode 1 frame to model.
+// Frames are the sensor's uint16 depth + optional RGB (the reference reads
+// them through utils::dataSet, which is not part of this path).
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "../dynamap.h"
+#include "../dynamap/types.h"
+#include "../geometry/tsdf/tsdf.h"
+#include "../solver/gnSolver/gnSolver.h"
+
+namespace DynaMap {
+
+class builder {
+ public:
+  rgbdSensor sensor;
+  dyn_frame_stats lastStats{};
+  int frameNum = 0;
+
+  builder() = default;
+  builder(const builder&) = delete;
+  builder& operator=(const builder&) = delete;
+  virtual ~builder() {
+    if (session_) dyn_session_destroy(session_);
+  }
+
+  // builder.cu:11-49
+  void init(const tsdf::tsdfProperties& tsdfProp, const solver::Properties optimizerProp,
+            const rgbdSensor& s, const gaussianKernal& kernel, int device = 0,
+            int precision = DYN_PRECISION_FP32) {
+    sensor = s;
+    tsdf_ = tsdfProp.to_c();
+    opt_ = optimizerProp;
+    bil_.diameter = kernel.diameter;
+    bil_.sigma_i = kernel.sigmaI;
+    bil_.sigma_s = kernel.sigmaS;
+    bil_.enabled = 1;
+    device_ = device;
+    precision_ = precision;
+  }
+
+  // builder.cu:70-139
+  void buildModelLS(const uint16_t* depth, const uint8_t* rgb = nullptr, int Mode = 1) {
+    ensure(Mode);
+    dyn_throw("builder::buildModelLS", dyn_frame_submit(session_, depth, rgb));
+    float pose[16];
+    dyn_status r = dyn_frame_result(session_, pose, &lastStats);
+    if (r != DYN_ERR_HASH_FULL) dyn_throw("builder::buildModelLS", r);
+    currentPose_ = Matrix4f::from_row_major(pose);
+    ++frameNum;
+  }
+
+  // builder.cu:140-160: integrate at a known pose (no tracking)
+  void buildModelGT(const uint16_t* depth, const uint8_t* rgb, const Matrix4f& pose) {
+    ensure(mode_ < 0 ? 1 : mode_);
+    float4x4 p = pose.to_row_major();
+    dyn_throw("builder::buildModelGT", dyn_integrate_with_pose(session_, depth, rgb, p.entries));
+    currentPose_ = pose;
+    ++frameNum;
+  }
+
+  // builder.cu:263-283
+  void setInitialPose(const Matrix4f& pose) {
+    ensure(mode_ < 0 ? 1 : mode_);
+    float4x4 p = pose.to_row_major();
+    dyn_throw("builder::setInitialPose", dyn_session_set_pose(session_, p.entries));
+    currentPose_ = pose;
+  }
+  Matrix4f getCurrentPose() const { return currentPose_; }
+
+  // builder.cu:161-196: render the model at the current pose for a virtual
+  // sensor of width x height (intrinsics scaled by width/cols, height/rows)
+  std::vector<float> GenerateDepth(int width, int height) {
+    std::vector<float> d((size_t)width * height);
+    dyn_sensor v = virtual_sensor(width, height);
+    float4x4 p = currentPose_.to_row_major();
+    dyn_throw("builder::GenerateDepth", dyn_raycast(session_, p.entries, &v, d.data(), nullptr));
+    return d;
+  }
+  std::vector<uint8_t> GenerateRgb(int width, int height) {
+    std::vector<float> d((size_t)width * height);
+    std::vector<uint8_t> c(d.size() * 3);
+    dyn_sensor v = virtual_sensor(width, height);
+    float4x4 p = currentPose_.to_row_major();
+    dyn_throw("builder::GenerateRgb", dyn_raycast(session_, p.entries, &v, d.data(), c.data()));
+    return c;
+  }
+
+  dyn_session* session() const { return session_; }
+
+ private:
+  void ensure(int mode) {
+    if (session_) {
+      if (mode != mode_) dyn_throw("builder: Mode changed after the first frame", DYN_ERR_INVALID_ARG);
+      return;
+    }
+    mode_ = mode;
+    dyn_gn_params g = opt_.to_c(mode);
+    dyn_sensor s = sensor.to_c();
+    dyn_throw("builder::init", dyn_session_create(&tsdf_, &g, &bil_, &s, precision_, device_,
+                                                  &session_));
+  }
+  dyn_sensor virtual_sensor(int width, int height) const {
+    dyn_sensor v = sensor.to_c();
+    float fx = (float)width / (float)sensor.cols, fy = (float)height / (float)sensor.rows;
+    v.rows = (uint32_t)height;
+    v.cols = (uint32_t)width;
+    v.fx = fx * sensor.f.x;
+    v.fy = fy * sensor.f.y;
+    v.cx = fx * sensor.c.x;
+    v.cy = fy * sensor.c.y;
+    return v;
+  }
+
+  dyn_session* session_ = nullptr;
+  dyn_tsdf_params tsdf_{};
+  solver::Properties opt_;
+  dyn_bilateral_params bil_{};
+  int device_ = 0;
+  int precision_ = DYN_PRECISION_FP32;
+  int mode_ = -1;
+  Matrix4f currentPose_;
+};
+
+}  // namespace DynaMap

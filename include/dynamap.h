@@ -208,6 +208,20 @@ dyn_status dyn_integrate_with_pose(dyn_session* s, const uint16_t* depth_host,
                                    const uint8_t* rgb_host /* nullable */,
                                    const float pose[16]);
 
+/* gnSolver::solve (gnSolver.cu:317-438) on caller images: registers the
+ * source depth (metres, rows*cols of the session sensor, optional RGB)
+ * against the target depth (same size, in the target camera's frame) with
+ * the session's pyramid and GN parameters; pose_inout (row-major) is
+ * composed with the increment as dyn_gn_params.compose_left says, and the
+ * final increment xi = [w; t] is returned.  Uses the session's image and
+ * solver buffers only: its map is not touched.  Synchronous. */
+dyn_status dyn_solver_solve(dyn_session* s, const float* target_depth_host,
+                            const uint8_t* target_rgb_host /* nullable */,
+                            const float* source_depth_host,
+                            const uint8_t* source_rgb_host /* nullable */,
+                            float pose_inout[16], double increment_out[6],
+                            dyn_frame_stats* stats /* nullable */);
+
 /* tsdfVolume::GenerateDepth / GenerateRgb (tsdf.cu:527-550; kernels
  * tsdf.cu:471-526) into caller buffers.  'virt' may be NULL for the session
  * sensor; otherwise its rows*cols must not exceed the session sensor's.

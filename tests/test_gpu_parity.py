@@ -204,7 +204,10 @@ def test_icp_normal_equations(gpu_lib, oracle, seq_cfg1):
 
 
 def rot_angle(R):
-    return float(np.arccos(np.clip((np.trace(R) - 1) / 2, -1, 1)))
+    """Angle of a near-identity rotation from its skew part (accurate for
+    small angles, unlike arccos of the trace)."""
+    w = np.array([R[2, 1] - R[1, 2], R[0, 2] - R[2, 0], R[1, 0] - R[0, 1]]) / 2
+    return float(np.arcsin(min(1.0, np.linalg.norm(w))))
 
 
 @pytest.mark.parametrize("bilateral", [1, 0])
