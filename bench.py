@@ -146,19 +146,30 @@ def algorithmic_bytes(stage: str, st_avg: dict, P: int, bsz: int, levels_iters, 
     return None
 
 
-def read_profile_traffic(kernel: str):
-    """dram bytes per launch of 'kernel' recorded from an ncu capture in
-    profiles/ (a line 'traffic_bytes_per_launch: N'), or None."""
+def read_profile_traffic(kernel: str, st_avg: dict):
+    """dram bytes per launch of 'kernel' from an ncu capture summarised in
+    profiles/<kernel>_kernel.md ('traffic_bytes_per_launch: N' measured at
+    'traffic_units: <counter> U'), scaled to this run's units (the traffic
+    grows with the counter: visible blocks for raycast/integrate)."""
     path = os.path.join(ROOT, "profiles", f"{kernel}_kernel.md")
     if not os.path.exists(path):
         return None
+    traffic, unit, units = None, None, None
     for ln in open(path):
-        if ln.strip().startswith("traffic_bytes_per_launch:"):
-            try:
-                return float(ln.split(":", 1)[1].strip().split()[0])
-            except ValueError:
-                return None
-    return None
+        ln = ln.strip()
+        try:
+            if ln.startswith("traffic_bytes_per_launch:"):
+                traffic = float(ln.split(":", 1)[1].split()[0])
+            elif ln.startswith("traffic_units:"):
+                unit, units = ln.split(":", 1)[1].split()[:2]
+                units = float(units)
+        except (ValueError, IndexError):
+            return None
+    if traffic is None:
+        return None
+    if unit and units and unit in st_avg and st_avg[unit] > 0:
+        traffic *= st_avg[unit] / units
+    return traffic
 
 
 def peaks():
@@ -393,7 +404,7 @@ def run_ours(args):
     roof = None
     if alg is not None and stage_ms[dom] > 0:
         ach = alg / (stage_ms[dom] / 1e3) / 1e9
-        traffic = read_profile_traffic(dom)
+        traffic = read_profile_traffic(dom, st_avg)
         roof = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": hbm, "unit": "GB/s",
                 "frac": ach / hbm, "peak_source": f"{peak_kind} hbm_gbs",
                 "algorithmic_bytes_per_launch": alg, "launch_ms": stage_ms[dom],

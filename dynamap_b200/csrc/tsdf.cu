@@ -317,41 +317,59 @@ struct VoxelSample {
 };
 
 struct BlockCache {
-  unsigned long long key;
+  int x, y, z;
   int ptr;
 };
 
-// tsdf.cu:189-225 for one axis: global voxel index by round-half-away of
-// p / voxelSize (IEEE division), block by floor division, local index by
-// non-negative remainder.
+// WorldToGlobalVoxelHashing for one axis (tsdf.cu:189-193): the voxel index
+// g = (int)(fl(p / vs) + sign(p) * 0.5), exactly.  Fast path: t = p * (1/vs)
+// + sign * 0.5 differs from the exactly rounded sum by at most 4 ulps (the
+// reciprocal, the product and the quotient each round once), so whenever t
+// is more than 2^-19 |t| (>= 16 ulps) away from every integer, truncating t
+// gives the same integer; otherwise the IEEE division decides.
+__device__ inline int voxel_index(float p, float vs, float inv_vs) {
+  const float sg = (float)((p > 0.0f) - (p < 0.0f));
+  const float t = __fadd_rn(__fmul_rn(p, inv_vs), sg * 0.5f);
+  const float n = rintf(t);
+  if (fabsf(t - n) > fmaxf(fabsf(t), 1.0f) * 1.9073486328125e-6f) return (int)t;
+  return (int)(p / vs + sg * 0.5f);
+}
+// WorldToBlock / WorldToLocalVoxel (tsdf.cu:195-225) for block size 8: the
+// reference's floor division and non-negative remainder are g >> 3, g & 7.
+__device__ inline int blk_of(int g) { return g >> 3; }
+__device__ inline int loc_of(int g) { return g & 7; }
+
 __device__ inline void axis_voxel(float p, float vs, int* blk, int* loc) {
-  float sg = (float)((p > 0.0f) - (p < 0.0f));
-  int g = (int)(p / vs + sg * 0.5f);
-  *blk = g < 0 ? (g - kBlockSize + 1) / kBlockSize : g / kBlockSize;
-  int r = g % kBlockSize;
-  *loc = r < 0 ? r + kBlockSize : r;
+  int g = voxel_index(p, vs, 1.0f / vs);
+  *blk = blk_of(g);
+  *loc = loc_of(g);
 }
 
 // tsdfVolume::GetVoxel, tsdf.cu:227-239, for a voxel already resolved to
 // (block, local index); a one-block lookup cache skips repeated bucket
 // scans of the same block.
-__device__ inline uint2 fetch_voxel(const VolumeDev& v, int bx, int by, int bz, int lin,
-                                    BlockCache& bc) {
-  unsigned long long key = pack_key(bx, by, bz);
-  if (key != bc.key) {
-    bc.key = key;
+__device__ inline int block_ptr(const VolumeDev& v, int bx, int by, int bz, BlockCache& bc) {
+  if (bx != bc.x || by != bc.y || bz != bc.z) {
+    bc.x = bx;
+    bc.y = by;
+    bc.z = bz;
     bc.ptr = find_block(v.entries, v.t, bx, by, bz);
   }
-  if (bc.ptr < 0) return make_uint2(0u, 0u);
-  return __ldg(reinterpret_cast<const uint2*>(v.voxels + (size_t)bc.ptr * kBlockVox + lin));
+  return bc.ptr;
+}
+__device__ inline uint2 load_voxel(const VolumeDev& v, int ptr, int lin) {
+  if (ptr < 0) return make_uint2(0u, 0u);
+  return __ldg(reinterpret_cast<const uint2*>(v.voxels + (size_t)ptr * kBlockVox + lin));
+}
+__device__ inline int lin_of(int gx, int gy, int gz) {
+  return (loc_of(gx) << 6) | (loc_of(gy) << 3) | loc_of(gz);
 }
 
-__device__ inline uint2 get_voxel(const VolumeDev& v, F3 pos, BlockCache& bc) {
-  int bx, by, bz, lx, ly, lz;
-  axis_voxel(pos.x, v.t.vs, &bx, &lx);
-  axis_voxel(pos.y, v.t.vs, &by, &ly);
-  axis_voxel(pos.z, v.t.vs, &bz, &lz);
-  return fetch_voxel(v, bx, by, bz, (lx * kBlockSize + ly) * kBlockSize + lz, bc);
+__device__ inline uint2 get_voxel(const VolumeDev& v, F3 pos, float inv_vs, BlockCache& bc) {
+  const float vs = v.t.vs;
+  int gx = voxel_index(pos.x, vs, inv_vs), gy = voxel_index(pos.y, vs, inv_vs),
+      gz = voxel_index(pos.z, vs, inv_vs);
+  return load_voxel(v, block_ptr(v, blk_of(gx), blk_of(gy), blk_of(gz), bc), lin_of(gx, gy, gz));
 }
 
 __device__ inline int vw(uint2 r) { return (int)(r.x >> 24); }
@@ -361,12 +379,15 @@ __device__ inline float vsdf(uint2 r) { return __uint_as_float(r.y); }
 // pos_dual + {0, vs} per axis, so each axis has two coordinate values: they
 // are resolved once (six index computations instead of twenty-four) and
 // combined per corner; every corner still gets exactly the reference's
-// float coordinate.  Corners are summed in the reference's order.  COLOR
-// false skips the colour sums (the marching loop only reads sdf/weight).
+// float coordinate.  When the 2x2x2 corners lie in one block (the common
+// case) the block is resolved once.  Corners are summed in the reference's
+// order.  COLOR false skips the colour sums (the marching loop only reads
+// sdf and weight).
 template <bool COLOR>
-__device__ inline VoxelSample get_interpolated(const VolumeDev& v, F3 position, BlockCache& bc) {
+__device__ inline VoxelSample get_interpolated(const VolumeDev& v, F3 position, float inv_vs,
+                                               BlockCache& bc) {
   VoxelSample out;
-  uint2 v0 = get_voxel(v, position, bc);
+  uint2 v0 = get_voxel(v, position, inv_vs, bc);
   out.w = vw(v0);
   if (out.w == 0) {
     out.sdf = vsdf(v0);
@@ -380,13 +401,17 @@ __device__ inline VoxelSample get_interpolated(const VolumeDev& v, F3 position, 
   const float inv = 1.0f / vs;
   F3 vp = position * inv;
   F3 wt = f3(vp.x - floorf(vp.x), vp.y - floorf(vp.y), vp.z - floorf(vp.z));
-  int bxv[2], lxv[2], byv[2], lyv[2], bzv[2], lzv[2];
-  axis_voxel(pos_dual.x + 0.0f, vs, &bxv[0], &lxv[0]);
-  axis_voxel(pos_dual.x + vs, vs, &bxv[1], &lxv[1]);
-  axis_voxel(pos_dual.y + 0.0f, vs, &byv[0], &lyv[0]);
-  axis_voxel(pos_dual.y + vs, vs, &byv[1], &lyv[1]);
-  axis_voxel(pos_dual.z + 0.0f, vs, &bzv[0], &lzv[0]);
-  axis_voxel(pos_dual.z + vs, vs, &bzv[1], &lzv[1]);
+  int gx[2], gy[2], gz[2];
+  gx[0] = voxel_index(pos_dual.x + 0.0f, vs, inv_vs);
+  gx[1] = voxel_index(pos_dual.x + vs, vs, inv_vs);
+  gy[0] = voxel_index(pos_dual.y + 0.0f, vs, inv_vs);
+  gy[1] = voxel_index(pos_dual.y + vs, vs, inv_vs);
+  gz[0] = voxel_index(pos_dual.z + 0.0f, vs, inv_vs);
+  gz[1] = voxel_index(pos_dual.z + vs, vs, inv_vs);
+  const bool one_block = blk_of(gx[0]) == blk_of(gx[1]) && blk_of(gy[0]) == blk_of(gy[1]) &&
+                         blk_of(gz[0]) == blk_of(gz[1]);
+  int ptr0 = 0;
+  if (one_block) ptr0 = block_ptr(v, blk_of(gx[0]), blk_of(gy[0]), blk_of(gz[0]), bc);
   float dist = 0.0f;
   float cr = 0.0f, cg = 0.0f, cb = 0.0f;
   const int off[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1},
@@ -394,8 +419,9 @@ __device__ inline VoxelSample get_interpolated(const VolumeDev& v, F3 position, 
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
     const int ox = off[k][0], oy = off[k][1], oz = off[k][2];
-    uint2 vv = fetch_voxel(v, bxv[ox], byv[oy], bzv[oz],
-                           (lxv[ox] * kBlockSize + lyv[oy]) * kBlockSize + lzv[oz], bc);
+    const int ptr = one_block ? ptr0
+                              : block_ptr(v, blk_of(gx[ox]), blk_of(gy[oy]), blk_of(gz[oz]), bc);
+    uint2 vv = load_voxel(v, ptr, lin_of(gx[ox], gy[oy], gz[oz]));
     uint2 src = (vw(vv) == 0) ? v0 : vv;
     float a = ox ? wt.x : 1.0f - wt.x;
     float b = oy ? wt.y : 1.0f - wt.y;
@@ -421,12 +447,13 @@ __global__ void __launch_bounds__(kRayTX* kRayTY)
     raycast_kernel(VolumeDev v, DSensor s, const PoseState* __restrict__ ps,
                    const float* __restrict__ pose_override, float* __restrict__ depth_out,
                    uint8_t* __restrict__ rgb_out) {
-  __shared__ M4f T;
+  __shared__ M4f Ts;
   __shared__ int over;
   const int tid = threadIdx.y * kRayTX + threadIdx.x;
-  if (tid < 16) T.m[tid] = pose_override ? pose_override[tid] : ps->posef[tid];
+  if (tid < 16) Ts.m[tid] = pose_override ? pose_override[tid] : ps->posef[tid];
   if (tid == 0) over = 0;
   __syncthreads();
+  const M4f T = Ts;  // the pose in registers for the whole march
   // warps cover 8x4 pixel sub-tiles for coherent rays
   const int warp = tid >> 5, lane = tid & 31;
   const int lx = (warp & 1) * 8 + (lane & 7);
@@ -435,8 +462,11 @@ __global__ void __launch_bounds__(kRayTX* kRayTY)
   if (x < s.cols && y < s.rows) {
     const int i = y * s.cols + x;
     const DTsdf& t = v.t;
+    const float inv_vs = 1.0f / t.vs;
+    // getPoint3d (utils.h:104-112) with the pixel's (u - cx), (v - cy) hoisted
+    const float ax = (float)x - s.cx, ay = (float)y - s.cy;
     BlockCache bc;
-    bc.key = kEmptyKey;
+    bc.x = bc.y = bc.z = 0x7fffffff;
     bc.ptr = -1;
     float cur = 0.0f;
     int steps = 0;
@@ -445,8 +475,9 @@ __global__ void __launch_bounds__(kRayTX* kRayTY)
         atomicAdd(&over, 1);
         break;
       }
-      F3 point = xform(T, point3d(i, cur, s));
-      VoxelSample vx = get_interpolated<false>(v, point, bc);
+      F3 pc = f3(ax * cur / s.fx, ay * cur / s.fy, cur);
+      F3 point = xform(T, pc);
+      VoxelSample vx = get_interpolated<false>(v, point, inv_vs, bc);
       if (vx.w == 0) cur += t.trunc;
       else cur += vx.sdf;
       if (vx.w != 0 && vx.sdf < t.vs) break;
@@ -456,7 +487,7 @@ __global__ void __launch_bounds__(kRayTX* kRayTY)
       uint8_t r = 0, g = 0, b = 0;
       if (cur < t.dmax) {
         F3 point = xform(T, point3d(i, cur, s));
-        VoxelSample vx = get_interpolated<true>(v, point, bc);
+        VoxelSample vx = get_interpolated<true>(v, point, inv_vs, bc);
         r = (uint8_t)vx.r;
         g = (uint8_t)vx.g;
         b = (uint8_t)vx.b;
