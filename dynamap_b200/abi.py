@@ -117,6 +117,9 @@ SIGNATURES = {
     "dyn_frame_d2h_bytes": (C.c_size_t, []),
     "dyn_solver_solve": (C.c_int, [_vp, _vp, _vp, _vp, _vp, P(C.c_float), P(C.c_double),
                                    P(FrameStats)]),
+    "dyn_icp_normal_equations_noalloc": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, P(Sensor),
+                                                   P(GnParams), P(C.c_float), P(C.c_double),
+                                                   _vp]),
 }
 
 _lib = None

@@ -459,4 +459,10 @@ void launch_icp_reduce_only(const IcpLevel& L, const IcpParams& P, const float* 
   icp_reduce_kernel<<<g, kIcpThreads, 0, stream>>>(L, P, T_dev, partials, ticket, out_dev);
 }
 
+void launch_icp_reduce_grid(const IcpLevel& L, const IcpParams& P, const float* T_dev,
+                            double* partials, unsigned int* ticket, double* out_dev, int grid,
+                            cudaStream_t stream) {
+  icp_reduce_kernel<<<grid, kIcpThreads, 0, stream>>>(L, P, T_dev, partials, ticket, out_dev);
+}
+
 }  // namespace dyn

@@ -68,5 +68,11 @@ void launch_pose_set(PoseState* ps, const double* pose_dev, cudaStream_t stream)
 void launch_icp_reduce_only(const IcpLevel& L, const IcpParams& P, const float* T_dev,
                             double* partials, unsigned int* ticket, double* out_dev,
                             cudaStream_t stream);
+// The same reduction on an explicit grid ('partials' holds grid * 29
+// doubles; pixels beyond grid * kIcpThreads are covered by the grid-stride
+// loop).
+void launch_icp_reduce_grid(const IcpLevel& L, const IcpParams& P, const float* T_dev,
+                            double* partials, unsigned int* ticket, double* out_dev, int grid,
+                            cudaStream_t stream);
 
 }  // namespace dyn

@@ -321,6 +321,26 @@ dyn_status dyn_icp_normal_equations(
     const dyn_sensor* level, const dyn_gn_params* gn, const float T[16],
     double out_host[29], void* stream);
 
+/* The same normal equations for callers that cannot allocate device memory
+ * (a host that reserves a fixed GPU-memory budget up front and forbids later
+ * cudaMalloc, e.g. a real-time executor running the tracker in its control
+ * loop).  No counterpart in the reference: this entry point exists for such
+ * callers.  Its scratch is one fixed file-scope device array (~465 KiB per
+ * GPU that loads the library, held until exit) instead of allocated
+ * buffers; it calls no cudaMalloc/cudaFree.  Levels up to 2,097,152 pixels
+ * (1920x1080 fits); larger ones return DYN_ERR_INVALID_ARG.  All calls on a
+ * device share the array: calls whose GPU work overlaps race and must be
+ * serialised by the caller.  The first call on a device does a one-time
+ * set-up (looks up the array's address with that device current); make it
+ * before any stream capture.  Results equal dyn_icp_normal_equations' to
+ * rounding (the partial sums are grouped differently).  Synchronous. */
+dyn_status dyn_icp_normal_equations_noalloc(
+    const float* src_depth_dev, const float* src_normal4_dev,
+    const float* src_intensity_dev, const float* tgt_depth_dev,
+    const float* tgt_normal4_dev, const float* tgt_intensity_dev,
+    const dyn_sensor* level, const dyn_gn_params* gn, const float T[16],
+    double out_host[29], void* stream);
+
 /* ---- batched multi-session stepping ------------------------------------
  * Process one frame for each of n sessions with as few launches as the
  * sessions' shapes allow.  Frames are given as host pointers (copied
