@@ -38,7 +38,7 @@ METRIC = "agg frames/s + p50/p99 frame latency vs plain FP32 path; ATE/SDF err v
 def _render_chunk(args):
     from dynamap_b200 import configs, scene
     name, seed, n_frames, idx = args
-    p = configs.preset(name)
+    p = configs.preset(name) if isinstance(name, str) else name
     s, q = p["sensor"], p["seq"]
     sc = scene.make_scene(seed, q["kind"])
     poses = scene.trajectory(sc, n_frames, seed, q["trans"], q["rot"])
@@ -53,21 +53,32 @@ def _render_chunk(args):
     return idx, out_d, out_c, poses
 
 
-def make_frames(name: str, seed: int, n_frames: int, workers: int):
+def make_frames(name, seed: int, n_frames: int, workers: int):
     """Render the sequence with a spawn process pool (started before CUDA)."""
+    return make_many([(name, seed)], n_frames, workers)[0]
+
+
+def make_many(jobs, n_frames: int, workers: int):
+    """Render several sequences [(preset name or dict, seed)] in one spawn
+    process pool; returns [(depth, rgb, poses)]."""
     import concurrent.futures as cf
     import multiprocessing as mp
     import numpy as np
     chunks = [list(range(i, min(i + 8, n_frames))) for i in range(0, n_frames, 8)]
-    depth, rgb, poses = [None] * n_frames, [None] * n_frames, None
+    work = [(j, (name, seed, n_frames, c)) for j, (name, seed) in enumerate(jobs) for c in chunks]
+    depth = [[None] * n_frames for _ in jobs]
+    rgb = [[None] * n_frames for _ in jobs]
+    poses = [None] * len(jobs)
     with cf.ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
-        for idx, ds, cs, ps in ex.map(_render_chunk, [(name, seed, n_frames, c) for c in chunks]):
-            poses = ps
+        for (j, _), (idx, ds, cs, ps) in zip(work, ex.map(_render_chunk, [w for _, w in work])):
+            poses[j] = ps
             for i, d, c in zip(idx, ds, cs):
-                depth[i], rgb[i] = d, c
-    depth = np.stack(depth)
-    rgb = np.stack(rgb) if rgb[0] is not None else None
-    return depth, rgb, poses
+                depth[j][i], rgb[j][i] = d, c
+    out = []
+    for j in range(len(jobs)):
+        out.append((np.stack(depth[j]), np.stack(rgb[j]) if rgb[j][0] is not None else None,
+                    poses[j]))
+    return out
 
 
 class ClockSampler:
@@ -250,8 +261,10 @@ def config_block(args, p):
                         f"{' + RGB' if p['seq']['rgb'] else ''}, {t['voxel_size']*1e3:g} mm voxels, "
                         f"2^{int(math.log2(t['num_buckets']))} buckets x {t['bucket_size']}, "
                         f"ICP iters {p['gn']['lvl_iteration_num']} at scales {p['gn']['lvl_scale']}, "
-                        f"photometric weight {p['gn']['color_weight']}, FP32 TSDF, frame-to-model",
-            "sessions_per_gpu": 1, "precision": "fp32", "seed": args.seed,
+                        f"photometric weight {p['gn']['color_weight']}, "
+                        f"{'FP32' if args.precision == 'fp32' else 'f16/u16 mixed-precision'} TSDF, "
+                        "frame-to-model",
+            "sessions_per_gpu": 1, "precision": args.precision, "seed": args.seed,
             "l2": "inputs larger than L2: the TSDF working set (voxel pool "
                   f"{t['num_blocks'] * 4096 / 2**30:.1f} GiB, hash "
                   f"{t['num_buckets'] * t['bucket_size'] * 16 / 2**20:.0f} MiB) exceeds the 126 MB L2"}
@@ -282,6 +295,7 @@ def run_ours(args):
         p["tsdf"]["num_blocks"] = min(p["tsdf"]["num_blocks"], args.max_blocks)
     t, g, b, s = configs.structs(p)
     lib = abi.load()
+    prec = abi.PRECISION_MIXED if args.precision == "mixed" else abi.PRECISION_FP32
     P = s.rows * s.cols
     has_rgb = rgb is not None
     d_dev = torch.from_numpy(depth).cuda()
@@ -311,7 +325,7 @@ def run_ours(args):
         return torch.cuda.ExternalStream(ptr.value, device=torch.device("cuda", local))
 
     # ---- pass A: device throughput --------------------------------------
-    with Session(t, g, b, s, device=local) as m:
+    with Session(t, g, b, s, precision=prec, device=local) as m:
         m.set_pose(poses[0])
         stream = session_stream(m)
         for i in range(args.warmup):
@@ -339,7 +353,7 @@ def run_ours(args):
 
     # ---- pass B: per-frame latency and stage times ------------------------
     lat_dev, lat_host, stats = [], [], []
-    with Session(t, g, b, s, device=local) as m:
+    with Session(t, g, b, s, precision=prec, device=local) as m:
         m.set_pose(poses[0])
         abi.check("profile", lib.dyn_session_profile(m.h, 1))
         for i in range(args.warmup):
@@ -366,7 +380,7 @@ def run_ours(args):
     pin_c = torch.from_numpy(rgb).pin_memory() if has_rgb else None
     d_np = pin_d.numpy()
     c_np = pin_c.numpy() if has_rgb else None
-    with Session(t, g, b, s, device=local) as m:
+    with Session(t, g, b, s, precision=prec, device=local) as m:
         m.set_pose(poses[0])
         stream = session_stream(m)
         for i in range(args.warmup):
@@ -440,6 +454,191 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_batched(args):
+    """The batched configuration: args.sessions independent sessions of mixed
+    resolution, one frame of every session per step.  value = aggregate
+    frames/s of the batched submission; 'plain' = the same sessions driven
+    one frame at a time, each waited for before the next (the reference's
+    per-frame loop) on the same GPU."""
+    import ctypes as C
+
+    import numpy as np
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    nframes = args.warmup + args.steps
+    from dynamap_b200 import configs
+    mix = configs.session_mix(args.sessions, nframes, base_seed=100 + 1000 * rank)
+    workers = max(1, min(32, ((os.cpu_count() or 2) - 1) // max(world, 1)))
+    frames = make_many([(p, seed) for _, p, seed in mix], nframes, workers)
+
+    import torch
+    from dynamap_b200 import abi
+    from dynamap_b200.session import Session
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    lib = abi.load()
+    prec = abi.PRECISION_MIXED if args.precision == "mixed" else abi.PRECISION_FP32
+    structs = [configs.structs(p) for _, p, _ in mix]
+    dev_frames = [torch.from_numpy(d).cuda() for d, _, _ in frames]
+    nbytes = [d.shape[1] * d.shape[2] * 2 for d, _, _ in frames]
+    pinned = [torch.from_numpy(d).pin_memory().numpy() for d, _, _ in frames]
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        v = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(v, op=dist.ReduceOp.MAX)
+        return float(v.item())
+
+    def timed(fn):
+        barrier()
+        ts = torch.cuda.Stream()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(ts)
+        fn()
+        torch.cuda.synchronize()
+        e1.record(ts)
+        torch.cuda.synchronize()
+        return max_over_ranks(e0.elapsed_time(e1) / 1e3)
+
+    def open_sessions(precision):
+        ss = [Session(*st, precision=precision, device=local) for st in structs]
+        for m, (_, _, poses) in zip(ss, frames):
+            m.set_pose(poses[0])
+        return ss
+
+    n = len(mix)
+    from dynamap_b200.session import Batch
+    # fused batch, frames resident on the device: one launch per stage for
+    # all sessions, one graph per frame
+    ss = open_sessions(prec)
+    bt = Batch(ss)
+    for k in range(args.warmup):
+        bt.submit_device([dev_frames[j].data_ptr() + k * nbytes[j] for j in range(n)])
+        bt.result(strict=False)
+
+    def fused_device():
+        for k in range(args.warmup, nframes):
+            bt.submit_device([dev_frames[j].data_ptr() + k * nbytes[j] for j in range(n)])
+            bt.result(strict=False)
+    clk = ClockSampler(local)
+    clk.start()
+    t_dev = timed(fused_device)
+    clocks = clk.stop()
+    launches = bt.kernels_per_frame() * args.steps
+    # stage split of the fused frame (profiled pass, not timed above)
+    bt.profile(True)
+    for k in range(args.warmup, min(nframes, args.warmup + 20)):
+        bt.submit_device([dev_frames[j].data_ptr() + k * nbytes[j] for j in range(n)])
+        bt.result(strict=False)
+    ms, nprof = bt.stage_times()
+    stage_ms = {abi.STAGES[i]: ms[i] / max(nprof, 1) for i in range(len(abi.STAGES))}
+    bt.close()
+    for m in ss:
+        m.close()
+    # fused batch, end to end from pinned host memory
+    ss = open_sessions(prec)
+    bt = Batch(ss)
+    for k in range(args.warmup):
+        bt.submit([pinned[j][k] for j in range(n)])
+        bt.result(strict=False)
+
+    def fused_e2e():
+        for k in range(args.warmup, nframes):
+            bt.submit([pinned[j][k] for j in range(n)])
+            bt.result(strict=False)
+    t_e2e = timed(fused_e2e)
+    bt.close()
+    for m in ss:
+        m.close()
+    # per-session graphs on concurrent streams (dyn_sessions_submit)
+    ss = open_sessions(prec)
+    handles = (C.c_void_p * n)(*[m.h.value for m in ss])
+    for k in range(args.warmup):
+        ptrs = (C.c_void_p * n)(*[pinned[j][k].ctypes.data for j in range(n)])
+        abi.check("sessions_submit", lib.dyn_sessions_submit(handles, n, ptrs, None))
+        for m in ss:
+            m.result(strict=False)
+
+    def streams_e2e():
+        for k in range(args.warmup, nframes):
+            ptrs = (C.c_void_p * n)(*[pinned[j][k].ctypes.data for j in range(n)])
+            abi.check("sessions_submit", lib.dyn_sessions_submit(handles, n, ptrs, None))
+            for m in ss:
+                m.result(strict=False)
+    t_streams = timed(streams_e2e)
+    for m in ss:
+        m.close()
+    # plain per-frame path: FP32, one frame at a time, waited for
+    ss = open_sessions(abi.PRECISION_FP32)
+    lat = []
+    for k in range(args.warmup):
+        for j, m in enumerate(ss):
+            m.submit_device(dev_frames[j].data_ptr() + k * nbytes[j])
+            m.result(strict=False)
+
+    def plain():
+        for k in range(args.warmup, nframes):
+            for j, m in enumerate(ss):
+                h0 = time.perf_counter()
+                m.submit_device(dev_frames[j].data_ptr() + k * nbytes[j])
+                m.result(strict=False)
+                lat.append(time.perf_counter() - h0)
+    t_plain = timed(plain)
+    for m in ss:
+        m.close()
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    K = args.steps
+    total = world * n * K
+    lat.sort()
+    kinds = {}
+    for k_, _, _ in mix:
+        kinds[k_] = kinds.get(k_, 0) + 1
+    line = {
+        "metric": METRIC, "value": total / t_dev, "unit": "frames/s", "n_gpus": world,
+        "steps": K, "warmup": args.warmup, "ms_per_step": 1e3 * t_dev / K,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: seeded analytic scenes, one per session",
+        "config": {"workload": f"cfg3: {n} sessions per GPU, resolutions "
+                               f"160x120/320x240/640x480 1:2:1 ({kinds}), voxels 10/8/5 mm, "
+                               "2^18-2^20 buckets, one frame of every session per step, "
+                               f"{args.precision}, one fused launch per stage for all "
+                               "sessions (dyn_batch), one CUDA graph per frame; plain = "
+                               "FP32 sessions one frame at a time",
+                   "sessions_per_gpu": n, "precision": args.precision,
+                   "l2": "per-step inputs and volumes exceed L2"},
+        "plain_fps": total / t_plain,
+        "speedup_vs_plain": t_plain / t_dev,
+        "plain_latency_ms": {"p50": 1e3 * lat[len(lat) // 2],
+                             "p99": 1e3 * lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
+        "step_ms": {"frame_of_all_sessions": 1e3 * t_dev / K},
+        "stage_ms_per_step": stage_ms,
+        "streams_e2e_fps": total / t_streams,
+        "gpu_launches": launches,
+        "clocks": clocks,
+        "e2e": {"value": total / t_e2e, "unit": "frames/s",
+                "h2d_bytes_per_step": int(sum(nbytes)),
+                "d2h_bytes_per_step": int(n * lib.dyn_frame_d2h_bytes())},
+    }
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -453,10 +652,16 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--max-blocks", type=int, default=0,
                     help="cap the voxel-block pool (small profiling runs)")
+    ap.add_argument("--sessions", type=int, default=32, help="sessions per GPU (cfg3)")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "mixed"],
+                    help="fp32: the drop-in path; mixed: f16/u16 voxels, compensated "
+                         "normal equations, fast raycast")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         run_reference(args)
+    elif args.config == "cfg3":
+        run_batched(args)
     else:
         run_ours(args)
 

@@ -120,6 +120,16 @@ SIGNATURES = {
     "dyn_icp_normal_equations_noalloc": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, P(Sensor),
                                                    P(GnParams), P(C.c_float), P(C.c_double),
                                                    _vp]),
+    "dyn_batch_create": (C.c_int, [P(_vp), C.c_int32, P(_vp)]),
+    "dyn_batch_destroy": (C.c_int, [_vp]),
+    "dyn_batch_submit": (C.c_int, [_vp, P(_vp), P(_vp)]),
+    "dyn_batch_submit_device": (C.c_int, [_vp, P(_vp), P(_vp)]),
+    "dyn_batch_result": (C.c_int, [_vp, P(C.c_float), P(FrameStats), P(C.c_int)]),
+    "dyn_batch_size": (C.c_int, [_vp, P(C.c_int32)]),
+    "dyn_batch_stream": (C.c_int, [_vp, P(_vp)]),
+    "dyn_batch_profile": (C.c_int, [_vp, C.c_int32]),
+    "dyn_batch_stage_times": (C.c_int, [_vp, P(C.c_double), P(C.c_int64), C.c_int32]),
+    "dyn_batch_kernels_per_frame": (C.c_int, [_vp, P(C.c_int32)]),
 }
 
 _lib = None

@@ -20,7 +20,7 @@ LIB = os.path.join(HERE, "libdynamap_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 SOURCES = ["image.cu", "icp.cu", "tsdf.cu", "session.cu", "noalloc.cu", "config.cpp"]
-HEADERS = ["common.cuh", "image.cuh", "icp.cuh", "tsdf.cuh", "dyn_exp.h"]
+HEADERS = ["common.cuh", "image.cuh", "icp.cuh", "tsdf.cuh", "sessdev.cuh", "dyn_exp.h"]
 
 # -fmad=false: no FMA contraction, IEEE div/sqrt: every float operation
 # rounds once, in source order (the bit-exact parity with the oracle relies
@@ -53,8 +53,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
         if force or _stale(obj, [sp] + hdrs):
             cmd = [NVCC] + NVCC_FLAGS + ["-c", sp, "-o", obj]
             if src.endswith(".cpp"):
-                cmd = [NVCC, "-x", "c++", "-O2", "-std=c++17", "-Xcompiler",
-                       "-fPIC,-ffp-contract=off", "-ccbin", "g++", "-c", sp, "-o", obj]
+                cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off",
+                       "-c", sp, "-o", obj]
             if verbose:
                 print(" ".join(cmd), flush=True)
             subprocess.run(cmd, check=True)

@@ -51,6 +51,37 @@ PRESETS = {
 }
 
 
+def session_mix(n_sessions: int = 32, n_frames: int = 200, base_seed: int = 100):
+    """The batched configuration: n independent sessions, resolutions
+    160x120 / 320x240 / 640x480 in the ratio 1:2:1, voxel sizes 5-10 mm,
+    2^18-2^20 buckets, each with its own seeded scene and trajectory.
+    Returns a list of (name, preset dict, seed)."""
+    out = []
+    kinds = ["s160", "s320", "s320", "s640"]
+    for i in range(n_sessions):
+        k = kinds[i % 4]
+        if k == "s160":
+            sensor = dict(rows=120, cols=160, fx=131.25, fy=131.25, cx=79.5, cy=59.5,
+                          depth_scaler=1000.0)
+            tsdf = dict(voxel_size=0.01, num_buckets=1 << 18, num_blocks=1 << 14)
+        elif k == "s320":
+            sensor = dict(rows=240, cols=320, fx=262.5, fy=262.5, cx=159.5, cy=119.5,
+                          depth_scaler=1000.0)
+            tsdf = dict(voxel_size=0.008, num_buckets=1 << 19, num_blocks=1 << 16)
+        else:
+            sensor = dict(rows=480, cols=640, fx=525.0, fy=525.0, cx=319.5, cy=239.5,
+                          depth_scaler=1000.0)
+            tsdf = dict(voxel_size=0.005, num_buckets=1 << 20, num_blocks=1 << 18)
+        tsdf.update(bucket_size=10, block_size=8, max_sdf_weight=64,
+                    truncation_distance=4 * tsdf["voxel_size"], max_sensor_depth=3.0,
+                    min_sensor_depth=0.15)
+        p = dict(sensor=sensor, tsdf=tsdf, gn=_gn([10, 5, 4]),
+                 bilateral=dict(diameter=8, sigma_i=10.0, sigma_s=1.0, enabled=1),
+                 seq=dict(n_frames=n_frames, trans=0.005, rot=0.5, rgb=False, kind="cube"))
+        out.append((k, p, base_seed + i))
+    return out
+
+
 def preset(name: str, **over):
     p = {k: (dict(v) if isinstance(v, dict) else v) for k, v in PRESETS[name].items()}
     for k, v in over.items():

@@ -14,6 +14,8 @@
 // round trip.
 #include "icp.cuh"
 
+#include "sessdev.cuh"
+
 namespace dyn {
 
 namespace {
@@ -302,10 +304,20 @@ __device__ bool gn_update(const double* acc, const IcpParams& P, int it, IcpStat
   return conv;
 }
 
+inline __host__ __device__ int icp_grid(int n) {
+  int g = (n + kIcpThreads - 1) / kIcpThreads;
+  if (g > kIcpMaxBlocks) g = kIcpMaxBlocks;
+  if (g < 1) g = 1;
+  return g;
+}
+
+// One GN iteration of level slot pl, iteration it (1-based), block 'bid' of
+// 'nb' blocks: the block's partial sums, then -- in the last block to finish
+// -- the FP64 total and the GN update (gnSolver.cu:379-415).
 template <bool KAHAN>
-__global__ void __launch_bounds__(kIcpThreads)
-    icp_iteration_kernel(IcpLevel L, IcpParams P, int pl, int it, IcpState* st,
-                         double* __restrict__ partials) {
+__device__ inline void icp_iteration_body(const IcpLevel& L, const IcpParams& P, int pl, int it,
+                                          IcpState* st, double* __restrict__ partials, int bid,
+                                          int nb) {
   __shared__ double red[(kIcpThreads / 32) * kIcpVals];
   __shared__ M4f Ts;
   __shared__ int skip;
@@ -321,19 +333,18 @@ __global__ void __launch_bounds__(kIcpThreads)
 #pragma unroll
   for (int k = 0; k < kIcpVals; ++k) a.v[k] = a.c[k] = 0.0f;
   const int n = L.s.rows * L.s.cols;
-  for (int idx = blockIdx.x * kIcpThreads + threadIdx.x; idx < n;
-       idx += gridDim.x * kIcpThreads)
+  for (int idx = bid * kIcpThreads + threadIdx.x; idx < n; idx += nb * kIcpThreads)
     pixel_terms<KAHAN>(L, P, T, idx, a);
   block_reduce(a, KAHAN, red);
-  if (threadIdx.x < kIcpVals) partials[(size_t)blockIdx.x * kIcpVals + threadIdx.x] = red[threadIdx.x];
+  if (threadIdx.x < kIcpVals) partials[(size_t)bid * kIcpVals + threadIdx.x] = red[threadIdx.x];
   __threadfence();
   __shared__ unsigned int ticket;
   if (threadIdx.x == 0) ticket = atomicAdd(&st->ticket, 1u);
   __syncthreads();
-  if (ticket != gridDim.x - 1) return;
+  if (ticket != (unsigned)nb - 1) return;
   __threadfence();
   __shared__ double tot[kIcpVals];
-  final_reduce(partials, gridDim.x, tot);
+  final_reduce(partials, nb, tot);
   if (threadIdx.x == 0) {
     st->ticket = 0;
     st->iters[pl] = it;
@@ -345,6 +356,36 @@ __global__ void __launch_bounds__(kIcpThreads)
     se3_exp(st->inc, Td);
     for (int k = 0; k < 16; ++k) st->T[k] = (float)Td[k];
   }
+}
+
+template <bool KAHAN>
+__global__ void __launch_bounds__(kIcpThreads)
+    icp_iteration_kernel(IcpLevel L, IcpParams P, int pl, int it, IcpState* st,
+                         double* __restrict__ partials) {
+  icp_iteration_body<KAHAN>(L, P, pl, it, st, partials, blockIdx.x, gridDim.x);
+}
+
+// Every session of the frame in one launch (blockIdx.z); a session uses
+// only the blocks of its own grid, so its reduction is the same as alone.
+// One instantiation per summation kind; sessions of the other kind return.
+template <bool KAHAN>
+__global__ void __launch_bounds__(kIcpThreads)
+    fused_icp_iteration_kernel(const SessDev* __restrict__ tab, int pl, int it) {
+  const SessDev& S = tab[blockIdx.z];
+  if ((S.icpp.kahan != 0) != KAHAN) return;
+  if (it >= S.slot_iters[pl]) return;  // the reference runs iterations 1 .. N-1
+  const int l = S.slot_level[pl];
+  IcpLevel L;
+  L.sd = S.sdep[l];
+  L.sn = S.snrm[l];
+  L.si = S.sint[l];
+  L.td = S.tdep[l];
+  L.tn = S.tnrm[l];
+  L.ti = S.tint[l];
+  L.s = S.ls[l];
+  const int nb = icp_grid(L.s.rows * L.s.cols);
+  if ((int)blockIdx.x >= nb) return;
+  icp_iteration_body<KAHAN>(L, S.icpp, pl, it, S.icp, S.partials, blockIdx.x, nb);
 }
 
 // Normal equations only (stage entry point): no solver state.
@@ -385,9 +426,8 @@ __device__ void finish_pose(PoseState* ps) {
   inverse4f(ps->posef, ps->invf);
 }
 
-// gnSolver.cu:426-430 + builder pose bookkeeping.
-__global__ void pose_finalize_kernel(IcpParams P, IcpState* st, PoseState* ps) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// gnSolver.cu:426-430 + builder pose bookkeeping (one thread).
+__device__ void pose_finalize_body(const IcpParams& P, IcpState* st, PoseState* ps) {
   ps->reset = 0;
   if (st->have_target) {
     double s = 0.0;
@@ -418,17 +458,24 @@ __global__ void pose_finalize_kernel(IcpParams P, IcpState* st, PoseState* ps) {
   finish_pose(ps);
 }
 
+__global__ void pose_finalize_kernel(IcpParams P, IcpState* st, PoseState* ps) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  pose_finalize_body(P, st, ps);
+}
+
+// one thread per session; bump != 0 also advances the frame counter
+__global__ void fused_pose_finalize_kernel(const SessDev* __restrict__ tab, int n, int bump) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const SessDev& S = tab[s];
+  pose_finalize_body(S.icpp, S.icp, S.pose);
+  if (bump) S.pose->frame += 1;
+}
+
 __global__ void pose_set_kernel(PoseState* ps, const double* pose) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   for (int k = 0; k < 16; ++k) ps->pose[k] = pose[k];
   finish_pose(ps);
-}
-
-inline int icp_grid(int n) {
-  int g = (n + kIcpThreads - 1) / kIcpThreads;
-  if (g > kIcpMaxBlocks) g = kIcpMaxBlocks;
-  if (g < 1) g = 1;
-  return g;
 }
 
 }  // namespace
@@ -463,6 +510,18 @@ void launch_icp_reduce_grid(const IcpLevel& L, const IcpParams& P, const float* 
                             double* partials, unsigned int* ticket, double* out_dev, int grid,
                             cudaStream_t stream) {
   icp_reduce_kernel<<<grid, kIcpThreads, 0, stream>>>(L, P, T_dev, partials, ticket, out_dev);
+}
+
+void fused_icp_iteration(const SessDev* tab, const BatchShape& b, int slot, int it,
+                         cudaStream_t st) {
+  if (it >= b.max_slot_iters[slot]) return;
+  const dim3 grid(icp_grid(b.max_slot_px[slot]), 1, b.n);
+  if (b.kahan_mask & 1) fused_icp_iteration_kernel<false><<<grid, kIcpThreads, 0, st>>>(tab, slot, it);
+  if (b.kahan_mask & 2) fused_icp_iteration_kernel<true><<<grid, kIcpThreads, 0, st>>>(tab, slot, it);
+}
+
+void fused_pose_finalize(const SessDev* tab, const BatchShape& b, int bump, cudaStream_t st) {
+  fused_pose_finalize_kernel<<<(b.n + 31) / 32, 32, 0, st>>>(tab, b.n, bump);
 }
 
 }  // namespace dyn

@@ -3,12 +3,17 @@
 // Reference: include/image/pyramid/pyramid.cu (bilateral :208-252, pyramid
 // :49-143), include/image/sensor/rgbdImage.cu (vertex map :23-38, normals
 // :126-157), include/solver/gnSolver/gnSolver.cu:457-465 (intensity).
+//
+// Each stage's arithmetic is one __device__ function, used by a by-value
+// kernel (stage entry points) and by a fused kernel that runs the stage for
+// every session of a frame in one launch (blockIdx.z = session).
 #include "image.cuh"
 
 #include <cmath>
 #include <cstring>
 
 #include "dyn_exp.h"
+#include "sessdev.cuh"
 
 namespace dyn {
 
@@ -22,13 +27,19 @@ __device__ inline float intensity_u8(const uint8_t* c) {
 }
 
 // u16 sensor units -> metres (builder.cu:111, utils_Dataset.cpp:233-235)
+__device__ inline void ingest_px(const uint16_t* __restrict__ raw, const uint8_t* __restrict__ rgb,
+                                 float scaler, float* __restrict__ depth,
+                                 float* __restrict__ inten, int i) {
+  depth[i] = (float)raw[i] / scaler;
+  if (inten) inten[i] = rgb ? intensity_u8(rgb + 3 * (size_t)i) : 0.0f;
+}
+
 __global__ void ingest_kernel(const uint16_t* __restrict__ raw,
                               const uint8_t* __restrict__ rgb, int n, float scaler,
                               float* __restrict__ depth, float* __restrict__ inten) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  depth[i] = (float)raw[i] / scaler;
-  if (inten) inten[i] = rgb ? intensity_u8(rgb + 3 * (size_t)i) : 0.0f;
+  ingest_px(raw, rgb, scaler, depth, inten, i);
 }
 
 constexpr int BTX = 32, BTY = 8;
@@ -37,32 +48,32 @@ constexpr int BTX = 32, BTY = 8;
 // window rows x-r..x+r-1, cols y-r..y+r-1, summed row-major.  The depth tile
 // plus halo is staged in shared memory; the spatial weights, a pure function
 // of the tap offset, come precomputed on the host in double and rounded to
-// float exactly as the reference rounds them per tap (kernel parameter,
-// read as warp-uniform constants).  The range weight uses dyn_expf, the
-// same operation sequence the oracle runs, so the filtered depth is
-// bit-identical to the oracle's.  Taps outside the image or with depth <= 0
-// are skipped and invalid centres stay 0.
-__global__ void bilateral_kernel(const float* __restrict__ src, float* __restrict__ dst,
-                                 int rows, int cols, const __grid_constant__ BilateralTable tb) {
-  extern __shared__ float tile[];
+// float exactly as the reference rounds them per tap (read as warp-uniform
+// values).  The range weight uses dyn_expf, the same operation sequence the
+// oracle runs, so the filtered depth is bit-identical to the oracle's.  Taps
+// outside the image or with depth <= 0 are skipped; invalid centres stay 0.
+__device__ inline void bilateral_tile(const float* __restrict__ src, float* __restrict__ dst,
+                                      int rows, int cols, const BilateralTable& tb, int bx,
+                                      int by, float* tile) {
   const int D = 2 * tb.radius, half = tb.radius;
   const int TW = BTX + D - 1, TH = BTY + D - 1;
   const int tid = threadIdx.y * BTX + threadIdx.x;
-  const int row0 = blockIdx.y * BTY - half, col0 = blockIdx.x * BTX - half;
+  const int row0 = by * BTY - half, col0 = bx * BTX - half;
   for (int k = tid; k < TW * TH; k += BTX * BTY) {
     int tr = k / TW, tc = k - (k / TW) * TW;
     int gr = row0 + tr, gc = col0 + tc;
     tile[k] = (gr >= 0 && gr < rows && gc >= 0 && gc < cols) ? src[gr * cols + gc] : 0.0f;
   }
   __syncthreads();
-  const int x = blockIdx.y * BTY + threadIdx.y;  // row (the reference's x)
-  const int y = blockIdx.x * BTX + threadIdx.x;  // column
+  const int x = by * BTY + threadIdx.y;  // row (the reference's x)
+  const int y = bx * BTX + threadIdx.x;  // column
   if (x >= rows || y >= cols) return;
   const float c = tile[(threadIdx.y + half) * TW + threadIdx.x + half];
   if (!(c > 0.0f)) {
     dst[x * cols + y] = 0.0f;
     return;
   }
+  const float inv2s2 = tb.inv2s2, norm = tb.norm;
   float acc = 0.0f, wp = 0.0f;
   for (int i = 0; i < D; ++i) {
     int nx = x - (half - i);
@@ -73,7 +84,7 @@ __global__ void bilateral_kernel(const float* __restrict__ src, float* __restric
       if (ny < 0 || ny >= cols) continue;
       float nv = trow[j];
       if (!(nv > 0.0f)) continue;
-      float gi = range_weight(nv - c, tb.inv2s2, tb.norm);
+      float gi = range_weight(nv - c, inv2s2, norm);
       float w = gi * tb.gs[i * D + j];
       acc += nv * w;
       wp += w;
@@ -82,13 +93,16 @@ __global__ void bilateral_kernel(const float* __restrict__ src, float* __restric
   dst[x * cols + y] = acc / wp;
 }
 
+__global__ void bilateral_kernel(const float* __restrict__ src, float* __restrict__ dst,
+                                 int rows, int cols, const __grid_constant__ BilateralTable tb) {
+  extern __shared__ float tile[];
+  bilateral_tile(src, dst, rows, cols, tb, blockIdx.x, blockIdx.y, tile);
+}
+
 // One 2x pyramid step: mean of the valid depths of each 2x2 cell (fix of
 // pyramid.cu:49-82, which scatters into a fixed 640x480 window).
-__global__ void downsample_depth_kernel(const float* __restrict__ src, int rows, int cols,
-                                        float* __restrict__ dst) {
-  int c2 = cols / 2, r2 = rows / 2;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= r2 * c2) return;
+__device__ inline void downsample_depth_px(const float* __restrict__ src, int cols, int c2,
+                                           float* __restrict__ dst, int i) {
   int y = i / c2, x = i - (i / c2) * c2;
   const float* a = src + (2 * y) * cols + 2 * x;
   float v[4] = {a[0], a[1], a[cols], a[cols + 1]};
@@ -102,45 +116,49 @@ __global__ void downsample_depth_kernel(const float* __restrict__ src, int rows,
     }
   dst[i] = n ? s / (float)n : 0.0f;
 }
+__device__ inline void downsample_intensity_px(const float* __restrict__ src, int cols, int c2,
+                                               float* __restrict__ dst, int i) {
+  int y = i / c2, x = i - (i / c2) * c2;
+  const float* a = src + (2 * y) * cols + 2 * x;
+  dst[i] = (((a[0] + a[1]) + a[cols]) + a[cols + 1]) * 0.25f;
+}
+
+__global__ void downsample_depth_kernel(const float* __restrict__ src, int rows, int cols,
+                                        float* __restrict__ dst) {
+  int c2 = cols / 2, r2 = rows / 2;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= r2 * c2) return;
+  downsample_depth_px(src, cols, c2, dst, i);
+}
 
 __global__ void downsample_intensity_kernel(const float* __restrict__ src, int rows, int cols,
                                             float* __restrict__ dst) {
   int c2 = cols / 2, r2 = rows / 2;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= r2 * c2) return;
-  int y = i / c2, x = i - (i / c2) * c2;
-  const float* a = src + (2 * y) * cols + 2 * x;
-  dst[i] = (((a[0] + a[1]) + a[cols]) + a[cols + 1]) * 0.25f;
+  downsample_intensity_px(src, cols, c2, dst, i);
 }
 
 // creatPointCloudKernel (rgbdImage.cu:23-38) and vertextoNormal
-// (rgbdImage.cu:126-145): n = normalize(cross(V(u+2)-V(u-2), V(v+1)-V(v-1))),
-// all pyramid levels in one launch.  Vertices are recomputed from depth, so
-// neighbours need no vertex map.  A normal is 0 when the centre or a
-// neighbour is invalid or outside the row/image.
-__global__ void maps_kernel(MapsArgs a) {
-  int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= a.total) return;
-  int l = 0;
-#pragma unroll
-  for (int k = 1; k < kLevels; ++k)
-    if (k < a.nlev && g >= a.lv[k].offset) l = k;
-  const LevelMaps& L = a.lv[l];
-  int i = g - L.offset;
-  const DSensor s = L.s;
+// (rgbdImage.cu:126-145): n = normalize(cross(V(u+2)-V(u-2), V(v+1)-V(v-1))).
+// Vertices are recomputed from depth, so neighbours need no vertex map.  A
+// normal is 0 when the centre or a neighbour is invalid or outside the
+// row/image.
+__device__ inline void maps_px(const float* __restrict__ depth, float4* __restrict__ normal,
+                               float4* __restrict__ vertex, const DSensor& s, int i) {
   int y = i / s.cols, x = i - (i / s.cols) * s.cols;
-  float d = L.depth[i];
+  float d = depth[i];
   float4 nrm = make_float4(0.f, 0.f, 0.f, 0.f);
   if (!(d > 0.0f)) {
-    L.normal[i] = nrm;
-    if (L.vertex) L.vertex[i] = nrm;
+    normal[i] = nrm;
+    if (vertex) vertex[i] = nrm;
     return;
   }
   F3 p = point3d(i, d, s);
-  if (L.vertex) L.vertex[i] = make_float4(p.x, p.y, p.z, 1.0f);
+  if (vertex) vertex[i] = make_float4(p.x, p.y, p.z, 1.0f);
   if (x - 2 >= 0 && x + 2 < s.cols && y - 1 >= 0 && y + 1 < s.rows) {
     int il = i - 2, ir = i + 2, iu = i - s.cols, id = i + s.cols;
-    float dl = L.depth[il], dr = L.depth[ir], du = L.depth[iu], dd = L.depth[id];
+    float dl = depth[il], dr = depth[ir], du = depth[iu], dd = depth[id];
     if (dl > 0.0f && dr > 0.0f && du > 0.0f && dd > 0.0f) {
       F3 left = point3d(il, dl, s), right = point3d(ir, dr, s);
       F3 up = point3d(iu, du, s), down = point3d(id, dd, s);
@@ -152,7 +170,27 @@ __global__ void maps_kernel(MapsArgs a) {
       }
     }
   }
-  L.normal[i] = nrm;
+  normal[i] = nrm;
+}
+
+// all pyramid levels of one image in one launch
+__global__ void maps_kernel(MapsArgs a) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= a.total) return;
+  int l = 0;
+#pragma unroll
+  for (int k = 1; k < kLevels; ++k)
+    if (k < a.nlev && g >= a.lv[k].offset) l = k;
+  const LevelMaps& L = a.lv[l];
+  maps_px(L.depth, L.normal, L.vertex, L.s, g - L.offset);
+}
+
+__device__ inline void target_prepare_px(const float* __restrict__ ray, float* __restrict__ d0,
+                                         float dmax, const uint8_t* __restrict__ rgb,
+                                         float* __restrict__ inten, int i) {
+  float d = ray[i];
+  d0[i] = (d < dmax) ? d : 0.0f;
+  if (inten) inten[i] = rgb ? intensity_u8(rgb + 3 * (size_t)i) : 0.0f;
 }
 
 __global__ void target_prepare_kernel(const float* __restrict__ ray, float* __restrict__ d0,
@@ -160,9 +198,72 @@ __global__ void target_prepare_kernel(const float* __restrict__ ray, float* __re
                                       float* __restrict__ inten, int n) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  float d = ray[i];
-  d0[i] = (d < dmax) ? d : 0.0f;
-  if (inten) inten[i] = rgb ? intensity_u8(rgb + 3 * (size_t)i) : 0.0f;
+  target_prepare_px(ray, d0, dmax, rgb, inten, i);
+}
+
+// ---------------------------------------------------------------- fused
+// ingest (+ the unfiltered copy when the bilateral filter is off)
+__global__ void fused_ingest_kernel(const SessDev* __restrict__ tab) {
+  const SessDev& S = tab[blockIdx.z];
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= S.npx) return;
+  ingest_px(S.u16, *S.rgb_flag ? S.rgb : nullptr, S.depth_scaler, S.raw,
+            S.use_color ? S.sint[0] : nullptr, i);
+  if (!S.bil_enabled) S.filt[i] = S.raw[i];
+}
+
+__global__ void fused_bilateral_kernel(const SessDev* __restrict__ tab) {
+  extern __shared__ float tile[];
+  const SessDev& S = tab[blockIdx.z];
+  if (!S.bil_enabled) return;
+  const int rows = S.ls[0].rows, cols = S.ls[0].cols;
+  if ((int)blockIdx.x * BTX >= cols || (int)blockIdx.y * BTY >= rows) return;
+  bilateral_tile(S.raw, S.filt, rows, cols, *S.btab, blockIdx.x, blockIdx.y, tile);
+}
+
+// level l of the source (target == 0) or target pyramid from level l-1
+__global__ void fused_downsample_kernel(const SessDev* __restrict__ tab, int l, int target) {
+  const SessDev& S = tab[blockIdx.z];
+  if (l >= S.nlev) return;
+  const DSensor& sp = S.ls[l - 1];
+  const int c2 = sp.cols / 2, n = (sp.rows / 2) * c2;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  downsample_depth_px(target ? S.tdep[l - 1] : S.sdep[l - 1], sp.cols, c2,
+                      target ? S.tdep[l] : S.sdep[l], i);
+  if (S.use_color)
+    downsample_intensity_px(target ? S.tint[l - 1] : S.sint[l - 1], sp.cols, c2,
+                            target ? S.tint[l] : S.sint[l], i);
+}
+
+__global__ void fused_maps_kernel(const SessDev* __restrict__ tab, int target) {
+  const SessDev& S = tab[blockIdx.z];
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  for (int l = 0; l < S.nlev; ++l) {
+    const int n = S.ls[l].rows * S.ls[l].cols;
+    if (g < n) {
+      float4* vtx = S.debug_maps ? (target ? S.tvtx[l] : S.svtx[l]) : nullptr;
+      maps_px(target ? S.tdep[l] : S.sdep[l], target ? S.tnrm[l] : S.snrm[l], vtx, S.ls[l], g);
+      return;
+    }
+    g -= n;
+  }
+}
+
+// next frame's target level 0: the raycast (mode 1, misses -> 0) or the
+// source itself (mode 0); flags the target as present
+__global__ void fused_target_prepare_kernel(const SessDev* __restrict__ tab) {
+  const SessDev& S = tab[blockIdx.z];
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) S.icp->have_target = 1;
+  if (i >= S.npx) return;
+  if (S.mode == 1) {
+    target_prepare_px(S.ray, S.tdep[0], S.vol.t.dmax, S.use_color ? S.trgb : nullptr,
+                      S.use_color ? S.tint[0] : nullptr, i);
+  } else {
+    S.tdep[0][i] = S.sdep[0][i];
+    if (S.use_color) S.tint[0][i] = S.sint[0][i];
+  }
 }
 
 inline int nblk(long long n, int t) { return (int)((n + t - 1) / t); }
@@ -198,12 +299,16 @@ BilateralTable make_bilateral_table(int radius, float sigma_i, float sigma_s) {
   return tb;
 }
 
+static size_t bilateral_smem(int radius) {
+  int D = 2 * radius;
+  return sizeof(float) * ((size_t)(BTX + D - 1) * (BTY + D - 1));
+}
+
 void launch_bilateral(const float* src, float* dst, int rows, int cols, const BilateralTable& tb,
                       cudaStream_t st) {
-  int D = 2 * tb.radius;
-  size_t smem = sizeof(float) * ((size_t)(BTX + D - 1) * (BTY + D - 1));
   dim3 grid(nblk(cols, BTX), nblk(rows, BTY));
-  bilateral_kernel<<<grid, dim3(BTX, BTY), smem, st>>>(src, dst, rows, cols, tb);
+  bilateral_kernel<<<grid, dim3(BTX, BTY), bilateral_smem(tb.radius), st>>>(src, dst, rows, cols,
+                                                                            tb);
 }
 
 void launch_downsample_depth(const float* src, int rows, int cols, float* dst, cudaStream_t st) {
@@ -225,6 +330,31 @@ void launch_target_prepare(const float* ray_depth, float* depth0, float dmax, co
 }
 void launch_copy_f(const float* src, float* dst, size_t n, cudaStream_t st) {
   if (n) cudaMemcpyAsync(dst, src, n * sizeof(float), cudaMemcpyDeviceToDevice, st);
+}
+
+// ---- fused stages
+void fused_ingest(const SessDev* tab, const BatchShape& b, cudaStream_t st) {
+  fused_ingest_kernel<<<dim3(nblk(b.max_npx, 256), 1, b.n), 256, 0, st>>>(tab);
+}
+
+void fused_bilateral(const SessDev* tab, const BatchShape& b, cudaStream_t st) {
+  if (b.max_bil_radius > 0)
+    fused_bilateral_kernel<<<dim3(nblk(b.max_cols, BTX), nblk(b.max_rows, BTY), b.n),
+                             dim3(BTX, BTY), bilateral_smem(b.max_bil_radius), st>>>(tab);
+}
+
+void fused_pyramid(const SessDev* tab, const BatchShape& b, int target, cudaStream_t st) {
+  for (int l = 1; l < b.max_nlev; ++l)
+    if (b.max_level_px[l] > 0)
+      fused_downsample_kernel<<<dim3(nblk(b.max_level_px[l], 256), 1, b.n), 256, 0, st>>>(
+          tab, l, target);
+  int tot = 0;
+  for (int l = 0; l < b.max_nlev; ++l) tot += b.max_level_px[l];
+  fused_maps_kernel<<<dim3(nblk(tot, 256), 1, b.n), 256, 0, st>>>(tab, target);
+}
+
+void fused_target_prepare(const SessDev* tab, const BatchShape& b, cudaStream_t st) {
+  fused_target_prepare_kernel<<<dim3(nblk(b.max_npx, 256), 1, b.n), 256, 0, st>>>(tab);
 }
 
 }  // namespace dyn

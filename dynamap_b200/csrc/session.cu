@@ -10,12 +10,19 @@
 // counters stay on the device, so a frame needs no host synchronisation
 // between stages (the reference synchronises after every launch and solves
 // each GN iteration on the host).
+//
+// Every stage is a fused launch over a device table of session descriptors
+// (SessDev): a session alone runs a table of one, a dyn_batch runs the
+// table of its members, one launch per stage for all of them and the whole
+// frame as one graph.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <cstdint>
 #include <mutex>
 #include <new>
 #include <vector>
@@ -23,6 +30,7 @@
 #include "common.cuh"
 #include "icp.cuh"
 #include "image.cuh"
+#include "sessdev.cuh"
 #include "tsdf.cuh"
 
 using namespace dyn;
@@ -34,6 +42,9 @@ struct ResultBlock {
   IcpState icp;
   Counters cnt;
 };
+static_assert(sizeof(PoseState) % 4 == 0 && sizeof(IcpState) % 4 == 0 &&
+                  sizeof(Counters) % 4 == 0,
+              "result parts are copied as 32-bit words");
 
 int level_of_scale(int scale) {
   int l = 0;
@@ -91,6 +102,12 @@ DTsdf dtsdf(const dyn_tsdf_params& p) {
     }                                                \
   } while (0)
 
+#define DYN_TRY(x)                 \
+  do {                             \
+    dyn_status r_ = (x);           \
+    if (r_ != DYN_OK) return r_;   \
+  } while (0)
+
 bool valid_sensor(const dyn_sensor* s) {
   return s && s->rows > 0 && s->cols > 0 && s->rows <= 8192 && s->cols <= 8192 &&
          s->fx > 0 && s->fy > 0 && s->depth_scaler > 0;
@@ -132,19 +149,29 @@ struct dyn_session {
   IcpState* d_icp = nullptr;
   PoseState* d_pose = nullptr;
   VolumeDev vol;
+  // fused-launch descriptor (host copy and its device table of one)
+  SessDev hsd;
+  SessDev* d_sd = nullptr;
+  BilateralTable* d_btab = nullptr;
+  int* d_rgb_flag = nullptr;   // nonzero: the current frame carries RGB
+  int rgb_flag_host = -1;      // last value written (-1: unknown)
+  int2* d_gvis = nullptr;      // visible list of the table of one
+  int* d_gcount = nullptr;
+  ResultBlock* d_res = nullptr;
+  BatchShape shape;
+  dyn_batch* batch = nullptr;  // member of this batch (frames go through it)
   // host
   uint16_t* h_depth = nullptr;
   uint8_t* h_rgb = nullptr;
   ResultBlock* h_res = nullptr;
-  // graphs: [has_rgb]
-  cudaGraphExec_t exec[2] = {nullptr, nullptr};
+  cudaGraphExec_t exec = nullptr;
   BilateralTable btab;
   // profiling: ev[i] ends stage i (DYN_STAGE_*), ev[DYN_STAGE_FRAME] starts the frame
   bool profile = false;
   cudaEvent_t ev[DYN_NUM_STAGES] = {};
   double stage_ms[DYN_NUM_STAGES] = {};
   int64_t prof_frames = 0;
-  int kernels_per_frame[2] = {0, 0};
+  int kernels_per_frame = 0;
   bool debug_maps = false;
   int frames = 0;
   bool pending = false;
@@ -178,16 +205,64 @@ struct dyn_session {
   }
 };
 
+// A fixed set of sessions on one device whose frames run together: each
+// stage is one launch over the members' descriptor table and the whole frame
+// one CUDA graph on the batch's stream.
+struct dyn_batch {
+  int device = 0;
+  int n = 0;
+  std::vector<dyn_session*> ss;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t h2d_done = nullptr;
+  std::vector<void*> allocs;
+  SessDev* d_tab = nullptr;
+  int2* d_gvis = nullptr;
+  int* d_gcount = nullptr;
+  ResultBlock* d_res = nullptr;
+  ResultBlock* h_res = nullptr;  // pinned, n entries
+  BatchShape shape;
+  cudaGraphExec_t exec = nullptr;
+  int kernels_per_frame = 0;
+  bool profile = false;
+  cudaEvent_t ev[DYN_NUM_STAGES] = {};
+  double stage_ms[DYN_NUM_STAGES] = {};
+  int64_t prof_frames = 0;
+  bool pending = false;
+};
+
 namespace {
+
+void release(dyn_batch* b) {
+  if (!b) return;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  for (dyn_session* s : b->ss)
+    if (s && s->batch == b) s->batch = nullptr;
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  for (void* p : b->allocs) cudaFree(p);
+  if (b->h_res) cudaFreeHost(b->h_res);
+  if (b->h2d_done) cudaEventDestroy(b->h2d_done);
+  for (int k = 0; k < DYN_NUM_STAGES; ++k)
+    if (b->ev[k]) cudaEventDestroy(b->ev[k]);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  cudaSetDevice(prev);
+  delete b;
+}
 
 void release(dyn_session* s) {
   if (!s) return;
   int prev = 0;
   cudaGetDevice(&prev);
   cudaSetDevice(s->device);
+  if (s->batch) {  // a destroyed member leaves its batch unusable
+    cudaStreamSynchronize(s->batch->stream);
+    for (auto& m : s->batch->ss)
+      if (m == s) m = nullptr;
+  }
   if (s->stream) cudaStreamSynchronize(s->stream);
-  for (int k = 0; k < 2; ++k)
-    if (s->exec[k]) cudaGraphExecDestroy(s->exec[k]);
+  if (s->exec) cudaGraphExecDestroy(s->exec);
   for (void* p : s->allocs) cudaFree(p);
   if (s->h_depth) cudaFreeHost(s->h_depth);
   if (s->h_rgb) cudaFreeHost(s->h_rgb);
@@ -213,12 +288,6 @@ struct DeviceGuard {
   }
 };
 
-void reset_frame_counters(dyn_session* s) {
-  // every counter but nalloc (the heap top persists)
-  cudaMemsetAsync(reinterpret_cast<char*>(s->vol.cnt) + sizeof(int), 0,
-                  sizeof(Counters) - sizeof(int), s->stream);
-}
-
 MapsArgs maps_args(dyn_session* s, bool target) {
   MapsArgs a;
   int off = 0;
@@ -235,11 +304,17 @@ MapsArgs maps_args(dyn_session* s, bool target) {
   return a;
 }
 
-// Stage boundary event (profiling only; captured into the frame graph).
-void mark(dyn_session* s, int stage) {
-  // External: during capture this becomes an event-record node of the graph
-  if (s->profile) cudaEventRecordWithFlags(s->ev[stage], s->stream, cudaEventRecordExternal);
-}
+// Stage boundary events (profiling only; captured into the frame graph):
+// ev[i] ends stage i, ev[DYN_STAGE_FRAME] starts the frame.
+struct Marks {
+  bool on = false;
+  cudaEvent_t* ev = nullptr;
+  cudaStream_t st = nullptr;
+  void operator()(int stage) const {
+    // External: during capture this becomes an event-record node of the graph
+    if (on) cudaEventRecordWithFlags(ev[stage], st, cudaEventRecordExternal);
+  }
+};
 
 __global__ void mark_target_kernel(IcpState* st) {
   if (threadIdx.x == 0 && blockIdx.x == 0) st->have_target = 1;
@@ -248,103 +323,80 @@ __global__ void bump_frame_kernel(PoseState* ps) {
   if (threadIdx.x == 0 && blockIdx.x == 0) ps->frame += 1;
 }
 
+__device__ inline void copy_words(void* dst, const void* src, int bytes) {
+  for (int k = threadIdx.x; k < bytes / 4; k += blockDim.x)
+    static_cast<unsigned*>(dst)[k] = static_cast<const unsigned*>(src)[k];
+}
+// pose, solver state and counters of every session into one array, read
+// back by one copy
+__global__ void gather_results_kernel(const SessDev* __restrict__ tab, int n,
+                                      ResultBlock* __restrict__ out) {
+  const int i = blockIdx.x;
+  if (i >= n) return;
+  const SessDev& S = tab[i];
+  copy_words(&out[i].pose, S.pose, (int)sizeof(PoseState));
+  copy_words(&out[i].icp, S.icp, (int)sizeof(IcpState));
+  copy_words(&out[i].cnt, S.vol.cnt, (int)sizeof(Counters));
+}
+
 // Source side of a frame: ingest, bilateral filter, pyramid, normal maps.
-void enqueue_source(dyn_session* s, bool has_rgb) {
-  cudaStream_t st = s->stream;
-  const int n = (int)s->npx;
-  const bool col = s->use_color();
-  mark(s, DYN_STAGE_FRAME);
-  launch_ingest(s->d_u16, has_rgb ? s->d_rgb : nullptr, n, s->sensor.depth_scaler, s->d_raw,
-                col ? s->d_sint[0] : nullptr, st);
-  mark(s, DYN_STAGE_INGEST);
-  if (s->bp.enabled)
-    launch_bilateral(s->d_raw, s->d_filt, (int)s->sensor.rows, (int)s->sensor.cols, s->btab, st);
-  else
-    launch_copy_f(s->d_raw, s->d_filt, s->npx, st);
-  mark(s, DYN_STAGE_BILATERAL);
-  for (int l = 1; l < s->nlev; ++l) {
-    launch_downsample_depth(s->d_sdep[l - 1], s->ls[l - 1].rows, s->ls[l - 1].cols, s->d_sdep[l], st);
-    if (col)
-      launch_downsample_intensity(s->d_sint[l - 1], s->ls[l - 1].rows, s->ls[l - 1].cols,
-                                  s->d_sint[l], st);
-  }
-  launch_maps(maps_args(s, false), st);
-  mark(s, DYN_STAGE_SOURCE_MAPS);
+void enqueue_source(const SessDev* tab, const BatchShape& b, cudaStream_t st, const Marks& m) {
+  m(DYN_STAGE_FRAME);
+  fused_reset_counters(tab, b, st);
+  fused_ingest(tab, b, st);
+  m(DYN_STAGE_INGEST);
+  fused_bilateral(tab, b, st);
+  m(DYN_STAGE_BILATERAL);
+  fused_pyramid(tab, b, 0, st);
+  m(DYN_STAGE_SOURCE_MAPS);
+}
+
+// gnSolver::solve's level loop (gnSolver.cu:340-431): iterations 1 .. N-1
+// of each level slot.
+void enqueue_icp(const SessDev* tab, const BatchShape& b, cudaStream_t st) {
+  for (int pl = 0; pl < 3; ++pl)
+    for (int it = 1; it < b.max_slot_iters[pl]; ++it) fused_icp_iteration(tab, b, pl, it, st);
 }
 
 // Integration at the session pose, then the next frame's target.
-void enqueue_map_update(dyn_session* s, bool has_rgb) {
-  cudaStream_t st = s->stream;
-  launch_allocate(s->vol, s->d_raw, s->ls[0], s->d_pose, st);
-  mark(s, DYN_STAGE_ALLOCATE);
-  launch_visible(s->vol, s->ls[0], s->d_pose, st);
-  mark(s, DYN_STAGE_VISIBLE);
-  launch_integrate(s->vol, s->d_raw, has_rgb ? s->d_rgb : nullptr, s->ls[0], s->d_pose, st);
-  mark(s, DYN_STAGE_INTEGRATE);
-  const bool col = s->use_color();
-  if (s->gp.mode == 1) {
-    launch_raycast(s->vol, s->ls[0], s->d_pose, nullptr, s->d_ray, col ? s->d_trgb : nullptr, st);
-    mark(s, DYN_STAGE_RAYCAST);
-    launch_target_prepare(s->d_ray, s->d_tdep[0], s->tp.max_sensor_depth,
-                          col ? s->d_trgb : nullptr, col ? s->d_tint[0] : nullptr, (int)s->npx, st);
-    for (int l = 1; l < s->nlev; ++l) {
-      launch_downsample_depth(s->d_tdep[l - 1], s->ls[l - 1].rows, s->ls[l - 1].cols,
-                              s->d_tdep[l], st);
-      if (col)
-        launch_downsample_intensity(s->d_tint[l - 1], s->ls[l - 1].rows, s->ls[l - 1].cols,
-                                    s->d_tint[l], st);
-    }
-    launch_maps(maps_args(s, true), st);
-  } else {
-    for (int l = 0; l < s->nlev; ++l) {
-      size_t n = (size_t)s->ls[l].rows * s->ls[l].cols;
-      launch_copy_f(s->d_sdep[l], s->d_tdep[l], n, st);
-      launch_copy_f(reinterpret_cast<const float*>(s->d_snrm[l]),
-                    reinterpret_cast<float*>(s->d_tnrm[l]), 4 * n, st);
-      if (col) launch_copy_f(s->d_sint[l], s->d_tint[l], n, st);
-    }
-    mark(s, DYN_STAGE_RAYCAST);
-  }
-  mark_target_kernel<<<1, 32, 0, st>>>(s->d_icp);
-  mark(s, DYN_STAGE_TARGET_MAPS);
+void enqueue_map_update(const SessDev* tab, const BatchShape& b, cudaStream_t st,
+                        const Marks& m) {
+  fused_allocate(tab, b, st);
+  m(DYN_STAGE_ALLOCATE);
+  fused_visible(tab, b, st);
+  m(DYN_STAGE_VISIBLE);
+  fused_integrate(tab, b, st);
+  m(DYN_STAGE_INTEGRATE);
+  fused_raycast(tab, b, st);
+  m(DYN_STAGE_RAYCAST);
+  fused_target_prepare(tab, b, st);
+  fused_pyramid(tab, b, 1, st);
+  m(DYN_STAGE_TARGET_MAPS);
 }
 
 // builder::buildModelLS with the intended order: track frame k against the
 // target of frame k-1, integrate frame k at the new pose, raycast the target
-// for frame k+1.
-void enqueue_icp(dyn_session* s) {
-  cudaStream_t st = s->stream;
-  IcpParams P = s->icp_params();
-  for (int pl = 0; pl < 3; ++pl) {
-    int l = level_of_scale(s->gp.lvl_scale[pl]);
-    IcpLevel L;
-    L.sd = s->d_sdep[l];
-    L.sn = s->d_snrm[l];
-    L.si = s->d_sint[l];
-    L.td = s->d_tdep[l];
-    L.tn = s->d_tnrm[l];
-    L.ti = s->d_tint[l];
-    L.s = s->ls[l];
-    for (int it = 1; it < s->gp.lvl_iteration_num[pl]; ++it)
-      launch_icp_iteration(L, P, pl, it, s->d_icp, s->d_partials, st);
-  }
-  launch_pose_finalize(P, s->d_icp, s->d_pose, st);
+// for frame k+1; then the results into 'res_host' (pinned).
+void enqueue_frame(const SessDev* tab, const BatchShape& b, ResultBlock* res_dev,
+                   ResultBlock* res_host, cudaStream_t st, const Marks& m) {
+  enqueue_source(tab, b, st, m);
+  enqueue_icp(tab, b, st);
+  fused_pose_finalize(tab, b, 1, st);
+  m(DYN_STAGE_ICP);
+  enqueue_map_update(tab, b, st, m);
+  gather_results_kernel<<<b.n, 128, 0, st>>>(tab, b.n, res_dev);
+  cudaMemcpyAsync(res_host, res_dev, sizeof(ResultBlock) * (size_t)b.n, cudaMemcpyDeviceToHost,
+                  st);
 }
 
-void enqueue_frame(dyn_session* s, bool has_rgb) {
-  reset_frame_counters(s);
-  enqueue_source(s, has_rgb);
-  enqueue_icp(s);
-  bump_frame_kernel<<<1, 32, 0, s->stream>>>(s->d_pose);
-  mark(s, DYN_STAGE_ICP);
-  enqueue_map_update(s, has_rgb);
-}
-
-dyn_status build_graph(dyn_session* s, bool has_rgb) {
+// Captures one frame of 'tab' on 'st' into an executable graph.
+dyn_status capture_frame(const SessDev* tab, const BatchShape& b, ResultBlock* res_dev,
+                         ResultBlock* res_host, cudaStream_t st, const Marks& m,
+                         cudaGraphExec_t* exec_out, int* kernels_out) {
   cudaGraph_t g = nullptr;
-  DYN_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-  enqueue_frame(s, has_rgb);
-  cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+  DYN_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  enqueue_frame(tab, b, res_dev, res_host, st, m);
+  cudaError_t e = cudaStreamEndCapture(st, &g);
   if (e != cudaSuccess) return DYN_ERR_CUDA;
   size_t nn = 0;
   cudaGraphGetNodes(g, nullptr, &nn);
@@ -355,12 +407,100 @@ dyn_status build_graph(dyn_session* s, bool has_rgb) {
     cudaGraphNodeType ty;
     if (cudaGraphNodeGetType(nodes[i], &ty) == cudaSuccess && ty == cudaGraphNodeTypeKernel) ++nk;
   }
-  s->kernels_per_frame[has_rgb ? 1 : 0] = nk;
+  *kernels_out = nk;
   cudaGraphExec_t ex = nullptr;
   e = cudaGraphInstantiate(&ex, g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return DYN_ERR_CUDA;
-  s->exec[has_rgb ? 1 : 0] = ex;
+  *exec_out = ex;
+  return DYN_OK;
+}
+
+// The launch shape of a table of sessions: the largest image, level and
+// heap of its members bound every grid.
+BatchShape make_shape(dyn_session* const* ss, int n, int2* gvis, int* gcount, int gvis_cap) {
+  BatchShape b;
+  std::memset(&b, 0, sizeof(b));
+  b.n = n;
+  b.gvis = gvis;
+  b.gcount = gcount;
+  b.gvis_cap = gvis_cap;
+  for (int i = 0; i < n; ++i) {
+    const dyn_session* s = ss[i];
+    b.max_rows = std::max(b.max_rows, s->ls[0].rows);
+    b.max_cols = std::max(b.max_cols, s->ls[0].cols);
+    b.max_npx = std::max(b.max_npx, (int)s->npx);
+    b.max_nlev = std::max(b.max_nlev, s->nlev);
+    b.max_blocks = std::max(b.max_blocks, s->tp.num_blocks);
+    for (int l = 0; l < s->nlev; ++l)
+      b.max_level_px[l] = std::max(b.max_level_px[l], s->ls[l].rows * s->ls[l].cols);
+    for (int pl = 0; pl < 3; ++pl) {
+      const int l = level_of_scale(s->gp.lvl_scale[pl]);
+      b.max_slot_px[pl] = std::max(b.max_slot_px[pl], s->ls[l].rows * s->ls[l].cols);
+      b.max_slot_iters[pl] = std::max(b.max_slot_iters[pl], s->gp.lvl_iteration_num[pl]);
+    }
+    if (s->bp.enabled) b.max_bil_radius = std::max(b.max_bil_radius, s->btab.radius);
+    b.kahan_mask |= s->icp_params().kahan ? 2 : 1;
+  }
+  return b;
+}
+
+// The session's descriptor (device buffers, sensor levels, parameters).
+void fill_sessdev(dyn_session* s) {
+  SessDev& d = s->hsd;
+  std::memset(&d, 0, sizeof(d));
+  for (int l = 0; l < kLevels; ++l) d.ls[l] = s->ls[l];
+  d.nlev = s->nlev;
+  d.npx = (int)s->npx;
+  d.depth_scaler = s->sensor.depth_scaler;
+  d.rgb_flag = s->d_rgb_flag;
+  d.use_color = s->use_color() ? 1 : 0;
+  d.bil_enabled = s->bp.enabled ? 1 : 0;
+  d.mode = s->gp.mode;
+  d.debug_maps = 0;
+  d.u16 = s->d_u16;
+  d.rgb = s->d_rgb;
+  d.raw = s->d_raw;
+  d.filt = s->d_filt;
+  for (int l = 0; l < s->nlev; ++l) {
+    d.sdep[l] = s->d_sdep[l];
+    d.snrm[l] = s->d_snrm[l];
+    d.svtx[l] = s->d_svtx[l];
+    d.sint[l] = s->d_sint[l];
+    d.tdep[l] = s->d_tdep[l];
+    d.tnrm[l] = s->d_tnrm[l];
+    d.tvtx[l] = s->d_tvtx[l];
+    d.tint[l] = s->d_tint[l];
+  }
+  d.ray = s->d_ray;
+  d.trgb = s->d_trgb;
+  d.btab = s->d_btab;
+  d.icp = s->d_icp;
+  d.pose = s->d_pose;
+  d.partials = s->d_partials;
+  d.icpp = s->icp_params();
+  for (int pl = 0; pl < 3; ++pl) {
+    d.slot_level[pl] = level_of_scale(s->gp.lvl_scale[pl]);
+    d.slot_iters[pl] = s->gp.lvl_iteration_num[pl];
+  }
+  d.vol = s->vol;
+}
+
+// Marks whether this frame of 's' carries RGB (stream-ordered; written only
+// when it changes).  The memset writes 0x01 into every byte: any nonzero
+// value means "RGB present".
+dyn_status set_rgb_flag(dyn_session* s, bool has_rgb, cudaStream_t st) {
+  const int v = has_rgb ? 1 : 0;
+  if (s->rgb_flag_host != v) {
+    DYN_CUDA(cudaMemsetAsync(s->d_rgb_flag, v, sizeof(int), st));
+    s->rgb_flag_host = v;
+  }
+  return DYN_OK;
+}
+
+// Session calls that read device state wait for the batch it belongs to.
+dyn_status quiesce(dyn_session* s) {
+  if (s->batch) DYN_CUDA(cudaStreamSynchronize(s->batch->stream));
   return DYN_OK;
 }
 
@@ -373,40 +513,74 @@ bool is_pinned(const void* p) {
   return a.type == cudaMemoryTypeHost;
 }
 
-dyn_status upload_frame(dyn_session* s, const uint16_t* depth, const uint8_t* rgb) {
+// Host frame into the session's device input buffers on 'st' (pinned
+// sources directly, others through the session's pinned staging buffers).
+dyn_status copy_frame_in(dyn_session* s, const uint16_t* depth, const uint8_t* rgb,
+                         cudaStream_t st) {
   size_t nd = s->npx * sizeof(uint16_t), nc = s->npx * 3;
-  // the staging buffers may still feed the previous frame's copies
-  DYN_CUDA(cudaEventSynchronize(s->h2d_done));
   if (is_pinned(depth)) {
-    DYN_CUDA(cudaMemcpyAsync(s->d_u16, depth, nd, cudaMemcpyHostToDevice, s->stream));
+    DYN_CUDA(cudaMemcpyAsync(s->d_u16, depth, nd, cudaMemcpyHostToDevice, st));
   } else {
     std::memcpy(s->h_depth, depth, nd);
-    DYN_CUDA(cudaMemcpyAsync(s->d_u16, s->h_depth, nd, cudaMemcpyHostToDevice, s->stream));
+    DYN_CUDA(cudaMemcpyAsync(s->d_u16, s->h_depth, nd, cudaMemcpyHostToDevice, st));
   }
   if (rgb) {
     if (is_pinned(rgb)) {
-      DYN_CUDA(cudaMemcpyAsync(s->d_rgb, rgb, nc, cudaMemcpyHostToDevice, s->stream));
+      DYN_CUDA(cudaMemcpyAsync(s->d_rgb, rgb, nc, cudaMemcpyHostToDevice, st));
     } else {
       std::memcpy(s->h_rgb, rgb, nc);
-      DYN_CUDA(cudaMemcpyAsync(s->d_rgb, s->h_rgb, nc, cudaMemcpyHostToDevice, s->stream));
+      DYN_CUDA(cudaMemcpyAsync(s->d_rgb, s->h_rgb, nc, cudaMemcpyHostToDevice, st));
     }
   }
+  return set_rgb_flag(s, rgb != nullptr, st);
+}
+
+dyn_status upload_frame(dyn_session* s, const uint16_t* depth, const uint8_t* rgb) {
+  // the staging buffers may still feed the previous frame's copies
+  DYN_CUDA(cudaEventSynchronize(s->h2d_done));
+  dyn_status r = copy_frame_in(s, depth, rgb, s->stream);
+  if (r != DYN_OK) return r;
   DYN_CUDA(cudaEventRecord(s->h2d_done, s->stream));
   return DYN_OK;
 }
 
-dyn_status launch_frame(dyn_session* s, bool has_rgb) {
-  int k = has_rgb ? 1 : 0;
-  if (!s->exec[k]) {
-    dyn_status r = build_graph(s, has_rgb);
+Marks session_marks(dyn_session* s) {
+  Marks m;
+  m.on = s->profile;
+  m.ev = s->ev;
+  m.st = s->stream;
+  return m;
+}
+
+dyn_status launch_frame(dyn_session* s) {
+  if (!s->exec) {
+    dyn_status r = capture_frame(s->d_sd, s->shape, s->d_res, s->h_res, s->stream,
+                                 session_marks(s), &s->exec, &s->kernels_per_frame);
     if (r != DYN_OK) return r;
   }
-  DYN_CUDA(cudaGraphLaunch(s->exec[k], s->stream));
-  DYN_CUDA(cudaMemcpyAsync(s->h_res, s->d_pose, sizeof(PoseState), cudaMemcpyDeviceToHost, s->stream));
-  DYN_CUDA(cudaMemcpyAsync(&s->h_res->icp, s->d_icp, sizeof(IcpState), cudaMemcpyDeviceToHost, s->stream));
-  DYN_CUDA(cudaMemcpyAsync(&s->h_res->cnt, s->vol.cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s->stream));
+  DYN_CUDA(cudaGraphLaunch(s->exec, s->stream));
   s->pending = true;
   s->frames++;
+  return DYN_OK;
+}
+
+// Stage times of one profiled frame added to 'ms'.
+void add_stage_times(cudaEvent_t* ev, double* ms_acc, int64_t* frames) {
+  float ms = 0.0f;
+  int prev = DYN_STAGE_FRAME;
+  for (int k = 0; k <= DYN_STAGE_TARGET_MAPS; ++k) {
+    if (cudaEventElapsedTime(&ms, ev[prev], ev[k]) == cudaSuccess) ms_acc[k] += ms;
+    prev = k;
+  }
+  if (cudaEventElapsedTime(&ms, ev[DYN_STAGE_FRAME], ev[DYN_STAGE_TARGET_MAPS]) == cudaSuccess)
+    ms_acc[DYN_STAGE_FRAME] += ms;
+  cudaGetLastError();
+  ++*frames;
+}
+
+dyn_status counters_status(const Counters& c) {
+  if (c.heap_exhausted) return DYN_ERR_HEAP_EXHAUSTED;
+  if (c.bucket_full) return DYN_ERR_HASH_FULL;
   return DYN_OK;
 }
 
@@ -450,16 +624,25 @@ dyn_status reset_state(dyn_session* s) {
   return DYN_OK;
 }
 
-size_t session_bytes(const dyn_tsdf_params& t, const dyn_sensor& s) {
+// Mixed-precision sessions keep per-voxel colour only when the photometric
+// term needs the model's colour.
+bool mixed_colour(const dyn_gn_params* gn) { return gn && gn->color_weight != 0.0f; }
+
+size_t session_bytes(const dyn_tsdf_params& t, const dyn_sensor& s, int precision = 0,
+                     bool colour = true) {
   size_t n = (size_t)s.rows * s.cols;
   size_t b = 0;
   b += sizeof(Entry) * (size_t)t.num_buckets * t.bucket_size;
   b += sizeof(unsigned long long) * (size_t)t.num_blocks;
-  b += sizeof(dyn_voxel) * (size_t)t.num_blocks * kBlockVox;
-  b += sizeof(int) * (size_t)t.num_blocks;
+  if (precision == DYN_PRECISION_MIXED)
+    b += (4 + (colour ? 4 : 0)) * (size_t)t.num_blocks * kBlockVox;
+  else
+    b += sizeof(dyn_voxel) * (size_t)t.num_blocks * kBlockVox;
+  b += sizeof(int2) * (size_t)t.num_blocks;  // visible list
   b += n * (2 + 3 + 4 + 4 + 4 + 3);  // inputs, raw, filtered, ray depth, target rgb
   b += 2 * n * (4 + 16 + 16 + 4) * 4 / 3;  // source + target pyramids
-  b += icp_scratch_bytes() + 4096;
+  b += icp_scratch_bytes() + sizeof(SessDev) + sizeof(BilateralTable) + sizeof(ResultBlock) +
+       8192;
   return b;
 }
 
@@ -498,9 +681,10 @@ const char* dyn_status_string(dyn_status s) {
 
 dyn_status dyn_session_bytes(const dyn_tsdf_params* tsdf, const dyn_sensor* sensor,
                              int32_t precision, size_t* bytes_out) {
-  (void)precision;
   if (!tsdf || !valid_sensor(sensor) || !bytes_out) return DYN_ERR_INVALID_ARG;
-  *bytes_out = session_bytes(*tsdf, *sensor);
+  // colour storage of a mixed session depends on its photometric weight,
+  // which is not passed here: count it (upper bound)
+  *bytes_out = session_bytes(*tsdf, *sensor, precision, true);
   return DYN_OK;
 }
 
@@ -511,7 +695,8 @@ dyn_status dyn_session_create(const dyn_tsdf_params* tsdf, const dyn_gn_params* 
   *out = nullptr;
   if (!tsdf || !gn || !bil || !valid_sensor(sensor)) return DYN_ERR_INVALID_ARG;
   if (tsdf->block_size != kBlockSize || tsdf->bucket_size < 1 || tsdf->num_buckets < 1 ||
-      tsdf->num_blocks < 1 || tsdf->max_sdf_weight < 1 || tsdf->max_sdf_weight > 255 ||
+      tsdf->num_blocks < 1 || tsdf->max_sdf_weight < 1 ||
+      tsdf->max_sdf_weight > (precision == DYN_PRECISION_MIXED ? 65535 : 255) ||
       !(tsdf->voxel_size > 0) || !(tsdf->truncation_distance > 0) ||
       !(tsdf->max_sensor_depth > 0))
     return DYN_ERR_INVALID_ARG;
@@ -547,6 +732,7 @@ dyn_status dyn_session_create(const dyn_tsdf_params* tsdf, const dyn_gn_params* 
   for (int k = 0; k < 3; ++k) maxl = std::max(maxl, level_of_scale(gn->lvl_scale[k]));
   s->nlev = maxl + 1;
   for (int l = 0; l < kLevels; ++l) s->ls[l] = dsensor(level_sensor(*sensor, 1 << l));
+  std::memset(&s->btab, 0, sizeof(s->btab));
   if (bil->enabled) s->btab = make_bilateral_table(bil->diameter, bil->sigma_i, bil->sigma_s);
   dyn_status r = DYN_OK;
 #define TRY(x)               \
@@ -590,9 +776,24 @@ dyn_status dyn_session_create(const dyn_tsdf_params* tsdf, const dyn_gn_params* 
   s->vol.t = dtsdf(*tsdf);
   TRY(s->dalloc(&s->vol.entries, sizeof(Entry) * (size_t)tsdf->num_buckets * tsdf->bucket_size));
   TRY(s->dalloc(&s->vol.block_keys, sizeof(unsigned long long) * (size_t)tsdf->num_blocks));
-  TRY(s->dalloc(&s->vol.voxels, sizeof(dyn_voxel) * (size_t)tsdf->num_blocks * kBlockVox));
-  TRY(s->dalloc(&s->vol.visible, sizeof(int) * (size_t)tsdf->num_blocks));
+  const size_t nvox = (size_t)tsdf->num_blocks * kBlockVox;
+  s->vol.voxels = nullptr;
+  s->vol.vox16 = nullptr;
+  s->vol.colors = nullptr;
+  s->vol.fp16 = precision == DYN_PRECISION_MIXED ? 1 : 0;
+  if (s->vol.fp16) {
+    TRY(s->dalloc(&s->vol.vox16, sizeof(unsigned) * nvox));
+    if (mixed_colour(gn)) TRY(s->dalloc(&s->vol.colors, sizeof(uchar4) * nvox));
+  } else {
+    TRY(s->dalloc(&s->vol.voxels, sizeof(dyn_voxel) * nvox));
+  }
   TRY(s->dalloc(&s->vol.cnt, sizeof(Counters)));
+  TRY(s->dalloc(&s->d_gvis, sizeof(int2) * (size_t)tsdf->num_blocks));
+  TRY(s->dalloc(&s->d_gcount, sizeof(int)));
+  TRY(s->dalloc(&s->d_rgb_flag, sizeof(int)));
+  TRY(s->dalloc(&s->d_res, sizeof(ResultBlock)));
+  TRY(s->dalloc(&s->d_btab, sizeof(BilateralTable)));
+  TRY(s->dalloc(&s->d_sd, sizeof(SessDev)));
   if (cudaMallocHost(&s->h_depth, n * 2) != cudaSuccess ||
       cudaMallocHost(&s->h_rgb, n * 3) != cudaSuccess ||
       cudaMallocHost(&s->h_res, sizeof(ResultBlock)) != cudaSuccess) {
@@ -607,6 +808,18 @@ dyn_status dyn_session_create(const dyn_tsdf_params* tsdf, const dyn_gn_params* 
     cudaMemsetAsync(s->d_tnrm[l], 0, m * 16, s->stream);
     cudaMemsetAsync(s->d_tint[l], 0, m * 4, s->stream);
     cudaMemsetAsync(s->d_sint[l], 0, m * 4, s->stream);
+  }
+  cudaMemsetAsync(s->d_rgb_flag, 0, sizeof(int), s->stream);
+  s->rgb_flag_host = 0;
+  fill_sessdev(s);
+  dyn_session* self = s;
+  s->shape = make_shape(&self, 1, s->d_gvis, s->d_gcount, tsdf->num_blocks);
+  if (cudaMemcpyAsync(s->d_btab, &s->btab, sizeof(BilateralTable), cudaMemcpyHostToDevice,
+                      s->stream) != cudaSuccess ||
+      cudaMemcpyAsync(s->d_sd, &s->hsd, sizeof(SessDev), cudaMemcpyHostToDevice, s->stream) !=
+          cudaSuccess) {
+    release(s);
+    return DYN_ERR_CUDA;
   }
   cudaEventRecord(s->h2d_done, s->stream);
   TRY(reset_state(s));
@@ -624,6 +837,7 @@ dyn_status dyn_session_destroy(dyn_session* s) {
 dyn_status dyn_session_reset(dyn_session* s) {
   if (!s) return DYN_ERR_INVALID_ARG;
   DeviceGuard dg(s->device);
+  DYN_TRY(quiesce(s));
   DYN_CUDA(cudaStreamSynchronize(s->stream));
   return reset_state(s);
 }
@@ -631,6 +845,7 @@ dyn_status dyn_session_reset(dyn_session* s) {
 dyn_status dyn_session_get_pose(dyn_session* s, float pose_out[16]) {
   if (!s || !pose_out) return DYN_ERR_INVALID_ARG;
   DeviceGuard dg(s->device);
+  DYN_TRY(quiesce(s));
   PoseState p;
   DYN_CUDA(cudaMemcpyAsync(&p, s->d_pose, sizeof(p), cudaMemcpyDeviceToHost, s->stream));
   DYN_CUDA(cudaStreamSynchronize(s->stream));
@@ -641,6 +856,7 @@ dyn_status dyn_session_get_pose(dyn_session* s, float pose_out[16]) {
 dyn_status dyn_session_set_pose(dyn_session* s, const float pose[16]) {
   if (!s || !pose) return DYN_ERR_INVALID_ARG;
   DeviceGuard dg(s->device);
+  DYN_TRY(quiesce(s));
   double P[16];
   for (int k = 0; k < 16; ++k) P[k] = (double)pose[k];
   DYN_CUDA(cudaMemcpyAsync(s->d_pose_in, P, sizeof(P), cudaMemcpyHostToDevice, s->stream));
@@ -650,20 +866,21 @@ dyn_status dyn_session_set_pose(dyn_session* s, const float pose[16]) {
 }
 
 dyn_status dyn_frame_submit(dyn_session* s, const uint16_t* depth_host, const uint8_t* rgb_host) {
-  if (!s || !depth_host) return DYN_ERR_INVALID_ARG;
+  if (!s || !depth_host || s->batch) return DYN_ERR_INVALID_ARG;
   DeviceGuard dg(s->device);
   dyn_status r = upload_frame(s, depth_host, rgb_host);
   if (r != DYN_OK) return r;
-  return launch_frame(s, rgb_host != nullptr);
+  return launch_frame(s);
 }
 
 dyn_status dyn_frame_submit_device(dyn_session* s, const uint16_t* depth_dev, const uint8_t* rgb_dev) {
-  if (!s || !depth_dev) return DYN_ERR_INVALID_ARG;
+  if (!s || !depth_dev || s->batch) return DYN_ERR_INVALID_ARG;
   DeviceGuard dg(s->device);
   DYN_CUDA(cudaMemcpyAsync(s->d_u16, depth_dev, s->npx * 2, cudaMemcpyDeviceToDevice, s->stream));
   if (rgb_dev)
     DYN_CUDA(cudaMemcpyAsync(s->d_rgb, rgb_dev, s->npx * 3, cudaMemcpyDeviceToDevice, s->stream));
-  return launch_frame(s, rgb_dev != nullptr);
+  DYN_TRY(set_rgb_flag(s, rgb_dev != nullptr, s->stream));
+  return launch_frame(s);
 }
 
 dyn_status dyn_frame_result(dyn_session* s, float pose_out[16], dyn_frame_stats* stats) {
@@ -672,56 +889,40 @@ dyn_status dyn_frame_result(dyn_session* s, float pose_out[16], dyn_frame_stats*
   DeviceGuard dg(s->device);
   DYN_CUDA(cudaStreamSynchronize(s->stream));
   s->pending = false;
-  if (s->profile) {
-    float ms = 0.0f;
-    int prev = DYN_STAGE_FRAME;
-    for (int k = 0; k <= DYN_STAGE_TARGET_MAPS; ++k) {
-      if (cudaEventElapsedTime(&ms, s->ev[prev], s->ev[k]) == cudaSuccess) s->stage_ms[k] += ms;
-      prev = k;
-    }
-    if (cudaEventElapsedTime(&ms, s->ev[DYN_STAGE_FRAME], s->ev[DYN_STAGE_TARGET_MAPS]) ==
-        cudaSuccess)
-      s->stage_ms[DYN_STAGE_FRAME] += ms;
-    cudaGetLastError();
-    s->prof_frames++;
-  }
+  if (s->profile) add_stage_times(s->ev, s->stage_ms, &s->prof_frames);
   if (pose_out)
     for (int k = 0; k < 16; ++k) pose_out[k] = (float)s->h_res->pose.pose[k];
   if (stats) fill_stats(s, *s->h_res, stats);
-  const Counters& c = s->h_res->cnt;
-  if (c.heap_exhausted) return DYN_ERR_HEAP_EXHAUSTED;
-  if (c.bucket_full) return DYN_ERR_HASH_FULL;
-  return DYN_OK;
+  return counters_status(s->h_res->cnt);
 }
 
 dyn_status dyn_integrate_with_pose(dyn_session* s, const uint16_t* depth_host,
                                    const uint8_t* rgb_host, const float pose[16]) {
-  if (!s || !depth_host || !pose) return DYN_ERR_INVALID_ARG;
+  if (!s || !depth_host || !pose || s->batch) return DYN_ERR_INVALID_ARG;
   DeviceGuard dg(s->device);
   dyn_status r = dyn_session_set_pose(s, pose);
   if (r != DYN_OK) return r;
   r = upload_frame(s, depth_host, rgb_host);
   if (r != DYN_OK) return r;
-  reset_frame_counters(s);
-  enqueue_source(s, rgb_host != nullptr);
+  const Marks none;
+  enqueue_source(s->d_sd, s->shape, s->stream, none);
   bump_frame_kernel<<<1, 32, 0, s->stream>>>(s->d_pose);
-  enqueue_map_update(s, rgb_host != nullptr);
-  DYN_CUDA(cudaMemcpyAsync(s->h_res, s->d_pose, sizeof(PoseState), cudaMemcpyDeviceToHost, s->stream));
-  DYN_CUDA(cudaMemcpyAsync(&s->h_res->cnt, s->vol.cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s->stream));
+  enqueue_map_update(s->d_sd, s->shape, s->stream, none);
+  gather_results_kernel<<<1, 128, 0, s->stream>>>(s->d_sd, 1, s->d_res);
+  DYN_CUDA(cudaMemcpyAsync(s->h_res, s->d_res, sizeof(ResultBlock), cudaMemcpyDeviceToHost,
+                           s->stream));
   DYN_CUDA(cudaStreamSynchronize(s->stream));
   DYN_CUDA(cudaGetLastError());
   s->frames++;
-  const Counters& c = s->h_res->cnt;
-  if (c.heap_exhausted) return DYN_ERR_HEAP_EXHAUSTED;
-  if (c.bucket_full) return DYN_ERR_HASH_FULL;
-  return DYN_OK;
+  return counters_status(s->h_res->cnt);
 }
 
 dyn_status dyn_solver_solve(dyn_session* s, const float* target_depth_host,
                             const uint8_t* target_rgb_host, const float* source_depth_host,
                             const uint8_t* source_rgb_host, float pose_inout[16],
                             double increment_out[6], dyn_frame_stats* stats) {
-  if (!s || !target_depth_host || !source_depth_host || !pose_inout) return DYN_ERR_INVALID_ARG;
+  if (!s || !target_depth_host || !source_depth_host || !pose_inout || s->batch)
+    return DYN_ERR_INVALID_ARG;
   DeviceGuard dg(s->device);
   cudaStream_t st = s->stream;
   const size_t n = s->npx;
@@ -755,10 +956,10 @@ dyn_status dyn_solver_solve(dyn_session* s, const float* target_depth_host,
   launch_maps(maps_args(s, true), st);
   launch_maps(maps_args(s, false), st);
   mark_target_kernel<<<1, 32, 0, st>>>(s->d_icp);
-  enqueue_icp(s);
-  DYN_CUDA(cudaMemcpyAsync(s->h_res, s->d_pose, sizeof(PoseState), cudaMemcpyDeviceToHost, st));
-  DYN_CUDA(cudaMemcpyAsync(&s->h_res->icp, s->d_icp, sizeof(IcpState), cudaMemcpyDeviceToHost, st));
-  DYN_CUDA(cudaMemcpyAsync(&s->h_res->cnt, s->vol.cnt, sizeof(Counters), cudaMemcpyDeviceToHost, st));
+  enqueue_icp(s->d_sd, s->shape, st);
+  fused_pose_finalize(s->d_sd, s->shape, 0, st);
+  gather_results_kernel<<<1, 128, 0, st>>>(s->d_sd, 1, s->d_res);
+  DYN_CUDA(cudaMemcpyAsync(s->h_res, s->d_res, sizeof(ResultBlock), cudaMemcpyDeviceToHost, st));
   DYN_CUDA(cudaStreamSynchronize(st));
   DYN_CUDA(cudaGetLastError());
   for (int k = 0; k < 16; ++k) pose_inout[k] = (float)s->h_res->pose.pose[k];
@@ -774,6 +975,7 @@ dyn_status dyn_raycast(dyn_session* s, const float pose[16], const dyn_sensor* v
   dyn_sensor vs = virt ? *virt : s->sensor;
   if (!valid_sensor(&vs) || (size_t)vs.rows * vs.cols > s->npx) return DYN_ERR_INVALID_ARG;
   DeviceGuard dg(s->device);
+  DYN_TRY(quiesce(s));
   DYN_CUDA(cudaMemcpyAsync(s->d_pose_override, pose, 64, cudaMemcpyHostToDevice, s->stream));
   size_t n = (size_t)vs.rows * vs.cols;
   launch_raycast(s->vol, dsensor(vs), s->d_pose, s->d_pose_override, s->d_ray,
@@ -789,6 +991,7 @@ dyn_status dyn_raycast(dyn_session* s, const float pose[16], const dyn_sensor* v
 dyn_status dyn_num_blocks(dyn_session* s, int64_t* n_out) {
   if (!s || !n_out) return DYN_ERR_INVALID_ARG;
   DeviceGuard dg(s->device);
+  DYN_TRY(quiesce(s));
   int n = 0;
   DYN_CUDA(cudaMemcpyAsync(&n, &s->vol.cnt->nalloc, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
   DYN_CUDA(cudaStreamSynchronize(s->stream));
@@ -817,10 +1020,33 @@ dyn_status dyn_download_blocks(dyn_session* s, int32_t* coords_out, dyn_voxel* v
       coords_out[3 * i + 2] = key_z(keys[i]);
     }
   }
-  if (voxels_out) {
+  if (voxels_out && !s->vol.fp16) {
     DYN_CUDA(cudaMemcpyAsync(voxels_out, s->vol.voxels, sizeof(dyn_voxel) * kBlockVox * m,
                              cudaMemcpyDeviceToHost, s->stream));
     DYN_CUDA(cudaStreamSynchronize(s->stream));
+  } else if (voxels_out) {
+    // mixed form: f16 sdf / u16 weight (+ colour) converted to the 8-byte
+    // voxel; weights above 255 saturate
+    const size_t nv = (size_t)kBlockVox * m;
+    std::vector<unsigned> v16(nv);
+    std::vector<uchar4> col(s->vol.colors ? nv : 0);
+    DYN_CUDA(cudaMemcpyAsync(v16.data(), s->vol.vox16, sizeof(unsigned) * nv,
+                             cudaMemcpyDeviceToHost, s->stream));
+    if (s->vol.colors)
+      DYN_CUDA(cudaMemcpyAsync(col.data(), s->vol.colors, sizeof(uchar4) * nv,
+                               cudaMemcpyDeviceToHost, s->stream));
+    DYN_CUDA(cudaStreamSynchronize(s->stream));
+    for (size_t i = 0; i < nv; ++i) {
+      __half_raw hr;
+      hr.x = (unsigned short)(v16[i] & 0xffffu);
+      dyn_voxel& o = voxels_out[i];
+      o.sdf = __half2float(__half(hr)) * s->tp.truncation_distance;  // stored as sdf / trunc
+      unsigned w = v16[i] >> 16;
+      o.weight = (uint8_t)(w > 255 ? 255 : w);
+      o.r = s->vol.colors ? col[i].x : 0;
+      o.g = s->vol.colors ? col[i].y : 0;
+      o.b = s->vol.colors ? col[i].z : 0;
+    }
   }
   return DYN_OK;
 }
@@ -829,6 +1055,7 @@ dyn_status dyn_debug_image(dyn_session* s, int32_t which, int32_t level, void* h
                            size_t bytes) {
   if (!s || !host_out || level < 0 || level >= s->nlev) return DYN_ERR_INVALID_ARG;
   DeviceGuard dg(s->device);
+  DYN_TRY(quiesce(s));
   size_t m = (size_t)s->ls[level].rows * s->ls[level].cols;
   const void* src = nullptr;
   size_t nb = 0;
@@ -872,11 +1099,10 @@ dyn_status dyn_session_profile(dyn_session* s, int32_t enable) {
   if (en && !s->ev[0])
     for (int k = 0; k < DYN_NUM_STAGES; ++k) DYN_CUDA(cudaEventCreate(&s->ev[k]));
   if (en != s->profile) {
-    for (int k = 0; k < 2; ++k)
-      if (s->exec[k]) {
-        cudaGraphExecDestroy(s->exec[k]);
-        s->exec[k] = nullptr;
-      }
+    if (s->exec) {
+      cudaGraphExecDestroy(s->exec);
+      s->exec = nullptr;
+    }
     s->profile = en;
   }
   return DYN_OK;
@@ -899,7 +1125,7 @@ size_t dyn_frame_d2h_bytes(void) { return sizeof(PoseState) + sizeof(IcpState) +
 
 dyn_status dyn_session_kernels_per_frame(dyn_session* s, int32_t* n_out) {
   if (!s || !n_out) return DYN_ERR_INVALID_ARG;
-  *n_out = std::max(s->kernels_per_frame[0], s->kernels_per_frame[1]);
+  *n_out = s->kernels_per_frame;
   return DYN_OK;
 }
 
@@ -988,6 +1214,205 @@ dyn_status dyn_sessions_submit(dyn_session* const* sessions, int32_t n,
     dyn_status r = dyn_frame_submit(sessions[i], depth_host[i], rgb_host ? rgb_host[i] : nullptr);
     if (r != DYN_OK) return r;
   }
+  return DYN_OK;
+}
+
+// ---------------------------------------------------------------- batches
+
+dyn_status dyn_batch_create(dyn_session* const* sessions, int32_t n, dyn_batch** out) {
+  if (!out) return DYN_ERR_INVALID_ARG;
+  *out = nullptr;
+  if (!sessions || n < 1 || n > 65535) return DYN_ERR_INVALID_ARG;
+  for (int i = 0; i < n; ++i) {
+    if (!sessions[i] || sessions[i]->batch || sessions[i]->device != sessions[0]->device)
+      return DYN_ERR_INVALID_ARG;
+    for (int j = 0; j < i; ++j)
+      if (sessions[j] == sessions[i]) return DYN_ERR_INVALID_ARG;
+  }
+  DeviceGuard dg(sessions[0]->device);
+  dyn_batch* b = new (std::nothrow) dyn_batch();
+  if (!b) return DYN_ERR_OOM;
+  b->device = sessions[0]->device;
+  b->n = n;
+  b->ss.assign(sessions, sessions + n);
+  int64_t cap = 0;
+  for (int i = 0; i < n; ++i) {
+    if (cudaStreamSynchronize(sessions[i]->stream) != cudaSuccess) {
+      delete b;
+      return DYN_ERR_CUDA;
+    }
+    cap += sessions[i]->tp.num_blocks;
+  }
+  if (cap > INT32_MAX) {
+    delete b;
+    return DYN_ERR_INVALID_ARG;
+  }
+  auto dalloc = [&](void** p, size_t bytes) -> dyn_status {
+    cudaError_t e = cudaMalloc(p, bytes < 256 ? 256 : bytes);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return e == cudaErrorMemoryAllocation ? DYN_ERR_OOM : DYN_ERR_CUDA;
+    }
+    b->allocs.push_back(*p);
+    return DYN_OK;
+  };
+  dyn_status r = DYN_OK;
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->h2d_done, cudaEventDisableTiming) != cudaSuccess ||
+      cudaMallocHost(&b->h_res, sizeof(ResultBlock) * (size_t)n) != cudaSuccess)
+    r = DYN_ERR_CUDA;
+  if (r == DYN_OK) r = dalloc((void**)&b->d_tab, sizeof(SessDev) * (size_t)n);
+  if (r == DYN_OK) r = dalloc((void**)&b->d_gvis, sizeof(int2) * (size_t)cap);
+  if (r == DYN_OK) r = dalloc((void**)&b->d_gcount, sizeof(int));
+  if (r == DYN_OK) r = dalloc((void**)&b->d_res, sizeof(ResultBlock) * (size_t)n);
+  if (r == DYN_OK) {
+    std::vector<SessDev> tab((size_t)n);
+    for (int i = 0; i < n; ++i) tab[i] = sessions[i]->hsd;
+    if (cudaMemcpyAsync(b->d_tab, tab.data(), sizeof(SessDev) * (size_t)n,
+                        cudaMemcpyHostToDevice, b->stream) != cudaSuccess ||
+        cudaEventRecord(b->h2d_done, b->stream) != cudaSuccess ||
+        cudaStreamSynchronize(b->stream) != cudaSuccess)
+      r = DYN_ERR_CUDA;
+  }
+  if (r != DYN_OK) {
+    cudaGetLastError();
+    release(b);
+    return r;
+  }
+  b->shape = make_shape(sessions, n, b->d_gvis, b->d_gcount, (int)cap);
+  for (int i = 0; i < n; ++i) sessions[i]->batch = b;
+  *out = b;
+  return DYN_OK;
+}
+
+dyn_status dyn_batch_destroy(dyn_batch* b) {
+  if (!b) return DYN_ERR_INVALID_ARG;
+  release(b);
+  return DYN_OK;
+}
+
+static dyn_status batch_ready(dyn_batch* b) {
+  for (dyn_session* s : b->ss)
+    if (!s) return DYN_ERR_INVALID_ARG;  // a member was destroyed
+  return DYN_OK;
+}
+
+static dyn_status batch_launch(dyn_batch* b) {
+  if (!b->exec) {
+    Marks m;
+    m.on = b->profile;
+    m.ev = b->ev;
+    m.st = b->stream;
+    dyn_status r = capture_frame(b->d_tab, b->shape, b->d_res, b->h_res, b->stream, m, &b->exec,
+                                 &b->kernels_per_frame);
+    if (r != DYN_OK) return r;
+  }
+  DYN_CUDA(cudaGraphLaunch(b->exec, b->stream));
+  b->pending = true;
+  for (dyn_session* s : b->ss) s->frames++;
+  return DYN_OK;
+}
+
+dyn_status dyn_batch_submit(dyn_batch* b, const uint16_t* const* depth_host,
+                            const uint8_t* const* rgb_host) {
+  if (!b || !depth_host) return DYN_ERR_INVALID_ARG;
+  DYN_TRY(batch_ready(b));
+  for (int i = 0; i < b->n; ++i)
+    if (!depth_host[i]) return DYN_ERR_INVALID_ARG;
+  DeviceGuard dg(b->device);
+  // the staging buffers may still feed the previous frame's copies
+  DYN_CUDA(cudaEventSynchronize(b->h2d_done));
+  for (int i = 0; i < b->n; ++i)
+    DYN_TRY(copy_frame_in(b->ss[i], depth_host[i], rgb_host ? rgb_host[i] : nullptr, b->stream));
+  DYN_CUDA(cudaEventRecord(b->h2d_done, b->stream));
+  return batch_launch(b);
+}
+
+dyn_status dyn_batch_submit_device(dyn_batch* b, const uint16_t* const* depth_dev,
+                                   const uint8_t* const* rgb_dev) {
+  if (!b || !depth_dev) return DYN_ERR_INVALID_ARG;
+  DYN_TRY(batch_ready(b));
+  for (int i = 0; i < b->n; ++i)
+    if (!depth_dev[i]) return DYN_ERR_INVALID_ARG;
+  DeviceGuard dg(b->device);
+  for (int i = 0; i < b->n; ++i) {
+    dyn_session* s = b->ss[i];
+    const uint8_t* rgb = rgb_dev ? rgb_dev[i] : nullptr;
+    DYN_CUDA(cudaMemcpyAsync(s->d_u16, depth_dev[i], s->npx * 2, cudaMemcpyDeviceToDevice,
+                             b->stream));
+    if (rgb)
+      DYN_CUDA(cudaMemcpyAsync(s->d_rgb, rgb, s->npx * 3, cudaMemcpyDeviceToDevice, b->stream));
+    DYN_TRY(set_rgb_flag(s, rgb != nullptr, b->stream));
+  }
+  return batch_launch(b);
+}
+
+dyn_status dyn_batch_result(dyn_batch* b, float* poses_out, dyn_frame_stats* stats_out,
+                            dyn_status* status_out) {
+  if (!b) return DYN_ERR_INVALID_ARG;
+  if (!b->pending) return DYN_ERR_NOT_READY;
+  DeviceGuard dg(b->device);
+  DYN_CUDA(cudaStreamSynchronize(b->stream));
+  b->pending = false;
+  if (b->profile) add_stage_times(b->ev, b->stage_ms, &b->prof_frames);
+  dyn_status first = DYN_OK;
+  for (int i = 0; i < b->n; ++i) {
+    const ResultBlock& r = b->h_res[i];
+    if (poses_out)
+      for (int k = 0; k < 16; ++k) poses_out[16 * i + k] = (float)r.pose.pose[k];
+    if (stats_out && b->ss[i]) fill_stats(b->ss[i], r, &stats_out[i]);
+    const dyn_status st = counters_status(r.cnt);
+    if (status_out) status_out[i] = st;
+    if (first == DYN_OK) first = st;
+  }
+  return first;
+}
+
+dyn_status dyn_batch_size(dyn_batch* b, int32_t* n_out) {
+  if (!b || !n_out) return DYN_ERR_INVALID_ARG;
+  *n_out = b->n;
+  return DYN_OK;
+}
+
+dyn_status dyn_batch_stream(dyn_batch* b, void** stream_out) {
+  if (!b || !stream_out) return DYN_ERR_INVALID_ARG;
+  *stream_out = (void*)b->stream;
+  return DYN_OK;
+}
+
+dyn_status dyn_batch_profile(dyn_batch* b, int32_t enable) {
+  if (!b) return DYN_ERR_INVALID_ARG;
+  DeviceGuard dg(b->device);
+  DYN_CUDA(cudaStreamSynchronize(b->stream));
+  bool en = enable != 0;
+  if (en && !b->ev[0])
+    for (int k = 0; k < DYN_NUM_STAGES; ++k) DYN_CUDA(cudaEventCreate(&b->ev[k]));
+  if (en != b->profile) {
+    if (b->exec) {
+      cudaGraphExecDestroy(b->exec);
+      b->exec = nullptr;
+    }
+    b->profile = en;
+  }
+  return DYN_OK;
+}
+
+dyn_status dyn_batch_stage_times(dyn_batch* b, double ms_out[DYN_NUM_STAGES],
+                                 int64_t* frames_out, int32_t reset) {
+  if (!b) return DYN_ERR_INVALID_ARG;
+  if (ms_out)
+    for (int k = 0; k < DYN_NUM_STAGES; ++k) ms_out[k] = b->stage_ms[k];
+  if (frames_out) *frames_out = b->prof_frames;
+  if (reset) {
+    for (int k = 0; k < DYN_NUM_STAGES; ++k) b->stage_ms[k] = 0.0;
+    b->prof_frames = 0;
+  }
+  return DYN_OK;
+}
+
+dyn_status dyn_batch_kernels_per_frame(dyn_batch* b, int32_t* n_out) {
+  if (!b || !n_out) return DYN_ERR_INVALID_ARG;
+  *n_out = b->kernels_per_frame;
   return DYN_OK;
 }
 

@@ -8,8 +8,17 @@
 // Layout in HBM (per session): a bucketed hash of 16-byte entries
 // {u64 packed block key, i32 heap index, i32 frame stamp}; a heap-index ->
 // key array; voxels as 8-byte {r,g,b,w,f32 sdf} (the reference's Voxel),
-// 512 per block in x-major order, so one block is 4 KB contiguous.
+// 512 per block in x-major order, so one block is 4 KB contiguous.  The
+// mixed form keeps {f16 sdf / truncation, u16 weight} per voxel (2 KB per
+// block) and an optional uchar4 colour array.
+//
+// Each stage is a __device__ body used by a by-value kernel (one session)
+// and by a fused kernel over every session of a frame (blockIdx.z).
 #include "tsdf.cuh"
+
+#include <cuda_fp16.h>
+
+#include "sessdev.cuh"
 
 namespace dyn {
 
@@ -116,9 +125,10 @@ __device__ inline bool dda_ray(F3 start_pt, F3 point, float trunc, float block_s
   return true;
 }
 
-__global__ void __launch_bounds__(kAllocT* kAllocT)
-    allocate_kernel(const float* __restrict__ depth, DSensor s, VolumeDev v,
-                    const PoseState* __restrict__ ps) {
+// One 16x16 pixel tile (tx, ty) of AllocateFromDepthKernel.
+__device__ inline void allocate_tile(const float* __restrict__ depth, const DSensor& s,
+                                     const VolumeDev& v, const PoseState* __restrict__ ps,
+                                     int tx, int ty) {
   __shared__ AllocSmem sm;
   __shared__ M4f T;
   __shared__ int stamp_s;
@@ -133,8 +143,8 @@ __global__ void __launch_bounds__(kAllocT* kAllocT)
   __syncthreads();
   const int stamp = stamp_s;
   const DTsdf& t = v.t;
-  const int x = blockIdx.x * kAllocT + threadIdx.x;
-  const int y = blockIdx.y * kAllocT + threadIdx.y;
+  const int x = tx * kAllocT + threadIdx.x;
+  const int y = ty * kAllocT + threadIdx.y;
   if (x < s.cols && y < s.rows) {
     const int i = y * s.cols + x;
     const float d = depth[i];
@@ -206,6 +216,14 @@ __global__ void __launch_bounds__(kAllocT* kAllocT)
   }
 }
 
+__global__ void __launch_bounds__(kAllocT* kAllocT)
+    fused_allocate_kernel(const SessDev* __restrict__ tab) {
+  const SessDev& S = tab[blockIdx.z];
+  const DSensor& s = S.ls[0];
+  if ((int)blockIdx.x * kAllocT >= s.cols || (int)blockIdx.y * kAllocT >= s.rows) return;
+  allocate_tile(S.raw, s, S.vol, S.pose, blockIdx.x, blockIdx.y);
+}
+
 // ------------------------------------------------------------ visibility
 // IntegrateScanKernel's block test (tsdf.cu:283-300): block origin to the
 // camera, z < 0 rejected, the origin plus half a block (in camera axes,
@@ -226,86 +244,139 @@ __device__ inline bool block_visible(unsigned long long key, const DTsdf& t, con
   return ix >= 0 && iy >= 0 && ix < s.cols && iy < s.rows;
 }
 
-__global__ void visible_kernel(VolumeDev v, DSensor s, const PoseState* __restrict__ ps) {
+// Every session's visible blocks appended to one batch-wide list of
+// (session, heap index), so integration balances across sessions.
+__global__ void fused_visible_kernel(const SessDev* __restrict__ tab, int2* __restrict__ gvis,
+                                     int* __restrict__ gcount) {
+  const SessDev& S = tab[blockIdx.z];
+  const VolumeDev& v = S.vol;
   __shared__ M4f invT;
-  if (threadIdx.x < 16) invT.m[threadIdx.x] = ps->invf[threadIdx.x];
+  if (threadIdx.x < 16) invT.m[threadIdx.x] = S.pose->invf[threadIdx.x];
   __syncthreads();
   int n = v.cnt->nalloc;
   if (n > v.t.num_blocks) n = v.t.num_blocks;
   const int lane = threadIdx.x & 31;
   for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
     int i = base + threadIdx.x;
-    bool vis = i < n && block_visible(v.block_keys[i], v.t, s, invT);
+    bool vis = i < n && block_visible(v.block_keys[i], v.t, S.ls[0], invT);
     unsigned m = __ballot_sync(0xffffffffu, vis);
     int off = 0;
-    if (lane == 0 && m) off = atomicAdd(&v.cnt->visible, __popc(m));
+    if (lane == 0 && m) {
+      atomicAdd(&v.cnt->visible, __popc(m));
+      off = atomicAdd(gcount, __popc(m));
+    }
     off = __shfl_sync(0xffffffffu, off, 0);
-    if (vis) v.visible[off + __popc(m & ((1u << lane) - 1))] = i;
+    if (vis) gvis[off + __popc(m & ((1u << lane) - 1))] = make_int2((int)blockIdx.z, i);
   }
 }
 
 // ------------------------------------------------------------ integration
 // IntegrateScanKernel voxel loop (tsdf.cu:301-341) + Voxel::mergeVoxel
-// (geom_Types.h:79-103), one thread per voxel of a visible block.  The
-// voxel updated is the thread's own: the reference's camera->world round
-// trip through UpdateVoxel lands on the same voxel (the oracle checks this).
-__global__ void __launch_bounds__(kBlockVox)
-    integrate_kernel(VolumeDev v, const float* __restrict__ depth,
-                     const uint8_t* __restrict__ rgb, DSensor s,
-                     const PoseState* __restrict__ ps) {
-  __shared__ M4f invT;
-  if (threadIdx.x < 16) invT.m[threadIdx.x] = ps->invf[threadIdx.x];
-  __syncthreads();
-  const int nvis = v.cnt->visible;
+// (geom_Types.h:79-103) for voxel 'lin' of block 'ptr'.  The voxel updated
+// is the thread's own: the reference's camera->world round trip through
+// UpdateVoxel lands on the same voxel (the oracle checks this).
+template <bool FP16>
+__device__ inline void integrate_voxel(const VolumeDev& v, const float* __restrict__ depth,
+                                       const uint8_t* __restrict__ rgb, const DSensor& s,
+                                       const M4f& invT, int ptr, int lin) {
   const DTsdf& t = v.t;
   const float vs = t.vs;
-  const int lin = threadIdx.x;
   const int bx = lin >> 6, by = (lin >> 3) & 7, bz = lin & 7;
-  for (int b = blockIdx.x; b < nvis; b += gridDim.x) {
-    const int ptr = v.visible[b];
-    const unsigned long long key = v.block_keys[ptr];
-    F3 position = f3((float)key_x(key) * vs * (float)kBlockSize,
-                     (float)key_y(key) * vs * (float)kBlockSize,
-                     (float)key_z(key) * vs * (float)kBlockSize);
-    F3 vp = f3(position.x + (float)bx * vs, position.y + (float)by * vs,
-               position.z + (float)bz * vs);
-    vp = xform(invT, vp);
-    int px, py;
-    if (!project(vp, s, &px, &py)) continue;
-    if (!(px >= 0 && py >= 0 && px < s.cols && py < s.rows)) continue;
-    const int idx = py * s.cols + px;
-    const float d = __ldg(depth + idx);
-    if (d < t.dmin) continue;
-    if (d > t.dmax) continue;
-    F3 p3 = point3d(idx, d, s);
-    float sd = norm3(p3);
-    float vd = norm3(vp);
-    float sdf;
-    if (vd > sd - t.trunc && vd < sd + t.trunc && d < t.dmax) sdf = sd - vd;
-    else if (vd < sd - t.trunc) sdf = t.trunc;
-    else continue;
-    uint8_t c0 = 0, c1 = 0, c2 = 0;
-    if (rgb) {
-      c0 = __ldg(rgb + 3 * (size_t)idx);
-      c1 = __ldg(rgb + 3 * (size_t)idx + 1);
-      c2 = __ldg(rgb + 3 * (size_t)idx + 2);
+  const unsigned long long key = v.block_keys[ptr];
+  F3 position = f3((float)key_x(key) * vs * (float)kBlockSize,
+                   (float)key_y(key) * vs * (float)kBlockSize,
+                   (float)key_z(key) * vs * (float)kBlockSize);
+  F3 vp = f3(position.x + (float)bx * vs, position.y + (float)by * vs,
+             position.z + (float)bz * vs);
+  vp = xform(invT, vp);
+  int px, py;
+  if (!project(vp, s, &px, &py)) return;
+  if (!(px >= 0 && py >= 0 && px < s.cols && py < s.rows)) return;
+  const int idx = py * s.cols + px;
+  const float d = __ldg(depth + idx);
+  if (d < t.dmin) return;
+  if (d > t.dmax) return;
+  F3 p3 = point3d(idx, d, s);
+  float sd = norm3(p3);
+  float vd = norm3(vp);
+  float sdf;
+  if (vd > sd - t.trunc && vd < sd + t.trunc && d < t.dmax) sdf = sd - vd;
+  else if (vd < sd - t.trunc) sdf = t.trunc;
+  else return;
+  uint8_t c0 = 0, c1 = 0, c2 = 0;
+  if (rgb) {
+    c0 = __ldg(rgb + 3 * (size_t)idx);
+    c1 = __ldg(rgb + 3 * (size_t)idx + 1);
+    c2 = __ldg(rgb + 3 * (size_t)idx + 2);
+  }
+  const size_t vi = (size_t)ptr * kBlockVox + lin;
+  if (FP16) {
+    // mixed form: the same FP32 merge, stored as f16 sdf / truncation
+    // (|value| <= 1, free space exactly 1) and a u16 weight
+    const unsigned raw = v.vox16[vi];
+    const float osdf =
+        __half2float(__ushort_as_half((unsigned short)(raw & 0xffffu))) * t.trunc;
+    const int w = (int)(raw >> 16);
+    const float fw = (float)w;
+    const float nsdf = (osdf * fw + sdf * 1.0f) / (fw + 1.0f);
+    int nw = w + 1;
+    if (nw > t.max_w) nw = t.max_w;
+    v.vox16[vi] =
+        (unsigned)__half_as_ushort(__float2half_rn(nsdf / t.trunc)) | ((unsigned)nw << 16);
+    if (v.colors) {
+      uchar4 c = v.colors[vi];
+      c.x = (uint8_t)(((float)c.x * fw + (float)c0 * 1.0f) / (fw + 1.0f));
+      c.y = (uint8_t)(((float)c.y * fw + (float)c1 * 1.0f) / (fw + 1.0f));
+      c.z = (uint8_t)(((float)c.z * fw + (float)c2 * 1.0f) / (fw + 1.0f));
+      v.colors[vi] = c;
     }
-    dyn_voxel* vox = v.voxels + (size_t)ptr * kBlockVox + lin;
-    uint2 raw = *reinterpret_cast<const uint2*>(vox);
-    uint8_t r0 = raw.x & 0xff, r1 = (raw.x >> 8) & 0xff, r2 = (raw.x >> 16) & 0xff,
-            w = raw.x >> 24;
-    float osdf = __uint_as_float(raw.y);
-    float fw = (float)w;
-    float nsdf = (osdf * fw + sdf * 1.0f) / (fw + 1.0f);
+    return;
+  }
+  dyn_voxel* vox = v.voxels + vi;
+  uint2 raw = *reinterpret_cast<const uint2*>(vox);
+  uint8_t r0 = raw.x & 0xff, r1 = (raw.x >> 8) & 0xff, r2 = (raw.x >> 16) & 0xff,
+          w = raw.x >> 24;
+  float osdf = __uint_as_float(raw.y);
+  float fw = (float)w;
+  float nsdf = (osdf * fw + sdf * 1.0f) / (fw + 1.0f);
+  // colour merge (geom_Types.h:87-91); a zero colour merged with a zero
+  // colour stays exactly zero, so depth-only frames skip the divisions
+  if (rgb || (raw.x & 0x00ffffffu)) {
     r0 = (uint8_t)(((float)r0 * fw + (float)c0 * 1.0f) / (fw + 1.0f));
     r1 = (uint8_t)(((float)r1 * fw + (float)c1 * 1.0f) / (fw + 1.0f));
     r2 = (uint8_t)(((float)r2 * fw + (float)c2 * 1.0f) / (fw + 1.0f));
-    int nw = (uint8_t)(w + 1);
-    if (nw > t.max_w) nw = t.max_w;
-    uint2 out;
-    out.x = (unsigned)r0 | ((unsigned)r1 << 8) | ((unsigned)r2 << 16) | ((unsigned)nw << 24);
-    out.y = __float_as_uint(nsdf);
-    *reinterpret_cast<uint2*>(vox) = out;
+  }
+  int nw = (uint8_t)(w + 1);
+  if (nw > t.max_w) nw = t.max_w;
+  uint2 out;
+  out.x = (unsigned)r0 | ((unsigned)r1 << 8) | ((unsigned)r2 << 16) | ((unsigned)nw << 24);
+  out.y = __float_as_uint(nsdf);
+  *reinterpret_cast<uint2*>(vox) = out;
+}
+
+// the batch-wide visible list: each item (session, block) by one CTA
+__global__ void __launch_bounds__(kBlockVox)
+    fused_integrate_kernel(const SessDev* __restrict__ tab, const int2* __restrict__ gvis,
+                           const int* __restrict__ gcount) {
+  __shared__ M4f invT;
+  __shared__ int cur_s;
+  const int n = *gcount;
+  if (threadIdx.x == 0) cur_s = -1;
+  __syncthreads();
+  for (int b = blockIdx.x; b < n; b += gridDim.x) {
+    const int2 item = gvis[b];
+    if (item.x != cur_s) {  // uniform across the CTA
+      __syncthreads();
+      if (threadIdx.x < 16) invT.m[threadIdx.x] = tab[item.x].pose->invf[threadIdx.x];
+      if (threadIdx.x == 0) cur_s = item.x;
+      __syncthreads();
+    }
+    const SessDev& S = tab[item.x];
+    const uint8_t* rgb = *S.rgb_flag ? S.rgb : nullptr;
+    if (S.vol.fp16)
+      integrate_voxel<true>(S.vol, S.raw, rgb, S.ls[0], invT, item.y, threadIdx.x);
+    else
+      integrate_voxel<false>(S.vol, S.raw, rgb, S.ls[0], invT, item.y, threadIdx.x);
   }
 }
 
@@ -338,12 +409,6 @@ __device__ inline int voxel_index(float p, float vs, float inv_vs) {
 // reference's floor division and non-negative remainder are g >> 3, g & 7.
 __device__ inline int blk_of(int g) { return g >> 3; }
 __device__ inline int loc_of(int g) { return g & 7; }
-
-__device__ inline void axis_voxel(float p, float vs, int* blk, int* loc) {
-  int g = voxel_index(p, vs, 1.0f / vs);
-  *blk = blk_of(g);
-  *loc = loc_of(g);
-}
 
 // tsdfVolume::GetVoxel, tsdf.cu:227-239, for a voxel already resolved to
 // (block, local index); a one-block lookup cache skips repeated bucket
@@ -443,62 +508,258 @@ __device__ inline VoxelSample get_interpolated(const VolumeDev& v, F3 position, 
 
 constexpr int kRayTX = 16, kRayTY = 16;
 
+// tsdfVolume raycast (tsdf.cu:471-526) of pixel (x, y) from camera pose T:
+// march from 0 by the interpolated sdf (a truncation where unobserved) until
+// the sdf drops under a voxel or the depth passes max_sensor_depth; then the
+// interpolated colour at the hit.  Returns true when the march hit the step
+// cap.
+__device__ inline bool raycast_exact_px(const VolumeDev& v, const DSensor& s, const M4f& T, int x,
+                                        int y, float* __restrict__ depth_out,
+                                        uint8_t* __restrict__ rgb_out) {
+  const int i = y * s.cols + x;
+  const DTsdf& t = v.t;
+  const float inv_vs = 1.0f / t.vs;
+  // getPoint3d (utils.h:104-112) with the pixel's (u - cx), (v - cy) hoisted
+  const float ax = (float)x - s.cx, ay = (float)y - s.cy;
+  BlockCache bc;
+  bc.x = bc.y = bc.z = 0x7fffffff;
+  bc.ptr = -1;
+  float cur = 0.0f;
+  int steps = 0;
+  bool over = false;
+  while (cur < t.dmax) {
+    if (steps++ >= t.rc_cap) {
+      over = true;
+      break;
+    }
+    F3 pc = f3(ax * cur / s.fx, ay * cur / s.fy, cur);
+    F3 point = xform(T, pc);
+    VoxelSample vx = get_interpolated<false>(v, point, inv_vs, bc);
+    if (vx.w == 0) cur += t.trunc;
+    else cur += vx.sdf;
+    if (vx.w != 0 && vx.sdf < t.vs) break;
+  }
+  depth_out[i] = cur;
+  if (rgb_out) {
+    uint8_t r = 0, g = 0, b = 0;
+    if (cur < t.dmax) {
+      F3 point = xform(T, point3d(i, cur, s));
+      VoxelSample vx = get_interpolated<true>(v, point, inv_vs, bc);
+      r = (uint8_t)vx.r;
+      g = (uint8_t)vx.g;
+      b = (uint8_t)vx.b;
+    }
+    rgb_out[3 * (size_t)i] = r;
+    rgb_out[3 * (size_t)i + 1] = g;
+    rgb_out[3 * (size_t)i + 2] = b;
+  }
+  return over;
+}
+
+// ------------------------------------------------------------ mixed-precision raycast
+// The mixed form marches the same ray with the reference's step rule
+// (tsdf.cu:471-526) and trilinear interpolation at every observed sample,
+// on f16 voxels, with voxel indices by multiplying with 1/vs (no
+// exactness check: an index off by one at a voxel boundary moves the sample
+// by under a voxel).  Skipping the interpolation where the sampled voxel is
+// far from the surface was tried and rejected: it changes the step sequence,
+// so the hit moves by up to a voxel and the tracked trajectory drifts by
+// more than a millimetre from the FP32 path.
+__device__ inline int vindex_fast(float p, float inv_vs) {
+  const float sg = (float)((p > 0.0f) - (p < 0.0f));
+  return (int)(p * inv_vs + sg * 0.5f);
+}
+__device__ inline unsigned load16(const VolumeDev& v, int ptr, int lin) {
+  return ptr < 0 ? 0u : __ldg(v.vox16 + (size_t)ptr * kBlockVox + lin);
+}
+// stored value is sdf / truncation
+__device__ inline float s16(unsigned r, float trunc) {
+  return __half2float(__ushort_as_half((unsigned short)(r & 0xffffu))) * trunc;
+}
+__device__ inline int w16(unsigned r) { return (int)(r >> 16); }
+
+template <bool COLOR>
+__device__ inline VoxelSample interp16(const VolumeDev& v, F3 position, unsigned raw0, int ptr0v,
+                                       int lin0, float inv_vs, BlockCache& bc) {
+  VoxelSample out;
+  const float vs = v.t.vs;
+  F3 pos_dual = position - f3(vs * 0.5f, vs * 0.5f, vs * 0.5f);
+  F3 vp = position * inv_vs;
+  F3 wt = f3(vp.x - floorf(vp.x), vp.y - floorf(vp.y), vp.z - floorf(vp.z));
+  int gx[2], gy[2], gz[2];
+  gx[0] = vindex_fast(pos_dual.x, inv_vs);
+  gx[1] = vindex_fast(pos_dual.x + vs, inv_vs);
+  gy[0] = vindex_fast(pos_dual.y, inv_vs);
+  gy[1] = vindex_fast(pos_dual.y + vs, inv_vs);
+  gz[0] = vindex_fast(pos_dual.z, inv_vs);
+  gz[1] = vindex_fast(pos_dual.z + vs, inv_vs);
+  const bool one_block = blk_of(gx[0]) == blk_of(gx[1]) && blk_of(gy[0]) == blk_of(gy[1]) &&
+                         blk_of(gz[0]) == blk_of(gz[1]);
+  int ptrb = 0;
+  if (one_block) ptrb = block_ptr(v, blk_of(gx[0]), blk_of(gy[0]), blk_of(gz[0]), bc);
+  const uchar4 c0 = (COLOR && v.colors && ptr0v >= 0)
+                        ? v.colors[(size_t)ptr0v * kBlockVox + lin0] : make_uchar4(0, 0, 0, 0);
+  float dist = 0.0f, cr = 0.0f, cg = 0.0f, cb = 0.0f;
+  const float s0 = s16(raw0, v.t.trunc);
+  const int off[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1},
+                         {1, 1, 0}, {0, 1, 1}, {1, 0, 1}, {1, 1, 1}};
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const int ox = off[k][0], oy = off[k][1], oz = off[k][2];
+    const int ptr = one_block ? ptrb
+                              : block_ptr(v, blk_of(gx[ox]), blk_of(gy[oy]), blk_of(gz[oz]), bc);
+    const int lin = lin_of(gx[ox], gy[oy], gz[oz]);
+    const unsigned r = load16(v, ptr, lin);
+    const bool use0 = w16(r) == 0;
+    const float a = ox ? wt.x : 1.0f - wt.x;
+    const float b = oy ? wt.y : 1.0f - wt.y;
+    const float c = oz ? wt.z : 1.0f - wt.z;
+    const float coef = a * b * c;
+    dist += coef * (use0 ? s0 : s16(r, v.t.trunc));
+    if (COLOR && v.colors) {
+      const uchar4 cc = use0 ? c0 : (ptr >= 0 ? v.colors[(size_t)ptr * kBlockVox + lin]
+                                              : make_uchar4(0, 0, 0, 0));
+      cr += (float)cc.x * coef;
+      cg += (float)cc.y * coef;
+      cb += (float)cc.z * coef;
+    }
+  }
+  out.sdf = dist;
+  out.w = w16(raw0);
+  out.r = cr;
+  out.g = cg;
+  out.b = cb;
+  return out;
+}
+
+__device__ inline bool raycast_mixed_px(const VolumeDev& v, const DSensor& s, const M4f& T, int x,
+                                        int y, float* __restrict__ depth_out,
+                                        uint8_t* __restrict__ rgb_out) {
+  const int i = y * s.cols + x;
+  const DTsdf& t = v.t;
+  const float inv_vs = 1.0f / t.vs;
+  const float axf = ((float)x - s.cx) / s.fx, ayf = ((float)y - s.cy) / s.fy;
+  BlockCache bc;
+  bc.x = bc.y = bc.z = 0x7fffffff;
+  bc.ptr = -1;
+  float cur = 0.0f;
+  int steps = 0;
+  bool over = false;
+  int ptr = -1, lin = 0;
+  unsigned raw = 0;
+  F3 point;
+  while (cur < t.dmax) {
+    if (steps++ >= t.rc_cap) {
+      over = true;
+      break;
+    }
+    point = xform(T, f3(axf * cur, ayf * cur, cur));
+    const int gx = vindex_fast(point.x, inv_vs), gy = vindex_fast(point.y, inv_vs),
+              gz = vindex_fast(point.z, inv_vs);
+    ptr = block_ptr(v, blk_of(gx), blk_of(gy), blk_of(gz), bc);
+    lin = lin_of(gx, gy, gz);
+    raw = load16(v, ptr, lin);
+    if (w16(raw) == 0) {
+      cur += t.trunc;
+      continue;
+    }
+    VoxelSample vx = interp16<false>(v, point, raw, ptr, lin, inv_vs, bc);
+    cur += vx.sdf;
+    if (vx.sdf < t.vs) break;
+  }
+  depth_out[i] = cur;
+  if (rgb_out) {
+    uint8_t r = 0, g = 0, b = 0;
+    if (cur < t.dmax) {
+      point = xform(T, f3(axf * cur, ayf * cur, cur));
+      const int gx = vindex_fast(point.x, inv_vs), gy = vindex_fast(point.y, inv_vs),
+                gz = vindex_fast(point.z, inv_vs);
+      ptr = block_ptr(v, blk_of(gx), blk_of(gy), blk_of(gz), bc);
+      lin = lin_of(gx, gy, gz);
+      raw = load16(v, ptr, lin);
+      if (w16(raw) != 0) {
+        VoxelSample vx = interp16<true>(v, point, raw, ptr, lin, inv_vs, bc);
+        r = (uint8_t)vx.r;
+        g = (uint8_t)vx.g;
+        b = (uint8_t)vx.b;
+      } else if (v.colors && ptr >= 0) {
+        uchar4 c = v.colors[(size_t)ptr * kBlockVox + lin];
+        r = c.x;
+        g = c.y;
+        b = c.z;
+      }
+    }
+    rgb_out[3 * (size_t)i] = r;
+    rgb_out[3 * (size_t)i + 1] = g;
+    rgb_out[3 * (size_t)i + 2] = b;
+  }
+  return over;
+}
+
+// One 16x16 pixel tile (tile bx, by) from pose16 (a float 4x4); warps cover
+// 8x4 pixel sub-tiles for coherent rays.  Step-cap overruns are counted.
+template <bool MIXED>
+__device__ inline void raycast_tile(const VolumeDev& v, const DSensor& s,
+                                    const float* __restrict__ pose16, float* __restrict__ depth_out,
+                                    uint8_t* __restrict__ rgb_out, int bx, int by) {
+  __shared__ M4f Ts;
+  __shared__ int over;
+  const int tid = threadIdx.y * kRayTX + threadIdx.x;
+  if (tid < 16) Ts.m[tid] = pose16[tid];
+  if (tid == 0) over = 0;
+  __syncthreads();
+  const M4f T = Ts;  // the pose in registers for the whole march
+  const int warp = tid >> 5, lane = tid & 31;
+  const int lx = (warp & 1) * 8 + (lane & 7);
+  const int ly = (warp >> 1) * 4 + (lane >> 3);
+  const int x = bx * kRayTX + lx, y = by * kRayTY + ly;
+  if (x < s.cols && y < s.rows) {
+    const bool o = MIXED ? raycast_mixed_px(v, s, T, x, y, depth_out, rgb_out)
+                         : raycast_exact_px(v, s, T, x, y, depth_out, rgb_out);
+    if (o) atomicAdd(&over, 1);
+  }
+  __syncthreads();
+  if (tid == 0 && over) atomicAdd(&v.cnt->raycast_overruns, over);
+}
+
+template <bool MIXED>
 __global__ void __launch_bounds__(kRayTX* kRayTY)
     raycast_kernel(VolumeDev v, DSensor s, const PoseState* __restrict__ ps,
                    const float* __restrict__ pose_override, float* __restrict__ depth_out,
                    uint8_t* __restrict__ rgb_out) {
-  __shared__ M4f Ts;
-  __shared__ int over;
-  const int tid = threadIdx.y * kRayTX + threadIdx.x;
-  if (tid < 16) Ts.m[tid] = pose_override ? pose_override[tid] : ps->posef[tid];
-  if (tid == 0) over = 0;
-  __syncthreads();
-  const M4f T = Ts;  // the pose in registers for the whole march
-  // warps cover 8x4 pixel sub-tiles for coherent rays
-  const int warp = tid >> 5, lane = tid & 31;
-  const int lx = (warp & 1) * 8 + (lane & 7);
-  const int ly = (warp >> 1) * 4 + (lane >> 3);
-  const int x = blockIdx.x * kRayTX + lx, y = blockIdx.y * kRayTY + ly;
-  if (x < s.cols && y < s.rows) {
-    const int i = y * s.cols + x;
-    const DTsdf& t = v.t;
-    const float inv_vs = 1.0f / t.vs;
-    // getPoint3d (utils.h:104-112) with the pixel's (u - cx), (v - cy) hoisted
-    const float ax = (float)x - s.cx, ay = (float)y - s.cy;
-    BlockCache bc;
-    bc.x = bc.y = bc.z = 0x7fffffff;
-    bc.ptr = -1;
-    float cur = 0.0f;
-    int steps = 0;
-    while (cur < t.dmax) {
-      if (steps++ >= t.rc_cap) {
-        atomicAdd(&over, 1);
-        break;
-      }
-      F3 pc = f3(ax * cur / s.fx, ay * cur / s.fy, cur);
-      F3 point = xform(T, pc);
-      VoxelSample vx = get_interpolated<false>(v, point, inv_vs, bc);
-      if (vx.w == 0) cur += t.trunc;
-      else cur += vx.sdf;
-      if (vx.w != 0 && vx.sdf < t.vs) break;
-    }
-    depth_out[i] = cur;
-    if (rgb_out) {
-      uint8_t r = 0, g = 0, b = 0;
-      if (cur < t.dmax) {
-        F3 point = xform(T, point3d(i, cur, s));
-        VoxelSample vx = get_interpolated<true>(v, point, inv_vs, bc);
-        r = (uint8_t)vx.r;
-        g = (uint8_t)vx.g;
-        b = (uint8_t)vx.b;
-      }
-      rgb_out[3 * (size_t)i] = r;
-      rgb_out[3 * (size_t)i + 1] = g;
-      rgb_out[3 * (size_t)i + 2] = b;
-    }
-  }
-  __syncthreads();
-  if (tid == 0 && over) atomicAdd(&v.cnt->raycast_overruns, over);
+  raycast_tile<MIXED>(v, s, pose_override ? pose_override : ps->posef, depth_out, rgb_out,
+                      blockIdx.x, blockIdx.y);
+}
+
+// next frame's target of every mode-1 session (blockIdx.z) at its new pose
+__global__ void __launch_bounds__(kRayTX* kRayTY)
+    fused_raycast_kernel(const SessDev* __restrict__ tab) {
+  const SessDev& S = tab[blockIdx.z];
+  if (S.mode != 1) return;
+  const DSensor& s = S.ls[0];
+  if ((int)blockIdx.x * kRayTX >= s.cols || (int)blockIdx.y * kRayTY >= s.rows) return;
+  uint8_t* rgb_out = S.use_color ? S.trgb : nullptr;
+  if (S.vol.fp16)
+    raycast_tile<true>(S.vol, s, S.pose->posef, S.ray, rgb_out, blockIdx.x, blockIdx.y);
+  else
+    raycast_tile<false>(S.vol, s, S.pose->posef, S.ray, rgb_out, blockIdx.x, blockIdx.y);
+}
+
+// per-frame counters of every session (all but nalloc, the heap top) and
+// the batch visible list
+__global__ void fused_reset_counters_kernel(const SessDev* __restrict__ tab, int n,
+                                            int* __restrict__ gcount) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) *gcount = 0;
+  if (i >= n) return;
+  Counters* c = tab[i].vol.cnt;
+  c->new_blocks = 0;
+  c->bucket_full = 0;
+  c->heap_exhausted = 0;
+  c->dda_overruns = 0;
+  c->raycast_overruns = 0;
+  c->visible = 0;
+  c->unique_probed = 0;
 }
 
 __global__ void clear_entries_kernel(Entry* e, size_t n) {
@@ -527,37 +788,55 @@ inline int nblk(long long n, int t) { return (int)((n + t - 1) / t); }
 void launch_volume_clear(const VolumeDev& v, cudaStream_t st) {
   size_t ne = (size_t)v.t.num_buckets * v.t.bucket_size;
   clear_entries_kernel<<<nblk((long long)ne, 256), 256, 0, st>>>(v.entries, ne);
-  cudaMemsetAsync(v.voxels, 0, sizeof(dyn_voxel) * (size_t)v.t.num_blocks * kBlockVox, st);
+  const size_t nv = (size_t)v.t.num_blocks * kBlockVox;
+  if (v.voxels) cudaMemsetAsync(v.voxels, 0, sizeof(dyn_voxel) * nv, st);
+  if (v.vox16) cudaMemsetAsync(v.vox16, 0, sizeof(unsigned) * nv, st);
+  if (v.colors) cudaMemsetAsync(v.colors, 0, sizeof(uchar4) * nv, st);
   cudaMemsetAsync(v.cnt, 0, sizeof(Counters), st);
-}
-
-void launch_allocate(const VolumeDev& v, const float* depth, const DSensor& s,
-                     const PoseState* ps, cudaStream_t st) {
-  dim3 grid(nblk(s.cols, kAllocT), nblk(s.rows, kAllocT));
-  allocate_kernel<<<grid, dim3(kAllocT, kAllocT), 0, st>>>(depth, s, v, ps);
-}
-
-void launch_visible(const VolumeDev& v, const DSensor& s, const PoseState* ps, cudaStream_t st) {
-  int g = nblk(v.t.num_blocks, 256);
-  if (g > 148 * 16) g = 148 * 16;
-  visible_kernel<<<g, 256, 0, st>>>(v, s, ps);
-}
-
-void launch_integrate(const VolumeDev& v, const float* depth, const uint8_t* rgb, const DSensor& s,
-                      const PoseState* ps, cudaStream_t st) {
-  integrate_kernel<<<148 * 4, kBlockVox, 0, st>>>(v, depth, rgb, s, ps);
 }
 
 void launch_raycast(const VolumeDev& v, const DSensor& s, const PoseState* ps,
                     const float* pose_override, float* depth_out, uint8_t* rgb_out,
                     cudaStream_t st) {
   dim3 grid(nblk(s.cols, kRayTX), nblk(s.rows, kRayTY));
-  raycast_kernel<<<grid, dim3(kRayTX, kRayTY), 0, st>>>(v, s, ps, pose_override, depth_out,
-                                                        rgb_out);
+  if (v.fp16)
+    raycast_kernel<true><<<grid, dim3(kRayTX, kRayTY), 0, st>>>(v, s, ps, pose_override,
+                                                                depth_out, rgb_out);
+  else
+    raycast_kernel<false><<<grid, dim3(kRayTX, kRayTY), 0, st>>>(v, s, ps, pose_override,
+                                                                 depth_out, rgb_out);
 }
 
 void launch_block_coords(const VolumeDev& v, int n, int* coords, cudaStream_t st) {
   if (n > 0) block_coords_kernel<<<nblk(n, 256), 256, 0, st>>>(v, n, coords);
+}
+
+// ---- fused stages
+void fused_reset_counters(const SessDev* tab, const BatchShape& b, cudaStream_t st) {
+  fused_reset_counters_kernel<<<nblk(b.n, 128), 128, 0, st>>>(tab, b.n, b.gcount);
+}
+
+void fused_allocate(const SessDev* tab, const BatchShape& b, cudaStream_t st) {
+  dim3 grid(nblk(b.max_cols, kAllocT), nblk(b.max_rows, kAllocT), b.n);
+  fused_allocate_kernel<<<grid, dim3(kAllocT, kAllocT), 0, st>>>(tab);
+}
+
+void fused_visible(const SessDev* tab, const BatchShape& b, cudaStream_t st) {
+  // grid-stride over each session's heap; about 600 CTAs in all
+  int cap = 592 / b.n;
+  if (cap < 8) cap = 8;
+  int g = nblk(b.max_blocks, 256);
+  if (g > cap) g = cap;
+  fused_visible_kernel<<<dim3(g, 1, b.n), 256, 0, st>>>(tab, b.gvis, b.gcount);
+}
+
+void fused_integrate(const SessDev* tab, const BatchShape& b, cudaStream_t st) {
+  fused_integrate_kernel<<<148 * 8, kBlockVox, 0, st>>>(tab, b.gvis, b.gcount);
+}
+
+void fused_raycast(const SessDev* tab, const BatchShape& b, cudaStream_t st) {
+  dim3 grid(nblk(b.max_cols, kRayTX), nblk(b.max_rows, kRayTY), b.n);
+  fused_raycast_kernel<<<grid, dim3(kRayTX, kRayTY), 0, st>>>(tab);
 }
 
 }  // namespace dyn

@@ -1,4 +1,7 @@
 // tsdf.cuh -- voxel-hashed TSDF: allocation, visibility, integration, raycast.
+// The per-frame stages run as fused launches over a table of sessions
+// (sessdev.cuh); the raycast also has a one-session form for
+// tsdfVolume::GenerateDepth / GenerateRgb.
 #pragma once
 #include "common.cuh"
 #include "icp.cuh"
@@ -8,23 +11,15 @@ namespace dyn {
 struct VolumeDev {
   Entry* entries;                 // num_buckets * bucket_size
   unsigned long long* block_keys; // key of each heap index
-  dyn_voxel* voxels;              // num_blocks * 512, x-major per block
-  int* visible;                   // heap indices of this frame's visible blocks
+  dyn_voxel* voxels;              // FP32 form: num_blocks * 512, x-major per block
+  unsigned* vox16;                // mixed form: {f16 sdf | u16 weight << 16} per voxel
+  uchar4* colors;                 // mixed form: r,g,b per voxel (null: no colour kept)
+  int fp16;                       // 1: mixed-precision voxels (vox16 [+ colors])
   Counters* cnt;
   DTsdf t;
 };
 
 void launch_volume_clear(const VolumeDev& v, cudaStream_t st);
-// AllocateFromDepthKernel (tsdf.cu:346-453) for 'depth' seen from the
-// session pose; blocks touched are stamped with the pose's frame number.
-void launch_allocate(const VolumeDev& v, const float* depth, const DSensor& s,
-                     const PoseState* ps, cudaStream_t st);
-// Frustum test of every allocated block (tsdf.cu:283-300), compacted.
-void launch_visible(const VolumeDev& v, const DSensor& s, const PoseState* ps,
-                    cudaStream_t st);
-// IntegrateScanKernel body (tsdf.cu:301-341) for the visible blocks.
-void launch_integrate(const VolumeDev& v, const float* depth, const uint8_t* rgb,
-                      const DSensor& s, const PoseState* ps, cudaStream_t st);
 // GenerateDepthKernel / GenerateRgbKernel (tsdf.cu:471-526).  pose_override
 // (device float[16]) replaces the session pose when non-null.
 void launch_raycast(const VolumeDev& v, const DSensor& s, const PoseState* ps,

@@ -7,6 +7,12 @@ include/builder/builder.h:49-117), over the C ABI.
         for depth in frames:
             pose, stats = m.process(depth)        # buildModelLS
         coords, voxels = m.download_blocks()
+
+Batch steps a fixed set of sessions together (one launch per stage for all
+of them, one CUDA graph per frame):
+
+    with Batch([m0, m1, m2]) as b:
+        poses, stats, status = b.process([d0, d1, d2])
 """
 from __future__ import annotations
 
@@ -126,3 +132,83 @@ class Session:
         abi.check("dyn_debug_image",
                   self.lib.dyn_debug_image(self.h, which, level, _ptr(out), out.nbytes))
         return out
+
+
+class Batch:
+    """dyn_batch over existing sessions (which stay owned by the caller)."""
+
+    def __init__(self, sessions):
+        self.lib = abi.load()
+        self.sessions = list(sessions)
+        self.n = len(self.sessions)
+        arr = (_vp * self.n)(*[s.h for s in self.sessions])
+        self.h = _vp()
+        abi.check("dyn_batch_create", self.lib.dyn_batch_create(arr, self.n, C.byref(self.h)))
+
+    def close(self) -> None:
+        if self.h:
+            self.lib.dyn_batch_destroy(self.h)
+            self.h = _vp()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, depths, rgbs=None) -> None:
+        d = [np.ascontiguousarray(x, np.uint16) for x in depths]
+        r = None if rgbs is None else [
+            None if x is None else np.ascontiguousarray(x, np.uint8) for x in rgbs]
+        self._keep = (d, r)
+        dp = (_vp * self.n)(*[x.ctypes.data for x in d])
+        rp = None if r is None else (_vp * self.n)(*[None if x is None else x.ctypes.data
+                                                    for x in r])
+        abi.check("dyn_batch_submit", self.lib.dyn_batch_submit(self.h, dp, rp))
+
+    def submit_device(self, depth_ptrs, rgb_ptrs=None) -> None:
+        dp = (_vp * self.n)(*depth_ptrs)
+        rp = None if rgb_ptrs is None else (_vp * self.n)(*rgb_ptrs)
+        abi.check("dyn_batch_submit_device", self.lib.dyn_batch_submit_device(self.h, dp, rp))
+
+    def result(self, strict: bool = True):
+        """(poses (n,4,4) float32, [FrameStats], [status])."""
+        poses = (C.c_float * (16 * self.n))()
+        stats = (abi.FrameStats * self.n)()
+        status = (C.c_int * self.n)()
+        r = self.lib.dyn_batch_result(self.h, poses, stats, status)
+        if strict or r not in (abi.DYN_ERR_HASH_FULL, abi.DYN_ERR_HEAP_EXHAUSTED):
+            abi.check("dyn_batch_result", r)
+        return (np.array(poses, np.float32).reshape(self.n, 4, 4), list(stats),
+                list(status))
+
+    def process(self, depths, rgbs=None, strict: bool = True):
+        self.submit(depths, rgbs)
+        return self.result(strict)
+
+    def stream(self) -> int:
+        p = _vp()
+        abi.check("dyn_batch_stream", self.lib.dyn_batch_stream(self.h, C.byref(p)))
+        return p.value or 0
+
+    def profile(self, enable: bool) -> None:
+        abi.check("dyn_batch_profile", self.lib.dyn_batch_profile(self.h, int(enable)))
+
+    def stage_times(self, reset: bool = True):
+        ms = (C.c_double * len(abi.STAGES))()
+        n = C.c_int64()
+        abi.check("dyn_batch_stage_times",
+                  self.lib.dyn_batch_stage_times(self.h, ms, C.byref(n), int(reset)))
+        return list(ms), n.value
+
+    def kernels_per_frame(self) -> int:
+        n = C.c_int32()
+        abi.check("dyn_batch_kernels_per_frame",
+                  self.lib.dyn_batch_kernels_per_frame(self.h, C.byref(n)))
+        return n.value

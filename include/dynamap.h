@@ -341,13 +341,50 @@ dyn_status dyn_icp_normal_equations_noalloc(
     const dyn_sensor* level, const dyn_gn_params* gn, const float T[16],
     double out_host[29], void* stream);
 
-/* ---- batched multi-session stepping ------------------------------------
- * Process one frame for each of n sessions with as few launches as the
- * sessions' shapes allow.  Frames are given as host pointers (copied
- * before return).  Results are read with dyn_frame_result per session. */
+/* ---- multi-session stepping ---------------------------------------------
+ * No counterpart in the reference (its builder drives one stream).
+ *
+ * dyn_sessions_submit: one frame for each of n sessions, each replayed as
+ * that session's own frame graph on its own stream (the streams overlap on
+ * the device).  Frames are host pointers, copied before return; results are
+ * read with dyn_frame_result per session. */
 dyn_status dyn_sessions_submit(dyn_session* const* sessions, int32_t n,
                                const uint16_t* const* depth_host,
                                const uint8_t* const* rgb_host /* nullable */);
+
+/* dyn_batch: a fixed set of sessions on one device stepped together.  Each
+ * stage of a frame is ONE kernel launch over all members (a member uses
+ * only its own part of the grid, so its results are bit-identical to
+ * stepping it alone) and the whole frame is one CUDA graph on the batch's
+ * stream, followed by one device->host copy of every member's results.
+ * Members may differ in sensor size, volume, parameters and precision.
+ * While a session belongs to a batch its frames go only through the batch
+ * (dyn_frame_submit, dyn_frame_submit_device, dyn_integrate_with_pose and
+ * dyn_solver_solve return DYN_ERR_INVALID_ARG); its other calls (pose,
+ * raycast, download, images) first wait for the batch's work in flight.
+ * Destroying a member makes the batch refuse further frames. */
+typedef struct dyn_batch dyn_batch;
+dyn_status dyn_batch_create(dyn_session* const* sessions, int32_t n, dyn_batch** out);
+dyn_status dyn_batch_destroy(dyn_batch* b);
+/* One frame per member: depth_host[i] (rows_i x cols_i u16), rgb_host
+ * nullable, or rgb_host[i] nullable per member.  Host buffers may be
+ * reused when the call returns. */
+dyn_status dyn_batch_submit(dyn_batch* b, const uint16_t* const* depth_host,
+                            const uint8_t* const* rgb_host);
+/* The same with device buffers (read on the batch's stream). */
+dyn_status dyn_batch_submit_device(dyn_batch* b, const uint16_t* const* depth_dev,
+                                   const uint8_t* const* rgb_dev);
+/* Waits for the frame; poses_out n x 16 floats, stats_out n entries and
+ * status_out n entries are each nullable.  Returns the first member error
+ * (DYN_ERR_HEAP_EXHAUSTED / DYN_ERR_HASH_FULL) or DYN_OK. */
+dyn_status dyn_batch_result(dyn_batch* b, float* poses_out, dyn_frame_stats* stats_out,
+                            dyn_status* status_out);
+dyn_status dyn_batch_size(dyn_batch* b, int32_t* n_out);
+dyn_status dyn_batch_stream(dyn_batch* b, void** stream_out);
+dyn_status dyn_batch_profile(dyn_batch* b, int32_t enable);
+dyn_status dyn_batch_stage_times(dyn_batch* b, double ms_out[DYN_NUM_STAGES],
+                                 int64_t* frames_out, int32_t reset);
+dyn_status dyn_batch_kernels_per_frame(dyn_batch* b, int32_t* n_out);
 
 #ifdef __cplusplus
 }  /* extern "C" */
