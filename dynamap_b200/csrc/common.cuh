@@ -32,6 +32,7 @@ struct DTsdf {
   float trunc;
   float dmin, dmax;  // min/maxSensorDepth
   int num_buckets;
+  int nb_mask;       // num_buckets - 1 when a power of two, else -1
   int bucket_size;
   int num_blocks;
   int max_w;
@@ -130,6 +131,15 @@ __host__ __device__ inline int hash_slot(int x, int y, int z, int nb, int bsz) {
   return r * bsz;
 }
 
+// The same slot: for a power-of-two bucket count the non-negative
+// remainder is the low bits of the two's-complement hash.
+__device__ inline int hash_slot(int x, int y, int z, const DTsdf& t) {
+  if (t.nb_mask < 0) return hash_slot(x, y, z, t.num_buckets, t.bucket_size);
+  int h = (int)(((unsigned)x * 73856093u) ^ ((unsigned)y * 19349669u) ^
+                ((unsigned)z * 83492791u));
+  return (h & t.nb_mask) * t.bucket_size;
+}
+
 __host__ __device__ inline unsigned long long pack_key(int x, int y, int z) {
   const unsigned long long m = (1ull << 21) - 1;
   return (((unsigned long long)x & m) << 42) | (((unsigned long long)y & m) << 21) |
@@ -149,7 +159,7 @@ __host__ __device__ inline int key_z(unsigned long long k) {
 // of the block or -1.
 __device__ inline int find_block(const Entry* __restrict__ entries, const DTsdf& t,
                                  int x, int y, int z) {
-  int b = hash_slot(x, y, z, t.num_buckets, t.bucket_size);
+  int b = hash_slot(x, y, z, t);
   unsigned long long k = pack_key(x, y, z);
   for (int i = 0; i < t.bucket_size; ++i) {
     int4 e = __ldg(reinterpret_cast<const int4*>(entries + b + i));

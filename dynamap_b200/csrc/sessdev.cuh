@@ -67,6 +67,7 @@ struct BatchShape {
   int max_slot_iters[3];   // largest lvl_iteration_num of each slot
   int max_bil_radius;      // 0: no session filters
   int kahan_mask;          // bit 0: some session sums plainly, bit 1: some use Kahan sums
+  int fp16_mask;           // bit 0: some session keeps FP32 voxels, bit 1: some mixed
   int2* gvis;              // batch-wide visible list (session, heap index)
   int* gcount;             // its length (device)
   int gvis_cap;

@@ -83,6 +83,7 @@ DTsdf dtsdf(const dyn_tsdf_params& p) {
   t.dmin = p.min_sensor_depth;
   t.dmax = p.max_sensor_depth;
   t.num_buckets = p.num_buckets;
+  t.nb_mask = (p.num_buckets & (p.num_buckets - 1)) == 0 ? p.num_buckets - 1 : -1;
   t.bucket_size = p.bucket_size;
   t.num_blocks = p.num_blocks;
   t.max_w = p.max_sdf_weight;
@@ -441,6 +442,7 @@ BatchShape make_shape(dyn_session* const* ss, int n, int2* gvis, int* gcount, in
     }
     if (s->bp.enabled) b.max_bil_radius = std::max(b.max_bil_radius, s->btab.radius);
     b.kahan_mask |= s->icp_params().kahan ? 2 : 1;
+    b.fp16_mask |= s->vol.fp16 ? 2 : 1;
   }
   return b;
 }

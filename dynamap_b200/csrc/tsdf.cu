@@ -50,7 +50,7 @@ struct AllocSmem {
 // if the key was present, -2 if the bucket is full.
 __device__ inline int bucket_insert(Entry* entries, const DTsdf& t, unsigned long long key,
                                     int stamp, int* unique) {
-  int b = hash_slot(key_x(key), key_y(key), key_z(key), t.num_buckets, t.bucket_size);
+  int b = hash_slot(key_x(key), key_y(key), key_z(key), t);
   for (int i = 0; i < t.bucket_size; ++i) {
     Entry* e = entries + b + i;
     unsigned long long cur = *(volatile unsigned long long*)&e->key;
@@ -731,18 +731,17 @@ __global__ void __launch_bounds__(kRayTX* kRayTY)
                       blockIdx.x, blockIdx.y);
 }
 
-// next frame's target of every mode-1 session (blockIdx.z) at its new pose
+// next frame's target of every mode-1 session (blockIdx.z) at its new pose;
+// one instantiation per voxel form, sessions of the other form return
+template <bool MIXED>
 __global__ void __launch_bounds__(kRayTX* kRayTY)
     fused_raycast_kernel(const SessDev* __restrict__ tab) {
   const SessDev& S = tab[blockIdx.z];
-  if (S.mode != 1) return;
+  if (S.mode != 1 || (S.vol.fp16 != 0) != MIXED) return;
   const DSensor& s = S.ls[0];
   if ((int)blockIdx.x * kRayTX >= s.cols || (int)blockIdx.y * kRayTY >= s.rows) return;
   uint8_t* rgb_out = S.use_color ? S.trgb : nullptr;
-  if (S.vol.fp16)
-    raycast_tile<true>(S.vol, s, S.pose->posef, S.ray, rgb_out, blockIdx.x, blockIdx.y);
-  else
-    raycast_tile<false>(S.vol, s, S.pose->posef, S.ray, rgb_out, blockIdx.x, blockIdx.y);
+  raycast_tile<MIXED>(S.vol, s, S.pose->posef, S.ray, rgb_out, blockIdx.x, blockIdx.y);
 }
 
 // per-frame counters of every session (all but nalloc, the heap top) and
@@ -836,7 +835,8 @@ void fused_integrate(const SessDev* tab, const BatchShape& b, cudaStream_t st) {
 
 void fused_raycast(const SessDev* tab, const BatchShape& b, cudaStream_t st) {
   dim3 grid(nblk(b.max_cols, kRayTX), nblk(b.max_rows, kRayTY), b.n);
-  fused_raycast_kernel<<<grid, dim3(kRayTX, kRayTY), 0, st>>>(tab);
+  if (b.fp16_mask & 1) fused_raycast_kernel<false><<<grid, dim3(kRayTX, kRayTY), 0, st>>>(tab);
+  if (b.fp16_mask & 2) fused_raycast_kernel<true><<<grid, dim3(kRayTX, kRayTY), 0, st>>>(tab);
 }
 
 }  // namespace dyn
