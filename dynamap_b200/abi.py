@@ -16,8 +16,11 @@ STATUS = {0: "ok", 1: "invalid argument", 2: "out of device memory",
           3: "memory budget exceeded", 4: "hash bucket full",
           5: "voxel block heap exhausted", 6: "icp diverged", 7: "timeout",
           8: "cuda error", 9: "not ready", 10: "no cuda device"}
+DYN_ERR_BUDGET_EXCEEDED = 3
 DYN_ERR_HASH_FULL = 4
 DYN_ERR_HEAP_EXHAUSTED = 5
+DYN_ERR_NOT_READY = 9
+DYN_ERR_NO_DEVICE = 10
 STAGES = ["ingest", "bilateral", "source_maps", "icp", "allocate", "visible", "integrate",
           "raycast", "target_maps", "frame"]
 PRECISION_FP32 = 0
@@ -81,6 +84,17 @@ class FrameStats(C.Structure):
         return out
 
 
+class ServerParams(C.Structure):
+    _fields_ = [("budget_bytes", C.c_size_t), ("max_sessions", C.c_int32),
+                ("device", C.c_int32)]
+
+
+class ServerUsage(C.Structure):
+    _fields_ = [("budget_bytes", C.c_size_t), ("used_bytes", C.c_size_t),
+                ("capacity", C.c_int32), ("sessions", C.c_int32), ("steps", C.c_int64),
+                ("frames", C.c_int64)]
+
+
 P = C.POINTER
 _vp = C.c_void_p
 
@@ -130,6 +144,18 @@ SIGNATURES = {
     "dyn_batch_profile": (C.c_int, [_vp, C.c_int32]),
     "dyn_batch_stage_times": (C.c_int, [_vp, P(C.c_double), P(C.c_int64), C.c_int32]),
     "dyn_batch_kernels_per_frame": (C.c_int, [_vp, P(C.c_int32)]),
+    "dyn_server_create": (C.c_int, [P(ServerParams), P(_vp)]),
+    "dyn_server_destroy": (C.c_int, [_vp]),
+    "dyn_server_admit": (C.c_int, [_vp, P(TsdfParams), P(GnParams), P(BilateralParams),
+                                   P(Sensor), C.c_int32, P(C.c_float), P(C.c_int32)]),
+    "dyn_server_release": (C.c_int, [_vp, C.c_int32]),
+    "dyn_server_push": (C.c_int, [_vp, C.c_int32, _vp, _vp]),
+    "dyn_server_step": (C.c_int, [_vp, P(C.c_int32)]),
+    "dyn_server_poll": (C.c_int, [_vp, C.c_int32, P(C.c_int32)]),
+    "dyn_server_result": (C.c_int, [_vp, C.c_int32, P(C.c_float), P(FrameStats)]),
+    "dyn_server_sync": (C.c_int, [_vp]),
+    "dyn_server_session": (C.c_int, [_vp, C.c_int32, P(_vp)]),
+    "dyn_server_info": (C.c_int, [_vp, P(ServerUsage)]),
 }
 
 _lib = None

@@ -1,0 +1,524 @@
+// serving.cu -- many sessions on one device: dyn_batch (a fixed set stepped
+// together, one CUDA graph per frame) and dyn_server (sessions admitted and
+// released at any time under an HBM budget, every step fusing the frames
+// that are waiting into one launch per stage).  No counterpart in the
+// reference, whose builder drives one stream.
+#include <cstdio>
+#include <mutex>
+#include <new>
+
+#include "session_impl.cuh"
+
+using namespace dyn;
+using namespace dyn::host;
+
+extern "C" {
+
+// ---------------------------------------------------------------- batches
+
+dyn_status dyn_batch_create(dyn_session* const* sessions, int32_t n, dyn_batch** out) {
+  if (!out) return DYN_ERR_INVALID_ARG;
+  *out = nullptr;
+  if (!sessions || n < 1 || n > 65535) return DYN_ERR_INVALID_ARG;
+  for (int i = 0; i < n; ++i) {
+    if (!sessions[i] || sessions[i]->batch || sessions[i]->device != sessions[0]->device)
+      return DYN_ERR_INVALID_ARG;
+    for (int j = 0; j < i; ++j)
+      if (sessions[j] == sessions[i]) return DYN_ERR_INVALID_ARG;
+  }
+  DeviceGuard dg(sessions[0]->device);
+  dyn_batch* b = new (std::nothrow) dyn_batch();
+  if (!b) return DYN_ERR_OOM;
+  b->device = sessions[0]->device;
+  b->n = n;
+  b->ss.assign(sessions, sessions + n);
+  int64_t cap = 0;
+  for (int i = 0; i < n; ++i) {
+    if (cudaStreamSynchronize(sessions[i]->stream) != cudaSuccess) {
+      delete b;
+      return DYN_ERR_CUDA;
+    }
+    cap += sessions[i]->tp.num_blocks;
+  }
+  if (cap > INT32_MAX) {
+    delete b;
+    return DYN_ERR_INVALID_ARG;
+  }
+  auto dalloc = [&](void** p, size_t bytes) -> dyn_status {
+    cudaError_t e = cudaMalloc(p, bytes < 256 ? 256 : bytes);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return e == cudaErrorMemoryAllocation ? DYN_ERR_OOM : DYN_ERR_CUDA;
+    }
+    b->allocs.push_back(*p);
+    return DYN_OK;
+  };
+  dyn_status r = DYN_OK;
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->h2d_done, cudaEventDisableTiming) != cudaSuccess ||
+      cudaMallocHost(&b->h_res, sizeof(ResultBlock) * (size_t)n) != cudaSuccess)
+    r = DYN_ERR_CUDA;
+  if (r == DYN_OK) r = dalloc((void**)&b->d_tab, sizeof(SessDev) * (size_t)n);
+  if (r == DYN_OK) r = dalloc((void**)&b->d_gvis, sizeof(int2) * (size_t)cap);
+  if (r == DYN_OK) r = dalloc((void**)&b->d_gcount, sizeof(int));
+  if (r == DYN_OK) r = dalloc((void**)&b->d_res, sizeof(ResultBlock) * (size_t)n);
+  if (r == DYN_OK) {
+    std::vector<SessDev> tab((size_t)n);
+    for (int i = 0; i < n; ++i) tab[i] = sessions[i]->hsd;
+    if (cudaMemcpyAsync(b->d_tab, tab.data(), sizeof(SessDev) * (size_t)n,
+                        cudaMemcpyHostToDevice, b->stream) != cudaSuccess ||
+        cudaEventRecord(b->h2d_done, b->stream) != cudaSuccess ||
+        cudaStreamSynchronize(b->stream) != cudaSuccess)
+      r = DYN_ERR_CUDA;
+  }
+  if (r != DYN_OK) {
+    cudaGetLastError();
+    release(b);
+    return r;
+  }
+  b->shape = make_shape(sessions, n, b->d_gvis, b->d_gcount, (int)cap);
+  for (int i = 0; i < n; ++i) sessions[i]->batch = b;
+  *out = b;
+  return DYN_OK;
+}
+
+dyn_status dyn_batch_destroy(dyn_batch* b) {
+  if (!b) return DYN_ERR_INVALID_ARG;
+  release(b);
+  return DYN_OK;
+}
+
+static dyn_status batch_ready(dyn_batch* b) {
+  for (dyn_session* s : b->ss)
+    if (!s) return DYN_ERR_INVALID_ARG;  // a member was destroyed
+  return DYN_OK;
+}
+
+static dyn_status batch_launch(dyn_batch* b) {
+  if (!b->exec) {
+    Marks m;
+    m.on = b->profile;
+    m.ev = b->ev;
+    m.st = b->stream;
+    dyn_status r = capture_frame(b->d_tab, b->shape, b->d_res, b->h_res, b->stream, m, &b->exec,
+                                 &b->kernels_per_frame);
+    if (r != DYN_OK) return r;
+  }
+  DYN_CUDA(cudaGraphLaunch(b->exec, b->stream));
+  b->pending = true;
+  for (dyn_session* s : b->ss) s->frames++;
+  return DYN_OK;
+}
+
+dyn_status dyn_batch_submit(dyn_batch* b, const uint16_t* const* depth_host,
+                            const uint8_t* const* rgb_host) {
+  if (!b || !depth_host) return DYN_ERR_INVALID_ARG;
+  DYN_TRY(batch_ready(b));
+  for (int i = 0; i < b->n; ++i)
+    if (!depth_host[i]) return DYN_ERR_INVALID_ARG;
+  DeviceGuard dg(b->device);
+  // the staging buffers may still feed the previous frame's copies
+  DYN_CUDA(cudaEventSynchronize(b->h2d_done));
+  for (int i = 0; i < b->n; ++i)
+    DYN_TRY(copy_frame_in(b->ss[i], depth_host[i], rgb_host ? rgb_host[i] : nullptr, b->stream));
+  DYN_CUDA(cudaEventRecord(b->h2d_done, b->stream));
+  return batch_launch(b);
+}
+
+dyn_status dyn_batch_submit_device(dyn_batch* b, const uint16_t* const* depth_dev,
+                                   const uint8_t* const* rgb_dev) {
+  if (!b || !depth_dev) return DYN_ERR_INVALID_ARG;
+  DYN_TRY(batch_ready(b));
+  for (int i = 0; i < b->n; ++i)
+    if (!depth_dev[i]) return DYN_ERR_INVALID_ARG;
+  DeviceGuard dg(b->device);
+  for (int i = 0; i < b->n; ++i) {
+    dyn_session* s = b->ss[i];
+    const uint8_t* rgb = rgb_dev ? rgb_dev[i] : nullptr;
+    DYN_CUDA(cudaMemcpyAsync(s->d_u16, depth_dev[i], s->npx * 2, cudaMemcpyDeviceToDevice,
+                             b->stream));
+    if (rgb)
+      DYN_CUDA(cudaMemcpyAsync(s->d_rgb, rgb, s->npx * 3, cudaMemcpyDeviceToDevice, b->stream));
+    DYN_TRY(set_rgb_flag(s, rgb != nullptr, b->stream));
+  }
+  return batch_launch(b);
+}
+
+dyn_status dyn_batch_result(dyn_batch* b, float* poses_out, dyn_frame_stats* stats_out,
+                            dyn_status* status_out) {
+  if (!b) return DYN_ERR_INVALID_ARG;
+  if (!b->pending) return DYN_ERR_NOT_READY;
+  DeviceGuard dg(b->device);
+  DYN_CUDA(cudaStreamSynchronize(b->stream));
+  b->pending = false;
+  if (b->profile) add_stage_times(b->ev, b->stage_ms, &b->prof_frames);
+  dyn_status first = DYN_OK;
+  for (int i = 0; i < b->n; ++i) {
+    const ResultBlock& r = b->h_res[i];
+    if (poses_out)
+      for (int k = 0; k < 16; ++k) poses_out[16 * i + k] = (float)r.pose.pose[k];
+    if (stats_out && b->ss[i]) fill_stats(b->ss[i], r, &stats_out[i]);
+    const dyn_status st = counters_status(r.cnt);
+    if (status_out) status_out[i] = st;
+    if (first == DYN_OK) first = st;
+  }
+  return first;
+}
+
+dyn_status dyn_batch_size(dyn_batch* b, int32_t* n_out) {
+  if (!b || !n_out) return DYN_ERR_INVALID_ARG;
+  *n_out = b->n;
+  return DYN_OK;
+}
+
+dyn_status dyn_batch_stream(dyn_batch* b, void** stream_out) {
+  if (!b || !stream_out) return DYN_ERR_INVALID_ARG;
+  *stream_out = (void*)b->stream;
+  return DYN_OK;
+}
+
+dyn_status dyn_batch_profile(dyn_batch* b, int32_t enable) {
+  if (!b) return DYN_ERR_INVALID_ARG;
+  DeviceGuard dg(b->device);
+  DYN_CUDA(cudaStreamSynchronize(b->stream));
+  bool en = enable != 0;
+  if (en && !b->ev[0])
+    for (int k = 0; k < DYN_NUM_STAGES; ++k) DYN_CUDA(cudaEventCreate(&b->ev[k]));
+  if (en != b->profile) {
+    if (b->exec) {
+      cudaGraphExecDestroy(b->exec);
+      b->exec = nullptr;
+    }
+    b->profile = en;
+  }
+  return DYN_OK;
+}
+
+dyn_status dyn_batch_stage_times(dyn_batch* b, double ms_out[DYN_NUM_STAGES],
+                                 int64_t* frames_out, int32_t reset) {
+  if (!b) return DYN_ERR_INVALID_ARG;
+  if (ms_out)
+    for (int k = 0; k < DYN_NUM_STAGES; ++k) ms_out[k] = b->stage_ms[k];
+  if (frames_out) *frames_out = b->prof_frames;
+  if (reset) {
+    for (int k = 0; k < DYN_NUM_STAGES; ++k) b->stage_ms[k] = 0.0;
+    b->prof_frames = 0;
+  }
+  return DYN_OK;
+}
+
+dyn_status dyn_batch_kernels_per_frame(dyn_batch* b, int32_t* n_out) {
+  if (!b || !n_out) return DYN_ERR_INVALID_ARG;
+  *n_out = b->kernels_per_frame;
+  return DYN_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- serving
+
+namespace {
+
+struct ServerSlot {
+  dyn_session* s = nullptr;
+  size_t bytes = 0;
+  bool queued = false;       // a frame is in the session's staging buffers
+  bool queued_rgb = false;
+  int64_t last_step = -1;    // id of the last step that processed the slot
+  int last_ring = 0;
+};
+
+// One step's device table: descriptors and slot indices of its sessions,
+// with pinned host copies (kept until the step has completed).
+struct StepBuf {
+  SessDev* d_tab = nullptr;
+  int* d_map = nullptr;
+  SessDev* h_tab = nullptr;
+  int* h_map = nullptr;
+  cudaEvent_t done = nullptr;
+  bool used = false;
+};
+
+constexpr int kServerRing = 4;
+
+}  // namespace
+
+struct dyn_server {
+  int device = 0;
+  size_t budget = 0, used = 0;
+  int capacity = 0;
+  std::vector<ServerSlot> slots;
+  cudaStream_t stream = nullptr;
+  StepBuf ring[kServerRing];
+  int ring_pos = 0;
+  int64_t steps = 0;
+  int64_t frames = 0;
+  int2* d_gvis = nullptr;
+  int* d_gcount = nullptr;
+  int64_t gvis_cap = 0;
+  ResultBlock* d_res = nullptr;
+  ResultBlock* h_res = nullptr;  // pinned, one entry per slot
+  std::vector<dyn_session*> act;
+};
+
+namespace {
+
+void release(dyn_server* sv) {
+  if (!sv) return;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(sv->device);
+  if (sv->stream) cudaStreamSynchronize(sv->stream);
+  for (ServerSlot& sl : sv->slots)
+    if (sl.s) {
+      sl.s->owner_stream = nullptr;
+      dyn_session_destroy(sl.s);
+    }
+  for (StepBuf& r : sv->ring) {
+    cudaFree(r.d_tab);
+    cudaFree(r.d_map);
+    if (r.h_tab) cudaFreeHost(r.h_tab);
+    if (r.h_map) cudaFreeHost(r.h_map);
+    if (r.done) cudaEventDestroy(r.done);
+  }
+  cudaFree(sv->d_gvis);
+  cudaFree(sv->d_gcount);
+  cudaFree(sv->d_res);
+  if (sv->h_res) cudaFreeHost(sv->h_res);
+  if (sv->stream) cudaStreamDestroy(sv->stream);
+  cudaSetDevice(prev);
+  delete sv;
+}
+
+dyn_status check_slot(dyn_server* sv, int32_t slot) {
+  if (!sv || slot < 0 || slot >= sv->capacity || !sv->slots[slot].s) return DYN_ERR_INVALID_ARG;
+  return DYN_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+dyn_status dyn_server_create(const dyn_server_params* p, dyn_server** out) {
+  if (!out || !p) return DYN_ERR_INVALID_ARG;
+  *out = nullptr;
+  const int cap = p->max_sessions > 0 ? p->max_sessions : 256;
+  if (cap > 65535) return DYN_ERR_INVALID_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return DYN_ERR_NO_DEVICE;
+  }
+  if (p->device < 0 || p->device >= ndev) return DYN_ERR_INVALID_ARG;
+  DeviceGuard dg(p->device);
+  dyn_server* sv = new (std::nothrow) dyn_server();
+  if (!sv) return DYN_ERR_OOM;
+  sv->device = p->device;
+  sv->capacity = cap;
+  sv->slots.resize((size_t)cap);
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+    delete sv;
+    return DYN_ERR_CUDA;
+  }
+  sv->budget = p->budget_bytes ? p->budget_bytes : free_b / 10 * 9;
+  bool ok = cudaStreamCreateWithFlags(&sv->stream, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaMalloc(&sv->d_gcount, 256) == cudaSuccess &&
+            cudaMalloc(&sv->d_res, sizeof(ResultBlock) * (size_t)cap) == cudaSuccess &&
+            cudaMallocHost(&sv->h_res, sizeof(ResultBlock) * (size_t)cap) == cudaSuccess;
+  for (StepBuf& r : sv->ring)
+    ok = ok && cudaMalloc(&r.d_tab, sizeof(SessDev) * (size_t)cap) == cudaSuccess &&
+         cudaMalloc(&r.d_map, sizeof(int) * (size_t)cap) == cudaSuccess &&
+         cudaMallocHost(&r.h_tab, sizeof(SessDev) * (size_t)cap) == cudaSuccess &&
+         cudaMallocHost(&r.h_map, sizeof(int) * (size_t)cap) == cudaSuccess &&
+         cudaEventCreateWithFlags(&r.done, cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) {
+    cudaGetLastError();
+    release(sv);
+    return DYN_ERR_OOM;
+  }
+  std::memset(sv->h_res, 0, sizeof(ResultBlock) * (size_t)cap);
+  *out = sv;
+  return DYN_OK;
+}
+
+dyn_status dyn_server_destroy(dyn_server* sv) {
+  if (!sv) return DYN_ERR_INVALID_ARG;
+  release(sv);
+  return DYN_OK;
+}
+
+dyn_status dyn_server_admit(dyn_server* sv, const dyn_tsdf_params* tsdf, const dyn_gn_params* gn,
+                            const dyn_bilateral_params* bil, const dyn_sensor* sensor,
+                            int32_t precision, const float pose0[16], int32_t* slot_out) {
+  if (!sv || !slot_out || !tsdf || !gn || !sensor) return DYN_ERR_INVALID_ARG;
+  *slot_out = -1;
+  int slot = -1;
+  for (int i = 0; i < sv->capacity && slot < 0; ++i)
+    if (!sv->slots[i].s) slot = i;
+  if (slot < 0) return DYN_ERR_BUDGET_EXCEEDED;
+  const size_t bytes = session_bytes(*tsdf, *sensor, precision,
+                                     precision == DYN_PRECISION_MIXED ? mixed_colour(gn) : true);
+  if (sv->used + bytes > sv->budget) return DYN_ERR_BUDGET_EXCEEDED;
+  dyn_session* s = nullptr;
+  dyn_status r = dyn_session_create(tsdf, gn, bil, sensor, precision, sv->device, &s);
+  if (r != DYN_OK) return r;
+  if (pose0 && (r = dyn_session_set_pose(s, pose0)) != DYN_OK) {
+    dyn_session_destroy(s);
+    return r;
+  }
+  s->owner_stream = sv->stream;
+  ServerSlot& sl = sv->slots[slot];
+  sl = ServerSlot();
+  sl.s = s;
+  sl.bytes = bytes;
+  sv->used += bytes;
+  *slot_out = slot;
+  return DYN_OK;
+}
+
+dyn_status dyn_server_release(dyn_server* sv, int32_t slot) {
+  DYN_TRY(check_slot(sv, slot));
+  DeviceGuard dg(sv->device);
+  DYN_CUDA(cudaStreamSynchronize(sv->stream));  // the session may be in a step in flight
+  ServerSlot& sl = sv->slots[slot];
+  sl.s->owner_stream = nullptr;
+  dyn_session_destroy(sl.s);
+  sv->used -= sl.bytes;
+  sl = ServerSlot();
+  return DYN_OK;
+}
+
+dyn_status dyn_server_push(dyn_server* sv, int32_t slot, const uint16_t* depth_host,
+                           const uint8_t* rgb_host) {
+  DYN_TRY(check_slot(sv, slot));
+  if (!depth_host) return DYN_ERR_INVALID_ARG;
+  ServerSlot& sl = sv->slots[slot];
+  if (sl.queued) return DYN_ERR_NOT_READY;  // the previous frame has not been stepped
+  dyn_session* s = sl.s;
+  DeviceGuard dg(sv->device);
+  // the staging buffers may still feed the copies of the slot's last step
+  DYN_CUDA(cudaEventSynchronize(s->h2d_done));
+  std::memcpy(s->h_depth, depth_host, s->npx * sizeof(uint16_t));
+  if (rgb_host) std::memcpy(s->h_rgb, rgb_host, s->npx * 3);
+  sl.queued = true;
+  sl.queued_rgb = rgb_host != nullptr;
+  return DYN_OK;
+}
+
+dyn_status dyn_server_step(dyn_server* sv, int32_t* n_out) {
+  if (!sv) return DYN_ERR_INVALID_ARG;
+  if (n_out) *n_out = 0;
+  DeviceGuard dg(sv->device);
+  StepBuf& rb = sv->ring[sv->ring_pos];
+  if (rb.used) DYN_CUDA(cudaEventSynchronize(rb.done));  // its table may still be read
+  sv->act.clear();
+  int64_t cap = 0;
+  for (int i = 0; i < sv->capacity; ++i) {
+    ServerSlot& sl = sv->slots[i];
+    if (!sl.s || !sl.queued) continue;
+    rb.h_tab[sv->act.size()] = sl.s->hsd;
+    rb.h_map[sv->act.size()] = i;
+    sv->act.push_back(sl.s);
+    cap += sl.s->tp.num_blocks;
+  }
+  const int n = (int)sv->act.size();
+  if (n == 0) return DYN_OK;
+  if (cap > sv->gvis_cap) {  // grow the batch visible list
+    DYN_CUDA(cudaStreamSynchronize(sv->stream));
+    cudaFree(sv->d_gvis);
+    sv->d_gvis = nullptr;
+    sv->gvis_cap = 0;
+    DYN_CUDA(cudaMalloc(&sv->d_gvis, sizeof(int2) * (size_t)cap));
+    sv->gvis_cap = cap;
+  }
+  cudaStream_t st = sv->stream;
+  DYN_CUDA(cudaMemcpyAsync(rb.d_tab, rb.h_tab, sizeof(SessDev) * (size_t)n,
+                           cudaMemcpyHostToDevice, st));
+  DYN_CUDA(cudaMemcpyAsync(rb.d_map, rb.h_map, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice,
+                           st));
+  for (int i = 0; i < n; ++i) {
+    dyn_session* s = sv->act[i];
+    ServerSlot& sl = sv->slots[rb.h_map[i]];
+    DYN_CUDA(cudaMemcpyAsync(s->d_u16, s->h_depth, s->npx * 2, cudaMemcpyHostToDevice, st));
+    if (sl.queued_rgb)
+      DYN_CUDA(cudaMemcpyAsync(s->d_rgb, s->h_rgb, s->npx * 3, cudaMemcpyHostToDevice, st));
+    DYN_TRY(set_rgb_flag(s, sl.queued_rgb, st));
+    DYN_CUDA(cudaEventRecord(s->h2d_done, st));
+  }
+  const BatchShape b = make_shape(sv->act.data(), n, sv->d_gvis, sv->d_gcount, (int)cap);
+  enqueue_frame(rb.d_tab, b, rb.d_map, sv->d_res, sv->h_res, sv->capacity, st, Marks());
+  DYN_CUDA(cudaGetLastError());
+  DYN_CUDA(cudaEventRecord(rb.done, st));
+  rb.used = true;
+  for (int i = 0; i < n; ++i) {
+    ServerSlot& sl = sv->slots[rb.h_map[i]];
+    sl.queued = false;
+    sl.last_step = sv->steps;
+    sl.last_ring = sv->ring_pos;
+    sl.s->frames++;
+  }
+  sv->ring_pos = (sv->ring_pos + 1) % kServerRing;
+  sv->steps++;
+  sv->frames += n;
+  if (n_out) *n_out = n;
+  return DYN_OK;
+}
+
+dyn_status dyn_server_poll(dyn_server* sv, int32_t slot, int32_t* ready_out) {
+  DYN_TRY(check_slot(sv, slot));
+  if (!ready_out) return DYN_ERR_INVALID_ARG;
+  const ServerSlot& sl = sv->slots[slot];
+  *ready_out = 0;
+  if (sl.last_step < 0) return DYN_OK;
+  DeviceGuard dg(sv->device);
+  cudaError_t e = cudaEventQuery(sv->ring[sl.last_ring].done);
+  if (e == cudaSuccess) *ready_out = 1;
+  else if (e != cudaErrorNotReady) return DYN_ERR_CUDA;
+  else cudaGetLastError();
+  return DYN_OK;
+}
+
+dyn_status dyn_server_result(dyn_server* sv, int32_t slot, float pose_out[16],
+                             dyn_frame_stats* stats) {
+  DYN_TRY(check_slot(sv, slot));
+  const ServerSlot& sl = sv->slots[slot];
+  if (sl.last_step < 0) return DYN_ERR_NOT_READY;
+  DeviceGuard dg(sv->device);
+  // a later step reusing the ring entry completes after this slot's step
+  DYN_CUDA(cudaEventSynchronize(sv->ring[sl.last_ring].done));
+  const ResultBlock& r = sv->h_res[slot];
+  if (pose_out)
+    for (int k = 0; k < 16; ++k) pose_out[k] = (float)r.pose.pose[k];
+  if (stats) fill_stats(sl.s, r, stats);
+  return counters_status(r.cnt);
+}
+
+dyn_status dyn_server_sync(dyn_server* sv) {
+  if (!sv) return DYN_ERR_INVALID_ARG;
+  DeviceGuard dg(sv->device);
+  DYN_CUDA(cudaStreamSynchronize(sv->stream));
+  return DYN_OK;
+}
+
+dyn_status dyn_server_session(dyn_server* sv, int32_t slot, dyn_session** out) {
+  DYN_TRY(check_slot(sv, slot));
+  if (!out) return DYN_ERR_INVALID_ARG;
+  *out = sv->slots[slot].s;
+  return DYN_OK;
+}
+
+dyn_status dyn_server_info(dyn_server* sv, dyn_server_usage* out) {
+  if (!sv || !out) return DYN_ERR_INVALID_ARG;
+  std::memset(out, 0, sizeof(*out));
+  out->budget_bytes = sv->budget;
+  out->used_bytes = sv->used;
+  out->capacity = sv->capacity;
+  for (const ServerSlot& sl : sv->slots)
+    if (sl.s) out->sessions++;
+  out->steps = sv->steps;
+  out->frames = sv->frames;
+  return DYN_OK;
+}
+
+}  // extern "C"

@@ -15,223 +15,17 @@
 // (SessDev): a session alone runs a table of one, a dyn_batch runs the
 // table of its members, one launch per stage for all of them and the whole
 // frame as one graph.
-#include <cuda_fp16.h>
-#include <cuda_runtime.h>
-
-#include <algorithm>
-#include <cmath>
 #include <cstdio>
-#include <cstring>
-#include <cstdint>
 #include <mutex>
 #include <new>
-#include <vector>
 
-#include "common.cuh"
-#include "icp.cuh"
-#include "image.cuh"
-#include "sessdev.cuh"
-#include "tsdf.cuh"
+#include "session_impl.cuh"
 
 using namespace dyn;
+using namespace dyn::host;
 
-namespace {
-
-struct ResultBlock {
-  PoseState pose;
-  IcpState icp;
-  Counters cnt;
-};
-static_assert(sizeof(PoseState) % 4 == 0 && sizeof(IcpState) % 4 == 0 &&
-                  sizeof(Counters) % 4 == 0,
-              "result parts are copied as 32-bit words");
-
-int level_of_scale(int scale) {
-  int l = 0;
-  while ((1 << l) < scale && l < kLevels - 1) ++l;
-  return l;
-}
-
-DSensor dsensor(const dyn_sensor& s) {
-  DSensor d;
-  d.rows = (int)s.rows;
-  d.cols = (int)s.cols;
-  d.fx = s.fx;
-  d.fy = s.fy;
-  d.cx = s.cx;
-  d.cy = s.cy;
-  return d;
-}
-
-// Level sensor for scale 2^l: f/s, (c+0.5)/s-0.5, dims floor(dim/s).
-dyn_sensor level_sensor(const dyn_sensor& s, int scale) {
-  dyn_sensor o = s;
-  o.rows = s.rows / (uint32_t)scale;
-  o.cols = s.cols / (uint32_t)scale;
-  o.fx = s.fx / (float)scale;
-  o.fy = s.fy / (float)scale;
-  o.cx = (s.cx + 0.5f) / (float)scale - 0.5f;
-  o.cy = (s.cy + 0.5f) / (float)scale - 0.5f;
-  return o;
-}
-
-DTsdf dtsdf(const dyn_tsdf_params& p) {
-  DTsdf t;
-  t.vs = p.voxel_size;
-  t.bsm = (float)p.block_size * p.voxel_size;  // tsdf.cu:437-438
-  t.trunc = p.truncation_distance;
-  t.dmin = p.min_sensor_depth;
-  t.dmax = p.max_sensor_depth;
-  t.num_buckets = p.num_buckets;
-  t.nb_mask = (p.num_buckets & (p.num_buckets - 1)) == 0 ? p.num_buckets - 1 : -1;
-  t.bucket_size = p.bucket_size;
-  t.num_blocks = p.num_blocks;
-  t.max_w = p.max_sdf_weight;
-  double bs = (double)p.block_size * (double)p.voxel_size;
-  t.dda_cap = 3 * (int)std::ceil(((double)p.max_sensor_depth + (double)p.truncation_distance) / bs) + 8;
-  double step = std::min((double)p.voxel_size, (double)p.truncation_distance);
-  t.rc_cap = (int)std::ceil((double)p.max_sensor_depth / step) + 4;
-  return t;
-}
-
-#define DYN_CUDA(x)                                  \
-  do {                                               \
-    cudaError_t e_ = (x);                            \
-    if (e_ != cudaSuccess) {                         \
-      if (e_ == cudaErrorMemoryAllocation) return DYN_ERR_OOM; \
-      return DYN_ERR_CUDA;                           \
-    }                                                \
-  } while (0)
-
-#define DYN_TRY(x)                 \
-  do {                             \
-    dyn_status r_ = (x);           \
-    if (r_ != DYN_OK) return r_;   \
-  } while (0)
-
-bool valid_sensor(const dyn_sensor* s) {
-  return s && s->rows > 0 && s->cols > 0 && s->rows <= 8192 && s->cols <= 8192 &&
-         s->fx > 0 && s->fy > 0 && s->depth_scaler > 0;
-}
-
-}  // namespace
-
-struct dyn_session {
-  int device = 0;
-  dyn_tsdf_params tp;
-  dyn_gn_params gp;
-  dyn_bilateral_params bp;
-  dyn_sensor sensor;
-  int precision = 0;
-  cudaStream_t stream = nullptr;
-  cudaEvent_t h2d_done = nullptr;
-  DSensor ls[kLevels];
-  int nlev = 1;
-  size_t npx = 0;
-  // device buffers
-  std::vector<void*> allocs;
-  uint16_t* d_u16 = nullptr;
-  uint8_t* d_rgb = nullptr;
-  float* d_raw = nullptr;
-  float* d_filt = nullptr;
-  float* d_sdep[kLevels] = {};
-  float4* d_snrm[kLevels] = {};
-  float4* d_svtx[kLevels] = {};
-  float* d_sint[kLevels] = {};
-  float* d_tdep[kLevels] = {};
-  float4* d_tnrm[kLevels] = {};
-  float4* d_tvtx[kLevels] = {};
-  float* d_tint[kLevels] = {};
-  float* d_ray = nullptr;
-  uint8_t* d_trgb = nullptr;
-  float* d_pose_override = nullptr;
-  double* d_pose_in = nullptr;
-  double* d_partials = nullptr;
-  IcpState* d_icp = nullptr;
-  PoseState* d_pose = nullptr;
-  VolumeDev vol;
-  // fused-launch descriptor (host copy and its device table of one)
-  SessDev hsd;
-  SessDev* d_sd = nullptr;
-  BilateralTable* d_btab = nullptr;
-  int* d_rgb_flag = nullptr;   // nonzero: the current frame carries RGB
-  int rgb_flag_host = -1;      // last value written (-1: unknown)
-  int2* d_gvis = nullptr;      // visible list of the table of one
-  int* d_gcount = nullptr;
-  ResultBlock* d_res = nullptr;
-  BatchShape shape;
-  dyn_batch* batch = nullptr;  // member of this batch (frames go through it)
-  // host
-  uint16_t* h_depth = nullptr;
-  uint8_t* h_rgb = nullptr;
-  ResultBlock* h_res = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  BilateralTable btab;
-  // profiling: ev[i] ends stage i (DYN_STAGE_*), ev[DYN_STAGE_FRAME] starts the frame
-  bool profile = false;
-  cudaEvent_t ev[DYN_NUM_STAGES] = {};
-  double stage_ms[DYN_NUM_STAGES] = {};
-  int64_t prof_frames = 0;
-  int kernels_per_frame = 0;
-  bool debug_maps = false;
-  int frames = 0;
-  bool pending = false;
-
-  template <class T>
-  dyn_status dalloc(T** p, size_t bytes) {
-    void* q = nullptr;
-    bytes = (bytes + 255) / 256 * 256;  // whole 16-byte vectors at the tail
-    cudaError_t e = cudaMalloc(&q, bytes < 256 ? 256 : bytes);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      return e == cudaErrorMemoryAllocation ? DYN_ERR_OOM : DYN_ERR_CUDA;
-    }
-    allocs.push_back(q);
-    *p = (T*)q;
-    return DYN_OK;
-  }
-  bool use_color() const { return gp.color_weight != 0.0f; }
-  IcpParams icp_params() const {
-    IcpParams P;
-    P.dmin = gp.icp_min_depth;
-    P.dmax = gp.icp_max_depth;
-    P.cos_thr = gp.normal_cos_thresh;
-    P.cw = gp.color_weight;
-    P.min_inc = gp.min_increment;
-    P.max_inc = gp.max_increment;
-    P.reg = gp.regularization;
-    P.compose_left = gp.compose_left;
-    P.kahan = precision == DYN_PRECISION_MIXED ? 1 : 0;
-    return P;
-  }
-};
-
-// A fixed set of sessions on one device whose frames run together: each
-// stage is one launch over the members' descriptor table and the whole frame
-// one CUDA graph on the batch's stream.
-struct dyn_batch {
-  int device = 0;
-  int n = 0;
-  std::vector<dyn_session*> ss;
-  cudaStream_t stream = nullptr;
-  cudaEvent_t h2d_done = nullptr;
-  std::vector<void*> allocs;
-  SessDev* d_tab = nullptr;
-  int2* d_gvis = nullptr;
-  int* d_gcount = nullptr;
-  ResultBlock* d_res = nullptr;
-  ResultBlock* h_res = nullptr;  // pinned, n entries
-  BatchShape shape;
-  cudaGraphExec_t exec = nullptr;
-  int kernels_per_frame = 0;
-  bool profile = false;
-  cudaEvent_t ev[DYN_NUM_STAGES] = {};
-  double stage_ms[DYN_NUM_STAGES] = {};
-  int64_t prof_frames = 0;
-  bool pending = false;
-};
-
-namespace {
+namespace dyn {
+namespace host {
 
 void release(dyn_batch* b) {
   if (!b) return;
@@ -276,19 +70,6 @@ void release(dyn_session* s) {
   delete s;
 }
 
-struct DeviceGuard {
-  int prev = -1;
-  explicit DeviceGuard(int dev) {
-    cudaGetDevice(&prev);
-    if (prev != dev) cudaSetDevice(dev);
-  }
-  ~DeviceGuard() {
-    int cur = -1;
-    cudaGetDevice(&cur);
-    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
-  }
-};
-
 MapsArgs maps_args(dyn_session* s, bool target) {
   MapsArgs a;
   int off = 0;
@@ -305,18 +86,6 @@ MapsArgs maps_args(dyn_session* s, bool target) {
   return a;
 }
 
-// Stage boundary events (profiling only; captured into the frame graph):
-// ev[i] ends stage i, ev[DYN_STAGE_FRAME] starts the frame.
-struct Marks {
-  bool on = false;
-  cudaEvent_t* ev = nullptr;
-  cudaStream_t st = nullptr;
-  void operator()(int stage) const {
-    // External: during capture this becomes an event-record node of the graph
-    if (on) cudaEventRecordWithFlags(ev[stage], st, cudaEventRecordExternal);
-  }
-};
-
 __global__ void mark_target_kernel(IcpState* st) {
   if (threadIdx.x == 0 && blockIdx.x == 0) st->have_target = 1;
 }
@@ -329,15 +98,17 @@ __device__ inline void copy_words(void* dst, const void* src, int bytes) {
     static_cast<unsigned*>(dst)[k] = static_cast<const unsigned*>(src)[k];
 }
 // pose, solver state and counters of every session into one array, read
-// back by one copy
+// back by one copy (entry slot_map[i] when a map is given)
 __global__ void gather_results_kernel(const SessDev* __restrict__ tab, int n,
+                                      const int* __restrict__ slot_map,
                                       ResultBlock* __restrict__ out) {
   const int i = blockIdx.x;
   if (i >= n) return;
   const SessDev& S = tab[i];
-  copy_words(&out[i].pose, S.pose, (int)sizeof(PoseState));
-  copy_words(&out[i].icp, S.icp, (int)sizeof(IcpState));
-  copy_words(&out[i].cnt, S.vol.cnt, (int)sizeof(Counters));
+  ResultBlock& o = out[slot_map ? slot_map[i] : i];
+  copy_words(&o.pose, S.pose, (int)sizeof(PoseState));
+  copy_words(&o.icp, S.icp, (int)sizeof(IcpState));
+  copy_words(&o.cnt, S.vol.cnt, (int)sizeof(Counters));
 }
 
 // Source side of a frame: ingest, bilateral filter, pyramid, normal maps.
@@ -378,16 +149,17 @@ void enqueue_map_update(const SessDev* tab, const BatchShape& b, cudaStream_t st
 // builder::buildModelLS with the intended order: track frame k against the
 // target of frame k-1, integrate frame k at the new pose, raycast the target
 // for frame k+1; then the results into 'res_host' (pinned).
-void enqueue_frame(const SessDev* tab, const BatchShape& b, ResultBlock* res_dev,
-                   ResultBlock* res_host, cudaStream_t st, const Marks& m) {
+void enqueue_frame(const SessDev* tab, const BatchShape& b, const int* slot_map,
+                   ResultBlock* res_dev, ResultBlock* res_host, int n_results, cudaStream_t st,
+                   const Marks& m) {
   enqueue_source(tab, b, st, m);
   enqueue_icp(tab, b, st);
   fused_pose_finalize(tab, b, 1, st);
   m(DYN_STAGE_ICP);
   enqueue_map_update(tab, b, st, m);
-  gather_results_kernel<<<b.n, 128, 0, st>>>(tab, b.n, res_dev);
-  cudaMemcpyAsync(res_host, res_dev, sizeof(ResultBlock) * (size_t)b.n, cudaMemcpyDeviceToHost,
-                  st);
+  gather_results_kernel<<<b.n, 128, 0, st>>>(tab, b.n, slot_map, res_dev);
+  cudaMemcpyAsync(res_host, res_dev, sizeof(ResultBlock) * (size_t)n_results,
+                  cudaMemcpyDeviceToHost, st);
 }
 
 // Captures one frame of 'tab' on 'st' into an executable graph.
@@ -396,7 +168,7 @@ dyn_status capture_frame(const SessDev* tab, const BatchShape& b, ResultBlock* r
                          cudaGraphExec_t* exec_out, int* kernels_out) {
   cudaGraph_t g = nullptr;
   DYN_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-  enqueue_frame(tab, b, res_dev, res_host, st, m);
+  enqueue_frame(tab, b, nullptr, res_dev, res_host, b.n, st, m);
   cudaError_t e = cudaStreamEndCapture(st, &g);
   if (e != cudaSuccess) return DYN_ERR_CUDA;
   size_t nn = 0;
@@ -503,6 +275,7 @@ dyn_status set_rgb_flag(dyn_session* s, bool has_rgb, cudaStream_t st) {
 // Session calls that read device state wait for the batch it belongs to.
 dyn_status quiesce(dyn_session* s) {
   if (s->batch) DYN_CUDA(cudaStreamSynchronize(s->batch->stream));
+  if (s->owner_stream) DYN_CUDA(cudaStreamSynchronize(s->owner_stream));
   return DYN_OK;
 }
 
@@ -630,8 +403,7 @@ dyn_status reset_state(dyn_session* s) {
 // term needs the model's colour.
 bool mixed_colour(const dyn_gn_params* gn) { return gn && gn->color_weight != 0.0f; }
 
-size_t session_bytes(const dyn_tsdf_params& t, const dyn_sensor& s, int precision = 0,
-                     bool colour = true) {
+size_t session_bytes(const dyn_tsdf_params& t, const dyn_sensor& s, int precision, bool colour) {
   size_t n = (size_t)s.rows * s.cols;
   size_t b = 0;
   b += sizeof(Entry) * (size_t)t.num_buckets * t.bucket_size;
@@ -658,7 +430,8 @@ struct StageScratch {
 std::mutex g_stage_mu;
 StageScratch g_stage[64];
 
-}  // namespace
+}  // namespace host
+}  // namespace dyn
 
 extern "C" {
 
@@ -868,7 +641,7 @@ dyn_status dyn_session_set_pose(dyn_session* s, const float pose[16]) {
 }
 
 dyn_status dyn_frame_submit(dyn_session* s, const uint16_t* depth_host, const uint8_t* rgb_host) {
-  if (!s || !depth_host || s->batch) return DYN_ERR_INVALID_ARG;
+  if (!s || !depth_host || s->batch || s->owner_stream) return DYN_ERR_INVALID_ARG;
   DeviceGuard dg(s->device);
   dyn_status r = upload_frame(s, depth_host, rgb_host);
   if (r != DYN_OK) return r;
@@ -876,7 +649,7 @@ dyn_status dyn_frame_submit(dyn_session* s, const uint16_t* depth_host, const ui
 }
 
 dyn_status dyn_frame_submit_device(dyn_session* s, const uint16_t* depth_dev, const uint8_t* rgb_dev) {
-  if (!s || !depth_dev || s->batch) return DYN_ERR_INVALID_ARG;
+  if (!s || !depth_dev || s->batch || s->owner_stream) return DYN_ERR_INVALID_ARG;
   DeviceGuard dg(s->device);
   DYN_CUDA(cudaMemcpyAsync(s->d_u16, depth_dev, s->npx * 2, cudaMemcpyDeviceToDevice, s->stream));
   if (rgb_dev)
@@ -900,7 +673,7 @@ dyn_status dyn_frame_result(dyn_session* s, float pose_out[16], dyn_frame_stats*
 
 dyn_status dyn_integrate_with_pose(dyn_session* s, const uint16_t* depth_host,
                                    const uint8_t* rgb_host, const float pose[16]) {
-  if (!s || !depth_host || !pose || s->batch) return DYN_ERR_INVALID_ARG;
+  if (!s || !depth_host || !pose || s->batch || s->owner_stream) return DYN_ERR_INVALID_ARG;
   DeviceGuard dg(s->device);
   dyn_status r = dyn_session_set_pose(s, pose);
   if (r != DYN_OK) return r;
@@ -910,7 +683,7 @@ dyn_status dyn_integrate_with_pose(dyn_session* s, const uint16_t* depth_host,
   enqueue_source(s->d_sd, s->shape, s->stream, none);
   bump_frame_kernel<<<1, 32, 0, s->stream>>>(s->d_pose);
   enqueue_map_update(s->d_sd, s->shape, s->stream, none);
-  gather_results_kernel<<<1, 128, 0, s->stream>>>(s->d_sd, 1, s->d_res);
+  gather_results_kernel<<<1, 128, 0, s->stream>>>(s->d_sd, 1, nullptr, s->d_res);
   DYN_CUDA(cudaMemcpyAsync(s->h_res, s->d_res, sizeof(ResultBlock), cudaMemcpyDeviceToHost,
                            s->stream));
   DYN_CUDA(cudaStreamSynchronize(s->stream));
@@ -923,7 +696,7 @@ dyn_status dyn_solver_solve(dyn_session* s, const float* target_depth_host,
                             const uint8_t* target_rgb_host, const float* source_depth_host,
                             const uint8_t* source_rgb_host, float pose_inout[16],
                             double increment_out[6], dyn_frame_stats* stats) {
-  if (!s || !target_depth_host || !source_depth_host || !pose_inout || s->batch)
+  if (!s || !target_depth_host || !source_depth_host || !pose_inout || s->batch || s->owner_stream)
     return DYN_ERR_INVALID_ARG;
   DeviceGuard dg(s->device);
   cudaStream_t st = s->stream;
@@ -960,7 +733,7 @@ dyn_status dyn_solver_solve(dyn_session* s, const float* target_depth_host,
   mark_target_kernel<<<1, 32, 0, st>>>(s->d_icp);
   enqueue_icp(s->d_sd, s->shape, st);
   fused_pose_finalize(s->d_sd, s->shape, 0, st);
-  gather_results_kernel<<<1, 128, 0, st>>>(s->d_sd, 1, s->d_res);
+  gather_results_kernel<<<1, 128, 0, st>>>(s->d_sd, 1, nullptr, s->d_res);
   DYN_CUDA(cudaMemcpyAsync(s->h_res, s->d_res, sizeof(ResultBlock), cudaMemcpyDeviceToHost, st));
   DYN_CUDA(cudaStreamSynchronize(st));
   DYN_CUDA(cudaGetLastError());
@@ -1216,205 +989,6 @@ dyn_status dyn_sessions_submit(dyn_session* const* sessions, int32_t n,
     dyn_status r = dyn_frame_submit(sessions[i], depth_host[i], rgb_host ? rgb_host[i] : nullptr);
     if (r != DYN_OK) return r;
   }
-  return DYN_OK;
-}
-
-// ---------------------------------------------------------------- batches
-
-dyn_status dyn_batch_create(dyn_session* const* sessions, int32_t n, dyn_batch** out) {
-  if (!out) return DYN_ERR_INVALID_ARG;
-  *out = nullptr;
-  if (!sessions || n < 1 || n > 65535) return DYN_ERR_INVALID_ARG;
-  for (int i = 0; i < n; ++i) {
-    if (!sessions[i] || sessions[i]->batch || sessions[i]->device != sessions[0]->device)
-      return DYN_ERR_INVALID_ARG;
-    for (int j = 0; j < i; ++j)
-      if (sessions[j] == sessions[i]) return DYN_ERR_INVALID_ARG;
-  }
-  DeviceGuard dg(sessions[0]->device);
-  dyn_batch* b = new (std::nothrow) dyn_batch();
-  if (!b) return DYN_ERR_OOM;
-  b->device = sessions[0]->device;
-  b->n = n;
-  b->ss.assign(sessions, sessions + n);
-  int64_t cap = 0;
-  for (int i = 0; i < n; ++i) {
-    if (cudaStreamSynchronize(sessions[i]->stream) != cudaSuccess) {
-      delete b;
-      return DYN_ERR_CUDA;
-    }
-    cap += sessions[i]->tp.num_blocks;
-  }
-  if (cap > INT32_MAX) {
-    delete b;
-    return DYN_ERR_INVALID_ARG;
-  }
-  auto dalloc = [&](void** p, size_t bytes) -> dyn_status {
-    cudaError_t e = cudaMalloc(p, bytes < 256 ? 256 : bytes);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      return e == cudaErrorMemoryAllocation ? DYN_ERR_OOM : DYN_ERR_CUDA;
-    }
-    b->allocs.push_back(*p);
-    return DYN_OK;
-  };
-  dyn_status r = DYN_OK;
-  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreateWithFlags(&b->h2d_done, cudaEventDisableTiming) != cudaSuccess ||
-      cudaMallocHost(&b->h_res, sizeof(ResultBlock) * (size_t)n) != cudaSuccess)
-    r = DYN_ERR_CUDA;
-  if (r == DYN_OK) r = dalloc((void**)&b->d_tab, sizeof(SessDev) * (size_t)n);
-  if (r == DYN_OK) r = dalloc((void**)&b->d_gvis, sizeof(int2) * (size_t)cap);
-  if (r == DYN_OK) r = dalloc((void**)&b->d_gcount, sizeof(int));
-  if (r == DYN_OK) r = dalloc((void**)&b->d_res, sizeof(ResultBlock) * (size_t)n);
-  if (r == DYN_OK) {
-    std::vector<SessDev> tab((size_t)n);
-    for (int i = 0; i < n; ++i) tab[i] = sessions[i]->hsd;
-    if (cudaMemcpyAsync(b->d_tab, tab.data(), sizeof(SessDev) * (size_t)n,
-                        cudaMemcpyHostToDevice, b->stream) != cudaSuccess ||
-        cudaEventRecord(b->h2d_done, b->stream) != cudaSuccess ||
-        cudaStreamSynchronize(b->stream) != cudaSuccess)
-      r = DYN_ERR_CUDA;
-  }
-  if (r != DYN_OK) {
-    cudaGetLastError();
-    release(b);
-    return r;
-  }
-  b->shape = make_shape(sessions, n, b->d_gvis, b->d_gcount, (int)cap);
-  for (int i = 0; i < n; ++i) sessions[i]->batch = b;
-  *out = b;
-  return DYN_OK;
-}
-
-dyn_status dyn_batch_destroy(dyn_batch* b) {
-  if (!b) return DYN_ERR_INVALID_ARG;
-  release(b);
-  return DYN_OK;
-}
-
-static dyn_status batch_ready(dyn_batch* b) {
-  for (dyn_session* s : b->ss)
-    if (!s) return DYN_ERR_INVALID_ARG;  // a member was destroyed
-  return DYN_OK;
-}
-
-static dyn_status batch_launch(dyn_batch* b) {
-  if (!b->exec) {
-    Marks m;
-    m.on = b->profile;
-    m.ev = b->ev;
-    m.st = b->stream;
-    dyn_status r = capture_frame(b->d_tab, b->shape, b->d_res, b->h_res, b->stream, m, &b->exec,
-                                 &b->kernels_per_frame);
-    if (r != DYN_OK) return r;
-  }
-  DYN_CUDA(cudaGraphLaunch(b->exec, b->stream));
-  b->pending = true;
-  for (dyn_session* s : b->ss) s->frames++;
-  return DYN_OK;
-}
-
-dyn_status dyn_batch_submit(dyn_batch* b, const uint16_t* const* depth_host,
-                            const uint8_t* const* rgb_host) {
-  if (!b || !depth_host) return DYN_ERR_INVALID_ARG;
-  DYN_TRY(batch_ready(b));
-  for (int i = 0; i < b->n; ++i)
-    if (!depth_host[i]) return DYN_ERR_INVALID_ARG;
-  DeviceGuard dg(b->device);
-  // the staging buffers may still feed the previous frame's copies
-  DYN_CUDA(cudaEventSynchronize(b->h2d_done));
-  for (int i = 0; i < b->n; ++i)
-    DYN_TRY(copy_frame_in(b->ss[i], depth_host[i], rgb_host ? rgb_host[i] : nullptr, b->stream));
-  DYN_CUDA(cudaEventRecord(b->h2d_done, b->stream));
-  return batch_launch(b);
-}
-
-dyn_status dyn_batch_submit_device(dyn_batch* b, const uint16_t* const* depth_dev,
-                                   const uint8_t* const* rgb_dev) {
-  if (!b || !depth_dev) return DYN_ERR_INVALID_ARG;
-  DYN_TRY(batch_ready(b));
-  for (int i = 0; i < b->n; ++i)
-    if (!depth_dev[i]) return DYN_ERR_INVALID_ARG;
-  DeviceGuard dg(b->device);
-  for (int i = 0; i < b->n; ++i) {
-    dyn_session* s = b->ss[i];
-    const uint8_t* rgb = rgb_dev ? rgb_dev[i] : nullptr;
-    DYN_CUDA(cudaMemcpyAsync(s->d_u16, depth_dev[i], s->npx * 2, cudaMemcpyDeviceToDevice,
-                             b->stream));
-    if (rgb)
-      DYN_CUDA(cudaMemcpyAsync(s->d_rgb, rgb, s->npx * 3, cudaMemcpyDeviceToDevice, b->stream));
-    DYN_TRY(set_rgb_flag(s, rgb != nullptr, b->stream));
-  }
-  return batch_launch(b);
-}
-
-dyn_status dyn_batch_result(dyn_batch* b, float* poses_out, dyn_frame_stats* stats_out,
-                            dyn_status* status_out) {
-  if (!b) return DYN_ERR_INVALID_ARG;
-  if (!b->pending) return DYN_ERR_NOT_READY;
-  DeviceGuard dg(b->device);
-  DYN_CUDA(cudaStreamSynchronize(b->stream));
-  b->pending = false;
-  if (b->profile) add_stage_times(b->ev, b->stage_ms, &b->prof_frames);
-  dyn_status first = DYN_OK;
-  for (int i = 0; i < b->n; ++i) {
-    const ResultBlock& r = b->h_res[i];
-    if (poses_out)
-      for (int k = 0; k < 16; ++k) poses_out[16 * i + k] = (float)r.pose.pose[k];
-    if (stats_out && b->ss[i]) fill_stats(b->ss[i], r, &stats_out[i]);
-    const dyn_status st = counters_status(r.cnt);
-    if (status_out) status_out[i] = st;
-    if (first == DYN_OK) first = st;
-  }
-  return first;
-}
-
-dyn_status dyn_batch_size(dyn_batch* b, int32_t* n_out) {
-  if (!b || !n_out) return DYN_ERR_INVALID_ARG;
-  *n_out = b->n;
-  return DYN_OK;
-}
-
-dyn_status dyn_batch_stream(dyn_batch* b, void** stream_out) {
-  if (!b || !stream_out) return DYN_ERR_INVALID_ARG;
-  *stream_out = (void*)b->stream;
-  return DYN_OK;
-}
-
-dyn_status dyn_batch_profile(dyn_batch* b, int32_t enable) {
-  if (!b) return DYN_ERR_INVALID_ARG;
-  DeviceGuard dg(b->device);
-  DYN_CUDA(cudaStreamSynchronize(b->stream));
-  bool en = enable != 0;
-  if (en && !b->ev[0])
-    for (int k = 0; k < DYN_NUM_STAGES; ++k) DYN_CUDA(cudaEventCreate(&b->ev[k]));
-  if (en != b->profile) {
-    if (b->exec) {
-      cudaGraphExecDestroy(b->exec);
-      b->exec = nullptr;
-    }
-    b->profile = en;
-  }
-  return DYN_OK;
-}
-
-dyn_status dyn_batch_stage_times(dyn_batch* b, double ms_out[DYN_NUM_STAGES],
-                                 int64_t* frames_out, int32_t reset) {
-  if (!b) return DYN_ERR_INVALID_ARG;
-  if (ms_out)
-    for (int k = 0; k < DYN_NUM_STAGES; ++k) ms_out[k] = b->stage_ms[k];
-  if (frames_out) *frames_out = b->prof_frames;
-  if (reset) {
-    for (int k = 0; k < DYN_NUM_STAGES; ++k) b->stage_ms[k] = 0.0;
-    b->prof_frames = 0;
-  }
-  return DYN_OK;
-}
-
-dyn_status dyn_batch_kernels_per_frame(dyn_batch* b, int32_t* n_out) {
-  if (!b || !n_out) return DYN_ERR_INVALID_ARG;
-  *n_out = b->kernels_per_frame;
   return DYN_OK;
 }
 

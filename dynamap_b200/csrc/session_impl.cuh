@@ -1,0 +1,280 @@
+// session_impl.cuh -- internal definitions shared by session.cu (sessions,
+// the per-frame pipeline, stage entry points) and serving.cu (batches and
+// the serving loop).  Not part of the public interface.
+#pragma once
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "icp.cuh"
+#include "image.cuh"
+#include "sessdev.cuh"
+#include "tsdf.cuh"
+
+namespace dyn {
+namespace host {
+
+struct ResultBlock {
+  PoseState pose;
+  IcpState icp;
+  Counters cnt;
+};
+static_assert(sizeof(PoseState) % 4 == 0 && sizeof(IcpState) % 4 == 0 &&
+                  sizeof(Counters) % 4 == 0,
+              "result parts are copied as 32-bit words");
+
+inline int level_of_scale(int scale) {
+  int l = 0;
+  while ((1 << l) < scale && l < kLevels - 1) ++l;
+  return l;
+}
+
+inline DSensor dsensor(const dyn_sensor& s) {
+  DSensor d;
+  d.rows = (int)s.rows;
+  d.cols = (int)s.cols;
+  d.fx = s.fx;
+  d.fy = s.fy;
+  d.cx = s.cx;
+  d.cy = s.cy;
+  return d;
+}
+
+// Level sensor for scale 2^l: f/s, (c+0.5)/s-0.5, dims floor(dim/s).
+inline dyn_sensor level_sensor(const dyn_sensor& s, int scale) {
+  dyn_sensor o = s;
+  o.rows = s.rows / (uint32_t)scale;
+  o.cols = s.cols / (uint32_t)scale;
+  o.fx = s.fx / (float)scale;
+  o.fy = s.fy / (float)scale;
+  o.cx = (s.cx + 0.5f) / (float)scale - 0.5f;
+  o.cy = (s.cy + 0.5f) / (float)scale - 0.5f;
+  return o;
+}
+
+inline DTsdf dtsdf(const dyn_tsdf_params& p) {
+  DTsdf t;
+  t.vs = p.voxel_size;
+  t.bsm = (float)p.block_size * p.voxel_size;  // tsdf.cu:437-438
+  t.trunc = p.truncation_distance;
+  t.dmin = p.min_sensor_depth;
+  t.dmax = p.max_sensor_depth;
+  t.num_buckets = p.num_buckets;
+  t.nb_mask = (p.num_buckets & (p.num_buckets - 1)) == 0 ? p.num_buckets - 1 : -1;
+  t.bucket_size = p.bucket_size;
+  t.num_blocks = p.num_blocks;
+  t.max_w = p.max_sdf_weight;
+  double bs = (double)p.block_size * (double)p.voxel_size;
+  t.dda_cap = 3 * (int)std::ceil(((double)p.max_sensor_depth + (double)p.truncation_distance) / bs) + 8;
+  double step = std::min((double)p.voxel_size, (double)p.truncation_distance);
+  t.rc_cap = (int)std::ceil((double)p.max_sensor_depth / step) + 4;
+  return t;
+}
+
+#define DYN_CUDA(x)                                  \
+  do {                                               \
+    cudaError_t e_ = (x);                            \
+    if (e_ != cudaSuccess) {                         \
+      if (e_ == cudaErrorMemoryAllocation) return DYN_ERR_OOM; \
+      return DYN_ERR_CUDA;                           \
+    }                                                \
+  } while (0)
+
+#define DYN_TRY(x)                 \
+  do {                             \
+    dyn_status r_ = (x);           \
+    if (r_ != DYN_OK) return r_;   \
+  } while (0)
+
+inline bool valid_sensor(const dyn_sensor* s) {
+  return s && s->rows > 0 && s->cols > 0 && s->rows <= 8192 && s->cols <= 8192 &&
+         s->fx > 0 && s->fy > 0 && s->depth_scaler > 0;
+}
+
+}  // namespace host
+}  // namespace dyn
+
+// The opaque handle types of the C ABI (global names), built from dyn:: parts.
+using namespace dyn;
+using dyn::host::ResultBlock;
+
+struct dyn_session {
+  int device = 0;
+  dyn_tsdf_params tp;
+  dyn_gn_params gp;
+  dyn_bilateral_params bp;
+  dyn_sensor sensor;
+  int precision = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t h2d_done = nullptr;
+  DSensor ls[kLevels];
+  int nlev = 1;
+  size_t npx = 0;
+  // device buffers
+  std::vector<void*> allocs;
+  uint16_t* d_u16 = nullptr;
+  uint8_t* d_rgb = nullptr;
+  float* d_raw = nullptr;
+  float* d_filt = nullptr;
+  float* d_sdep[kLevels] = {};
+  float4* d_snrm[kLevels] = {};
+  float4* d_svtx[kLevels] = {};
+  float* d_sint[kLevels] = {};
+  float* d_tdep[kLevels] = {};
+  float4* d_tnrm[kLevels] = {};
+  float4* d_tvtx[kLevels] = {};
+  float* d_tint[kLevels] = {};
+  float* d_ray = nullptr;
+  uint8_t* d_trgb = nullptr;
+  float* d_pose_override = nullptr;
+  double* d_pose_in = nullptr;
+  double* d_partials = nullptr;
+  IcpState* d_icp = nullptr;
+  PoseState* d_pose = nullptr;
+  VolumeDev vol;
+  // fused-launch descriptor (host copy and its device table of one)
+  SessDev hsd;
+  SessDev* d_sd = nullptr;
+  BilateralTable* d_btab = nullptr;
+  int* d_rgb_flag = nullptr;   // nonzero: the current frame carries RGB
+  int rgb_flag_host = -1;      // last value written (-1: unknown)
+  int2* d_gvis = nullptr;      // visible list of the table of one
+  int* d_gcount = nullptr;
+  ResultBlock* d_res = nullptr;
+  BatchShape shape;
+  dyn_batch* batch = nullptr;  // member of this batch (frames go through it)
+  cudaStream_t owner_stream = nullptr;  // a server's stream when it owns the session
+  // host
+  uint16_t* h_depth = nullptr;
+  uint8_t* h_rgb = nullptr;
+  ResultBlock* h_res = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  BilateralTable btab;
+  // profiling: ev[i] ends stage i (DYN_STAGE_*), ev[DYN_STAGE_FRAME] starts the frame
+  bool profile = false;
+  cudaEvent_t ev[DYN_NUM_STAGES] = {};
+  double stage_ms[DYN_NUM_STAGES] = {};
+  int64_t prof_frames = 0;
+  int kernels_per_frame = 0;
+  bool debug_maps = false;
+  int frames = 0;
+  bool pending = false;
+
+  template <class T>
+  dyn_status dalloc(T** p, size_t bytes) {
+    void* q = nullptr;
+    bytes = (bytes + 255) / 256 * 256;  // whole 16-byte vectors at the tail
+    cudaError_t e = cudaMalloc(&q, bytes < 256 ? 256 : bytes);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return e == cudaErrorMemoryAllocation ? DYN_ERR_OOM : DYN_ERR_CUDA;
+    }
+    allocs.push_back(q);
+    *p = (T*)q;
+    return DYN_OK;
+  }
+  bool use_color() const { return gp.color_weight != 0.0f; }
+  IcpParams icp_params() const {
+    IcpParams P;
+    P.dmin = gp.icp_min_depth;
+    P.dmax = gp.icp_max_depth;
+    P.cos_thr = gp.normal_cos_thresh;
+    P.cw = gp.color_weight;
+    P.min_inc = gp.min_increment;
+    P.max_inc = gp.max_increment;
+    P.reg = gp.regularization;
+    P.compose_left = gp.compose_left;
+    P.kahan = precision == DYN_PRECISION_MIXED ? 1 : 0;
+    return P;
+  }
+};
+
+// A fixed set of sessions on one device whose frames run together: each
+// stage is one launch over the members' descriptor table and the whole frame
+// one CUDA graph on the batch's stream.
+struct dyn_batch {
+  int device = 0;
+  int n = 0;
+  std::vector<dyn_session*> ss;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t h2d_done = nullptr;
+  std::vector<void*> allocs;
+  SessDev* d_tab = nullptr;
+  int2* d_gvis = nullptr;
+  int* d_gcount = nullptr;
+  ResultBlock* d_res = nullptr;
+  ResultBlock* h_res = nullptr;  // pinned, n entries
+  BatchShape shape;
+  cudaGraphExec_t exec = nullptr;
+  int kernels_per_frame = 0;
+  bool profile = false;
+  cudaEvent_t ev[DYN_NUM_STAGES] = {};
+  double stage_ms[DYN_NUM_STAGES] = {};
+  int64_t prof_frames = 0;
+  bool pending = false;
+};
+
+namespace dyn {
+namespace host {
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+// Stage boundary events (profiling only; captured into the frame graph):
+// ev[i] ends stage i, ev[DYN_STAGE_FRAME] starts the frame.
+struct Marks {
+  bool on = false;
+  cudaEvent_t* ev = nullptr;
+  cudaStream_t st = nullptr;
+  void operator()(int stage) const {
+    // External: during capture this becomes an event-record node of the graph
+    if (on) cudaEventRecordWithFlags(ev[stage], st, cudaEventRecordExternal);
+  }
+};
+
+void release(dyn_session* s);
+void release(dyn_batch* b);
+// The launch shape of a table of sessions (the largest member bounds every
+// grid).
+BatchShape make_shape(dyn_session* const* ss, int n, int2* gvis, int* gcount, int gvis_cap);
+// Marks whether this frame of 's' carries RGB (stream-ordered).
+dyn_status set_rgb_flag(dyn_session* s, bool has_rgb, cudaStream_t st);
+// Host frame into the session's device input buffers on 'st'.
+dyn_status copy_frame_in(dyn_session* s, const uint16_t* depth, const uint8_t* rgb,
+                         cudaStream_t st);
+// One frame of every session of 'tab' on 'st', then every session's results
+// into res_dev[slot_map ? slot_map[i] : i] and n_results entries of res_dev
+// back into res_host (pinned).
+void enqueue_frame(const SessDev* tab, const BatchShape& b, const int* slot_map,
+                   ResultBlock* res_dev, ResultBlock* res_host, int n_results, cudaStream_t st,
+                   const Marks& m);
+// The same captured into an executable graph.
+dyn_status capture_frame(const SessDev* tab, const BatchShape& b, ResultBlock* res_dev,
+                         ResultBlock* res_host, cudaStream_t st, const Marks& m,
+                         cudaGraphExec_t* exec_out, int* kernels_out);
+void add_stage_times(cudaEvent_t* ev, double* ms_acc, int64_t* frames);
+// Device bytes a session with these parameters allocates (colour: a mixed
+// session keeps per-voxel colour).
+size_t session_bytes(const dyn_tsdf_params& t, const dyn_sensor& s, int precision, bool colour);
+bool mixed_colour(const dyn_gn_params* gn);
+dyn_status counters_status(const Counters& c);
+void fill_stats(const dyn_session* s, const ResultBlock& r, dyn_frame_stats* st);
+
+}  // namespace host
+}  // namespace dyn

@@ -13,6 +13,15 @@ of them, one CUDA graph per frame):
 
     with Batch([m0, m1, m2]) as b:
         poses, stats, status = b.process([d0, d1, d2])
+
+Server admits sessions under an HBM budget and steps whichever have a frame
+waiting (continuous batching):
+
+    with Server(budget_bytes=150 << 30) as sv:
+        slot = sv.admit(t, g, b, s, pose0=pose0)
+        sv.push(slot, depth)
+        sv.step()
+        pose, stats = sv.result(slot)
 """
 from __future__ import annotations
 
@@ -27,6 +36,20 @@ _vp = C.c_void_p
 
 def _ptr(a):
     return None if a is None else a.ctypes.data_as(_vp)
+
+
+def _download_blocks(lib, h):
+    n = C.c_int64()
+    abi.check("dyn_num_blocks", lib.dyn_num_blocks(h, C.byref(n)))
+    n = n.value
+    coords = np.empty((n, 3), np.int32)
+    vox = np.empty((n, 512, 2), np.uint32)  # {rgbw, sdf bits} per voxel
+    got = C.c_int64()
+    abi.check("dyn_download_blocks", lib.dyn_download_blocks(
+        h, _ptr(coords), _ptr(vox), n, C.byref(got)))
+    rgbw = vox[..., 0].copy().view(np.uint8).reshape(n, 512, 4)
+    sdf = vox[..., 1].copy().view(np.float32)
+    return coords, rgbw, sdf
 
 
 def _f16(pose) -> C.Array:
@@ -117,15 +140,7 @@ class Session:
 
     def download_blocks(self):
         """(coords (n,3) int32, rgbw (n,512,4) uint8, sdf (n,512) float32)."""
-        n = self.num_blocks()
-        coords = np.empty((n, 3), np.int32)
-        vox = np.empty((n, 512, 2), np.uint32)  # {rgbw, sdf bits} per voxel
-        got = C.c_int64()
-        abi.check("dyn_download_blocks", self.lib.dyn_download_blocks(
-            self.h, _ptr(coords), _ptr(vox), n, C.byref(got)))
-        rgbw = vox[..., 0].copy().view(np.uint8).reshape(n, 512, 4)
-        sdf = vox[..., 1].copy().view(np.float32)
-        return coords, rgbw, sdf
+        return _download_blocks(self.lib, self.h)
 
     def image(self, which: int, level: int, shape, dtype) -> np.ndarray:
         out = np.empty(shape, dtype)
@@ -212,3 +227,92 @@ class Batch:
         abi.check("dyn_batch_kernels_per_frame",
                   self.lib.dyn_batch_kernels_per_frame(self.h, C.byref(n)))
         return n.value
+
+
+class Server:
+    """dyn_server: sessions admitted by HBM budget, stepped together."""
+
+    def __init__(self, budget_bytes: int = 0, max_sessions: int = 0, device: int = 0):
+        self.lib = abi.load()
+        p = abi.ServerParams(budget_bytes, max_sessions, device)
+        self.h = _vp()
+        abi.check("dyn_server_create", self.lib.dyn_server_create(C.byref(p), C.byref(self.h)))
+        self.sensors = {}
+
+    def close(self) -> None:
+        if self.h:
+            self.lib.dyn_server_destroy(self.h)
+            self.h = _vp()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def admit(self, tsdf, gn, bil, sensor, precision: int = abi.PRECISION_FP32, pose0=None):
+        """Slot index, or None when the budget (or the slot table) is full."""
+        slot = C.c_int32(-1)
+        r = self.lib.dyn_server_admit(self.h, C.byref(tsdf), C.byref(gn), C.byref(bil),
+                                      C.byref(sensor), precision,
+                                      None if pose0 is None else _f16(pose0), C.byref(slot))
+        if r == abi.DYN_ERR_BUDGET_EXCEEDED:
+            return None
+        abi.check("dyn_server_admit", r)
+        self.sensors[slot.value] = sensor
+        return slot.value
+
+    def release(self, slot: int) -> None:
+        abi.check("dyn_server_release", self.lib.dyn_server_release(self.h, slot))
+        self.sensors.pop(slot, None)
+
+    def push(self, slot: int, depth, rgb=None) -> bool:
+        """False when the slot's previous frame has not been stepped yet."""
+        d = np.ascontiguousarray(depth, np.uint16)
+        c = None if rgb is None else np.ascontiguousarray(rgb, np.uint8)
+        r = self.lib.dyn_server_push(self.h, slot, _ptr(d), _ptr(c))
+        if r == abi.DYN_ERR_NOT_READY:
+            return False
+        abi.check("dyn_server_push", r)
+        return True
+
+    def step(self) -> int:
+        n = C.c_int32()
+        abi.check("dyn_server_step", self.lib.dyn_server_step(self.h, C.byref(n)))
+        return n.value
+
+    def ready(self, slot: int) -> bool:
+        r = C.c_int32()
+        abi.check("dyn_server_poll", self.lib.dyn_server_poll(self.h, slot, C.byref(r)))
+        return bool(r.value)
+
+    def result(self, slot: int, strict: bool = True):
+        pose = (C.c_float * 16)()
+        st = abi.FrameStats()
+        r = self.lib.dyn_server_result(self.h, slot, pose, C.byref(st))
+        if strict or r not in (abi.DYN_ERR_HASH_FULL, abi.DYN_ERR_HEAP_EXHAUSTED):
+            abi.check("dyn_server_result", r)
+        return np.array(pose, np.float32).reshape(4, 4), st
+
+    def sync(self) -> None:
+        abi.check("dyn_server_sync", self.lib.dyn_server_sync(self.h))
+
+    def session_handle(self, slot: int):
+        p = _vp()
+        abi.check("dyn_server_session", self.lib.dyn_server_session(self.h, slot, C.byref(p)))
+        return p
+
+    def usage(self) -> dict:
+        u = abi.ServerUsage()
+        abi.check("dyn_server_info", self.lib.dyn_server_info(self.h, C.byref(u)))
+        return {k: getattr(u, k) for k, _ in u._fields_}
+
+    def download_blocks(self, slot: int):
+        """The slot's map, as Session.download_blocks."""
+        return _download_blocks(self.lib, self.session_handle(slot))

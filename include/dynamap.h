@@ -386,6 +386,52 @@ dyn_status dyn_batch_stage_times(dyn_batch* b, double ms_out[DYN_NUM_STAGES],
                                  int64_t* frames_out, int32_t reset);
 dyn_status dyn_batch_kernels_per_frame(dyn_batch* b, int32_t* n_out);
 
+/* dyn_server: the serving loop's device side.  Sessions are admitted while
+ * their device bytes (dyn_session_bytes, with a mixed session's colour only
+ * when its photometric weight is nonzero) fit the budget and a slot is free
+ * (else DYN_ERR_BUDGET_EXCEEDED: retry when a session has been released),
+ * and released at any time.  dyn_server_push copies a host frame into the
+ * session's pinned staging buffers; dyn_server_step then runs one frame of
+ * every session that has one waiting, all of them fused into one launch per
+ * stage on the server's stream, and returns without waiting: frames pushed
+ * while a step runs join the next step (continuous batching).  A session's
+ * results are the same whichever sessions share its steps.
+ * dyn_server_result waits for the last step that processed the slot and
+ * returns its latest result.  A served session takes frames only through
+ * the server; its other calls (raycast, download, pose, images) wait for
+ * the server's work in flight.  Calls on one server are not thread-safe. */
+typedef struct dyn_server dyn_server;
+typedef struct {
+  size_t budget_bytes;   /* device bytes for sessions (0: 90% of free memory) */
+  int32_t max_sessions;  /* slots (0: 256) */
+  int32_t device;
+} dyn_server_params;
+typedef struct {
+  size_t budget_bytes;
+  size_t used_bytes;
+  int32_t capacity;
+  int32_t sessions;
+  int64_t steps;
+  int64_t frames;
+} dyn_server_usage;
+dyn_status dyn_server_create(const dyn_server_params* p, dyn_server** out);
+dyn_status dyn_server_destroy(dyn_server* sv);
+dyn_status dyn_server_admit(dyn_server* sv, const dyn_tsdf_params* tsdf,
+                            const dyn_gn_params* gn, const dyn_bilateral_params* bil,
+                            const dyn_sensor* sensor, int32_t precision,
+                            const float pose0[16] /* nullable */, int32_t* slot_out);
+dyn_status dyn_server_release(dyn_server* sv, int32_t slot);
+/* DYN_ERR_NOT_READY: the slot's previous frame has not been stepped yet. */
+dyn_status dyn_server_push(dyn_server* sv, int32_t slot, const uint16_t* depth_host,
+                           const uint8_t* rgb_host /* nullable */);
+dyn_status dyn_server_step(dyn_server* sv, int32_t* n_out /* frames in the step */);
+dyn_status dyn_server_poll(dyn_server* sv, int32_t slot, int32_t* ready_out);
+dyn_status dyn_server_result(dyn_server* sv, int32_t slot, float pose_out[16],
+                             dyn_frame_stats* stats);
+dyn_status dyn_server_sync(dyn_server* sv);
+dyn_status dyn_server_session(dyn_server* sv, int32_t slot, dyn_session** out);
+dyn_status dyn_server_info(dyn_server* sv, dyn_server_usage* out);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif

@@ -125,3 +125,29 @@ def test_session_create_without_device_reports_it():
     h = C.c_void_p()
     assert lib.dyn_session_create(C.byref(t), C.byref(g), C.byref(b), C.byref(s), 0, 0,
                                   C.byref(h)) == 10
+
+
+def test_server_create_without_device_reports_it():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    lib = abi.load()
+    h = C.c_void_p()
+    assert lib.dyn_server_create(None, C.byref(h)) == 1
+    p = abi.ServerParams(1 << 30, 8, 0)
+    assert lib.dyn_server_create(C.byref(p), C.byref(h)) == 10
+    assert lib.dyn_server_step(None, None) == 1
+    assert lib.dyn_server_push(None, 0, None, None) == 1
+
+
+def test_session_bytes_follow_the_voxel_form():
+    lib = abi.load()
+    t, g, b, s = abi.defaults()
+    n32, n16 = C.c_size_t(), C.c_size_t()
+    abi.check("bytes", lib.dyn_session_bytes(C.byref(t), C.byref(s), 0, C.byref(n32)))
+    abi.check("bytes", lib.dyn_session_bytes(C.byref(t), C.byref(s), 1, C.byref(n16)))
+    vox = t.num_blocks * 512
+    # FP32 voxels are 8 bytes; the mixed bound counts 4 + 4 (colour kept)
+    assert n32.value - n16.value == 0
+    assert n32.value > vox * 8
+    assert lib.dyn_session_bytes(C.byref(t), C.byref(s), 0, None) == 1
