@@ -92,7 +92,7 @@ class ServerParams(C.Structure):
 class ServerUsage(C.Structure):
     _fields_ = [("budget_bytes", C.c_size_t), ("used_bytes", C.c_size_t),
                 ("capacity", C.c_int32), ("sessions", C.c_int32), ("steps", C.c_int64),
-                ("frames", C.c_int64)]
+                ("steps_done", C.c_int64), ("frames", C.c_int64)]
 
 
 P = C.POINTER

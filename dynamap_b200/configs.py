@@ -82,6 +82,37 @@ def session_mix(n_sessions: int = 32, n_frames: int = 200, base_seed: int = 100)
     return out
 
 
+# The serving configuration: sessions arrive as a Poisson process (rate
+# 4/s), each streams depth at 30 Hz for U[5, 60] s; resolutions 320x240 /
+# 640x480 / 1280x720 (ratio 2:2:1); each session's hash table holds 84 /
+# 168 / 336 MB of entries (2^19 / 2^20 / 2^21 buckets x 10); mixed
+# precision; a 150 GB device budget.
+SERVING = dict(rate_per_s=4.0, duration_s=(5.0, 60.0), fps=30.0, budget_gb=150.0,
+               kinds=["s320", "s320", "s640", "s640", "s1280"])
+
+
+def serving_kind(kind: str, n_frames: int = 24):
+    """Preset of one serving session kind."""
+    if kind == "s320":
+        sensor = dict(rows=240, cols=320, fx=262.5, fy=262.5, cx=159.5, cy=119.5,
+                      depth_scaler=1000.0)
+        tsdf = dict(voxel_size=0.008, num_buckets=1 << 19, num_blocks=1 << 16)
+    elif kind == "s640":
+        sensor = dict(rows=480, cols=640, fx=525.0, fy=525.0, cx=319.5, cy=239.5,
+                      depth_scaler=1000.0)
+        tsdf = dict(voxel_size=0.005, num_buckets=1 << 20, num_blocks=1 << 18)
+    else:
+        sensor = dict(rows=720, cols=1280, fx=910.0, fy=910.0, cx=639.5, cy=359.5,
+                      depth_scaler=1000.0)
+        tsdf = dict(voxel_size=0.004, num_buckets=1 << 21, num_blocks=1 << 19)
+    tsdf.update(bucket_size=10, block_size=8, max_sdf_weight=64,
+                truncation_distance=4 * tsdf["voxel_size"], max_sensor_depth=3.0,
+                min_sensor_depth=0.15)
+    return dict(sensor=sensor, tsdf=tsdf, gn=_gn([10, 5, 4]),
+                bilateral=dict(diameter=8, sigma_i=10.0, sigma_s=1.0, enabled=1),
+                seq=dict(n_frames=n_frames, trans=0.005, rot=0.5, rgb=False, kind="cube"))
+
+
 def preset(name: str, **over):
     p = {k: (dict(v) if isinstance(v, dict) else v) for k, v in PRESETS[name].items()}
     for k, v in over.items():

@@ -222,8 +222,10 @@ namespace {
 struct ServerSlot {
   dyn_session* s = nullptr;
   size_t bytes = 0;
-  bool queued = false;       // a frame is in the session's staging buffers
+  bool queued = false;       // a frame waits for the next step
   bool queued_rgb = false;
+  const uint16_t* src_depth = nullptr;  // pinned caller buffers read at step time
+  const uint8_t* src_rgb = nullptr;     // (null: the session's staging buffers)
   int64_t last_step = -1;    // id of the last step that processed the slot
   int last_ring = 0;
 };
@@ -252,6 +254,7 @@ struct dyn_server {
   StepBuf ring[kServerRing];
   int ring_pos = 0;
   int64_t steps = 0;
+  int64_t steps_done = 0;  // steps known to have completed (in order)
   int64_t frames = 0;
   int2* d_gvis = nullptr;
   int* d_gcount = nullptr;
@@ -380,8 +383,11 @@ dyn_status dyn_server_admit(dyn_server* sv, const dyn_tsdf_params* tsdf, const d
 dyn_status dyn_server_release(dyn_server* sv, int32_t slot) {
   DYN_TRY(check_slot(sv, slot));
   DeviceGuard dg(sv->device);
-  DYN_CUDA(cudaStreamSynchronize(sv->stream));  // the session may be in a step in flight
   ServerSlot& sl = sv->slots[slot];
+  // the last step that used the session must have completed (older ring
+  // entries were waited for when they were reused)
+  if (sl.last_step >= 0 && sl.last_step >= sv->steps - kServerRing)
+    DYN_CUDA(cudaEventSynchronize(sv->ring[sl.last_ring].done));
   sl.s->owner_stream = nullptr;
   dyn_session_destroy(sl.s);
   sv->used -= sl.bytes;
@@ -397,10 +403,18 @@ dyn_status dyn_server_push(dyn_server* sv, int32_t slot, const uint16_t* depth_h
   if (sl.queued) return DYN_ERR_NOT_READY;  // the previous frame has not been stepped
   dyn_session* s = sl.s;
   DeviceGuard dg(sv->device);
-  // the staging buffers may still feed the copies of the slot's last step
-  DYN_CUDA(cudaEventSynchronize(s->h2d_done));
-  std::memcpy(s->h_depth, depth_host, s->npx * sizeof(uint16_t));
-  if (rgb_host) std::memcpy(s->h_rgb, rgb_host, s->npx * 3);
+  sl.src_depth = nullptr;
+  sl.src_rgb = nullptr;
+  if (is_pinned(depth_host) && (!rgb_host || is_pinned(rgb_host))) {
+    // page-locked: copied to the device by the step itself
+    sl.src_depth = depth_host;
+    sl.src_rgb = rgb_host;
+  } else {
+    // the staging buffers may still feed the copies of the slot's last step
+    DYN_CUDA(cudaEventSynchronize(s->h2d_done));
+    std::memcpy(s->h_depth, depth_host, s->npx * sizeof(uint16_t));
+    if (rgb_host) std::memcpy(s->h_rgb, rgb_host, s->npx * 3);
+  }
   sl.queued = true;
   sl.queued_rgb = rgb_host != nullptr;
   return DYN_OK;
@@ -440,9 +454,11 @@ dyn_status dyn_server_step(dyn_server* sv, int32_t* n_out) {
   for (int i = 0; i < n; ++i) {
     dyn_session* s = sv->act[i];
     ServerSlot& sl = sv->slots[rb.h_map[i]];
-    DYN_CUDA(cudaMemcpyAsync(s->d_u16, s->h_depth, s->npx * 2, cudaMemcpyHostToDevice, st));
+    DYN_CUDA(cudaMemcpyAsync(s->d_u16, sl.src_depth ? sl.src_depth : s->h_depth, s->npx * 2,
+                             cudaMemcpyHostToDevice, st));
     if (sl.queued_rgb)
-      DYN_CUDA(cudaMemcpyAsync(s->d_rgb, s->h_rgb, s->npx * 3, cudaMemcpyHostToDevice, st));
+      DYN_CUDA(cudaMemcpyAsync(s->d_rgb, sl.src_rgb ? sl.src_rgb : s->h_rgb, s->npx * 3,
+                               cudaMemcpyHostToDevice, st));
     DYN_TRY(set_rgb_flag(s, sl.queued_rgb, st));
     DYN_CUDA(cudaEventRecord(s->h2d_done, st));
   }
@@ -518,6 +534,19 @@ dyn_status dyn_server_info(dyn_server* sv, dyn_server_usage* out) {
     if (sl.s) out->sessions++;
   out->steps = sv->steps;
   out->frames = sv->frames;
+  DeviceGuard dg(sv->device);
+  // steps complete in order; those a ring length back are known complete
+  int64_t id = std::max(sv->steps_done, sv->steps - (int64_t)kServerRing);
+  for (; id < sv->steps; ++id) {
+    const cudaError_t e = cudaEventQuery(sv->ring[id % kServerRing].done);
+    if (e == cudaErrorNotReady) {
+      cudaGetLastError();
+      break;
+    }
+    if (e != cudaSuccess) return DYN_ERR_CUDA;
+  }
+  sv->steps_done = id;
+  out->steps_done = id;
   return DYN_OK;
 }
 

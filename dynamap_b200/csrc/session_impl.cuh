@@ -269,6 +269,8 @@ dyn_status capture_frame(const SessDev* tab, const BatchShape& b, ResultBlock* r
                          ResultBlock* res_host, cudaStream_t st, const Marks& m,
                          cudaGraphExec_t* exec_out, int* kernels_out);
 void add_stage_times(cudaEvent_t* ev, double* ms_acc, int64_t* frames);
+// Page-locked host memory (read by the copy engines without staging).
+bool is_pinned(const void* p);
 // Device bytes a session with these parameters allocates (colour: a mixed
 // session keeps per-voxel colour).
 size_t session_bytes(const dyn_tsdf_params& t, const dyn_sensor& s, int precision, bool colour);

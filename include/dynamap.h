@@ -411,7 +411,8 @@ typedef struct {
   size_t used_bytes;
   int32_t capacity;
   int32_t sessions;
-  int64_t steps;
+  int64_t steps;       /* steps submitted */
+  int64_t steps_done;  /* steps completed on the device (they complete in order) */
   int64_t frames;
 } dyn_server_usage;
 dyn_status dyn_server_create(const dyn_server_params* p, dyn_server** out);
@@ -421,7 +422,12 @@ dyn_status dyn_server_admit(dyn_server* sv, const dyn_tsdf_params* tsdf,
                             const dyn_sensor* sensor, int32_t precision,
                             const float pose0[16] /* nullable */, int32_t* slot_out);
 dyn_status dyn_server_release(dyn_server* sv, int32_t slot);
-/* DYN_ERR_NOT_READY: the slot's previous frame has not been stepped yet. */
+/* DYN_ERR_NOT_READY: the slot's previous frame has not been stepped yet.
+ * Page-locked buffers (cudaHostAlloc / cudaHostRegister) are not copied
+ * here: the next dyn_server_step reads them, so they must stay unchanged
+ * until that step has completed (dyn_server_poll / dyn_server_result).
+ * Other buffers are copied into the session's staging buffers and may be
+ * reused when the call returns. */
 dyn_status dyn_server_push(dyn_server* sv, int32_t slot, const uint16_t* depth_host,
                            const uint8_t* rgb_host /* nullable */);
 dyn_status dyn_server_step(dyn_server* sv, int32_t* n_out /* frames in the step */);
