@@ -282,14 +282,10 @@ def run_ours(args):
 
     import torch
     from dynamap_b200 import abi, configs
+    from dynamap_b200.replicas import Ranks
     from dynamap_b200.session import Session
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
+    ranks = Ranks()  # replicas: one independent session per GPU
     p = configs.preset(args.config)
     if args.max_blocks:
         p["tsdf"]["num_blocks"] = min(p["tsdf"]["num_blocks"], args.max_blocks)
@@ -307,15 +303,9 @@ def run_ours(args):
 
     def barrier():
         torch.cuda.synchronize()
-        if dist is not None:
-            dist.barrier()
+        ranks.barrier()
 
-    def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        v = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(v, op=dist.ReduceOp.MAX)
-        return float(v.item())
+    max_over_ranks = ranks.max
 
     import ctypes as C
 
@@ -398,8 +388,7 @@ def run_ours(args):
     elapsed_c = max_over_ranks(elapsed_c_host)
 
     if rank != 0:
-        if dist is not None:
-            dist.destroy_process_group()
+        ranks.close()
         return
 
     K = args.steps
@@ -450,8 +439,7 @@ def run_ours(args):
                 "load_factor": st_avg["blocks_total"] / (t.num_buckets * t.bucket_size)},
     }
     print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.destroy_process_group()
+    ranks.close()
 
 
 def run_batched(args):
@@ -474,14 +462,10 @@ def run_batched(args):
 
     import torch
     from dynamap_b200 import abi
+    from dynamap_b200.replicas import Ranks
     from dynamap_b200.session import Session
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
+    ranks = Ranks()  # each GPU runs its own session mix: weak scaling
     lib = abi.load()
     prec = abi.PRECISION_MIXED if args.precision == "mixed" else abi.PRECISION_FP32
     structs = [configs.structs(p) for _, p, _ in mix]
@@ -491,15 +475,9 @@ def run_batched(args):
 
     def barrier():
         torch.cuda.synchronize()
-        if dist is not None:
-            dist.barrier()
+        ranks.barrier()
 
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        v = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(v, op=dist.ReduceOp.MAX)
-        return float(v.item())
+    max_over_ranks = ranks.max
 
     def timed(fn):
         barrier()
@@ -599,8 +577,7 @@ def run_batched(args):
     for m in ss:
         m.close()
     if rank != 0:
-        if dist is not None:
-            dist.destroy_process_group()
+        ranks.close()
         return
     K = args.steps
     total = world * n * K
@@ -635,8 +612,7 @@ def run_batched(args):
                 "d2h_bytes_per_step": int(n * lib.dyn_frame_d2h_bytes())},
     }
     print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.destroy_process_group()
+    ranks.close()
 
 
 def run_serving(args):
@@ -670,14 +646,10 @@ def run_serving(args):
                                        for i, k in enumerate(kinds)], n_pool, workers)))
     import torch
     from dynamap_b200 import abi
+    from dynamap_b200.replicas import Ranks
     from dynamap_b200.session import Server
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
+    ranks = Ranks()  # each GPU serves its own arrivals: weak scaling
     # page-locked frame pools: the server's steps read them directly
     pinned = {k: torch.from_numpy(v[0]).pin_memory() for k, v in pools.items()}
     pin_np = {k: v.numpy() for k, v in pinned.items()}
@@ -691,8 +663,7 @@ def run_serving(args):
     queued = set()  # slots with a frame pushed for the next step
     step_slots = []
     ai = 0
-    if dist is not None:
-        dist.barrier()
+    ranks.barrier()
     clk = ClockSampler(local)
     clk.start()
     t0 = time.perf_counter()
@@ -752,13 +723,7 @@ def run_serving(args):
     sv.sync()
     usage = sv.usage()
     sv.close()
-    tot = torch.tensor([frames_done, elapsed], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        f = tot[:1].clone()
-        dist.all_reduce(f)
-        e = tot[1:].clone()
-        dist.all_reduce(e, op=dist.ReduceOp.MAX)
-        tot = torch.cat([f, e])
+    tot = (ranks.sum(frames_done), ranks.max(elapsed))
     if rank == 0:
         lat.sort()
         q = lambda f: 1e3 * lat[min(len(lat) - 1, int(f * len(lat)))] if lat else None
@@ -787,8 +752,7 @@ def run_serving(args):
                     "note": "the serving loop is end to end: host frames in, poses out"},
         }
         print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.destroy_process_group()
+    ranks.close()
 
 
 def main():
