@@ -440,6 +440,34 @@ __device__ inline uint2 get_voxel(const VolumeDev& v, F3 pos, float inv_vs, Bloc
 __device__ inline int vw(uint2 r) { return (int)(r.x >> 24); }
 __device__ inline float vsdf(uint2 r) { return __uint_as_float(r.y); }
 
+// The heap indices of the (up to eight) blocks a 2x2x2 cell touches: the
+// cell's low corner is in block b, its high corner steps into b + 1 along
+// the axes where the low corner is the block's last voxel (cx, cy, cz).
+// Each distinct block is resolved once (the low one through the ray's
+// cache); named fields, so that corner selection folds to a few selects.
+struct CellBlocks {
+  int p0, px, py, pz, pxy, pxz, pyz, pxyz;
+};
+__device__ inline void cell_blocks(const VolumeDev& v, int bx, int by, int bz, bool cx, bool cy,
+                                   bool cz, BlockCache& bc, CellBlocks& cb) {
+  const DTsdf& t = v.t;
+  cb.p0 = block_ptr(v, bx, by, bz, bc);
+  cb.px = cx ? find_block(v.entries, t, bx + 1, by, bz) : -1;
+  cb.py = cy ? find_block(v.entries, t, bx, by + 1, bz) : -1;
+  cb.pz = cz ? find_block(v.entries, t, bx, by, bz + 1) : -1;
+  cb.pxy = (cx && cy) ? find_block(v.entries, t, bx + 1, by + 1, bz) : -1;
+  cb.pxz = (cx && cz) ? find_block(v.entries, t, bx + 1, by, bz + 1) : -1;
+  cb.pyz = (cy && cz) ? find_block(v.entries, t, bx, by + 1, bz + 1) : -1;
+  cb.pxyz = (cx && cy && cz) ? find_block(v.entries, t, bx + 1, by + 1, bz + 1) : -1;
+}
+// the block of corner (ox, oy, oz) (compile-time offsets after unrolling)
+__device__ inline int corner_block(const CellBlocks& cb, bool cx, bool cy, bool cz, int ox,
+                                   int oy, int oz) {
+  const bool kx = ox && cx, ky = oy && cy, kz = oz && cz;
+  return kx ? (ky ? (kz ? cb.pxyz : cb.pxy) : (kz ? cb.pxz : cb.px))
+            : (ky ? (kz ? cb.pyz : cb.py) : (kz ? cb.pz : cb.p0));
+}
+
 // tsdfVolume::GetInterpolatedVoxel, tsdf.cu:47-175.  The eight corners are
 // pos_dual + {0, vs} per axis, so each axis has two coordinate values: they
 // are resolved once (six index computations instead of twenty-four) and
@@ -473,10 +501,11 @@ __device__ inline VoxelSample get_interpolated(const VolumeDev& v, F3 position, 
   gy[1] = voxel_index(pos_dual.y + vs, vs, inv_vs);
   gz[0] = voxel_index(pos_dual.z + 0.0f, vs, inv_vs);
   gz[1] = voxel_index(pos_dual.z + vs, vs, inv_vs);
-  const bool one_block = blk_of(gx[0]) == blk_of(gx[1]) && blk_of(gy[0]) == blk_of(gy[1]) &&
-                         blk_of(gz[0]) == blk_of(gz[1]);
-  int ptr0 = 0;
-  if (one_block) ptr0 = block_ptr(v, blk_of(gx[0]), blk_of(gy[0]), blk_of(gz[0]), bc);
+  // the high corners lie in the next block along an axis where they cross
+  const bool cx = blk_of(gx[1]) != blk_of(gx[0]), cy = blk_of(gy[1]) != blk_of(gy[0]),
+             cz = blk_of(gz[1]) != blk_of(gz[0]);
+  CellBlocks cells;
+  cell_blocks(v, blk_of(gx[0]), blk_of(gy[0]), blk_of(gz[0]), cx, cy, cz, bc, cells);
   float dist = 0.0f;
   float cr = 0.0f, cg = 0.0f, cb = 0.0f;
   const int off[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1},
@@ -484,8 +513,7 @@ __device__ inline VoxelSample get_interpolated(const VolumeDev& v, F3 position, 
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
     const int ox = off[k][0], oy = off[k][1], oz = off[k][2];
-    const int ptr = one_block ? ptr0
-                              : block_ptr(v, blk_of(gx[ox]), blk_of(gy[oy]), blk_of(gz[oz]), bc);
+    const int ptr = corner_block(cells, cx, cy, cz, ox, oy, oz);
     uint2 vv = load_voxel(v, ptr, lin_of(gx[ox], gy[oy], gz[oz]));
     uint2 src = (vw(vv) == 0) ? v0 : vv;
     float a = ox ? wt.x : 1.0f - wt.x;
@@ -578,37 +606,34 @@ __device__ inline float s16(unsigned r, float trunc) {
 }
 __device__ inline int w16(unsigned r) { return (int)(r >> 16); }
 
+// Trilinear sample of the f16 sdf (and colour) at 'position': the cell's
+// corners are floor(p / vs) and floor(p / vs) + 1 per axis (the reference's
+// rounded p - vs/2 and p + vs/2, up to ties) with weights p/vs - floor(p/vs);
+// unobserved corners take the centre voxel's value (raw0, heap index ptr0v,
+// local index lin0), as GetInterpolatedVoxel does.
 template <bool COLOR>
 __device__ inline VoxelSample interp16(const VolumeDev& v, F3 position, unsigned raw0, int ptr0v,
                                        int lin0, float inv_vs, BlockCache& bc) {
   VoxelSample out;
-  const float vs = v.t.vs;
-  F3 pos_dual = position - f3(vs * 0.5f, vs * 0.5f, vs * 0.5f);
-  F3 vp = position * inv_vs;
-  F3 wt = f3(vp.x - floorf(vp.x), vp.y - floorf(vp.y), vp.z - floorf(vp.z));
-  int gx[2], gy[2], gz[2];
-  gx[0] = vindex_fast(pos_dual.x, inv_vs);
-  gx[1] = vindex_fast(pos_dual.x + vs, inv_vs);
-  gy[0] = vindex_fast(pos_dual.y, inv_vs);
-  gy[1] = vindex_fast(pos_dual.y + vs, inv_vs);
-  gz[0] = vindex_fast(pos_dual.z, inv_vs);
-  gz[1] = vindex_fast(pos_dual.z + vs, inv_vs);
-  const bool one_block = blk_of(gx[0]) == blk_of(gx[1]) && blk_of(gy[0]) == blk_of(gy[1]) &&
-                         blk_of(gz[0]) == blk_of(gz[1]);
-  int ptrb = 0;
-  if (one_block) ptrb = block_ptr(v, blk_of(gx[0]), blk_of(gy[0]), blk_of(gz[0]), bc);
+  const F3 q = position * inv_vs;
+  const float fx = floorf(q.x), fy = floorf(q.y), fz = floorf(q.z);
+  const F3 wt = f3(q.x - fx, q.y - fy, q.z - fz);
+  const int gx = (int)fx, gy = (int)fy, gz = (int)fz;
+  const int lx = gx & 7, ly = gy & 7, lz = gz & 7;
+  const bool cx = lx == 7, cy = ly == 7, cz = lz == 7;
+  CellBlocks cb;
+  cell_blocks(v, gx >> 3, gy >> 3, gz >> 3, cx, cy, cz, bc, cb);
   const uchar4 c0 = (COLOR && v.colors && ptr0v >= 0)
                         ? v.colors[(size_t)ptr0v * kBlockVox + lin0] : make_uchar4(0, 0, 0, 0);
-  float dist = 0.0f, cr = 0.0f, cg = 0.0f, cb = 0.0f;
+  float dist = 0.0f, cr = 0.0f, cg = 0.0f, cb_ = 0.0f;
   const float s0 = s16(raw0, v.t.trunc);
   const int off[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1},
                          {1, 1, 0}, {0, 1, 1}, {1, 0, 1}, {1, 1, 1}};
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
     const int ox = off[k][0], oy = off[k][1], oz = off[k][2];
-    const int ptr = one_block ? ptrb
-                              : block_ptr(v, blk_of(gx[ox]), blk_of(gy[oy]), blk_of(gz[oz]), bc);
-    const int lin = lin_of(gx[ox], gy[oy], gz[oz]);
+    const int ptr = corner_block(cb, cx, cy, cz, ox, oy, oz);
+    const int lin = (((lx + ox) & 7) << 6) | (((ly + oy) & 7) << 3) | ((lz + oz) & 7);
     const unsigned r = load16(v, ptr, lin);
     const bool use0 = w16(r) == 0;
     const float a = ox ? wt.x : 1.0f - wt.x;
@@ -621,14 +646,14 @@ __device__ inline VoxelSample interp16(const VolumeDev& v, F3 position, unsigned
                                               : make_uchar4(0, 0, 0, 0));
       cr += (float)cc.x * coef;
       cg += (float)cc.y * coef;
-      cb += (float)cc.z * coef;
+      cb_ += (float)cc.z * coef;
     }
   }
   out.sdf = dist;
   out.w = w16(raw0);
   out.r = cr;
   out.g = cg;
-  out.b = cb;
+  out.b = cb_;
   return out;
 }
 
