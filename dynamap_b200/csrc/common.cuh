@@ -110,6 +110,16 @@ __device__ inline F3 point3d(int i, float depth, const DSensor& s) {
   p.y = ((float)v - s.cy) * p.z / s.fy;
   return p;
 }
+// getPoint3d for pixel (u, v) known as coordinates: the same arithmetic
+// without recovering them from the linear index.
+__device__ inline F3 point3d_uv(int u, int v, float depth, const DSensor& s) {
+  F3 p;
+  p.z = depth;
+  p.x = ((float)u - s.cx) * p.z / s.fx;
+  p.y = ((float)v - s.cy) * p.z / s.fy;
+  return p;
+}
+
 // Project, utils.h:114-119; non-finite coordinates are rejected (the
 // reference converts them to int unchecked).
 __device__ inline bool project(F3 p, const DSensor& s, int* px, int* py) {

@@ -304,8 +304,10 @@ __device__ bool gn_update(const double* acc, const IcpParams& P, int it, IcpStat
   return conv;
 }
 
+// Blocks of a level's reduction: about four pixels per thread (fewer
+// partial sums to combine than one pixel per thread), at most kIcpMaxBlocks.
 inline __host__ __device__ int icp_grid(int n) {
-  int g = (n + kIcpThreads - 1) / kIcpThreads;
+  int g = (n + 4 * kIcpThreads - 1) / (4 * kIcpThreads);
   if (g > kIcpMaxBlocks) g = kIcpMaxBlocks;
   if (g < 1) g = 1;
   return g;

@@ -52,6 +52,9 @@ constexpr int BTX = 32, BTY = 8;
 // values).  The range weight uses dyn_expf, the same operation sequence the
 // oracle runs, so the filtered depth is bit-identical to the oracle's.  Taps
 // outside the image or with depth <= 0 are skipped; invalid centres stay 0.
+// FAST (mixed-precision sessions): the range weight from the hardware
+// exponential (__expf) instead of dyn_expf.
+template <bool FAST>
 __device__ inline void bilateral_tile(const float* __restrict__ src, float* __restrict__ dst,
                                       int rows, int cols, const BilateralTable& tb, int bx,
                                       int by, float* tile) {
@@ -84,7 +87,8 @@ __device__ inline void bilateral_tile(const float* __restrict__ src, float* __re
       if (ny < 0 || ny >= cols) continue;
       float nv = trow[j];
       if (!(nv > 0.0f)) continue;
-      float gi = range_weight(nv - c, inv2s2, norm);
+      const float dn = nv - c;
+      float gi = FAST ? __expf(-(dn * dn) * inv2s2) * norm : range_weight(dn, inv2s2, norm);
       float w = gi * tb.gs[i * D + j];
       acc += nv * w;
       wp += w;
@@ -96,7 +100,7 @@ __device__ inline void bilateral_tile(const float* __restrict__ src, float* __re
 __global__ void bilateral_kernel(const float* __restrict__ src, float* __restrict__ dst,
                                  int rows, int cols, const __grid_constant__ BilateralTable tb) {
   extern __shared__ float tile[];
-  bilateral_tile(src, dst, rows, cols, tb, blockIdx.x, blockIdx.y, tile);
+  bilateral_tile<false>(src, dst, rows, cols, tb, blockIdx.x, blockIdx.y, tile);
 }
 
 // One 2x pyramid step: mean of the valid depths of each 2x2 cell (fix of
@@ -218,7 +222,10 @@ __global__ void fused_bilateral_kernel(const SessDev* __restrict__ tab) {
   if (!S.bil_enabled) return;
   const int rows = S.ls[0].rows, cols = S.ls[0].cols;
   if ((int)blockIdx.x * BTX >= cols || (int)blockIdx.y * BTY >= rows) return;
-  bilateral_tile(S.raw, S.filt, rows, cols, *S.btab, blockIdx.x, blockIdx.y, tile);
+  if (S.vol.fp16)  // mixed-precision session
+    bilateral_tile<true>(S.raw, S.filt, rows, cols, *S.btab, blockIdx.x, blockIdx.y, tile);
+  else
+    bilateral_tile<false>(S.raw, S.filt, rows, cols, *S.btab, blockIdx.x, blockIdx.y, tile);
 }
 
 // level l of the source (target == 0) or target pyramid from level l-1

@@ -289,6 +289,8 @@ __device__ inline void integrate_voxel(const VolumeDev& v, const float* __restri
   F3 vp = f3(position.x + (float)bx * vs, position.y + (float)by * vs,
              position.z + (float)bz * vs);
   vp = xform(invT, vp);
+  // pixel, depth gate and band decide which voxels a frame updates: IEEE
+  // arithmetic in both forms, so that the mixed form's weights stay exact
   int px, py;
   if (!project(vp, s, &px, &py)) return;
   if (!(px >= 0 && py >= 0 && px < s.cols && py < s.rows)) return;
@@ -296,7 +298,7 @@ __device__ inline void integrate_voxel(const VolumeDev& v, const float* __restri
   const float d = __ldg(depth + idx);
   if (d < t.dmin) return;
   if (d > t.dmax) return;
-  F3 p3 = point3d(idx, d, s);
+  F3 p3 = point3d_uv(px, py, d, s);
   float sd = norm3(p3);
   float vd = norm3(vp);
   float sdf;
@@ -318,13 +320,14 @@ __device__ inline void integrate_voxel(const VolumeDev& v, const float* __restri
         __half2float(__ushort_as_half((unsigned short)(raw & 0xffffu))) * t.trunc;
     const int w = (int)(raw >> 16);
     const float fw = (float)w;
-    const float nsdf = (osdf * fw + sdf * 1.0f) / (fw + 1.0f);
+    const float nsdf = __fdividef(osdf * fw + sdf, fw + 1.0f);
     int nw = w + 1;
     if (nw > t.max_w) nw = t.max_w;
-    v.vox16[vi] =
-        (unsigned)__half_as_ushort(__float2half_rn(nsdf / t.trunc)) | ((unsigned)nw << 16);
+    v.vox16[vi] = (unsigned)__half_as_ushort(__float2half_rn(__fdividef(nsdf, t.trunc))) |
+                  ((unsigned)nw << 16);
     if (v.colors) {
       uchar4 c = v.colors[vi];
+      // colour exactly as the FP32 form (truncated to bytes)
       c.x = (uint8_t)(((float)c.x * fw + (float)c0 * 1.0f) / (fw + 1.0f));
       c.y = (uint8_t)(((float)c.y * fw + (float)c1 * 1.0f) / (fw + 1.0f));
       c.z = (uint8_t)(((float)c.z * fw + (float)c2 * 1.0f) / (fw + 1.0f));
