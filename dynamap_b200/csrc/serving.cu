@@ -3,6 +3,7 @@
 // released at any time under an HBM budget, every step fusing the frames
 // that are waiting into one launch per stage).  No counterpart in the
 // reference, whose builder drives one stream.
+#include <algorithm>
 #include <cstdio>
 #include <mutex>
 #include <new>
@@ -58,15 +59,53 @@ dyn_status dyn_batch_create(dyn_session* const* sessions, int32_t n, dyn_batch**
       cudaEventCreateWithFlags(&b->h2d_done, cudaEventDisableTiming) != cudaSuccess ||
       cudaMallocHost(&b->h_res, sizeof(ResultBlock) * (size_t)n) != cudaSuccess)
     r = DYN_ERR_CUDA;
+  // members in decreasing image size, split into runs of about equal pixel
+  // count (one run per 8 members, at most kMaxGroups): sessions of a group
+  // have similar grids, and the groups' streams overlap each other's tails
+  std::vector<int> order((size_t)n);
+  for (int i = 0; i < n; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int c) { return sessions[a]->npx > sessions[c]->npx; });
+  const int k = std::max(1, std::min(kMaxGroups, n / 8));
+  std::vector<int> start(k + 1, n);
+  {
+    double total = 0.0, acc = 0.0;
+    for (int i = 0; i < n; ++i) total += (double)sessions[i]->npx;
+    int g = 1;
+    start[0] = 0;
+    for (int j = 0; j < n && g < k; ++j) {
+      acc += (double)sessions[order[j]]->npx;
+      // close group g-1 once it holds its share (leaving a member per later group)
+      if (acc >= total * g / k && j + 1 <= n - (k - g)) start[g++] = j + 1;
+    }
+    for (; g < k; ++g) start[g] = std::max(start[g - 1] + 1, n - (k - g));
+    start[k] = n;
+  }
   if (r == DYN_OK) r = dalloc((void**)&b->d_tab, sizeof(SessDev) * (size_t)n);
+  if (r == DYN_OK) r = dalloc((void**)&b->d_map, sizeof(int) * (size_t)n);
   if (r == DYN_OK) r = dalloc((void**)&b->d_gvis, sizeof(int2) * (size_t)cap);
-  if (r == DYN_OK) r = dalloc((void**)&b->d_gcount, sizeof(int));
+  if (r == DYN_OK) r = dalloc((void**)&b->d_gcount, sizeof(int) * kMaxGroups);
   if (r == DYN_OK) r = dalloc((void**)&b->d_res, sizeof(ResultBlock) * (size_t)n);
+  for (int g = 1; g < k && r == DYN_OK; ++g)
+    if (cudaStreamCreateWithFlags(&b->groups.st[g], cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->groups.join[g], cudaEventDisableTiming) != cudaSuccess)
+      r = DYN_ERR_CUDA;
+  if (r == DYN_OK &&
+      cudaEventCreateWithFlags(&b->groups.fork, cudaEventDisableTiming) != cudaSuccess)
+    r = DYN_ERR_CUDA;
+  std::vector<dyn_session*> sorted((size_t)n);
   if (r == DYN_OK) {
     std::vector<SessDev> tab((size_t)n);
-    for (int i = 0; i < n; ++i) tab[i] = sessions[i]->hsd;
+    std::vector<int> map((size_t)n);
+    for (int j = 0; j < n; ++j) {
+      sorted[j] = sessions[order[j]];
+      tab[j] = sorted[j]->hsd;
+      map[j] = order[j];
+    }
     if (cudaMemcpyAsync(b->d_tab, tab.data(), sizeof(SessDev) * (size_t)n,
                         cudaMemcpyHostToDevice, b->stream) != cudaSuccess ||
+        cudaMemcpyAsync(b->d_map, map.data(), sizeof(int) * (size_t)n, cudaMemcpyHostToDevice,
+                        b->stream) != cudaSuccess ||
         cudaEventRecord(b->h2d_done, b->stream) != cudaSuccess ||
         cudaStreamSynchronize(b->stream) != cudaSuccess)
       r = DYN_ERR_CUDA;
@@ -76,7 +115,27 @@ dyn_status dyn_batch_create(dyn_session* const* sessions, int32_t n, dyn_batch**
     release(b);
     return r;
   }
-  b->shape = make_shape(sessions, n, b->d_gvis, b->d_gcount, (int)cap);
+  FrameGroups& G = b->groups;
+  G.k = k;
+  G.st[0] = b->stream;
+  int64_t voff = 0;
+  for (int g = 0; g < k; ++g) {
+    const int n_g = start[g + 1] - start[g];
+    int64_t cap_g = 0;
+    for (int j = start[g]; j < start[g + 1]; ++j) cap_g += sorted[j]->tp.num_blocks;
+    G.tab[g] = b->d_tab + start[g];
+    G.map[g] = b->d_map + start[g];
+    G.shape[g] = make_shape(sorted.data() + start[g], n_g, b->d_gvis + voff, b->d_gcount + g,
+                            (int)cap_g);
+    voff += cap_g;
+  }
+  FrameGroups& one = b->single;
+  one.k = 1;
+  one.st[0] = b->stream;
+  one.tab[0] = b->d_tab;
+  one.map[0] = b->d_map;
+  one.shape[0] = make_shape(sorted.data(), n, b->d_gvis, b->d_gcount, (int)cap);
+  b->shape = one.shape[0];
   for (int i = 0; i < n; ++i) sessions[i]->batch = b;
   *out = b;
   return DYN_OK;
@@ -100,8 +159,10 @@ static dyn_status batch_launch(dyn_batch* b) {
     m.on = b->profile;
     m.ev = b->ev;
     m.st = b->stream;
-    dyn_status r = capture_frame(b->d_tab, b->shape, b->d_res, b->h_res, b->stream, m, &b->exec,
-                                 &b->kernels_per_frame);
+    // a profiled frame runs as one group, so that stage boundaries are
+    // those of the whole batch
+    dyn_status r = capture_groups(b->profile ? b->single : b->groups, b->d_res, b->h_res, b->n,
+                                  m, &b->exec, &b->kernels_per_frame);
     if (r != DYN_OK) return r;
   }
   DYN_CUDA(cudaGraphLaunch(b->exec, b->stream));

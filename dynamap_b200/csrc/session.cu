@@ -36,6 +36,11 @@ void release(dyn_batch* b) {
   for (dyn_session* s : b->ss)
     if (s && s->batch == b) s->batch = nullptr;
   if (b->exec) cudaGraphExecDestroy(b->exec);
+  for (int g = 1; g < kMaxGroups; ++g) {
+    if (b->groups.st[g]) cudaStreamDestroy(b->groups.st[g]);
+    if (b->groups.join[g]) cudaEventDestroy(b->groups.join[g]);
+  }
+  if (b->groups.fork) cudaEventDestroy(b->groups.fork);
   for (void* p : b->allocs) cudaFree(p);
   if (b->h_res) cudaFreeHost(b->h_res);
   if (b->h2d_done) cudaEventDestroy(b->h2d_done);
@@ -158,19 +163,31 @@ void enqueue_frame(const SessDev* tab, const BatchShape& b, const int* slot_map,
   m(DYN_STAGE_ICP);
   enqueue_map_update(tab, b, st, m);
   gather_results_kernel<<<b.n, 128, 0, st>>>(tab, b.n, slot_map, res_dev);
-  cudaMemcpyAsync(res_host, res_dev, sizeof(ResultBlock) * (size_t)n_results,
-                  cudaMemcpyDeviceToHost, st);
+  if (res_host)
+    cudaMemcpyAsync(res_host, res_dev, sizeof(ResultBlock) * (size_t)n_results,
+                    cudaMemcpyDeviceToHost, st);
 }
 
-// Captures one frame of 'tab' on 'st' into an executable graph.
-dyn_status capture_frame(const SessDev* tab, const BatchShape& b, ResultBlock* res_dev,
-                         ResultBlock* res_host, cudaStream_t st, const Marks& m,
-                         cudaGraphExec_t* exec_out, int* kernels_out) {
-  cudaGraph_t g = nullptr;
-  DYN_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-  enqueue_frame(tab, b, nullptr, res_dev, res_host, b.n, st, m);
-  cudaError_t e = cudaStreamEndCapture(st, &g);
-  if (e != cudaSuccess) return DYN_ERR_CUDA;
+void enqueue_groups(const FrameGroups& G, ResultBlock* res_dev, ResultBlock* res_host,
+                    int n_results, const Marks& m) {
+  cudaStream_t main = G.st[0];
+  if (G.k > 1) {
+    cudaEventRecord(G.fork, main);
+    for (int g = 1; g < G.k; ++g) cudaStreamWaitEvent(G.st[g], G.fork, 0);
+  }
+  for (int g = 0; g < G.k; ++g)
+    enqueue_frame(G.tab[g], G.shape[g], G.map[g], res_dev, nullptr, 0, G.st[g],
+                  g == 0 ? m : Marks());
+  for (int g = 1; g < G.k; ++g) {
+    cudaEventRecord(G.join[g], G.st[g]);
+    cudaStreamWaitEvent(main, G.join[g], 0);
+  }
+  cudaMemcpyAsync(res_host, res_dev, sizeof(ResultBlock) * (size_t)n_results,
+                  cudaMemcpyDeviceToHost, main);
+}
+
+// Kernel nodes of a captured graph, then its executable form.
+static dyn_status instantiate(cudaGraph_t g, cudaGraphExec_t* exec_out, int* kernels_out) {
   size_t nn = 0;
   cudaGraphGetNodes(g, nullptr, &nn);
   std::vector<cudaGraphNode_t> nodes(nn);
@@ -182,11 +199,32 @@ dyn_status capture_frame(const SessDev* tab, const BatchShape& b, ResultBlock* r
   }
   *kernels_out = nk;
   cudaGraphExec_t ex = nullptr;
-  e = cudaGraphInstantiate(&ex, g, 0);
+  const cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return DYN_ERR_CUDA;
   *exec_out = ex;
   return DYN_OK;
+}
+
+dyn_status capture_groups(const FrameGroups& G, ResultBlock* res_dev, ResultBlock* res_host,
+                          int n_results, const Marks& m, cudaGraphExec_t* exec_out,
+                          int* kernels_out) {
+  cudaGraph_t g = nullptr;
+  DYN_CUDA(cudaStreamBeginCapture(G.st[0], cudaStreamCaptureModeThreadLocal));
+  enqueue_groups(G, res_dev, res_host, n_results, m);
+  if (cudaStreamEndCapture(G.st[0], &g) != cudaSuccess) return DYN_ERR_CUDA;
+  return instantiate(g, exec_out, kernels_out);
+}
+
+// Captures one frame of 'tab' on 'st' into an executable graph.
+dyn_status capture_frame(const SessDev* tab, const BatchShape& b, ResultBlock* res_dev,
+                         ResultBlock* res_host, cudaStream_t st, const Marks& m,
+                         cudaGraphExec_t* exec_out, int* kernels_out) {
+  cudaGraph_t g = nullptr;
+  DYN_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  enqueue_frame(tab, b, nullptr, res_dev, res_host, b.n, st, m);
+  if (cudaStreamEndCapture(st, &g) != cudaSuccess) return DYN_ERR_CUDA;
+  return instantiate(g, exec_out, kernels_out);
 }
 
 // The launch shape of a table of sessions: the largest image, level and

@@ -198,11 +198,28 @@ struct dyn_session {
 // A fixed set of sessions on one device whose frames run together: each
 // stage is one launch over the members' descriptor table and the whole frame
 // one CUDA graph on the batch's stream.
+// A table of sessions split into groups, each group's fused stage chain on
+// its own stream (group 0 on the caller's stream): groups overlap the
+// tails of each other's launches.
+constexpr int kMaxGroups = 4;
+struct FrameGroups {
+  int k = 1;
+  const SessDev* tab[kMaxGroups] = {};  // group sub-tables (device)
+  const int* map[kMaxGroups] = {};      // group-local index -> result index (device)
+  BatchShape shape[kMaxGroups];
+  cudaStream_t st[kMaxGroups] = {};     // st[0]: the caller's stream
+  cudaEvent_t fork = nullptr;
+  cudaEvent_t join[kMaxGroups] = {};
+};
+
 struct dyn_batch {
   int device = 0;
   int n = 0;
   std::vector<dyn_session*> ss;
   cudaStream_t stream = nullptr;
+  FrameGroups groups;     // members in size order, split into groups
+  FrameGroups single;     // all members as one group (profiled frames)
+  int* d_map = nullptr;   // table position -> member index
   cudaEvent_t h2d_done = nullptr;
   std::vector<void*> allocs;
   SessDev* d_tab = nullptr;
@@ -268,6 +285,13 @@ void enqueue_frame(const SessDev* tab, const BatchShape& b, const int* slot_map,
 dyn_status capture_frame(const SessDev* tab, const BatchShape& b, ResultBlock* res_dev,
                          ResultBlock* res_host, cudaStream_t st, const Marks& m,
                          cudaGraphExec_t* exec_out, int* kernels_out);
+// One frame of every group (fork from and join back into G.st[0]), then
+// n_results entries of res_dev back into res_host; marks on group 0 only.
+void enqueue_groups(const FrameGroups& G, ResultBlock* res_dev, ResultBlock* res_host,
+                    int n_results, const Marks& m);
+dyn_status capture_groups(const FrameGroups& G, ResultBlock* res_dev, ResultBlock* res_host,
+                          int n_results, const Marks& m, cudaGraphExec_t* exec_out,
+                          int* kernels_out);
 void add_stage_times(cudaEvent_t* ev, double* ms_acc, int64_t* frames);
 // Page-locked host memory (read by the copy engines without staging).
 bool is_pinned(const void* p);

@@ -151,3 +151,33 @@ def test_batch_profile_stage_times(gpu_lib, members):
     finally:
         for m in sess:
             m.close()
+
+
+def test_grouped_batch_matches_sessions_alone(gpu_lib):
+    """17 members: the batch splits them into groups on separate streams."""
+    p = configs.preset("cfg1")
+    p["sensor"].update(rows=120, cols=160, fx=131.25, fy=131.25, cx=79.5, cy=59.5)
+    p["tsdf"].update(voxel_size=0.01, truncation_distance=0.04, num_blocks=1 << 13,
+                     num_buckets=1 << 14)
+    n = 17
+    seqs = [configs.sequence(p, seed=90 + i, n_frames=3) for i in range(n)]
+    t, g, b, s = configs.structs(p)
+    precs = [abi.PRECISION_MIXED if i % 3 == 0 else abi.PRECISION_FP32 for i in range(n)]
+    alone = []
+    for i in range(n):
+        with Session(t, g, b, s, precision=precs[i]) as m:
+            m.set_pose(seqs[i].poses[0])
+            alone.append([m.process(d)[0] for d in seqs[i].depth])
+    sess = [Session(t, g, b, s, precision=precs[i]) for i in range(n)]
+    try:
+        for i, m in enumerate(sess):
+            m.set_pose(seqs[i].poses[0])
+        with Batch(sess) as bt:
+            for k in range(3):
+                poses, _, status = bt.process([q.depth[k] for q in seqs])
+                assert status == [0] * n
+                for i in range(n):
+                    assert np.array_equal(poses[i], alone[i][k]), (i, k)
+    finally:
+        for m in sess:
+            m.close()
