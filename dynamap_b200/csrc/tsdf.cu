@@ -590,69 +590,70 @@ __device__ inline bool raycast_exact_px(const VolumeDev& v, const DSensor& s, co
 // ------------------------------------------------------------ mixed-precision raycast
 // The mixed form marches the same ray with the reference's step rule
 // (tsdf.cu:471-526) and trilinear interpolation at every observed sample,
-// on f16 voxels, with voxel indices by multiplying with 1/vs (no
-// exactness check: an index off by one at a voxel boundary moves the sample
-// by under a voxel).  Skipping the interpolation where the sampled voxel is
-// far from the surface was tried and rejected: it changes the step sequence,
-// so the hit moves by up to a voxel and the tracked trajectory drifts by
-// more than a millimetre from the FP32 path.
-__device__ inline int vindex_fast(float p, float inv_vs) {
-  const float sg = (float)((p > 0.0f) - (p < 0.0f));
-  return (int)(p * inv_vs + sg * 0.5f);
-}
+// on f16 voxels, in voxel units with fused multiply-adds and without the
+// exact-rounding checks (a sample's voxel or cell can differ from the
+// reference's at a tie, moving it by under a voxel).  Skipping the
+// interpolation where the sampled voxel is far from the surface was tried
+// and rejected: it changes the step sequence, so the hit moves by up to a
+// voxel and the tracked trajectory drifts by more than a millimetre from
+// the FP32 path.
 __device__ inline unsigned load16(const VolumeDev& v, int ptr, int lin) {
   return ptr < 0 ? 0u : __ldg(v.vox16 + (size_t)ptr * kBlockVox + lin);
 }
-// stored value is sdf / truncation
-__device__ inline float s16(unsigned r, float trunc) {
-  return __half2float(__ushort_as_half((unsigned short)(r & 0xffffu))) * trunc;
-}
 __device__ inline int w16(unsigned r) { return (int)(r >> 16); }
 
-// Trilinear sample of the f16 sdf (and colour) at 'position': the cell's
-// corners are floor(p / vs) and floor(p / vs) + 1 per axis (the reference's
-// rounded p - vs/2 and p + vs/2, up to ties) with weights p/vs - floor(p/vs);
-// unobserved corners take the centre voxel's value (raw0, heap index ptr0v,
-// local index lin0), as GetInterpolatedVoxel does.
+// f16 value of a mixed voxel: sdf / truncation
+__device__ inline float n16(unsigned r) {
+  return __half2float(__ushort_as_half((unsigned short)(r & 0xffffu)));
+}
+
+// Trilinear sample of the f16 sdf (and colour) at q, the sample in voxel
+// units (p / vs): the cell's corners are floor(q) and floor(q) + 1 per axis
+// (the reference's rounded p - vs/2 and p + vs/2, up to ties) with weights
+// q - floor(q); unobserved corners take the centre voxel's value (raw0,
+// heap index ptr0v, local index lin0), as GetInterpolatedVoxel does.  Sums
+// use fused multiply-adds, in units of the truncation distance.
 template <bool COLOR>
-__device__ inline VoxelSample interp16(const VolumeDev& v, F3 position, unsigned raw0, int ptr0v,
-                                       int lin0, float inv_vs, BlockCache& bc) {
+__device__ inline VoxelSample interp16(const VolumeDev& v, F3 q, unsigned raw0, int ptr0v,
+                                       int lin0, BlockCache& bc) {
   VoxelSample out;
-  const F3 q = position * inv_vs;
   const float fx = floorf(q.x), fy = floorf(q.y), fz = floorf(q.z);
-  const F3 wt = f3(q.x - fx, q.y - fy, q.z - fz);
+  const float wx = q.x - fx, wy = q.y - fy, wz = q.z - fz;
   const int gx = (int)fx, gy = (int)fy, gz = (int)fz;
   const int lx = gx & 7, ly = gy & 7, lz = gz & 7;
   const bool cx = lx == 7, cy = ly == 7, cz = lz == 7;
   CellBlocks cb;
   cell_blocks(v, gx >> 3, gy >> 3, gz >> 3, cx, cy, cz, bc, cb);
+  // local index of the low corner and the steps to the high ones (wrapping
+  // into the next block where the cell crosses)
+  const int base = (lx << 6) | (ly << 3) | lz;
+  const int dx = cx ? -448 : 64, dy = cy ? -56 : 8, dz = cz ? -7 : 1;
   const uchar4 c0 = (COLOR && v.colors && ptr0v >= 0)
                         ? v.colors[(size_t)ptr0v * kBlockVox + lin0] : make_uchar4(0, 0, 0, 0);
+  const float n0 = n16(raw0);
+  // weight products per (x, y) pair, then times the z weight
+  const float ax[2] = {1.0f - wx, wx}, ay[2] = {1.0f - wy, wy}, az[2] = {1.0f - wz, wz};
   float dist = 0.0f, cr = 0.0f, cg = 0.0f, cb_ = 0.0f;
-  const float s0 = s16(raw0, v.t.trunc);
   const int off[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1},
                          {1, 1, 0}, {0, 1, 1}, {1, 0, 1}, {1, 1, 1}};
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
     const int ox = off[k][0], oy = off[k][1], oz = off[k][2];
     const int ptr = corner_block(cb, cx, cy, cz, ox, oy, oz);
-    const int lin = (((lx + ox) & 7) << 6) | (((ly + oy) & 7) << 3) | ((lz + oz) & 7);
+    const int lin = base + (ox ? dx : 0) + (oy ? dy : 0) + (oz ? dz : 0);
     const unsigned r = load16(v, ptr, lin);
     const bool use0 = w16(r) == 0;
-    const float a = ox ? wt.x : 1.0f - wt.x;
-    const float b = oy ? wt.y : 1.0f - wt.y;
-    const float c = oz ? wt.z : 1.0f - wt.z;
-    const float coef = a * b * c;
-    dist += coef * (use0 ? s0 : s16(r, v.t.trunc));
+    const float coef = (ax[ox] * ay[oy]) * az[oz];
+    dist = __fmaf_rn(coef, use0 ? n0 : n16(r), dist);
     if (COLOR && v.colors) {
       const uchar4 cc = use0 ? c0 : (ptr >= 0 ? v.colors[(size_t)ptr * kBlockVox + lin]
                                               : make_uchar4(0, 0, 0, 0));
-      cr += (float)cc.x * coef;
-      cg += (float)cc.y * coef;
-      cb_ += (float)cc.z * coef;
+      cr = __fmaf_rn((float)cc.x, coef, cr);
+      cg = __fmaf_rn((float)cc.y, coef, cg);
+      cb_ = __fmaf_rn((float)cc.z, coef, cb_);
     }
   }
-  out.sdf = dist;
+  out.sdf = dist * v.t.trunc;
   out.w = w16(raw0);
   out.r = cr;
   out.g = cg;
@@ -660,6 +661,10 @@ __device__ inline VoxelSample interp16(const VolumeDev& v, F3 position, unsigned
   return out;
 }
 
+// The march of the mixed form in voxel units: the sample at depth z is
+// o + z * d with o the camera centre and d the pixel's ray direction per
+// unit depth (both divided by vs), by fused multiply-adds; its voxel is
+// floor(q + 0.5).
 __device__ inline bool raycast_mixed_px(const VolumeDev& v, const DSensor& s, const M4f& T, int x,
                                         int y, float* __restrict__ depth_out,
                                         uint8_t* __restrict__ rgb_out) {
@@ -667,31 +672,32 @@ __device__ inline bool raycast_mixed_px(const VolumeDev& v, const DSensor& s, co
   const DTsdf& t = v.t;
   const float inv_vs = 1.0f / t.vs;
   const float axf = ((float)x - s.cx) / s.fx, ayf = ((float)y - s.cy) / s.fy;
+  const F3 o = f3(T.m[3] * inv_vs, T.m[7] * inv_vs, T.m[11] * inv_vs);
+  const F3 d = f3((T.m[0] * axf + T.m[1] * ayf + T.m[2]) * inv_vs,
+                  (T.m[4] * axf + T.m[5] * ayf + T.m[6]) * inv_vs,
+                  (T.m[8] * axf + T.m[9] * ayf + T.m[10]) * inv_vs);
   BlockCache bc;
   bc.x = bc.y = bc.z = 0x7fffffff;
   bc.ptr = -1;
   float cur = 0.0f;
   int steps = 0;
   bool over = false;
-  int ptr = -1, lin = 0;
-  unsigned raw = 0;
-  F3 point;
   while (cur < t.dmax) {
     if (steps++ >= t.rc_cap) {
       over = true;
       break;
     }
-    point = xform(T, f3(axf * cur, ayf * cur, cur));
-    const int gx = vindex_fast(point.x, inv_vs), gy = vindex_fast(point.y, inv_vs),
-              gz = vindex_fast(point.z, inv_vs);
-    ptr = block_ptr(v, blk_of(gx), blk_of(gy), blk_of(gz), bc);
-    lin = lin_of(gx, gy, gz);
-    raw = load16(v, ptr, lin);
+    const F3 q = f3(__fmaf_rn(cur, d.x, o.x), __fmaf_rn(cur, d.y, o.y), __fmaf_rn(cur, d.z, o.z));
+    const int gx = (int)floorf(q.x + 0.5f), gy = (int)floorf(q.y + 0.5f),
+              gz = (int)floorf(q.z + 0.5f);
+    const int ptr = block_ptr(v, blk_of(gx), blk_of(gy), blk_of(gz), bc);
+    const int lin = lin_of(gx, gy, gz);
+    const unsigned raw = load16(v, ptr, lin);
     if (w16(raw) == 0) {
       cur += t.trunc;
       continue;
     }
-    VoxelSample vx = interp16<false>(v, point, raw, ptr, lin, inv_vs, bc);
+    VoxelSample vx = interp16<false>(v, q, raw, ptr, lin, bc);
     cur += vx.sdf;
     if (vx.sdf < t.vs) break;
   }
@@ -699,14 +705,15 @@ __device__ inline bool raycast_mixed_px(const VolumeDev& v, const DSensor& s, co
   if (rgb_out) {
     uint8_t r = 0, g = 0, b = 0;
     if (cur < t.dmax) {
-      point = xform(T, f3(axf * cur, ayf * cur, cur));
-      const int gx = vindex_fast(point.x, inv_vs), gy = vindex_fast(point.y, inv_vs),
-                gz = vindex_fast(point.z, inv_vs);
-      ptr = block_ptr(v, blk_of(gx), blk_of(gy), blk_of(gz), bc);
-      lin = lin_of(gx, gy, gz);
-      raw = load16(v, ptr, lin);
+      const F3 q =
+          f3(__fmaf_rn(cur, d.x, o.x), __fmaf_rn(cur, d.y, o.y), __fmaf_rn(cur, d.z, o.z));
+      const int gx = (int)floorf(q.x + 0.5f), gy = (int)floorf(q.y + 0.5f),
+                gz = (int)floorf(q.z + 0.5f);
+      const int ptr = block_ptr(v, blk_of(gx), blk_of(gy), blk_of(gz), bc);
+      const int lin = lin_of(gx, gy, gz);
+      const unsigned raw = load16(v, ptr, lin);
       if (w16(raw) != 0) {
-        VoxelSample vx = interp16<true>(v, point, raw, ptr, lin, inv_vs, bc);
+        VoxelSample vx = interp16<true>(v, q, raw, ptr, lin, bc);
         r = (uint8_t)vx.r;
         g = (uint8_t)vx.g;
         b = (uint8_t)vx.b;
