@@ -135,10 +135,12 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def algorithmic_bytes(stage: str, st_avg: dict, P: int, bsz: int, levels_iters, rgb: bool):
+def algorithmic_bytes(stage: str, st_avg: dict, P: int, bsz: int, levels_iters, rgb: bool,
+                      Sv: int = 8):
     """Bytes a kernel must move per launch (the per-unit figures of the
-    design's measurement section), from the run's own counters."""
-    Sv = 8
+    design's measurement section), from the run's own counters.  Sv = voxel
+    bytes: 8 for the FP32 form, 4 for the mixed form (8 when it keeps
+    colour)."""
     if stage == "integrate":
         return st_avg["blocks_visible"] * (16 + 2 * 512 * Sv) + 4 * P + (3 * P if rgb else 0)
     if stage == "raycast":
@@ -402,12 +404,13 @@ def run_ours(args):
     lv = [(P >> (2 * {1: 0, 2: 1, 4: 2, 8: 3}[p["gn"]["lvl_scale"][k]]), iters[k]) for k in range(3)]
     kernel_stages = [k for k in abi.STAGES if k != "frame"]
     dom = max(kernel_stages, key=lambda k: stage_ms[k])
-    alg = algorithmic_bytes(dom, st_avg, P, t.bucket_size, lv, has_rgb)
+    Sv = 8 if (prec == abi.PRECISION_FP32 or g.color_weight != 0.0) else 4
+    alg = algorithmic_bytes(dom, st_avg, P, t.bucket_size, lv, has_rgb, Sv)
     hbm, peak_kind = peaks()
     roof = None
     if alg is not None and stage_ms[dom] > 0:
         ach = alg / (stage_ms[dom] / 1e3) / 1e9
-        traffic = read_profile_traffic(dom, st_avg)
+        traffic = read_profile_traffic(dom if prec == abi.PRECISION_FP32 else dom + "_mixed", st_avg)
         roof = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": hbm, "unit": "GB/s",
                 "frac": ach / hbm, "peak_source": f"{peak_kind} hbm_gbs",
                 "algorithmic_bytes_per_launch": alg, "launch_ms": stage_ms[dom],
