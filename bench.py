@@ -33,6 +33,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "agg frames/s + p50/p99 frame latency vs plain FP32 path; ATE/SDF err vs FP64"
+# --precision: the drop-in FP32 form, the mixed form, the mixed form with
+# band allocation (values of dyn_precision)
+PRECISIONS = {"fp32": 0, "mixed": 1, "band": 2}
 
 
 def _render_chunk(args):
@@ -264,7 +267,7 @@ def config_block(args, p):
                         f"2^{int(math.log2(t['num_buckets']))} buckets x {t['bucket_size']}, "
                         f"ICP iters {p['gn']['lvl_iteration_num']} at scales {p['gn']['lvl_scale']}, "
                         f"photometric weight {p['gn']['color_weight']}, "
-                        f"{'FP32' if args.precision == 'fp32' else 'f16/u16 mixed-precision'} TSDF, "
+                        f"{ {'fp32': 'FP32', 'mixed': 'f16/u16 mixed-precision', 'band': 'f16/u16 mixed-precision band-allocated'}[args.precision]} TSDF, "
                         "frame-to-model",
             "sessions_per_gpu": 1, "precision": args.precision, "seed": args.seed,
             "l2": "inputs larger than L2: the TSDF working set (voxel pool "
@@ -293,7 +296,7 @@ def run_ours(args):
         p["tsdf"]["num_blocks"] = min(p["tsdf"]["num_blocks"], args.max_blocks)
     t, g, b, s = configs.structs(p)
     lib = abi.load()
-    prec = abi.PRECISION_MIXED if args.precision == "mixed" else abi.PRECISION_FP32
+    prec = PRECISIONS[args.precision]
     P = s.rows * s.cols
     has_rgb = rgb is not None
     d_dev = torch.from_numpy(depth).cuda()
@@ -470,7 +473,7 @@ def run_batched(args):
     torch.cuda.set_device(local)
     ranks = Ranks()  # each GPU runs its own session mix: weak scaling
     lib = abi.load()
-    prec = abi.PRECISION_MIXED if args.precision == "mixed" else abi.PRECISION_FP32
+    prec = PRECISIONS[args.precision]
     structs = [configs.structs(p) for _, p, _ in mix]
     dev_frames = [torch.from_numpy(d).cuda() for d, _, _ in frames]
     nbytes = [d.shape[1] * d.shape[2] * 2 for d, _, _ in frames]
@@ -657,7 +660,7 @@ def run_serving(args):
     pinned = {k: torch.from_numpy(v[0]).pin_memory() for k, v in pools.items()}
     pin_np = {k: v.numpy() for k, v in pinned.items()}
     structs = {k: configs.structs(configs.serving_kind(k, n_pool)) for k in kinds}
-    prec = abi.PRECISION_MIXED if args.precision == "mixed" else abi.PRECISION_FP32
+    prec = PRECISIONS[args.precision]
     sv = Server(budget_bytes=int(S["budget_gb"] * 1e9), max_sessions=1024, device=local)
     fps = S["fps"]
     waiting, active = [], {}
@@ -774,9 +777,10 @@ def main():
     ap.add_argument("--sessions", type=int, default=32, help="sessions per GPU (cfg3)")
     ap.add_argument("--serve-seconds", type=float, default=40.0,
                     help="arrival window of the serving run (cfg4)")
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "mixed"],
+    ap.add_argument("--precision", default="fp32", choices=sorted(PRECISIONS),
                     help="fp32: the drop-in path; mixed: f16/u16 voxels, compensated "
-                         "normal equations, fast raycast")
+                         "normal equations, fast raycast; band: mixed with band-limited "
+                         "allocation (no free-space carving)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

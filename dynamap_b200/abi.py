@@ -25,6 +25,7 @@ STAGES = ["ingest", "bilateral", "source_maps", "icp", "allocate", "visible", "i
           "raycast", "target_maps", "frame"]
 PRECISION_FP32 = 0
 PRECISION_MIXED = 1
+PRECISION_MIXED_BAND = 2
 
 
 class Sensor(C.Structure):

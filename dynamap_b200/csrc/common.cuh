@@ -37,6 +37,7 @@ struct DTsdf {
   int num_blocks;
   int max_w;
   int dda_cap;       // DDA step bound (3*ceil((dmax+trunc)/bsm)+8)
+  int band;          // allocation rays start a truncation distance before the surface
   int rc_cap;        // raycast step bound (ceil(dmax/min(vs,trunc))+4)
 };
 

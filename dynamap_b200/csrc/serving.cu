@@ -422,7 +422,7 @@ dyn_status dyn_server_admit(dyn_server* sv, const dyn_tsdf_params* tsdf, const d
     if (!sv->slots[i].s) slot = i;
   if (slot < 0) return DYN_ERR_BUDGET_EXCEEDED;
   const size_t bytes = session_bytes(*tsdf, *sensor, precision,
-                                     precision == DYN_PRECISION_MIXED ? mixed_colour(gn) : true);
+                                     precision != DYN_PRECISION_FP32 ? mixed_colour(gn) : true);
   if (sv->used + bytes > sv->budget) return DYN_ERR_BUDGET_EXCEEDED;
   dyn_session* s = nullptr;
   dyn_status r = dyn_session_create(tsdf, gn, bil, sensor, precision, sv->device, &s);

@@ -41,6 +41,8 @@ struct SessDev {
   float* tint[kLevels];
   float* ray;
   uint8_t* trgb;
+  unsigned* rbound;     // band sessions: ray-start bound per 8x8 tile (float
+  int rb_tx, rb_ty;     // bits), rb_tx x rb_ty tiles; null otherwise
   const BilateralTable* btab;  // device copy
   // solver
   IcpState* icp;
@@ -66,6 +68,7 @@ struct BatchShape {
   int max_slot_px[3];      // largest pixel count of each ICP level slot
   int max_slot_iters[3];   // largest lvl_iteration_num of each slot
   int max_bil_radius;      // 0: no session filters
+  int max_rb_tiles;        // largest ray-start bound (tiles; at least 1)
   int kahan_mask;          // bit 0: some session sums plainly, bit 1: some use Kahan sums
   int fp16_mask;           // bit 0: some session keeps FP32 voxels, bit 1: some mixed
   int2* gvis;              // batch-wide visible list (session, heap index)

@@ -251,6 +251,7 @@ BatchShape make_shape(dyn_session* const* ss, int n, int2* gvis, int* gcount, in
       b.max_slot_iters[pl] = std::max(b.max_slot_iters[pl], s->gp.lvl_iteration_num[pl]);
     }
     if (s->bp.enabled) b.max_bil_radius = std::max(b.max_bil_radius, s->btab.radius);
+    b.max_rb_tiles = std::max(b.max_rb_tiles, std::max(1, s->rb_tx * s->rb_ty));
     b.kahan_mask |= s->icp_params().kahan ? 2 : 1;
     b.fp16_mask |= s->vol.fp16 ? 2 : 1;
   }
@@ -286,6 +287,9 @@ void fill_sessdev(dyn_session* s) {
   }
   d.ray = s->d_ray;
   d.trgb = s->d_trgb;
+  d.rbound = s->d_rbound;
+  d.rb_tx = s->rb_tx;
+  d.rb_ty = s->rb_ty;
   d.btab = s->d_btab;
   d.icp = s->d_icp;
   d.pose = s->d_pose;
@@ -446,12 +450,14 @@ size_t session_bytes(const dyn_tsdf_params& t, const dyn_sensor& s, int precisio
   size_t b = 0;
   b += sizeof(Entry) * (size_t)t.num_buckets * t.bucket_size;
   b += sizeof(unsigned long long) * (size_t)t.num_blocks;
-  if (precision == DYN_PRECISION_MIXED)
+  if (precision != DYN_PRECISION_FP32)
     b += (4 + (colour ? 4 : 0)) * (size_t)t.num_blocks * kBlockVox;
   else
     b += sizeof(dyn_voxel) * (size_t)t.num_blocks * kBlockVox;
   b += sizeof(int2) * (size_t)t.num_blocks;  // visible list
   b += n * (2 + 3 + 4 + 4 + 4 + 3);  // inputs, raw, filtered, ray depth, target rgb
+  if (precision == DYN_PRECISION_MIXED_BAND)
+    b += 4 * (size_t)((s.rows + 7) / 8) * ((s.cols + 7) / 8) + 256;  // ray-start bound
   b += 2 * n * (4 + 16 + 16 + 4) * 4 / 3;  // source + target pyramids
   b += icp_scratch_bytes() + sizeof(SessDev) + sizeof(BilateralTable) + sizeof(ResultBlock) +
        8192;
@@ -509,7 +515,7 @@ dyn_status dyn_session_create(const dyn_tsdf_params* tsdf, const dyn_gn_params* 
   if (!tsdf || !gn || !bil || !valid_sensor(sensor)) return DYN_ERR_INVALID_ARG;
   if (tsdf->block_size != kBlockSize || tsdf->bucket_size < 1 || tsdf->num_buckets < 1 ||
       tsdf->num_blocks < 1 || tsdf->max_sdf_weight < 1 ||
-      tsdf->max_sdf_weight > (precision == DYN_PRECISION_MIXED ? 65535 : 255) ||
+      tsdf->max_sdf_weight > (precision != DYN_PRECISION_FP32 ? 65535 : 255) ||
       !(tsdf->voxel_size > 0) || !(tsdf->truncation_distance > 0) ||
       !(tsdf->max_sensor_depth > 0))
     return DYN_ERR_INVALID_ARG;
@@ -524,7 +530,9 @@ dyn_status dyn_session_create(const dyn_tsdf_params* tsdf, const dyn_gn_params* 
                        !(bil->sigma_i > 0)))
     return DYN_ERR_INVALID_ARG;
   if (gn->mode != 0 && gn->mode != 1) return DYN_ERR_INVALID_ARG;
-  if (precision != DYN_PRECISION_FP32 && precision != DYN_PRECISION_MIXED) return DYN_ERR_INVALID_ARG;
+  if (precision != DYN_PRECISION_FP32 && precision != DYN_PRECISION_MIXED &&
+      precision != DYN_PRECISION_MIXED_BAND)
+    return DYN_ERR_INVALID_ARG;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
     cudaGetLastError();
@@ -586,14 +594,14 @@ dyn_status dyn_session_create(const dyn_tsdf_params* tsdf, const dyn_gn_params* 
   TRY(s->dalloc(&s->d_partials, icp_scratch_bytes()));
   TRY(s->dalloc(&s->d_icp, sizeof(IcpState)));
   TRY(s->dalloc(&s->d_pose, sizeof(PoseState)));
-  s->vol.t = dtsdf(*tsdf);
+  s->vol.t = dtsdf(*tsdf, precision);
   TRY(s->dalloc(&s->vol.entries, sizeof(Entry) * (size_t)tsdf->num_buckets * tsdf->bucket_size));
   TRY(s->dalloc(&s->vol.block_keys, sizeof(unsigned long long) * (size_t)tsdf->num_blocks));
   const size_t nvox = (size_t)tsdf->num_blocks * kBlockVox;
   s->vol.voxels = nullptr;
   s->vol.vox16 = nullptr;
   s->vol.colors = nullptr;
-  s->vol.fp16 = precision == DYN_PRECISION_MIXED ? 1 : 0;
+  s->vol.fp16 = precision != DYN_PRECISION_FP32 ? 1 : 0;
   if (s->vol.fp16) {
     TRY(s->dalloc(&s->vol.vox16, sizeof(unsigned) * nvox));
     if (mixed_colour(gn)) TRY(s->dalloc(&s->vol.colors, sizeof(uchar4) * nvox));
@@ -602,6 +610,11 @@ dyn_status dyn_session_create(const dyn_tsdf_params* tsdf, const dyn_gn_params* 
   }
   TRY(s->dalloc(&s->vol.cnt, sizeof(Counters)));
   TRY(s->dalloc(&s->d_gvis, sizeof(int2) * (size_t)tsdf->num_blocks));
+  if (precision == DYN_PRECISION_MIXED_BAND) {
+    s->rb_tx = ((int)sensor->cols + 7) / 8;
+    s->rb_ty = ((int)sensor->rows + 7) / 8;
+    TRY(s->dalloc(&s->d_rbound, sizeof(unsigned) * (size_t)s->rb_tx * s->rb_ty));
+  }
   TRY(s->dalloc(&s->d_gcount, sizeof(int)));
   TRY(s->dalloc(&s->d_rgb_flag, sizeof(int)));
   TRY(s->dalloc(&s->d_res, sizeof(ResultBlock)));

@@ -58,7 +58,7 @@ inline dyn_sensor level_sensor(const dyn_sensor& s, int scale) {
   return o;
 }
 
-inline DTsdf dtsdf(const dyn_tsdf_params& p) {
+inline DTsdf dtsdf(const dyn_tsdf_params& p, int precision) {
   DTsdf t;
   t.vs = p.voxel_size;
   t.bsm = (float)p.block_size * p.voxel_size;  // tsdf.cu:437-438
@@ -74,6 +74,7 @@ inline DTsdf dtsdf(const dyn_tsdf_params& p) {
   t.dda_cap = 3 * (int)std::ceil(((double)p.max_sensor_depth + (double)p.truncation_distance) / bs) + 8;
   double step = std::min((double)p.voxel_size, (double)p.truncation_distance);
   t.rc_cap = (int)std::ceil((double)p.max_sensor_depth / step) + 4;
+  t.band = precision == DYN_PRECISION_MIXED_BAND ? 1 : 0;
   return t;
 }
 
@@ -144,6 +145,8 @@ struct dyn_session {
   BilateralTable* d_btab = nullptr;
   int* d_rgb_flag = nullptr;   // nonzero: the current frame carries RGB
   int rgb_flag_host = -1;      // last value written (-1: unknown)
+  unsigned* d_rbound = nullptr;  // band sessions: ray-start bound per 8x8 pixel tile
+  int rb_tx = 0, rb_ty = 0;
   int2* d_gvis = nullptr;      // visible list of the table of one
   int* d_gcount = nullptr;
   ResultBlock* d_res = nullptr;
@@ -190,7 +193,7 @@ struct dyn_session {
     P.max_inc = gp.max_increment;
     P.reg = gp.regularization;
     P.compose_left = gp.compose_left;
-    P.kahan = precision == DYN_PRECISION_MIXED ? 1 : 0;
+    P.kahan = precision != DYN_PRECISION_FP32 ? 1 : 0;
     return P;
   }
 };

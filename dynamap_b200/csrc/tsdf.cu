@@ -152,6 +152,9 @@ __device__ inline void allocate_tile(const float* __restrict__ depth, const DSen
       F3 point = xform(T, point3d(i, d, s));
       if (!(point.x == 0 && point.y == 0 && point.z == 0)) {
         F3 start_pt = f3(T.m[3], T.m[7], T.m[11]);
+        // band allocation: the ray starts a truncation distance before the
+        // surface point instead of at the camera
+        if (t.band) start_pt = point - normalize3(point - start_pt) * t.trunc;
         bool ok = dda_ray(start_pt, point, t.trunc, t.bsm, t.dda_cap, [&](int bx, int by, int bz) {
           unsigned long long key = pack_key(bx, by, bz);
           unsigned h = set_hash(key);
@@ -244,6 +247,80 @@ __device__ inline bool block_visible(unsigned long long key, const DTsdf& t, con
   return ix >= 0 && iy >= 0 && ix < s.cols && iy < s.rows;
 }
 
+// ------------------------------------------------------------ ray-start bound
+// Band sessions allocate blocks only near surfaces.  A ray sample whose
+// voxel lies in no allocated block reads weight 0 and steps one truncation
+// distance (tsdf.cu:505-507), so for every 8x8 pixel tile the frame's
+// raycast gets a lower bound on the camera depth at which any of its rays
+// can first enter an allocated block: below it (and beyond the near
+// distance, where rays are marched normally) a sample needs no lookup, the
+// march adds the truncation distance just as the lookup would have made it.
+// Each allocated block contributes its box widened by one voxel beyond the
+// rounding cells of its outer voxels, clipped to camera depth >= the near
+// distance, projected and widened by one pixel: the tiles its bounding
+// rectangle touches get min(bound, nearest depth of the box).
+constexpr int kRbTile = 8;
+
+__device__ inline float ray_near(const DTsdf& t) { return t.bsm; }
+
+__device__ inline void bound_block(unsigned long long key, const DTsdf& t, const DSensor& s,
+                                   const M4f& invT, unsigned* __restrict__ rb, int tiles_x,
+                                   int tiles_y) {
+  const float vs = t.vs;
+  const float znear = ray_near(t);
+  const float lo[3] = {((float)key_x(key) * 8.0f - 1.5f) * vs,
+                       ((float)key_y(key) * 8.0f - 1.5f) * vs,
+                       ((float)key_z(key) * 8.0f - 1.5f) * vs};
+  const float ext = 11.0f * vs;
+  F3 c[8];
+  float zmin = 3.0e38f, zmax = -3.0e38f;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    c[k] = xform(invT, f3(lo[0] + ((k & 1) ? ext : 0.0f), lo[1] + ((k & 2) ? ext : 0.0f),
+                          lo[2] + ((k & 4) ? ext : 0.0f)));
+    zmin = fminf(zmin, c[k].z);
+    zmax = fmaxf(zmax, c[k].z);
+  }
+  if (!(zmax >= znear)) return;  // wholly nearer than the near distance
+  float umin = 3.0e38f, umax = -3.0e38f, vmin = 3.0e38f, vmax = -3.0e38f;
+  auto add = [&](float X, float Y, float Z) {
+    const float u = s.fx * X / Z + s.cx, w = s.fy * Y / Z + s.cy;
+    umin = fminf(umin, u);
+    umax = fmaxf(umax, u);
+    vmin = fminf(vmin, w);
+    vmax = fmaxf(vmax, w);
+  };
+#pragma unroll
+  for (int k = 0; k < 8; ++k)
+    if (c[k].z >= znear) add(c[k].x, c[k].y, c[k].z);
+  // the 12 box edges (corner pairs differing in one bit) cut by z = znear
+#pragma unroll
+  for (int k = 0; k < 8; ++k)
+#pragma unroll
+    for (int bit = 1; bit < 8; bit <<= 1) {
+      if (k & bit) continue;
+      const F3 a = c[k], b = c[k | bit];
+      if ((a.z < znear) != (b.z < znear)) {
+        const float f = (znear - a.z) / (b.z - a.z);
+        add(a.x + f * (b.x - a.x), a.y + f * (b.y - a.y), znear);
+      }
+    }
+  umin -= 1.0f;
+  vmin -= 1.0f;
+  umax += 1.0f;
+  vmax += 1.0f;
+  if (!(umax >= 0.0f && vmax >= 0.0f && umin <= (float)(s.cols - 1) &&
+        vmin <= (float)(s.rows - 1)))
+    return;
+  const int tx0 = umin <= 0.0f ? 0 : min((int)umin / kRbTile, tiles_x - 1);
+  const int ty0 = vmin <= 0.0f ? 0 : min((int)vmin / kRbTile, tiles_y - 1);
+  const int tx1 = umax >= (float)(s.cols - 1) ? tiles_x - 1 : (int)umax / kRbTile;
+  const int ty1 = vmax >= (float)(s.rows - 1) ? tiles_y - 1 : (int)vmax / kRbTile;
+  const unsigned zb = __float_as_uint(fmaxf(zmin, 0.0f));
+  for (int ty = ty0; ty <= ty1; ++ty)
+    for (int tx = tx0; tx <= tx1; ++tx) atomicMin(rb + ty * tiles_x + tx, zb);
+}
+
 // Every session's visible blocks appended to one batch-wide list of
 // (session, heap index), so integration balances across sessions.
 __global__ void fused_visible_kernel(const SessDev* __restrict__ tab, int2* __restrict__ gvis,
@@ -258,7 +335,13 @@ __global__ void fused_visible_kernel(const SessDev* __restrict__ tab, int2* __re
   const int lane = threadIdx.x & 31;
   for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
     int i = base + threadIdx.x;
-    bool vis = i < n && block_visible(v.block_keys[i], v.t, S.ls[0], invT);
+    bool vis = false;
+    if (i < n) {
+      const unsigned long long key = v.block_keys[i];
+      vis = block_visible(key, v.t, S.ls[0], invT);
+      // every allocated block (visible or not) enters the ray-start bound
+      if (S.rbound) bound_block(key, v.t, S.ls[0], invT, S.rbound, S.rb_tx, S.rb_ty);
+    }
     unsigned m = __ballot_sync(0xffffffffu, vis);
     int off = 0;
     if (lane == 0 && m) {
@@ -666,7 +749,7 @@ __device__ inline VoxelSample interp16(const VolumeDev& v, F3 q, unsigned raw0, 
 // unit depth (both divided by vs), by fused multiply-adds; its voxel is
 // floor(q + 0.5).
 __device__ inline bool raycast_mixed_px(const VolumeDev& v, const DSensor& s, const M4f& T, int x,
-                                        int y, float* __restrict__ depth_out,
+                                        int y, float skip_to, float* __restrict__ depth_out,
                                         uint8_t* __restrict__ rgb_out) {
   const int i = y * s.cols + x;
   const DTsdf& t = v.t;
@@ -682,10 +765,15 @@ __device__ inline bool raycast_mixed_px(const VolumeDev& v, const DSensor& s, co
   float cur = 0.0f;
   int steps = 0;
   bool over = false;
+  const float znear = ray_near(t);
   while (cur < t.dmax) {
     if (steps++ >= t.rc_cap) {
       over = true;
       break;
+    }
+    if (cur >= znear && cur < skip_to) {  // no allocated block here: weight 0
+      cur += t.trunc;
+      continue;
     }
     const F3 q = f3(__fmaf_rn(cur, d.x, o.x), __fmaf_rn(cur, d.y, o.y), __fmaf_rn(cur, d.z, o.z));
     const int gx = (int)floorf(q.x + 0.5f), gy = (int)floorf(q.y + 0.5f),
@@ -736,7 +824,8 @@ __device__ inline bool raycast_mixed_px(const VolumeDev& v, const DSensor& s, co
 template <bool MIXED>
 __device__ inline void raycast_tile(const VolumeDev& v, const DSensor& s,
                                     const float* __restrict__ pose16, float* __restrict__ depth_out,
-                                    uint8_t* __restrict__ rgb_out, int bx, int by) {
+                                    uint8_t* __restrict__ rgb_out, int bx, int by,
+                                    const unsigned* __restrict__ rbound, int tiles_x) {
   __shared__ M4f Ts;
   __shared__ int over;
   const int tid = threadIdx.y * kRayTX + threadIdx.x;
@@ -749,7 +838,9 @@ __device__ inline void raycast_tile(const VolumeDev& v, const DSensor& s,
   const int ly = (warp >> 1) * 4 + (lane >> 3);
   const int x = bx * kRayTX + lx, y = by * kRayTY + ly;
   if (x < s.cols && y < s.rows) {
-    const bool o = MIXED ? raycast_mixed_px(v, s, T, x, y, depth_out, rgb_out)
+    const float skip_to =
+        rbound ? __uint_as_float(rbound[(y / kRbTile) * tiles_x + x / kRbTile]) : 0.0f;
+    const bool o = MIXED ? raycast_mixed_px(v, s, T, x, y, skip_to, depth_out, rgb_out)
                          : raycast_exact_px(v, s, T, x, y, depth_out, rgb_out);
     if (o) atomicAdd(&over, 1);
   }
@@ -763,7 +854,7 @@ __global__ void __launch_bounds__(kRayTX* kRayTY)
                    const float* __restrict__ pose_override, float* __restrict__ depth_out,
                    uint8_t* __restrict__ rgb_out) {
   raycast_tile<MIXED>(v, s, pose_override ? pose_override : ps->posef, depth_out, rgb_out,
-                      blockIdx.x, blockIdx.y);
+                      blockIdx.x, blockIdx.y, nullptr, 0);
 }
 
 // next frame's target of every mode-1 session (blockIdx.z) at its new pose;
@@ -776,17 +867,21 @@ __global__ void __launch_bounds__(kRayTX* kRayTY)
   const DSensor& s = S.ls[0];
   if ((int)blockIdx.x * kRayTX >= s.cols || (int)blockIdx.y * kRayTY >= s.rows) return;
   uint8_t* rgb_out = S.use_color ? S.trgb : nullptr;
-  raycast_tile<MIXED>(S.vol, s, S.pose->posef, S.ray, rgb_out, blockIdx.x, blockIdx.y);
+  raycast_tile<MIXED>(S.vol, s, S.pose->posef, S.ray, rgb_out, blockIdx.x, blockIdx.y,
+                      MIXED ? S.rbound : nullptr, S.rb_tx);
 }
 
 // per-frame counters of every session (all but nalloc, the heap top) and
 // the batch visible list
-__global__ void fused_reset_counters_kernel(const SessDev* __restrict__ tab, int n,
+// (and, for band sessions, the ray-start bound to "no block": 3.4e38)
+__global__ void fused_reset_counters_kernel(const SessDev* __restrict__ tab,
                                             int* __restrict__ gcount) {
+  const SessDev& S = tab[blockIdx.z];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i == 0) *gcount = 0;
-  if (i >= n) return;
-  Counters* c = tab[i].vol.cnt;
+  if (S.rbound && i < S.rb_tx * S.rb_ty) S.rbound[i] = 0x7f7f7f7fu;
+  if (i != 0) return;
+  if (blockIdx.z == 0) *gcount = 0;
+  Counters* c = S.vol.cnt;
   c->new_blocks = 0;
   c->bucket_full = 0;
   c->heap_exhausted = 0;
@@ -847,7 +942,8 @@ void launch_block_coords(const VolumeDev& v, int n, int* coords, cudaStream_t st
 
 // ---- fused stages
 void fused_reset_counters(const SessDev* tab, const BatchShape& b, cudaStream_t st) {
-  fused_reset_counters_kernel<<<nblk(b.n, 128), 128, 0, st>>>(tab, b.n, b.gcount);
+  fused_reset_counters_kernel<<<dim3(nblk(b.max_rb_tiles, 256), 1, b.n), 256, 0, st>>>(
+      tab, b.gcount);
 }
 
 void fused_allocate(const SessDev* tab, const BatchShape& b, cudaStream_t st) {

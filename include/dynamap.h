@@ -117,7 +117,15 @@ typedef struct dyn_bilateral_params {
 
 typedef enum dyn_precision {
   DYN_PRECISION_FP32 = 0,   /* 8-byte voxels {r,g,b,w,f32 sdf}: the drop-in */
-  DYN_PRECISION_MIXED = 1   /* f16 sdf + u16 weight, Kahan-f32 normal eqns */
+  DYN_PRECISION_MIXED = 1,  /* f16 sdf + u16 weight, Kahan-f32 normal eqns */
+  /* DYN_PRECISION_MIXED, and each depth ray allocates only the blocks
+   * within the truncation band of its surface point (the reference
+   * allocates every block from the camera to the surface,
+   * tsdf.cu:346-453): free space farther than a block from any surface is
+   * left unobserved instead of carved, which the raycast steps through
+   * exactly as it steps through carved free space (one truncation
+   * distance per sample).  No counterpart in the reference. */
+  DYN_PRECISION_MIXED_BAND = 2
 } dyn_precision;
 
 /* One voxel as downloaded.  Same 8-byte layout as geometry::Voxel

@@ -28,6 +28,9 @@ def member_params():
     p["tsdf"].update(num_blocks=1 << 15, num_buckets=1 << 16)
     p["gn"].update(mode=0, lvl_scale=[4, 2, 1], lvl_iteration_num=[6, 4, 3])
     out.append((p, abi.PRECISION_MIXED))
+    p = configs.preset("cfg1")  # band allocation (ray-start bound in the raycast)
+    p["tsdf"].update(num_blocks=1 << 15, num_buckets=1 << 16)
+    out.append((p, abi.PRECISION_MIXED_BAND))
     return out
 
 

@@ -1,8 +1,9 @@
 """The frame's raycast (the fused per-frame launch) must equal the stage
 entry point dyn_raycast at the same pose bit for bit, in depth and colour,
-FP32 and mixed, after several frames (block summaries in use), for a camera
-looking into a box (cube) and inside a room (blocks beside and behind the
-camera)."""
+FP32, mixed and mixed with band allocation (whose frame raycast skips the
+lookups below its per-tile ray-start bound, which dyn_raycast does not use),
+after several frames, for a camera looking into a box (cube) and inside a
+room (blocks beside and behind the camera)."""
 import numpy as np
 import pytest
 
@@ -13,7 +14,8 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("kind", ["cube", "room"])
-@pytest.mark.parametrize("prec", [abi.PRECISION_FP32, abi.PRECISION_MIXED])
+@pytest.mark.parametrize("prec", [abi.PRECISION_FP32, abi.PRECISION_MIXED,
+                                  abi.PRECISION_MIXED_BAND])
 def test_frame_target_equals_full_march(gpu_lib, kind, prec):
     p = configs.preset("cfg2")
     p["sensor"].update(rows=240, cols=320, fx=262.5, fy=262.5, cx=159.5, cy=119.5)

@@ -92,3 +92,27 @@ def test_mixed_tracking_within_1mm_of_plain(gpu_lib):
     diff = max(np.linalg.norm(a[:3, 3] - b_[:3, 3])
                for a, b_ in zip(tracks[abi.PRECISION_FP32], tracks[abi.PRECISION_MIXED]))
     assert diff < 2e-3
+
+
+def test_band_allocation_tracking_within_1mm_of_plain(gpu_lib):
+    """Mixed form with band allocation: no carving of free space; the
+    trajectory stays within 1 mm ATE of the FP32 drop-in and the map holds
+    only blocks the carving form also allocates."""
+    p = small()
+    seq = configs.sequence(p, seed=14, n_frames=20)
+    t, g, b, s = configs.structs(p)
+    tracks, maps = {}, {}
+    for prec in (abi.PRECISION_FP32, abi.PRECISION_MIXED_BAND):
+        with Session(t, g, b, s, precision=prec) as m:
+            m.set_pose(seq.poses[0])
+            tracks[prec] = [m.process(seq.depth[k])[0] for k in range(len(seq.depth))]
+            maps[prec] = m.download_blocks()[0]
+    def ate(tr):
+        return float(np.sqrt(np.mean([np.sum((a[:3, 3] - gt[:3, 3]) ** 2)
+                                      for a, gt in zip(tr, seq.poses)])))
+    a32, aband = ate(tracks[abi.PRECISION_FP32]), ate(tracks[abi.PRECISION_MIXED_BAND])
+    assert abs(aband - a32) < 1e-3, (a32, aband)
+    full = {tuple(c) for c in maps[abi.PRECISION_FP32]}
+    band = {tuple(c) for c in maps[abi.PRECISION_MIXED_BAND]}
+    assert len(band) < 0.7 * len(full)
+    assert len(band - full) <= 0.01 * len(band)  # poses differ slightly: nearly a subset

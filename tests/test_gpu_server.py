@@ -24,6 +24,9 @@ def params():
     p["tsdf"].update(num_blocks=1 << 15, num_buckets=1 << 16)
     p["bilateral"].update(enabled=0)
     out.append((p, abi.PRECISION_MIXED, 3))     # joins at step 3
+    p = configs.preset("cfg1")
+    p["tsdf"].update(num_blocks=1 << 15, num_buckets=1 << 16)
+    out.append((p, abi.PRECISION_MIXED_BAND, 2))  # band allocation, joins at step 2
     return out
 
 
