@@ -5,6 +5,7 @@
 // reference, whose builder drives one stream.
 #include <algorithm>
 #include <cstdio>
+#include <map>
 #include <mutex>
 #include <new>
 
@@ -280,9 +281,53 @@ dyn_status dyn_batch_kernels_per_frame(dyn_batch* b, int32_t* n_out) {
 
 namespace {
 
+// The server's device budget, reserved once: sessions are carved from it
+// and returned to it, so admission and release allocate and free nothing
+// on the device (cudaMalloc and cudaFree would stall the steps in flight).
+// First fit by address over free ranges; freed ranges merge with their
+// neighbours.  All sizes are multiples of 256 bytes.
+struct Arena {
+  char* base = nullptr;
+  size_t size = 0;
+  std::map<size_t, size_t> free_;  // offset -> length
+  void init(char* b, size_t n) {
+    base = b;
+    size = n;
+    free_.clear();
+    if (n) free_[0] = n;
+  }
+  // offset of 'n' bytes, or SIZE_MAX
+  size_t take(size_t n) {
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second < n) continue;
+      const size_t off = it->first, len = it->second;
+      free_.erase(it);
+      if (len > n) free_[off + n] = len - n;
+      return off;
+    }
+    return SIZE_MAX;
+  }
+  void give(size_t off, size_t n) {
+    auto it = free_.emplace(off, n).first;
+    auto next = std::next(it);
+    if (next != free_.end() && it->first + it->second == next->first) {
+      it->second += next->second;
+      free_.erase(next);
+    }
+    if (it != free_.begin()) {
+      auto prev = std::prev(it);
+      if (prev->first + prev->second == it->first) {
+        prev->second += it->second;
+        free_.erase(it);
+      }
+    }
+  }
+};
+
 struct ServerSlot {
   dyn_session* s = nullptr;
   size_t bytes = 0;
+  size_t offset = 0;         // of its region in the server's arena
   bool queued = false;       // a frame waits for the next step
   bool queued_rgb = false;
   const uint16_t* src_depth = nullptr;  // pinned caller buffers read at step time
@@ -309,6 +354,8 @@ constexpr int kServerRing = 4;
 struct dyn_server {
   int device = 0;
   size_t budget = 0, used = 0;
+  char* d_arena = nullptr;  // the budget, reserved at creation
+  Arena arena;
   int capacity = 0;
   std::vector<ServerSlot> slots;
   cudaStream_t stream = nullptr;
@@ -345,6 +392,7 @@ void release(dyn_server* sv) {
     if (r.h_map) cudaFreeHost(r.h_map);
     if (r.done) cudaEventDestroy(r.done);
   }
+  cudaFree(sv->d_arena);
   cudaFree(sv->d_gvis);
   cudaFree(sv->d_gcount);
   cudaFree(sv->d_res);
@@ -385,8 +433,9 @@ dyn_status dyn_server_create(const dyn_server_params* p, dyn_server** out) {
     delete sv;
     return DYN_ERR_CUDA;
   }
-  sv->budget = p->budget_bytes ? p->budget_bytes : free_b / 10 * 9;
-  bool ok = cudaStreamCreateWithFlags(&sv->stream, cudaStreamNonBlocking) == cudaSuccess &&
+  sv->budget = (p->budget_bytes ? p->budget_bytes : free_b / 10 * 9) / 256 * 256;
+  bool ok = cudaMalloc(&sv->d_arena, sv->budget ? sv->budget : 256) == cudaSuccess &&
+            cudaStreamCreateWithFlags(&sv->stream, cudaStreamNonBlocking) == cudaSuccess &&
             cudaMalloc(&sv->d_gcount, 256) == cudaSuccess &&
             cudaMalloc(&sv->d_res, sizeof(ResultBlock) * (size_t)cap) == cudaSuccess &&
             cudaMallocHost(&sv->h_res, sizeof(ResultBlock) * (size_t)cap) == cudaSuccess;
@@ -402,6 +451,7 @@ dyn_status dyn_server_create(const dyn_server_params* p, dyn_server** out) {
     return DYN_ERR_OOM;
   }
   std::memset(sv->h_res, 0, sizeof(ResultBlock) * (size_t)cap);
+  sv->arena.init(sv->d_arena, sv->budget);
   *out = sv;
   return DYN_OK;
 }
@@ -421,14 +471,28 @@ dyn_status dyn_server_admit(dyn_server* sv, const dyn_tsdf_params* tsdf, const d
   for (int i = 0; i < sv->capacity && slot < 0; ++i)
     if (!sv->slots[i].s) slot = i;
   if (slot < 0) return DYN_ERR_BUDGET_EXCEEDED;
-  const size_t bytes = session_bytes(*tsdf, *sensor, precision,
-                                     precision != DYN_PRECISION_FP32 ? mixed_colour(gn) : true);
-  if (sv->used + bytes > sv->budget) return DYN_ERR_BUDGET_EXCEEDED;
+  const size_t bytes = session_device_bytes(tsdf, gn, bil, sensor, precision);
+  if (bytes == 0) return DYN_ERR_INVALID_ARG;
+  const size_t off = sv->arena.take(bytes);
+  if (off == SIZE_MAX) return DYN_ERR_BUDGET_EXCEEDED;
+  DeviceGuard dg(sv->device);
+  // the session's buffers from its region; no pinned staging yet (page-
+  // locked frames need none); initialisation enqueued on the session's
+  // stream, which the server's stream waits for
+  SessionMemory mem;
+  mem.region = sv->d_arena + off;
+  mem.region_size = bytes;
+  mem.host_staging = false;
+  mem.sync = false;
   dyn_session* s = nullptr;
-  dyn_status r = dyn_session_create(tsdf, gn, bil, sensor, precision, sv->device, &s);
-  if (r != DYN_OK) return r;
-  if (pose0 && (r = dyn_session_set_pose(s, pose0)) != DYN_OK) {
-    dyn_session_destroy(s);
+  dyn_status r = create_session(tsdf, gn, bil, sensor, precision, sv->device, mem, &s);
+  if (r == DYN_OK && pose0) r = set_pose_async(s, pose0);
+  if (r == DYN_OK && (cudaEventRecord(s->h2d_done, s->stream) != cudaSuccess ||
+                      cudaStreamWaitEvent(sv->stream, s->h2d_done, 0) != cudaSuccess))
+    r = DYN_ERR_CUDA;
+  if (r != DYN_OK) {
+    if (s) dyn_session_destroy(s);
+    sv->arena.give(off, bytes);
     return r;
   }
   s->owner_stream = sv->stream;
@@ -436,6 +500,7 @@ dyn_status dyn_server_admit(dyn_server* sv, const dyn_tsdf_params* tsdf, const d
   sl = ServerSlot();
   sl.s = s;
   sl.bytes = bytes;
+  sl.offset = off;
   sv->used += bytes;
   *slot_out = slot;
   return DYN_OK;
@@ -450,7 +515,8 @@ dyn_status dyn_server_release(dyn_server* sv, int32_t slot) {
   if (sl.last_step >= 0 && sl.last_step >= sv->steps - kServerRing)
     DYN_CUDA(cudaEventSynchronize(sv->ring[sl.last_ring].done));
   sl.s->owner_stream = nullptr;
-  dyn_session_destroy(sl.s);
+  dyn_session_destroy(sl.s);  // its device buffers are the region: nothing freed
+  sv->arena.give(sl.offset, sl.bytes);
   sv->used -= sl.bytes;
   sl = ServerSlot();
   return DYN_OK;
@@ -471,6 +537,7 @@ dyn_status dyn_server_push(dyn_server* sv, int32_t slot, const uint16_t* depth_h
     sl.src_depth = depth_host;
     sl.src_rgb = rgb_host;
   } else {
+    DYN_TRY(ensure_staging(s));  // pinned staging on the first pageable frame
     // the staging buffers may still feed the copies of the slot's last step
     DYN_CUDA(cudaEventSynchronize(s->h2d_done));
     std::memcpy(s->h_depth, depth_host, s->npx * sizeof(uint16_t));
@@ -499,13 +566,16 @@ dyn_status dyn_server_step(dyn_server* sv, int32_t* n_out) {
   }
   const int n = (int)sv->act.size();
   if (n == 0) return DYN_OK;
-  if (cap > sv->gvis_cap) {  // grow the batch visible list
+  if (cap > sv->gvis_cap) {
+    // grow the batch visible list (at least doubling: the wait for the
+    // steps in flight and the reallocation happen a few times per run)
+    const int64_t want = std::max(cap, 2 * sv->gvis_cap);
     DYN_CUDA(cudaStreamSynchronize(sv->stream));
     cudaFree(sv->d_gvis);
     sv->d_gvis = nullptr;
     sv->gvis_cap = 0;
-    DYN_CUDA(cudaMalloc(&sv->d_gvis, sizeof(int2) * (size_t)cap));
-    sv->gvis_cap = cap;
+    DYN_CUDA(cudaMalloc(&sv->d_gvis, sizeof(int2) * (size_t)want));
+    sv->gvis_cap = want;
   }
   cudaStream_t st = sv->stream;
   DYN_CUDA(cudaMemcpyAsync(rb.d_tab, rb.h_tab, sizeof(SessDev) * (size_t)n,

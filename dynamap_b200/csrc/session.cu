@@ -421,7 +421,7 @@ void fill_stats(const dyn_session* s, const ResultBlock& r, dyn_frame_stats* st)
   for (int k = 0; k < 6; ++k) st->pose_increment[k] = r.pose.last_inc[k];
 }
 
-dyn_status reset_state(dyn_session* s) {
+dyn_status reset_state(dyn_session* s, bool sync = true) {
   cudaStream_t st = s->stream;
   launch_volume_clear(s->vol, st);
   IcpState z;
@@ -435,7 +435,7 @@ dyn_status reset_state(dyn_session* s) {
   for (int k = 0; k < 16; ++k) I[k] = (k % 5 == 0) ? 1.0 : 0.0;
   DYN_CUDA(cudaMemcpyAsync(s->d_pose_in, I, sizeof(I), cudaMemcpyHostToDevice, st));
   launch_pose_set(s->d_pose, s->d_pose_in, st);
-  DYN_CUDA(cudaStreamSynchronize(st));
+  if (sync) DYN_CUDA(cudaStreamSynchronize(st));
   s->frames = 0;
   s->pending = false;
   return DYN_OK;
@@ -474,6 +474,212 @@ struct StageScratch {
 std::mutex g_stage_mu;
 StageScratch g_stage[64];
 
+dyn_status validate_params(const dyn_tsdf_params* tsdf, const dyn_gn_params* gn,
+                           const dyn_bilateral_params* bil, const dyn_sensor* sensor,
+                           int precision) {
+  if (!tsdf || !gn || !bil || !valid_sensor(sensor)) return DYN_ERR_INVALID_ARG;
+  if (tsdf->block_size != kBlockSize || tsdf->bucket_size < 1 || tsdf->num_buckets < 1 ||
+      tsdf->num_blocks < 1 || tsdf->max_sdf_weight < 1 ||
+      tsdf->max_sdf_weight > (precision != DYN_PRECISION_FP32 ? 65535 : 255) ||
+      !(tsdf->voxel_size > 0) || !(tsdf->truncation_distance > 0) ||
+      !(tsdf->max_sensor_depth > 0))
+    return DYN_ERR_INVALID_ARG;
+  if ((int64_t)tsdf->num_buckets * tsdf->bucket_size > (int64_t)1 << 30) return DYN_ERR_INVALID_ARG;
+  for (int k = 0; k < 3; ++k) {
+    int sc = gn->lvl_scale[k];
+    if (sc != 1 && sc != 2 && sc != 4 && sc != 8) return DYN_ERR_INVALID_ARG;
+    if (gn->lvl_iteration_num[k] < 0 || gn->lvl_iteration_num[k] > 1000) return DYN_ERR_INVALID_ARG;
+    if ((int)(sensor->rows / sc) < 3 || (int)(sensor->cols / sc) < 5) return DYN_ERR_INVALID_ARG;
+  }
+  if (bil->enabled && (bil->diameter < 1 || bil->diameter > 16 || !(bil->sigma_s > 0) ||
+                       !(bil->sigma_i > 0)))
+    return DYN_ERR_INVALID_ARG;
+  if (gn->mode != 0 && gn->mode != 1) return DYN_ERR_INVALID_ARG;
+  if (precision != DYN_PRECISION_FP32 && precision != DYN_PRECISION_MIXED &&
+      precision != DYN_PRECISION_MIXED_BAND)
+    return DYN_ERR_INVALID_ARG;
+  return DYN_OK;
+}
+
+// Parameters and derived sizes of a session (no CUDA calls).
+void init_fields(dyn_session* s, const dyn_tsdf_params* tsdf, const dyn_gn_params* gn,
+                 const dyn_bilateral_params* bil, const dyn_sensor* sensor, int precision,
+                 int device) {
+  s->device = device;
+  s->tp = *tsdf;
+  s->gp = *gn;
+  s->bp = *bil;
+  s->sensor = *sensor;
+  s->precision = precision;
+  s->npx = (size_t)sensor->rows * sensor->cols;
+  int maxl = 0;
+  for (int k = 0; k < 3; ++k) maxl = std::max(maxl, level_of_scale(gn->lvl_scale[k]));
+  s->nlev = maxl + 1;
+  for (int l = 0; l < kLevels; ++l) s->ls[l] = dsensor(level_sensor(*sensor, 1 << l));
+  std::memset(&s->btab, 0, sizeof(s->btab));
+  if (bil->enabled) s->btab = make_bilateral_table(bil->diameter, bil->sigma_i, bil->sigma_s);
+}
+
+// Every device buffer of a session (counted only when s->measure).
+dyn_status alloc_device_buffers(dyn_session* s) {
+  const dyn_tsdf_params* tsdf = &s->tp;
+  const int precision = s->precision;
+  const size_t n = s->npx;
+  DYN_TRY(s->dalloc(&s->d_u16, n * 2));
+  DYN_TRY(s->dalloc(&s->d_rgb, n * 3));
+  DYN_TRY(s->dalloc(&s->d_raw, n * 4));
+  DYN_TRY(s->dalloc(&s->d_filt, n * 4));
+  DYN_TRY(s->dalloc(&s->d_ray, n * 4));
+  DYN_TRY(s->dalloc(&s->d_trgb, n * 3));
+  for (int l = 0; l < s->nlev; ++l) {
+    size_t m = (size_t)s->ls[l].rows * s->ls[l].cols;
+    size_t m4 = (m + 3) / 4 * 4;
+    if (l == 0) s->d_sdep[0] = s->d_filt;
+    else DYN_TRY(s->dalloc(&s->d_sdep[l], m4 * 4));
+    DYN_TRY(s->dalloc(&s->d_snrm[l], m * 16));
+    DYN_TRY(s->dalloc(&s->d_svtx[l], m * 16));
+    DYN_TRY(s->dalloc(&s->d_sint[l], m4 * 4));
+    DYN_TRY(s->dalloc(&s->d_tdep[l], m4 * 4));
+    DYN_TRY(s->dalloc(&s->d_tnrm[l], m * 16));
+    DYN_TRY(s->dalloc(&s->d_tvtx[l], m * 16));
+    DYN_TRY(s->dalloc(&s->d_tint[l], m4 * 4));
+  }
+  DYN_TRY(s->dalloc(&s->d_pose_override, 64));
+  DYN_TRY(s->dalloc(&s->d_pose_in, 128));
+  DYN_TRY(s->dalloc(&s->d_partials, icp_scratch_bytes()));
+  DYN_TRY(s->dalloc(&s->d_icp, sizeof(IcpState)));
+  DYN_TRY(s->dalloc(&s->d_pose, sizeof(PoseState)));
+  s->vol.t = dtsdf(*tsdf, precision);
+  DYN_TRY(s->dalloc(&s->vol.entries, sizeof(Entry) * (size_t)tsdf->num_buckets * tsdf->bucket_size));
+  DYN_TRY(s->dalloc(&s->vol.block_keys, sizeof(unsigned long long) * (size_t)tsdf->num_blocks));
+  const size_t nvox = (size_t)tsdf->num_blocks * kBlockVox;
+  s->vol.voxels = nullptr;
+  s->vol.vox16 = nullptr;
+  s->vol.colors = nullptr;
+  s->vol.fp16 = precision != DYN_PRECISION_FP32 ? 1 : 0;
+  if (s->vol.fp16) {
+    DYN_TRY(s->dalloc(&s->vol.vox16, sizeof(unsigned) * nvox));
+    if (mixed_colour(&s->gp)) DYN_TRY(s->dalloc(&s->vol.colors, sizeof(uchar4) * nvox));
+  } else {
+    DYN_TRY(s->dalloc(&s->vol.voxels, sizeof(dyn_voxel) * nvox));
+  }
+  DYN_TRY(s->dalloc(&s->vol.cnt, sizeof(Counters)));
+  DYN_TRY(s->dalloc(&s->d_gvis, sizeof(int2) * (size_t)tsdf->num_blocks));
+  if (precision == DYN_PRECISION_MIXED_BAND) {
+    s->rb_tx = ((int)s->sensor.cols + 7) / 8;
+    s->rb_ty = ((int)s->sensor.rows + 7) / 8;
+    DYN_TRY(s->dalloc(&s->d_rbound, sizeof(unsigned) * (size_t)s->rb_tx * s->rb_ty));
+  }
+  DYN_TRY(s->dalloc(&s->d_gcount, sizeof(int)));
+  DYN_TRY(s->dalloc(&s->d_rgb_flag, sizeof(int)));
+  DYN_TRY(s->dalloc(&s->d_res, sizeof(ResultBlock)));
+  DYN_TRY(s->dalloc(&s->d_btab, sizeof(BilateralTable)));
+  DYN_TRY(s->dalloc(&s->d_sd, sizeof(SessDev)));
+  return DYN_OK;
+}
+
+size_t session_device_bytes(const dyn_tsdf_params* tsdf, const dyn_gn_params* gn,
+                            const dyn_bilateral_params* bil, const dyn_sensor* sensor,
+                            int precision) {
+  if (validate_params(tsdf, gn, bil, sensor, precision) != DYN_OK) return 0;
+  dyn_session* s = new (std::nothrow) dyn_session();
+  if (!s) return 0;
+  init_fields(s, tsdf, gn, bil, sensor, precision, 0);
+  s->measure = true;
+  alloc_device_buffers(s);
+  const size_t b = s->measured;
+  delete s;
+  return b;
+}
+
+dyn_status ensure_staging(dyn_session* s) {
+  if (s->h_depth) return DYN_OK;
+  if (cudaMallocHost(&s->h_depth, s->npx * 2) != cudaSuccess ||
+      cudaMallocHost(&s->h_rgb, s->npx * 3) != cudaSuccess) {
+    cudaGetLastError();
+    return DYN_ERR_OOM;
+  }
+  return DYN_OK;
+}
+
+dyn_status set_pose_async(dyn_session* s, const float pose[16]) {
+  double P[16];
+  for (int k = 0; k < 16; ++k) P[k] = (double)pose[k];
+  // pageable source: the copy is staged before the call returns
+  DYN_CUDA(cudaMemcpyAsync(s->d_pose_in, P, sizeof(P), cudaMemcpyHostToDevice, s->stream));
+  launch_pose_set(s->d_pose, s->d_pose_in, s->stream);
+  return DYN_OK;
+}
+
+dyn_status create_session(const dyn_tsdf_params* tsdf, const dyn_gn_params* gn,
+                          const dyn_bilateral_params* bil, const dyn_sensor* sensor,
+                          int precision, int device, const SessionMemory& mem,
+                          dyn_session** out) {
+  if (!out) return DYN_ERR_INVALID_ARG;
+  *out = nullptr;
+  DYN_TRY(validate_params(tsdf, gn, bil, sensor, precision));
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return DYN_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= ndev) return DYN_ERR_INVALID_ARG;
+  DeviceGuard dg(device);
+  dyn_session* s = new (std::nothrow) dyn_session();
+  if (!s) return DYN_ERR_OOM;
+  init_fields(s, tsdf, gn, bil, sensor, precision, device);
+  s->region = mem.region;
+  s->region_size = mem.region_size;
+  dyn_status r = DYN_OK;
+#define TRY(x)               \
+  do {                       \
+    r = (x);                 \
+    if (r != DYN_OK) {       \
+      release(s);            \
+      return r;              \
+    }                        \
+  } while (0)
+  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&s->h2d_done, cudaEventDisableTiming) != cudaSuccess) {
+    release(s);
+    return DYN_ERR_CUDA;
+  }
+  TRY(alloc_device_buffers(s));
+  if (mem.host_staging) {
+    TRY(ensure_staging(s));
+    if (cudaMallocHost(&s->h_res, sizeof(ResultBlock)) != cudaSuccess) {
+      cudaGetLastError();
+      release(s);
+      return DYN_ERR_OOM;
+    }
+  }
+  // zero the images so unused levels and borders read as invalid
+  for (int l = 0; l < s->nlev; ++l) {
+    size_t m = (size_t)s->ls[l].rows * s->ls[l].cols;
+    cudaMemsetAsync(s->d_tdep[l], 0, m * 4, s->stream);
+    cudaMemsetAsync(s->d_tnrm[l], 0, m * 16, s->stream);
+    cudaMemsetAsync(s->d_tint[l], 0, m * 4, s->stream);
+    cudaMemsetAsync(s->d_sint[l], 0, m * 4, s->stream);
+  }
+  cudaMemsetAsync(s->d_rgb_flag, 0, sizeof(int), s->stream);
+  s->rgb_flag_host = 0;
+  fill_sessdev(s);
+  dyn_session* self = s;
+  s->shape = make_shape(&self, 1, s->d_gvis, s->d_gcount, tsdf->num_blocks);
+  if (cudaMemcpyAsync(s->d_btab, &s->btab, sizeof(BilateralTable), cudaMemcpyHostToDevice,
+                      s->stream) != cudaSuccess ||
+      cudaMemcpyAsync(s->d_sd, &s->hsd, sizeof(SessDev), cudaMemcpyHostToDevice, s->stream) !=
+          cudaSuccess) {
+    release(s);
+    return DYN_ERR_CUDA;
+  }
+  TRY(reset_state(s, mem.sync));
+  cudaEventRecord(s->h2d_done, s->stream);  // also: initialisation enqueued
+#undef TRY
+  *out = s;
+  return DYN_OK;
+}
+
 }  // namespace host
 }  // namespace dyn
 
@@ -510,148 +716,7 @@ dyn_status dyn_session_bytes(const dyn_tsdf_params* tsdf, const dyn_sensor* sens
 dyn_status dyn_session_create(const dyn_tsdf_params* tsdf, const dyn_gn_params* gn,
                               const dyn_bilateral_params* bil, const dyn_sensor* sensor,
                               int32_t precision, int32_t device, dyn_session** out) {
-  if (!out) return DYN_ERR_INVALID_ARG;
-  *out = nullptr;
-  if (!tsdf || !gn || !bil || !valid_sensor(sensor)) return DYN_ERR_INVALID_ARG;
-  if (tsdf->block_size != kBlockSize || tsdf->bucket_size < 1 || tsdf->num_buckets < 1 ||
-      tsdf->num_blocks < 1 || tsdf->max_sdf_weight < 1 ||
-      tsdf->max_sdf_weight > (precision != DYN_PRECISION_FP32 ? 65535 : 255) ||
-      !(tsdf->voxel_size > 0) || !(tsdf->truncation_distance > 0) ||
-      !(tsdf->max_sensor_depth > 0))
-    return DYN_ERR_INVALID_ARG;
-  if ((int64_t)tsdf->num_buckets * tsdf->bucket_size > (int64_t)1 << 30) return DYN_ERR_INVALID_ARG;
-  for (int k = 0; k < 3; ++k) {
-    int sc = gn->lvl_scale[k];
-    if (sc != 1 && sc != 2 && sc != 4 && sc != 8) return DYN_ERR_INVALID_ARG;
-    if (gn->lvl_iteration_num[k] < 0 || gn->lvl_iteration_num[k] > 1000) return DYN_ERR_INVALID_ARG;
-    if ((int)(sensor->rows / sc) < 3 || (int)(sensor->cols / sc) < 5) return DYN_ERR_INVALID_ARG;
-  }
-  if (bil->enabled && (bil->diameter < 1 || bil->diameter > 16 || !(bil->sigma_s > 0) ||
-                       !(bil->sigma_i > 0)))
-    return DYN_ERR_INVALID_ARG;
-  if (gn->mode != 0 && gn->mode != 1) return DYN_ERR_INVALID_ARG;
-  if (precision != DYN_PRECISION_FP32 && precision != DYN_PRECISION_MIXED &&
-      precision != DYN_PRECISION_MIXED_BAND)
-    return DYN_ERR_INVALID_ARG;
-  int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
-    cudaGetLastError();
-    return DYN_ERR_NO_DEVICE;
-  }
-  if (device < 0 || device >= ndev) return DYN_ERR_INVALID_ARG;
-  DeviceGuard dg(device);
-  dyn_session* s = new (std::nothrow) dyn_session();
-  if (!s) return DYN_ERR_OOM;
-  s->device = device;
-  s->tp = *tsdf;
-  s->gp = *gn;
-  s->bp = *bil;
-  s->sensor = *sensor;
-  s->precision = precision;
-  s->npx = (size_t)sensor->rows * sensor->cols;
-  int maxl = 0;
-  for (int k = 0; k < 3; ++k) maxl = std::max(maxl, level_of_scale(gn->lvl_scale[k]));
-  s->nlev = maxl + 1;
-  for (int l = 0; l < kLevels; ++l) s->ls[l] = dsensor(level_sensor(*sensor, 1 << l));
-  std::memset(&s->btab, 0, sizeof(s->btab));
-  if (bil->enabled) s->btab = make_bilateral_table(bil->diameter, bil->sigma_i, bil->sigma_s);
-  dyn_status r = DYN_OK;
-#define TRY(x)               \
-  do {                       \
-    r = (x);                 \
-    if (r != DYN_OK) {       \
-      release(s);            \
-      return r;              \
-    }                        \
-  } while (0)
-  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreateWithFlags(&s->h2d_done, cudaEventDisableTiming) != cudaSuccess) {
-    release(s);
-    return DYN_ERR_CUDA;
-  }
-  size_t n = s->npx;
-  TRY(s->dalloc(&s->d_u16, n * 2));
-  TRY(s->dalloc(&s->d_rgb, n * 3));
-  TRY(s->dalloc(&s->d_raw, n * 4));
-  TRY(s->dalloc(&s->d_filt, n * 4));
-  TRY(s->dalloc(&s->d_ray, n * 4));
-  TRY(s->dalloc(&s->d_trgb, n * 3));
-  for (int l = 0; l < s->nlev; ++l) {
-    size_t m = (size_t)s->ls[l].rows * s->ls[l].cols;
-    size_t m4 = (m + 3) / 4 * 4;
-    if (l == 0) s->d_sdep[0] = s->d_filt;
-    else TRY(s->dalloc(&s->d_sdep[l], m4 * 4));
-    TRY(s->dalloc(&s->d_snrm[l], m * 16));
-    TRY(s->dalloc(&s->d_svtx[l], m * 16));
-    TRY(s->dalloc(&s->d_sint[l], m4 * 4));
-    TRY(s->dalloc(&s->d_tdep[l], m4 * 4));
-    TRY(s->dalloc(&s->d_tnrm[l], m * 16));
-    TRY(s->dalloc(&s->d_tvtx[l], m * 16));
-    TRY(s->dalloc(&s->d_tint[l], m4 * 4));
-  }
-  TRY(s->dalloc(&s->d_pose_override, 64));
-  TRY(s->dalloc(&s->d_pose_in, 128));
-  TRY(s->dalloc(&s->d_partials, icp_scratch_bytes()));
-  TRY(s->dalloc(&s->d_icp, sizeof(IcpState)));
-  TRY(s->dalloc(&s->d_pose, sizeof(PoseState)));
-  s->vol.t = dtsdf(*tsdf, precision);
-  TRY(s->dalloc(&s->vol.entries, sizeof(Entry) * (size_t)tsdf->num_buckets * tsdf->bucket_size));
-  TRY(s->dalloc(&s->vol.block_keys, sizeof(unsigned long long) * (size_t)tsdf->num_blocks));
-  const size_t nvox = (size_t)tsdf->num_blocks * kBlockVox;
-  s->vol.voxels = nullptr;
-  s->vol.vox16 = nullptr;
-  s->vol.colors = nullptr;
-  s->vol.fp16 = precision != DYN_PRECISION_FP32 ? 1 : 0;
-  if (s->vol.fp16) {
-    TRY(s->dalloc(&s->vol.vox16, sizeof(unsigned) * nvox));
-    if (mixed_colour(gn)) TRY(s->dalloc(&s->vol.colors, sizeof(uchar4) * nvox));
-  } else {
-    TRY(s->dalloc(&s->vol.voxels, sizeof(dyn_voxel) * nvox));
-  }
-  TRY(s->dalloc(&s->vol.cnt, sizeof(Counters)));
-  TRY(s->dalloc(&s->d_gvis, sizeof(int2) * (size_t)tsdf->num_blocks));
-  if (precision == DYN_PRECISION_MIXED_BAND) {
-    s->rb_tx = ((int)sensor->cols + 7) / 8;
-    s->rb_ty = ((int)sensor->rows + 7) / 8;
-    TRY(s->dalloc(&s->d_rbound, sizeof(unsigned) * (size_t)s->rb_tx * s->rb_ty));
-  }
-  TRY(s->dalloc(&s->d_gcount, sizeof(int)));
-  TRY(s->dalloc(&s->d_rgb_flag, sizeof(int)));
-  TRY(s->dalloc(&s->d_res, sizeof(ResultBlock)));
-  TRY(s->dalloc(&s->d_btab, sizeof(BilateralTable)));
-  TRY(s->dalloc(&s->d_sd, sizeof(SessDev)));
-  if (cudaMallocHost(&s->h_depth, n * 2) != cudaSuccess ||
-      cudaMallocHost(&s->h_rgb, n * 3) != cudaSuccess ||
-      cudaMallocHost(&s->h_res, sizeof(ResultBlock)) != cudaSuccess) {
-    cudaGetLastError();
-    release(s);
-    return DYN_ERR_OOM;
-  }
-  // zero the images so unused levels and borders read as invalid
-  for (int l = 0; l < s->nlev; ++l) {
-    size_t m = (size_t)s->ls[l].rows * s->ls[l].cols;
-    cudaMemsetAsync(s->d_tdep[l], 0, m * 4, s->stream);
-    cudaMemsetAsync(s->d_tnrm[l], 0, m * 16, s->stream);
-    cudaMemsetAsync(s->d_tint[l], 0, m * 4, s->stream);
-    cudaMemsetAsync(s->d_sint[l], 0, m * 4, s->stream);
-  }
-  cudaMemsetAsync(s->d_rgb_flag, 0, sizeof(int), s->stream);
-  s->rgb_flag_host = 0;
-  fill_sessdev(s);
-  dyn_session* self = s;
-  s->shape = make_shape(&self, 1, s->d_gvis, s->d_gcount, tsdf->num_blocks);
-  if (cudaMemcpyAsync(s->d_btab, &s->btab, sizeof(BilateralTable), cudaMemcpyHostToDevice,
-                      s->stream) != cudaSuccess ||
-      cudaMemcpyAsync(s->d_sd, &s->hsd, sizeof(SessDev), cudaMemcpyHostToDevice, s->stream) !=
-          cudaSuccess) {
-    release(s);
-    return DYN_ERR_CUDA;
-  }
-  cudaEventRecord(s->h2d_done, s->stream);
-  TRY(reset_state(s));
-#undef TRY
-  *out = s;
-  return DYN_OK;
+  return create_session(tsdf, gn, bil, sensor, precision, device, SessionMemory(), out);
 }
 
 dyn_status dyn_session_destroy(dyn_session* s) {

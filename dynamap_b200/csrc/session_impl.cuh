@@ -169,11 +169,30 @@ struct dyn_session {
   int frames = 0;
   bool pending = false;
 
+  // device memory: cudaMalloc per buffer, or carved from a region a server
+  // reserved (region != null), or only counted (measure)
+  char* region = nullptr;
+  size_t region_size = 0, region_used = 0;
+  bool measure = false;
+  size_t measured = 0;
+
   template <class T>
   dyn_status dalloc(T** p, size_t bytes) {
     void* q = nullptr;
     bytes = (bytes + 255) / 256 * 256;  // whole 16-byte vectors at the tail
-    cudaError_t e = cudaMalloc(&q, bytes < 256 ? 256 : bytes);
+    if (bytes < 256) bytes = 256;
+    if (measure) {
+      measured += bytes;
+      *p = nullptr;
+      return DYN_OK;
+    }
+    if (region) {
+      if (region_used + bytes > region_size) return DYN_ERR_OOM;
+      *p = (T*)(region + region_used);
+      region_used += bytes;
+      return DYN_OK;
+    }
+    cudaError_t e = cudaMalloc(&q, bytes);
     if (e != cudaSuccess) {
       cudaGetLastError();
       return e == cudaErrorMemoryAllocation ? DYN_ERR_OOM : DYN_ERR_CUDA;
@@ -301,6 +320,28 @@ bool is_pinned(const void* p);
 // Device bytes a session with these parameters allocates (colour: a mixed
 // session keeps per-voxel colour).
 size_t session_bytes(const dyn_tsdf_params& t, const dyn_sensor& s, int precision, bool colour);
+
+// Where a session's memory comes from (dyn_session_create: cudaMalloc per
+// buffer, pinned staging now, initialisation waited for).
+struct SessionMemory {
+  char* region = nullptr;    // carve the device buffers from [region, region + size)
+  size_t region_size = 0;
+  bool host_staging = true;  // pinned staging and result buffers now (else on first use)
+  bool sync = true;          // return after the initialisation has run
+};
+// Exact device bytes of a session with these parameters (no CUDA calls);
+// 0 when the parameters are invalid.
+size_t session_device_bytes(const dyn_tsdf_params* tsdf, const dyn_gn_params* gn,
+                            const dyn_bilateral_params* bil, const dyn_sensor* sensor,
+                            int precision);
+dyn_status create_session(const dyn_tsdf_params* tsdf, const dyn_gn_params* gn,
+                          const dyn_bilateral_params* bil, const dyn_sensor* sensor,
+                          int precision, int device, const SessionMemory& mem,
+                          dyn_session** out);
+// The pose from the host without waiting (stream-ordered on the session).
+dyn_status set_pose_async(dyn_session* s, const float pose[16]);
+// Pinned staging buffers of a session created without them.
+dyn_status ensure_staging(dyn_session* s);
 bool mixed_colour(const dyn_gn_params* gn);
 dyn_status counters_status(const Counters& c);
 void fill_stats(const dyn_session* s, const ResultBlock& r, dyn_frame_stats* st);

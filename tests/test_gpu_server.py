@@ -92,21 +92,22 @@ def test_results_same_alone_and_in_the_mix(gpu_lib, streams):
 
 
 def test_admission_by_budget(gpu_lib, streams):
-    import ctypes as C
-    lib = abi.load()
+    """The server reserves its budget once and carves sessions from it: a
+    session is refused when its bytes do not fit, admitted after a release."""
     (p0, prec0), (p1, prec1) = streams[0][:2], streams[1][:2]
     need = []
-    for p, prec in ((p0, prec0), (p1, prec1)):
-        t, g, b, s = configs.structs(p)
-        n = C.c_size_t()
-        abi.check("bytes", lib.dyn_session_bytes(C.byref(t), C.byref(s), prec, C.byref(n)))
-        need.append(n.value)
-    with Server(budget_bytes=need[0] + need[1] - 1) as sv:
+    with Server(budget_bytes=4 << 30) as sv:
+        for p, prec in ((p0, prec0), (p1, prec1)):
+            slot = sv.admit(*configs.structs(p), precision=prec)
+            need.append(sv.usage()["used_bytes"])
+            sv.release(slot)
+            assert sv.usage()["used_bytes"] == 0
+    with Server(budget_bytes=need[0] + need[1] - 256) as sv:
         a = sv.admit(*configs.structs(p0), precision=prec0)
         assert a is not None
         assert sv.admit(*configs.structs(p1), precision=prec1) is None  # over budget
         u = sv.usage()
-        assert u["sessions"] == 1 and 0 < u["used_bytes"] <= u["budget_bytes"]
+        assert u["sessions"] == 1 and u["used_bytes"] == need[0] <= u["budget_bytes"]
         sv.release(a)
         assert sv.usage()["used_bytes"] == 0
         b_ = sv.admit(*configs.structs(p1), precision=prec1)
@@ -114,3 +115,6 @@ def test_admission_by_budget(gpu_lib, streams):
         assert not sv.ready(b_)  # nothing stepped yet
         with pytest.raises(abi.DynError):
             sv.result(b_)
+        # released space is reused: the first session fits again beside it
+        # only if both fit
+        assert sv.admit(*configs.structs(p0), precision=prec0) is None
