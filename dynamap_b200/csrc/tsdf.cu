@@ -358,7 +358,20 @@ __global__ void fused_visible_kernel(const SessDev* __restrict__ tab, int2* __re
 // (geom_Types.h:79-103) for voxel 'lin' of block 'ptr'.  The voxel updated
 // is the thread's own: the reference's camera->world round trip through
 // UpdateVoxel lands on the same voxel (the oracle checks this).
-template <bool FP16>
+// FAST (band sessions, whose allocation already departs from the
+// reference's): fused multiply-adds and hardware-approximate division and
+// square root throughout.
+__device__ inline F3 xform_fma(const M4f& T, F3 v) {
+  return f3(__fmaf_rn(T.m[0], v.x, __fmaf_rn(T.m[1], v.y, __fmaf_rn(T.m[2], v.z, T.m[3]))),
+            __fmaf_rn(T.m[4], v.x, __fmaf_rn(T.m[5], v.y, __fmaf_rn(T.m[6], v.z, T.m[7]))),
+            __fmaf_rn(T.m[8], v.x, __fmaf_rn(T.m[9], v.y, __fmaf_rn(T.m[10], v.z, T.m[11]))));
+}
+__device__ inline float norm3_fast(F3 v) {
+  const float q = __fmaf_rn(v.x, v.x, __fmaf_rn(v.y, v.y, v.z * v.z));
+  return q > 0.0f ? q * rsqrtf(q) : 0.0f;
+}
+
+template <bool FP16, bool FAST>
 __device__ inline void integrate_voxel(const VolumeDev& v, const float* __restrict__ depth,
                                        const uint8_t* __restrict__ rgb, const DSensor& s,
                                        const M4f& invT, int ptr, int lin) {
@@ -371,19 +384,39 @@ __device__ inline void integrate_voxel(const VolumeDev& v, const float* __restri
                    (float)key_z(key) * vs * (float)kBlockSize);
   F3 vp = f3(position.x + (float)bx * vs, position.y + (float)by * vs,
              position.z + (float)bz * vs);
-  vp = xform(invT, vp);
   // pixel, depth gate and band decide which voxels a frame updates: IEEE
-  // arithmetic in both forms, so that the mixed form's weights stay exact
+  // arithmetic in the FP32 and mixed forms, so that the mixed form's
+  // weights stay exact
   int px, py;
-  if (!project(vp, s, &px, &py)) return;
-  if (!(px >= 0 && py >= 0 && px < s.cols && py < s.rows)) return;
+  float sd, vd, d;
+  if (FAST) {
+    vp = xform_fma(invT, vp);
+    if (!(vp.z > 0.0f)) return;
+    const float rz = __fdividef(1.0f, vp.z);
+    const float xf = __fmaf_rn(s.fx * vp.x, rz, s.cx), yf = __fmaf_rn(s.fy * vp.y, rz, s.cy);
+    if (!(fabsf(xf) < 2e9f) || !(fabsf(yf) < 2e9f)) return;
+    px = (int)roundf(xf);
+    py = (int)roundf(yf);
+    if (!(px >= 0 && py >= 0 && px < s.cols && py < s.rows)) return;
+    d = __ldg(depth + py * s.cols + px);
+    if (d < t.dmin) return;
+    if (d > t.dmax) return;
+    const F3 p3 = f3(__fdividef(((float)px - s.cx) * d, s.fx),
+                     __fdividef(((float)py - s.cy) * d, s.fy), d);
+    sd = norm3_fast(p3);
+    vd = norm3_fast(vp);
+  } else {
+    vp = xform(invT, vp);
+    if (!project(vp, s, &px, &py)) return;
+    if (!(px >= 0 && py >= 0 && px < s.cols && py < s.rows)) return;
+    d = __ldg(depth + py * s.cols + px);
+    if (d < t.dmin) return;
+    if (d > t.dmax) return;
+    F3 p3 = point3d_uv(px, py, d, s);
+    sd = norm3(p3);
+    vd = norm3(vp);
+  }
   const int idx = py * s.cols + px;
-  const float d = __ldg(depth + idx);
-  if (d < t.dmin) return;
-  if (d > t.dmax) return;
-  F3 p3 = point3d_uv(px, py, d, s);
-  float sd = norm3(p3);
-  float vd = norm3(vp);
   float sdf;
   if (vd > sd - t.trunc && vd < sd + t.trunc && d < t.dmax) sdf = sd - vd;
   else if (vd < sd - t.trunc) sdf = t.trunc;
@@ -459,10 +492,12 @@ __global__ void __launch_bounds__(kBlockVox)
     }
     const SessDev& S = tab[item.x];
     const uint8_t* rgb = *S.rgb_flag ? S.rgb : nullptr;
-    if (S.vol.fp16)
-      integrate_voxel<true>(S.vol, S.raw, rgb, S.ls[0], invT, item.y, threadIdx.x);
+    if (!S.vol.fp16)
+      integrate_voxel<false, false>(S.vol, S.raw, rgb, S.ls[0], invT, item.y, threadIdx.x);
+    else if (S.vol.t.band)
+      integrate_voxel<true, true>(S.vol, S.raw, rgb, S.ls[0], invT, item.y, threadIdx.x);
     else
-      integrate_voxel<false>(S.vol, S.raw, rgb, S.ls[0], invT, item.y, threadIdx.x);
+      integrate_voxel<true, false>(S.vol, S.raw, rgb, S.ls[0], invT, item.y, threadIdx.x);
   }
 }
 
