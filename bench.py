@@ -397,6 +397,32 @@ def run_ours(args):
     elapsed_a = max_over_ranks(elapsed_a)
     barrier()
 
+    # ---- the other forms on the same frames (pass A only), for the line's
+    # plain-vs-precision comparison
+    forms = {}
+    if prec == abi.PRECISION_FP32 and args.forms:
+        for name, fp in (("mixed", abi.PRECISION_MIXED), ("band", abi.PRECISION_MIXED_BAND)):
+            with Session(t, g, b, s, precision=fp, device=local) as m:
+                m.set_pose(poses[0])
+                st_f = session_stream(m)
+                for i in range(args.warmup):
+                    m.submit_device(fptr(d_dev, i, fbytes_d),
+                                    fptr(c_dev, i, fbytes_c) if has_rgb else None)
+                    m.result(strict=False)
+                torch.cuda.synchronize()
+                f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                f0.record(st_f)
+                for i in range(args.warmup, nframes):
+                    m.submit_device(fptr(d_dev, i, fbytes_d),
+                                    fptr(c_dev, i, fbytes_c) if has_rgb else None)
+                f1.record(st_f)
+                m.result(strict=False)
+                torch.cuda.synchronize()
+                el = max_over_ranks(f0.elapsed_time(f1) / 1e3)
+                forms[name] = {"value": world * args.steps / el, "unit": "frames/s",
+                               "vs_fp32": elapsed_a / el}
+        barrier()
+
     # ---- pass B: per-frame latency and stage times ------------------------
     lat_dev, lat_host, stats = [], [], []
     with Session(t, g, b, s, precision=prec, device=local) as m:
@@ -495,6 +521,7 @@ def run_ours(args):
         "kernels_per_frame": int(kpf.value),
         "ate_gt_mm": ate * 1e3,
         "accuracy_vs_fp64": acc,
+        "precision_forms": forms or None,
         "map": {"blocks_total": st_avg["blocks_total"], "visible_per_frame": st_avg["blocks_visible"],
                 "load_factor": st_avg["blocks_total"] / (t.num_buckets * t.bucket_size)},
     }
@@ -955,6 +982,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--ref-seconds", type=float, default=90.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-forms", dest="forms", action="store_false",
+                    help="skip the mixed / band throughput passes of the default run")
     ap.add_argument("--fp64-frames", type=int, default=8,
                     help="frames scored against the FP64 oracle (0: skip)")
     ap.add_argument("--max-blocks", type=int, default=0,
