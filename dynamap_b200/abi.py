@@ -114,6 +114,8 @@ SIGNATURES = {
     "dyn_session_set_pose": (C.c_int, [_vp, P(C.c_float)]),
     "dyn_frame_submit": (C.c_int, [_vp, _vp, _vp]),
     "dyn_frame_submit_device": (C.c_int, [_vp, _vp, _vp]),
+    "dyn_frame_submit_hint": (C.c_int, [_vp, _vp, _vp, P(C.c_float)]),
+    "dyn_raycast_maps": (C.c_int, [_vp, P(C.c_float), P(Sensor), _vp, _vp, _vp, _vp]),
     "dyn_frame_result": (C.c_int, [_vp, P(C.c_float), P(FrameStats)]),
     "dyn_integrate_with_pose": (C.c_int, [_vp, _vp, _vp, P(C.c_float)]),
     "dyn_raycast": (C.c_int, [_vp, P(C.c_float), P(Sensor), _vp, _vp]),

@@ -474,6 +474,78 @@ __global__ void fused_pose_finalize_kernel(const SessDev* __restrict__ tab, int 
   if (bump) S.pose->frame += 1;
 }
 
+// SE(3) logarithm of a rigid transform T (row-major 4x4), the inverse of
+// se3_exp: w from the rotation angle and axis, t = V^-1 translation with
+// V^-1 = I - W/2 + (1 - a / (2 b)) / th^2 W^2 (a = sin th / th,
+// b = (1 - cos th) / th^2; series below th = 1e-4).
+__device__ void se3_log(const double* T, double* xi) {
+  const double tr = T[0] + T[5] + T[10];
+  double c = 0.5 * (tr - 1.0);
+  c = c > 1.0 ? 1.0 : (c < -1.0 ? -1.0 : c);
+  const double th = acos(c);
+  const double vx = T[9] - T[6], vy = T[2] - T[8], vz = T[4] - T[1];
+  double f;  // th / (2 sin th)
+  if (th < 1e-4) f = 0.5 + th * th / 12.0;
+  else f = th / (2.0 * sin(th));
+  const double w0 = f * vx, w1 = f * vy, w2 = f * vz;
+  double g;  // (1 - a / (2 b)) / th^2
+  if (th < 1e-4) g = 1.0 / 12.0 + th * th / 720.0;
+  else g = (1.0 - (sin(th) / th) / (2.0 * (1.0 - cos(th)) / (th * th))) / (th * th);
+  const double W[9] = {0, -w2, w1, w2, 0, -w0, -w1, w0, 0};
+  double W2[9];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double s = 0;
+      for (int k = 0; k < 3; ++k) s += W[i * 3 + k] * W[k * 3 + j];
+      W2[i * 3 + j] = s;
+    }
+  const double t[3] = {T[3], T[7], T[11]};
+  xi[0] = w0;
+  xi[1] = w1;
+  xi[2] = w2;
+  for (int i = 0; i < 3; ++i) {
+    double s = 0;
+    for (int j = 0; j < 3; ++j) {
+      const double Vi = (i == j ? 1.0 : 0.0) - 0.5 * W[i * 3 + j] + g * W2[i * 3 + j];
+      s += Vi * t[j];
+    }
+    xi[3 + i] = s;
+  }
+}
+
+// rel = pose^-1 * hint (hint * pose^-1 when increments compose on the
+// left); the solver starts at log(rel).  Before the first target exists
+// the hint becomes the pose.
+__global__ void pose_hint_kernel(PoseState* ps, IcpState* st, const double* hint,
+                                 int compose_left) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (!st->have_target) {
+    for (int k = 0; k < 16; ++k) ps->pose[k] = hint[k];
+    finish_pose(ps);
+    return;
+  }
+  const double* P = ps->pose;
+  double inv[16];
+  for (int i = 0; i < 3; ++i) {
+    for (int j = 0; j < 3; ++j) inv[i * 4 + j] = P[j * 4 + i];
+    inv[i * 4 + 3] = -(P[0 * 4 + i] * P[3] + P[1 * 4 + i] * P[7] + P[2 * 4 + i] * P[11]);
+  }
+  inv[12] = inv[13] = inv[14] = 0.0;
+  inv[15] = 1.0;
+  double rel[16];
+  if (compose_left) matmul4d(hint, inv, rel);
+  else matmul4d(inv, hint, rel);
+  double xi[6];
+  se3_log(rel, xi);
+  for (int k = 0; k < 6; ++k) {
+    st->inc[k] = xi[k];
+    st->prev[k] = xi[k];
+  }
+  double Td[16];
+  se3_exp(xi, Td);
+  for (int k = 0; k < 16; ++k) st->T[k] = (float)Td[k];
+}
+
 __global__ void pose_set_kernel(PoseState* ps, const double* pose) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   for (int k = 0; k < 16; ++k) ps->pose[k] = pose[k];
@@ -495,6 +567,11 @@ void launch_icp_iteration(const IcpLevel& L, const IcpParams& P, int pl, int it,
 
 void launch_pose_finalize(const IcpParams& P, IcpState* st, PoseState* ps, cudaStream_t stream) {
   pose_finalize_kernel<<<1, 32, 0, stream>>>(P, st, ps);
+}
+
+void launch_pose_hint(PoseState* ps, IcpState* st, const double* hint_dev, int compose_left,
+                      cudaStream_t stream) {
+  pose_hint_kernel<<<1, 32, 0, stream>>>(ps, st, hint_dev, compose_left);
 }
 
 void launch_pose_set(PoseState* ps, const double* pose_dev, cudaStream_t stream) {

@@ -62,6 +62,11 @@ void launch_icp_iteration(const IcpLevel& L, const IcpParams& P, int pl, int it,
 // of the solver state.  Runs with one thread.
 void launch_pose_finalize(const IcpParams& P, IcpState* st, PoseState* ps,
                           cudaStream_t stream);
+// Tracking of the next frame starts from the motion from the current pose
+// to 'hint' (double[16], camera-to-world): the solver's increment becomes
+// its SE(3) logarithm (before the first target, the hint becomes the pose).
+void launch_pose_hint(PoseState* ps, IcpState* st, const double* hint_dev, int compose_left,
+                      cudaStream_t stream);
 // Set the pose from the host (double[16]); recomputes posef/invf.
 void launch_pose_set(PoseState* ps, const double* pose_dev, cudaStream_t stream);
 // Normal equations only (no solve): out[29] doubles on the device.

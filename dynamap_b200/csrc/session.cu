@@ -764,6 +764,23 @@ dyn_status dyn_frame_submit(dyn_session* s, const uint16_t* depth_host, const ui
   return launch_frame(s);
 }
 
+dyn_status dyn_frame_submit_hint(dyn_session* s, const uint16_t* depth_host,
+                                 const uint8_t* rgb_host, const float pose_hint[16]) {
+  if (!s || !depth_host || s->batch || s->owner_stream) return DYN_ERR_INVALID_ARG;
+  if (!pose_hint) return dyn_frame_submit(s, depth_host, rgb_host);
+  DeviceGuard dg(s->device);
+  double H[16];
+  for (int k = 0; k < 16; ++k) H[k] = (double)pose_hint[k];
+  // pageable source: staged before the call returns; stream-ordered after
+  // the previous frame (whose pose the hint is taken relative to)
+  DYN_CUDA(cudaMemcpyAsync(s->d_pose_in, H, sizeof(H), cudaMemcpyHostToDevice, s->stream));
+  launch_pose_hint(s->d_pose, s->d_icp, s->d_pose_in, s->gp.compose_left, s->stream);
+  DYN_CUDA(cudaGetLastError());
+  dyn_status r = upload_frame(s, depth_host, rgb_host);
+  if (r != DYN_OK) return r;
+  return launch_frame(s);
+}
+
 dyn_status dyn_frame_submit_device(dyn_session* s, const uint16_t* depth_dev, const uint8_t* rgb_dev) {
   if (!s || !depth_dev || s->batch || s->owner_stream) return DYN_ERR_INVALID_ARG;
   DeviceGuard dg(s->device);
@@ -876,6 +893,44 @@ dyn_status dyn_raycast(dyn_session* s, const float pose[16], const dyn_sensor* v
   if (rgb_host)
     DYN_CUDA(cudaMemcpyAsync(rgb_host, s->d_trgb, n * 3, cudaMemcpyDeviceToHost, s->stream));
   DYN_CUDA(cudaStreamSynchronize(s->stream));
+  return DYN_OK;
+}
+
+dyn_status dyn_raycast_maps(dyn_session* s, const float pose[16], const dyn_sensor* virt,
+                            float* depth_host, float* vertex4_host, float* normal4_host,
+                            uint8_t* rgb_host) {
+  if (!s || !pose) return DYN_ERR_INVALID_ARG;
+  dyn_sensor vs = virt ? *virt : s->sensor;
+  if (!valid_sensor(&vs) || (size_t)vs.rows * vs.cols > s->npx) return DYN_ERR_INVALID_ARG;
+  DeviceGuard dg(s->device);
+  DYN_TRY(quiesce(s));
+  cudaStream_t st = s->stream;
+  DYN_CUDA(cudaMemcpyAsync(s->d_pose_override, pose, 64, cudaMemcpyHostToDevice, st));
+  const size_t n = (size_t)vs.rows * vs.cols;
+  launch_raycast(s->vol, dsensor(vs), s->d_pose, s->d_pose_override, s->d_ray,
+                 rgb_host ? s->d_trgb : nullptr, st);
+  // misses (at max_sensor_depth or beyond) become invalid depth, then the
+  // maps of that depth in the raycast camera's frame
+  launch_target_prepare(s->d_ray, s->d_filt, s->tp.max_sensor_depth, nullptr, nullptr, (int)n,
+                        st);
+  MapsArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.lv[0].depth = s->d_filt;
+  a.lv[0].normal = s->d_snrm[0];
+  a.lv[0].vertex = s->d_svtx[0];
+  a.lv[0].s = dsensor(vs);
+  a.nlev = 1;
+  a.total = (int)n;
+  launch_maps(a, st);
+  DYN_CUDA(cudaGetLastError());
+  if (depth_host)
+    DYN_CUDA(cudaMemcpyAsync(depth_host, s->d_ray, n * 4, cudaMemcpyDeviceToHost, st));
+  if (vertex4_host)
+    DYN_CUDA(cudaMemcpyAsync(vertex4_host, s->d_svtx[0], n * 16, cudaMemcpyDeviceToHost, st));
+  if (normal4_host)
+    DYN_CUDA(cudaMemcpyAsync(normal4_host, s->d_snrm[0], n * 16, cudaMemcpyDeviceToHost, st));
+  if (rgb_host) DYN_CUDA(cudaMemcpyAsync(rgb_host, s->d_trgb, n * 3, cudaMemcpyDeviceToHost, st));
+  DYN_CUDA(cudaStreamSynchronize(st));
   return DYN_OK;
 }
 

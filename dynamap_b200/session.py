@@ -96,11 +96,15 @@ class Session:
         return np.array(out, np.float32).reshape(4, 4)
 
     # ---- frames
-    def submit(self, depth: np.ndarray, rgb: np.ndarray | None = None) -> None:
+    def submit(self, depth: np.ndarray, rgb: np.ndarray | None = None, pose_hint=None) -> None:
         d = np.ascontiguousarray(depth, np.uint16)
         r = None if rgb is None else np.ascontiguousarray(rgb, np.uint8)
         self._keep = (d, r)
-        abi.check("dyn_frame_submit", self.lib.dyn_frame_submit(self.h, _ptr(d), _ptr(r)))
+        if pose_hint is None:
+            abi.check("dyn_frame_submit", self.lib.dyn_frame_submit(self.h, _ptr(d), _ptr(r)))
+        else:
+            abi.check("dyn_frame_submit_hint", self.lib.dyn_frame_submit_hint(
+                self.h, _ptr(d), _ptr(r), _f16(pose_hint)))
 
     def submit_device(self, depth_ptr: int, rgb_ptr: int | None = None) -> None:
         abi.check("dyn_frame_submit_device",
@@ -114,8 +118,8 @@ class Session:
             abi.check("dyn_frame_result", r)
         return np.array(pose, np.float32).reshape(4, 4), st
 
-    def process(self, depth, rgb=None, strict: bool = True):
-        self.submit(depth, rgb)
+    def process(self, depth, rgb=None, strict: bool = True, pose_hint=None):
+        self.submit(depth, rgb, pose_hint)
         return self.result(strict)
 
     def integrate_with_pose(self, depth, rgb, pose) -> None:
@@ -131,6 +135,18 @@ class Session:
         abi.check("dyn_raycast", self.lib.dyn_raycast(
             self.h, _f16(pose), C.byref(s) if sensor is not None else None, _ptr(d), _ptr(c)))
         return d, c
+
+    def raycast_maps(self, pose, sensor=None, rgb: bool = False):
+        """(depth, vertex4, normal4, rgb) of the model seen from 'pose'."""
+        s = sensor if sensor is not None else self.sensor
+        d = np.empty((s.rows, s.cols), np.float32)
+        v = np.empty((s.rows, s.cols, 4), np.float32)
+        n = np.empty((s.rows, s.cols, 4), np.float32)
+        c = np.empty((s.rows, s.cols, 3), np.uint8) if rgb else None
+        abi.check("dyn_raycast_maps", self.lib.dyn_raycast_maps(
+            self.h, _f16(pose), C.byref(s) if sensor is not None else None, _ptr(d), _ptr(v),
+            _ptr(n), _ptr(c)))
+        return d, v, n, c
 
     # ---- map access
     def num_blocks(self) -> int:

@@ -206,6 +206,14 @@ dyn_status dyn_frame_submit(dyn_session* s, const uint16_t* depth_host,
 /* Same, with the frame already resident on the device. */
 dyn_status dyn_frame_submit_device(dyn_session* s, const uint16_t* depth_dev,
                                    const uint8_t* rgb_dev /* nullable */);
+/* dyn_frame_submit with an initial estimate of the new camera pose
+ * (row-major camera-to-world, e.g. from odometry): tracking starts from
+ * the motion it implies relative to the current pose instead of from no
+ * motion.  A null hint is dyn_frame_submit.  No counterpart in the
+ * reference (its ICP always starts from the previous pose). */
+dyn_status dyn_frame_submit_hint(dyn_session* s, const uint16_t* depth_host,
+                                 const uint8_t* rgb_host /* nullable */,
+                                 const float pose_hint[16] /* nullable */);
 /* Waits for the last submitted frame; returns its pose and counters. */
 dyn_status dyn_frame_result(dyn_session* s, float pose_out[16],
                             dyn_frame_stats* stats /* nullable */);
@@ -237,6 +245,16 @@ dyn_status dyn_solver_solve(dyn_session* s, const float* target_depth_host,
 dyn_status dyn_raycast(dyn_session* s, const float pose[16],
                        const dyn_sensor* virt, float* depth_host,
                        uint8_t* rgb_host /* nullable */);
+
+/* dyn_raycast plus the raycast's vertex and normal maps in the camera frame
+ * (rgbdImage::getPointCloudXYZ / getNormalsfromVertices, rgbdImage.cu:23-167,
+ * applied to the raycast depth with misses as invalid): float4 per pixel,
+ * zero where invalid.  Any output may be NULL.  Uses the session's source
+ * image buffers as scratch (they are rewritten by the next frame).
+ * Synchronous. */
+dyn_status dyn_raycast_maps(dyn_session* s, const float pose[16], const dyn_sensor* virt,
+                            float* depth_host, float* vertex4_host, float* normal4_host,
+                            uint8_t* rgb_host);
 
 /* Number of allocated blocks (HashTable::GetNumAllocatedBlocks,
  * hashTable.cu:165). */
