@@ -147,6 +147,8 @@ SIGNATURES = {
     "dyn_batch_profile": (C.c_int, [_vp, C.c_int32]),
     "dyn_batch_stage_times": (C.c_int, [_vp, P(C.c_double), P(C.c_int64), C.c_int32]),
     "dyn_batch_kernels_per_frame": (C.c_int, [_vp, P(C.c_int32)]),
+    "dyn_batch_autotune": (C.c_int, [_vp, C.c_int32]),
+    "dyn_batch_tuning": (C.c_int, [_vp, P(C.c_int32), P(C.c_int32), P(C.c_int32)]),
     "dyn_server_create": (C.c_int, [P(ServerParams), P(_vp)]),
     "dyn_server_destroy": (C.c_int, [_vp]),
     "dyn_server_admit": (C.c_int, [_vp, P(TsdfParams), P(GnParams), P(BilateralParams),

@@ -154,7 +154,59 @@ static dyn_status batch_ready(dyn_batch* b) {
   return DYN_OK;
 }
 
+// Autotuner candidates: launch shapes that change no result (integration
+// CTAs, raycast tile), so they can be timed on live frames.
+struct TuneCandidate {
+  int integrate_ctas, ray_tile;
+};
+constexpr TuneCandidate kTune[] = {{148 * 8, 0}, {148 * 4, 0}, {148 * 16, 0},
+                                   {148 * 8, 1}, {148 * 4, 1}, {148 * 16, 1},
+                                   {148 * 8, 2}, {148 * 4, 2}, {148 * 16, 2}};
+constexpr int kNumTune = (int)(sizeof(kTune) / sizeof(kTune[0]));
+
+static void apply_shape(dyn_batch* b, const TuneCandidate& c) {
+  for (int g = 0; g < b->groups.k; ++g) {
+    b->groups.shape[g].integrate_ctas = c.integrate_ctas;
+    b->groups.shape[g].ray_tile = c.ray_tile;
+  }
+  b->single.shape[0].integrate_ctas = c.integrate_ctas;
+  b->single.shape[0].ray_tile = c.ray_tile;
+  if (b->exec) {
+    cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+  }
+}
+
+// Reads the last timed frame and moves through the candidates: each runs
+// tune_frames frames, its first (graph capture and upload) not counted;
+// after the last one the fastest is kept.
+static dyn_status tune_step(dyn_batch* b) {
+  if (b->tune_pending) {
+    DYN_CUDA(cudaEventSynchronize(b->tune_ev[1]));
+    float ms = 0.0f;
+    DYN_CUDA(cudaEventElapsedTime(&ms, b->tune_ev[0], b->tune_ev[1]));
+    b->tune_pending = false;
+    if (b->tune_count > 0) b->tune_ms[b->tune_idx] += ms;
+    if (++b->tune_count >= b->tune_frames) {
+      b->tune_count = 0;
+      if (++b->tune_idx == kNumTune) {
+        int best = 0;
+        for (int i = 1; i < kNumTune; ++i)
+          if (b->tune_ms[i] < b->tune_ms[best]) best = i;
+        b->tune_best = best;
+        apply_shape(b, kTune[best]);
+        return DYN_OK;
+      }
+      apply_shape(b, kTune[b->tune_idx]);
+    }
+  }
+  return DYN_OK;
+}
+
 static dyn_status batch_launch(dyn_batch* b) {
+  const bool tuning = b->tune_frames > 0 && b->tune_best < 0;
+  if (tuning) DYN_TRY(tune_step(b));
+  const bool timed = b->tune_frames > 0 && b->tune_best < 0;
   if (!b->exec) {
     Marks m;
     m.on = b->profile;
@@ -166,7 +218,12 @@ static dyn_status batch_launch(dyn_batch* b) {
                                   m, &b->exec, &b->kernels_per_frame);
     if (r != DYN_OK) return r;
   }
+  if (timed) DYN_CUDA(cudaEventRecord(b->tune_ev[0], b->stream));
   DYN_CUDA(cudaGraphLaunch(b->exec, b->stream));
+  if (timed) {
+    DYN_CUDA(cudaEventRecord(b->tune_ev[1], b->stream));
+    b->tune_pending = true;
+  }
   b->pending = true;
   for (dyn_session* s : b->ss) s->frames++;
   return DYN_OK;
@@ -266,6 +323,32 @@ dyn_status dyn_batch_stage_times(dyn_batch* b, double ms_out[DYN_NUM_STAGES],
     for (int k = 0; k < DYN_NUM_STAGES; ++k) b->stage_ms[k] = 0.0;
     b->prof_frames = 0;
   }
+  return DYN_OK;
+}
+
+dyn_status dyn_batch_autotune(dyn_batch* b, int32_t frames_per_candidate) {
+  if (!b || frames_per_candidate < 0 || frames_per_candidate == 1) return DYN_ERR_INVALID_ARG;
+  DeviceGuard dg(b->device);
+  DYN_CUDA(cudaStreamSynchronize(b->stream));
+  for (int k = 0; k < 2; ++k)
+    if (!b->tune_ev[k]) DYN_CUDA(cudaEventCreate(&b->tune_ev[k]));
+  b->tune_frames = frames_per_candidate;
+  b->tune_idx = 0;
+  b->tune_count = 0;
+  b->tune_best = -1;
+  b->tune_pending = false;
+  b->tune_ms.assign(kNumTune, 0.0f);
+  apply_shape(b, kTune[0]);  // the default shape, measured first
+  return DYN_OK;
+}
+
+dyn_status dyn_batch_tuning(dyn_batch* b, int32_t* done, int32_t* integrate_ctas,
+                            int32_t* ray_tile) {
+  if (!b) return DYN_ERR_INVALID_ARG;
+  const BatchShape& sh = b->groups.shape[0];
+  if (done) *done = b->tune_best >= 0 ? 1 : 0;
+  if (integrate_ctas) *integrate_ctas = sh.integrate_ctas > 0 ? sh.integrate_ctas : 148 * 8;
+  if (ray_tile) *ray_tile = sh.ray_tile;
   return DYN_OK;
 }
 

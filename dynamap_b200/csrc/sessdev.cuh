@@ -71,6 +71,11 @@ struct BatchShape {
   int max_rb_tiles;        // largest ray-start bound (tiles; at least 1)
   int kahan_mask;          // bit 0: some session sums plainly, bit 1: some use Kahan sums
   int fp16_mask;           // bit 0: some session keeps FP32 voxels, bit 1: some mixed
+  // launch shapes that leave every result unchanged (chosen by a batch's
+  // autotuner): CTAs of the integration grid (0: 148 x 8) and the raycast
+  // tile (0: 16x16, 1: 32x8, 2: 8x8 pixels)
+  int integrate_ctas;
+  int ray_tile;
   int2* gvis;              // batch-wide visible list (session, heap index)
   int* gcount;             // its length (device)
   int gvis_cap;

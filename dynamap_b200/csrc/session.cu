@@ -41,6 +41,8 @@ void release(dyn_batch* b) {
     if (b->groups.join[g]) cudaEventDestroy(b->groups.join[g]);
   }
   if (b->groups.fork) cudaEventDestroy(b->groups.fork);
+  for (cudaEvent_t e : b->tune_ev)
+    if (e) cudaEventDestroy(e);
   for (void* p : b->allocs) cudaFree(p);
   if (b->h_res) cudaFreeHost(b->h_res);
   if (b->h2d_done) cudaEventDestroy(b->h2d_done);

@@ -256,6 +256,15 @@ struct dyn_batch {
   cudaEvent_t ev[DYN_NUM_STAGES] = {};
   double stage_ms[DYN_NUM_STAGES] = {};
   int64_t prof_frames = 0;
+  // autotuner: result-invariant launch shapes timed on the batch's own
+  // frames (tune_frames per candidate; tune_idx the candidate measured)
+  int tune_frames = 0;
+  int tune_idx = -1;
+  int tune_count = 0;
+  int tune_best = -1;
+  bool tune_pending = false;
+  cudaEvent_t tune_ev[2] = {nullptr, nullptr};
+  std::vector<float> tune_ms;
   bool pending = false;
 };
 

@@ -856,22 +856,24 @@ __device__ inline bool raycast_mixed_px(const VolumeDev& v, const DSensor& s, co
 
 // One 16x16 pixel tile (tile bx, by) from pose16 (a float 4x4); warps cover
 // 8x4 pixel sub-tiles for coherent rays.  Step-cap overruns are counted.
-template <bool MIXED>
+// The tile is TX x TY pixels (multiples of 8 x 4; TX * TY >= 64).
+template <bool MIXED, int TX = kRayTX, int TY = kRayTY>
 __device__ inline void raycast_tile(const VolumeDev& v, const DSensor& s,
                                     const float* __restrict__ pose16, float* __restrict__ depth_out,
                                     uint8_t* __restrict__ rgb_out, int bx, int by,
                                     const unsigned* __restrict__ rbound, int tiles_x) {
+  static_assert(TX % 8 == 0 && TY % 4 == 0 && TX * TY >= 64, "tile of 8x4 warps");
   __shared__ M4f Ts;
   __shared__ int over;
-  const int tid = threadIdx.y * kRayTX + threadIdx.x;
+  const int tid = threadIdx.y * TX + threadIdx.x;
   if (tid < 16) Ts.m[tid] = pose16[tid];
   if (tid == 0) over = 0;
   __syncthreads();
   const M4f T = Ts;  // the pose in registers for the whole march
   const int warp = tid >> 5, lane = tid & 31;
-  const int lx = (warp & 1) * 8 + (lane & 7);
-  const int ly = (warp >> 1) * 4 + (lane >> 3);
-  const int x = bx * kRayTX + lx, y = by * kRayTY + ly;
+  const int lx = (warp % (TX / 8)) * 8 + (lane & 7);
+  const int ly = (warp / (TX / 8)) * 4 + (lane >> 3);
+  const int x = bx * TX + lx, y = by * TY + ly;
   if (x < s.cols && y < s.rows) {
     const float skip_to =
         rbound ? __uint_as_float(rbound[(y / kRbTile) * tiles_x + x / kRbTile]) : 0.0f;
@@ -893,17 +895,25 @@ __global__ void __launch_bounds__(kRayTX* kRayTY)
 }
 
 // next frame's target of every mode-1 session (blockIdx.z) at its new pose;
-// one instantiation per voxel form, sessions of the other form return
-template <bool MIXED>
-__global__ void __launch_bounds__(kRayTX* kRayTY)
+// one instantiation per voxel form (sessions of the other form return) and
+// per tile shape (every pixel's march is independent of the tiling)
+template <bool MIXED, int TX, int TY>
+__global__ void __launch_bounds__(TX* TY)
     fused_raycast_kernel(const SessDev* __restrict__ tab) {
   const SessDev& S = tab[blockIdx.z];
   if (S.mode != 1 || (S.vol.fp16 != 0) != MIXED) return;
   const DSensor& s = S.ls[0];
-  if ((int)blockIdx.x * kRayTX >= s.cols || (int)blockIdx.y * kRayTY >= s.rows) return;
+  if ((int)blockIdx.x * TX >= s.cols || (int)blockIdx.y * TY >= s.rows) return;
   uint8_t* rgb_out = S.use_color ? S.trgb : nullptr;
-  raycast_tile<MIXED>(S.vol, s, S.pose->posef, S.ray, rgb_out, blockIdx.x, blockIdx.y,
-                      MIXED ? S.rbound : nullptr, S.rb_tx);
+  raycast_tile<MIXED, TX, TY>(S.vol, s, S.pose->posef, S.ray, rgb_out, blockIdx.x, blockIdx.y,
+                              MIXED ? S.rbound : nullptr, S.rb_tx);
+}
+
+template <int TX, int TY>
+void launch_fused_raycast(const SessDev* tab, const BatchShape& b, cudaStream_t st) {
+  dim3 grid((b.max_cols + TX - 1) / TX, (b.max_rows + TY - 1) / TY, b.n);
+  if (b.fp16_mask & 1) fused_raycast_kernel<false, TX, TY><<<grid, dim3(TX, TY), 0, st>>>(tab);
+  if (b.fp16_mask & 2) fused_raycast_kernel<true, TX, TY><<<grid, dim3(TX, TY), 0, st>>>(tab);
 }
 
 // per-frame counters of every session (all but nalloc, the heap top) and
@@ -996,13 +1006,16 @@ void fused_visible(const SessDev* tab, const BatchShape& b, cudaStream_t st) {
 }
 
 void fused_integrate(const SessDev* tab, const BatchShape& b, cudaStream_t st) {
-  fused_integrate_kernel<<<148 * 8, kBlockVox, 0, st>>>(tab, b.gvis, b.gcount);
+  fused_integrate_kernel<<<b.integrate_ctas > 0 ? b.integrate_ctas : 148 * 8, kBlockVox, 0,
+                           st>>>(tab, b.gvis, b.gcount);
 }
 
 void fused_raycast(const SessDev* tab, const BatchShape& b, cudaStream_t st) {
-  dim3 grid(nblk(b.max_cols, kRayTX), nblk(b.max_rows, kRayTY), b.n);
-  if (b.fp16_mask & 1) fused_raycast_kernel<false><<<grid, dim3(kRayTX, kRayTY), 0, st>>>(tab);
-  if (b.fp16_mask & 2) fused_raycast_kernel<true><<<grid, dim3(kRayTX, kRayTY), 0, st>>>(tab);
+  switch (b.ray_tile) {
+    case 1: launch_fused_raycast<32, 8>(tab, b, st); break;
+    case 2: launch_fused_raycast<8, 8>(tab, b, st); break;
+    default: launch_fused_raycast<16, 16>(tab, b, st); break;
+  }
 }
 
 }  // namespace dyn

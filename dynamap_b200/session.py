@@ -238,6 +238,16 @@ class Batch:
                   self.lib.dyn_batch_stage_times(self.h, ms, C.byref(n), int(reset)))
         return list(ms), n.value
 
+    def autotune(self, frames_per_candidate: int = 3) -> None:
+        abi.check("dyn_batch_autotune", self.lib.dyn_batch_autotune(self.h, frames_per_candidate))
+
+    def tuning(self):
+        """(done, integration CTAs, raycast tile: 0 16x16, 1 32x8, 2 8x8)."""
+        d, c, t = C.c_int32(), C.c_int32(), C.c_int32()
+        abi.check("dyn_batch_tuning",
+                  self.lib.dyn_batch_tuning(self.h, C.byref(d), C.byref(c), C.byref(t)))
+        return bool(d.value), c.value, t.value
+
     def kernels_per_frame(self) -> int:
         n = C.c_int32()
         abi.check("dyn_batch_kernels_per_frame",

@@ -411,6 +411,16 @@ dyn_status dyn_batch_profile(dyn_batch* b, int32_t enable);
 dyn_status dyn_batch_stage_times(dyn_batch* b, double ms_out[DYN_NUM_STAGES],
                                  int64_t* frames_out, int32_t reset);
 dyn_status dyn_batch_kernels_per_frame(dyn_batch* b, int32_t* n_out);
+/* Autotuner: over the next frames the batch times each candidate launch
+ * shape -- integration grid 592 / 1184 / 2368 CTAs x raycast tile 16x16 /
+ * 32x8 / 8x8 pixels, shapes that change no result -- for
+ * frames_per_candidate frames (the first of each not counted; at least 2),
+ * then keeps the fastest.  0 restores the default shape.  No counterpart in
+ * the reference. */
+dyn_status dyn_batch_autotune(dyn_batch* b, int32_t frames_per_candidate);
+/* done: tuning finished; the shape in use (ray_tile: 0 16x16, 1 32x8, 2 8x8). */
+dyn_status dyn_batch_tuning(dyn_batch* b, int32_t* done, int32_t* integrate_ctas,
+                            int32_t* ray_tile);
 
 /* dyn_server: the serving loop's device side.  Sessions are admitted while
  * their device bytes (dyn_session_bytes, with a mixed session's colour only

@@ -184,3 +184,38 @@ def test_grouped_batch_matches_sessions_alone(gpu_lib):
     finally:
         for m in sess:
             m.close()
+
+
+def test_autotune_keeps_results(gpu_lib):
+    """The autotuner times nine launch shapes on the batch's own frames and
+    keeps the fastest; the shapes change no result, so every frame matches
+    the sessions stepped alone."""
+    p = configs.preset("cfg1")
+    p["sensor"].update(rows=120, cols=160, fx=131.25, fy=131.25, cx=79.5, cy=59.5)
+    p["tsdf"].update(voxel_size=0.01, truncation_distance=0.04, num_blocks=1 << 13,
+                     num_buckets=1 << 14)
+    n, nf = 3, 22
+    seqs = [configs.sequence(p, seed=120 + i, n_frames=nf) for i in range(n)]
+    t, g, b, s = configs.structs(p)
+    precs = [abi.PRECISION_FP32, abi.PRECISION_MIXED, abi.PRECISION_MIXED_BAND]
+    alone = []
+    for i in range(n):
+        with Session(t, g, b, s, precision=precs[i]) as m:
+            m.set_pose(seqs[i].poses[0])
+            alone.append([m.process(d)[0] for d in seqs[i].depth])
+    sess = [Session(t, g, b, s, precision=precs[i]) for i in range(n)]
+    try:
+        for i, m in enumerate(sess):
+            m.set_pose(seqs[i].poses[0])
+        with Batch(sess) as bt:
+            bt.autotune(2)
+            assert not bt.tuning()[0]
+            for k in range(nf):
+                poses, _, _ = bt.process([q.depth[k] for q in seqs])
+                for i in range(n):
+                    assert np.array_equal(poses[i], alone[i][k]), (i, k)
+            done, ctas, tile = bt.tuning()
+            assert done and ctas in (592, 1184, 2368) and tile in (0, 1, 2)
+    finally:
+        for m in sess:
+            m.close()
