@@ -143,33 +143,58 @@ __device__ inline void final_reduce(const double* __restrict__ partials, int nbl
 }
 
 // ---- FP64 6x6 algebra (one thread) --------------------------------------
-// LDL^T of a symmetric positive definite 6x6 (stands in for Eigen's
-// A.ldlt().solve(b), gnSolver.cu:439-442).  Returns false on a zero pivot.
-__device__ bool ldlt6(const double* A, const double* b, double* x) {
-  double L[36], D[6];
-  for (int k = 0; k < 36; ++k) L[k] = 0.0;
+// The 6x6 system lives in registers: every loop below has compile-time
+// bounds and is unrolled, so no array is indexed at run time (a run-time
+// index would put the arrays in local memory and make each dependent step
+// of the one-thread solve wait on an L1 round trip).  The lower triangle is
+// kept packed, row i at tri(i, 0) (the system is symmetric; the
+// factorisation reads only the lower triangle).
+__host__ __device__ constexpr int tri(int i, int j) { return i * (i + 1) / 2 + j; }
+
+// LDL^T of a symmetric positive definite 6x6 in place (stands in for
+// Eigen's A.ldlt().solve(b), gnSolver.cu:439-442): column j gives the pivot
+// D[j] = A[j][j] - sum_k L[j][k]^2 D[k] and L[i][j] = (A[i][j] - sum_k
+// L[i][k] L[j][k] D[k]) / D[j], each sum in increasing k; then forward
+// substitution, division by D, back substitution.  L overwrites the strict
+// lower triangle of a, D its diagonal.  Returns false on a zero pivot.
+__device__ __forceinline__ bool ldlt6(double (&a)[21], const double (&b)[6], double (&x)[6]) {
+  // triangular bounds are written as guards on fixed-length loops, so that
+  // every loop has a constant trip count and unrolls completely
+#pragma unroll
   for (int j = 0; j < 6; ++j) {
-    double s = A[j * 6 + j];
-    for (int k = 0; k < j; ++k) s -= L[j * 6 + k] * L[j * 6 + k] * D[k];
-    D[j] = s;
+    double s = a[tri(j, j)];
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+      if (k < j) s -= a[tri(j, k)] * a[tri(j, k)] * a[tri(k, k)];
+    a[tri(j, j)] = s;
     if (!(fabs(s) > 0.0)) return false;
-    L[j * 6 + j] = 1.0;
-    for (int i = j + 1; i < 6; ++i) {
-      double t = A[i * 6 + j];
-      for (int k = 0; k < j; ++k) t -= L[i * 6 + k] * L[j * 6 + k] * D[k];
-      L[i * 6 + j] = t / D[j];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+      if (i <= j) continue;
+      double t = a[tri(i, j)];
+#pragma unroll
+      for (int k = 0; k < 6; ++k)
+        if (k < j) t -= a[tri(i, k)] * a[tri(j, k)] * a[tri(k, k)];
+      a[tri(i, j)] = t / s;
     }
   }
   double y[6];
+#pragma unroll
   for (int i = 0; i < 6; ++i) {
     double t = b[i];
-    for (int k = 0; k < i; ++k) t -= L[i * 6 + k] * y[k];
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+      if (k < i) t -= a[tri(i, k)] * y[k];
     y[i] = t;
   }
-  for (int i = 0; i < 6; ++i) y[i] /= D[i];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) y[i] /= a[tri(i, i)];
+#pragma unroll
   for (int i = 5; i >= 0; --i) {
     double t = y[i];
-    for (int k = i + 1; k < 6; ++k) t -= L[k * 6 + i] * x[k];
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+      if (k > i) t -= a[tri(k, i)] * x[k];
     x[i] = t;
   }
   return true;
@@ -179,7 +204,7 @@ __device__ bool ldlt6(const double* A, const double* b, double* x) {
 // Rodrigues' formula and translation through the SE(3) left Jacobian,
 // R = I + a W + b W^2, t = (I + b W + c W^2) v, with a = sin t / t,
 // b = (1 - cos t)/t^2, c = (t - sin t)/t^3 (Taylor below t = 1e-4).
-__device__ void se3_exp(const double* xi, double* T) {
+__device__ __forceinline__ void se3_exp(const double* xi, double* T) {
   double w0 = xi[0], w1 = xi[1], w2 = xi[2];
   double th2 = w0 * w0 + w1 * w1 + w2 * w2, th = sqrt(th2);
   double a, b, c;
@@ -269,38 +294,57 @@ __device__ void inverse4f(const float* e, float* out) {
 }
 
 // gnSolver::solve's per-iteration host block (gnSolver.cu:389-415) for the
-// summed system 'acc'.  Updates inc/prev; returns true when converged.
+// summed system 'acc' (upper triangle row by row, then the 6 right-hand
+// sides): scale by 1 / max(A), add reg * max(scaled A) / it to the
+// diagonal, solve, accumulate.  The maxima run over all 36 entries in
+// row-major order, as over the full symmetric matrix.  Updates inc/prev;
+// returns true when converged.
+__device__ __forceinline__ double sym_at(const double (&a)[21], int i, int j) {
+  return i >= j ? a[tri(i, j)] : a[tri(j, i)];
+}
 __device__ bool gn_update(const double* acc, const IcpParams& P, int it, IcpState* st) {
-  double A[36], b[6];
-  int u = 0;
-  for (int i = 0; i < 6; ++i)
-    for (int j = i; j < 6; ++j) {
-      A[i * 6 + j] = acc[u];
-      A[j * 6 + i] = acc[u];
-      ++u;
-    }
+  double a[21], b[6];
+  {  // acc holds the upper triangle row by row
+#pragma unroll
+    for (int i = 0; i < 6; ++i)
+#pragma unroll
+      for (int j = 0; j < 6; ++j)
+        if (j >= i) a[tri(j, i)] = acc[i * 6 - i * (i - 1) / 2 + (j - i)];
+  }
+#pragma unroll
   for (int k = 0; k < 6; ++k) b[k] = acc[21 + k];
-  double mx = A[0];
-  for (int k = 1; k < 36; ++k) mx = fmax(mx, A[k]);
-  double scaling = 1.0 / mx;
+  double mx = a[0];
+#pragma unroll
+  for (int k = 1; k < 36; ++k) mx = fmax(mx, sym_at(a, k / 6, k % 6));
+  const double scaling = 1.0 / mx;
+#pragma unroll
   for (int k = 0; k < 6; ++k) b[k] *= scaling;
-  for (int k = 0; k < 36; ++k) A[k] *= scaling;
-  double mx2 = A[0];
-  for (int k = 1; k < 36; ++k) mx2 = fmax(mx2, A[k]);
-  double alpha = (double)P.reg * mx2;
-  for (int k = 0; k < 6; ++k) A[k * 6 + k] += alpha / (double)it;
+#pragma unroll
+  for (int k = 0; k < 21; ++k) a[k] *= scaling;
+  double mx2 = a[0];
+#pragma unroll
+  for (int k = 1; k < 36; ++k) mx2 = fmax(mx2, sym_at(a, k / 6, k % 6));
+  const double alpha = (double)P.reg * mx2;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) a[tri(k, k)] += alpha / (double)it;
   double d[6] = {0, 0, 0, 0, 0, 0};
-  if (!ldlt6(A, b, d))
+  if (!ldlt6(a, b, d)) {
+#pragma unroll
     for (int k = 0; k < 6; ++k) d[k] = __longlong_as_double(0x7ff8000000000000LL);
-  double ch = 0.0;
+  }
+  double inc[6], ch = 0.0;
+#pragma unroll
   for (int k = 0; k < 6; ++k) {
-    st->inc[k] += d[k];
-    double c = st->inc[k] - st->prev[k];
+    inc[k] = st->inc[k] + d[k];
+    st->inc[k] = inc[k];
+    double c = inc[k] - st->prev[k];
     ch += c * c;
   }
   bool conv = fabs(sqrt(ch)) <= (double)P.min_inc;
-  if (!conv)
-    for (int k = 0; k < 6; ++k) st->prev[k] = st->inc[k];
+  if (!conv) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) st->prev[k] = inc[k];
+  }
   return conv;
 }
 
@@ -371,7 +415,7 @@ __global__ void __launch_bounds__(kIcpThreads)
 // only the blocks of its own grid, so its reduction is the same as alone.
 // One instantiation per summation kind; sessions of the other kind return.
 template <bool KAHAN>
-__global__ void __launch_bounds__(kIcpThreads)
+__global__ void __launch_bounds__(kIcpThreads, 2)
     fused_icp_iteration_kernel(const SessDev* __restrict__ tab, int pl, int it) {
   const SessDev& S = tab[blockIdx.z];
   if ((S.icpp.kahan != 0) != KAHAN) return;

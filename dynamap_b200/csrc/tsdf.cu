@@ -517,13 +517,17 @@ struct BlockCache {
 // g = (int)(fl(p / vs) + sign(p) * 0.5), exactly.  Fast path: t = p * (1/vs)
 // + sign * 0.5 differs from the exactly rounded sum by at most 4 ulps (the
 // reciprocal, the product and the quotient each round once), so whenever t
-// is more than 2^-19 |t| (>= 16 ulps) away from every integer, truncating t
-// gives the same integer; otherwise the IEEE division decides.
+// is more than 2^-19 (|t| + 1) (>= 16 ulps) away from every integer,
+// truncating t gives the same integer; otherwise the IEEE division decides.
+// copysign(0.5, p) is sign(p) * 0.5 for p != 0; for p = +-0 the fast path
+// sees t = +-0.5, which truncates to the reference's 0; NaN and infinite t
+// fail the test and take the reference's expression.
 __device__ inline int voxel_index(float p, float vs, float inv_vs) {
-  const float sg = (float)((p > 0.0f) - (p < 0.0f));
-  const float t = __fadd_rn(__fmul_rn(p, inv_vs), sg * 0.5f);
+  const float t = __fadd_rn(__fmul_rn(p, inv_vs), copysignf(0.5f, p));
   const float n = rintf(t);
-  if (fabsf(t - n) > fmaxf(fabsf(t), 1.0f) * 1.9073486328125e-6f) return (int)t;
+  if (fabsf(t - n) > __fmaf_rn(fabsf(t), 1.9073486328125e-6f, 1.9073486328125e-6f))
+    return (int)t;
+  const float sg = (float)((p > 0.0f) - (p < 0.0f));
   return (int)(p / vs + sg * 0.5f);
 }
 // WorldToBlock / WorldToLocalVoxel (tsdf.cu:195-225) for block size 8: the
@@ -897,8 +901,10 @@ __global__ void __launch_bounds__(kRayTX* kRayTY)
 // next frame's target of every mode-1 session (blockIdx.z) at its new pose;
 // one instantiation per voxel form (sessions of the other form return) and
 // per tile shape (every pixel's march is independent of the tiling)
+// (at least 1024 threads resident per SM: the march is latency-bound, and
+// 4 CTAs of 256 hide more of it than the 3 that 76 registers allow)
 template <bool MIXED, int TX, int TY>
-__global__ void __launch_bounds__(TX* TY)
+__global__ void __launch_bounds__(TX* TY, 1024 / (TX * TY))
     fused_raycast_kernel(const SessDev* __restrict__ tab) {
   const SessDev& S = tab[blockIdx.z];
   if (S.mode != 1 || (S.vol.fp16 != 0) != MIXED) return;
