@@ -63,7 +63,10 @@ __device__ inline int bucket_insert(Entry* entries, const DTsdf& t, unsigned lon
       }
     }
     if (cur == key) {
-      if (atomicExch(&e->stamp, stamp) != stamp) atomicAdd(unique, 1);
+      // stamps only move forward to this frame's, so a stamp that already
+      // reads 'stamp' was counted by another ray: skip the contended atomic
+      if (*(volatile int*)&e->stamp != stamp && atomicExch(&e->stamp, stamp) != stamp)
+        atomicAdd(unique, 1);
       return -1;
     }
   }
@@ -160,8 +163,14 @@ __device__ inline void allocate_tile(const float* __restrict__ depth, const DSen
           unsigned h = set_hash(key);
           for (int p = 0; p < kSetProbes; ++p) {
             unsigned slot = (h + p) & (kSetSlots - 1);
-            unsigned long long old = atomicCAS(&sm.set[slot], kEmptyKey, key);
-            if (old == kEmptyKey || old == key) return;
+            // neighbouring rays visit the same blocks: most visits find
+            // their key already in the set with a plain read
+            unsigned long long old = *(volatile unsigned long long*)&sm.set[slot];
+            if (old == key) return;
+            if (old == kEmptyKey) {
+              old = atomicCAS(&sm.set[slot], kEmptyKey, key);
+              if (old == kEmptyKey || old == key) return;
+            }
           }
           // set saturated: insert directly
           int r = bucket_insert(v.entries, t, key, stamp, &sm.unique);
