@@ -206,14 +206,23 @@ __global__ void target_prepare_kernel(const float* __restrict__ ray, float* __re
 }
 
 // ---------------------------------------------------------------- fused
-// ingest (+ the unfiltered copy when the bilateral filter is off)
+// ingest (+ the unfiltered copy when the bilateral filter is off), and the
+// distance from the camera centre to each pixel's back-projected point
+// (IntegrateScanKernel's per-voxel |getPoint3d(pixel, depth)|,
+// tsdf.cu:316-317): it depends only on the pixel, so integration reads it
+// instead of recomputing it (two divisions and a square root) for every
+// voxel that projects there -- the same operations, so the same bits
 __global__ void fused_ingest_kernel(const SessDev* __restrict__ tab) {
   const SessDev& S = tab[blockIdx.z];
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= S.npx) return;
   ingest_px(S.u16, *S.rgb_flag ? S.rgb : nullptr, S.depth_scaler, S.raw,
             S.use_color ? S.sint[0] : nullptr, i);
-  if (!S.bil_enabled) S.filt[i] = S.raw[i];
+  const float d = S.raw[i];
+  if (!S.bil_enabled) S.filt[i] = d;
+  const DSensor& s0 = S.ls[0];
+  const int y = i / s0.cols;
+  S.sdist[i] = norm3(point3d_uv(i - y * s0.cols, y, d, s0));
 }
 
 __global__ void fused_bilateral_kernel(const SessDev* __restrict__ tab) {

@@ -30,6 +30,7 @@ struct SessDev {
   const uint8_t* rgb;
   // images
   float* raw;
+  float* sdist;         // |point3d_uv(x, y, raw)| per pixel (integration)
   float* filt;
   float* sdep[kLevels];
   float4* snrm[kLevels];

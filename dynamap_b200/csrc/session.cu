@@ -276,6 +276,7 @@ void fill_sessdev(dyn_session* s) {
   d.u16 = s->d_u16;
   d.rgb = s->d_rgb;
   d.raw = s->d_raw;
+  d.sdist = s->d_sdist;
   d.filt = s->d_filt;
   for (int l = 0; l < s->nlev; ++l) {
     d.sdep[l] = s->d_sdep[l];
@@ -530,6 +531,7 @@ dyn_status alloc_device_buffers(dyn_session* s) {
   DYN_TRY(s->dalloc(&s->d_u16, n * 2));
   DYN_TRY(s->dalloc(&s->d_rgb, n * 3));
   DYN_TRY(s->dalloc(&s->d_raw, n * 4));
+  DYN_TRY(s->dalloc(&s->d_sdist, n * 4));
   DYN_TRY(s->dalloc(&s->d_filt, n * 4));
   DYN_TRY(s->dalloc(&s->d_ray, n * 4));
   DYN_TRY(s->dalloc(&s->d_trgb, n * 3));

@@ -122,6 +122,7 @@ struct dyn_session {
   uint16_t* d_u16 = nullptr;
   uint8_t* d_rgb = nullptr;
   float* d_raw = nullptr;
+  float* d_sdist = nullptr;
   float* d_filt = nullptr;
   float* d_sdep[kLevels] = {};
   float4* d_snrm[kLevels] = {};

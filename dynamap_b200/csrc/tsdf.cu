@@ -382,6 +382,7 @@ __device__ inline float norm3_fast(F3 v) {
 
 template <bool FP16, bool FAST>
 __device__ inline void integrate_voxel(const VolumeDev& v, const float* __restrict__ depth,
+                                       const float* __restrict__ sdist,
                                        const uint8_t* __restrict__ rgb, const DSensor& s,
                                        const M4f& invT, int ptr, int lin) {
   const DTsdf& t = v.t;
@@ -421,8 +422,7 @@ __device__ inline void integrate_voxel(const VolumeDev& v, const float* __restri
     d = __ldg(depth + py * s.cols + px);
     if (d < t.dmin) return;
     if (d > t.dmax) return;
-    F3 p3 = point3d_uv(px, py, d, s);
-    sd = norm3(p3);
+    sd = __ldg(sdist + py * s.cols + px);  // norm3(point3d_uv(px, py, d, s))
     vd = norm3(vp);
   }
   const int idx = py * s.cols + px;
@@ -502,11 +502,11 @@ __global__ void __launch_bounds__(kBlockVox)
     const SessDev& S = tab[item.x];
     const uint8_t* rgb = *S.rgb_flag ? S.rgb : nullptr;
     if (!S.vol.fp16)
-      integrate_voxel<false, false>(S.vol, S.raw, rgb, S.ls[0], invT, item.y, threadIdx.x);
+      integrate_voxel<false, false>(S.vol, S.raw, S.sdist, rgb, S.ls[0], invT, item.y, threadIdx.x);
     else if (S.vol.t.band)
-      integrate_voxel<true, true>(S.vol, S.raw, rgb, S.ls[0], invT, item.y, threadIdx.x);
+      integrate_voxel<true, true>(S.vol, S.raw, S.sdist, rgb, S.ls[0], invT, item.y, threadIdx.x);
     else
-      integrate_voxel<true, false>(S.vol, S.raw, rgb, S.ls[0], invT, item.y, threadIdx.x);
+      integrate_voxel<true, false>(S.vol, S.raw, S.sdist, rgb, S.ls[0], invT, item.y, threadIdx.x);
   }
 }
 
