@@ -6,18 +6,34 @@
 // ln2), r computed with ln2 split into a 12-bit-exact high part and a low
 // part so that k*hi is exact; exp(r), |r| <= ln2/2, by its Taylor series to
 // degree 7 (truncation error below 6e-9 relative, under half a float ulp)
-// in Horner form with fused multiply-adds; the result scaled by 2^k
-// exactly.  Inputs below -87 return 0 (float underflow).
+// in Horner form with fused multiply-adds; the result times 2^k, one IEEE
+// multiplication by a power of two built from its bits (exact unless the
+// product is subnormal, where it rounds once: the correctly rounded
+// ldexpf(p, k)).  Inputs below -87 return 0 (float underflow).
 #pragma once
 
 #ifdef __CUDACC__
 #define DYN_HD __host__ __device__ inline
 #else
 #define DYN_HD inline
-#include <cmath>
 #endif
+#include <cmath>
+#include <cstdint>
+#include <cstring>
 
 namespace dyn {
+
+// 2^k for -126 <= k <= 127 (a normal float), exactly.
+DYN_HD float pow2i(int k) {
+#ifdef __CUDA_ARCH__
+  return __int_as_float((k + 127) << 23);
+#else
+  const uint32_t u = (uint32_t)(k + 127) << 23;
+  float f;
+  std::memcpy(&f, &u, sizeof f);
+  return f;
+#endif
+}
 
 DYN_HD float dyn_expf(float x) {
   if (!(x >= -87.0f)) return 0.0f;
@@ -36,7 +52,7 @@ DYN_HD float dyn_expf(float x) {
   p = fmaf(p, r, 0.5f);                           // 1/2!
   p = fmaf(p, r, 1.0f);
   p = fmaf(p, r, 1.0f);
-  return ldexpf(p, (int)k);
+  return p * pow2i((int)k);  // |x| <= 88: -126 <= k <= 127
 }
 
 // Bilateral range weight exp(-(x^2)/(2 sigma^2)) / (2 pi sigma^2) given

@@ -60,6 +60,7 @@ __device__ inline void bilateral_tile(const float* __restrict__ src, float* __re
                                       int by, float* tile) {
   const int D = 2 * tb.radius, half = tb.radius;
   const int TW = BTX + D - 1, TH = BTY + D - 1;
+  float* gs = tile + TW * TH;  // the spatial weights, staged once per CTA
   const int tid = threadIdx.y * BTX + threadIdx.x;
   const int row0 = by * BTY - half, col0 = bx * BTX - half;
   for (int k = tid; k < TW * TH; k += BTX * BTY) {
@@ -67,6 +68,7 @@ __device__ inline void bilateral_tile(const float* __restrict__ src, float* __re
     int gr = row0 + tr, gc = col0 + tc;
     tile[k] = (gr >= 0 && gr < rows && gc >= 0 && gc < cols) ? src[gr * cols + gc] : 0.0f;
   }
+  for (int k = tid; k < D * D; k += BTX * BTY) gs[k] = tb.gs[k];
   __syncthreads();
   const int x = by * BTY + threadIdx.y;  // row (the reference's x)
   const int y = bx * BTX + threadIdx.x;  // column
@@ -78,18 +80,19 @@ __device__ inline void bilateral_tile(const float* __restrict__ src, float* __re
   }
   const float inv2s2 = tb.inv2s2, norm = tb.norm;
   float acc = 0.0f, wp = 0.0f;
-  for (int i = 0; i < D; ++i) {
-    int nx = x - (half - i);
-    if (nx < 0 || nx >= rows) continue;
+  // the taps inside the image: row x - half + i in [0, rows), column
+  // y - half + j in [0, cols); summed in the reference's order
+  const int i0 = max(0, half - x), i1 = min(D, rows - x + half);
+  const int j0 = max(0, half - y), j1 = min(D, cols - y + half);
+  for (int i = i0; i < i1; ++i) {
     const float* trow = tile + (threadIdx.y + i) * TW + threadIdx.x;
-    for (int j = 0; j < D; ++j) {
-      int ny = y - (half - j);
-      if (ny < 0 || ny >= cols) continue;
+    const float* grow = gs + i * D;
+    for (int j = j0; j < j1; ++j) {
       float nv = trow[j];
       if (!(nv > 0.0f)) continue;
       const float dn = nv - c;
       float gi = FAST ? __expf(-(dn * dn) * inv2s2) * norm : range_weight(dn, inv2s2, norm);
-      float w = gi * tb.gs[i * D + j];
+      float w = gi * grow[j];
       acc += nv * w;
       wp += w;
     }
@@ -315,9 +318,10 @@ BilateralTable make_bilateral_table(int radius, float sigma_i, float sigma_s) {
   return tb;
 }
 
+// depth tile with its halo, then the D x D spatial weights
 static size_t bilateral_smem(int radius) {
   int D = 2 * radius;
-  return sizeof(float) * ((size_t)(BTX + D - 1) * (BTY + D - 1));
+  return sizeof(float) * ((size_t)(BTX + D - 1) * (BTY + D - 1) + (size_t)D * D);
 }
 
 void launch_bilateral(const float* src, float* dst, int rows, int cols, const BilateralTable& tb,
