@@ -127,17 +127,28 @@ __device__ inline void block_reduce(const Acc& a, bool kahan, double* red /*[8][
   __syncthreads();
 }
 
-// Sum of the per-block partials in FP64 (block order fixed per lane, then a
-// fixed shuffle tree).  out[29] in shared memory.
+// Sum of the per-block partials in FP64, in a fixed order: thread (g, k)
+// of 8 x 29 sums value k of blocks g, g + 8, g + 16, ... (all 29 values'
+// loads in flight at once, coalesced along k), then thread k adds the 8
+// group sums in group order.  'scratch' is 8 x 29 doubles of shared memory;
+// out[29] in shared memory.
 __device__ inline void final_reduce(const double* __restrict__ partials, int nblocks,
-                                    double* out) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int k = warp; k < kIcpVals; k += kIcpThreads / 32) {
+                                    double* out, double* scratch) {
+  constexpr int kGroups = kIcpThreads / 32;  // 8: scratch is the block-reduce array
+  const int t = threadIdx.x;
+  if (t < kGroups * kIcpVals) {
+    const int g = t / kIcpVals, k = t - g * kIcpVals;
     double s = 0.0;
-    for (int b = lane; b < nblocks; b += 32) s += __ldcg(partials + (size_t)b * kIcpVals + k);
+#pragma unroll 4
+    for (int b = g; b < nblocks; b += kGroups) s += __ldcg(partials + (size_t)b * kIcpVals + k);
+    scratch[g * kIcpVals + k] = s;
+  }
+  __syncthreads();
+  if (t < kIcpVals) {
+    double s = 0.0;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) out[k] = s;
+    for (int g = 0; g < kGroups; ++g) s += scratch[g * kIcpVals + t];
+    out[t] = s;
   }
   __syncthreads();
 }
@@ -390,7 +401,7 @@ __device__ inline void icp_iteration_body(const IcpLevel& L, const IcpParams& P,
   if (ticket != (unsigned)nb - 1) return;
   __threadfence();
   __shared__ double tot[kIcpVals];
-  final_reduce(partials, nb, tot);
+  final_reduce(partials, nb, tot, red);
   if (threadIdx.x == 0) {
     st->ticket = 0;
     st->iters[pl] = it;
@@ -409,6 +420,18 @@ __global__ void __launch_bounds__(kIcpThreads)
     icp_iteration_kernel(IcpLevel L, IcpParams P, int pl, int it, IcpState* st,
                          double* __restrict__ partials) {
   icp_iteration_body<KAHAN>(L, P, pl, it, st, partials, blockIdx.x, gridDim.x);
+}
+
+// Programmatic dependent launch: an iteration kernel launched with the
+// programmatic-serialization attribute may start while its predecessor
+// still runs.  It reads only data that no kernel of the ICP chain writes
+// (the session table, the level maps) before griddepcontrol.wait, which
+// returns once the predecessor grid has completed and its writes are
+// visible; it then lets its own successor launch.  Without the attribute
+// both instructions are no-ops.
+__device__ inline void wait_predecessor() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ inline void release_successor() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
 // Every session of the frame in one launch (blockIdx.z); a session uses
@@ -431,6 +454,8 @@ __global__ void __launch_bounds__(kIcpThreads, 2)
   L.s = S.ls[l];
   const int nb = icp_grid(L.s.rows * L.s.cols);
   if ((int)blockIdx.x >= nb) return;
+  wait_predecessor();  // the solver state and partials of the previous iteration
+  release_successor();
   icp_iteration_body<KAHAN>(L, S.icpp, pl, it, S.icp, S.partials, blockIdx.x, nb);
 }
 
@@ -462,7 +487,7 @@ __global__ void __launch_bounds__(kIcpThreads)
   if (ticket != gridDim.x - 1) return;
   __threadfence();
   __shared__ double tot[kIcpVals];
-  final_reduce(partials, gridDim.x, tot);
+  final_reduce(partials, gridDim.x, tot, red);
   if (threadIdx.x < kIcpVals) out[threadIdx.x] = tot[threadIdx.x];
   if (threadIdx.x == 0) *ticket_ctr = 0;
 }
@@ -635,12 +660,31 @@ void launch_icp_reduce_grid(const IcpLevel& L, const IcpParams& P, const float* 
   icp_reduce_kernel<<<grid, kIcpThreads, 0, stream>>>(L, P, T_dev, partials, ticket, out_dev);
 }
 
-void fused_icp_iteration(const SessDev* tab, const BatchShape& b, int slot, int it,
+// 'chained': launched with programmatic stream serialization, so that the
+// kernel's launch and prologue overlap its predecessor (an earlier ICP
+// iteration kernel, never the first of the frame, whose predecessor writes
+// the level maps).
+void fused_icp_iteration(const SessDev* tab, const BatchShape& b, int slot, int it, bool chained,
                          cudaStream_t st) {
   if (it >= b.max_slot_iters[slot]) return;
-  const dim3 grid(icp_grid(b.max_slot_px[slot]), 1, b.n);
-  if (b.kahan_mask & 1) fused_icp_iteration_kernel<false><<<grid, kIcpThreads, 0, st>>>(tab, slot, it);
-  if (b.kahan_mask & 2) fused_icp_iteration_kernel<true><<<grid, kIcpThreads, 0, st>>>(tab, slot, it);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(icp_grid(b.max_slot_px[slot]), 1, b.n);
+  cfg.blockDim = dim3(kIcpThreads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  if (b.kahan_mask & 1) {
+    cfg.numAttrs = chained ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, fused_icp_iteration_kernel<false>, tab, slot, it);
+    chained = true;
+  }
+  if (b.kahan_mask & 2) {
+    cfg.numAttrs = chained ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, fused_icp_iteration_kernel<true>, tab, slot, it);
+  }
 }
 
 void fused_pose_finalize(const SessDev* tab, const BatchShape& b, int bump, cudaStream_t st) {

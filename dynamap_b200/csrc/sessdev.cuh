@@ -88,7 +88,7 @@ void fused_bilateral(const SessDev* tab, const BatchShape& b, cudaStream_t st);
 void fused_pyramid(const SessDev* tab, const BatchShape& b, int target, cudaStream_t st);
 void fused_target_prepare(const SessDev* tab, const BatchShape& b, cudaStream_t st);
 // icp.cu
-void fused_icp_iteration(const SessDev* tab, const BatchShape& b, int slot, int it,
+void fused_icp_iteration(const SessDev* tab, const BatchShape& b, int slot, int it, bool chained,
                          cudaStream_t st);
 void fused_pose_finalize(const SessDev* tab, const BatchShape& b, int bump, cudaStream_t st);
 // tsdf.cu

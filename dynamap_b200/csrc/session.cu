@@ -131,10 +131,15 @@ void enqueue_source(const SessDev* tab, const BatchShape& b, cudaStream_t st, co
 }
 
 // gnSolver::solve's level loop (gnSolver.cu:340-431): iterations 1 .. N-1
-// of each level slot.
+// of each level slot; every launch after the first overlaps its
+// predecessor's tail (programmatic dependent launch).
 void enqueue_icp(const SessDev* tab, const BatchShape& b, cudaStream_t st) {
+  bool chained = false;
   for (int pl = 0; pl < 3; ++pl)
-    for (int it = 1; it < b.max_slot_iters[pl]; ++it) fused_icp_iteration(tab, b, pl, it, st);
+    for (int it = 1; it < b.max_slot_iters[pl]; ++it) {
+      fused_icp_iteration(tab, b, pl, it, chained, st);
+      chained = true;
+    }
 }
 
 // Integration at the session pose, then the next frame's target.
