@@ -52,8 +52,11 @@ constexpr int BTX = 32, BTY = 8;
 // values).  The range weight uses dyn_expf, the same operation sequence the
 // oracle runs, so the filtered depth is bit-identical to the oracle's.  Taps
 // outside the image or with depth <= 0 are skipped; invalid centres stay 0.
-// FAST (mixed-precision sessions): the range weight from the hardware
-// exponential (__expf) instead of dyn_expf.
+// FAST (mixed-precision sessions): each tap's weight in one hardware
+// base-2 exponential, gs * exp(-dn^2 / (2 s^2)) = 2^(log2 gs - dn^2 c) with
+// c = log2(e) / (2 s^2), the spatial weights staged as their logarithms;
+// the range normalisation 1/(2 pi s^2), common to every weight, cancels in
+// acc / wp and is left out.
 template <bool FAST>
 __device__ inline void bilateral_tile(const float* __restrict__ src, float* __restrict__ dst,
                                       int rows, int cols, const BilateralTable& tb, int bx,
@@ -68,7 +71,7 @@ __device__ inline void bilateral_tile(const float* __restrict__ src, float* __re
     int gr = row0 + tr, gc = col0 + tc;
     tile[k] = (gr >= 0 && gr < rows && gc >= 0 && gc < cols) ? src[gr * cols + gc] : 0.0f;
   }
-  for (int k = tid; k < D * D; k += BTX * BTY) gs[k] = tb.gs[k];
+  for (int k = tid; k < D * D; k += BTX * BTY) gs[k] = FAST ? __log2f(tb.gs[k]) : tb.gs[k];
   __syncthreads();
   const int x = by * BTY + threadIdx.y;  // row (the reference's x)
   const int y = bx * BTX + threadIdx.x;  // column
@@ -79,6 +82,7 @@ __device__ inline void bilateral_tile(const float* __restrict__ src, float* __re
     return;
   }
   const float inv2s2 = tb.inv2s2, norm = tb.norm;
+  const float c2 = inv2s2 * 1.4426950408889634f;  // FAST: log2(e) / (2 s^2)
   float acc = 0.0f, wp = 0.0f;
   // the taps inside the image: row x - half + i in [0, rows), column
   // y - half + j in [0, cols); summed in the reference's order
@@ -91,10 +95,16 @@ __device__ inline void bilateral_tile(const float* __restrict__ src, float* __re
       float nv = trow[j];
       if (!(nv > 0.0f)) continue;
       const float dn = nv - c;
-      float gi = FAST ? __expf(-(dn * dn) * inv2s2) * norm : range_weight(dn, inv2s2, norm);
-      float w = gi * grow[j];
-      acc += nv * w;
-      wp += w;
+      if (FAST) {
+        float w;
+        asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(w) : "f"(__fmaf_rn(-(dn * dn), c2, grow[j])));
+        acc = __fmaf_rn(nv, w, acc);
+        wp += w;
+      } else {
+        float w = range_weight(dn, inv2s2, norm) * grow[j];
+        acc += nv * w;
+        wp += w;
+      }
     }
   }
   dst[x * cols + y] = acc / wp;
