@@ -15,6 +15,15 @@
 
 namespace dyn {
 
+// Ray depth bounds of the frame raycast: 8x8-pixel fine tiles, and coarse
+// tiles of kRbCoarse x kRbCoarse fine ones; near and far bound per tile.
+constexpr int kRbTile = 8;
+constexpr int kRbCoarse = 8;
+inline __host__ __device__ int ray_bounds_words(int tiles_x, int tiles_y) {
+  const int cx = (tiles_x + kRbCoarse - 1) / kRbCoarse, cy = (tiles_y + kRbCoarse - 1) / kRbCoarse;
+  return 2 * tiles_x * tiles_y + 2 * cx * cy;
+}
+
 struct SessDev {
   DSensor ls[kLevels];  // level sensors (scale 1, 2, 4, 8)
   int nlev;             // levels in use
@@ -42,8 +51,8 @@ struct SessDev {
   float* tint[kLevels];
   float* ray;
   uint8_t* trgb;
-  unsigned* rbound;     // band sessions: ray-start bound per 8x8 tile (float
-  int rb_tx, rb_ty;     // bits), rb_tx x rb_ty tiles; null otherwise
+  unsigned* rbound;     // ray depth bounds (float bits), ray_bounds_words(rb_tx,
+  int rb_tx, rb_ty;     // rb_ty) words; rb_tx x rb_ty fine tiles
   const BilateralTable* btab;  // device copy
   // solver
   IcpState* icp;

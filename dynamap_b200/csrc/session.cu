@@ -574,11 +574,9 @@ dyn_status alloc_device_buffers(dyn_session* s) {
   }
   DYN_TRY(s->dalloc(&s->vol.cnt, sizeof(Counters)));
   DYN_TRY(s->dalloc(&s->d_gvis, sizeof(int2) * (size_t)tsdf->num_blocks));
-  if (precision == DYN_PRECISION_MIXED_BAND) {
-    s->rb_tx = ((int)s->sensor.cols + 7) / 8;
-    s->rb_ty = ((int)s->sensor.rows + 7) / 8;
-    DYN_TRY(s->dalloc(&s->d_rbound, sizeof(unsigned) * (size_t)s->rb_tx * s->rb_ty));
-  }
+  s->rb_tx = ((int)s->sensor.cols + 7) / 8;
+  s->rb_ty = ((int)s->sensor.rows + 7) / 8;
+  DYN_TRY(s->dalloc(&s->d_rbound, sizeof(unsigned) * (size_t)ray_bounds_words(s->rb_tx, s->rb_ty)));
   DYN_TRY(s->dalloc(&s->d_gcount, sizeof(int)));
   DYN_TRY(s->dalloc(&s->d_rgb_flag, sizeof(int)));
   DYN_TRY(s->dalloc(&s->d_res, sizeof(ResultBlock)));

@@ -256,19 +256,40 @@ __device__ inline bool block_visible(unsigned long long key, const DTsdf& t, con
   return ix >= 0 && iy >= 0 && ix < s.cols && iy < s.rows;
 }
 
-// ------------------------------------------------------------ ray-start bound
-// Band sessions allocate blocks only near surfaces.  A ray sample whose
-// voxel lies in no allocated block reads weight 0 and steps one truncation
-// distance (tsdf.cu:505-507), so for every 8x8 pixel tile the frame's
-// raycast gets a lower bound on the camera depth at which any of its rays
-// can first enter an allocated block: below it (and beyond the near
-// distance, where rays are marched normally) a sample needs no lookup, the
-// march adds the truncation distance just as the lookup would have made it.
-// Each allocated block contributes its box widened by one voxel beyond the
-// rounding cells of its outer voxels, clipped to camera depth >= the near
-// distance, projected and widened by one pixel: the tiles its bounding
-// rectangle touches get min(bound, nearest depth of the box).
-constexpr int kRbTile = 8;
+// ------------------------------------------------------------ ray depth bounds
+// A ray sample whose voxel lies in no allocated block reads weight 0 and
+// steps one truncation distance (tsdf.cu:505-507), so for every 8x8 pixel
+// tile the frame's raycast gets a lower bound on the camera depth at which
+// any of its rays can first enter an allocated block and an upper bound on
+// the depth at which the last one leaves one: below the first and above the
+// second (and beyond the near distance, where rays are marched normally) a
+// sample needs no lookup, the march adds the truncation distance just as
+// the lookup would have made it -- the same steps, so the same depths.
+// Band sessions (blocks only near surfaces) skip most of every ray; the
+// reference's carving allocation fills the space in front of surfaces, so
+// there the far bound is what skips (rays past the scene).  Each allocated
+// block contributes its box widened by one voxel beyond the rounding cells
+// of its outer voxels, clipped to camera depth >= the near distance,
+// projected and widened by one pixel: the tiles its bounding rectangle
+// touches get min(near, nearest depth of the box) and max(far, farthest
+// depth of the box).
+// The bounds buffer of a session with tiles_x x tiles_y fine tiles
+// (ray_bounds_words): near and far per fine tile, then near and far per
+// coarse tile; a pixel's bounds are min(near) / max(far) over both levels.
+struct RayBounds {
+  unsigned *near8, *far8, *near64, *far64;
+  int cx, cy;
+};
+__device__ inline RayBounds ray_bounds(unsigned* rb, int tiles_x, int tiles_y) {
+  RayBounds B;
+  B.cx = (tiles_x + kRbCoarse - 1) / kRbCoarse;
+  B.cy = (tiles_y + kRbCoarse - 1) / kRbCoarse;
+  B.near8 = rb;
+  B.far8 = rb + tiles_x * tiles_y;
+  B.near64 = B.far8 + tiles_x * tiles_y;
+  B.far64 = B.near64 + B.cx * B.cy;
+  return B;
+}
 
 __device__ inline float ray_near(const DTsdf& t) { return t.bsm; }
 
@@ -325,9 +346,30 @@ __device__ inline void bound_block(unsigned long long key, const DTsdf& t, const
   const int ty0 = vmin <= 0.0f ? 0 : min((int)vmin / kRbTile, tiles_y - 1);
   const int tx1 = umax >= (float)(s.cols - 1) ? tiles_x - 1 : (int)umax / kRbTile;
   const int ty1 = vmax >= (float)(s.rows - 1) ? tiles_y - 1 : (int)vmax / kRbTile;
-  const unsigned zb = __float_as_uint(fmaxf(zmin, 0.0f));
-  for (int ty = ty0; ty <= ty1; ++ty)
-    for (int tx = tx0; tx <= tx1; ++tx) atomicMin(rb + ty * tiles_x + tx, zb);
+  // Non-negative floats order as their bit patterns.  A block whose
+  // rectangle spans more than 16 tiles (one close to the camera) goes to
+  // the coarse level instead, so that no thread walks hundreds of tiles;
+  // the coarse bounds of such blocks are loose only near the camera.
+  // Carving sessions keep the near bound at 0: their blocks start at the
+  // camera.
+  const unsigned zb = __float_as_uint(fmaxf(zmin, 0.0f)), ze = __float_as_uint(zmax);
+  RayBounds B = ray_bounds(rb, tiles_x, tiles_y);
+  unsigned *nb = B.near8, *fb = B.far8;
+  int tw = tiles_x, x0 = tx0, x1 = tx1, y0 = ty0, y1 = ty1;
+  if ((tx1 - tx0 + 1) * (ty1 - ty0 + 1) > 16) {
+    nb = B.near64;
+    fb = B.far64;
+    tw = B.cx;
+    x0 = tx0 / kRbCoarse;
+    x1 = tx1 / kRbCoarse;
+    y0 = ty0 / kRbCoarse;
+    y1 = ty1 / kRbCoarse;
+  }
+  for (int ty = y0; ty <= y1; ++ty)
+    for (int tx = x0; tx <= x1; ++tx) {
+      if (t.band) atomicMin(nb + ty * tw + tx, zb);
+      atomicMax(fb + ty * tw + tx, ze);
+    }
 }
 
 // Every session's visible blocks appended to one batch-wide list of
@@ -676,7 +718,8 @@ constexpr int kRayTX = 16, kRayTY = 16;
 // interpolated colour at the hit.  Returns true when the march hit the step
 // cap.
 __device__ inline bool raycast_exact_px(const VolumeDev& v, const DSensor& s, const M4f& T, int x,
-                                        int y, float* __restrict__ depth_out,
+                                        int y, float skip_to, float skip_far,
+                                        float* __restrict__ depth_out,
                                         uint8_t* __restrict__ rgb_out) {
   const int i = y * s.cols + x;
   const DTsdf& t = v.t;
@@ -689,10 +732,15 @@ __device__ inline bool raycast_exact_px(const VolumeDev& v, const DSensor& s, co
   float cur = 0.0f;
   int steps = 0;
   bool over = false;
+  const float znear = ray_near(t);
   while (cur < t.dmax) {
     if (steps++ >= t.rc_cap) {
       over = true;
       break;
+    }
+    if (cur >= znear && (cur < skip_to || cur > skip_far)) {  // no allocated block here
+      cur += t.trunc;
+      continue;
     }
     F3 pc = f3(ax * cur / s.fx, ay * cur / s.fy, cur);
     F3 point = xform(T, pc);
@@ -797,7 +845,8 @@ __device__ inline VoxelSample interp16(const VolumeDev& v, F3 q, unsigned raw0, 
 // unit depth (both divided by vs), by fused multiply-adds; its voxel is
 // floor(q + 0.5).
 __device__ inline bool raycast_mixed_px(const VolumeDev& v, const DSensor& s, const M4f& T, int x,
-                                        int y, float skip_to, float* __restrict__ depth_out,
+                                        int y, float skip_to, float skip_far,
+                                        float* __restrict__ depth_out,
                                         uint8_t* __restrict__ rgb_out) {
   const int i = y * s.cols + x;
   const DTsdf& t = v.t;
@@ -819,7 +868,7 @@ __device__ inline bool raycast_mixed_px(const VolumeDev& v, const DSensor& s, co
       over = true;
       break;
     }
-    if (cur >= znear && cur < skip_to) {  // no allocated block here: weight 0
+    if (cur >= znear && (cur < skip_to || cur > skip_far)) {  // no allocated block: weight 0
       cur += t.trunc;
       continue;
     }
@@ -888,10 +937,17 @@ __device__ inline void raycast_tile(const VolumeDev& v, const DSensor& s,
   const int ly = (warp / (TX / 8)) * 4 + (lane >> 3);
   const int x = bx * TX + lx, y = by * TY + ly;
   if (x < s.cols && y < s.rows) {
-    const float skip_to =
-        rbound ? __uint_as_float(rbound[(y / kRbTile) * tiles_x + x / kRbTile]) : 0.0f;
-    const bool o = MIXED ? raycast_mixed_px(v, s, T, x, y, skip_to, depth_out, rgb_out)
-                         : raycast_exact_px(v, s, T, x, y, depth_out, rgb_out);
+    float skip_to = 0.0f, skip_far = 3.402823466e+38f;
+    if (rbound) {
+      const int tx = x / kRbTile, ty = y / kRbTile;
+      const RayBounds B =
+          ray_bounds(const_cast<unsigned*>(rbound), tiles_x, (s.rows + kRbTile - 1) / kRbTile);
+      const int f = ty * tiles_x + tx, c = (ty / kRbCoarse) * B.cx + tx / kRbCoarse;
+      skip_to = fminf(__uint_as_float(B.near8[f]), __uint_as_float(B.near64[c]));
+      skip_far = fmaxf(__uint_as_float(B.far8[f]), __uint_as_float(B.far64[c]));
+    }
+    const bool o = MIXED ? raycast_mixed_px(v, s, T, x, y, skip_to, skip_far, depth_out, rgb_out)
+                         : raycast_exact_px(v, s, T, x, y, skip_to, skip_far, depth_out, rgb_out);
     if (o) atomicAdd(&over, 1);
   }
   __syncthreads();
@@ -921,7 +977,7 @@ __global__ void __launch_bounds__(TX* TY, 1024 / (TX * TY))
   if ((int)blockIdx.x * TX >= s.cols || (int)blockIdx.y * TY >= s.rows) return;
   uint8_t* rgb_out = S.use_color ? S.trgb : nullptr;
   raycast_tile<MIXED, TX, TY>(S.vol, s, S.pose->posef, S.ray, rgb_out, blockIdx.x, blockIdx.y,
-                              MIXED ? S.rbound : nullptr, S.rb_tx);
+                              S.rbound, S.rb_tx);
 }
 
 template <int TX, int TY>
@@ -933,12 +989,24 @@ void launch_fused_raycast(const SessDev* tab, const BatchShape& b, cudaStream_t 
 
 // per-frame counters of every session (all but nalloc, the heap top) and
 // the batch visible list
-// (and, for band sessions, the ray-start bound to "no block": 3.4e38)
+// (and the ray depth bounds to "no block")
 __global__ void fused_reset_counters_kernel(const SessDev* __restrict__ tab,
                                             int* __restrict__ gcount) {
   const SessDev& S = tab[blockIdx.z];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (S.rbound && i < S.rb_tx * S.rb_ty) S.rbound[i] = 0x7f7f7f7fu;
+  if (S.rbound) {
+    // near: no block (3.4e38), or 0 where unused; far: no block (0)
+    const unsigned nb = S.vol.t.band ? 0x7f7f7f7fu : 0u;
+    const RayBounds B = ray_bounds(S.rbound, S.rb_tx, S.rb_ty);
+    if (i < S.rb_tx * S.rb_ty) {
+      B.near8[i] = nb;
+      B.far8[i] = 0u;
+    }
+    if (i < B.cx * B.cy) {
+      B.near64[i] = nb;
+      B.far64[i] = 0u;
+    }
+  }
   if (i != 0) return;
   if (blockIdx.z == 0) *gcount = 0;
   Counters* c = S.vol.cnt;

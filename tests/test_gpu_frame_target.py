@@ -1,7 +1,7 @@
 """The frame's raycast (the fused per-frame launch) must equal the stage
 entry point dyn_raycast at the same pose bit for bit, in depth and colour,
-FP32, mixed and mixed with band allocation (whose frame raycast skips the
-lookups below its per-tile ray-start bound, which dyn_raycast does not use),
+FP32, mixed and mixed with band allocation (the frame raycast skips the
+lookups outside its per-tile depth bounds, which dyn_raycast does not use),
 after several frames, for a camera looking into a box (cube) and inside a
 room (blocks beside and behind the camera)."""
 import numpy as np
