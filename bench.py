@@ -800,7 +800,7 @@ def run_large(args):
         "data": "synthetic: seeded room scene (8 x 8 x 3 m, walls, 40 primitives) and "
                 "cube scenes, Perlin albedo RGB",
         "config": {"workload": "cfg5: one 1280x720 RGB-D session (room, 4 mm voxels, 2^23 "
-                               "buckets x 10, 2^20 blocks, 8 m range) batched with eight "
+                               "buckets x 10, 2^21 blocks, 8 m range) batched with eight "
                                f"640x480 RGB-D sessions (cfg2), {args.precision}, one frame "
                                "of every session per step",
                    "precision": args.precision, "sessions_per_gpu": n,
