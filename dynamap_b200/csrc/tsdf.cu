@@ -228,7 +228,9 @@ __device__ inline void allocate_tile(const float* __restrict__ depth, const DSen
   }
 }
 
-__global__ void __launch_bounds__(kAllocT* kAllocT)
+// (8 CTAs per SM -- at most 32 registers, 24.7 KB of shared memory each --
+// so that a 640x480 frame's 1,200 tiles run in one wave instead of 1.35)
+__global__ void __launch_bounds__(kAllocT* kAllocT, 8)
     fused_allocate_kernel(const SessDev* __restrict__ tab) {
   const SessDev& S = tab[blockIdx.z];
   const DSensor& s = S.ls[0];
