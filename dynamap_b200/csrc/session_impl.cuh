@@ -224,7 +224,7 @@ struct dyn_session {
 // A table of sessions split into groups, each group's fused stage chain on
 // its own stream (group 0 on the caller's stream): groups overlap the
 // tails of each other's launches.
-constexpr int kMaxGroups = 4;
+constexpr int kMaxGroups = 8;
 struct FrameGroups {
   int k = 1;
   const SessDev* tab[kMaxGroups] = {};  // group sub-tables (device)
