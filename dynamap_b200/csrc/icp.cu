@@ -135,6 +135,7 @@ __device__ inline void block_reduce(const Acc& a, bool kahan, double* red /*[8][
 __device__ inline void final_reduce(const double* __restrict__ partials, int nblocks,
                                     double* out, double* scratch) {
   constexpr int kGroups = kIcpThreads / 32;  // 8: scratch is the block-reduce array
+  static_assert(kGroups * kIcpVals <= kIcpThreads, "one thread per (group, value)");
   const int t = threadIdx.x;
   if (t < kGroups * kIcpVals) {
     const int g = t / kIcpVals, k = t - g * kIcpVals;
