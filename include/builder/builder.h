@@ -10,9 +10,11 @@
 #pragma once
 
 #include <cstdint>
+#include <fstream>
 #include <vector>
 
 #include "../dynamap.h"
+#include "../dynamap/pose_io.h"
 #include "../dynamap/types.h"
 #include "../geometry/tsdf/tsdf.h"
 #include "../solver/gnSolver/gnSolver.h"
@@ -95,6 +97,26 @@ class builder {
   }
 
   dyn_session* session() const { return session_; }
+
+  // builder.cu:222-241: a TUM ground-truth line {stamp, tx, ty, tz, qx, qy,
+  // qz, qw} as a pose (quaternion normalised, rotation rounded to float)
+  static Matrix4f v2tRef(std::vector<double>& vec) {
+    if (vec.size() < 8) dyn_throw("builder::v2tRef", DYN_ERR_INVALID_ARG);
+    float p[16];
+    pose_io::pose_from_tum(vec.data(), p);
+    return Matrix4f::from_row_major(p);
+  }
+
+  // builder.cu:243-257: append "stamp tx ty tz qx qy qz qw" (fixed, four
+  // decimals; vec[0] is the stamp) for Pose to fileName.  'count' is unused,
+  // as in the reference.
+  static void writePoseToTxt(const char* fileName, std::vector<double>& vec, const Matrix4f& Pose,
+                             int count) {
+    (void)count;
+    if (vec.empty()) dyn_throw("builder::writePoseToTxt", DYN_ERR_INVALID_ARG);
+    std::ofstream file(fileName, std::ios::ate | std::ios::app);
+    if (file.is_open()) file << pose_io::tum_line(vec[0], Pose.to_row_major().entries) << "\n";
+  }
 
  private:
   void ensure(int mode) {
