@@ -755,18 +755,68 @@ inline bool normal_ok(const R* n4, int i) {
   return !(x == 0 && y == 0 && z == 0);
 }
 
-// buildNLSKernel, gnSolver.cu:26-196 (per pixel in R, sums in double) with
-// F8.  out[0..20] upper-triangular A, out[21..26] acc_b (= -sum b),
-// out[27] sum r^2, out[28] count.
+// buildNLSKernel's terms for one source pixel, gnSolver.cu:55-190 (in R)
+// with F8: A (6x6, full), b and the residual r; false when the pixel has no
+// correspondence.
+template <class R>
+bool icp_pixel_terms(const R* sd, const R* sn, const R* si, const R* td, const R* tn,
+                     const R* ti, const Sensor<R>& s, const dyn_gn_params& g, const M4<R>& T,
+                     int idx, R A[36], R b[6], R* res) {
+  R dmin = (R)g.icp_min_depth, dmax = (R)g.icp_max_depth;
+  R thr = (R)g.normal_cos_thresh;
+  R cw = (R)g.color_weight;
+  R d = sd[idx];
+  if (d < dmin || d > dmax || !normal_ok(sn, idx)) return false;
+  V3<R> s_n = v3(sn[4 * (size_t)idx], sn[4 * (size_t)idx + 1], sn[4 * (size_t)idx + 2]);
+  V3<R> p = xform(T, getPoint3d(idx, d, s));
+  if (!(p.z > 0)) return false;
+  int px, py;
+  if (!project(p, s, &px, &py)) return false;
+  if (px < 0 || py < 0 || px >= s.cols || py >= s.rows) return false;
+  int index = py * s.cols + px;
+  R tdd = td[index];
+  if (tdd < dmin || tdd > dmax || !normal_ok(tn, index)) return false;
+  V3<R> nn = v3(tn[4 * (size_t)index], tn[4 * (size_t)index + 1], tn[4 * (size_t)index + 2]);
+  R cosT = dot(nn, s_n);
+  V3<R> q = getPoint3d(index, tdd, s);
+  if (!(std::fabs(cosT) > thr)) return false;
+  V3<R> c = cross(p, nn);
+  R cn[6] = {c.x, c.y, c.z, nn.x, nn.y, nn.z};
+  V3<R> pq = p - q;
+  for (int i = 0; i < 6; ++i)
+    for (int j = 0; j < 6; ++j) A[i * 6 + j] = cn[i] * cn[j];
+  for (int k = 0; k < 6; ++k)
+    b[k] = pq.x * (cn[k] * nn.x) + pq.y * (cn[k] * nn.y) + pq.z * (cn[k] * nn.z);
+  if (cw != 0) {
+    // gnSolver.cu:137-190: J_c = grad(I_t) [ -p^ | I ]
+    int il = px >= 1 ? index - 1 : index;
+    int iu = py >= 1 ? index - s.cols : index;
+    R gx = (ti[index] - ti[il]) / 2;
+    R gy = (ti[index] - ti[iu]) / 2;
+    R D[3][6] = {{0, p.z, -p.y, 1, 0, 0},
+                 {-p.z, 0, p.x, 0, 1, 0},
+                 {p.y, -p.x, 0, 0, 0, 1}};
+    R Jc[6];
+    for (int j = 0; j < 6; ++j) Jc[j] = gx * D[0][j] + gy * D[1][j] + R(0) * D[2][j];
+    R ediff = ti[index] - si[idx];
+    for (int i = 0; i < 6; ++i)
+      for (int j = 0; j < 6; ++j)
+        A[i * 6 + j] = (R(1) - cw) * A[i * 6 + j] + (cw * Jc[i]) * Jc[j];
+    for (int k = 0; k < 6; ++k) b[k] = (R(1) - cw) * b[k] + (cw * Jc[k]) * ediff;
+  }
+  *res = dot(pq, nn);
+  return true;
+}
+
+// The normal equations of a level, sums in double: out[0..20] the upper
+// triangle of A, out[21..26] acc_b (= -sum b), out[27] sum r^2, out[28]
+// count.
 template <class R>
 void icp_normal_equations(const R* sd, const R* sn, const R* si, const R* td,
                           const R* tn, const R* ti, const Sensor<R>& s,
                           const dyn_gn_params& g, const M4<R>& T,
                           double out[29]) {
   int n = s.rows * s.cols;
-  R dmin = (R)g.icp_min_depth, dmax = (R)g.icp_max_depth;
-  R thr = (R)g.normal_cos_thresh;
-  R cw = (R)g.color_weight;
   int nt = std::max(1, g_threads);
   std::vector<double> part((size_t)nt * 29, 0.0);
 #pragma omp parallel for num_threads(nt) schedule(static)
@@ -774,51 +824,12 @@ void icp_normal_equations(const R* sd, const R* sn, const R* si, const R* td,
     double* acc = &part[(size_t)t * 29];
     int lo = (int)((int64_t)n * t / nt), hi = (int)((int64_t)n * (t + 1) / nt);
     for (int idx = lo; idx < hi; ++idx) {
-      R d = sd[idx];
-      if (d < dmin || d > dmax || !normal_ok(sn, idx)) continue;
-      V3<R> s_n = v3(sn[4 * (size_t)idx], sn[4 * (size_t)idx + 1], sn[4 * (size_t)idx + 2]);
-      V3<R> p = xform(T, getPoint3d(idx, d, s));
-      if (!(p.z > 0)) continue;
-      int px, py;
-      if (!project(p, s, &px, &py)) continue;
-      if (px < 0 || py < 0 || px >= s.cols || py >= s.rows) continue;
-      int index = py * s.cols + px;
-      R tdd = td[index];
-      if (tdd < dmin || tdd > dmax || !normal_ok(tn, index)) continue;
-      V3<R> nn = v3(tn[4 * (size_t)index], tn[4 * (size_t)index + 1], tn[4 * (size_t)index + 2]);
-      R cosT = dot(nn, s_n);
-      V3<R> q = getPoint3d(index, tdd, s);
-      if (!(std::fabs(cosT) > thr)) continue;
-      V3<R> c = cross(p, nn);
-      R cn[6] = {c.x, c.y, c.z, nn.x, nn.y, nn.z};
-      V3<R> pq = p - q;
-      R A[36], b[6];
-      for (int i = 0; i < 6; ++i)
-        for (int j = 0; j < 6; ++j) A[i * 6 + j] = cn[i] * cn[j];
-      for (int k = 0; k < 6; ++k)
-        b[k] = pq.x * (cn[k] * nn.x) + pq.y * (cn[k] * nn.y) + pq.z * (cn[k] * nn.z);
-      if (cw != 0) {
-        // gnSolver.cu:137-190: J_c = grad(I_t) [ -p^ | I ]
-        int il = px >= 1 ? index - 1 : index;
-        int iu = py >= 1 ? index - s.cols : index;
-        R gx = (ti[index] - ti[il]) / 2;
-        R gy = (ti[index] - ti[iu]) / 2;
-        R D[3][6] = {{0, p.z, -p.y, 1, 0, 0},
-                     {-p.z, 0, p.x, 0, 1, 0},
-                     {p.y, -p.x, 0, 0, 0, 1}};
-        R Jc[6];
-        for (int j = 0; j < 6; ++j) Jc[j] = gx * D[0][j] + gy * D[1][j] + R(0) * D[2][j];
-        R ediff = ti[index] - si[idx];
-        for (int i = 0; i < 6; ++i)
-          for (int j = 0; j < 6; ++j)
-            A[i * 6 + j] = (R(1) - cw) * A[i * 6 + j] + (cw * Jc[i]) * Jc[j];
-        for (int k = 0; k < 6; ++k) b[k] = (R(1) - cw) * b[k] + (cw * Jc[k]) * ediff;
-      }
+      R A[36], b[6], r;
+      if (!icp_pixel_terms(sd, sn, si, td, tn, ti, s, g, T, idx, A, b, &r)) continue;
       int u = 0;
       for (int i = 0; i < 6; ++i)
         for (int j = i; j < 6; ++j) acc[u++] += (double)A[i * 6 + j];
       for (int k = 0; k < 6; ++k) acc[21 + k] -= (double)b[k];
-      R r = dot(pq, nn);
       acc[27] += (double)r * (double)r;
       acc[28] += 1.0;
     }
@@ -826,6 +837,27 @@ void icp_normal_equations(const R* sd, const R* sn, const R* si, const R* td,
   for (int k = 0; k < 29; ++k) out[k] = 0;
   for (int t = 0; t < nt; ++t)
     for (int k = 0; k < 29; ++k) out[k] += part[(size_t)t * 29 + k];
+}
+
+// The same terms summed as the reference's buildNLSKernel sums them when
+// its pixels run one after another: FP32 accumulators of the full 6x6 A and
+// of -b, in pixel order (gnSolver.cu:192-193).  Returns the pixel count.
+int64_t icp_normal_equations_refsum(const float* sd, const float* sn, const float* si,
+                                    const float* td, const float* tn, const float* ti,
+                                    const Sensor<float>& s, const dyn_gn_params& g,
+                                    const M4<float>& T, float A_out[36], float b_out[6]) {
+  for (int j = 0; j < 36; ++j) A_out[j] = 0.0f;
+  for (int j = 0; j < 6; ++j) b_out[j] = 0.0f;
+  int64_t cnt = 0;
+  const int n = s.rows * s.cols;
+  for (int idx = 0; idx < n; ++idx) {
+    float A[36], b[6], r;
+    if (!icp_pixel_terms(sd, sn, si, td, tn, ti, s, g, T, idx, A, b, &r)) continue;
+    for (int j = 0; j < 36; ++j) A_out[j] += A[j];
+    for (int j = 0; j < 6; ++j) b_out[j] += -b[j];
+    ++cnt;
+  }
+  return cnt;
 }
 
 // ------------------------------------------------------------- GN algebra
@@ -1239,6 +1271,13 @@ void dyo_icp_normal_equations(const float* sd, const float* sn, const float* si,
                               const float T[16], double out[29]) {
   icp_normal_equations<float>(sd, sn, si, td, tn, ti, mk_sensor<float>(*level),
                               *gn, m4_from<float>(T), out);
+}
+int64_t dyo_icp_normal_equations_refsum(const float* sd, const float* sn, const float* si,
+                                        const float* td, const float* tn, const float* ti,
+                                        const dyn_sensor* level, const dyn_gn_params* gn,
+                                        const float T[16], float A_out[36], float b_out[6]) {
+  return icp_normal_equations_refsum(sd, sn, si, td, tn, ti, mk_sensor<float>(*level), *gn,
+                                     m4_from<float>(T), A_out, b_out);
 }
 void dyo_inverse4(const float m[16], float out[16]) {
   M4<float> r = inverse4(m4_from<float>(m));

@@ -75,6 +75,14 @@ void dyo_icp_normal_equations(const float* src_depth, const float* src_n4,
                               const float* tgt_n4, const float* tgt_i,
                               const dyn_sensor* level, const dyn_gn_params* gn,
                               const float T[16], double out[29]);
+/* The same terms as the reference's buildNLSKernel accumulates them on one
+ * thread (gnSolver.cu:192-193): FP32 sums of the full 6x6 A and of -b in
+ * pixel order.  Returns the number of pixels with a correspondence. */
+int64_t dyo_icp_normal_equations_refsum(const float* src_depth, const float* src_n4,
+                                        const float* src_i, const float* tgt_depth,
+                                        const float* tgt_n4, const float* tgt_i,
+                                        const dyn_sensor* level, const dyn_gn_params* gn,
+                                        const float T[16], float A_out[36], float b_out[6]);
 /* float4x4::getInverse, utils_matrix.h:970-1086 */
 void dyo_inverse4(const float m[16], float out[16]);
 /* closed-form SE(3) exponential of xi = [w; t] (double), row-major */

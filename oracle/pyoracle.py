@@ -51,6 +51,8 @@ def lib() -> C.CDLL:
             "dyo_maps": (None, [_vp, P(abi.Sensor), _vp, _vp]),
             "dyo_icp_normal_equations": (None, [_vp] * 6 + [P(abi.Sensor), P(abi.GnParams),
                                                            P(C.c_float), P(C.c_double)]),
+            "dyo_icp_normal_equations_refsum": (C.c_int64, [_vp] * 6 + [
+                P(abi.Sensor), P(abi.GnParams), P(C.c_float), P(C.c_float), P(C.c_float)]),
             "dyo_inverse4": (None, [P(C.c_float), P(C.c_float)]),
             "dyo_se3_exp": (None, [P(C.c_double), P(C.c_double)]),
             "dyo_ldlt_solve6": (C.c_int, [P(C.c_double), P(C.c_double), P(C.c_double)]),
@@ -169,6 +171,19 @@ def icp_normal_equations(sd, sn, si, td, tn, ti, s, g, T) -> np.ndarray:
     lib().dyo_icp_normal_equations(*[ptr(a) for a in args], C.byref(s), C.byref(g),
                                    fptr(T), out.ctypes.data_as(P(C.c_double)))
     return out
+
+
+def icp_normal_equations_refsum(sd, sn, si, td, tn, ti, s, g, T):
+    """(A float32 [36], acc_b float32 [6], pixel count) summed as the
+    reference's buildNLSKernel sums them on one thread."""
+    A = np.zeros(36, np.float32)
+    b = np.zeros(6, np.float32)
+    T = np.ascontiguousarray(T, np.float32).reshape(16)
+    args = [np.ascontiguousarray(a, np.float32) if a is not None else None
+            for a in (sd, sn, si, td, tn, ti)]
+    n = lib().dyo_icp_normal_equations_refsum(*[ptr(a) for a in args], C.byref(s), C.byref(g),
+                                              fptr(T), fptr(A), fptr(b))
+    return A, b, int(n)
 
 
 def inverse4(m: np.ndarray) -> np.ndarray:

@@ -6,8 +6,9 @@
 # compiled unmodified except for the CUDA launch syntax, which a C++
 # compiler cannot parse: each `K<<<grid, block>>>(` becomes
 # `DYNREF_LAUNCH(K)(` (see shim/cuda_runtime.h).  The rewritten copies live
-# only under oracle/_ref/src and are never committed.  Eigen, OpenCV and the
-# CUDA runtime are replaced by the small headers in shim/.
+# only under oracle/_ref/src and are never committed.  Eigen, OpenCV, the
+# CUDA runtime and the CUDA math libraries gnSolver.h includes are replaced
+# by the small headers in shim/.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 REF="${REF:-/root/reference}"
@@ -20,7 +21,7 @@ fi
 mkdir -p "$OUT/src"
 SRCS=(geometry/tsdf/tsdf.cu dataStructure/hashTable/hashTable.cu dataStructure/heap/heap.cu
       image/sensor/rgbdImage.cu image/pyramid/pyramid.cu image/conv2D/conv2D.cu
-      image/kernel2D/kernel2D.cu)
+      image/kernel2D/kernel2D.cu solver/gnSolver/gnSolver.cu)
 OBJS=()
 INCS=(-I"$HERE/shim" -I"$INC" -I"$INC/dataStructure" -I"$INC/dataStructure/heap"
       -I"$INC/dataStructure/hashTable" -I"$INC/image" -I"$INC/image/sensor"

@@ -4,21 +4,34 @@
 // box without the reference tree, never built.
 //
 // The reference's sources (tsdf.cu, hashTable.cu, heap.cu, rgbdImage.cu,
-// pyramid.cu, conv2D.cu, kernel2D.cu) are compiled unmodified apart from the
-// launch syntax (build_ref.sh); this file only drives them:
+// pyramid.cu, conv2D.cu, kernel2D.cu, gnSolver.cu) are compiled unmodified
+// apart from the launch syntax (build_ref.sh); this file only drives them:
 //   tsdfVolume::init / IntegrateScan / GenerateDepth / GenerateRgb
 //   (include/geometry/tsdf/tsdf.cu:18-550), the vertex map and normals of
-//   rgbdImage (include/image/sensor/rgbdImage.cu:23-167), and
-//   pyramid::applyBilateralFilter (include/image/pyramid/pyramid.cu:213-233).
+//   rgbdImage (include/image/sensor/rgbdImage.cu:23-167),
+//   pyramid::applyBilateralFilter (include/image/pyramid/pyramid.cu:213-233)
+//   and the ICP normal equations of buildNLSKernel
+//   (include/solver/gnSolver/gnSolver.cu:26-196).
 #include <cstdint>
 #include <cstring>
 
 #include "../../include/dynamap.h"
+#include "gnSolver/gnSolver.h"
 #include "meshExtractor/meshExtractor.h"
 #include "pyramid/pyramid.h"
 #include "tsdf/tsdf.h"
 
 using namespace DynaMap;
+
+// defined in gnSolver.cu, not declared in its header
+namespace DynaMap {
+namespace solver {
+void buildNLSKernel(gnSolver& solver, uchar3* target_rgb, float* target_depth, uchar3* source_rgb,
+                    float* source_depth, rgbdSensor sensor, float4x4 last_transform,
+                    mat6x6* acc_A, mat6x1* acc_b, geometry::PointCloudXYZ& targetCloud,
+                    geometry::PointCloudXYZ& sourceCloud, float scale, float huberConstant);
+}  // namespace solver
+}  // namespace DynaMap
 
 // tsdf.cu's ExtractMesh names the mesh extractor; mesh extraction is not on
 // the path, so these definitions only satisfy the linker.
@@ -169,6 +182,51 @@ float ref_bilateral_pixel(const float* src, int rows, int cols, int x, int y, in
                           sigma_s, s);
   out = dst[(size_t)x * cols + y];
   return out;
+}
+
+// buildNLSKernel at pyramid scale 1 on one host thread, so its float
+// atomics sum the pixels' terms in index order: the 6x6 A (all 36 entries)
+// and b accumulated as the reference accumulates them (b with its minus
+// sign).  Normals are float3 per pixel; T is the row-major source-to-target
+// transform; the reference's depth window (0.15, 2.0 m) and colour weight
+// (0) are its own constants.  The caller keeps every valid source pixel's
+// projection, and its left and upper neighbours, inside the image (the
+// reference does not check them).
+void ref_icp_normal_equations(const float* src_depth, const float* src_n3, const float* tgt_depth,
+                              const float* tgt_n3, const uint8_t* src_rgb, const uint8_t* tgt_rgb,
+                              const dyn_sensor* s, const float T[16], float A_out[36],
+                              float b_out[6]) {
+  static solver::gnSolver* g = nullptr;  // never destroyed: its pyramids own no buffers
+  if (!g) g = new solver::gnSolver();
+  const size_t n = (size_t)s->rows * s->cols;
+  std::vector<float> sd(src_depth, src_depth + n), td(tgt_depth, tgt_depth + n);
+  std::vector<float3> sn(n), tn(n);
+  std::vector<uchar3> sc(n), tc(n);
+  for (size_t i = 0; i < n; ++i) {
+    sn[i] = make_float3(src_n3[3 * i], src_n3[3 * i + 1], src_n3[3 * i + 2]);
+    tn[i] = make_float3(tgt_n3[3 * i], tgt_n3[3 * i + 1], tgt_n3[3 * i + 2]);
+    sc[i] = src_rgb ? make_uchar3(src_rgb[3 * i], src_rgb[3 * i + 1], src_rgb[3 * i + 2])
+                    : make_uchar3(0, 0, 0);
+    tc[i] = tgt_rgb ? make_uchar3(tgt_rgb[3 * i], tgt_rgb[3 * i + 1], tgt_rgb[3 * i + 2])
+                    : make_uchar3(0, 0, 0);
+  }
+  geometry::PointCloudXYZ src_cloud, tgt_cloud;
+  src_cloud.points = nullptr;
+  src_cloud.normals = sn.data();
+  tgt_cloud.points = nullptr;
+  tgt_cloud.normals = tn.data();
+  mat6x6 A;
+  mat6x1 b;
+  A.setZero();
+  b.setZero();
+  const int saved = dynref::nthreads();
+  dynref::nthreads() = 1;
+  DYNREF_LAUNCH(solver::buildNLSKernel)(*g, tc.data(), td.data(), sc.data(), sd.data(),
+                                        to_sensor(s), float4x4(T), &A, &b, tgt_cloud, src_cloud,
+                                        1.0f, 0.0f);
+  dynref::nthreads() = saved;
+  for (int j = 0; j < 36; ++j) A_out[j] = A(j);
+  for (int j = 0; j < 6; ++j) b_out[j] = b(j);
 }
 
 }  // extern "C"

@@ -1,11 +1,112 @@
-// Type-only stand-in for the Eigen 3 matrix types named by the reference's
-// headers (see eigen3/Eigen/Core in this directory).
+// Stand-in for the Eigen 3 matrix types named by the reference's headers
+// (see eigen3/Eigen/Core in this directory), used ONLY to compile the
+// reference's sources for the CPU (test infrastructure).  Column-major
+// fixed-size storage as Eigen's, with the element access, comma
+// initialisation and the few element-wise operations that
+// include/solver/gnSolver/gnSolver.cu names.  Eigen's LDLT solve and
+// matrix exponential are NOT provided: they abort if called.  The drivers
+// in this directory only run the reference's kernels (for the solver,
+// buildNLSKernel), never gnSolver::solve.
 #pragma once
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+
 namespace Eigen {
+
 template <class S, int R, int C>
 struct Matrix {
   S v[R * C];
+
+  S& operator()(int r, int c) { return v[c * R + r]; }
+  const S& operator()(int r, int c) const { return v[c * R + r]; }
+  S& operator()(int i) { return v[i]; }
+  const S& operator()(int i) const { return v[i]; }
+  S* data() { return v; }
+  const S* data() const { return v; }
+
+  // m << a, b, c, ...: row by row
+  struct CommaInit {
+    Matrix* m;
+    int k;
+    template <class T>
+    CommaInit& operator,(T x) {
+      (*m)(k / C, k % C) = (S)x;
+      ++k;
+      return *this;
+    }
+  };
+  template <class T>
+  CommaInit operator<<(T x) {
+    (*this)(0, 0) = (S)x;
+    return CommaInit{this, 1};
+  }
+
+  S sum() const {
+    S s = 0;
+    for (int i = 0; i < R * C; ++i) s += v[i];
+    return s;
+  }
+  S norm() const {
+    S s = 0;
+    for (int i = 0; i < R * C; ++i) s += v[i] * v[i];
+    return std::sqrt(s);
+  }
+  S maxCoeff() const {
+    S s = v[0];
+    for (int i = 1; i < R * C; ++i) s = v[i] > s ? v[i] : s;
+    return s;
+  }
+  Matrix& operator*=(S x) {
+    for (int i = 0; i < R * C; ++i) v[i] *= x;
+    return *this;
+  }
+  Matrix operator+(const Matrix& o) const {
+    Matrix r;
+    for (int i = 0; i < R * C; ++i) r.v[i] = v[i] + o.v[i];
+    return r;
+  }
+  Matrix operator-(const Matrix& o) const {
+    Matrix r;
+    for (int i = 0; i < R * C; ++i) r.v[i] = v[i] - o.v[i];
+    return r;
+  }
+  friend Matrix operator*(S x, const Matrix& m) {
+    Matrix r;
+    for (int i = 0; i < R * C; ++i) r.v[i] = x * m.v[i];
+    return r;
+  }
+  template <int K>
+  Matrix<S, R, K> operator*(const Matrix<S, C, K>& o) const {
+    Matrix<S, R, K> r;
+    for (int i = 0; i < R; ++i)
+      for (int j = 0; j < K; ++j) {
+        S s = 0;
+        for (int k = 0; k < C; ++k) s += (*this)(i, k) * o(k, j);
+        r(i, j) = s;
+      }
+    return r;
+  }
+  template <class T>
+  Matrix<T, R, C> cast() const {
+    Matrix<T, R, C> r;
+    for (int i = 0; i < R * C; ++i) r.v[i] = (T)v[i];
+    return r;
+  }
+
+  struct LDLT {
+    Matrix<S, C, 1> solve(const Matrix<S, C, 1>&) const {
+      std::fprintf(stderr, "eigen shim: LDLT solve is not provided\n");
+      std::abort();
+    }
+  };
+  LDLT ldlt() const { return LDLT(); }
+  Matrix exp() const {
+    std::fprintf(stderr, "eigen shim: the matrix exponential is not provided\n");
+    std::abort();
+  }
 };
+
 typedef Matrix<float, 4, 4> Matrix4f;
 typedef Matrix<double, 4, 4> Matrix4d;
 typedef Matrix<float, 3, 3> Matrix3f;
@@ -13,4 +114,15 @@ typedef Matrix<double, 3, 3> Matrix3d;
 typedef Matrix<float, 3, 1> Vector3f;
 typedef Matrix<double, 3, 1> Vector3d;
 typedef Matrix<double, 6, 1> Vector6d;
+
+// gnSolver.cu adds a 6x6 identity written as MatrixXd::Identity(6, 6).
+struct MatrixXd {
+  static Matrix<double, 6, 6> Identity(int r, int c) {
+    if (r != 6 || c != 6) std::abort();
+    Matrix<double, 6, 6> m;
+    for (int i = 0; i < 36; ++i) m.v[i] = (i % 7 == 0) ? 1.0 : 0.0;
+    return m;
+  }
+};
+
 }  // namespace Eigen

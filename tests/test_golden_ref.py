@@ -1,6 +1,7 @@
 """The oracle reproduces the reference's own outputs (golden vectors made
-by tests/golden/make_golden.py from the reference sources compiled for the
-CPU): allocation, integration, raycast, vertex/normal maps and the hash
+by tests/golden/make_golden.py and make_icp_golden.py from the reference
+sources compiled for the CPU): allocation, integration, raycast,
+vertex/normal maps, the hash and the ICP normal equations of buildNLSKernel
 bit for bit; the bilateral filter within 2 ulp-scale relative error (the
 oracle's range weight uses a portable FP32 exp, the reference libm's FP64
 exp)."""
@@ -110,3 +111,40 @@ def test_reference_hash(gold, oracle):
     L = oracle.lib()
     for (x, y, z), h in zip(gold["hash_coords"], gold["hash_values"]):
         assert L.dyo_hash(int(x), int(y), int(z), tsdf.num_buckets, tsdf.bucket_size) == h
+
+
+def test_reference_icp_normal_equations(oracle):
+    """buildNLSKernel's 6x6 A and b (gnSolver.cu:26-196) for three
+    transforms: the oracle's per-pixel terms summed in the reference's order
+    (FP32, pixel order) are bit-identical; its FP64 sums agree to FP32
+    summation error."""
+    z = np.load(os.path.join(HERE, "golden", "ref_icp_normal_equations.npz"))
+    r, c, fx, fy, cx, cy, ds = z["sensor"]
+    s = abi.Sensor(rows=int(r), cols=int(c), fx=fx, fy=fy, cx=cx, cy=cy, depth_scaler=ds)
+    _, g, _, _ = abi.defaults()
+    # the reference's constants: depth window 0.15-2.0 m (pyramid.h:15-16),
+    # colour weight 0 (gnSolver.cu:180), |cos| > cos(pi/10) compared in
+    # double -- for a float cosine, > the float just below float(cos(pi/10))
+    g.icp_min_depth, g.icp_max_depth, g.color_weight = 0.15, 2.0, 0.0
+    thr = np.float32(np.cos(np.pi / 10))
+    g.normal_cos_thresh = float(np.nextafter(thr, np.float32(0)))
+
+    def n4(n3):
+        n = np.zeros(n3.shape[:2] + (4,), np.float32)
+        n[..., :3] = n3
+        return n
+
+    sn, tn = n4(z["src_normals"]), n4(z["tgt_normals"])
+    for k in range(len(z["transforms"])):
+        A, b, cnt = oracle.icp_normal_equations_refsum(z["src_depth"], sn, None, z["tgt_depth"],
+                                                        tn, None, s, g, z["transforms"][k])
+        assert cnt > 250
+        np.testing.assert_array_equal(A.view(np.uint32), z["A"][k].view(np.uint32))
+        np.testing.assert_array_equal(b.view(np.uint32), z["b"][k].view(np.uint32))
+        out = oracle.icp_normal_equations(z["src_depth"], sn, None, z["tgt_depth"], tn, None,
+                                          s, g, z["transforms"][k])
+        Af = z["A"][k].astype(np.float64).reshape(6, 6)
+        up = np.array([Af[i, j] for i in range(6) for j in range(i, 6)])
+        np.testing.assert_allclose(out[:21], up, rtol=1e-5, atol=1e-4)
+        np.testing.assert_allclose(out[21:27], z["b"][k], rtol=1e-5, atol=1e-4)
+        assert out[28] == cnt
