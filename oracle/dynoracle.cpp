@@ -32,6 +32,7 @@
 #include <cmath>
 
 #include "../dynamap_b200/csrc/dyn_exp.h"
+#include "gn_algebra.h"
 #include <cfloat>
 #include <cmath>
 #include <cstdint>
@@ -861,75 +862,8 @@ int64_t icp_normal_equations_refsum(const float* sd, const float* sn, const floa
 }
 
 // ------------------------------------------------------------- GN algebra
-// Solve A x = b, A symmetric positive definite (6x6): LDL^T without
-// pivoting.  Stands in for Eigen's A.ldlt().solve(b) (gnSolver.cu:439-442).
-int ldlt6(const double* A, const double* b, double* x) {
-  double L[36] = {0}, D[6];
-  for (int j = 0; j < 6; ++j) {
-    double s = A[j * 6 + j];
-    for (int k = 0; k < j; ++k) s -= L[j * 6 + k] * L[j * 6 + k] * D[k];
-    D[j] = s;
-    if (!(std::fabs(s) > 0)) return 0;
-    L[j * 6 + j] = 1;
-    for (int i = j + 1; i < 6; ++i) {
-      double t = A[i * 6 + j];
-      for (int k = 0; k < j; ++k) t -= L[i * 6 + k] * L[j * 6 + k] * D[k];
-      L[i * 6 + j] = t / D[j];
-    }
-  }
-  double y[6];
-  for (int i = 0; i < 6; ++i) {
-    double t = b[i];
-    for (int k = 0; k < i; ++k) t -= L[i * 6 + k] * y[k];
-    y[i] = t;
-  }
-  for (int i = 0; i < 6; ++i) y[i] /= D[i];
-  for (int i = 5; i >= 0; --i) {
-    double t = y[i];
-    for (int k = i + 1; k < 6; ++k) t -= L[k * 6 + i] * x[k];
-    x[i] = t;
-  }
-  return 1;
-}
-
-// exp of the twist matrix v2t(xi) (gnSolver.cu:446-455, Eigen exp at :443):
-// closed form R = I + a W + b W^2, t = (I + b W + c W^2) v with
-// a = sin(th)/th, b = (1-cos th)/th^2, c = (th - sin th)/th^3 (Rodrigues
-// and the SE(3) left Jacobian); Taylor series below th = 1e-4.
-void se3_exp(const double* xi, double* T) {
-  double w0 = xi[0], w1 = xi[1], w2 = xi[2];
-  double th2 = w0 * w0 + w1 * w1 + w2 * w2, th = std::sqrt(th2);
-  double a, b, c;
-  if (th < 1e-4) {
-    a = 1.0 - th2 / 6.0;
-    b = 0.5 - th2 / 24.0;
-    c = 1.0 / 6.0 - th2 / 120.0;
-  } else {
-    a = std::sin(th) / th;
-    b = (1.0 - std::cos(th)) / th2;
-    c = (th - std::sin(th)) / (th2 * th);
-  }
-  double W[9] = {0, -w2, w1, w2, 0, -w0, -w1, w0, 0};
-  double W2[9];
-  for (int i = 0; i < 3; ++i)
-    for (int j = 0; j < 3; ++j) {
-      double s = 0;
-      for (int k = 0; k < 3; ++k) s += W[i * 3 + k] * W[k * 3 + j];
-      W2[i * 3 + j] = s;
-    }
-  double Rm[9], Vm[9];
-  for (int i = 0; i < 9; ++i) {
-    double I = (i % 4 == 0) ? 1.0 : 0.0;
-    Rm[i] = I + a * W[i] + b * W2[i];
-    Vm[i] = I + b * W[i] + c * W2[i];
-  }
-  for (int i = 0; i < 3; ++i) {
-    for (int j = 0; j < 3; ++j) T[i * 4 + j] = Rm[i * 3 + j];
-    T[i * 4 + 3] = Vm[i * 3 + 0] * xi[3] + Vm[i * 3 + 1] * xi[4] + Vm[i * 3 + 2] * xi[5];
-  }
-  T[12] = T[13] = T[14] = 0;
-  T[15] = 1;
-}
+using dyo_gn::ldlt6;
+using dyo_gn::se3_exp;
 
 void matmul4d(const double* A, const double* B, double* C) {
   double t[16];
@@ -978,6 +912,35 @@ bool gn_update(const double* acc, const dyn_gn_params& g, int it, double* inc,
   if (!conv)
     for (int k = 0; k < 6; ++k) prev[k] = inc[k];
   return conv;
+}
+
+// gnSolver::solve's loop (gnSolver.cu:340-430) with every level at the
+// full-resolution images and the normal equations summed as the reference
+// sums them (icp_normal_equations_refsum): xi from zero, iterations 1..N-1
+// per level, then the NaN and max_increment guards.  Returns xi in inc.
+void gn_solve_refsum(const float* sd, const float* sn, const float* td, const float* tn,
+                     const Sensor<float>& s, const dyn_gn_params& g, double inc[6]) {
+  double prev[6] = {0, 0, 0, 0, 0, 0};
+  for (int k = 0; k < 6; ++k) inc[k] = 0;
+  for (int pl = 0; pl < 3; ++pl)
+    for (int it = 1; it < g.lvl_iteration_num[pl]; ++it) {
+      double Td[16];
+      se3_exp(inc, Td);
+      M4<float> T;
+      for (int k = 0; k < 16; ++k) T.m[k] = (float)Td[k];
+      float A[36], b[6];
+      icp_normal_equations_refsum(sd, sn, nullptr, td, tn, nullptr, s, g, T, A, b);
+      double acc[29];
+      int u = 0;
+      for (int i = 0; i < 6; ++i)
+        for (int j = i; j < 6; ++j) acc[u++] = (double)A[i * 6 + j];
+      for (int k = 0; k < 6; ++k) acc[21 + k] = (double)b[k];
+      if (gn_update(acc, g, it, inc, prev)) break;
+    }
+  double sum = 0;
+  for (int k = 0; k < 6; ++k) sum += inc[k];
+  if (std::isnan(sum) || std::isinf(sum) || sum >= (double)g.max_increment)
+    for (int k = 0; k < 6; ++k) inc[k] = 0;
 }
 
 int scale_level(int scale) {
@@ -1278,6 +1241,10 @@ int64_t dyo_icp_normal_equations_refsum(const float* sd, const float* sn, const 
                                         const float T[16], float A_out[36], float b_out[6]) {
   return icp_normal_equations_refsum(sd, sn, si, td, tn, ti, mk_sensor<float>(*level), *gn,
                                      m4_from<float>(T), A_out, b_out);
+}
+void dyo_gn_solve_refsum(const float* sd, const float* sn, const float* td, const float* tn,
+                         const dyn_sensor* level, const dyn_gn_params* gn, double inc_out[6]) {
+  gn_solve_refsum(sd, sn, td, tn, mk_sensor<float>(*level), *gn, inc_out);
 }
 void dyo_inverse4(const float m[16], float out[16]) {
   M4<float> r = inverse4(m4_from<float>(m));

@@ -83,6 +83,11 @@ int64_t dyo_icp_normal_equations_refsum(const float* src_depth, const float* src
                                         const float* tgt_n4, const float* tgt_i,
                                         const dyn_sensor* level, const dyn_gn_params* gn,
                                         const float T[16], float A_out[36], float b_out[6]);
+/* gnSolver::solve's loop on full-resolution images with those sums
+ * (gnSolver.cu:340-430): the final increment xi from zero. */
+void dyo_gn_solve_refsum(const float* src_depth, const float* src_n4, const float* tgt_depth,
+                         const float* tgt_n4, const dyn_sensor* level, const dyn_gn_params* gn,
+                         double inc_out[6]);
 /* float4x4::getInverse, utils_matrix.h:970-1086 */
 void dyo_inverse4(const float m[16], float out[16]);
 /* closed-form SE(3) exponential of xi = [w; t] (double), row-major */

@@ -53,6 +53,8 @@ def lib() -> C.CDLL:
                                                            P(C.c_float), P(C.c_double)]),
             "dyo_icp_normal_equations_refsum": (C.c_int64, [_vp] * 6 + [
                 P(abi.Sensor), P(abi.GnParams), P(C.c_float), P(C.c_float), P(C.c_float)]),
+            "dyo_gn_solve_refsum": (None, [_vp] * 4 + [P(abi.Sensor), P(abi.GnParams),
+                                                       P(C.c_double)]),
             "dyo_inverse4": (None, [P(C.c_float), P(C.c_float)]),
             "dyo_se3_exp": (None, [P(C.c_double), P(C.c_double)]),
             "dyo_ldlt_solve6": (C.c_int, [P(C.c_double), P(C.c_double), P(C.c_double)]),
@@ -184,6 +186,16 @@ def icp_normal_equations_refsum(sd, sn, si, td, tn, ti, s, g, T):
     n = lib().dyo_icp_normal_equations_refsum(*[ptr(a) for a in args], C.byref(s), C.byref(g),
                                               fptr(T), fptr(A), fptr(b))
     return A, b, int(n)
+
+
+def gn_solve_refsum(sd, sn, td, tn, s, g) -> np.ndarray:
+    """xi of gnSolver::solve's loop on full-resolution images, the normal
+    equations summed as the reference sums them."""
+    inc = np.zeros(6, np.float64)
+    args = [np.ascontiguousarray(a, np.float32) for a in (sd, sn, td, tn)]
+    lib().dyo_gn_solve_refsum(*[ptr(a) for a in args], C.byref(s), C.byref(g),
+                              inc.ctypes.data_as(P(C.c_double)))
+    return inc
 
 
 def inverse4(m: np.ndarray) -> np.ndarray:

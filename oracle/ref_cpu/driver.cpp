@@ -10,8 +10,9 @@
 //   (include/geometry/tsdf/tsdf.cu:18-550), the vertex map and normals of
 //   rgbdImage (include/image/sensor/rgbdImage.cu:23-167),
 //   pyramid::applyBilateralFilter (include/image/pyramid/pyramid.cu:213-233)
-//   and the ICP normal equations of buildNLSKernel
-//   (include/solver/gnSolver/gnSolver.cu:26-196).
+//   and the ICP of gnSolver: buildNLSKernel's normal equations and the
+//   whole gnSolver::solve (include/solver/gnSolver/gnSolver.cu:26-438, with
+//   the Eigen calls answered by shim/eigen_stub.h).
 #include <cstdint>
 #include <cstring>
 
@@ -227,6 +228,63 @@ void ref_icp_normal_equations(const float* src_depth, const float* src_n3, const
   dynref::nthreads() = saved;
   for (int j = 0; j < 36; ++j) A_out[j] = A(j);
   for (int j = 0; j < 6; ++j) b_out[j] = b(j);
+}
+
+// gnSolver::init + solve (gnSolver.cu:12-21, 317-438) of a source frame
+// against a target frame, every pyramid level at scale 1 (the reference's
+// pyramid is only defined there), from the identity: the final increment
+// xi = [w; t] (prev_increment_ on return) and the composed pose (row-major).
+// The caller keeps every valid source pixel's projection inside the image,
+// as for ref_icp_normal_equations.
+void ref_gn_solve(const float* src_depth, const float* tgt_depth, const uint8_t* src_rgb,
+                  const uint8_t* tgt_rgb, const dyn_sensor* s, const int32_t iters[3],
+                  float min_increment, float max_increment, float regularization,
+                  double inc_out[6], float pose_out[16]) {
+  const rgbdSensor sensor = to_sensor(s);
+  solver::Properties P;
+  for (int l = 0; l < 3; ++l) {
+    P.lvlIterationNum[l] = iters[l];
+    P.lvlScale[l] = 1;
+  }
+  P.maxIteration = iters[0] + iters[1] + iters[2];
+  P.minIncrement = min_increment;
+  P.maxIncrement = max_increment;
+  P.regularization = regularization;
+  P.huberConstant = 0.0f;
+  // never destroyed: the reference's pyramids are not meant to be freed here
+  solver::gnSolver* g = new solver::gnSolver();
+  g->init(P, sensor);
+  rgbdImage* tgt = new rgbdImage();
+  rgbdImage* src = new rgbdImage();
+  tgt->init(sensor);
+  src->init(sensor);
+  const size_t n = (size_t)s->rows * s->cols;
+  std::memcpy(tgt->depth, tgt_depth, n * sizeof(float));
+  std::memcpy(src->depth, src_depth, n * sizeof(float));
+  for (size_t i = 0; i < n; ++i) {
+    tgt->rgb[i] = tgt_rgb ? make_uchar3(tgt_rgb[3 * i], tgt_rgb[3 * i + 1], tgt_rgb[3 * i + 2])
+                          : make_uchar3(0, 0, 0);
+    src->rgb[i] = src_rgb ? make_uchar3(src_rgb[3 * i], src_rgb[3 * i + 1], src_rgb[3 * i + 2])
+                          : make_uchar3(0, 0, 0);
+  }
+  geometry::PointCloudXYZ tc, sc;
+  for (geometry::PointCloudXYZ* c : {&tc, &sc}) {
+    cudaMallocManaged(&c->points, n * sizeof(float3));
+    cudaMallocManaged(&c->normals, n * sizeof(float3));
+    std::memset(c->points, 0, n * sizeof(float3));
+    std::memset(c->normals, 0, n * sizeof(float3));
+  }
+  Eigen::Matrix4f pose;
+  for (int i = 0; i < 16; ++i) pose.v[i] = (i % 5 == 0) ? 1.0f : 0.0f;
+  solver::Vector6d prev;
+  for (int i = 0; i < 6; ++i) prev(i) = 0.0;
+  const int saved = dynref::nthreads();
+  dynref::nthreads() = 1;
+  g->solve(pose, prev, *tgt, *src, tc, sc);
+  dynref::nthreads() = saved;
+  for (int i = 0; i < 6; ++i) inc_out[i] = prev(i);
+  for (int r = 0; r < 4; ++r)
+    for (int c = 0; c < 4; ++c) pose_out[r * 4 + c] = pose(r, c);
 }
 
 }  // extern "C"

@@ -1,16 +1,20 @@
 // Stand-in for the Eigen 3 matrix types named by the reference's headers
-// (see eigen3/Eigen/Core in this directory), used ONLY to compile the
-// reference's sources for the CPU (test infrastructure).  Column-major
+// (see eigen3/Eigen/Core in this directory), used ONLY to compile and run
+// the reference's sources on the CPU (test infrastructure).  Column-major
 // fixed-size storage as Eigen's, with the element access, comma
 // initialisation and the few element-wise operations that
-// include/solver/gnSolver/gnSolver.cu names.  Eigen's LDLT solve and
-// matrix exponential are NOT provided: they abort if called.  The drivers
-// in this directory only run the reference's kernels (for the solver,
-// buildNLSKernel), never gnSolver::solve.
+// include/solver/gnSolver/gnSolver.cu names.  The two numerical routines
+// the reference takes from Eigen -- the 6x6 LDLT solve and the exponential
+// of an se(3) twist matrix (gnSolver.cu:439-445) -- are the oracle's own
+// (../../gn_algebra.h), so a reference solve driven through this header
+// and the oracle share that algebra and differ only where the reference's
+// own code does.  exp() accepts only twist matrices (bottom row zero).
 #pragma once
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+
+#include "../../gn_algebra.h"
 
 namespace Eigen {
 
@@ -94,16 +98,40 @@ struct Matrix {
     return r;
   }
 
+  // A.ldlt().solve(b) for the 6x6 systems of gnSolver.cu:439-442 (a zero
+  // pivot gives NaN, which the reference's NaN guard then zeroes)
   struct LDLT {
-    Matrix<S, C, 1> solve(const Matrix<S, C, 1>&) const {
-      std::fprintf(stderr, "eigen shim: LDLT solve is not provided\n");
-      std::abort();
+    const Matrix* a;
+    Matrix<S, C, 1> solve(const Matrix<S, C, 1>& b) const {
+      static_assert(R == 6 && C == 6, "the shim solves 6x6 systems only");
+      double A[36], bb[6], x[6] = {0, 0, 0, 0, 0, 0};
+      for (int i = 0; i < 6; ++i) {
+        for (int j = 0; j < 6; ++j) A[i * 6 + j] = (double)(*a)(i, j);
+        bb[i] = (double)b(i);
+      }
+      Matrix<S, C, 1> r;
+      if (!dyo_gn::ldlt6(A, bb, x))
+        for (int i = 0; i < 6; ++i) x[i] = NAN;
+      for (int i = 0; i < 6; ++i) r(i) = (S)x[i];
+      return r;
     }
   };
-  LDLT ldlt() const { return LDLT(); }
+  LDLT ldlt() const { return LDLT{this}; }
+  // exp() of v2t(xi) (gnSolver.cu:443-455): xi read back from the twist
   Matrix exp() const {
-    std::fprintf(stderr, "eigen shim: the matrix exponential is not provided\n");
-    std::abort();
+    static_assert(R == 4 && C == 4, "the shim exponentiates 4x4 twists only");
+    if ((*this)(3, 0) != 0 || (*this)(3, 1) != 0 || (*this)(3, 2) != 0 || (*this)(3, 3) != 0) {
+      std::fprintf(stderr, "eigen shim: exp() of a matrix that is not a twist\n");
+      std::abort();
+    }
+    const double xi[6] = {(double)(*this)(2, 1), (double)(*this)(0, 2), (double)(*this)(1, 0),
+                          (double)(*this)(0, 3), (double)(*this)(1, 3), (double)(*this)(2, 3)};
+    double T[16];
+    dyo_gn::se3_exp(xi, T);
+    Matrix r;
+    for (int i = 0; i < 4; ++i)
+      for (int j = 0; j < 4; ++j) r(i, j) = (S)T[i * 4 + j];
+    return r;
   }
 };
 

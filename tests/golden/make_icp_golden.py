@@ -8,7 +8,12 @@ bound its projections, so every valid source pixel must land inside the
 image); normals of both from the reference's rgbdImage.  For three source-
 to-target transforms (identity, the true relative motion, a perturbed one)
 the kernel runs at pyramid scale 1 on one host thread, so its float atomics
-sum the per-pixel terms in pixel order; the 6x6 A and b are stored.
+sum the per-pixel terms in pixel order; the 6x6 A and b are stored.  Then
+gnSolver::init + solve (gnSolver.cu:12-21, 317-438) from the identity with
+every level at scale 1, for three iteration / threshold settings (the last
+one trips the max_increment guard); its Eigen calls are answered by the
+oracle's own LDL^T and SE(3) exponential (oracle/gn_algebra.h through
+oracle/ref_cpu/shim/eigen_stub.h), and the final increments are stored.
 
 Usage (needs the reference tree, present only where the fixtures are made):
     bash oracle/ref_cpu/build_ref.sh && python tests/golden/make_icp_golden.py
@@ -45,6 +50,8 @@ def main():
     L.ref_normals.argtypes = [vp, C.POINTER(abi.Sensor), vp, vp]
     L.ref_icp_normal_equations.argtypes = [vp, vp, vp, vp, vp, vp, C.POINTER(abi.Sensor),
                                            C.POINTER(C.c_float), vp, vp]
+    L.ref_gn_solve.argtypes = [vp, vp, vp, vp, C.POINTER(abi.Sensor), C.POINTER(C.c_int32),
+                               C.c_float, C.c_float, C.c_float, vp, vp]
     L.ref_set_threads(1)
     sensor = abi.Sensor(rows=60, cols=80, fx=65.625, fy=65.625, cx=39.5, cy=29.5,
                         depth_scaler=1000.0)
@@ -76,11 +83,26 @@ def main():
         Ts.append(T)
         As.append(A)
         bs.append(b)
+    # whole solves: (iterations per level, min_increment, max_increment,
+    # regularization)
+    settings = [((5, 4, 3), 1e-3, 0.3, 0.02), ((10, 5, 4), 1e-5, 0.3, 0.02),
+                ((3, 3, 3), 1e-3, 1e-9, 0.02)]
+    incs, poses = [], []
+    for iters, mi, ma, rg in settings:
+        inc = np.zeros(6, np.float64)
+        pose = np.zeros(16, np.float32)
+        L.ref_gn_solve(p(src), p(tgt), None, None, C.byref(sensor), (C.c_int32 * 3)(*iters),
+                       mi, ma, rg, p(inc), p(pose))
+        incs.append(inc)
+        poses.append(pose.reshape(4, 4))
     np.savez_compressed(
         OUT, src_depth=src, tgt_depth=tgt, src_normals=nrm[0], tgt_normals=nrm[1],
         sensor=np.array([sensor.rows, sensor.cols, sensor.fx, sensor.fy, sensor.cx, sensor.cy,
                          sensor.depth_scaler], np.float64),
-        transforms=np.array(Ts), A=np.array(As), b=np.array(bs))
+        transforms=np.array(Ts), A=np.array(As), b=np.array(bs),
+        solve_iters=np.array([s_[0] for s_ in settings], np.int32),
+        solve_thresholds=np.array([s_[1:] for s_ in settings], np.float32),
+        solve_inc=np.array(incs), solve_pose=np.array(poses))
     print(f"wrote {OUT}: {len(Ts)} transforms, A[1] diag {np.array(As)[1].reshape(6, 6).diagonal()}")
 
 

@@ -148,3 +148,35 @@ def test_reference_icp_normal_equations(oracle):
         np.testing.assert_allclose(out[:21], up, rtol=1e-5, atol=1e-4)
         np.testing.assert_allclose(out[21:27], z["b"][k], rtol=1e-5, atol=1e-4)
         assert out[28] == cnt
+
+
+def test_reference_gn_solve(oracle):
+    """gnSolver::solve (gnSolver.cu:317-438) from the identity, every level
+    at full resolution, for three settings (the last trips the
+    max_increment guard): the oracle's GN loop over the reference-order sums
+    reproduces the reference's final increment bit for bit.  The Eigen calls
+    are the shared LDL^T / SE(3) exponential of oracle/gn_algebra.h, so this
+    pins the reference's own loop: scaling, damping, convergence test,
+    iteration counts and guards."""
+    z = np.load(os.path.join(HERE, "golden", "ref_icp_normal_equations.npz"))
+    r, c, fx, fy, cx, cy, ds = z["sensor"]
+    s = abi.Sensor(rows=int(r), cols=int(c), fx=fx, fy=fy, cx=cx, cy=cy, depth_scaler=ds)
+
+    def n4(n3):
+        n = np.zeros(n3.shape[:2] + (4,), np.float32)
+        n[..., :3] = n3
+        return n
+
+    sn, tn = n4(z["src_normals"]), n4(z["tgt_normals"])
+    moved = 0
+    for iters, (mi, ma, rg), inc in zip(z["solve_iters"], z["solve_thresholds"], z["solve_inc"]):
+        _, g, _, _ = abi.defaults()
+        g.icp_min_depth, g.icp_max_depth, g.color_weight = 0.15, 2.0, 0.0
+        g.normal_cos_thresh = float(np.nextafter(np.float32(np.cos(np.pi / 10)), np.float32(0)))
+        g.lvl_iteration_num[:] = [int(x) for x in iters]
+        g.lvl_scale[:] = [1, 1, 1]
+        g.min_increment, g.max_increment, g.regularization = float(mi), float(ma), float(rg)
+        got = oracle.gn_solve_refsum(z["src_depth"], sn, z["tgt_depth"], tn, s, g)
+        np.testing.assert_array_equal(got.view(np.uint64), inc.view(np.uint64))
+        moved += int(np.any(inc != 0))
+    assert moved == 2  # two settings converge to a motion, the guard zeroes the third
