@@ -717,8 +717,10 @@ constexpr int kRayTX = 16, kRayTY = 16;
 // tsdfVolume raycast (tsdf.cu:471-526) of pixel (x, y) from camera pose T:
 // march from 0 by the interpolated sdf (a truncation where unobserved) until
 // the sdf drops under a voxel or the depth passes max_sensor_depth; then the
-// interpolated colour at the hit.  Returns true when the march hit the step
-// cap.
+// interpolated colour at the hit.  Beyond the near distance, samples before
+// skip_to or after skip_far (the tile's ray depth bounds: no allocated block
+// there) step by the truncation without a lookup -- what the lookup would
+// have returned.  Returns true when the march hit the step cap.
 __device__ inline bool raycast_exact_px(const VolumeDev& v, const DSensor& s, const M4f& T, int x,
                                         int y, float skip_to, float skip_far,
                                         float* __restrict__ depth_out,
@@ -845,7 +847,7 @@ __device__ inline VoxelSample interp16(const VolumeDev& v, F3 q, unsigned raw0, 
 // The march of the mixed form in voxel units: the sample at depth z is
 // o + z * d with o the camera centre and d the pixel's ray direction per
 // unit depth (both divided by vs), by fused multiply-adds; its voxel is
-// floor(q + 0.5).
+// floor(q + 0.5).  skip_to / skip_far as in raycast_exact_px.
 __device__ inline bool raycast_mixed_px(const VolumeDev& v, const DSensor& s, const M4f& T, int x,
                                         int y, float skip_to, float skip_far,
                                         float* __restrict__ depth_out,
