@@ -115,8 +115,12 @@ def associate(stamps_a: Sequence[float], stamps_b: Sequence[float],
     first, each stamp used at most once; sorted by i."""
     a = np.asarray(stamps_a, dtype=np.float64)
     b = np.asarray(stamps_b, dtype=np.float64)
-    cand = sorted((abs(a[i] - b[j]), i, j) for i in range(len(a)) for j in range(len(b))
-                  if abs(a[i] - b[j]) < max_difference)
+    order = np.argsort(b, kind="stable")
+    bs = b[order]
+    lo = np.searchsorted(bs, a - max_difference, side="left")
+    hi = np.searchsorted(bs, a + max_difference, side="right")
+    cand = sorted((abs(a[i] - bs[k]), i, int(order[k])) for i in range(len(a))
+                  for k in range(lo[i], hi[i]) if abs(a[i] - bs[k]) < max_difference)
     used_a, used_b, out = set(), set(), []
     for _, i, j in cand:
         if i not in used_a and j not in used_b:
