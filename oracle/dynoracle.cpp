@@ -365,6 +365,107 @@ struct Volume {
   }
 };
 
+// ---------------------------------------------------------- mesh vertices
+// MeshExtractor's TrilinearInterpolation (meshExtractor.cu:22-93): the
+// 2x2x2 cell around position, false as soon as a corner is unobserved
+// (unlike GetInterpolatedVoxel, which substitutes the centre voxel);
+// weights from position * (1/vs), corners summed in the order below.
+template <class R>
+bool mesh_trilinear(const Volume<R>& V, V3<R> position, R* dist) {
+  R vs = (R)V.p.voxel_size;
+  V3<R> pos_dual = position - v3(vs / R(2), vs / R(2), vs / R(2));
+  V3<R> vp = position * (R(1) / vs);  // float3 / float, cuda_math.h:357-361
+  V3<R> w = v3(vp.x - std::floor(vp.x), vp.y - std::floor(vp.y), vp.z - std::floor(vp.z));
+  static const int off[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1},
+                                {1, 1, 0}, {0, 1, 1}, {1, 0, 1}, {1, 1, 1}};
+  R d = 0;
+  for (int k = 0; k < 8; ++k) {
+    Voxel<R> v = V.get_voxel(pos_dual + v3(off[k][0] ? vs : R(0), off[k][1] ? vs : R(0),
+                                           off[k][2] ? vs : R(0)));
+    if (v.w == 0) return false;
+    R a = off[k][0] ? w.x : R(1) - w.x;
+    R b = off[k][1] ? w.y : R(1) - w.y;
+    R c = off[k][2] ? w.z : R(1) - w.z;
+    d += a * b * c * v.sdf;
+  }
+  *dist = d;
+  return true;
+}
+
+// MeshExtractor::ExtractMesh (meshExtractor.cu:364-407) up to the vertices:
+// the grid of the box [lo, hi) with twice the box's extent in voxel steps
+// (as the reference's grid_size), per grid position the eight corner
+// samples at +-vs/2 (ExtractMeshAtPosition :126-214) and, on every cube
+// edge whose ends are on opposite sides of 0, the vertex VertexInterpolation
+// (:95-121) places, coloured by the centre voxel.  Each vertex is
+// {x, y, z, r, g, b}; the reference's triangles (its marching-cubes table)
+// use exactly these vertices.  Returns the count (at most cap written).
+int64_t mesh_vertices(const Volume<float>& V, const float lo[3], const float hi[3],
+                      float* out, int64_t cap) {
+  const float vs = (float)V.p.voxel_size;
+  V3<float> size = v3(std::fabs(lo[0] - hi[0]), std::fabs(lo[1] - hi[1]),
+                      std::fabs(lo[2] - hi[2]));
+  const int gx = (int)(size.x / vs * 2), gy = (int)(size.y / vs * 2), gz = (int)(size.z / vs * 2);
+  const int64_t total = (int64_t)gx * gy * gz;
+  const float P = vs / 2.0f, M = -P;
+  // corners in the reference's cube-index order (bit k: corner k inside)
+  // and the 12 edges between them
+  static const int corner[8][3] = {{0, 1, 0}, {1, 1, 0}, {1, 0, 0}, {0, 0, 0},
+                                   {0, 1, 1}, {1, 1, 1}, {1, 0, 1}, {0, 0, 1}};
+  static const int edge[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6},
+                                  {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+  int64_t n = 0;
+  for (int64_t i = 0; i < total; ++i) {
+    const int px = (int)(i % gx), py = (int)((i / gx) % gy), pz = (int)(i / ((int64_t)gx * gy));
+    const V3<float> pos = v3((float)px * vs + lo[0], (float)py * vs + lo[1], (float)pz * vs + lo[2]);
+    V3<float> p[8];
+    float d[8];
+    bool ok = true;
+    for (int k = 0; k < 8 && ok; ++k) {
+      p[k] = pos + v3(corner[k][0] ? P : M, corner[k][1] ? P : M, corner[k][2] ? P : M);
+      ok = mesh_trilinear(V, p[k], &d[k]);
+    }
+    if (!ok) continue;
+    unsigned cube = 0;
+    for (int k = 0; k < 8; ++k)
+      if (d[k] < 0.0f) cube |= 1u << k;
+    if (cube == 0 || cube == 255) continue;
+    const Voxel<float> c = V.get_voxel(pos);
+    const float rgb0[3] = {(float)c.c[0] * (1.0f / 255.f), (float)c.c[1] * (1.0f / 255.f),
+                           (float)c.c[2] * (1.0f / 255.f)};
+    for (int e = 0; e < 12; ++e) {
+      const int a = edge[e][0], b = edge[e][1];
+      if (((cube >> a) & 1u) == ((cube >> b) & 1u)) continue;
+      float vtx[6];
+      const float d1 = d[a], d2 = d[b];
+      const V3<float> p1 = p[a], p2 = p[b];
+      bool end = true;
+      V3<float> q = p1;
+      if (std::fabs(0.0f - d1) < 0.00001f) q = p1;
+      else if (std::fabs(0.0f - d2) < 0.00001f) q = p2;
+      else if (std::fabs(d1 - d2) < 0.00001f) q = p1;
+      else end = false;
+      if (end) {
+        vtx[3] = rgb0[0];
+        vtx[4] = rgb0[1];
+        vtx[5] = rgb0[2];
+      } else {
+        const float mu = (0.0f - d1) / (d2 - d1);
+        q = v3(p1.x + mu * (p2.x - p1.x), p1.y + mu * (p2.y - p1.y), p1.z + mu * (p2.z - p1.z));
+        for (int k = 0; k < 3; ++k)
+          vtx[3 + k] = (float)((float)c.c[k] + mu * (float)(c.c[k] - c.c[k])) / 255.f;
+      }
+      vtx[0] = q.x;
+      vtx[1] = q.y;
+      vtx[2] = q.z;
+      if (n < cap)
+        for (int k = 0; k < 6; ++k) out[6 * n + k] = vtx[k];
+      ++n;
+    }
+  }
+  return n;
+}
+
 // AllocateFromDepthKernel, tsdf.cu:346-453 for one pixel: visits blocks in
 // the reference's DDA order and calls f(x, y, z) for each (the `diff`
 // pre-step included).  Returns false if the step cap (F3) cut the ray.
@@ -1316,6 +1417,12 @@ int64_t dyo_volume_num_blocks(void* v) {
   return a->fp64 ? ((Volume<double>*)a->v)->nalloc : ((Volume<float>*)a->v)->nalloc;
 }
 
+int64_t dyo_mesh_vertices(void* v, const float lo[3], const float hi[3], float* out,
+                          int64_t cap) {
+  AnyVolume* a = (AnyVolume*)v;
+  if (a->fp64) return -1;
+  return mesh_vertices(*(Volume<float>*)a->v, lo, hi, out, cap);
+}
 int64_t dyo_volume_download(void* v, int32_t* coords, uint8_t* rgbw,
                             void* sdf_out, int64_t cap) {
   AnyVolume* a = (AnyVolume*)v;

@@ -107,6 +107,11 @@ void dyo_volume_raycast(void* v, const float pose[16], const dyn_sensor* s,
                         float* depth_out, uint8_t* rgb_out,
                         int64_t counters[DYO_C_N]);
 int64_t dyo_volume_num_blocks(void* v);
+/* MeshExtractor::ExtractMesh over the box [lo, hi] up to its vertices
+ * (meshExtractor.cu:22-214, 364-407): {x, y, z, r, g, b} of every vertex its
+ * triangles use, per grid cell in grid order (FP32 volumes; -1 otherwise). */
+int64_t dyo_mesh_vertices(void* v, const float lo[3], const float hi[3], float* out,
+                          int64_t cap);
 /* sdf_out: float (fp32 volume) or double (fp64 volume) per voxel; voxels in
  * x-major order.  Any output may be NULL. */
 int64_t dyo_volume_download(void* v, int32_t* coords, uint8_t* rgbw,

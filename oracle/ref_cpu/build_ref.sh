@@ -21,7 +21,9 @@ fi
 mkdir -p "$OUT/src"
 SRCS=(geometry/tsdf/tsdf.cu dataStructure/hashTable/hashTable.cu dataStructure/heap/heap.cu
       image/sensor/rgbdImage.cu image/pyramid/pyramid.cu image/conv2D/conv2D.cu
-      image/kernel2D/kernel2D.cu solver/gnSolver/gnSolver.cu)
+      image/kernel2D/kernel2D.cu solver/gnSolver/gnSolver.cu
+      geometry/mesh/meshExtractor/meshExtractor.cu geometry/mesh/mesh.cu
+      geometry/mesh/meshSTD.cu)
 OBJS=()
 INCS=(-I"$HERE/shim" -I"$INC" -I"$INC/dataStructure" -I"$INC/dataStructure/heap"
       -I"$INC/dataStructure/hashTable" -I"$INC/image" -I"$INC/image/sensor"

@@ -10,9 +10,11 @@
 //   (include/geometry/tsdf/tsdf.cu:18-550), the vertex map and normals of
 //   rgbdImage (include/image/sensor/rgbdImage.cu:23-167),
 //   pyramid::applyBilateralFilter (include/image/pyramid/pyramid.cu:213-233)
-//   and the ICP of gnSolver: buildNLSKernel's normal equations and the
-//   whole gnSolver::solve (include/solver/gnSolver/gnSolver.cu:26-438, with
-//   the Eigen calls answered by shim/eigen_stub.h).
+//   the ICP of gnSolver: buildNLSKernel's normal equations and the whole
+//   gnSolver::solve (include/solver/gnSolver/gnSolver.cu:26-438, with the
+//   Eigen calls answered by shim/eigen_stub.h), and
+//   MeshExtractor::ExtractMesh (include/geometry/mesh/meshExtractor/
+//   meshExtractor.cu:364-407) with mesh.cu / meshSTD.cu.
 #include <cstdint>
 #include <cstring>
 
@@ -32,16 +34,6 @@ void buildNLSKernel(gnSolver& solver, uchar3* target_rgb, float* target_depth, u
                     mat6x6* acc_A, mat6x1* acc_b, geometry::PointCloudXYZ& targetCloud,
                     geometry::PointCloudXYZ& sourceCloud, float scale, float huberConstant);
 }  // namespace solver
-}  // namespace DynaMap
-
-// tsdf.cu's ExtractMesh names the mesh extractor; mesh extraction is not on
-// the path, so these definitions only satisfy the linker.
-namespace DynaMap {
-namespace geometry {
-void MeshExtractor::Init(unsigned int, float) {}
-void MeshExtractor::ExtractMesh(tsdf::tsdfVolume*, float3, float3) {}
-Mesh MeshExtractor::GetMesh() { return Mesh(); }
-}  // namespace geometry
 }  // namespace DynaMap
 
 namespace {
@@ -228,6 +220,37 @@ void ref_icp_normal_equations(const float* src_depth, const float* src_n3, const
   dynref::nthreads() = saved;
   for (int j = 0; j < 36; ++j) A_out[j] = A(j);
   for (int j = 0; j < 6; ++j) b_out[j] = b(j);
+}
+
+// MeshExtractor::Init + ExtractMesh + GetMesh over the box [lo, hi] of a
+// volume (one host thread, so triangles come out in grid order): per
+// triangle its three vertices' positions and colours, 18 floats, into out
+// (at most cap triangles).  Returns the triangle count.
+int64_t ref_extract_mesh(void* v, const float lo[3], const float hi[3], float voxel_size,
+                         float* out, int64_t cap) {
+  tsdf::tsdfVolume* vol = (tsdf::tsdfVolume*)v;
+  geometry::MeshExtractor* me = new geometry::MeshExtractor();  // kept: its mesh is read below
+  me->Init((unsigned)(cap > 0 ? cap : 1), voxel_size);
+  const int saved = dynref::nthreads();
+  dynref::nthreads() = 1;
+  me->ExtractMesh(vol, make_float3(lo[0], lo[1], lo[2]), make_float3(hi[0], hi[1], hi[2]));
+  dynref::nthreads() = saved;
+  geometry::Mesh m = me->GetMesh();
+  const int64_t n = (int64_t)m.num_triangles_;
+  for (int64_t i = 0; i < n && i < cap; ++i) {
+    const geometry::Vertex* vs[3] = {&m.triangles_[i].v0, &m.triangles_[i].v1,
+                                     &m.triangles_[i].v2};
+    for (int k = 0; k < 3; ++k) {
+      float* o = out + 18 * i + 6 * k;
+      o[0] = vs[k]->position.x;
+      o[1] = vs[k]->position.y;
+      o[2] = vs[k]->position.z;
+      o[3] = vs[k]->color.x;
+      o[4] = vs[k]->color.y;
+      o[5] = vs[k]->color.z;
+    }
+  }
+  return n;
 }
 
 // gnSolver::init + solve (gnSolver.cu:12-21, 317-438) of a source frame

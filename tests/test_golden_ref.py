@@ -1,8 +1,9 @@
 """The oracle reproduces the reference's own outputs (golden vectors made
 by tests/golden/make_golden.py and make_icp_golden.py from the reference
 sources compiled for the CPU): allocation, integration, raycast,
-vertex/normal maps, the hash and the ICP normal equations of buildNLSKernel
-bit for bit; the bilateral filter within 2 ulp-scale relative error (the
+vertex/normal maps, the hash, the ICP normal equations of buildNLSKernel,
+gnSolver::solve's increments and the vertices of MeshExtractor's mesh bit
+for bit; the bilateral filter within 2 ulp-scale relative error (the
 oracle's range weight uses a portable FP32 exp, the reference libm's FP64
 exp)."""
 import os
@@ -180,3 +181,18 @@ def test_reference_gn_solve(oracle):
         np.testing.assert_array_equal(got.view(np.uint64), inc.view(np.uint64))
         moved += int(np.any(inc != 0))
     assert moved == 2  # two settings converge to a motion, the guard zeroes the third
+
+
+def test_reference_mesh_vertices(oracle_volume):
+    """MeshExtractor::ExtractMesh (meshExtractor.cu:22-214, 364-407) over a
+    box of the pinned volume: the oracle's vertices -- corner samples that
+    give up at an unobserved corner, the cube edges that cross zero, the
+    reference's edge interpolation and centre-voxel colour -- are exactly
+    the distinct vertices of the reference's triangles."""
+    vol, _ = oracle_volume
+    z = np.load(os.path.join(HERE, "golden", "ref_mesh_vertices.npz"))
+    lo, hi = z["box"]
+    got = vol.mesh_vertices(lo, hi)
+    uniq = np.unique(np.ascontiguousarray(got).view(np.uint32), axis=0)
+    assert len(got) >= len(uniq) > 1000
+    np.testing.assert_array_equal(uniq, z["vertices"].view(np.uint32))
