@@ -32,6 +32,7 @@
 #include <cmath>
 
 #include "../dynamap_b200/csrc/dyn_exp.h"
+#include "../dynamap_b200/csrc/mc_tables.h"
 #include "gn_algebra.h"
 #include <cfloat>
 #include <cmath>
@@ -400,8 +401,11 @@ bool mesh_trilinear(const Volume<R>& V, V3<R> position, R* dist) {
 // (:95-121) places, coloured by the centre voxel.  Each vertex is
 // {x, y, z, r, g, b}; the reference's triangles (its marching-cubes table)
 // use exactly these vertices.  Returns the count (at most cap written).
-int64_t mesh_vertices(const Volume<float>& V, const float lo[3], const float hi[3],
-                      float* out, int64_t cap) {
+// The cell walk shared by mesh_vertices and mesh_triangles: for every grid
+// cell with all corners observed and a zero crossing, cell(cube, vert)
+// with vert[e] = {x, y, z, r, g, b} for every cut edge e.
+template <class F>
+void mesh_cells(const Volume<float>& V, const float lo[3], const float hi[3], F&& cell) {
   const float vs = (float)V.p.voxel_size;
   V3<float> size = v3(std::fabs(lo[0] - hi[0]), std::fabs(lo[1] - hi[1]),
                       std::fabs(lo[2] - hi[2]));
@@ -414,7 +418,6 @@ int64_t mesh_vertices(const Volume<float>& V, const float lo[3], const float hi[
                                    {0, 1, 1}, {1, 1, 1}, {1, 0, 1}, {0, 0, 1}};
   static const int edge[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6},
                                   {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
-  int64_t n = 0;
   for (int64_t i = 0; i < total; ++i) {
     const int px = (int)(i % gx), py = (int)((i / gx) % gy), pz = (int)(i / ((int64_t)gx * gy));
     const V3<float> pos = v3((float)px * vs + lo[0], (float)py * vs + lo[1], (float)pz * vs + lo[2]);
@@ -433,10 +436,11 @@ int64_t mesh_vertices(const Volume<float>& V, const float lo[3], const float hi[
     const Voxel<float> c = V.get_voxel(pos);
     const float rgb0[3] = {(float)c.c[0] * (1.0f / 255.f), (float)c.c[1] * (1.0f / 255.f),
                            (float)c.c[2] * (1.0f / 255.f)};
+    float vert[12][6];
     for (int e = 0; e < 12; ++e) {
       const int a = edge[e][0], b = edge[e][1];
       if (((cube >> a) & 1u) == ((cube >> b) & 1u)) continue;
-      float vtx[6];
+      float* vtx = vert[e];
       const float d1 = d[a], d2 = d[b];
       const V3<float> p1 = p[a], p2 = p[b];
       bool end = true;
@@ -458,11 +462,43 @@ int64_t mesh_vertices(const Volume<float>& V, const float lo[3], const float hi[
       vtx[0] = q.x;
       vtx[1] = q.y;
       vtx[2] = q.z;
+    }
+    cell(cube, vert);
+  }
+}
+
+int64_t mesh_vertices(const Volume<float>& V, const float lo[3], const float hi[3],
+                      float* out, int64_t cap) {
+  static const int edge[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6},
+                                  {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+  int64_t n = 0;
+  mesh_cells(V, lo, hi, [&](unsigned cube, const float (*vert)[6]) {
+    for (int e = 0; e < 12; ++e) {
+      if (((cube >> edge[e][0]) & 1u) == ((cube >> edge[e][1]) & 1u)) continue;
       if (n < cap)
-        for (int k = 0; k < 6; ++k) out[6 * n + k] = vtx[k];
+        for (int k = 0; k < 6; ++k) out[6 * n + k] = vert[e][k];
       ++n;
     }
-  }
+  });
+  return n;
+}
+
+// The mesh of the same cells with this project's marching-cubes table
+// (dynamap_b200/csrc/mc_tables.h, generated by dynamap_b200/mc_tables.py,
+// not the reference's table): 18 floats per triangle, three vertices
+// {x, y, z, r, g, b}.  Returns the triangle count.
+int64_t mesh_triangles(const Volume<float>& V, const float lo[3], const float hi[3],
+                       float* out, int64_t cap) {
+  int64_t n = 0;
+  mesh_cells(V, lo, hi, [&](unsigned cube, const float (*vert)[6]) {
+    const signed char* row = dyn::kMcTriangles[cube];
+    for (int j = 0; j + 2 < dyn::kMcMaxTriIdx && row[j] >= 0; j += 3) {
+      if (n < cap)
+        for (int k = 0; k < 3; ++k)
+          for (int c = 0; c < 6; ++c) out[18 * n + 6 * k + c] = vert[row[j + k]][c];
+      ++n;
+    }
+  });
   return n;
 }
 
@@ -1422,6 +1458,12 @@ int64_t dyo_mesh_vertices(void* v, const float lo[3], const float hi[3], float* 
   AnyVolume* a = (AnyVolume*)v;
   if (a->fp64) return -1;
   return mesh_vertices(*(Volume<float>*)a->v, lo, hi, out, cap);
+}
+int64_t dyo_mesh_triangles(void* v, const float lo[3], const float hi[3], float* out,
+                           int64_t cap) {
+  AnyVolume* a = (AnyVolume*)v;
+  if (a->fp64) return -1;
+  return mesh_triangles(*(Volume<float>*)a->v, lo, hi, out, cap);
 }
 int64_t dyo_volume_download(void* v, int32_t* coords, uint8_t* rgbw,
                             void* sdf_out, int64_t cap) {

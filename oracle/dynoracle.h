@@ -112,6 +112,10 @@ int64_t dyo_volume_num_blocks(void* v);
  * triangles use, per grid cell in grid order (FP32 volumes; -1 otherwise). */
 int64_t dyo_mesh_vertices(void* v, const float lo[3], const float hi[3], float* out,
                           int64_t cap);
+/* The mesh of the same cells with this project's marching-cubes table
+ * (dynamap_b200/csrc/mc_tables.h): 18 floats per triangle. */
+int64_t dyo_mesh_triangles(void* v, const float lo[3], const float hi[3], float* out,
+                           int64_t cap);
 /* sdf_out: float (fp32 volume) or double (fp64 volume) per voxel; voxels in
  * x-major order.  Any output may be NULL. */
 int64_t dyo_volume_download(void* v, int32_t* coords, uint8_t* rgbw,

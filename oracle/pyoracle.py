@@ -65,6 +65,7 @@ def lib() -> C.CDLL:
             "dyo_volume_raycast": (None, [_vp, P(C.c_float), P(abi.Sensor), _vp, _vp, P(C.c_int64)]),
             "dyo_volume_num_blocks": (C.c_int64, [_vp]),
             "dyo_mesh_vertices": (C.c_int64, [_vp, P(C.c_float), P(C.c_float), _vp, C.c_int64]),
+            "dyo_mesh_triangles": (C.c_int64, [_vp, P(C.c_float), P(C.c_float), _vp, C.c_int64]),
             "dyo_volume_download": (C.c_int64, [_vp, _vp, _vp, _vp, C.c_int64]),
             "dyo_session_create": (_vp, [P(abi.TsdfParams), P(abi.GnParams),
                                          P(abi.BilateralParams), P(abi.Sensor), C.c_int32]),
@@ -264,6 +265,17 @@ class Volume:
         out = np.zeros((max(n, 0), 6), np.float32)
         if n > 0:
             lib().dyo_mesh_vertices(self.h, lo_c, hi_c, ptr(out), n)
+        return out
+
+    def mesh_triangles(self, lo, hi) -> np.ndarray:
+        """[n, 3, 6] triangles of the same cells with this project's
+        marching-cubes table."""
+        lo_c = (C.c_float * 3)(*[float(x) for x in lo])
+        hi_c = (C.c_float * 3)(*[float(x) for x in hi])
+        n = lib().dyo_mesh_triangles(self.h, lo_c, hi_c, None, 0)
+        out = np.zeros((max(n, 0), 3, 6), np.float32)
+        if n > 0:
+            lib().dyo_mesh_triangles(self.h, lo_c, hi_c, ptr(out), n)
         return out
 
     def num_blocks(self) -> int:

@@ -6,9 +6,9 @@ oracle/ref_cpu/build_ref.sh into oracle/_ref/libdynref.so).
 The volume is the one ref_rigid_small.npz pins (its three frames integrated
 at their poses by the reference); the mesh of a box through the observed
 surfaces is extracted on one host thread.  Stored: the box, the triangle
-count and the distinct vertices {x, y, z, r, g, b} of the triangles (sorted
-by their bit patterns) -- the part of the mesh that does not depend on the
-marching-cubes triangle table.
+count, the total area and the distinct vertices {x, y, z, r, g, b} of the
+triangles (sorted by their bit patterns) -- the part of the mesh that does
+not depend on the marching-cubes triangle table.
 
 Usage (needs the reference tree, present only where the fixtures are made):
     bash oracle/ref_cpu/build_ref.sh && python tests/golden/make_mesh_golden.py
@@ -61,8 +61,10 @@ def main():
     assert 0 < n < cap
     verts = out[:n].reshape(-1, 6)
     uniq = np.unique(np.ascontiguousarray(verts).view(np.uint32), axis=0).view(np.float32)
+    t = out[:n].reshape(-1, 3, 6)[:, :, :3].astype(np.float64)
+    area = 0.5 * np.linalg.norm(np.cross(t[:, 1] - t[:, 0], t[:, 2] - t[:, 0]), axis=1).sum()
     np.savez_compressed(OUT, box=np.array(BOX, np.float32), triangles=np.int64(n),
-                        vertices=uniq)
+                        area=np.float64(area), vertices=uniq)
     print(f"wrote {OUT}: {n} triangles, {len(uniq)} distinct vertices")
 
 

@@ -196,3 +196,20 @@ def test_reference_mesh_vertices(oracle_volume):
     uniq = np.unique(np.ascontiguousarray(got).view(np.uint32), axis=0)
     assert len(got) >= len(uniq) > 1000
     np.testing.assert_array_equal(uniq, z["vertices"].view(np.uint32))
+
+
+def test_mesh_with_own_table_against_reference(oracle_volume):
+    """The same box meshed with this project's generated marching-cubes
+    table (the reference's table is not copied): its vertices are the
+    reference's, and its triangle count and area match the reference's
+    mesh (the tables may split a cell's polygons differently)."""
+    vol, _ = oracle_volume
+    z = np.load(os.path.join(HERE, "golden", "ref_mesh_vertices.npz"))
+    lo, hi = z["box"]
+    tris = vol.mesh_triangles(lo, hi)
+    uniq = np.unique(np.ascontiguousarray(tris.reshape(-1, 6)).view(np.uint32), axis=0)
+    np.testing.assert_array_equal(uniq, z["vertices"].view(np.uint32))
+    assert len(tris) == int(z["triangles"])
+    p = tris[:, :, :3].astype(np.float64)
+    area = 0.5 * np.linalg.norm(np.cross(p[:, 1] - p[:, 0], p[:, 2] - p[:, 0]), axis=1).sum()
+    assert abs(area - float(z["area"])) < 5e-3 * float(z["area"])
