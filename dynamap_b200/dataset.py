@@ -12,9 +12,9 @@ Differences from the reference, each a fix:
 * RGB is returned in RGB order (OpenCV reads BGR);
 * an association file is read by its paths, so both column orders work
   (the reference takes word 0 as the depth name and word 2 as the RGB name,
-  getAssociateContent :154-155);
+  getAssociateContent :174-175);
 * ground truth is matched to each frame by time stamp (the reference takes
-  line curID + offsetLineGroundTruth, :196).
+  line curID + offsetLineGroundTruth, :210-221).
 
 Images are decoded with OpenCV when it is importable, else with Pillow.
 """

@@ -5,8 +5,8 @@
 // buildModelLS runs the per-frame path in the intended order (track the
 // frame against the previous target, integrate it at the new pose, raycast
 // the next target); Mode 0 tracks frame to frame, Mode 1 frame to model.
-// Frames are the sensor's uint16 depth + optional RGB (the reference reads
-// them through utils::dataSet, which is not part of this path).
+// Frames are the sensor's uint16 depth + optional RGB, passed directly or
+// through utils::dataSet (include/utils/dataSet.h) as the reference does.
 #pragma once
 
 #include <cstdint>
@@ -58,6 +58,26 @@ class builder {
     if (r != DYN_ERR_HASH_FULL) dyn_throw("builder::buildModelLS", r);
     currentPose_ = Matrix4f::from_row_major(pose);
     ++frameNum;
+  }
+
+  // builder.cu:70 / builder.h:58: the frame dataset.image, read by
+  // dataSet::invokeNextFrame (any type with that member and frame layout)
+  template <class DataSet>
+  auto buildModelLS(DataSet& dataset, int Mode = 0) -> decltype(dataset.image.depth.data(), void()) {
+    check_frame(dataset.image, "builder::buildModelLS");
+    buildModelLS(dataset.image.depth.data(),
+                 dataset.image.rgb.empty() ? nullptr : dataset.image.rgb.data(), Mode);
+  }
+  // builder.cu:140-160 / builder.h:60: integrate dataset.image at the
+  // frame's ground-truth pose
+  template <class DataSet>
+  auto buildModelGT(DataSet& dataset) -> decltype(dataset.image.depth.data(), void()) {
+    check_frame(dataset.image, "builder::buildModelGT");
+    if (dataset.groundTruthLine.size() < 8)
+      dyn_throw("builder::buildModelGT: the frame has no ground truth", DYN_ERR_INVALID_ARG);
+    buildModelGT(dataset.image.depth.data(),
+                 dataset.image.rgb.empty() ? nullptr : dataset.image.rgb.data(),
+                 v2tRef(dataset.groundTruthLine));
   }
 
   // builder.cu:140-160: integrate at a known pose (no tracking)
@@ -119,6 +139,13 @@ class builder {
   }
 
  private:
+  template <class Frame>
+  void check_frame(const Frame& f, const char* what) const {
+    const size_t n = (size_t)sensor.rows * sensor.cols;
+    if ((size_t)f.rows != (size_t)sensor.rows || (size_t)f.cols != (size_t)sensor.cols ||
+        f.depth.size() != n || (!f.rgb.empty() && f.rgb.size() != 3 * n))
+      dyn_throw(what, DYN_ERR_INVALID_ARG);
+  }
   void ensure(int mode) {
     if (session_) {
       if (mode != mode_) dyn_throw("builder: Mode changed after the first frame", DYN_ERR_INVALID_ARG);
