@@ -566,27 +566,8 @@ struct BlockCache {
   int ptr;
 };
 
-// WorldToGlobalVoxelHashing for one axis (tsdf.cu:189-193): the voxel index
-// g = (int)(fl(p / vs) + sign(p) * 0.5), exactly.  Fast path: t = p * (1/vs)
-// + sign * 0.5 differs from the exactly rounded sum by at most 4 ulps (the
-// reciprocal, the product and the quotient each round once), so whenever t
-// is more than 2^-19 (|t| + 1) (>= 16 ulps) away from every integer,
-// truncating t gives the same integer; otherwise the IEEE division decides.
-// copysign(0.5, p) is sign(p) * 0.5 for p != 0; for p = +-0 the fast path
-// sees t = +-0.5, which truncates to the reference's 0; NaN and infinite t
-// fail the test and take the reference's expression.
-__device__ inline int voxel_index(float p, float vs, float inv_vs) {
-  const float t = __fadd_rn(__fmul_rn(p, inv_vs), copysignf(0.5f, p));
-  const float n = rintf(t);
-  if (fabsf(t - n) > __fmaf_rn(fabsf(t), 1.9073486328125e-6f, 1.9073486328125e-6f))
-    return (int)t;
-  const float sg = (float)((p > 0.0f) - (p < 0.0f));
-  return (int)(p / vs + sg * 0.5f);
-}
-// WorldToBlock / WorldToLocalVoxel (tsdf.cu:195-225) for block size 8: the
-// reference's floor division and non-negative remainder are g >> 3, g & 7.
-__device__ inline int blk_of(int g) { return g >> 3; }
-__device__ inline int loc_of(int g) { return g & 7; }
+// voxel_index, blk_of and loc_of (WorldToGlobalVoxelHashing / WorldToBlock /
+// WorldToLocalVoxel) are in common.cuh.
 
 // tsdfVolume::GetVoxel, tsdf.cu:227-239, for a voxel already resolved to
 // (block, local index); a one-block lookup cache skips repeated bucket

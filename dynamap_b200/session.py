@@ -158,6 +158,22 @@ class Session:
         """(coords (n,3) int32, rgbw (n,512,4) uint8, sdf (n,512) float32)."""
         return _download_blocks(self.lib, self.h)
 
+    def extract_mesh(self, lower, upper, capacity: int | None = None) -> np.ndarray:
+        """Triangles [n, 3, 6] ({x, y, z, r, g, b} per vertex, colour 0..1)
+        of the model over the box between lower and upper
+        (tsdfVolume::ExtractMesh); with no capacity, counted first."""
+        lo = (C.c_float * 3)(*[float(x) for x in lower])
+        hi = (C.c_float * 3)(*[float(x) for x in upper])
+        n = C.c_int64()
+        if capacity is None:
+            abi.check("dyn_extract_mesh",
+                      self.lib.dyn_extract_mesh(self.h, lo, hi, None, 0, C.byref(n)))
+            capacity = n.value
+        out = np.zeros((capacity, 3, 6), np.float32)
+        abi.check("dyn_extract_mesh",
+                  self.lib.dyn_extract_mesh(self.h, lo, hi, _ptr(out), capacity, C.byref(n)))
+        return out[:min(n.value, capacity)]
+
     def image(self, which: int, level: int, shape, dtype) -> np.ndarray:
         out = np.empty(shape, dtype)
         abi.check("dyn_debug_image",

@@ -116,6 +116,14 @@ class builder {
     return c;
   }
 
+  // builder.cu:66-69: the mesh of the box between the corners
+  geometry::Mesh ExtractMesh(const geometry::float3_& lower_corner,
+                             const geometry::float3_& upper_corner) {
+    const float lo[3] = {lower_corner.x, lower_corner.y, lower_corner.z};
+    const float hi[3] = {upper_corner.x, upper_corner.y, upper_corner.z};
+    return geometry::ExtractMesh(session_, lo, hi);
+  }
+
   dyn_session* session() const { return session_; }
 
   // builder.cu:222-241: a TUM ground-truth line {stamp, tx, ty, tz, qx, qy,

@@ -267,6 +267,21 @@ dyn_status dyn_download_blocks(dyn_session* s, int32_t* coords_out,
                                dyn_voxel* voxels_out, int64_t capacity,
                                int64_t* n_out);
 
+/* Triangle mesh of the volume over the box between 'lower' and 'upper'
+ * (tsdfVolume::ExtractMesh, tsdf.cu:551-560; MeshExtractor::ExtractMesh,
+ * meshExtractor.cu:364-407): the reference's cells (|upper - lower| / vs * 2
+ * per axis from 'lower', corners at +-vs/2, each sampled by trilinear
+ * interpolation that gives up at an unobserved voxel), vertices by its edge
+ * interpolation coloured by the cell's centre voxel, triangles from a
+ * generated marching-cubes table.  18 floats per triangle: three vertices
+ * {x, y, z, r, g, b}, colour in 0..1.  *n_out = the number of triangles;
+ * min(*n_out, capacity) are written, in a fixed order (allocated blocks in
+ * heap order, cells x-fastest within a block).  triangles_host may be NULL
+ * (count only).  Synchronous.  DYN_ERR_INVALID_ARG for a box that is not
+ * finite or has 2^24 or more cells along an axis. */
+dyn_status dyn_extract_mesh(dyn_session* s, const float lower[3], const float upper[3],
+                            float* triangles_host, int64_t capacity, int64_t* n_out);
+
 /* Internal images of the last frame, for inspection and parity tests.
  * which: 0 raw depth (f32, level 0), 1 filtered depth (f32, level 0),
  *        2 source depth pyramid level L (f32), 3 source vertices level L

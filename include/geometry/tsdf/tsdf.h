@@ -16,6 +16,7 @@
 #include "../../dynamap.h"
 #include "../../dynamap/types.h"
 #include "../../image/sensor/rgbdImage.h"
+#include "../mesh/mesh.h"
 
 namespace DynaMap {
 namespace tsdf {
@@ -98,6 +99,14 @@ class tsdfVolume {
     dyn_throw("tsdfVolume::GenerateRgb",
               dyn_raycast(session_, camera_pose.entries, &s, d.data(), c.data()));
     return c;
+  }
+
+  // tsdf.cu:551-560: the mesh of the box between the corners
+  geometry::Mesh ExtractMesh(const geometry::float3_& lower_corner,
+                             const geometry::float3_& upper_corner) {
+    const float lo[3] = {lower_corner.x, lower_corner.y, lower_corner.z};
+    const float hi[3] = {upper_corner.x, upper_corner.y, upper_corner.z};
+    return geometry::ExtractMesh(session_, lo, hi);
   }
 
   // HashTable::GetNumAllocatedBlocks, hashTable.cu:165

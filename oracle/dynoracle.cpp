@@ -1293,6 +1293,28 @@ static int64_t download(Volume<R>& V, int32_t* coords, uint8_t* rgbw, R* sdf,
   }
   return V.nalloc;
 }
+// The inverse of download for FP32 volumes: each block allocated in turn
+// (heap indices follow the order given) and its voxels set.  Returns the
+// blocks placed; stops at the first that does not fit.
+static int64_t upload(Volume<float>& V, const int32_t* coords, const uint8_t* rgbw,
+                      const float* sdf, int64_t n) {
+  const int bs3 = V.p.block_size * V.p.block_size * V.p.block_size;
+  for (int64_t b = 0; b < n; ++b) {
+    const int x = coords[3 * b], y = coords[3 * b + 1], z = coords[3 * b + 2];
+    if (V.allocate(x, y, z) < 0) return b;
+    const int ptr = V.find(x, y, z);
+    for (int k = 0; k < bs3; ++k) {
+      Voxel<float>& vx = V.vox[(size_t)ptr * bs3 + k];
+      const uint8_t* c = rgbw + 4 * ((size_t)b * bs3 + k);
+      vx.c[0] = c[0];
+      vx.c[1] = c[1];
+      vx.c[2] = c[2];
+      vx.w = c[3];
+      vx.sdf = sdf[(size_t)b * bs3 + k];
+    }
+  }
+  return n;
+}
 }  // namespace
 
 extern "C" {
@@ -1471,6 +1493,13 @@ int64_t dyo_volume_download(void* v, int32_t* coords, uint8_t* rgbw,
   if (a->fp64)
     return download(*(Volume<double>*)a->v, coords, rgbw, (double*)sdf_out, cap);
   return download(*(Volume<float>*)a->v, coords, rgbw, (float*)sdf_out, cap);
+}
+
+int64_t dyo_volume_upload(void* v, const int32_t* coords, const uint8_t* rgbw,
+                          const float* sdf, int64_t n) {
+  AnyVolume* a = (AnyVolume*)v;
+  if (a->fp64) return -1;
+  return upload(*(Volume<float>*)a->v, coords, rgbw, sdf, n);
 }
 
 void* dyo_session_create(const dyn_tsdf_params* t, const dyn_gn_params* g,

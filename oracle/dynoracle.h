@@ -120,6 +120,11 @@ int64_t dyo_mesh_triangles(void* v, const float lo[3], const float hi[3], float*
  * x-major order.  Any output may be NULL. */
 int64_t dyo_volume_download(void* v, int32_t* coords, uint8_t* rgbw,
                             void* sdf_out, int64_t capacity);
+/* The inverse for FP32 volumes: blocks allocated in the order given, voxels
+ * set (rgbw and sdf as dyo_volume_download writes them).  Returns the blocks
+ * placed (fewer when one does not fit), -1 for an FP64 volume. */
+int64_t dyo_volume_upload(void* v, const int32_t* coords, const uint8_t* rgbw,
+                          const float* sdf, int64_t n);
 
 /* ---- full per-frame pipeline (builder::buildModelLS with fixes) ---- */
 void* dyo_session_create(const dyn_tsdf_params* t, const dyn_gn_params* g,

@@ -67,6 +67,7 @@ def lib() -> C.CDLL:
             "dyo_mesh_vertices": (C.c_int64, [_vp, P(C.c_float), P(C.c_float), _vp, C.c_int64]),
             "dyo_mesh_triangles": (C.c_int64, [_vp, P(C.c_float), P(C.c_float), _vp, C.c_int64]),
             "dyo_volume_download": (C.c_int64, [_vp, _vp, _vp, _vp, C.c_int64]),
+            "dyo_volume_upload": (C.c_int64, [_vp, _vp, _vp, _vp, C.c_int64]),
             "dyo_session_create": (_vp, [P(abi.TsdfParams), P(abi.GnParams),
                                          P(abi.BilateralParams), P(abi.Sensor), C.c_int32]),
             "dyo_session_destroy": (None, [_vp]),
@@ -280,6 +281,16 @@ class Volume:
 
     def num_blocks(self) -> int:
         return int(lib().dyo_volume_num_blocks(self.h))
+
+    def upload(self, coords, rgbw, sdf) -> int:
+        """Blocks [n, 3] with voxels rgbw [n, 512, 4] u8 and sdf [n, 512]
+        (FP32 volumes); returns the blocks placed."""
+        coords = np.ascontiguousarray(coords, np.int32)
+        rgbw = np.ascontiguousarray(rgbw, np.uint8)
+        sdf = np.ascontiguousarray(sdf, np.float32)
+        n = len(coords)
+        assert rgbw.shape == (n, 512, 4) and sdf.shape == (n, 512)
+        return int(lib().dyo_volume_upload(self.h, ptr(coords), ptr(rgbw), ptr(sdf), n))
 
     def download(self):
         n = self.num_blocks()

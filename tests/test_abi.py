@@ -151,3 +151,13 @@ def test_session_bytes_follow_the_voxel_form():
     assert n32.value - n16.value == 0
     assert n32.value > vox * 8
     assert lib.dyn_session_bytes(C.byref(t), C.byref(s), 0, None) == 1
+
+
+def test_extract_mesh_validates_before_touching_a_device():
+    lib = abi.load()
+    lo = (C.c_float * 3)(0.0, 0.0, 0.0)
+    hi = (C.c_float * 3)(1.0, 1.0, 1.0)
+    n = C.c_int64(-7)
+    assert lib.dyn_extract_mesh(None, lo, hi, None, 0, C.byref(n)) == 1
+    assert lib.dyn_extract_mesh(None, lo, hi, None, -1, C.byref(n)) == 1
+    assert lib.dyn_extract_mesh(None, None, hi, None, 0, C.byref(n)) == 1

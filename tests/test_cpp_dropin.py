@@ -26,7 +26,8 @@ def test_dropin_headers_compile_and_link(tmp_path):
     compile_example(str(tmp_path / "dropin"))
     # every header is self-contained
     for h in ("builder/builder.h", "geometry/tsdf/tsdf.h", "solver/gnSolver/gnSolver.h",
-              "image/sensor/rgbdImage.h", "dynamap/types.h", "dynamap/pose_io.h", "utils/dataSet.h", "dynamap.h"):
+              "image/sensor/rgbdImage.h", "dynamap/types.h", "dynamap/pose_io.h", "utils/dataSet.h", "geometry/mesh/mesh.h",
+              "dynamap.h"):
         src = tmp_path / "inc.cpp"
         src.write_text(f'#include "{h}"\nint main() {{ return 0; }}\n')
         subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-I", os.path.join(ROOT, "include"),
