@@ -10,6 +10,15 @@ if ROOT not in sys.path:
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and libdynamap_b200.so")
+    config.addinivalue_line(
+        "markers", "first_b200_run: GPU tests of code that has not yet passed on a B200")
+
+
+def pytest_collection_modifyitems(config, items):
+    """Tests of code not yet run on a B200 go after all others, so that
+    under -x a failure there cannot hide the results of the established
+    tests."""
+    items.sort(key=lambda it: it.get_closest_marker("first_b200_run") is not None)
 
 
 @pytest.fixture(scope="session")
