@@ -123,6 +123,9 @@ SIGNATURES = {
     "dyn_download_blocks": (C.c_int, [_vp, _vp, _vp, C.c_int64, P(C.c_int64)]),
     "dyn_extract_mesh": (C.c_int, [_vp, P(C.c_float), P(C.c_float), _vp, C.c_int64,
                                    P(C.c_int64)]),
+    "dyn_evict_blocks": (C.c_int, [_vp, C.c_int32, _vp, _vp, C.c_int64, P(C.c_int64)]),
+    "dyn_delete_blocks": (C.c_int, [_vp, _vp, C.c_int64, _vp, _vp, C.c_int64, P(C.c_int64)]),
+    "dyn_upload_blocks": (C.c_int, [_vp, _vp, _vp, C.c_int64, P(C.c_int64)]),
     "dyn_debug_image": (C.c_int, [_vp, C.c_int32, C.c_int32, _vp, C.c_size_t]),
     "dyn_bilateral_filter": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint32, P(BilateralParams), _vp]),
     "dyn_depth_to_maps": (C.c_int, [_vp, P(Sensor), _vp, _vp, _vp]),

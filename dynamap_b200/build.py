@@ -20,9 +20,9 @@ LIB = os.path.join(HERE, "libdynamap_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 SOURCES = ["image.cu", "icp.cu", "tsdf.cu", "session.cu", "serving.cu", "noalloc.cu",
-           "mesh.cu", "config.cpp"]
+           "mesh.cu", "evict.cu", "config.cpp"]
 HEADERS = ["common.cuh", "image.cuh", "icp.cuh", "tsdf.cuh", "sessdev.cuh", "session_impl.cuh",
-           "dyn_exp.h", "mesh_cell.h", "mc_tables.h"]
+           "dyn_exp.h", "mesh_cell.h", "mc_tables.h", "evict_ops.h"]
 
 # -fmad=false: no FMA contraction, IEEE div/sqrt: every float operation
 # rounds once, in source order (the bit-exact parity with the oracle relies

@@ -299,6 +299,9 @@ struct Marks {
 
 void release(dyn_session* s);
 void release(dyn_batch* b);
+// Session calls that read device state wait for the batch or server that
+// runs its frames.
+dyn_status quiesce(dyn_session* s);
 // The launch shape of a table of sessions (the largest member bounds every
 // grid).
 BatchShape make_shape(dyn_session* const* ss, int n, int2* gvis, int* gcount, int gvis_cap);

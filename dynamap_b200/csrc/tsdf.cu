@@ -41,37 +41,7 @@ struct AllocSmem {
   int new_blocks, bucket_full, heap_exhausted, unique, overruns;
 };
 
-// Lock-free unique insert into the key's bucket (the set semantics of
-// HashTable::AllocateBlock, hashTable.cu:80-110, without its duplicate-
-// insert race): scan the bucket in slot order, claim the first empty slot by
-// CAS on the key; a lost CAS re-reads the slot.  Slots are claimed in order
-// and never freed, so occupied slots form a prefix of the bucket.  Returns
-// the entry index if this call claimed it (heap index assigned later), -1
-// if the key was present, -2 if the bucket is full.
-__device__ inline int bucket_insert(Entry* entries, const DTsdf& t, unsigned long long key,
-                                    int stamp, int* unique) {
-  int b = hash_slot(key_x(key), key_y(key), key_z(key), t);
-  for (int i = 0; i < t.bucket_size; ++i) {
-    Entry* e = entries + b + i;
-    unsigned long long cur = *(volatile unsigned long long*)&e->key;
-    if (cur == kEmptyKey) {
-      cur = atomicCAS(&e->key, kEmptyKey, key);
-      if (cur == kEmptyKey) {
-        atomicExch(&e->stamp, stamp);
-        atomicAdd(unique, 1);
-        return b + i;
-      }
-    }
-    if (cur == key) {
-      // stamps only move forward to this frame's, so a stamp that already
-      // reads 'stamp' was counted by another ray: skip the contended atomic
-      if (*(volatile int*)&e->stamp != stamp && atomicExch(&e->stamp, stamp) != stamp)
-        atomicAdd(unique, 1);
-      return -1;
-    }
-  }
-  return -2;
-}
+// bucket_insert (the lock-free unique insert) is in common.cuh.
 
 // AllocateFromDepthKernel (tsdf.cu:346-453) for one pixel: the reference's
 // DDA over blocks, exact FP32 (this file is built with -fmad=false), with

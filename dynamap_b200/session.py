@@ -158,6 +158,43 @@ class Session:
         """(coords (n,3) int32, rgbw (n,512,4) uint8, sdf (n,512) float32)."""
         return _download_blocks(self.lib, self.h)
 
+    def _removed(self, fn, args, out: bool):
+        n = self.num_blocks()
+        coords = np.empty((n, 3), np.int32) if out else None
+        vox = np.empty((n, 512, 2), np.uint32) if out else None
+        k = C.c_int64()
+        abi.check(fn, getattr(self.lib, fn)(self.h, *args, _ptr(coords), _ptr(vox),
+                                             n if out else 0, C.byref(k)))
+        if not out:
+            return k.value
+        m = min(k.value, n)
+        rgbw = vox[:m, :, 0].copy().view(np.uint8).reshape(m, 512, 4)
+        return coords[:m], rgbw, vox[:m, :, 1].copy().view(np.float32)
+
+    def evict_blocks(self, max_age: int, out: bool = True):
+        """Remove the blocks the allocation has not touched in the last
+        max_age + 1 frames; with 'out', returns them as download_blocks
+        does (heap order), else their count."""
+        return self._removed("dyn_evict_blocks", (int(max_age),), out)
+
+    def delete_blocks(self, coords, out: bool = True):
+        """Remove the blocks at the given block coordinates [m, 3]."""
+        c = np.ascontiguousarray(coords, np.int32).reshape(-1, 3)
+        return self._removed("dyn_delete_blocks", (_ptr(c), len(c)), out)
+
+    def upload_blocks(self, coords, rgbw, sdf) -> np.ndarray:
+        """Put blocks (as download_blocks returns them) into the volume;
+        returns [placed, already present, bucket full, heap exhausted]."""
+        c = np.ascontiguousarray(coords, np.int32).reshape(-1, 3)
+        n = len(c)
+        vox = np.empty((n, 512, 2), np.uint32)
+        vox[..., 0] = np.ascontiguousarray(rgbw, np.uint8).reshape(n, 512, 4).view(np.uint32)[..., 0]
+        vox[..., 1] = np.ascontiguousarray(sdf, np.float32).reshape(n, 512).view(np.uint32)
+        counts = np.zeros(4, np.int64)
+        abi.check("dyn_upload_blocks", self.lib.dyn_upload_blocks(
+            self.h, _ptr(c), _ptr(vox), n, counts.ctypes.data_as(C.POINTER(C.c_int64))))
+        return counts
+
     def extract_mesh(self, lower, upper, capacity: int | None = None) -> np.ndarray:
         """Triangles [n, 3, 6] ({x, y, z, r, g, b} per vertex, colour 0..1)
         of the model over the box between lower and upper

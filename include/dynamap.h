@@ -282,6 +282,36 @@ dyn_status dyn_download_blocks(dyn_session* s, int32_t* coords_out,
 dyn_status dyn_extract_mesh(dyn_session* s, const float lower[3], const float upper[3],
                             float* triangles_host, int64_t capacity, int64_t* n_out);
 
+/* ---- block eviction and streaming ----------------------------------------
+ * The reference has HashTable::DeleteBlock (hashTable.cu:112-134) but never
+ * calls it; these remove blocks between frames so that a session stays
+ * inside its memory, can hand them to the host first, and put blocks back.
+ * Removal keeps the heap dense (survivors move into the freed slots, the
+ * rest is cleared), so dyn_download_blocks afterwards lists exactly the
+ * survivors and the next frames allocate from the freed space.  The
+ * removed blocks' coordinates and voxels (the 8-byte form of
+ * dyn_download_blocks) go to coords_out / voxels_out (either may be NULL),
+ * at most 'capacity' of them, in heap order; *n_out = the blocks removed.
+ * Synchronous; not for a session whose frames a batch or server is running
+ * at the same time. */
+/* Blocks the allocation has not touched in the last frame or the
+ * max_age_frames frames before it (0: keep only the last frame's). */
+dyn_status dyn_evict_blocks(dyn_session* s, int32_t max_age_frames, int32_t* coords_out,
+                            dyn_voxel* voxels_out, int64_t capacity, int64_t* n_out);
+/* The blocks at n_coords block coordinates (coords[3*i..]); coordinates
+ * without a block are ignored, repeats count once. */
+dyn_status dyn_delete_blocks(dyn_session* s, const int32_t* coords, int64_t n_coords,
+                             int32_t* coords_out, dyn_voxel* voxels_out, int64_t capacity,
+                             int64_t* n_out);
+/* n blocks (coordinates, 512 voxels each in the 8-byte form) into the
+ * volume, as touched by the last frame; a block whose key is present is
+ * left as it is.  counts_out = {placed, already present, bucket full, heap
+ * exhausted}.  The mixed form stores sdf / truncation as f16 and the weight
+ * as u16 (the round trip through dyn_download_blocks is exact for weights
+ * up to 255). */
+dyn_status dyn_upload_blocks(dyn_session* s, const int32_t* coords, const dyn_voxel* voxels,
+                             int64_t n, int64_t counts_out[4]);
+
 /* Internal images of the last frame, for inspection and parity tests.
  * which: 0 raw depth (f32, level 0), 1 filtered depth (f32, level 0),
  *        2 source depth pyramid level L (f32), 3 source vertices level L

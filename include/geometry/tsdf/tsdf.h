@@ -124,9 +124,54 @@ class tsdfVolume {
               dyn_download_blocks(session_, coords.data(), voxels.data(), n, &got));
   }
 
+  // HashTable::DeleteBlock (hashTable.cu:112-134) for many blocks at once,
+  // and its use for a memory budget: the blocks at 'coords' (x, y, z per
+  // block), or those the allocation has not touched in the last maxAge + 1
+  // frames, are removed; their coordinates and voxels are returned (heap
+  // order) for UploadBlocks to bring back.
+  int64_t DeleteBlocks(const std::vector<int32_t>& coords, std::vector<int32_t>* removedCoords,
+                       std::vector<dyn_voxel>* removedVoxels) {
+    return removed("tsdfVolume::DeleteBlocks", removedCoords, removedVoxels,
+                   [&](int32_t* c, dyn_voxel* v, int64_t cap, int64_t* n) {
+                     return dyn_delete_blocks(session_, coords.data(),
+                                              (int64_t)(coords.size() / 3), c, v, cap, n);
+                   });
+  }
+  int64_t EvictBlocks(int maxAge, std::vector<int32_t>* removedCoords,
+                      std::vector<dyn_voxel>* removedVoxels) {
+    return removed("tsdfVolume::EvictBlocks", removedCoords, removedVoxels,
+                   [&](int32_t* c, dyn_voxel* v, int64_t cap, int64_t* n) {
+                     return dyn_evict_blocks(session_, maxAge, c, v, cap, n);
+                   });
+  }
+  // blocks placed (keys already present are left as they are)
+  int64_t UploadBlocks(const std::vector<int32_t>& coords, const std::vector<dyn_voxel>& voxels) {
+    int64_t counts[4] = {0, 0, 0, 0};
+    const int64_t n = (int64_t)(coords.size() / 3);
+    if ((int64_t)voxels.size() < n * 512) dyn_throw("tsdfVolume::UploadBlocks", DYN_ERR_INVALID_ARG);
+    dyn_throw("tsdfVolume::UploadBlocks",
+              dyn_upload_blocks(session_, coords.data(), voxels.data(), n, counts));
+    return counts[0];
+  }
+
   dyn_session* session() const { return session_; }
 
  private:
+  template <class F>
+  int64_t removed(const char* what, std::vector<int32_t>* coords, std::vector<dyn_voxel>* voxels,
+                  F call) {
+    const int64_t cap = (coords || voxels) ? GetNumAllocatedBlocks() : 0;
+    if (coords) coords->resize((size_t)cap * 3);
+    if (voxels) voxels->resize((size_t)cap * 512);
+    int64_t n = 0;
+    dyn_throw(what, call(coords ? coords->data() : nullptr, voxels ? voxels->data() : nullptr,
+                         cap, &n));
+    const int64_t m = n < cap ? n : cap;
+    if (coords) coords->resize((size_t)m * 3);
+    if (voxels) voxels->resize((size_t)m * 512);
+    return n;
+  }
+
   dyn_session* session_ = nullptr;
   rgbdSensor sensor_;
 };

@@ -161,3 +161,12 @@ def test_extract_mesh_validates_before_touching_a_device():
     assert lib.dyn_extract_mesh(None, lo, hi, None, 0, C.byref(n)) == 1
     assert lib.dyn_extract_mesh(None, lo, hi, None, -1, C.byref(n)) == 1
     assert lib.dyn_extract_mesh(None, None, hi, None, 0, C.byref(n)) == 1
+
+
+def test_eviction_entries_validate_before_touching_a_device():
+    lib = abi.load()
+    n = C.c_int64(-7)
+    counts = (C.c_int64 * 4)()
+    assert lib.dyn_evict_blocks(None, 3, None, None, 0, C.byref(n)) == 1
+    assert lib.dyn_delete_blocks(None, None, 0, None, None, 0, C.byref(n)) == 1
+    assert lib.dyn_upload_blocks(None, None, None, 0, counts) == 1
