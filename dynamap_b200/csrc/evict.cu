@@ -303,7 +303,7 @@ dyn_status remove_blocks(dyn_session* s, Mark mark, int32_t* coords_out, dyn_vox
       e = cudaMemsetAsync(s->vol.colors + from, 0, sizeof(uchar4) * tail, st);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(&s->vol.cnt->nalloc, &L, sizeof(int), cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // L lives on this frame
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // the copy reads L from this stack
     if (e != cudaSuccess) r = DYN_ERR_CUDA;
   } while (false);
   if (r != DYN_OK) cudaGetLastError();
