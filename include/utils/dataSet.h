@@ -257,18 +257,19 @@ class dataSet {
           image.rgb[3 * i + k] = c.data[i * c.channels + (c.channels == 1 ? 0 : k)];
     }
   }
-  // the ground-truth line nearest in time to the frame (within 0.02 s)
+  // the ground-truth line nearest in time to the frame (within 0.02 s; the
+  // earlier line on a tie)
   void invokeNextGroundTruthLine() {
     groundTruthLine.clear();
+    if (gt_.size() != refLines.size()) parse_ground_truth();
+    auto it = std::lower_bound(gt_order_.begin(), gt_order_.end(), stamp,
+                               [&](size_t i, double t) { return gt_[i][0] < t; });
     double best = 0.02;
-    for (const std::string& ln : refLines) {
-      std::istringstream ss(ln);
-      std::vector<double> v;
-      double x;
-      while (ss >> x) v.push_back(x);
-      if (v.size() < 8) continue;
+    for (auto c : {it - (it != gt_order_.begin() ? 1 : 0), it}) {
+      if (c == gt_order_.end()) continue;
+      const std::vector<double>& v = gt_[*c];
       const double dt = std::fabs(v[0] - stamp);
-      if (dt < best) {
+      if (dt < best || (dt == best && !groundTruthLine.empty() && v[0] < groundTruthLine[0])) {
         best = dt;
         groundTruthLine = v;
       }
@@ -290,6 +291,22 @@ class dataSet {
   }
 
  private:
+  // refLines parsed once: the lines with 8 values, ordered by time stamp
+  void parse_ground_truth() {
+    gt_.assign(refLines.size(), std::vector<double>());
+    gt_order_.clear();
+    for (size_t i = 0; i < refLines.size(); ++i) {
+      std::istringstream ss(refLines[i]);
+      double x;
+      while (ss >> x) gt_[i].push_back(x);
+      if (gt_[i].size() >= 8) gt_order_.push_back(i);
+    }
+    std::stable_sort(gt_order_.begin(), gt_order_.end(),
+                     [&](size_t a, size_t b) { return gt_[a][0] < gt_[b][0]; });
+  }
+
+  std::vector<std::vector<double>> gt_;
+  std::vector<size_t> gt_order_;
   std::string mainDir_;
   static double file_stamp(const std::string& path) {
     return std::strtod(std::filesystem::path(path).stem().string().c_str(), nullptr);
