@@ -22,7 +22,8 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 SOURCES = ["image.cu", "icp.cu", "tsdf.cu", "session.cu", "serving.cu", "noalloc.cu",
            "mesh.cu", "evict.cu", "config.cpp"]
 HEADERS = ["common.cuh", "image.cuh", "icp.cuh", "tsdf.cuh", "sessdev.cuh", "session_impl.cuh",
-           "dyn_exp.h", "mesh_cell.h", "mc_tables.h", "evict_ops.h"]
+           "dyn_exp.h", "mesh_cell.h", "mc_tables.h", "evict_ops.h", "mesh_kernels.cuh",
+           "evict_kernels.cuh"]
 
 # -fmad=false: no FMA contraction, IEEE div/sqrt: every float operation
 # rounds once, in source order (the bit-exact parity with the oracle relies

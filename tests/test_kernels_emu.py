@@ -1,0 +1,174 @@
+"""The mesh-extraction and eviction kernels themselves
+(dynamap_b200/csrc/{mesh,evict}_kernels.cuh), run on the CPU under a
+thread-block emulation (tests/cpp/cuda_emu.h: one host thread per CUDA
+thread, barriers for __syncthreads, a per-warp exchange for shuffles), in
+the launch order of the library's entry points, on volumes built by the
+library's own upload kernel in both voxel forms: the mesh equals the host
+build of the same walk in content and order, and eviction leaves the same
+volume and hands out the same blocks as the host build of the same steps.
+This covers what the host builds do not: the two-pass mesh output with its
+scans and offsets, the shared-memory tile, and the kernels' indexing."""
+import ctypes as C
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+from meshutil import build_mesh_host, sphere_volume
+from test_evict_host import Host, blocks, lib as evict_lib  # noqa: F401 (fixture)
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CUDA_INC = "/usr/local/cuda/include"
+
+
+@pytest.fixture(scope="module")
+def emu(tmp_path_factory):
+    cxx = shutil.which("g++")
+    if cxx is None or not os.path.exists(os.path.join(CUDA_INC, "cuda_fp16.h")):
+        pytest.skip("no C++ compiler or CUDA headers")
+    so = str(tmp_path_factory.mktemp("emu") / "libkernels_emu.so")
+    subprocess.run([cxx, "-std=c++20", "-O1", "-fPIC", "-shared", "-ffp-contract=off",
+                    "-I", CUDA_INC, os.path.join(HERE, "cpp", "kernels_emu.cpp"), "-o", so,
+                    "-pthread"], check=True)
+    L = C.CDLL(so)
+    vp, i64, i32, f32 = C.c_void_p, C.c_int64, C.c_int, C.c_float
+    L.emu_volume.restype = vp
+    L.emu_volume.argtypes = [f32, f32, i32, i32, i32, i32]
+    L.emu_volume_free.argtypes = [vp]
+    L.emu_nalloc.argtypes = [vp]
+    L.emu_upload.argtypes = [vp, vp, vp, vp, i64, vp]
+    L.emu_download.restype = i64
+    L.emu_download.argtypes = [vp, vp, vp]
+    L.emu_mesh.restype = i64
+    L.emu_mesh.argtypes = [vp, C.POINTER(f32), C.POINTER(f32), vp, i64]
+    L.emu_remove.restype = i64
+    L.emu_remove.argtypes = [vp, i32, i32, i32, vp, i64, vp, vp, i64]
+    L.emu_find.argtypes = [vp, i32, i32, i32]
+    return L
+
+
+@pytest.fixture(scope="module")
+def mesh_host(tmp_path_factory):
+    f = build_mesh_host(tmp_path_factory.mktemp("mesh"))
+    if f is None:
+        pytest.skip("no C++ compiler")
+    return f
+
+
+class EmuVolume:
+    def __init__(self, L, vs, trunc, nb, bsz, num_blocks, fp16):
+        self.L = L
+        self.h = L.emu_volume(vs, trunc, nb, bsz, num_blocks, int(fp16))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.emu_volume_free(self.h)
+
+    def upload(self, coords, vox8, stamps=None):
+        coords = np.ascontiguousarray(coords, np.int32)
+        vox8 = np.ascontiguousarray(vox8, np.uint8)
+        st = None if stamps is None else np.ascontiguousarray(stamps, np.int32)
+        c = np.zeros(4, np.int64)
+        self.L.emu_upload(self.h, coords.ctypes.data, vox8.ctypes.data,
+                          None if st is None else st.ctypes.data, len(coords), c.ctypes.data)
+        return c
+
+    def download(self):
+        n = self.L.emu_nalloc(self.h)
+        c = np.zeros((n, 3), np.int32)
+        v = np.zeros((n, 512, 8), np.uint8)
+        assert self.L.emu_download(self.h, c.ctypes.data, v.ctypes.data) == n
+        return c, v
+
+    def mesh(self, lo, hi, cap=200000):
+        lo_c = (C.c_float * 3)(*[float(x) for x in lo])
+        hi_c = (C.c_float * 3)(*[float(x) for x in hi])
+        out = np.zeros((cap, 3, 6), np.float32)
+        n = self.L.emu_mesh(self.h, lo_c, hi_c, out.ctypes.data, cap)
+        assert 0 <= n <= cap
+        return out[:n]
+
+    def remove(self, mode, last=0, max_age=0, coords=None):
+        n = self.L.emu_nalloc(self.h)
+        d = np.ascontiguousarray(coords if coords is not None else np.zeros((0, 3)), np.int32)
+        oc = np.zeros((n, 3), np.int32)
+        ov = np.zeros((n, 512, 8), np.uint8)
+        k = self.L.emu_remove(self.h, mode, last, max_age, d.ctypes.data, len(d),
+                              oc.ctypes.data, ov.ctypes.data, n)
+        assert k >= 0
+        return k, oc[:k], ov[:k]
+
+
+def vox8_of(rgbw, sdf):
+    v = np.zeros(rgbw.shape[:2] + (8,), np.uint8)
+    v[..., :4] = rgbw
+    v[..., 4:] = np.ascontiguousarray(sdf, np.float32)[..., None].view(np.uint8)
+    return v
+
+
+def split8(v8):
+    return v8[..., :4], np.ascontiguousarray(v8[..., 4:]).view(np.float32)[..., 0]
+
+
+@pytest.mark.parametrize("fp16", [False, True])
+def test_mesh_kernels_match_host_walk(emu, mesh_host, fp16):
+    vs = 0.01
+    coords, rgbw, sdf = sphere_volume(7, vs=vs, radius=0.12)
+    vol = EmuVolume(emu, vs, 0.04, 1 << 12, 10, len(coords) + 8, fp16)
+    assert list(vol.upload(coords, vox8_of(rgbw, sdf))) == [len(coords), 0, 0, 0]
+    hc, hv = vol.download()  # heap order; f16-rounded sdf in the mixed form
+    h_rgbw, h_sdf = split8(hv)
+    rng = np.random.default_rng(8)
+    boxes = [np.array([[-0.12, -0.27, 0.13], [0.22, 0.07, 0.47]], np.float32)]
+    lo = np.array([-0.05, -0.2, 0.2]) + rng.uniform(-0.03, 0.03, 3)
+    boxes.append(np.array([lo, lo + 0.12], np.float32))
+    for lo, hi in boxes:
+        got = vol.mesh(lo, hi)
+        want = mesh_host(hc, h_rgbw, h_sdf, vs, lo, hi)
+        assert len(got) > 200
+        np.testing.assert_array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+@pytest.mark.parametrize("fp16", [False, True])
+def test_evict_kernels_match_host_build(emu, evict_lib, fp16):  # noqa: F811
+    coords, vox = blocks(11, 260)
+    vox[..., 4:] = np.random.default_rng(12).uniform(-0.03, 0.03, (260, 512, 1)).astype(
+        np.float32).view(np.uint8)  # sdf values of a TSDF
+    vox[..., 3] = np.minimum(vox[..., 3], 200)
+    stamps = np.random.default_rng(13).integers(1, 30, 260).astype(np.int32)
+    vol = EmuVolume(emu, 0.01, 0.04, 257, 6, 300, fp16)
+    counts = vol.upload(coords, vox, stamps)
+    assert counts[0] + counts[2] == 260
+    hc, hv = vol.download()
+    st = dict(zip(map(tuple, coords.tolist()), stamps.tolist()))
+    hst = np.array([st[tuple(c)] for c in hc.tolist()], np.int32)
+    host = Host(evict_lib, 257, 6, 300)
+    assert host.insert(hc, hv, hst)[0] == len(hc)
+    # by age, then by coordinate (with repeats and absent ones)
+    for step in range(2):
+        if step == 0:
+            k1, c1, v1 = vol.remove(0, last=29, max_age=9)
+            k2, c2, v2 = host.remove(0, last=29, max_age=9)
+        else:
+            cur = vol.download()[0]
+            dels = np.concatenate([cur[::3], cur[:4], [[500, 500, 500]]]).astype(np.int32)
+            k1, c1, v1 = vol.remove(1, coords=dels)
+            k2, c2, v2 = host.remove(1, coords=dels)
+        assert k1 == k2 > 0
+        np.testing.assert_array_equal(c1, c2)
+        np.testing.assert_array_equal(v1, v2)
+        e, h = vol.download(), host.download()
+        np.testing.assert_array_equal(e[0], h[0])
+        np.testing.assert_array_equal(e[1], h[1])
+        assert host.check() == 0
+        for c in c1[:50]:
+            assert emu.emu_find(vol.h, *[int(x) for x in c]) == -1
+        for i, c in enumerate(e[0][:50]):
+            assert emu.emu_find(vol.h, *[int(x) for x in c]) == i
+    # streamed back: the removed blocks return (new heap indices from the top)
+    counts = vol.upload(c1, v1)
+    assert list(counts) == [len(c1), 0, 0, 0]
+    e = vol.download()
+    assert len(e[0]) == len(h[0]) + len(c1)

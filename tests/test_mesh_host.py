@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 from dynamap_b200 import abi
-from meshutil import assert_same_mesh as same_mesh, build_mesh_host
+from meshutil import assert_same_mesh as same_mesh, build_mesh_host, sphere_volume
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 
@@ -57,33 +57,6 @@ def test_reference_volume(mesh_host, reference_volume):
         assert len(want) > 1000
         same_mesh(got, want)
     assert len(mesh_host(coords, rgbw, sdf, tsdf.voxel_size, *z["box"])) == int(z["triangles"])
-
-
-def sphere_volume(seed, vs=0.01, centre=(0.05, -0.1, 0.3), radius=0.23, trunc=0.04,
-                  hole_frac=0.03, drop_frac=0.08):
-    """Blocks of a noisy sphere SDF around centre (negative coordinates
-    included) with unobserved voxels and missing blocks."""
-    rng = np.random.default_rng(seed)
-    c = np.asarray(centre)
-    lo = np.floor((c - radius - trunc) / (8 * vs)).astype(int) - 1
-    hi = np.ceil((c + radius + trunc) / (8 * vs)).astype(int) + 1
-    bl = np.stack(np.meshgrid(*[np.arange(a, b) for a, b in zip(lo, hi)], indexing="ij"),
-                  -1).reshape(-1, 3)
-    centres = (bl * 8 + 3.5) * vs
-    dist = np.abs(np.linalg.norm(centres - c, axis=1) - radius)
-    bl = bl[dist < trunc + 8 * vs]
-    bl = bl[rng.random(len(bl)) >= drop_frac]
-    bl = bl[rng.permutation(len(bl))]
-    loc = np.stack(np.meshgrid(np.arange(8), np.arange(8), np.arange(8), indexing="ij"),
-                   -1).reshape(512, 3)  # x-major, as the voxel order
-    g = bl[:, None, :] * 8 + loc[None]
-    p = g * vs
-    sdf = np.clip(np.linalg.norm(p - c, axis=2) - radius, -trunc, trunc)
-    sdf = (sdf + rng.normal(0, 0.002, sdf.shape)).astype(np.float32)
-    rgbw = rng.integers(0, 256, size=(len(bl), 512, 4)).astype(np.uint8)
-    rgbw[..., 3] = rng.integers(1, 65, size=(len(bl), 512))
-    rgbw[..., 3][rng.random((len(bl), 512)) < hole_frac] = 0
-    return bl.astype(np.int32), rgbw, sdf
 
 
 @pytest.mark.parametrize("seed", [0, 1, 2])
