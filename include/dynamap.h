@@ -262,7 +262,8 @@ dyn_status dyn_num_blocks(dyn_session* s, int64_t* n_out);
 /* Copies every allocated block: coords_out[3*i..] = block coordinate
  * (HashEntry::position, hashTable.h:22), voxels_out[512*i..] = its voxels in
  * the reference's x-major order (VoxelBlock::at, geom_Types.h:116-119).
- * Order of blocks is unspecified.  voxels_out may be NULL. */
+ * Blocks come in heap order (the order dyn_extract_mesh walks them and
+ * eviction hands them out).  voxels_out may be NULL. */
 dyn_status dyn_download_blocks(dyn_session* s, int32_t* coords_out,
                                dyn_voxel* voxels_out, int64_t capacity,
                                int64_t* n_out);
