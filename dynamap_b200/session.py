@@ -52,6 +52,24 @@ def _download_blocks(lib, h):
     return coords, rgbw, sdf
 
 
+def _removed(lib, h, fn, args, out: bool):
+    """dyn_evict_blocks / dyn_delete_blocks on session handle h: the removed
+    blocks as _download_blocks returns them (out), else their count."""
+    n = C.c_int64()
+    abi.check("dyn_num_blocks", lib.dyn_num_blocks(h, C.byref(n)))
+    n = n.value
+    coords = np.empty((n, 3), np.int32) if out else None
+    vox = np.empty((n, 512, 2), np.uint32) if out else None
+    k = C.c_int64()
+    abi.check(fn, getattr(lib, fn)(h, *args, _ptr(coords), _ptr(vox), n if out else 0,
+                                   C.byref(k)))
+    if not out:
+        return k.value
+    m = min(k.value, n)
+    rgbw = vox[:m, :, 0].copy().view(np.uint8).reshape(m, 512, 4)
+    return coords[:m], rgbw, vox[:m, :, 1].copy().view(np.float32)
+
+
 def _f16(pose) -> C.Array:
     p = np.ascontiguousarray(pose, np.float32).reshape(16)
     return (C.c_float * 16)(*p.tolist())
@@ -159,17 +177,7 @@ class Session:
         return _download_blocks(self.lib, self.h)
 
     def _removed(self, fn, args, out: bool):
-        n = self.num_blocks()
-        coords = np.empty((n, 3), np.int32) if out else None
-        vox = np.empty((n, 512, 2), np.uint32) if out else None
-        k = C.c_int64()
-        abi.check(fn, getattr(self.lib, fn)(self.h, *args, _ptr(coords), _ptr(vox),
-                                             n if out else 0, C.byref(k)))
-        if not out:
-            return k.value
-        m = min(k.value, n)
-        rgbw = vox[:m, :, 0].copy().view(np.uint8).reshape(m, 512, 4)
-        return coords[:m], rgbw, vox[:m, :, 1].copy().view(np.float32)
+        return _removed(self.lib, self.h, fn, args, out)
 
     def evict_blocks(self, max_age: int, out: bool = True):
         """Remove the blocks the allocation has not touched in the last
@@ -395,3 +403,10 @@ class Server:
     def download_blocks(self, slot: int):
         """The slot's map, as Session.download_blocks."""
         return _download_blocks(self.lib, self.session_handle(slot))
+
+    def evict_blocks(self, slot: int, max_age: int, out: bool = True):
+        """Between steps: the slot's blocks not touched in its last
+        max_age + 1 frames removed, as Session.evict_blocks."""
+        self.sync()
+        return _removed(self.lib, self.session_handle(slot), "dyn_evict_blocks",
+                        (int(max_age),), out)

@@ -125,3 +125,23 @@ def test_extract_mesh_layout():
     assert t.shape == (7, 3, 6) and t.dtype == np.float32
     np.testing.assert_array_equal(t.reshape(7, 18)[0, :3], [3.0, 4.0, 5.0])
     assert s.extract_mesh([1.0, 0, 0], [0, 0, 2.0], capacity=2).shape == (2, 3, 6)
+
+
+def test_server_evict_syncs_then_evicts_the_slot():
+    from dynamap_b200.session import Server
+    coords, rgbw, sdf, vox8 = blocks(6, seed=2)
+    fake = FakeLib(coords, vox8)
+    calls = []
+    fake.dyn_server_sync = lambda h: calls.append("sync") or 0
+
+    def session(h, slot, out):
+        calls.append(("session", slot))
+        out._obj.value = 42
+        return 0
+    fake.dyn_server_session = session
+    sv = Server.__new__(Server)
+    sv.lib, sv.h = fake, C.c_void_p(1)
+    out = sv.evict_blocks(3, max_age=10)
+    assert calls == ["sync", ("session", 3)]
+    np.testing.assert_array_equal(out[0], coords[[0, 2, 4]])
+    np.testing.assert_array_equal(out[2].view(np.uint32), sdf[[0, 2, 4]].view(np.uint32))
