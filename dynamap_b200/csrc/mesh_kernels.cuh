@@ -12,7 +12,15 @@
 namespace dyn {
 namespace {
 
-constexpr int kTile = 11;  // voxels per tile edge: a block plus 3 above
+// Voxels per tile edge: a block plus the 3 above it that its cells' samples
+// reach.  Samples outside the tile read the volume, so any edge of at least
+// 8 gives the same mesh; the tests build a smaller tile to exercise that
+// path.
+#ifndef DYN_MESH_TILE
+#define DYN_MESH_TILE 11
+#endif
+constexpr int kTile = DYN_MESH_TILE;
+static_assert(kTile >= 8 && kTile <= 16, "the tile spans the block and at most one more");
 constexpr int kTileVox = kTile * kTile * kTile;
 constexpr int kMeshThreads = 256;
 constexpr int kMeshWarps = kMeshThreads / 32;

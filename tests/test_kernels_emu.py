@@ -7,7 +7,9 @@ library's own upload kernel in both voxel forms: the mesh equals the host
 build of the same walk in content and order, and eviction leaves the same
 volume and hands out the same blocks as the host build of the same steps.
 This covers what the host builds do not: the two-pass mesh output with its
-scans and offsets, the shared-memory tile, and the kernels' indexing."""
+scans and offsets, the shared-memory tile (and, built with a smaller tile,
+its fallback to the volume), the upload's counts, and the kernels'
+indexing."""
 import ctypes as C
 import os
 import shutil
@@ -23,15 +25,15 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CUDA_INC = "/usr/local/cuda/include"
 
 
-@pytest.fixture(scope="module")
-def emu(tmp_path_factory):
+def build_emu(outdir, tile=None):
     cxx = shutil.which("g++")
     if cxx is None or not os.path.exists(os.path.join(CUDA_INC, "cuda_fp16.h")):
         pytest.skip("no C++ compiler or CUDA headers")
-    so = str(tmp_path_factory.mktemp("emu") / "libkernels_emu.so")
+    so = str(outdir / "libkernels_emu.so")
+    extra = [] if tile is None else [f"-DDYN_MESH_TILE={tile}"]
     subprocess.run([cxx, "-std=c++20", "-O1", "-fPIC", "-shared", "-ffp-contract=off",
-                    "-I", CUDA_INC, os.path.join(HERE, "cpp", "kernels_emu.cpp"), "-o", so,
-                    "-pthread"], check=True)
+                    "-I", CUDA_INC] + extra + [os.path.join(HERE, "cpp", "kernels_emu.cpp"),
+                                               "-o", so, "-pthread"], check=True)
     L = C.CDLL(so)
     vp, i64, i32, f32 = C.c_void_p, C.c_int64, C.c_int, C.c_float
     L.emu_volume.restype = vp
@@ -50,6 +52,18 @@ def emu(tmp_path_factory):
 
 
 @pytest.fixture(scope="module")
+def emu(tmp_path_factory):
+    return build_emu(tmp_path_factory.mktemp("emu"))
+
+
+@pytest.fixture(scope="module")
+def emu_small_tile(tmp_path_factory):
+    """The kernels with a 9-voxel tile: the samples of the top layers of
+    cells read the volume instead of shared memory."""
+    return build_emu(tmp_path_factory.mktemp("emu9"), tile=9)
+
+
+@pytest.fixture(scope="module")
 def mesh_host(tmp_path_factory):
     f = build_mesh_host(tmp_path_factory.mktemp("mesh"))
     if f is None:
@@ -60,6 +74,7 @@ def mesh_host(tmp_path_factory):
 class EmuVolume:
     def __init__(self, L, vs, trunc, nb, bsz, num_blocks, fp16):
         self.L = L
+        self.num_blocks = num_blocks
         self.h = L.emu_volume(vs, trunc, nb, bsz, num_blocks, int(fp16))
 
     def __del__(self):
@@ -76,7 +91,7 @@ class EmuVolume:
         return c
 
     def download(self):
-        n = self.L.emu_nalloc(self.h)
+        n = min(self.L.emu_nalloc(self.h), self.num_blocks)  # as dyn_num_blocks
         c = np.zeros((n, 3), np.int32)
         v = np.zeros((n, 512, 8), np.uint8)
         assert self.L.emu_download(self.h, c.ctypes.data, v.ctypes.data) == n
@@ -112,8 +127,9 @@ def split8(v8):
     return v8[..., :4], np.ascontiguousarray(v8[..., 4:]).view(np.float32)[..., 0]
 
 
-@pytest.mark.parametrize("fp16", [False, True])
-def test_mesh_kernels_match_host_walk(emu, mesh_host, fp16):
+@pytest.mark.parametrize("fp16,tile", [(False, 11), (True, 11), (False, 9)])
+def test_mesh_kernels_match_host_walk(emu, emu_small_tile, mesh_host, fp16, tile):
+    emu = emu if tile == 11 else emu_small_tile
     vs = 0.01
     coords, rgbw, sdf = sphere_volume(7, vs=vs, radius=0.12)
     vol = EmuVolume(emu, vs, 0.04, 1 << 12, 10, len(coords) + 8, fp16)
@@ -172,3 +188,22 @@ def test_evict_kernels_match_host_build(emu, evict_lib, fp16):  # noqa: F811
     assert list(counts) == [len(c1), 0, 0, 0]
     e = vol.download()
     assert len(e[0]) == len(h[0]) + len(c1)
+
+
+def test_upload_counts_heap_exhausted_and_present(emu):
+    coords, vox = blocks(21, 15)
+    vox[..., 4:] = np.zeros((15, 512, 4), np.uint8)
+    vol = EmuVolume(emu, 0.01, 0.04, 64, 4, 10, False)
+    assert list(vol.upload(coords, vox)) == [10, 0, 0, 5]
+    assert list(vol.upload(coords[:3], vox[:3])) == [0, 3, 0, 0]
+    c, v = vol.download()
+    assert len(c) == 10
+    # keys whose block the heap could not hold are found as absent, and go at
+    # the next removal; the freed space takes them afterwards
+    placed = {tuple(x) for x in c.tolist()}
+    for x in coords.tolist():
+        assert (emu.emu_find(vol.h, *x) >= 0) == (tuple(x) in placed)
+    k, _, _ = vol.remove(1, coords=c[:6])
+    assert k == 6
+    rest = [x for x in coords.tolist() if tuple(x) not in placed]
+    assert list(vol.upload(np.array(rest, np.int32), vox[:len(rest)])) == [len(rest), 0, 0, 0]
