@@ -60,8 +60,10 @@ def test_delete_then_upload_restores_the_map(gpu_lib, precision):
 
 def test_evict_by_age_keeps_the_last_frames_blocks(gpu_lib, oracle):
     p = small_rgb()
-    seq = configs.sequence(p, seed=42, n_frames=7)
+    p["tsdf"].update(num_blocks=1 << 17, num_buckets=1 << 18)  # the far views hold more
+    seq = configs.sequence(p, seed=42, n_frames=51)
     t, g, b, s = configs.structs(p)
+    order = [0, 1, 2, 3, 40, 45, 50]  # the last views far from the first ones
 
     def frame_blocks(k):
         vol = oracle.Volume(t)
@@ -70,11 +72,11 @@ def test_evict_by_age_keeps_the_last_frames_blocks(gpu_lib, oracle):
         return {tuple(c) for c in vol.download()[0].tolist()}
 
     with Session(t, g, b, s) as m:
-        for k in range(6):
+        for k in order[:6]:
             m.integrate_with_pose(seq.depth[k], seq.rgb[k], seq.poses[k].astype(np.float32))
         before = {tuple(c) for c in m.download_blocks()[0].tolist()}
         assert m.evict_blocks(10, out=False) == 0  # all within ten frames
-        keep = frame_blocks(4) | frame_blocks(5)
+        keep = frame_blocks(order[4]) | frame_blocks(order[5])
         assert keep < before
         gone = m.evict_blocks(1)
         assert {tuple(c) for c in gone[0].tolist()} == before - keep
@@ -82,7 +84,8 @@ def test_evict_by_age_keeps_the_last_frames_blocks(gpu_lib, oracle):
         assert {tuple(c) for c in after.tolist()} == keep
         assert len(after) == len(keep)
         # integration goes on from the freed heap
-        m.integrate_with_pose(seq.depth[6], seq.rgb[6], seq.poses[6].astype(np.float32))
+        k = order[6]
+        m.integrate_with_pose(seq.depth[k], seq.rgb[k], seq.poses[k].astype(np.float32))
         c6 = m.download_blocks()[0]
         got = {tuple(c) for c in c6.tolist()}
-        assert len(got) == len(c6) and got == keep | frame_blocks(6)
+        assert len(got) == len(c6) and got == keep | frame_blocks(k)
