@@ -51,3 +51,24 @@ def test_dropin_builder_tracks(tmp_path, gpu_lib):
     r = subprocess.run([exe, str(path)], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "trans_err" in r.stdout
+
+
+def test_mesh_save_to_file_and_volume_calls_compile(tmp_path):
+    """Mesh::SaveToFile writes the reference's OBJ layout (mesh.cu:39-64):
+    'v x y z r g b' per vertex, then 'f i i+1 i+2' (1-based) per triangle;
+    the volume's mesh and eviction calls compile with the caller's types."""
+    exe = str(tmp_path / "mesh_io")
+    subprocess.run(["g++", "-std=c++17", "-O1", "-Wall", "-Werror", "-I",
+                    os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "cpp", "mesh_io_example.cpp"), "-L", LIBDIR,
+                    "-ldynamap_b200", f"-Wl,-rpath,{LIBDIR}", "-o", exe], check=True)
+    tri = np.arange(2 * 18, dtype=np.float32) * 0.25 - 1.0
+    obj = tmp_path / "m.obj"
+    r = subprocess.run([exe, str(obj)], input=" ".join("%.9g" % v for v in tri),
+                       capture_output=True, text=True, check=True)
+    assert r.stdout.strip() == "2"
+    lines = obj.read_text().splitlines()
+    assert lines[6:] == ["f 1 2 3", "f 4 5 6"]
+    v = np.array([[float(a) for a in ln.split()[1:]] for ln in lines[:6]], np.float32)
+    assert all(ln.startswith("v ") for ln in lines[:6])
+    np.testing.assert_allclose(v.reshape(-1), tri, rtol=1e-5, atol=1e-6)
