@@ -404,13 +404,15 @@ bool mesh_trilinear(const Volume<R>& V, V3<R> position, R* dist) {
 // The cell walk shared by mesh_vertices and mesh_triangles: for every grid
 // cell with all corners observed and a zero crossing, cell(cube, vert)
 // with vert[e] = {x, y, z, r, g, b} for every cut edge e.
+// cell(z, cube, vert) is called for the cells of z-slice z in grid order,
+// the slices in parallel (OpenMP); the callers keep one output per slice
+// and join them in slice order, so the result is the serial walk's.
 template <class F>
 void mesh_cells(const Volume<float>& V, const float lo[3], const float hi[3], F&& cell) {
   const float vs = (float)V.p.voxel_size;
   V3<float> size = v3(std::fabs(lo[0] - hi[0]), std::fabs(lo[1] - hi[1]),
                       std::fabs(lo[2] - hi[2]));
   const int gx = (int)(size.x / vs * 2), gy = (int)(size.y / vs * 2), gz = (int)(size.z / vs * 2);
-  const int64_t total = (int64_t)gx * gy * gz;
   const float P = vs / 2.0f, M = -P;
   // corners in the reference's cube-index order (bit k: corner k inside)
   // and the 12 edges between them
@@ -418,8 +420,11 @@ void mesh_cells(const Volume<float>& V, const float lo[3], const float hi[3], F&
                                    {0, 1, 1}, {1, 1, 1}, {1, 0, 1}, {0, 0, 1}};
   static const int edge[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6},
                                   {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
-  for (int64_t i = 0; i < total; ++i) {
-    const int px = (int)(i % gx), py = (int)((i / gx) % gy), pz = (int)(i / ((int64_t)gx * gy));
+  const int nt = std::max(1, g_threads);
+#pragma omp parallel for num_threads(nt) schedule(dynamic, 1)
+  for (int pz = 0; pz < gz; ++pz)
+  for (int64_t j = 0; j < (int64_t)gx * gy; ++j) {
+    const int px = (int)(j % gx), py = (int)(j / gx);
     const V3<float> pos = v3((float)px * vs + lo[0], (float)py * vs + lo[1], (float)pz * vs + lo[2]);
     V3<float> p[8];
     float d[8];
@@ -463,24 +468,42 @@ void mesh_cells(const Volume<float>& V, const float lo[3], const float hi[3], F&
       vtx[1] = q.y;
       vtx[2] = q.z;
     }
-    cell(cube, vert);
+    cell(pz, cube, vert);
   }
+}
+
+// The slice outputs of mesh_cells joined in slice order: 'per' floats per
+// item, at most cap items into out; returns the item count.
+static int64_t join_slices(const std::vector<std::vector<float>>& sl, int per, float* out,
+                           int64_t cap) {
+  int64_t n = 0;
+  for (const std::vector<float>& v : sl) {
+    const int64_t k = (int64_t)v.size() / per;
+    for (int64_t i = 0; i < k; ++i, ++n)
+      if (n < cap) std::copy(v.begin() + i * per, v.begin() + (i + 1) * per, out + n * per);
+  }
+  return n;
+}
+
+// The number of z-slices mesh_cells walks.
+static size_t mesh_slices(const Volume<float>& V, const float lo[3], const float hi[3]) {
+  const float vs = (float)V.p.voxel_size;
+  const int gz = (int)(std::fabs(lo[2] - hi[2]) / vs * 2);
+  return gz > 0 ? (size_t)gz : 0;
 }
 
 int64_t mesh_vertices(const Volume<float>& V, const float lo[3], const float hi[3],
                       float* out, int64_t cap) {
   static const int edge[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6},
                                   {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
-  int64_t n = 0;
-  mesh_cells(V, lo, hi, [&](unsigned cube, const float (*vert)[6]) {
+  std::vector<std::vector<float>> sl(mesh_slices(V, lo, hi));
+  mesh_cells(V, lo, hi, [&](int z, unsigned cube, const float (*vert)[6]) {
     for (int e = 0; e < 12; ++e) {
       if (((cube >> edge[e][0]) & 1u) == ((cube >> edge[e][1]) & 1u)) continue;
-      if (n < cap)
-        for (int k = 0; k < 6; ++k) out[6 * n + k] = vert[e][k];
-      ++n;
+      sl[z].insert(sl[z].end(), vert[e], vert[e] + 6);
     }
   });
-  return n;
+  return join_slices(sl, 6, out, cap);
 }
 
 // The mesh of the same cells with this project's marching-cubes table
@@ -489,17 +512,13 @@ int64_t mesh_vertices(const Volume<float>& V, const float lo[3], const float hi[
 // {x, y, z, r, g, b}.  Returns the triangle count.
 int64_t mesh_triangles(const Volume<float>& V, const float lo[3], const float hi[3],
                        float* out, int64_t cap) {
-  int64_t n = 0;
-  mesh_cells(V, lo, hi, [&](unsigned cube, const float (*vert)[6]) {
+  std::vector<std::vector<float>> sl(mesh_slices(V, lo, hi));
+  mesh_cells(V, lo, hi, [&](int z, unsigned cube, const float (*vert)[6]) {
     const signed char* row = dyn::kMcTriangles[cube];
-    for (int j = 0; j + 2 < dyn::kMcMaxTriIdx && row[j] >= 0; j += 3) {
-      if (n < cap)
-        for (int k = 0; k < 3; ++k)
-          for (int c = 0; c < 6; ++c) out[18 * n + 6 * k + c] = vert[row[j + k]][c];
-      ++n;
-    }
+    for (int j = 0; j + 2 < dyn::kMcMaxTriIdx && row[j] >= 0; j += 3)
+      for (int k = 0; k < 3; ++k) sl[z].insert(sl[z].end(), vert[row[j + k]], vert[row[j + k]] + 6);
   });
-  return n;
+  return join_slices(sl, 18, out, cap);
 }
 
 // AllocateFromDepthKernel, tsdf.cu:346-453 for one pixel: visits blocks in
