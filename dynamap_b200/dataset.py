@@ -52,8 +52,14 @@ def _imread(path: str, depth: bool) -> np.ndarray:
     return np.ascontiguousarray(img)
 
 
-def _stamp(name: str) -> float:
-    return float(os.path.splitext(os.path.basename(name))[0])
+def _stamp(name: str, prefix: str = "", suffix: str = ".png") -> float:
+    """The number in a file name between prefix and suffix."""
+    b = os.path.basename(name)
+    if prefix and b.startswith(prefix):
+        b = b[len(prefix):]
+    if suffix and b.endswith(suffix):
+        b = b[:-len(suffix)]
+    return float(b)
 
 
 @dataclass
@@ -70,12 +76,17 @@ class TumDataset:
 
     first/last/skip select frames like the reference's firstFrameID /
     lastFrameID / skipFrameNum; gt_max_difference bounds the time difference
-    of a matched ground-truth pose (seconds)."""
+    of a matched ground-truth pose (seconds).  Without an association file,
+    the folders list files named prefix + number + suffix (the reference's
+    depthPrefix / rgbPrefix / suffixes; TUM: no prefix, ".png"), ordered by
+    the number."""
 
     def __init__(self, main_dir: str, association: str = "association.txt",
                  groundtruth: str = "groundtruth.txt", first: int = 0,
-                 last: Optional[int] = None, skip: int = 1, gt_max_difference: float = 0.02):
+                 last: Optional[int] = None, skip: int = 1, gt_max_difference: float = 0.02,
+                 depth_prefix: str = "", rgb_prefix: str = "", suffix: str = ".png"):
         self.main_dir = main_dir
+        self.depth_prefix, self.rgb_prefix, self.suffix = depth_prefix, rgb_prefix, suffix
         self.pairs = self._pairs(association)
         self.pairs = self.pairs[first:last:max(1, skip)]
         self.gt_stamps = None
@@ -85,7 +96,7 @@ class TumDataset:
             self.gt_stamps, self.gt_poses = trajectory.read_tum(gpath)
         self._gt_index = {}
         if self.gt_stamps is not None and len(self.gt_stamps):
-            depth_stamps = [_stamp(d) for d, _ in self.pairs]
+            depth_stamps = [_stamp(d, self.depth_prefix, self.suffix) for d, _ in self.pairs]
             for i, j in trajectory.associate(depth_stamps, self.gt_stamps, gt_max_difference):
                 self._gt_index[i] = j
 
@@ -105,14 +116,18 @@ class TumDataset:
                     depth, rgb = (a, b) if a.startswith("depth") else (b, a)
                     out.append((os.path.join(self.main_dir, depth),
                                 os.path.join(self.main_dir, rgb)))
-            return sorted(out, key=lambda p: _stamp(p[0]))
+            return sorted(out, key=lambda p: _stamp(p[0], self.depth_prefix, self.suffix))
         dd = os.path.join(self.main_dir, "depth")
         if not os.path.isdir(dd):
             raise FileNotFoundError(f"{dd}: no depth folder and no {association}")
-        depth = sorted((n for n in os.listdir(dd) if n.endswith(".png")), key=_stamp)
+        def listed(folder, prefix):
+            names = [n for n in os.listdir(folder)
+                     if n.startswith(prefix) and n.endswith(self.suffix)
+                     and len(n) > len(prefix) + len(self.suffix)]
+            return sorted(names, key=lambda n: _stamp(n, prefix, self.suffix))
+        depth = listed(dd, self.depth_prefix)
         rd = os.path.join(self.main_dir, "rgb")
-        rgb = sorted((n for n in os.listdir(rd) if n.endswith(".png")), key=_stamp) \
-            if os.path.isdir(rd) else []
+        rgb = listed(rd, self.rgb_prefix) if os.path.isdir(rd) else []
         # the reference pairs the sorted lists by index
         return [(os.path.join(dd, d), os.path.join(rd, rgb[i]) if i < len(rgb) else None)
                 for i, d in enumerate(depth)]
@@ -123,7 +138,8 @@ class TumDataset:
     def __getitem__(self, i: int) -> Frame:
         dpath, rpath = self.pairs[i]
         j = self._gt_index.get(i)
-        return Frame(index=i, stamp=_stamp(dpath), depth=_imread(dpath, True),
+        return Frame(index=i, stamp=_stamp(dpath, self.depth_prefix, self.suffix),
+                     depth=_imread(dpath, True),
                      rgb=_imread(rpath, False) if rpath else None,
                      gt_pose=self.gt_poses[j].copy() if j is not None else None)
 

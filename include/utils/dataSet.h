@@ -144,6 +144,13 @@ class dataSet {
   std::string associationFileAddress;
   std::vector<std::string> depthFileNames;  // paths, in time order
   std::vector<std::string> rgbFileNames;    // paired with depthFileNames ("" if none)
+  // file names are prefix + time stamp (or frame number) + suffix
+  // (utils_Dataset.cpp:40-48: TUM "" / ".png"; other layouts "depth_",
+  // "color_"); set them and call loadData() again to re-list
+  std::string depthPrefix;
+  std::string rgbPrefix;
+  std::string depthSuffix = ".png";
+  std::string rgbSuffix = ".png";
   std::size_t firstFrameID = 0;  // kept for the reference's callers; unused there too
   std::size_t lastFrameID = 0;
   std::size_t skipFrameNum = 0;
@@ -185,17 +192,18 @@ class dataSet {
         if (p0.rfind("depth", 0) == 0) pairs.push_back({mainDir + "/" + p0, mainDir + "/" + p1});
         else pairs.push_back({mainDir + "/" + p1, mainDir + "/" + p0});
       }
-      std::stable_sort(pairs.begin(), pairs.end(), [](const auto& x, const auto& y) {
-        return file_stamp(x.first) < file_stamp(y.first);
+      std::stable_sort(pairs.begin(), pairs.end(), [&](const auto& x, const auto& y) {
+        return file_stamp(x.first, depthPrefix, depthSuffix) <
+               file_stamp(y.first, depthPrefix, depthSuffix);
       });
       for (auto& p : pairs) {
         depthFileNames.push_back(p.first);
         rgbFileNames.push_back(p.second);
       }
     } else {
-      depthFileNames = invokeFileNames(depthFolderAddress);
+      depthFileNames = invokeFileNames(depthFolderAddress, depthSuffix, depthPrefix);
       std::vector<std::string> rgb = fs::is_directory(rgbFolderAddress)
-                                         ? invokeFileNames(rgbFolderAddress)
+                                         ? invokeFileNames(rgbFolderAddress, rgbSuffix, rgbPrefix)
                                          : std::vector<std::string>();
       rgb.resize(depthFileNames.size());  // paired by index, as the reference
       rgbFileNames = rgb;
@@ -204,13 +212,20 @@ class dataSet {
     return true;
   }
 
-  // utils_Dataset.cpp:111-148: the .png files of a folder in time order
-  static std::vector<std::string> invokeFileNames(const std::string& folder) {
+  // utils_Dataset.cpp:111-148: the files prefix*suffix of a folder, ordered
+  // by the number between prefix and suffix (paths)
+  static std::vector<std::string> invokeFileNames(const std::string& folder,
+                                                  const std::string& suffix = ".png",
+                                                  const std::string& prefix = "") {
     std::vector<std::string> names;
-    for (const auto& e : std::filesystem::directory_iterator(folder))
-      if (e.path().extension() == ".png") names.push_back(e.path().string());
-    std::stable_sort(names.begin(), names.end(), [](const std::string& a, const std::string& b) {
-      return file_stamp(a) < file_stamp(b);
+    for (const auto& e : std::filesystem::directory_iterator(folder)) {
+      const std::string f = e.path().filename().string();
+      if (f.size() > prefix.size() + suffix.size() && f.compare(0, prefix.size(), prefix) == 0 &&
+          f.compare(f.size() - suffix.size(), suffix.size(), suffix) == 0)
+        names.push_back(e.path().string());
+    }
+    std::stable_sort(names.begin(), names.end(), [&](const std::string& a, const std::string& b) {
+      return file_stamp(a, prefix, suffix) < file_stamp(b, prefix, suffix);
     });
     return names;
   }
@@ -245,7 +260,7 @@ class dataSet {
     image.depth.resize((size_t)d.rows * d.cols);
     for (size_t i = 0; i < image.depth.size(); ++i)
       image.depth[i] = (uint16_t)((d.data[2 * i] << 8) | d.data[2 * i + 1]);  // big endian
-    stamp = file_stamp(depthFileNames[curID]);
+    stamp = file_stamp(depthFileNames[curID], depthPrefix, depthSuffix);
     image.rgb.clear();
     if (!rgbFileNames[curID].empty()) {
       const png::Image c = png::read(rgbFileNames[curID]);
@@ -308,8 +323,14 @@ class dataSet {
   std::vector<std::vector<double>> gt_;
   std::vector<size_t> gt_order_;
   std::string mainDir_;
-  static double file_stamp(const std::string& path) {
-    return std::strtod(std::filesystem::path(path).stem().string().c_str(), nullptr);
+  // the number in a file name between prefix and suffix
+  static double file_stamp(const std::string& path, const std::string& prefix,
+                           const std::string& suffix) {
+    std::string f = std::filesystem::path(path).filename().string();
+    if (f.compare(0, prefix.size(), prefix) == 0) f.erase(0, prefix.size());
+    if (f.size() >= suffix.size() && f.compare(f.size() - suffix.size(), suffix.size(), suffix) == 0)
+      f.erase(f.size() - suffix.size());
+    return std::strtod(f.c_str(), nullptr);
   }
 };
 

@@ -1,7 +1,8 @@
 // Reads a TUM-layout directory through DynaMap::utils::dataSet (the C++
 // drop-in) and writes what it decoded, for the tests to compare against
 // OpenCV and the Python reader.
-//   dataset_example DIR OUTDIR   per frame: OUTDIR/depth_K.bin (uint16),
+//   dataset_example DIR OUTDIR [DEPTH_PREFIX RGB_PREFIX]
+//                                per frame: OUTDIR/depth_K.bin (uint16),
 //                                OUTDIR/rgb_K.bin (uint8 RGB); stdout one
 //                                line "stamp rows cols has_gt p00 .. p33"
 //   dataset_example --png FILE OUT   OUT: rows cols channels bits (int32)
@@ -71,11 +72,18 @@ int main(int argc, char** argv) {
     return 0;
   }
   if (argc == 11 && std::strcmp(argv[1], "--track") == 0) return track(argv + 2);
-  if (argc != 3) {
-    std::fprintf(stderr, "usage: dataset_example DIR OUTDIR | --png FILE OUT | --track ...\n");
+  if (argc != 3 && argc != 5) {
+    std::fprintf(stderr,
+                 "usage: dataset_example DIR OUTDIR [DEPTH_PREFIX RGB_PREFIX] | --png FILE OUT"
+                 " | --track ...\n");
     return 2;
   }
   DynaMap::utils::dataSet ds(argv[1]);
+  if (argc == 5) {  // another layout: re-list with its prefixes
+    ds.depthPrefix = argv[3];
+    ds.rgbPrefix = argv[4];
+    ds.loadData();
+  }
   for (size_t k = 0; ds.curID < ds.size(); ++k) {
     ds.invokeNextFrame();
     const std::string o = std::string(argv[2]) + "/";

@@ -234,3 +234,39 @@ def test_cpp_builder_tracks_from_files(tmp_path, cpp_reader, gpu_lib):
     np.testing.assert_allclose(st, np.round(want, 4), atol=1e-9)
     e = trajectory.ate(est, seq.poses, aligned=False)
     assert e["rmse"] < 0.02
+
+
+def test_prefixed_layout_python_and_cpp(tmp_path, cpp_reader):
+    """Another layout (the reference's depthPrefix / rgbPrefix, e.g.
+    depth_N.png / color_N.png with frame numbers): both readers list the
+    frames in numeric order (not name order) and read them alike."""
+    import subprocess
+    root = tmp_path / "seq"
+    (root / "depth").mkdir(parents=True)
+    (root / "rgb").mkdir()
+    rng = np.random.default_rng(9)
+    n = 12
+    depth = rng.integers(0, 4000, (n, 24, 32)).astype(np.uint16)
+    rgb = rng.integers(0, 256, (n, 24, 32, 3)).astype(np.uint8)
+    for k in range(n):  # numbers whose name order is not their order
+        num = [3, 10, 1, 25, 7, 100, 2, 50, 8, 9, 11, 4][k]
+        cv2.imwrite(str(root / "depth" / f"depth_{num}.png"), depth[k])
+        cv2.imwrite(str(root / "rgb" / f"color_{num}.png"), rgb[k][:, :, ::-1])
+        (root / "rgb" / f"other_{num}.txt").write_text("not a frame")
+    order = np.argsort([3, 10, 1, 25, 7, 100, 2, 50, 8, 9, 11, 4], kind="stable")
+    ds = dataset.TumDataset(str(root), depth_prefix="depth_", rgb_prefix="color_")
+    assert [fr.stamp for fr in ds] == sorted([3, 10, 1, 25, 7, 100, 2, 50, 8, 9, 11, 4])
+    for fr, k in zip(ds, order):
+        np.testing.assert_array_equal(fr.depth, depth[k])
+        np.testing.assert_array_equal(fr.rgb, rgb[k])
+    out = tmp_path / "out"
+    out.mkdir()
+    r = subprocess.run([cpp_reader, str(root), str(out), "depth_", "color_"], capture_output=True,
+                       text=True, check=True)
+    lines = r.stdout.splitlines()
+    assert [float(ln.split()[0]) for ln in lines] == [fr.stamp for fr in ds]
+    for i, k in enumerate(order):
+        d = np.fromfile(out / f"depth_{i}.bin", np.uint16).reshape(24, 32)
+        c = np.fromfile(out / f"rgb_{i}.bin", np.uint8).reshape(24, 32, 3)
+        np.testing.assert_array_equal(d, depth[k])
+        np.testing.assert_array_equal(c, rgb[k])
