@@ -207,3 +207,39 @@ def test_upload_counts_heap_exhausted_and_present(emu):
     assert k == 6
     rest = [x for x in coords.tolist() if tuple(x) not in placed]
     assert list(vol.upload(np.array(rest, np.int32), vox[:len(rest)])) == [len(rest), 0, 0, 0]
+
+
+def test_mesh_kernels_reproduce_the_reference_vertices(emu, oracle):
+    """The mesh kernels on the volume the reference's own MeshExtractor
+    golden was made from (tests/golden/make_mesh_golden.py): the distinct
+    vertices of their triangles are the reference's, bit for bit, and the
+    triangle count is the reference's."""
+    g = np.load(os.path.join(HERE, "golden", "ref_rigid_small.npz"))
+    z = np.load(os.path.join(HERE, "golden", "ref_mesh_vertices.npz"))
+    from dynamap_b200 import abi
+    s, t = g["sensor"], g["tsdf"]
+    sensor = abi.Sensor(rows=int(s[0]), cols=int(s[1]), fx=s[2], fy=s[3], cx=s[4], cy=s[5],
+                        depth_scaler=s[6])
+    tsdf = abi.TsdfParams(voxel_size=t[0], num_buckets=int(t[1]), bucket_size=int(t[2]),
+                          num_blocks=int(t[3]), block_size=int(t[4]), max_sdf_weight=int(t[5]),
+                          truncation_distance=t[6], max_sensor_depth=t[7], min_sensor_depth=t[8])
+    vol = oracle.Volume(tsdf)
+    for k in range(3):
+        d = oracle.depth_from_raw(g["depth"][k], sensor.depth_scaler)
+        vol.allocate(d, sensor, g["poses"][k])
+        vol.integrate(d, g["rgb"][k], sensor, g["poses"][k])
+    coords, rgbw, sdf = vol.download()
+    lo, hi = z["box"]
+    # only the blocks the walk can read: its cells span lo .. lo + 2 |hi - lo|
+    # (the reference's grid), their samples 1.5 voxels beyond
+    vs = float(tsdf.voxel_size)
+    a, b = lo - 2 * vs, lo + 2 * np.abs(hi - lo) + 2 * vs
+    near = np.all((coords * 8 * vs < b) & ((coords + 1) * 8 * vs > a), axis=1)
+    coords, rgbw, sdf = coords[near], rgbw[near], sdf[near]
+    ev = EmuVolume(emu, float(tsdf.voxel_size), float(tsdf.truncation_distance),
+                   int(tsdf.num_buckets), int(tsdf.bucket_size), int(tsdf.num_blocks), False)
+    assert ev.upload(coords, vox8_of(rgbw, sdf))[0] == len(coords)
+    tris = ev.mesh(lo, hi)
+    assert len(tris) == int(z["triangles"])
+    uniq = np.unique(np.ascontiguousarray(tris.reshape(-1, 6)).view(np.uint32), axis=0)
+    np.testing.assert_array_equal(uniq, z["vertices"].view(np.uint32))
