@@ -1,7 +1,7 @@
 """The mesh-extraction and eviction kernels themselves
 (dynamap_b200/csrc/{mesh,evict}_kernels.cuh), run on the CPU under a
-thread-block emulation (tests/cpp/cuda_emu.h: one host thread per CUDA
-thread, barriers for __syncthreads, a per-warp exchange for shuffles), in
+thread-block emulation (tests/cpp/cuda_emu.h: one user-space context per
+CUDA thread, barriers for __syncthreads, a per-warp exchange for shuffles), in
 the launch order of the library's entry points, on volumes built by the
 library's own upload kernel in both voxel forms: the mesh equals the host
 build of the same walk in content and order, and eviction leaves the same
@@ -33,7 +33,7 @@ def build_emu(outdir, tile=None):
     extra = [] if tile is None else [f"-DDYN_MESH_TILE={tile}"]
     subprocess.run([cxx, "-std=c++20", "-O1", "-fPIC", "-shared", "-ffp-contract=off",
                     "-I", CUDA_INC] + extra + [os.path.join(HERE, "cpp", "kernels_emu.cpp"),
-                                               "-o", so, "-pthread"], check=True)
+                                               "-o", so], check=True)
     L = C.CDLL(so)
     vp, i64, i32, f32 = C.c_void_p, C.c_int64, C.c_int, C.c_float
     L.emu_volume.restype = vp
@@ -136,10 +136,8 @@ def test_mesh_kernels_match_host_walk(emu, emu_small_tile, mesh_host, fp16, tile
     assert list(vol.upload(coords, vox8_of(rgbw, sdf))) == [len(coords), 0, 0, 0]
     hc, hv = vol.download()  # heap order; f16-rounded sdf in the mixed form
     h_rgbw, h_sdf = split8(hv)
-    rng = np.random.default_rng(8)
-    boxes = [np.array([[-0.12, -0.27, 0.13], [0.22, 0.07, 0.47]], np.float32)]
-    lo = np.array([-0.05, -0.2, 0.2]) + rng.uniform(-0.03, 0.03, 3)
-    boxes.append(np.array([lo, lo + 0.12], np.float32))
+    # one box, off the voxel grid (the reference-volume test below adds another)
+    boxes = [np.array([[-0.123, -0.271, 0.134], [0.22, 0.07, 0.47]], np.float32)]
     for lo, hi in boxes:
         got = vol.mesh(lo, hi)
         want = mesh_host(hc, h_rgbw, h_sdf, vs, lo, hi)
