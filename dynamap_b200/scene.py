@@ -125,8 +125,9 @@ def trajectory(scene: Scene, n_frames: int, seed: int, trans_per_frame: float,
     ph = rng.uniform(0, 2 * math.pi, size=6)
     k = np.arange(n_frames, dtype=np.float64)
     max_span = math.radians(40.0)
+    # the sweep's period follows from the motion per frame alone, so that a
+    # short sequence is the start of a long one (same motion per frame)
     period = max(4.0 * radius * max_span / max(trans_per_frame, 1e-9), 8.0)
-    period = min(period, max(2.0 * n_frames, 8.0))
     pw = 60.0
     wander = np.stack([np.sin(2 * math.pi * k / pw + ph[2]),
                        0.5 * np.sin(2 * math.pi * k / (pw * 1.3) + ph[3]),

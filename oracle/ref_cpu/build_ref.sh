@@ -2,16 +2,18 @@
 # Builds the reference's own rigid-path kernels for the CPU into
 # oracle/_ref/libdynref.so (test infrastructure; git-ignored output).
 #
-# The reference sources are read from $REF (default /root/reference) and
+# The reference sources are read from $DYNAMAP_REFERENCE (default
+# /root/reference, as in oracle/refsrc.py) and
 # compiled unmodified except for the CUDA launch syntax, which a C++
 # compiler cannot parse: each `K<<<grid, block>>>(` becomes
-# `DYNREF_LAUNCH(K)(` (see shim/cuda_runtime.h).  The rewritten copies live
+# `DYNREF_LAUNCH(K)(` (see shim/cuda_runtime.h), and for buildNLSKernel's
+# hard-coded photometric weight, which becomes a settable value (below).  The rewritten copies live
 # only under oracle/_ref/src and are never committed.  Eigen, OpenCV, the
 # CUDA runtime and the CUDA math libraries gnSolver.h includes are replaced
 # by the small headers in shim/.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${REF:-/root/reference}"
+REF="${DYNAMAP_REFERENCE:-/root/reference}"
 OUT="$HERE/../_ref"
 INC="$REF/include"
 if [ ! -d "$INC" ]; then
@@ -36,6 +38,20 @@ for s in "${SRCS[@]}"; do
   gen="$OUT/src/${base%.cu}.cpp"
   sed -E 's/\b([A-Za-z_][A-Za-z0-9_]*)[[:space:]]*<<<[^>]*>>>[[:space:]]*\(/DYNREF_LAUNCH(\1)(/g' \
     "$INC/$s" > "$gen"
+  if [ "$s" = solver/gnSolver/gnSolver.cu ]; then
+    # The one substitution beyond the launch syntax: buildNLSKernel's
+    # hard-coded photometric weight (gnSolver.cu:180,
+    # `float color_weight = 0.0f;`) reads dynref::color_weight() instead
+    # (shim/cuda_runtime.h, default 0), so the colour term can be pinned at
+    # a nonzero weight.  The build stops if the declaration is not found
+    # exactly once.
+    n="$(grep -c 'float color_weight = 0\.0f;' "$gen" || true)"
+    if [ "$n" != 1 ]; then
+      echo "gnSolver.cu: expected one 'float color_weight = 0.0f;', found $n" >&2
+      exit 1
+    fi
+    sed -i -E 's/float color_weight = 0\.0f;/float color_weight = ::dynref::color_weight();/' "$gen"
+  fi
   obj="$OUT/src/${base%.cu}.o"
   g++ "${CXXFLAGS[@]}" "${INCS[@]}" -I"$(dirname "$INC/$s")" -c "$gen" -o "$obj"
   OBJS+=("$obj")

@@ -58,6 +58,9 @@ rgbdSensor to_sensor(const dyn_sensor* s) {
 extern "C" {
 
 void ref_set_threads(int n) { dynref::nthreads() = n < 1 ? 1 : n; }
+// buildNLSKernel's photometric weight (the reference's constant 0 at
+// gnSolver.cu:180, made settable by build_ref.sh)
+void ref_set_color_weight(float w) { dynref::color_weight() = w; }
 
 void* ref_volume_create(const dyn_tsdf_params* p) {
   tsdf::tsdfProperties props;

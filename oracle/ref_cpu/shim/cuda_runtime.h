@@ -150,6 +150,14 @@ inline int& nthreads() {
   static int n = 1;
   return n;
 }
+// The photometric weight of buildNLSKernel.  The reference hard-codes
+// `float color_weight = 0.0f;` (gnSolver.cu:180); build_ref.sh rewrites
+// that one declaration to read this value, so the golden generator can run
+// the kernel's colour term at a nonzero weight.  Default 0: unchanged.
+inline float& color_weight() {
+  static float w = 0.0f;
+  return w;
+}
 template <class F>
 struct Launcher {
   F f;

@@ -14,6 +14,10 @@ every level at scale 1, for three iteration / threshold settings (the last
 one trips the max_increment guard); its Eigen calls are answered by the
 oracle's own LDL^T and SE(3) exponential (oracle/gn_algebra.h through
 oracle/ref_cpu/shim/eigen_stub.h), and the final increments are stored.
+Last, the same three transforms with the kernel's photometric term on:
+its hard-coded colour weight (gnSolver.cu:180) set to 0.1 through the one
+substitution build_ref.sh makes, RGB from the sequence's procedural
+texture; A and b are stored with both RGB images.
 
 Usage (needs the reference tree, present only where the fixtures are made):
     bash oracle/ref_cpu/build_ref.sh && python tests/golden/make_icp_golden.py
@@ -53,6 +57,7 @@ def main():
     L.ref_gn_solve.argtypes = [vp, vp, vp, vp, C.POINTER(abi.Sensor), C.POINTER(C.c_int32),
                                C.c_float, C.c_float, C.c_float, vp, vp]
     L.ref_set_threads(1)
+    L.ref_set_color_weight.argtypes = [C.c_float]
     sensor = abi.Sensor(rows=60, cols=80, fx=65.625, fy=65.625, cx=39.5, cy=29.5,
                         depth_scaler=1000.0)
     seq = scene.make_sequence(17, 2, sensor.rows, sensor.cols, sensor.fx, sensor.fy, sensor.cx,
@@ -83,6 +88,20 @@ def main():
         Ts.append(T)
         As.append(A)
         bs.append(b)
+    # the photometric term at weight 0.1 (the weight of the 640x480 RGB-D
+    # configuration), same frames and transforms
+    L.ref_set_color_weight(0.1)
+    Acs, bcs = [], []
+    for T in Ts:
+        A = np.zeros(36, np.float32)
+        b = np.zeros(6, np.float32)
+        L.ref_icp_normal_equations(p(src), p(nrm[0]), p(tgt), p(nrm[1]),
+                                   p(np.ascontiguousarray(seq.rgb[1])),
+                                   p(np.ascontiguousarray(seq.rgb[0])), C.byref(sensor),
+                                   (C.c_float * 16)(*T.reshape(16).tolist()), p(A), p(b))
+        Acs.append(A)
+        bcs.append(b)
+    L.ref_set_color_weight(0.0)
     # whole solves: (iterations per level, min_increment, max_increment,
     # regularization)
     settings = [((5, 4, 3), 1e-3, 0.3, 0.02), ((10, 5, 4), 1e-5, 0.3, 0.02),
@@ -100,6 +119,8 @@ def main():
         sensor=np.array([sensor.rows, sensor.cols, sensor.fx, sensor.fy, sensor.cx, sensor.cy,
                          sensor.depth_scaler], np.float64),
         transforms=np.array(Ts), A=np.array(As), b=np.array(bs),
+        src_rgb=np.ascontiguousarray(seq.rgb[1]), tgt_rgb=np.ascontiguousarray(seq.rgb[0]),
+        color_weight=np.float32(0.1), A_color=np.array(Acs), b_color=np.array(bcs),
         solve_iters=np.array([s_[0] for s_ in settings], np.int32),
         solve_thresholds=np.array([s_[1:] for s_ in settings], np.float32),
         solve_inc=np.array(incs), solve_pose=np.array(poses))

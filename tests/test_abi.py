@@ -7,6 +7,7 @@ import re
 import pytest
 
 from dynamap_b200 import abi
+from oracle import refsrc
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -78,12 +79,13 @@ def test_yaml_parser(tmp_path):
     assert lib.dyn_load_yaml(b"/nonexistent.yaml", None, None, None, None) == 1
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference/config"), reason="reference tree absent")
+@pytest.mark.skipif(not os.path.isdir(os.path.join(refsrc.reference_root(), "config")),
+                    reason="reference tree absent")
 def test_yaml_parser_reads_reference_files():
     lib = abi.load()
     t, g, b, s = abi.TsdfParams(), abi.GnParams(), abi.BilateralParams(), abi.Sensor()
     for f in ("tsdfParams", "gnOptimParams", "bilateralFParams", "cameraParams"):
-        path = f"/root/reference/config/{f}.yaml".encode()
+        path = os.path.join(refsrc.reference_root(), "config", f"{f}.yaml").encode()
         abi.check(f, lib.dyn_load_yaml(path, C.byref(t), C.byref(g), C.byref(b), C.byref(s)))
     d = abi.defaults()
     for a, c in zip((t, g, b, s), d):

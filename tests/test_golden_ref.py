@@ -151,6 +151,47 @@ def test_reference_icp_normal_equations(oracle):
         assert out[28] == cnt
 
 
+def test_reference_icp_photometric(oracle):
+    """buildNLSKernel with its photometric term on (gnSolver.cu:136-193):
+    the reference's colour weight (a constant 0 at :180) set to 0.1, RGB
+    from the sequence's texture.  The oracle's per-pixel terms -- luma
+    intensities, the one-sided gradient at (x-1) and (y-1) halved, the
+    Jacobian grad(I) [-p^ | I], the blend (1-w) A + w Jc^T Jc and
+    (1-w) b + w Jc^T (I_t - I_s) -- summed in the reference's order are
+    bit-identical for three transforms."""
+    z = np.load(os.path.join(HERE, "golden", "ref_icp_normal_equations.npz"))
+    r, c, fx, fy, cx, cy, ds = z["sensor"]
+    s = abi.Sensor(rows=int(r), cols=int(c), fx=fx, fy=fy, cx=cx, cy=cy, depth_scaler=ds)
+    _, g, _, _ = abi.defaults()
+    g.icp_min_depth, g.icp_max_depth = 0.15, 2.0
+    g.color_weight = float(z["color_weight"])
+    thr = np.float32(np.cos(np.pi / 10))
+    g.normal_cos_thresh = float(np.nextafter(thr, np.float32(0)))
+
+    def n4(n3):
+        n = np.zeros(n3.shape[:2] + (4,), np.float32)
+        n[..., :3] = n3
+        return n
+
+    sn, tn = n4(z["src_normals"]), n4(z["tgt_normals"])
+    si, ti = oracle.intensity(z["src_rgb"]), oracle.intensity(z["tgt_rgb"])
+    for k in range(len(z["transforms"])):
+        A, b, cnt = oracle.icp_normal_equations_refsum(z["src_depth"], sn, si, z["tgt_depth"],
+                                                        tn, ti, s, g, z["transforms"][k])
+        assert cnt > 250
+        # the colour term changes the system
+        assert not np.array_equal(z["A_color"][k], z["A"][k])
+        np.testing.assert_array_equal(A.view(np.uint32), z["A_color"][k].view(np.uint32))
+        np.testing.assert_array_equal(b.view(np.uint32), z["b_color"][k].view(np.uint32))
+        out = oracle.icp_normal_equations(z["src_depth"], sn, si, z["tgt_depth"], tn, ti,
+                                          s, g, z["transforms"][k])
+        Af = z["A_color"][k].astype(np.float64).reshape(6, 6)
+        up = np.array([Af[i, j] for i in range(6) for j in range(i, 6)])
+        np.testing.assert_allclose(out[:21], up, rtol=1e-5, atol=1e-4)
+        np.testing.assert_allclose(out[21:27], z["b_color"][k], rtol=1e-5, atol=1e-4)
+        assert out[28] == cnt
+
+
 def test_reference_gn_solve(oracle):
     """gnSolver::solve (gnSolver.cu:317-438) from the identity, every level
     at full resolution, for three settings (the last trips the
