@@ -203,6 +203,17 @@ __device__ inline int find_block(const Entry* __restrict__ entries, const DTsdf&
   return -1;
 }
 
+// Entry index of a key in its bucket, or -1 (the same scan as find_block).
+__device__ inline int find_entry(const Entry* entries, const DTsdf& t, unsigned long long k) {
+  int b = hash_slot(key_x(k), key_y(k), key_z(k), t);
+  for (int i = 0; i < t.bucket_size; ++i) {
+    unsigned long long ek = *(const volatile unsigned long long*)&entries[b + i].key;
+    if (ek == k) return b + i;
+    if (ek == kEmptyKey) return -1;
+  }
+  return -1;
+}
+
 // Lock-free unique insert into the key's bucket (the set semantics of
 // HashTable::AllocateBlock, hashTable.cu:80-110, without its duplicate-
 // insert race): scan the bucket in slot order, claim the first empty slot by

@@ -157,8 +157,13 @@ __global__ void rewrite_kernel(Entry* entries, int nbuckets, int bsz, int n,
 
 // Blocks from the host into the volume: each key inserted (stamped with the
 // last frame), a heap index taken for a new one, its voxels written in the
-// volume's form.  Keys already present are left as they are.  counts:
-// [placed, present, bucket full, heap exhausted].
+// volume's form.  Keys already present with a block are left as they are.
+// A key whose entry has no block (an earlier insert found the heap full)
+// takes a heap index now if there is one, so a retry after a heap-exhausted
+// result places the block or reports the heap exhausted again, never
+// "present".  Whichever CTA moves the entry's ptr from -1 to the claim mark
+// -3 gives it its heap index, so a key that occurs twice is placed once.
+// counts: [placed, present, bucket full, heap exhausted].
 __global__ void upload_kernel(VolumeDev v, const PoseState* __restrict__ ps,
                               const int* __restrict__ coords, const dyn_voxel* __restrict__ vox,
                               int m, int* __restrict__ counts) {
@@ -168,19 +173,23 @@ __global__ void upload_kernel(VolumeDev v, const PoseState* __restrict__ ps,
     if (threadIdx.x == 0) {
       const unsigned long long key = pack_key(coords[3 * k], coords[3 * k + 1], coords[3 * k + 2]);
       const int r = bucket_insert(v.entries, v.t, key, ps->frame, &unique_s);
+      const int e = r >= 0 ? r : (r == -1 ? find_entry(v.entries, v.t, key) : -1);
       int ptr = -1;
-      if (r >= 0) {
+      if (e < 0) {
+        atomicAdd(&counts[2], 1);  // bucket full
+      } else if (atomicCAS(&v.entries[e].ptr, -1, -3) == -1) {
         ptr = atomicAdd(&v.cnt->nalloc, 1);
         if (ptr < v.t.num_blocks) {
-          v.entries[r].ptr = ptr;
+          atomicExch(&v.entries[e].ptr, ptr);
           v.block_keys[ptr] = key;
           atomicAdd(&counts[0], 1);
         } else {
           ptr = -1;
+          atomicExch(&v.entries[e].ptr, -1);
           atomicAdd(&counts[3], 1);
         }
       } else {
-        atomicAdd(&counts[r == -1 ? 1 : 2], 1);
+        atomicAdd(&counts[1], 1);  // present with a block (or placed by another CTA)
       }
       ptr_s = ptr;
     }

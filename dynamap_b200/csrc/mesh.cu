@@ -24,12 +24,33 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 
 #include "mesh_kernels.cuh"
 #include "session_impl.cuh"
 
 
 using namespace dyn::host;
+
+namespace {
+
+// The marching-cubes triangle table (d_mc_tri) is written once per device,
+// synchronously, before the first mesh kernel on that device runs; later
+// calls (from any session's stream) only read it.
+std::mutex g_mc_mu;
+bool g_mc_ready[64] = {};
+
+dyn_status mc_table_ready(int dev) {
+  if (dev < 0 || dev >= 64) return DYN_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(g_mc_mu);
+  if (!g_mc_ready[dev]) {
+    DYN_CUDA(cudaMemcpyToSymbol(dyn::d_mc_tri, dyn::kMcTriangles, sizeof(dyn::kMcTriangles)));
+    g_mc_ready[dev] = true;
+  }
+  return DYN_OK;
+}
+
+}  // namespace
 
 dyn_status dyn_extract_mesh(dyn_session* s, const float lower[3], const float upper[3],
                             float* triangles_host, int64_t capacity, int64_t* n_out) {
@@ -42,8 +63,7 @@ dyn_status dyn_extract_mesh(dyn_session* s, const float lower[3], const float up
   if (nb == 0 || g.n[0] == 0 || g.n[1] == 0 || g.n[2] == 0) return DYN_OK;
   DeviceGuard dg(s->device);
   cudaStream_t st = s->stream;
-  DYN_CUDA(cudaMemcpyToSymbolAsync(dyn::d_mc_tri, dyn::kMcTriangles, sizeof(dyn::kMcTriangles), 0,
-                                   cudaMemcpyHostToDevice, st));
+  DYN_TRY(mc_table_ready(s->device));
   const int n = (int)nb;
   long long* counts = nullptr;
   long long* offsets = nullptr;  // n offsets, then the total

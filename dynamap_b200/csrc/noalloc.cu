@@ -24,12 +24,20 @@
 // same device at once) race on the array and must be serialised by the
 // caller.  The first call on a device looks up the array's device address
 // (cudaGetSymbolAddress) with that device current; make that first call
-// before any stream capture on the device.
+// before any stream capture on the device.  The address is kept for the
+// life of the process, so the library must not be used across a
+// cudaDeviceReset of that device (the allocating entry point keeps its
+// buffers the same way).
+//
+// Inputs are checked exactly as dyn_icp_normal_equations checks them
+// (valid_sensor: sides 1..8192, positive focal lengths and depth scaler),
+// so both entry points accept and reject the same levels.
 #include <cuda_runtime.h>
 
 #include <mutex>
 
 #include "icp.cuh"
+#include "session_impl.cuh"
 
 using namespace dyn;
 
@@ -77,9 +85,8 @@ extern "C" dyn_status dyn_icp_normal_equations_noalloc(
     const float* tgt_depth_dev, const float* tgt_normal4_dev, const float* tgt_intensity_dev,
     const dyn_sensor* level, const dyn_gn_params* gn, const float T[16], double out_host[29],
     void* stream) {
-  if (!src_depth_dev || !src_normal4_dev || !tgt_depth_dev || !tgt_normal4_dev || !level ||
-      !gn || !T || !out_host || level->rows == 0 || level->cols == 0 || !(level->fx > 0) ||
-      !(level->fy > 0))
+  if (!src_depth_dev || !src_normal4_dev || !tgt_depth_dev || !tgt_normal4_dev ||
+      !dyn::host::valid_sensor(level) || !gn || !T || !out_host)
     return DYN_ERR_INVALID_ARG;
   if (gn->color_weight != 0.0f && (!src_intensity_dev || !tgt_intensity_dev))
     return DYN_ERR_INVALID_ARG;

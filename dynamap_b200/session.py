@@ -54,7 +54,13 @@ def _download_blocks(lib, h):
 
 def _removed(lib, h, fn, args, out: bool):
     """dyn_evict_blocks / dyn_delete_blocks on session handle h: the removed
-    blocks as _download_blocks returns them (out), else their count."""
+    blocks as _download_blocks returns them (out), else their count.
+
+    With 'out' the host buffers are sized for every allocated block, since
+    the removal itself decides how many go: 4 KiB + 12 B per allocated block
+    (8 GiB for a full pool of 2^21 blocks), whatever the number removed.
+    Callers that only need the count pass out=False, which allocates
+    nothing."""
     n = C.c_int64()
     abi.check("dyn_num_blocks", lib.dyn_num_blocks(h, C.byref(n)))
     n = n.value

@@ -404,8 +404,11 @@ dyn_status dyn_icp_normal_equations(
  * device share the array: calls whose GPU work overlaps race and must be
  * serialised by the caller.  The first call on a device does a one-time
  * set-up (looks up the array's address with that device current); make it
- * before any stream capture.  Results equal dyn_icp_normal_equations' to
- * rounding (the partial sums are grouped differently).  Synchronous. */
+ * before any stream capture.  That address is kept until exit: do not use
+ * the library across a cudaDeviceReset of the device.  Levels are checked
+ * as dyn_icp_normal_equations checks them.  Results equal
+ * dyn_icp_normal_equations' to rounding (the partial sums are grouped
+ * differently).  Synchronous. */
 dyn_status dyn_icp_normal_equations_noalloc(
     const float* src_depth_dev, const float* src_normal4_dev,
     const float* src_intensity_dev, const float* tgt_depth_dev,

@@ -17,8 +17,10 @@ def pytest_configure(config):
 def pytest_collection_modifyitems(config, items):
     """Tests of code not yet run on a B200 go after all others, so that
     under -x a failure there cannot hide the results of the established
-    tests."""
-    items.sort(key=lambda it: it.get_closest_marker("first_b200_run") is not None)
+    tests; the allocation-free entry point's file (test_zz_*) stays last of
+    all."""
+    items.sort(key=lambda it: (os.path.basename(str(it.fspath)).startswith("test_zz"),
+                               it.get_closest_marker("first_b200_run") is not None))
 
 
 @pytest.fixture(scope="session")

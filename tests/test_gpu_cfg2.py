@@ -1,0 +1,157 @@
+"""Parity of the CUDA path with the oracle on the 640x480 depth + RGB
+configuration the benchmark runs: 5 mm voxels, truncation 4 voxels, 2^20
+hash buckets x 10, 2^19 blocks, geometric + photometric ICP at colour
+weight 0.1.
+
+Bars (the same as tests/test_gpu_parity.py): the normal equations with the
+photometric term within 1e-6 relative of the oracle's (FP32 per-pixel terms
+summed in a different order); tracked poses within 1e-4 m / 1e-4 rad of the
+oracle's every frame with the same iteration counts; allocation and
+integration at the full table size bit-exact (block set, sdf bits, weights,
+colours).  The oracle's photometric terms are pinned to the reference's
+buildNLSKernel at weight 0.1 (tests/test_golden_ref.py).
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from dynamap_b200 import abi, configs
+from dynamap_b200.session import Session
+
+pytestmark = [pytest.mark.gpu, pytest.mark.first_b200_run]
+
+
+def cfg2(rows=480, cols=640):
+    p = configs.preset("cfg2")
+    if (rows, cols) != (480, 640):
+        s = cols / 640.0
+        p["sensor"].update(rows=rows, cols=cols, fx=525.0 * s, fy=525.0 * s,
+                           cx=(319.5 + 0.5) * s - 0.5, cy=(239.5 + 0.5) * s - 0.5)
+    return p
+
+
+def sort_blocks(coords, *arrs):
+    order = np.lexsort((coords[:, 2], coords[:, 1], coords[:, 0]))
+    return (coords[order],) + tuple(a[order] for a in arrs)
+
+
+def rot_angle(R):
+    w = np.array([R[2, 1] - R[1, 2], R[0, 2] - R[2, 0], R[1, 0] - R[0, 1]]) / 2
+    return float(np.arcsin(min(1.0, np.linalg.norm(w))))
+
+
+@pytest.fixture(scope="module")
+def seq640():
+    return configs.sequence(cfg2(), seed=21, n_frames=5)
+
+
+@pytest.fixture(scope="module")
+def seq160():
+    return configs.sequence(cfg2(120, 160), seed=22, n_frames=20)
+
+
+def test_photometric_normal_equations(gpu_lib, oracle, seq640):
+    """dyn_icp_normal_equations with source/target intensities at weight 0.1
+    against the oracle, at the coarsest and the finest level."""
+    import torch
+    p = cfg2()
+    t, g, b, s = configs.structs(p)
+    assert g.color_weight == pytest.approx(0.1)
+    rel = np.linalg.inv(seq640.poses[0]) @ seq640.poses[1]
+    for scale in (4, 1):
+        ls = oracle.level_sensor(s, scale)
+
+        def level(k):
+            d = oracle.bilateral(oracle.depth_from_raw(seq640.depth[k], s.depth_scaler), b)
+            i = oracle.intensity(seq640.rgb[k])
+            while d.shape[0] > ls.rows:
+                d = oracle.downsample_depth(d)
+                i = oracle.downsample_intensity(i)
+            return d, i
+        (sd, si), (td, ti) = level(1), level(0)
+        _, sn = oracle.maps(sd, ls)
+        _, tn = oracle.maps(td, ls)
+        for T in (rel, np.eye(4)):
+            T = T.astype(np.float32)
+            ref = oracle.icp_normal_equations(sd, sn, si, td, tn, ti, ls, g, T)
+            geo = oracle.icp_normal_equations(sd, sn, None, td, tn, None, ls,
+                                              _with(g, color_weight=0.0), T)
+            assert ref[28] > 100
+            assert not np.allclose(ref[:27], geo[:27])  # the colour term is in play
+            dev = [torch.from_numpy(np.ascontiguousarray(a)).cuda()
+                   for a in (sd, sn, si, td, tn, ti)]
+            out = (C.c_double * 29)()
+            Tc = (C.c_float * 16)(*T.reshape(16).tolist())
+            abi.check("dyn_icp_normal_equations", gpu_lib.dyn_icp_normal_equations(
+                dev[0].data_ptr(), dev[1].data_ptr(), dev[2].data_ptr(), dev[3].data_ptr(),
+                dev[4].data_ptr(), dev[5].data_ptr(), C.byref(ls), C.byref(g), Tc, out, None))
+            got = np.array(out)
+            assert got[28] == ref[28]
+            np.testing.assert_allclose(got, ref, rtol=1e-6, atol=1e-9 * np.abs(ref).max())
+
+
+def _with(g, **kw):
+    o = abi.GnParams()
+    C.memmove(C.byref(o), C.byref(g), C.sizeof(abi.GnParams))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def _track(p, seq, oracle, n):
+    t, g, b, s = configs.structs(p)
+    os_ = oracle.Session(t, g, b, s)
+    os_.set_pose(seq.poses[0])
+    worst = (0.0, 0.0)
+    with Session(t, g, b, s) as m:
+        m.set_pose(seq.poses[0])
+        for k in range(n):
+            gp, gst = m.process(seq.depth[k], seq.rgb[k])
+            op, ost = os_.frame(seq.depth[k], seq.rgb[k])
+            dt = float(np.linalg.norm(gp[:3, 3] - op[:3, 3]))
+            dr = rot_angle(gp[:3, :3].astype(np.float64).T @ op[:3, :3].astype(np.float64))
+            worst = (max(worst[0], dt), max(worst[1], dr))
+            assert dt < 1e-4 and dr < 1e-4, (k, dt, dr)
+            assert list(gst.icp_iterations) == list(ost.icp_iterations), k
+        te = float(np.linalg.norm(gp[:3, 3] - seq.poses[n - 1][:3, 3]))
+    return worst, te
+
+
+def test_rgb_tracking_160x120_matches_oracle(gpu_lib, oracle, seq160):
+    """20 frames of the configuration at 160x120 (intrinsics scaled), RGB
+    tracking at weight 0.1, full-size tables."""
+    worst, te = _track(cfg2(120, 160), seq160, oracle, 20)
+    assert te < 0.02
+
+
+def test_rgb_tracking_640x480_matches_oracle(gpu_lib, oracle, seq640):
+    """5 frames of the benchmark's configuration as it runs."""
+    worst, te = _track(cfg2(), seq640, oracle, 5)
+    assert te < 0.01
+
+
+def test_integration_full_tables_bitexact(gpu_lib, oracle, seq640):
+    """Allocation and integration of 3 RGB frames at the ground-truth poses
+    with the configuration's full tables: block set, sdf bits, weights and
+    colours equal to the oracle's."""
+    p = cfg2()
+    t, g, b, s = configs.structs(p)
+    assert t.num_buckets == 1 << 20 and t.bucket_size == 10 and t.num_blocks == 1 << 19
+    ovol = oracle.Volume(t)
+    with Session(t, g, b, s) as m:
+        for k in range(3):
+            pose = seq640.poses[k].astype(np.float32)
+            m.integrate_with_pose(seq640.depth[k], seq640.rgb[k], pose)
+            d = oracle.depth_from_raw(seq640.depth[k], s.depth_scaler)
+            c1 = ovol.allocate(d, s, pose)
+            c2 = ovol.integrate(d, seq640.rgb[k], s, pose)
+            assert c1[oracle.C_BUCKET_FULL] == 0 and c1[oracle.C_HEAP] == 0
+            assert c2[oracle.C_REHASH] == 0
+        gc, grgbw, gsdf = sort_blocks(*m.download_blocks())
+        oc, orgbw, osdf = sort_blocks(*ovol.download())
+        assert len(gc) > 10000
+        np.testing.assert_array_equal(gc, oc)
+        np.testing.assert_array_equal(grgbw[..., 3], orgbw[..., 3])
+        np.testing.assert_array_equal(grgbw, orgbw)
+        np.testing.assert_array_equal(gsdf.view(np.uint32), osdf.view(np.uint32))

@@ -16,7 +16,7 @@ from dynamap_b200 import abi, configs
 from dynamap_b200.session import Session
 from meshutil import assert_same_mesh, build_mesh_host
 
-pytestmark = [pytest.mark.gpu, pytest.mark.first_b200_run]
+pytestmark = pytest.mark.gpu
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)

@@ -193,9 +193,14 @@ def test_upload_counts_heap_exhausted_and_present(emu):
     vox[..., 4:] = np.zeros((15, 512, 4), np.uint8)
     vol = EmuVolume(emu, 0.01, 0.04, 64, 4, 10, False)
     assert list(vol.upload(coords, vox)) == [10, 0, 0, 5]
-    assert list(vol.upload(coords[:3], vox[:3])) == [0, 3, 0, 0]
     c, v = vol.download()
     assert len(c) == 10
+    assert list(vol.upload(c[:3], v[:3])) == [0, 3, 0, 0]
+    # a retry of the keys the heap could not hold reports the heap exhausted
+    # again (their entries exist without a block), not "present"
+    held = {tuple(x) for x in c.tolist()}
+    miss = np.array([i for i, x in enumerate(coords.tolist()) if tuple(x) not in held])
+    assert list(vol.upload(coords[miss], vox[miss])) == [0, 0, 0, 5]
     # keys whose block the heap could not hold are found as absent, and go at
     # the next removal; the freed space takes them afterwards
     placed = {tuple(x) for x in c.tolist()}
@@ -205,6 +210,15 @@ def test_upload_counts_heap_exhausted_and_present(emu):
     assert k == 6
     rest = [x for x in coords.tolist() if tuple(x) not in placed]
     assert list(vol.upload(np.array(rest, np.int32), vox[:len(rest)])) == [len(rest), 0, 0, 0]
+
+
+def test_upload_places_a_repeated_key_once(emu):
+    coords, vox = blocks(22, 3)
+    vol = EmuVolume(emu, 0.01, 0.04, 64, 4, 10, False)
+    twice = np.concatenate([coords, coords[:1]])
+    assert list(vol.upload(twice, np.concatenate([vox, vox[:1]]))) == [3, 1, 0, 0]
+    c, _ = vol.download()
+    assert sorted(map(tuple, c.tolist())) == sorted(map(tuple, coords.tolist()))
 
 
 def test_mesh_kernels_reproduce_the_reference_vertices(emu, oracle):

@@ -72,3 +72,18 @@ def test_noalloc_rejects_levels_beyond_its_capacity(gpu_lib):
     st = gpu_lib.dyn_icp_normal_equations_noalloc(dummy, dummy, None, dummy, dummy, None,
                                                   C.byref(big), C.byref(g), Tc, out, None)
     assert st == 1  # DYN_ERR_INVALID_ARG
+
+
+def test_noalloc_checks_levels_as_the_allocating_entry_point_does(gpu_lib):
+    """A 1 x 2,000,000 level fits the array but is not a sensor either entry
+    point accepts (sides are limited to 8192): both reject it."""
+    t, g, b, s = abi.defaults()
+    thin = abi.Sensor(rows=1, cols=2_000_000, fx=500.0, fy=500.0, cx=0.0, cy=0.0,
+                      depth_scaler=1000.0)
+    out = (C.c_double * 29)()
+    Tc = (C.c_float * 16)(*np.eye(4, dtype=np.float32).reshape(16).tolist())
+    dummy = C.c_void_p(16)  # never dereferenced: the level check comes first
+    for fn in ("dyn_icp_normal_equations", "dyn_icp_normal_equations_noalloc"):
+        st = getattr(gpu_lib, fn)(dummy, dummy, None, dummy, dummy, None, C.byref(thin),
+                                  C.byref(g), Tc, out, None)
+        assert st == 1, fn  # DYN_ERR_INVALID_ARG
