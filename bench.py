@@ -470,6 +470,18 @@ def run_ours(args):
         elapsed_c_host = time.perf_counter() - h0
     elapsed_c = max_over_ranks(elapsed_c_host)
 
+    # ---- the north star's forms in the same run: the batched configuration
+    # (mixed and band against the plain FP32 per-frame path) and a
+    # shortened serving run
+    batched = serving = None
+    if args.batched and prec == abi.PRECISION_FP32:
+        del d_dev, c_dev, pin_d, pin_c
+        torch.cuda.empty_cache()
+        batched = measure_batched(args, ranks, local, args.sessions, args.steps, args.warmup,
+                                  ["mixed", "band"], e2e=True)
+    if args.serving and prec == abi.PRECISION_FP32:
+        serving = measure_serving(args, ranks, local, args.embed_serve_seconds, "band")
+
     if rank != 0:
         ranks.close()
         return
@@ -523,6 +535,8 @@ def run_ours(args):
         "ate_gt_mm": ate * 1e3,
         "accuracy_vs_fp64": acc,
         "precision_forms": forms or None,
+        "batched": batched,
+        "serving": serving,
         "map": {"blocks_total": st_avg["blocks_total"], "visible_per_frame": st_avg["blocks_visible"],
                 "load_factor": st_avg["blocks_total"] / (t.num_buckets * t.bucket_size)},
     }
@@ -530,42 +544,40 @@ def run_ours(args):
     ranks.close()
 
 
-def run_batched(args):
-    """The batched configuration: args.sessions independent sessions of mixed
-    resolution, one frame of every session per step.  value = aggregate
-    frames/s of the batched submission; 'plain' = the same sessions driven
-    one frame at a time, each waited for before the next (the reference's
-    per-frame loop) on the same GPU."""
+def measure_batched(args, ranks, local, n_sessions, steps, warmup, precisions,
+                    e2e=True, streams=False, stage_split=False):
+    """The batched configuration: n_sessions independent sessions of mixed
+    resolution (160x120 / 320x240 / 640x480 at 1:2:1), one frame of every
+    session per step, for each precision in 'precisions' as one fused launch
+    per stage (dyn_batch, one CUDA graph per frame), beside the plain FP32
+    per-frame path on the same GPU: the same sessions driven one frame at a
+    time, each waited for before the next (the reference's per-frame loop).
+    Returns the per-form figures: aggregate frames/s (device-resident
+    frames; end to end from pinned host memory with 'e2e'), the speed-up
+    over the plain path, and each session's trajectory against the plain
+    path's (ATE against the ground truth, and the difference)."""
     import ctypes as C
 
     import numpy as np
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    nframes = args.warmup + args.steps
-    from dynamap_b200 import configs
-    mix = configs.session_mix(args.sessions, nframes, base_seed=100 + 1000 * rank)
+    import torch
+    from dynamap_b200 import abi, configs
+    from dynamap_b200.session import Batch, Session
+    world, rank = ranks.world, ranks.rank
+    nframes = warmup + steps
+    mix = configs.session_mix(n_sessions, nframes, base_seed=100 + 1000 * rank)
     workers = max(1, min(32, ((os.cpu_count() or 2) - 1) // max(world, 1)))
     frames = make_many([(p, seed) for _, p, seed in mix], nframes, workers)
-
-    import torch
-    from dynamap_b200 import abi
-    from dynamap_b200.replicas import Ranks
-    from dynamap_b200.session import Session
-    torch.cuda.set_device(local)
-    ranks = Ranks()  # each GPU runs its own session mix: weak scaling
     lib = abi.load()
-    prec = PRECISIONS[args.precision]
     structs = [configs.structs(p) for _, p, _ in mix]
     dev_frames = [torch.from_numpy(d).cuda() for d, _, _ in frames]
     nbytes = [d.shape[1] * d.shape[2] * 2 for d, _, _ in frames]
-    pinned = [torch.from_numpy(d).pin_memory().numpy() for d, _, _ in frames]
+    pinned = [torch.from_numpy(d).pin_memory().numpy() for d, _, _ in frames] if e2e else None
+    gt = [poses[warmup:nframes] for _, _, poses in frames]
+    n = len(mix)
 
     def barrier():
         torch.cuda.synchronize()
         ranks.barrier()
-
-    max_over_ranks = ranks.max
 
     def timed(fn):
         barrier()
@@ -576,7 +588,7 @@ def run_batched(args):
         torch.cuda.synchronize()
         e1.record(ts)
         torch.cuda.synchronize()
-        return max_over_ranks(e0.elapsed_time(e1) / 1e3)
+        return ranks.max(e0.elapsed_time(e1) / 1e3)
 
     def open_sessions(precision):
         ss = [Session(*st, precision=precision, device=local) for st in structs]
@@ -584,120 +596,163 @@ def run_batched(args):
             m.set_pose(poses[0])
         return ss
 
-    n = len(mix)
-    from dynamap_b200.session import Batch
-    # fused batch, frames resident on the device: one launch per stage for
-    # all sessions, one graph per frame
-    ss = open_sessions(prec)
-    bt = Batch(ss)
-    for k in range(args.warmup):
-        bt.submit_device([dev_frames[j].data_ptr() + k * nbytes[j] for j in range(n)])
-        bt.result(strict=False)
+    def ate_mm(track, j):
+        return 1e3 * float(np.sqrt(np.mean([np.sum((a[:3, 3] - b_[:3, 3]) ** 2)
+                                            for a, b_ in zip(track, gt[j])])))
 
-    def fused_device():
-        for k in range(args.warmup, nframes):
-            bt.submit_device([dev_frames[j].data_ptr() + k * nbytes[j] for j in range(n)])
-            bt.result(strict=False)
-    clk = ClockSampler(local)
-    clk.start()
-    t_dev = timed(fused_device)
-    clocks = clk.stop()
-    launches = bt.kernels_per_frame() * args.steps
-    # stage split of the fused frame (profiled pass, not timed above)
-    bt.profile(True)
-    for k in range(args.warmup, min(nframes, args.warmup + 20)):
-        bt.submit_device([dev_frames[j].data_ptr() + k * nbytes[j] for j in range(n)])
-        bt.result(strict=False)
-    ms, nprof = bt.stage_times()
-    stage_ms = {abi.STAGES[i]: ms[i] / max(nprof, 1) for i in range(len(abi.STAGES))}
-    bt.close()
-    for m in ss:
-        m.close()
-    # fused batch, end to end from pinned host memory
-    ss = open_sessions(prec)
-    bt = Batch(ss)
-    for k in range(args.warmup):
-        bt.submit([pinned[j][k] for j in range(n)])
-        bt.result(strict=False)
-
-    def fused_e2e():
-        for k in range(args.warmup, nframes):
-            bt.submit([pinned[j][k] for j in range(n)])
-            bt.result(strict=False)
-    t_e2e = timed(fused_e2e)
-    bt.close()
-    for m in ss:
-        m.close()
-    # per-session graphs on concurrent streams (dyn_sessions_submit)
-    ss = open_sessions(prec)
-    handles = (C.c_void_p * n)(*[m.h.value for m in ss])
-    for k in range(args.warmup):
-        ptrs = (C.c_void_p * n)(*[pinned[j][k].ctypes.data for j in range(n)])
-        abi.check("sessions_submit", lib.dyn_sessions_submit(handles, n, ptrs, None))
-        for m in ss:
-            m.result(strict=False)
-
-    def streams_e2e():
-        for k in range(args.warmup, nframes):
-            ptrs = (C.c_void_p * n)(*[pinned[j][k].ctypes.data for j in range(n)])
-            abi.check("sessions_submit", lib.dyn_sessions_submit(handles, n, ptrs, None))
-            for m in ss:
-                m.result(strict=False)
-    t_streams = timed(streams_e2e)
-    for m in ss:
-        m.close()
     # plain per-frame path: FP32, one frame at a time, waited for
     ss = open_sessions(abi.PRECISION_FP32)
     lat = []
-    for k in range(args.warmup):
+    for k in range(warmup):
         for j, m in enumerate(ss):
             m.submit_device(dev_frames[j].data_ptr() + k * nbytes[j])
             m.result(strict=False)
+    plain_track = [[] for _ in range(n)]
 
     def plain():
-        for k in range(args.warmup, nframes):
+        for k in range(warmup, nframes):
             for j, m in enumerate(ss):
                 h0 = time.perf_counter()
                 m.submit_device(dev_frames[j].data_ptr() + k * nbytes[j])
-                m.result(strict=False)
+                pose, _ = m.result(strict=False)
                 lat.append(time.perf_counter() - h0)
+                plain_track[j].append(pose.astype(np.float64))
     t_plain = timed(plain)
     for m in ss:
         m.close()
-    if rank != 0:
-        ranks.close()
-        return
-    K = args.steps
-    total = world * n * K
+    total = world * n * steps
     lat.sort()
+    plain_ate = [ate_mm(plain_track[j], j) for j in range(n)]
     kinds = {}
     for k_, _, _ in mix:
         kinds[k_] = kinds.get(k_, 0) + 1
+    out = {"sessions": n, "mix": kinds, "steps": steps, "warmup": warmup,
+           "plain": {"fps": total / t_plain, "precision": "fp32",
+                     "latency_ms": {"p50": 1e3 * lat[len(lat) // 2],
+                                    "p99": 1e3 * lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
+                     "ate_gt_mm_mean": float(np.mean(plain_ate))},
+           "forms": {}}
+    for pname in precisions:
+        prec = PRECISIONS[pname]
+        ss = open_sessions(prec)
+        bt = Batch(ss)
+        for k in range(warmup):
+            bt.submit_device([dev_frames[j].data_ptr() + k * nbytes[j] for j in range(n)])
+            bt.result(strict=False)
+        track = [[] for _ in range(n)]
+
+        def fused_device():
+            for k in range(warmup, nframes):
+                bt.submit_device([dev_frames[j].data_ptr() + k * nbytes[j] for j in range(n)])
+                poses, _, _ = bt.result(strict=False)
+                for j in range(n):
+                    track[j].append(poses[j].astype(np.float64))
+        clk = ClockSampler(local)
+        clk.start()
+        t_dev = timed(fused_device)
+        clocks = clk.stop()
+        launches = bt.kernels_per_frame() * steps
+        form = {"fps": total / t_dev, "ms_per_step": 1e3 * t_dev / steps,
+                "speedup_vs_plain": t_plain / t_dev, "gpu_launches": launches,
+                "clocks": clocks}
+        if stage_split:
+            bt.profile(True)
+            for k in range(warmup, min(nframes, warmup + 20)):
+                bt.submit_device([dev_frames[j].data_ptr() + k * nbytes[j] for j in range(n)])
+                bt.result(strict=False)
+            ms, nprof = bt.stage_times()
+            form["stage_ms_per_step"] = {abi.STAGES[i]: ms[i] / max(nprof, 1)
+                                         for i in range(len(abi.STAGES))}
+        bt.close()
+        for m in ss:
+            m.close()
+        ate = [ate_mm(track[j], j) for j in range(n)]
+        dpos = [1e3 * max(float(np.linalg.norm(a[:3, 3] - b_[:3, 3]))
+                          for a, b_ in zip(track[j], plain_track[j])) for j in range(n)]
+        form["ate_gt_mm_mean"] = float(np.mean(ate))
+        form["ate_delta_vs_plain_mm"] = {
+            "max": float(np.max(np.abs(np.array(ate) - np.array(plain_ate)))),
+            "mean": float(np.mean(np.abs(np.array(ate) - np.array(plain_ate))))}
+        form["max_position_diff_vs_plain_mm"] = float(np.max(dpos))
+        if e2e:
+            ss = open_sessions(prec)
+            bt = Batch(ss)
+            for k in range(warmup):
+                bt.submit([pinned[j][k] for j in range(n)])
+                bt.result(strict=False)
+
+            def fused_e2e():
+                for k in range(warmup, nframes):
+                    bt.submit([pinned[j][k] for j in range(n)])
+                    bt.result(strict=False)
+            t_e2e = timed(fused_e2e)
+            bt.close()
+            for m in ss:
+                m.close()
+            form["e2e"] = {"value": total / t_e2e, "unit": "frames/s",
+                           "h2d_bytes_per_step": int(sum(nbytes)),
+                           "d2h_bytes_per_step": int(n * lib.dyn_frame_d2h_bytes())}
+        if streams:
+            ss = open_sessions(prec)
+            handles = (C.c_void_p * n)(*[m.h.value for m in ss])
+            for k in range(warmup):
+                ptrs = (C.c_void_p * n)(*[pinned[j][k].ctypes.data for j in range(n)])
+                abi.check("sessions_submit", lib.dyn_sessions_submit(handles, n, ptrs, None))
+                for m in ss:
+                    m.result(strict=False)
+
+            def streams_e2e():
+                for k in range(warmup, nframes):
+                    ptrs = (C.c_void_p * n)(*[pinned[j][k].ctypes.data for j in range(n)])
+                    abi.check("sessions_submit", lib.dyn_sessions_submit(handles, n, ptrs, None))
+                    for m in ss:
+                        m.result(strict=False)
+            form["streams_e2e_fps"] = total / timed(streams_e2e)
+            for m in ss:
+                m.close()
+        out["forms"][pname] = form
+    del dev_frames
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_batched(args):
+    """--config cfg3: the batched configuration alone (--precision's form)."""
+    import torch
+    from dynamap_b200.replicas import Ranks
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    ranks = Ranks()  # each GPU runs its own session mix: weak scaling
+    r = measure_batched(args, ranks, local, args.sessions, args.steps, args.warmup,
+                        [args.precision], e2e=True, streams=True, stage_split=True)
+    if ranks.rank != 0:
+        ranks.close()
+        return
+    f = r["forms"][args.precision]
+    n, K = r["sessions"], args.steps
     line = {
-        "metric": METRIC, "value": total / t_dev, "unit": "frames/s", "n_gpus": world,
-        "steps": K, "warmup": args.warmup, "ms_per_step": 1e3 * t_dev / K,
+        "metric": METRIC, "value": f["fps"], "unit": "frames/s", "n_gpus": ranks.world,
+        "steps": K, "warmup": args.warmup, "ms_per_step": f["ms_per_step"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic: seeded analytic scenes, one per session",
         "config": {"workload": f"cfg3: {n} sessions per GPU, resolutions "
-                               f"160x120/320x240/640x480 1:2:1 ({kinds}), voxels 10/8/5 mm, "
+                               f"160x120/320x240/640x480 1:2:1 ({r['mix']}), voxels 10/8/5 mm, "
                                "2^18-2^20 buckets, one frame of every session per step, "
                                f"{args.precision}, one fused launch per stage for all "
                                "sessions (dyn_batch), one CUDA graph per frame; plain = "
                                "FP32 sessions one frame at a time",
                    "sessions_per_gpu": n, "precision": args.precision,
                    "l2": "per-step inputs and volumes exceed L2"},
-        "plain_fps": total / t_plain,
-        "speedup_vs_plain": t_plain / t_dev,
-        "plain_latency_ms": {"p50": 1e3 * lat[len(lat) // 2],
-                             "p99": 1e3 * lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
-        "step_ms": {"frame_of_all_sessions": 1e3 * t_dev / K},
-        "stage_ms_per_step": stage_ms,
-        "streams_e2e_fps": total / t_streams,
-        "gpu_launches": launches,
-        "clocks": clocks,
-        "e2e": {"value": total / t_e2e, "unit": "frames/s",
-                "h2d_bytes_per_step": int(sum(nbytes)),
-                "d2h_bytes_per_step": int(n * lib.dyn_frame_d2h_bytes())},
+        "plain_fps": r["plain"]["fps"],
+        "speedup_vs_plain": f["speedup_vs_plain"],
+        "plain_latency_ms": r["plain"]["latency_ms"],
+        "ate_delta_vs_plain_mm": f["ate_delta_vs_plain_mm"],
+        "step_ms": {"frame_of_all_sessions": f["ms_per_step"]},
+        "stage_ms_per_step": f.get("stage_ms_per_step"),
+        "streams_e2e_fps": f.get("streams_e2e_fps"),
+        "gpu_launches": f["gpu_launches"],
+        "clocks": f["clocks"],
+        "e2e": f["e2e"],
     }
     print(json.dumps(line), flush=True)
     ranks.close()
@@ -821,23 +876,25 @@ def run_large(args):
     ranks.close()
 
 
-def run_serving(args):
+def measure_serving(args, ranks, local, seconds, precision, clip_frames=16):
     """The serving configuration: sessions arrive as a Poisson process, are
     admitted by HBM budget into one dyn_server and stream depth at 30 Hz for
     their duration; the host loop pushes every due frame (the newest one when
     a session is behind: older due frames are dropped and counted), steps
     the server whenever frames wait (one fused step for all of them, at most
     two steps in flight) and releases sessions when their stream ends.
-    value = frames completed per second of the run; latency = frame due
-    time -> step completion seen by the host loop."""
+    Every session has its own seeded scene and trajectory, rendered as a
+    clip of clip_frames frames that its stream replays forth and back.
+    Returns frames completed per second of the run and the latency of each
+    frame from its due time to the completion of its step."""
     import numpy as np
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
     from dynamap_b200 import configs
+    from dynamap_b200.session import Server
+    world, rank = ranks.world, ranks.rank
     S = configs.SERVING
     rng = np.random.default_rng(args.seed * 7919 + rank)
-    T = float(args.serve_seconds)
+    T = float(seconds)
     arrivals = []
     t = 0.0
     while True:
@@ -846,59 +903,56 @@ def run_serving(args):
             break
         arrivals.append((t, str(rng.choice(S["kinds"])), float(rng.uniform(*S["duration_s"]))))
     kinds = sorted(set(S["kinds"]))
-    n_pool = 24
     workers = max(1, min(32, ((os.cpu_count() or 2) - 1) // max(world, 1)))
-    pools = dict(zip(kinds, make_many([(configs.serving_kind(k, n_pool), 500 + i)
-                                       for i, k in enumerate(kinds)], n_pool, workers)))
-    import torch
-    from dynamap_b200 import abi
-    from dynamap_b200.replicas import Ranks
-    from dynamap_b200.session import Server
-    torch.cuda.set_device(local)
-    ranks = Ranks()  # each GPU serves its own arrivals: weak scaling
-    # page-locked frame pools: the server's steps read them directly
-    pinned = {k: torch.from_numpy(v[0]).pin_memory() for k, v in pools.items()}
-    pin_np = {k: v.numpy() for k, v in pinned.items()}
-    structs = {k: configs.structs(configs.serving_kind(k, n_pool)) for k in kinds}
-    prec = PRECISIONS[args.precision]
+    warm = [(configs.serving_kind(k, clip_frames), 500 + i) for i, k in enumerate(kinds)]
+    jobs = warm + [(configs.serving_kind(kind, clip_frames), 20000 + 1000 * rank + j)
+                   for j, (_, kind, _) in enumerate(arrivals)]
+    clips = make_many(jobs, clip_frames, workers)
+    # page-locked clips: the server's steps read them directly
+    pin = [torch.from_numpy(d).pin_memory() for d, _, _ in clips]
+    pin_np = [x.numpy() for x in pin]
+    structs = {k: configs.structs(configs.serving_kind(k, clip_frames)) for k in kinds}
+    prec = PRECISIONS[precision]
     sv = Server(budget_bytes=int(S["budget_gb"] * 1e9), max_sessions=1024, device=local)
     fps = S["fps"]
     waiting, active = [], {}
     lat, drops, refused_waits, admitted, peak, frames_done = [], 0, 0, 0, 0, 0
     inflight = {}   # slot -> (step id, due time)
     queued = set()  # slots with a frame pushed for the next step
-    step_slots = []
     ai = 0
     # warm-up (untimed): one session of each kind through a few frames, so
     # that module loading and first-launch costs stay out of the run
-    for kind in kinds:
+    for i, kind in enumerate(kinds):
         t_, g_, b_, s_ = structs[kind]
-        slot = sv.admit(t_, g_, b_, s_, precision=prec, pose0=pools[kind][2][0])
+        slot = sv.admit(t_, g_, b_, s_, precision=prec, pose0=clips[i][2][0])
         for k in range(3):
-            sv.push(slot, pin_np[kind][k])
+            sv.push(slot, pin_np[i][k])
             sv.step()
             sv.result(slot, strict=False)
         sv.release(slot)
     sv.sync()
     ranks.barrier()
+    n_pool = clip_frames
     clk = ClockSampler(local)
     clk.start()
     t0 = time.perf_counter()
     while True:
         now = time.perf_counter() - t0
         while ai < len(arrivals) and arrivals[ai][0] <= now:
-            waiting.append(arrivals[ai])
+            waiting.append((ai,) + arrivals[ai])
             ai += 1
         while waiting:  # FIFO admission
-            ta, kind, dur = waiting[0]
+            j, ta, kind, dur = waiting[0]
             t_, g_, b_, s_ = structs[kind]
-            slot = sv.admit(t_, g_, b_, s_, precision=prec, pose0=pools[kind][2][0])
+            clip = len(kinds) + j
+            slot = sv.admit(t_, g_, b_, s_, precision=prec, pose0=clips[clip][2][0])
             if slot is None:
                 refused_waits += 1
                 break
             waiting.pop(0)
             admitted += 1
-            active[slot] = dict(kind=kind, start=now, end=now + dur, k=0, last_due=None)
+            active[slot] = dict(kind=kind, clip=clip, start=now, end=now + dur, k=0,
+                                last_due=None)
         peak = max(peak, len(active))
         u = sv.usage()
         done_steps = u["steps_done"]
@@ -919,8 +973,8 @@ def run_serving(args):
                 continue
             drops += due_k - a["k"]  # frames that came due while the slot was busy
             i = due_k % (2 * n_pool - 2)
-            i = i if i < n_pool else 2 * n_pool - 2 - i  # ping-pong through the pool
-            assert sv.push(slot, pin_np[a["kind"]][i])
+            i = i if i < n_pool else 2 * n_pool - 2 - i  # forth and back through the clip
+            assert sv.push(slot, pin_np[a["clip"]][i])
             a["k"] = due_k + 1
             a["last_due"] = a["start"] + due_k / fps
             queued.add(slot)
@@ -940,31 +994,53 @@ def run_serving(args):
     sv.sync()
     usage = sv.usage()
     sv.close()
+    del pin
     tot = (ranks.sum(frames_done), ranks.max(elapsed))
-    if rank == 0:
-        lat.sort()
-        q = lambda f: 1e3 * lat[min(len(lat) - 1, int(f * len(lat)))] if lat else None
-        line = {
-            "metric": METRIC, "value": float(tot[0] / tot[1]), "unit": "frames/s",
-            "n_gpus": world, "steps": int(usage["steps"]), "warmup": 0,
-            "ms_per_step": 1e3 * elapsed / max(1, usage["steps"]), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None,
-            "dtype": "f16/u16 voxels" if prec else "f32",
-            "data": "synthetic: 24-frame seeded sequences per resolution, replayed forth "
-                    "and back",
-            "config": {"workload": f"cfg4: Poisson arrivals {S['rate_per_s']}/s for {T:.0f} s, "
-                                   f"durations U{list(S['duration_s'])} s, {fps:.0f} Hz depth, "
-                                   "320x240/640x480/1280x720 at 2:2:1, 84/168/336 MB hash "
-                                   f"tables, {S['budget_gb']:.0f} GB budget, {args.precision}",
-                       "precision": args.precision, "serve_seconds": T},
+    lat.sort()
+    q = lambda f: 1e3 * lat[min(len(lat) - 1, int(f * len(lat)))] if lat else None
+    return {"fps": float(tot[0] / tot[1]), "seconds": T, "elapsed_s": elapsed,
+            "precision": precision,
             "latency_ms": {"p50": q(0.5), "p99": q(0.99), "max": q(1.0),
                            "what": "frame due time -> step completion seen by the host loop"},
             "frames_completed": int(frames_done), "frames_dropped": int(drops),
             "sessions_admitted": admitted, "sessions_arrived": len(arrivals),
             "sessions_peak": peak, "admission_waits": refused_waits,
-            "budget_bytes": int(usage["budget_bytes"]),
-            "clocks": clocks,
-            "e2e": {"value": float(tot[0] / tot[1]), "unit": "frames/s",
+            "steps": int(usage["steps"]), "budget_bytes": int(usage["budget_bytes"]),
+            "clip_frames": clip_frames, "clocks": clocks}
+
+
+def run_serving(args):
+    """--config cfg4: the serving configuration alone."""
+    import torch
+    from dynamap_b200 import configs
+    from dynamap_b200.replicas import Ranks
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    ranks = Ranks()  # each GPU serves its own arrivals: weak scaling
+    r = measure_serving(args, ranks, local, args.serve_seconds, args.precision)
+    S = configs.SERVING
+    if ranks.rank == 0:
+        line = {
+            "metric": METRIC, "value": r["fps"], "unit": "frames/s",
+            "n_gpus": ranks.world, "steps": r["steps"], "warmup": 0,
+            "ms_per_step": 1e3 * r["elapsed_s"] / max(1, r["steps"]), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f16/u16 voxels" if PRECISIONS[args.precision] else "f32",
+            "data": f"synthetic: every session its own seeded scene and trajectory, a "
+                    f"{r['clip_frames']}-frame clip its stream replays forth and back",
+            "config": {"workload": f"cfg4: Poisson arrivals {S['rate_per_s']}/s for "
+                                   f"{r['seconds']:.0f} s, durations U{list(S['duration_s'])} s, "
+                                   f"{S['fps']:.0f} Hz depth, 320x240/640x480/1280x720 at 2:2:1, "
+                                   f"84/168/336 MB hash tables, {S['budget_gb']:.0f} GB budget, "
+                                   f"{args.precision}",
+                       "precision": args.precision, "serve_seconds": r["seconds"]},
+            "latency_ms": r["latency_ms"],
+            "frames_completed": r["frames_completed"], "frames_dropped": r["frames_dropped"],
+            "sessions_admitted": r["sessions_admitted"],
+            "sessions_arrived": r["sessions_arrived"], "sessions_peak": r["sessions_peak"],
+            "admission_waits": r["admission_waits"], "budget_bytes": r["budget_bytes"],
+            "clocks": r["clocks"],
+            "e2e": {"value": r["fps"], "unit": "frames/s",
                     "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
                     "note": "the serving loop is end to end: host frames in, poses out"},
         }
@@ -992,6 +1068,12 @@ def main():
     ap.add_argument("--sessions", type=int, default=32, help="sessions per GPU (cfg3)")
     ap.add_argument("--serve-seconds", type=float, default=40.0,
                     help="arrival window of the serving run (cfg4)")
+    ap.add_argument("--no-batched", dest="batched", action="store_false",
+                    help="skip the batched block (cfg3 mix) of the default run")
+    ap.add_argument("--no-serving", dest="serving", action="store_false",
+                    help="skip the serving block (cfg4, shortened) of the default run")
+    ap.add_argument("--embed-serve-seconds", type=float, default=20.0,
+                    help="arrival window of the default run's serving block")
     ap.add_argument("--precision", default="fp32", choices=sorted(PRECISIONS),
                     help="fp32: the drop-in path; mixed: f16/u16 voxels, compensated "
                          "normal equations, fast raycast; band: mixed with band-limited "

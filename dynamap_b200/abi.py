@@ -120,6 +120,7 @@ SIGNATURES = {
     "dyn_integrate_with_pose": (C.c_int, [_vp, _vp, _vp, P(C.c_float)]),
     "dyn_raycast": (C.c_int, [_vp, P(C.c_float), P(Sensor), _vp, _vp]),
     "dyn_num_blocks": (C.c_int, [_vp, P(C.c_int64)]),
+    "dyn_find_blocks": (C.c_int, [_vp, _vp, C.c_int64, _vp]),
     "dyn_download_blocks": (C.c_int, [_vp, _vp, _vp, C.c_int64, P(C.c_int64)]),
     "dyn_extract_mesh": (C.c_int, [_vp, P(C.c_float), P(C.c_float), _vp, C.c_int64,
                                    P(C.c_int64)]),
@@ -129,6 +130,7 @@ SIGNATURES = {
     "dyn_debug_image": (C.c_int, [_vp, C.c_int32, C.c_int32, _vp, C.c_size_t]),
     "dyn_bilateral_filter": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint32, P(BilateralParams), _vp]),
     "dyn_depth_to_maps": (C.c_int, [_vp, P(Sensor), _vp, _vp, _vp]),
+    "dyn_depth_to_maps_host": (C.c_int, [_vp, P(Sensor), _vp, _vp]),
     "dyn_icp_normal_equations": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, P(Sensor), P(GnParams),
                                            P(C.c_float), P(C.c_double), _vp]),
     "dyn_sessions_submit": (C.c_int, [P(_vp), C.c_int32, P(_vp), P(_vp)]),

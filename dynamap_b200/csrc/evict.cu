@@ -109,6 +109,10 @@ dyn_status remove_blocks(dyn_session* s, Mark mark, int32_t* coords_out, dyn_vox
       e = cudaMemsetAsync(s->vol.vox16 + from, 0, sizeof(unsigned) * tail, st);
     if (e == cudaSuccess && s->vol.colors)
       e = cudaMemsetAsync(s->vol.colors + from, 0, sizeof(uchar4) * tail, st);
+    if (e == cudaSuccess && s->vol.nonsat)
+      e = cudaMemsetAsync(s->vol.nonsat + L, 0, sizeof(int) * (size_t)(n - L), st);
+    if (e == cudaSuccess && s->vol.freecell)
+      e = cudaMemsetAsync(s->vol.freecell + L, 0, (size_t)(n - L), st);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(&s->vol.cnt->nalloc, &L, sizeof(int), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // the copy reads L from this stack

@@ -145,7 +145,13 @@ __global__ void move_kernel(VolumeDev v, int n, int L, const int* __restrict__ d
         for (int q = threadIdx.x; q < kBlockVox * 4 / 16; q += blockDim.x) e4[q] = c4[q];
       }
     }
-    if (threadIdx.x == 0) v.block_keys[d] = v.block_keys[j];
+    if (threadIdx.x == 0) {
+      v.block_keys[d] = v.block_keys[j];
+      if (v.nonsat) {  // the free-space summaries move with the block
+        v.nonsat[d] = v.nonsat[j];
+        v.freecell[d] = v.freecell[j];
+      }
+    }
   }
 }
 
@@ -164,11 +170,16 @@ __global__ void rewrite_kernel(Entry* entries, int nbuckets, int bsz, int n,
 // "present".  Whichever CTA moves the entry's ptr from -1 to the claim mark
 // -3 gives it its heap index, so a key that occurs twice is placed once.
 // counts: [placed, present, bucket full, heap exhausted].
+// A placed block's free-space summaries: its count of observed,
+// non-saturated voxels, its own free-cell flag cleared (set again by the
+// next frame that sees it), and, when it holds such voxels, the flags of
+// its seven lower neighbours cleared (their cells read it).
 __global__ void upload_kernel(VolumeDev v, const PoseState* __restrict__ ps,
                               const int* __restrict__ coords, const dyn_voxel* __restrict__ vox,
                               int m, int* __restrict__ counts) {
   __shared__ int ptr_s;
   __shared__ int unique_s;  // bucket_insert's probe count (unused here)
+  __shared__ int nonsat_s;
   for (int k = blockIdx.x; k < m; k += gridDim.x) {
     if (threadIdx.x == 0) {
       const unsigned long long key = pack_key(coords[3 * k], coords[3 * k + 1], coords[3 * k + 2]);
@@ -192,23 +203,41 @@ __global__ void upload_kernel(VolumeDev v, const PoseState* __restrict__ ps,
         atomicAdd(&counts[1], 1);  // present with a block (or placed by another CTA)
       }
       ptr_s = ptr;
+      nonsat_s = 0;
     }
     __syncthreads();
     const int ptr = ptr_s;
     if (ptr >= 0) {
+      int ns = 0;
       for (int j = threadIdx.x; j < kBlockVox; j += blockDim.x) {
         const dyn_voxel o = vox[(size_t)k * kBlockVox + j];
         const size_t i = (size_t)ptr * kBlockVox + j;
         if (!v.fp16) {
           v.voxels[i] = o;
+          ns += o.weight != 0 && !(o.sdf >= v.t.sat_lo);
         } else {
           const __half h = __float2half_rn(o.sdf / v.t.trunc);
           v.vox16[i] = (unsigned)__half_as_ushort(h) | ((unsigned)o.weight << 16);
           if (v.colors) v.colors[i] = make_uchar4(o.r, o.g, o.b, 0);
+          ns += o.weight != 0 && __half_as_ushort(h) != 0x3C00u;
+        }
+      }
+      if (ns) atomicAdd(&nonsat_s, ns);
+    }
+    __syncthreads();
+    if (ptr >= 0 && threadIdx.x == 0 && v.nonsat) {
+      v.nonsat[ptr] = nonsat_s;
+      v.freecell[ptr] = 0;
+      if (nonsat_s) {
+        const int x = coords[3 * k], y = coords[3 * k + 1], z = coords[3 * k + 2];
+        for (int q = 1; q < 8; ++q) {
+          const int lo = find_block(v.entries, v.t, x - (q & 1), y - ((q >> 1) & 1),
+                                    z - ((q >> 2) & 1));
+          if (lo >= 0) v.freecell[lo] = 0;
         }
       }
     }
-    __syncthreads();  // ptr_s is rewritten for the next block
+    __syncthreads();  // ptr_s and nonsat_s are rewritten for the next block
   }
 }
 

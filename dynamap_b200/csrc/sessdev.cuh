@@ -105,6 +105,7 @@ void fused_reset_counters(const SessDev* tab, const BatchShape& b, cudaStream_t 
 void fused_allocate(const SessDev* tab, const BatchShape& b, cudaStream_t st);
 void fused_visible(const SessDev* tab, const BatchShape& b, cudaStream_t st);
 void fused_integrate(const SessDev* tab, const BatchShape& b, cudaStream_t st);
+void fused_free_cells(const SessDev* tab, const BatchShape& b, cudaStream_t st);
 void fused_raycast(const SessDev* tab, const BatchShape& b, cudaStream_t st);
 
 }  // namespace dyn

@@ -150,6 +150,7 @@ void enqueue_map_update(const SessDev* tab, const BatchShape& b, cudaStream_t st
   fused_visible(tab, b, st);
   m(DYN_STAGE_VISIBLE);
   fused_integrate(tab, b, st);
+  fused_free_cells(tab, b, st);
   m(DYN_STAGE_INTEGRATE);
   fused_raycast(tab, b, st);
   m(DYN_STAGE_RAYCAST);
@@ -463,6 +464,7 @@ size_t session_bytes(const dyn_tsdf_params& t, const dyn_sensor& s, int precisio
   else
     b += sizeof(dyn_voxel) * (size_t)t.num_blocks * kBlockVox;
   b += sizeof(int2) * (size_t)t.num_blocks;  // visible list
+  b += (sizeof(int) + 1) * (size_t)t.num_blocks;  // free-space summaries
   b += n * (2 + 3 + 4 + 4 + 4 + 3);  // inputs, raw, filtered, ray depth, target rgb
   if (precision == DYN_PRECISION_MIXED_BAND)
     b += 4 * (size_t)((s.rows + 7) / 8) * ((s.cols + 7) / 8) + 256;  // ray-start bound
@@ -572,6 +574,8 @@ dyn_status alloc_device_buffers(dyn_session* s) {
   } else {
     DYN_TRY(s->dalloc(&s->vol.voxels, sizeof(dyn_voxel) * nvox));
   }
+  DYN_TRY(s->dalloc(&s->vol.nonsat, sizeof(int) * (size_t)tsdf->num_blocks));
+  DYN_TRY(s->dalloc(&s->vol.freecell, (size_t)tsdf->num_blocks));
   DYN_TRY(s->dalloc(&s->vol.cnt, sizeof(Counters)));
   DYN_TRY(s->dalloc(&s->d_gvis, sizeof(int2) * (size_t)tsdf->num_blocks));
   s->rb_tx = ((int)s->sensor.cols + 7) / 8;
@@ -952,6 +956,41 @@ dyn_status dyn_num_blocks(dyn_session* s, int64_t* n_out) {
   return DYN_OK;
 }
 
+dyn_status dyn_find_blocks(dyn_session* s, const int32_t* coords, int64_t n,
+                           int32_t* heap_index_out) {
+  if (!s || n < 0 || (n > 0 && (!coords || !heap_index_out))) return DYN_ERR_INVALID_ARG;
+  if (n == 0) return DYN_OK;
+  if (n > (int64_t)1 << 30) return DYN_ERR_INVALID_ARG;
+  DeviceGuard dg(s->device);
+  DYN_TRY(quiesce(s));
+  cudaStream_t st = s->stream;
+  int32_t* dc = nullptr;
+  int32_t* dp = nullptr;
+  dyn_status r = DYN_OK;
+  do {
+    if (cudaMallocAsync(&dc, sizeof(int32_t) * 3 * (size_t)n, st) != cudaSuccess ||
+        cudaMallocAsync(&dp, sizeof(int32_t) * (size_t)n, st) != cudaSuccess) {
+      r = DYN_ERR_OOM;
+      break;
+    }
+    if (cudaMemcpyAsync(dc, coords, sizeof(int32_t) * 3 * (size_t)n, cudaMemcpyHostToDevice,
+                        st) != cudaSuccess) {
+      r = DYN_ERR_CUDA;
+      break;
+    }
+    launch_find_blocks(s->vol, dc, (int)n, dp, st);
+    if (cudaGetLastError() != cudaSuccess ||
+        cudaMemcpyAsync(heap_index_out, dp, sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToHost,
+                        st) != cudaSuccess)
+      r = DYN_ERR_CUDA;
+  } while (false);
+  if (r != DYN_OK) cudaGetLastError();
+  for (void* p : {(void*)dc, (void*)dp})
+    if (p) cudaFreeAsync(p, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess && r == DYN_OK) r = DYN_ERR_CUDA;
+  return r;
+}
+
 dyn_status dyn_download_blocks(dyn_session* s, int32_t* coords_out, dyn_voxel* voxels_out,
                                int64_t capacity, int64_t* n_out) {
   if (!s || !n_out || capacity < 0) return DYN_ERR_INVALID_ARG;
@@ -1091,6 +1130,41 @@ dyn_status dyn_bilateral_filter(const float* depth_dev, float* out_dev, uint32_t
   launch_bilateral(depth_dev, out_dev, (int)rows, (int)cols, tb, (cudaStream_t)stream);
   DYN_CUDA(cudaGetLastError());
   return DYN_OK;
+}
+
+dyn_status dyn_depth_to_maps_host(const float* depth_host, const dyn_sensor* level,
+                                  float* vertex4_host, float* normal4_host) {
+  if (!depth_host || !valid_sensor(level) || !normal4_host) return DYN_ERR_INVALID_ARG;
+  const size_t n = (size_t)level->rows * level->cols;
+  cudaStream_t st = cudaStreamPerThread;
+  float* d = nullptr;
+  float4* v = nullptr;
+  float4* nm = nullptr;
+  dyn_status r = DYN_OK;
+  do {
+    if (cudaMallocAsync(&d, n * 4, st) != cudaSuccess ||
+        cudaMallocAsync(&nm, n * 16, st) != cudaSuccess ||
+        (vertex4_host && cudaMallocAsync(&v, n * 16, st) != cudaSuccess)) {
+      r = DYN_ERR_OOM;
+      break;
+    }
+    if (cudaMemcpyAsync(d, depth_host, n * 4, cudaMemcpyHostToDevice, st) != cudaSuccess) {
+      r = DYN_ERR_CUDA;
+      break;
+    }
+    r = dyn_depth_to_maps(d, level, reinterpret_cast<float*>(v), reinterpret_cast<float*>(nm),
+                          st);
+    if (r != DYN_OK) break;
+    if (cudaMemcpyAsync(normal4_host, nm, n * 16, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        (vertex4_host &&
+         cudaMemcpyAsync(vertex4_host, v, n * 16, cudaMemcpyDeviceToHost, st) != cudaSuccess))
+      r = DYN_ERR_CUDA;
+  } while (false);
+  if (r != DYN_OK) cudaGetLastError();
+  for (void* p : {(void*)d, (void*)v, (void*)nm})
+    if (p) cudaFreeAsync(p, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess && r == DYN_OK) r = DYN_ERR_CUDA;
+  return r;
 }
 
 dyn_status dyn_depth_to_maps(const float* depth_dev, const dyn_sensor* level, float* vertex4_dev,

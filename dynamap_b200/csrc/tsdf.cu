@@ -394,8 +394,10 @@ __device__ inline float norm3_fast(F3 v) {
   return q > 0.0f ? q * rsqrtf(q) : 0.0f;
 }
 
+// Returns the change of the block's count of observed, non-saturated voxels
+// (-1, 0 or +1) that this voxel's update makes (0 when it is not updated).
 template <bool FP16, bool FAST>
-__device__ inline void integrate_voxel(const VolumeDev& v, const float* __restrict__ depth,
+__device__ inline int integrate_voxel(const VolumeDev& v, const float* __restrict__ depth,
                                        const float* __restrict__ sdist,
                                        const uint8_t* __restrict__ rgb, const DSensor& s,
                                        const M4f& invT, int ptr, int lin) {
@@ -415,27 +417,27 @@ __device__ inline void integrate_voxel(const VolumeDev& v, const float* __restri
   float sd, vd, d;
   if (FAST) {
     vp = xform_fma(invT, vp);
-    if (!(vp.z > 0.0f)) return;
+    if (!(vp.z > 0.0f)) return 0;
     const float rz = __fdividef(1.0f, vp.z);
     const float xf = __fmaf_rn(s.fx * vp.x, rz, s.cx), yf = __fmaf_rn(s.fy * vp.y, rz, s.cy);
-    if (!(fabsf(xf) < 2e9f) || !(fabsf(yf) < 2e9f)) return;
+    if (!(fabsf(xf) < 2e9f) || !(fabsf(yf) < 2e9f)) return 0;
     px = (int)roundf(xf);
     py = (int)roundf(yf);
-    if (!(px >= 0 && py >= 0 && px < s.cols && py < s.rows)) return;
+    if (!(px >= 0 && py >= 0 && px < s.cols && py < s.rows)) return 0;
     d = __ldg(depth + py * s.cols + px);
-    if (d < t.dmin) return;
-    if (d > t.dmax) return;
+    if (d < t.dmin) return 0;
+    if (d > t.dmax) return 0;
     const F3 p3 = f3(__fdividef(((float)px - s.cx) * d, s.fx),
                      __fdividef(((float)py - s.cy) * d, s.fy), d);
     sd = norm3_fast(p3);
     vd = norm3_fast(vp);
   } else {
     vp = xform(invT, vp);
-    if (!project(vp, s, &px, &py)) return;
-    if (!(px >= 0 && py >= 0 && px < s.cols && py < s.rows)) return;
+    if (!project(vp, s, &px, &py)) return 0;
+    if (!(px >= 0 && py >= 0 && px < s.cols && py < s.rows)) return 0;
     d = __ldg(depth + py * s.cols + px);
-    if (d < t.dmin) return;
-    if (d > t.dmax) return;
+    if (d < t.dmin) return 0;
+    if (d > t.dmax) return 0;
     sd = __ldg(sdist + py * s.cols + px);  // norm3(point3d_uv(px, py, d, s))
     vd = norm3(vp);
   }
@@ -443,7 +445,7 @@ __device__ inline void integrate_voxel(const VolumeDev& v, const float* __restri
   float sdf;
   if (vd > sd - t.trunc && vd < sd + t.trunc && d < t.dmax) sdf = sd - vd;
   else if (vd < sd - t.trunc) sdf = t.trunc;
-  else return;
+  else return 0;
   uint8_t c0 = 0, c1 = 0, c2 = 0;
   if (rgb) {
     c0 = __ldg(rgb + 3 * (size_t)idx);
@@ -462,8 +464,8 @@ __device__ inline void integrate_voxel(const VolumeDev& v, const float* __restri
     const float nsdf = __fdividef(osdf * fw + sdf, fw + 1.0f);
     int nw = w + 1;
     if (nw > t.max_w) nw = t.max_w;
-    v.vox16[vi] = (unsigned)__half_as_ushort(__float2half_rn(__fdividef(nsdf, t.trunc))) |
-                  ((unsigned)nw << 16);
+    const unsigned short nh = __half_as_ushort(__float2half_rn(__fdividef(nsdf, t.trunc)));
+    v.vox16[vi] = (unsigned)nh | ((unsigned)nw << 16);
     if (v.colors) {
       uchar4 c = v.colors[vi];
       // colour exactly as the FP32 form (truncated to bytes)
@@ -472,7 +474,9 @@ __device__ inline void integrate_voxel(const VolumeDev& v, const float* __restri
       c.z = (uint8_t)(((float)c.z * fw + (float)c2 * 1.0f) / (fw + 1.0f));
       v.colors[vi] = c;
     }
-    return;
+    // saturated: f16 value exactly 1 (free space); unobserved before
+    const bool was = w == 0 || (raw & 0xffffu) == 0x3C00u, now = nh == 0x3C00u;
+    return (int)was - (int)now;
   }
   dyn_voxel* vox = v.voxels + vi;
   uint2 raw = *reinterpret_cast<const uint2*>(vox);
@@ -494,6 +498,8 @@ __device__ inline void integrate_voxel(const VolumeDev& v, const float* __restri
   out.x = (unsigned)r0 | ((unsigned)r1 << 8) | ((unsigned)r2 << 16) | ((unsigned)nw << 24);
   out.y = __float_as_uint(nsdf);
   *reinterpret_cast<uint2*>(vox) = out;
+  const bool was = w == 0 || osdf >= t.sat_lo, now = nsdf >= t.sat_lo;
+  return (int)was - (int)now;
 }
 
 // the batch-wide visible list: each item (session, block) by one CTA
@@ -515,12 +521,57 @@ __global__ void __launch_bounds__(kBlockVox)
     }
     const SessDev& S = tab[item.x];
     const uint8_t* rgb = *S.rgb_flag ? S.rgb : nullptr;
+    int d;
     if (!S.vol.fp16)
-      integrate_voxel<false, false>(S.vol, S.raw, S.sdist, rgb, S.ls[0], invT, item.y, threadIdx.x);
+      d = integrate_voxel<false, false>(S.vol, S.raw, S.sdist, rgb, S.ls[0], invT, item.y,
+                                        threadIdx.x);
     else if (S.vol.t.band)
-      integrate_voxel<true, true>(S.vol, S.raw, S.sdist, rgb, S.ls[0], invT, item.y, threadIdx.x);
+      d = integrate_voxel<true, true>(S.vol, S.raw, S.sdist, rgb, S.ls[0], invT, item.y,
+                                      threadIdx.x);
     else
-      integrate_voxel<true, false>(S.vol, S.raw, S.sdist, rgb, S.ls[0], invT, item.y, threadIdx.x);
+      d = integrate_voxel<true, false>(S.vol, S.raw, S.sdist, rgb, S.ls[0], invT, item.y,
+                                       threadIdx.x);
+    // the block's non-saturated count follows its voxels exactly (one CTA
+    // per visible block, so the owner thread updates it alone)
+    const int up = __syncthreads_count(d > 0), down = __syncthreads_count(d < 0);
+    if (threadIdx.x == 0 && up != down && S.vol.nonsat) S.vol.nonsat[item.y] += up - down;
+  }
+}
+
+// Free-cell flags of the visible blocks (after their integration): a block's
+// flag is set when it and its seven upper neighbours (+x, +y, +z and their
+// combinations; missing ones count as free) hold no observed non-saturated
+// voxel.  A visible block that holds one clears the flags of its seven lower
+// neighbours, whose cells read it; those may be blocks that are not visible
+// this frame.  Both writers of a flag agree: a block whose flag a neighbour
+// clears computes 0 for itself.  Flags are only ever set here, for visible
+// blocks, so a flag is never 1 where a cell of its block reads a
+// non-saturated voxel.
+__global__ void fused_free_cells_kernel(const SessDev* __restrict__ tab,
+                                        const int2* __restrict__ gvis,
+                                        const int* __restrict__ gcount) {
+  const int n = *gcount;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int2 item = gvis[i];
+    const VolumeDev& v = tab[item.x].vol;
+    if (!v.freecell) continue;
+    const unsigned long long key = v.block_keys[item.y];
+    const int x = key_x(key), y = key_y(key), z = key_z(key);
+    const bool own = v.nonsat[item.y] == 0;
+    bool free = own && v.t.free_ok;
+#pragma unroll
+    for (int k = 1; k < 8; ++k) {
+      const int dx = k & 1, dy = (k >> 1) & 1, dz = (k >> 2) & 1;
+      if (free) {
+        const int p = find_block(v.entries, v.t, x + dx, y + dy, z + dz);
+        if (p >= 0 && v.nonsat[p] != 0) free = false;
+      }
+      if (!own) {
+        const int q = find_block(v.entries, v.t, x - dx, y - dy, z - dz);
+        if (q >= 0) v.freecell[q] = 0;
+      }
+    }
+    v.freecell[item.y] = free ? 1 : 0;
   }
 }
 
@@ -534,6 +585,7 @@ struct VoxelSample {
 struct BlockCache {
   int x, y, z;
   int ptr;
+  int free;  // the block's free-cell flag (cell_block_free)
 };
 
 // voxel_index, blk_of and loc_of (WorldToGlobalVoxelHashing / WorldToBlock /
@@ -551,19 +603,8 @@ __device__ inline int block_ptr(const VolumeDev& v, int bx, int by, int bz, Bloc
   }
   return bc.ptr;
 }
-__device__ inline uint2 load_voxel(const VolumeDev& v, int ptr, int lin) {
-  if (ptr < 0) return make_uint2(0u, 0u);
-  return __ldg(reinterpret_cast<const uint2*>(v.voxels + (size_t)ptr * kBlockVox + lin));
-}
 __device__ inline int lin_of(int gx, int gy, int gz) {
   return (loc_of(gx) << 6) | (loc_of(gy) << 3) | loc_of(gz);
-}
-
-__device__ inline uint2 get_voxel(const VolumeDev& v, F3 pos, float inv_vs, BlockCache& bc) {
-  const float vs = v.t.vs;
-  int gx = voxel_index(pos.x, vs, inv_vs), gy = voxel_index(pos.y, vs, inv_vs),
-      gz = voxel_index(pos.z, vs, inv_vs);
-  return load_voxel(v, block_ptr(v, blk_of(gx), blk_of(gy), blk_of(gz), bc), lin_of(gx, gy, gz));
 }
 
 __device__ inline int vw(uint2 r) { return (int)(r.x >> 24); }
@@ -597,159 +638,74 @@ __device__ inline int corner_block(const CellBlocks& cb, bool cx, bool cy, bool 
             : (ky ? (kz ? cb.pyz : cb.py) : (kz ? cb.pz : cb.p0));
 }
 
-// tsdfVolume::GetInterpolatedVoxel, tsdf.cu:47-175.  The eight corners are
-// pos_dual + {0, vs} per axis, so each axis has two coordinate values: they
-// are resolved once (six index computations instead of twenty-four) and
-// combined per corner; every corner still gets exactly the reference's
-// float coordinate.  When the 2x2x2 corners lie in one block (the common
-// case) the block is resolved once.  Corners are summed in the reference's
-// order.  COLOR false skips the colour sums (the marching loop only reads
-// sdf and weight).
-template <bool COLOR>
-__device__ inline VoxelSample get_interpolated(const VolumeDev& v, F3 position, float inv_vs,
-                                               BlockCache& bc) {
-  VoxelSample out;
-  uint2 v0 = get_voxel(v, position, inv_vs, bc);
-  out.w = vw(v0);
-  if (out.w == 0) {
-    out.sdf = vsdf(v0);
-    out.r = (float)(v0.x & 0xff);
-    out.g = (float)((v0.x >> 8) & 0xff);
-    out.b = (float)((v0.x >> 16) & 0xff);
-    return out;
-  }
-  const float vs = v.t.vs;
-  F3 pos_dual = position - f3(vs / 2.0f, vs / 2.0f, vs / 2.0f);
-  const float inv = 1.0f / vs;
-  F3 vp = position * inv;
-  F3 wt = f3(vp.x - floorf(vp.x), vp.y - floorf(vp.y), vp.z - floorf(vp.z));
-  int gx[2], gy[2], gz[2];
-  gx[0] = voxel_index(pos_dual.x + 0.0f, vs, inv_vs);
-  gx[1] = voxel_index(pos_dual.x + vs, vs, inv_vs);
-  gy[0] = voxel_index(pos_dual.y + 0.0f, vs, inv_vs);
-  gy[1] = voxel_index(pos_dual.y + vs, vs, inv_vs);
-  gz[0] = voxel_index(pos_dual.z + 0.0f, vs, inv_vs);
-  gz[1] = voxel_index(pos_dual.z + vs, vs, inv_vs);
-  // the high corners lie in the next block along an axis where they cross
-  const bool cx = blk_of(gx[1]) != blk_of(gx[0]), cy = blk_of(gy[1]) != blk_of(gy[0]),
-             cz = blk_of(gz[1]) != blk_of(gz[0]);
-  CellBlocks cells;
-  cell_blocks(v, blk_of(gx[0]), blk_of(gy[0]), blk_of(gz[0]), cx, cy, cz, bc, cells);
-  float dist = 0.0f;
-  float cr = 0.0f, cg = 0.0f, cb = 0.0f;
-  const int off[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1},
-                         {1, 1, 0}, {0, 1, 1}, {1, 0, 1}, {1, 1, 1}};
-#pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    const int ox = off[k][0], oy = off[k][1], oz = off[k][2];
-    const int ptr = corner_block(cells, cx, cy, cz, ox, oy, oz);
-    uint2 vv = load_voxel(v, ptr, lin_of(gx[ox], gy[oy], gz[oz]));
-    uint2 src = (vw(vv) == 0) ? v0 : vv;
-    float a = ox ? wt.x : 1.0f - wt.x;
-    float b = oy ? wt.y : 1.0f - wt.y;
-    float c = oz ? wt.z : 1.0f - wt.z;
-    float coef = a * b * c;
-    dist += coef * vsdf(src);
-    if (COLOR) {
-      cr = cr + (float)(src.x & 0xff) * coef;
-      cg = cg + (float)((src.x >> 8) & 0xff) * coef;
-      cb = cb + (float)((src.x >> 16) & 0xff) * coef;
-    }
-  }
-  out.sdf = dist;
-  out.r = cr;
-  out.g = cg;
-  out.b = cb;
-  return out;
-}
-
+// ------------------------------------------------------------ the march
 constexpr int kRayTX = 16, kRayTY = 16;
 
-// tsdfVolume raycast (tsdf.cu:471-526) of pixel (x, y) from camera pose T:
-// march from 0 by the interpolated sdf (a truncation where unobserved) until
-// the sdf drops under a voxel or the depth passes max_sensor_depth; then the
-// interpolated colour at the hit.  Beyond the near distance, samples before
-// skip_to or after skip_far (the tile's ray depth bounds: no allocated block
-// there) step by the truncation without a lookup -- what the lookup would
-// have returned.  Returns true when the march hit the step cap.
-__device__ inline bool raycast_exact_px(const VolumeDev& v, const DSensor& s, const M4f& T, int x,
-                                        int y, float skip_to, float skip_far,
-                                        float* __restrict__ depth_out,
-                                        uint8_t* __restrict__ rgb_out) {
-  const int i = y * s.cols + x;
-  const DTsdf& t = v.t;
-  const float inv_vs = 1.0f / t.vs;
-  // getPoint3d (utils.h:104-112) with the pixel's (u - cx), (v - cy) hoisted
-  const float ax = (float)x - s.cx, ay = (float)y - s.cy;
-  BlockCache bc;
-  bc.x = bc.y = bc.z = 0x7fffffff;
-  bc.ptr = -1;
-  float cur = 0.0f;
-  int steps = 0;
-  bool over = false;
-  const float znear = ray_near(t);
-  while (cur < t.dmax) {
-    if (steps++ >= t.rc_cap) {
-      over = true;
-      break;
-    }
-    if (cur >= znear && (cur < skip_to || cur > skip_far)) {  // no allocated block here
-      cur += t.trunc;
-      continue;
-    }
-    F3 pc = f3(ax * cur / s.fx, ay * cur / s.fy, cur);
-    F3 point = xform(T, pc);
-    VoxelSample vx = get_interpolated<false>(v, point, inv_vs, bc);
-    if (vx.w == 0) cur += t.trunc;
-    else cur += vx.sdf;
-    if (vx.w != 0 && vx.sdf < t.vs) break;
+// tsdfVolume::GenerateDepthKernel / GenerateRgbKernel (tsdf.cu:471-526)
+// with GetInterpolatedVoxel (tsdf.cu:47-175), in voxel units: the sample at
+// depth z is q = o + z * d (o the camera centre, d the pixel's ray direction
+// per unit depth, both divided by the voxel size) by fused multiply-adds.
+// The reference's step rule is kept: from 0, step by the interpolated sdf
+// where the sample's voxel (floor(q + 0.5), the reference's rounding of
+// p / vs up to ties) is observed, by the truncation distance where it is
+// not, until the sdf drops under a voxel or the depth passes
+// max_sensor_depth.  The trilinear cell is floor(q) .. floor(q) + 1 with
+// weights q - floor(q) (the reference's rounded p - vs/2 and p + vs/2 and
+// its weights from p / vs); unobserved corners take the centre voxel's
+// value.  Two shortcuts give what the full sample would give:
+//  * beyond the near distance, a sample before the tile's near bound or
+//    after its far bound (no allocated block there) steps by the truncation
+//    without a lookup;
+//  * a sample whose cell lies in a free-cell block (every voxel the cell can
+//    read is unobserved or saturated, VolumeDev::freecell) steps by the
+//    truncation distance without reading voxels: the reference's step there
+//    is the truncation (unobserved centre) or the interpolation of
+//    saturated values, which is the truncation to within 1e-6 relative, and
+//    never ends the march (free_ok).
+// Voxel values: FP32 form sdf in metres; mixed form f16 sdf / truncation
+// (scaled back by the truncation after the sum).
+template <bool FP16>
+struct Vox;
+template <>
+struct Vox<false> {
+  using raw_t = uint2;
+  static __device__ raw_t load(const VolumeDev& v, int ptr, int lin) {
+    if (ptr < 0) return make_uint2(0u, 0u);
+    return __ldg(reinterpret_cast<const uint2*>(v.voxels + (size_t)ptr * kBlockVox + lin));
   }
-  depth_out[i] = cur;
-  if (rgb_out) {
-    uint8_t r = 0, g = 0, b = 0;
-    if (cur < t.dmax) {
-      F3 point = xform(T, point3d(i, cur, s));
-      VoxelSample vx = get_interpolated<true>(v, point, inv_vs, bc);
-      r = (uint8_t)vx.r;
-      g = (uint8_t)vx.g;
-      b = (uint8_t)vx.b;
-    }
-    rgb_out[3 * (size_t)i] = r;
-    rgb_out[3 * (size_t)i + 1] = g;
-    rgb_out[3 * (size_t)i + 2] = b;
+  static __device__ int w(raw_t r) { return (int)(r.x >> 24); }
+  static __device__ float val(raw_t r) { return __uint_as_float(r.y); }
+  static __device__ float unit(const DTsdf&) { return 1.0f; }
+  static __device__ uchar4 color(const VolumeDev&, raw_t r, int, int) {
+    return make_uchar4(r.x & 0xff, (r.x >> 8) & 0xff, (r.x >> 16) & 0xff, 0);
   }
-  return over;
-}
+  static constexpr bool kHasColor = true;
+};
+template <>
+struct Vox<true> {
+  using raw_t = unsigned;
+  static __device__ raw_t load(const VolumeDev& v, int ptr, int lin) {
+    return ptr < 0 ? 0u : __ldg(v.vox16 + (size_t)ptr * kBlockVox + lin);
+  }
+  static __device__ int w(raw_t r) { return (int)(r >> 16); }
+  static __device__ float val(raw_t r) {
+    return __half2float(__ushort_as_half((unsigned short)(r & 0xffffu)));
+  }
+  static __device__ float unit(const DTsdf& t) { return t.trunc; }
+  static __device__ uchar4 color(const VolumeDev& v, raw_t, int ptr, int lin) {
+    return (v.colors && ptr >= 0) ? v.colors[(size_t)ptr * kBlockVox + lin]
+                                  : make_uchar4(0, 0, 0, 0);
+  }
+  static constexpr bool kHasColor = false;  // colour lives in v.colors
+};
 
-// ------------------------------------------------------------ mixed-precision raycast
-// The mixed form marches the same ray with the reference's step rule
-// (tsdf.cu:471-526) and trilinear interpolation at every observed sample,
-// on f16 voxels, in voxel units with fused multiply-adds and without the
-// exact-rounding checks (a sample's voxel or cell can differ from the
-// reference's at a tie, moving it by under a voxel).  Skipping the
-// interpolation where the sampled voxel is far from the surface was tried
-// and rejected: it changes the step sequence, so the hit moves by up to a
-// voxel and the tracked trajectory drifts by more than a millimetre from
-// the FP32 path.
-__device__ inline unsigned load16(const VolumeDev& v, int ptr, int lin) {
-  return ptr < 0 ? 0u : __ldg(v.vox16 + (size_t)ptr * kBlockVox + lin);
-}
-__device__ inline int w16(unsigned r) { return (int)(r >> 16); }
-
-// f16 value of a mixed voxel: sdf / truncation
-__device__ inline float n16(unsigned r) {
-  return __half2float(__ushort_as_half((unsigned short)(r & 0xffffu)));
-}
-
-// Trilinear sample of the f16 sdf (and colour) at q, the sample in voxel
-// units (p / vs): the cell's corners are floor(q) and floor(q) + 1 per axis
-// (the reference's rounded p - vs/2 and p + vs/2, up to ties) with weights
-// q - floor(q); unobserved corners take the centre voxel's value (raw0,
-// heap index ptr0v, local index lin0), as GetInterpolatedVoxel does.  Sums
-// use fused multiply-adds, in units of the truncation distance.
-template <bool COLOR>
-__device__ inline VoxelSample interp16(const VolumeDev& v, F3 q, unsigned raw0, int ptr0v,
-                                       int lin0, BlockCache& bc) {
+// The interpolated sample at q (voxel units) whose centre voxel raw0 (heap
+// index ptr0, local index lin0) is observed.  Sums by fused multiply-adds
+// in the reference's corner order.
+template <bool FP16, bool COLOR>
+__device__ inline VoxelSample interp(const VolumeDev& v, F3 q, typename Vox<FP16>::raw_t raw0,
+                                     int ptr0, int lin0, BlockCache& bc) {
+  using V = Vox<FP16>;
   VoxelSample out;
   const float fx = floorf(q.x), fy = floorf(q.y), fz = floorf(q.z);
   const float wx = q.x - fx, wy = q.y - fy, wz = q.z - fz;
@@ -762,12 +718,10 @@ __device__ inline VoxelSample interp16(const VolumeDev& v, F3 q, unsigned raw0, 
   // into the next block where the cell crosses)
   const int base = (lx << 6) | (ly << 3) | lz;
   const int dx = cx ? -448 : 64, dy = cy ? -56 : 8, dz = cz ? -7 : 1;
-  const uchar4 c0 = (COLOR && v.colors && ptr0v >= 0)
-                        ? v.colors[(size_t)ptr0v * kBlockVox + lin0] : make_uchar4(0, 0, 0, 0);
-  const float n0 = n16(raw0);
-  // weight products per (x, y) pair, then times the z weight
+  const uchar4 c0 = COLOR ? V::color(v, raw0, ptr0, lin0) : make_uchar4(0, 0, 0, 0);
+  const float n0 = V::val(raw0);
   const float ax[2] = {1.0f - wx, wx}, ay[2] = {1.0f - wy, wy}, az[2] = {1.0f - wz, wz};
-  float dist = 0.0f, cr = 0.0f, cg = 0.0f, cb_ = 0.0f;
+  float dist = 0.0f, cr = 0.0f, cg = 0.0f, cbl = 0.0f;
   const int off[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1},
                          {1, 1, 0}, {0, 1, 1}, {1, 0, 1}, {1, 1, 1}};
 #pragma unroll
@@ -775,34 +729,48 @@ __device__ inline VoxelSample interp16(const VolumeDev& v, F3 q, unsigned raw0, 
     const int ox = off[k][0], oy = off[k][1], oz = off[k][2];
     const int ptr = corner_block(cb, cx, cy, cz, ox, oy, oz);
     const int lin = base + (ox ? dx : 0) + (oy ? dy : 0) + (oz ? dz : 0);
-    const unsigned r = load16(v, ptr, lin);
-    const bool use0 = w16(r) == 0;
+    const typename V::raw_t r = V::load(v, ptr, lin);
+    const bool use0 = V::w(r) == 0;
     const float coef = (ax[ox] * ay[oy]) * az[oz];
-    dist = __fmaf_rn(coef, use0 ? n0 : n16(r), dist);
-    if (COLOR && v.colors) {
-      const uchar4 cc = use0 ? c0 : (ptr >= 0 ? v.colors[(size_t)ptr * kBlockVox + lin]
-                                              : make_uchar4(0, 0, 0, 0));
+    dist = __fmaf_rn(coef, use0 ? n0 : V::val(r), dist);
+    if (COLOR) {
+      const uchar4 cc = use0 ? c0 : V::color(v, r, ptr, lin);
       cr = __fmaf_rn((float)cc.x, coef, cr);
       cg = __fmaf_rn((float)cc.y, coef, cg);
-      cb_ = __fmaf_rn((float)cc.z, coef, cb_);
+      cbl = __fmaf_rn((float)cc.z, coef, cbl);
     }
   }
-  out.sdf = dist * v.t.trunc;
-  out.w = w16(raw0);
+  out.sdf = dist * V::unit(v.t);
+  out.w = V::w(raw0);
   out.r = cr;
   out.g = cg;
-  out.b = cb_;
+  out.b = cbl;
   return out;
 }
 
-// The march of the mixed form in voxel units: the sample at depth z is
-// o + z * d with o the camera centre and d the pixel's ray direction per
-// unit depth (both divided by vs), by fused multiply-adds; its voxel is
-// floor(q + 0.5).  skip_to / skip_far as in raycast_exact_px.
-__device__ inline bool raycast_mixed_px(const VolumeDev& v, const DSensor& s, const M4f& T, int x,
-                                        int y, float skip_to, float skip_far,
-                                        float* __restrict__ depth_out,
-                                        uint8_t* __restrict__ rgb_out) {
+// The block of a cell's low corner through the ray's cache, with its
+// free-cell flag (0 where no flags are kept).
+__device__ inline int cell_block_free(const VolumeDev& v, int bx, int by, int bz, BlockCache& bc,
+                                      int* free) {
+  if (bx != bc.x || by != bc.y || bz != bc.z) {
+    bc.x = bx;
+    bc.y = by;
+    bc.z = bz;
+    bc.ptr = find_block(v.entries, v.t, bx, by, bz);
+    bc.free = (v.freecell && bc.ptr >= 0) ? (int)__ldg(v.freecell + bc.ptr) : 0;
+  }
+  *free = bc.free;
+  return bc.ptr;
+}
+
+// The march of pixel (x, y) from camera pose T; the colour at the hit when
+// rgb_out is given.  skip_to / skip_far: the tile's ray depth bounds.
+// Returns true when the march hit the step cap.
+template <bool FP16>
+__device__ inline bool raycast_px(const VolumeDev& v, const DSensor& s, const M4f& T, int x,
+                                  int y, float skip_to, float skip_far,
+                                  float* __restrict__ depth_out, uint8_t* __restrict__ rgb_out) {
+  using V = Vox<FP16>;
   const int i = y * s.cols + x;
   const DTsdf& t = v.t;
   const float inv_vs = 1.0f / t.vs;
@@ -811,9 +779,10 @@ __device__ inline bool raycast_mixed_px(const VolumeDev& v, const DSensor& s, co
   const F3 d = f3((T.m[0] * axf + T.m[1] * ayf + T.m[2]) * inv_vs,
                   (T.m[4] * axf + T.m[5] * ayf + T.m[6]) * inv_vs,
                   (T.m[8] * axf + T.m[9] * ayf + T.m[10]) * inv_vs);
-  BlockCache bc;
-  bc.x = bc.y = bc.z = 0x7fffffff;
-  bc.ptr = -1;
+  BlockCache bc, bc0;  // the cell's low-corner block (with its flag); the centre voxel's block
+  bc.x = bc.y = bc.z = bc0.x = bc0.y = bc0.z = 0x7fffffff;
+  bc.ptr = bc0.ptr = -1;
+  bc.free = bc0.free = 0;
   float cur = 0.0f;
   int steps = 0;
   bool over = false;
@@ -828,16 +797,23 @@ __device__ inline bool raycast_mixed_px(const VolumeDev& v, const DSensor& s, co
       continue;
     }
     const F3 q = f3(__fmaf_rn(cur, d.x, o.x), __fmaf_rn(cur, d.y, o.y), __fmaf_rn(cur, d.z, o.z));
-    const int gx = (int)floorf(q.x + 0.5f), gy = (int)floorf(q.y + 0.5f),
-              gz = (int)floorf(q.z + 0.5f);
-    const int ptr = block_ptr(v, blk_of(gx), blk_of(gy), blk_of(gz), bc);
-    const int lin = lin_of(gx, gy, gz);
-    const unsigned raw = load16(v, ptr, lin);
-    if (w16(raw) == 0) {
+    const float flx = floorf(q.x), fly = floorf(q.y), flz = floorf(q.z);
+    int free;
+    cell_block_free(v, (int)flx >> 3, (int)fly >> 3, (int)flz >> 3, bc, &free);
+    if (free) {  // the interpolated sdf is the truncation distance
       cur += t.trunc;
       continue;
     }
-    VoxelSample vx = interp16<false>(v, q, raw, ptr, lin, bc);
+    const int gx = (int)flx + (q.x - flx >= 0.5f), gy = (int)fly + (q.y - fly >= 0.5f),
+              gz = (int)flz + (q.z - flz >= 0.5f);
+    const int ptr = block_ptr(v, blk_of(gx), blk_of(gy), blk_of(gz), bc0);
+    const int lin = lin_of(gx, gy, gz);
+    const typename V::raw_t raw = V::load(v, ptr, lin);
+    if (V::w(raw) == 0) {
+      cur += t.trunc;
+      continue;
+    }
+    const VoxelSample vx = interp<FP16, false>(v, q, raw, ptr, lin, bc);
     cur += vx.sdf;
     if (vx.sdf < t.vs) break;
   }
@@ -849,20 +825,19 @@ __device__ inline bool raycast_mixed_px(const VolumeDev& v, const DSensor& s, co
           f3(__fmaf_rn(cur, d.x, o.x), __fmaf_rn(cur, d.y, o.y), __fmaf_rn(cur, d.z, o.z));
       const int gx = (int)floorf(q.x + 0.5f), gy = (int)floorf(q.y + 0.5f),
                 gz = (int)floorf(q.z + 0.5f);
-      const int ptr = block_ptr(v, blk_of(gx), blk_of(gy), blk_of(gz), bc);
+      const int ptr = block_ptr(v, blk_of(gx), blk_of(gy), blk_of(gz), bc0);
       const int lin = lin_of(gx, gy, gz);
-      const unsigned raw = load16(v, ptr, lin);
-      if (w16(raw) != 0) {
-        VoxelSample vx = interp16<true>(v, q, raw, ptr, lin, bc);
-        r = (uint8_t)vx.r;
-        g = (uint8_t)vx.g;
-        b = (uint8_t)vx.b;
-      } else if (v.colors && ptr >= 0) {
-        uchar4 c = v.colors[(size_t)ptr * kBlockVox + lin];
-        r = c.x;
-        g = c.y;
-        b = c.z;
+      const typename V::raw_t raw = V::load(v, ptr, lin);
+      uchar4 c;
+      if (V::w(raw) != 0) {
+        const VoxelSample vx = interp<FP16, true>(v, q, raw, ptr, lin, bc);
+        c = make_uchar4((uint8_t)vx.r, (uint8_t)vx.g, (uint8_t)vx.b, 0);
+      } else {
+        c = V::color(v, raw, ptr, lin);  // GetInterpolatedVoxel returns the centre voxel
       }
+      r = c.x;
+      g = c.y;
+      b = c.z;
     }
     rgb_out[3 * (size_t)i] = r;
     rgb_out[3 * (size_t)i + 1] = g;
@@ -901,8 +876,7 @@ __device__ inline void raycast_tile(const VolumeDev& v, const DSensor& s,
       skip_to = fminf(__uint_as_float(B.near8[f]), __uint_as_float(B.near64[c]));
       skip_far = fmaxf(__uint_as_float(B.far8[f]), __uint_as_float(B.far64[c]));
     }
-    const bool o = MIXED ? raycast_mixed_px(v, s, T, x, y, skip_to, skip_far, depth_out, rgb_out)
-                         : raycast_exact_px(v, s, T, x, y, skip_to, skip_far, depth_out, rgb_out);
+    const bool o = raycast_px<MIXED>(v, s, T, x, y, skip_to, skip_far, depth_out, rgb_out);
     if (o) atomicAdd(&over, 1);
   }
   __syncthreads();
@@ -993,6 +967,14 @@ __global__ void block_coords_kernel(VolumeDev v, int n, int* coords) {
   coords[3 * i + 2] = key_z(k);
 }
 
+__global__ void find_blocks_kernel(VolumeDev v, const int* __restrict__ coords, int n,
+                                   int* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int p = find_block(v.entries, v.t, coords[3 * i], coords[3 * i + 1], coords[3 * i + 2]);
+  out[i] = (p >= 0 && p < v.t.num_blocks) ? p : -1;
+}
+
 inline int nblk(long long n, int t) { return (int)((n + t - 1) / t); }
 
 }  // namespace
@@ -1004,6 +986,8 @@ void launch_volume_clear(const VolumeDev& v, cudaStream_t st) {
   if (v.voxels) cudaMemsetAsync(v.voxels, 0, sizeof(dyn_voxel) * nv, st);
   if (v.vox16) cudaMemsetAsync(v.vox16, 0, sizeof(unsigned) * nv, st);
   if (v.colors) cudaMemsetAsync(v.colors, 0, sizeof(uchar4) * nv, st);
+  if (v.nonsat) cudaMemsetAsync(v.nonsat, 0, sizeof(int) * (size_t)v.t.num_blocks, st);
+  if (v.freecell) cudaMemsetAsync(v.freecell, 0, (size_t)v.t.num_blocks, st);
   cudaMemsetAsync(v.cnt, 0, sizeof(Counters), st);
 }
 
@@ -1021,6 +1005,11 @@ void launch_raycast(const VolumeDev& v, const DSensor& s, const PoseState* ps,
 
 void launch_block_coords(const VolumeDev& v, int n, int* coords, cudaStream_t st) {
   if (n > 0) block_coords_kernel<<<nblk(n, 256), 256, 0, st>>>(v, n, coords);
+}
+
+void launch_find_blocks(const VolumeDev& v, const int* coords, int n, int* ptr_out,
+                        cudaStream_t st) {
+  if (n > 0) find_blocks_kernel<<<nblk(n, 256), 256, 0, st>>>(v, coords, n, ptr_out);
 }
 
 // ---- fused stages
@@ -1046,6 +1035,10 @@ void fused_visible(const SessDev* tab, const BatchShape& b, cudaStream_t st) {
 void fused_integrate(const SessDev* tab, const BatchShape& b, cudaStream_t st) {
   fused_integrate_kernel<<<b.integrate_ctas > 0 ? b.integrate_ctas : 148 * 8, kBlockVox, 0,
                            st>>>(tab, b.gvis, b.gcount);
+}
+
+void fused_free_cells(const SessDev* tab, const BatchShape& b, cudaStream_t st) {
+  fused_free_cells_kernel<<<148 * 2, 256, 0, st>>>(tab, b.gvis, b.gcount);
 }
 
 void fused_raycast(const SessDev* tab, const BatchShape& b, cudaStream_t st) {

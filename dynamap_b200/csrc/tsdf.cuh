@@ -14,6 +14,15 @@ struct VolumeDev {
   dyn_voxel* voxels;              // FP32 form: num_blocks * 512, x-major per block
   unsigned* vox16;                // mixed form: {f16 sdf | u16 weight << 16} per voxel
   uchar4* colors;                 // mixed form: r,g,b per voxel (null: no colour kept)
+  // Free-space summaries per heap index (null: not kept): nonsat = voxels
+  // that are observed and not saturated (t.sat_lo), kept exact by the
+  // integration; freecell = 1 when every voxel a trilinear cell keyed in the
+  // block can read (the block and its seven upper neighbours, missing
+  // neighbours included) is unobserved or saturated, so the raycast's
+  // interpolated sdf there is the truncation distance.  freecell may be 0
+  // where it could be 1, never the reverse.
+  int* nonsat;
+  unsigned char* freecell;
   int fp16;                       // 1: mixed-precision voxels (vox16 [+ colors])
   Counters* cnt;
   DTsdf t;
@@ -27,5 +36,8 @@ void launch_raycast(const VolumeDev& v, const DSensor& s, const PoseState* ps,
                     cudaStream_t st);
 // Download helpers: block coordinates of heap indices [0, n).
 void launch_block_coords(const VolumeDev& v, int n, int* coords, cudaStream_t st);
+// Heap index (or -1) of each of n block coordinates (x, y, z triples).
+void launch_find_blocks(const VolumeDev& v, const int* coords, int n, int* ptr_out,
+                        cudaStream_t st);
 
 }  // namespace dyn

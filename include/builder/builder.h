@@ -26,6 +26,16 @@ class builder {
   rgbdSensor sensor;
   dyn_frame_stats lastStats{};
   int frameNum = 0;
+  // builder.h:98-99: the target's and the source's vertex and normal maps
+  // (rows*cols each), refreshed after every frame while keepClouds is set:
+  // the target is the model seen from the new pose (the next frame's
+  // target), the source the frame just tracked (its filtered depth).  The
+  // reference fills them inside gnSolver::solve with the target it tracked
+  // against; here they cost a device->host copy per frame, so callers that
+  // do not read them clear keepClouds.
+  geometry::PointCloudXYZ* targetPCL = &target_pcl_;
+  geometry::PointCloudXYZ* sourcePCL = &source_pcl_;
+  bool keepClouds = true;
 
   builder() = default;
   builder(const builder&) = delete;
@@ -58,6 +68,7 @@ class builder {
     if (r != DYN_ERR_HASH_FULL) dyn_throw("builder::buildModelLS", r);
     currentPose_ = Matrix4f::from_row_major(pose);
     ++frameNum;
+    if (keepClouds) refresh_clouds();
   }
 
   // builder.cu:70 / builder.h:58: the frame dataset.image, read by
@@ -99,30 +110,35 @@ class builder {
   Matrix4f getCurrentPose() const { return currentPose_; }
 
   // builder.cu:161-196: render the model at the current pose for a virtual
-  // sensor of width x height (intrinsics scaled by width/cols, height/rows)
-  std::vector<float> GenerateDepth(int width, int height) {
-    std::vector<float> d((size_t)width * height);
+  // sensor of width x height (intrinsics scaled by width/cols, height/rows).
+  // The image is the builder's, valid until the next call of the same
+  // method (the reference returns a managed buffer it never frees).
+  float* GenerateDepth(int width, int height) {
+    depth_out_.resize((size_t)width * height);
     dyn_sensor v = virtual_sensor(width, height);
     float4x4 p = currentPose_.to_row_major();
-    dyn_throw("builder::GenerateDepth", dyn_raycast(session_, p.entries, &v, d.data(), nullptr));
-    return d;
+    dyn_throw("builder::GenerateDepth",
+              dyn_raycast(session_, p.entries, &v, depth_out_.data(), nullptr));
+    return depth_out_.data();
   }
-  std::vector<uint8_t> GenerateRgb(int width, int height) {
+  uchar3* GenerateRgb(int width, int height) {
     std::vector<float> d((size_t)width * height);
-    std::vector<uint8_t> c(d.size() * 3);
+    rgb_out_.resize(d.size());
     dyn_sensor v = virtual_sensor(width, height);
     float4x4 p = currentPose_.to_row_major();
-    dyn_throw("builder::GenerateRgb", dyn_raycast(session_, p.entries, &v, d.data(), c.data()));
-    return c;
+    dyn_throw("builder::GenerateRgb",
+              dyn_raycast(session_, p.entries, &v, d.data(),
+                          reinterpret_cast<uint8_t*>(rgb_out_.data())));
+    return rgb_out_.data();
   }
 
   // builder.cu:66-69: the mesh of the box between the corners
-  geometry::Mesh ExtractMesh(const geometry::float3_& lower_corner,
-                             const geometry::float3_& upper_corner) {
+  geometry::Mesh ExtractMesh(const float3& lower_corner, const float3& upper_corner) {
     const float lo[3] = {lower_corner.x, lower_corner.y, lower_corner.z};
     const float hi[3] = {upper_corner.x, upper_corner.y, upper_corner.z};
     return geometry::ExtractMesh(session_, lo, hi);
   }
+
 
   dyn_session* session() const { return session_; }
 
@@ -177,6 +193,37 @@ class builder {
     return v;
   }
 
+  // the session's level-0 target (which 5) or source (which 2) depth and
+  // its vertex and normal maps into the clouds
+  void refresh_clouds() {
+    const size_t n = (size_t)sensor.rows * sensor.cols;
+    std::vector<float> d(n), v(4 * n), nm(4 * n);
+    cloud_points_[0].resize(n);
+    cloud_normals_[0].resize(n);
+    cloud_points_[1].resize(n);
+    cloud_normals_[1].resize(n);
+    const dyn_sensor s = sensor.to_c();
+    for (int k = 0; k < 2; ++k) {
+      dyn_throw("builder: clouds", dyn_debug_image(session_, k == 0 ? 5 : 2, 0, d.data(),
+                                                   (int64_t)(n * sizeof(float))));
+      for (float& z : d)
+        if (!(z > 0.0f && z < tsdf_.max_sensor_depth)) z = 0.0f;  // no surface
+      dyn_throw("builder: clouds", dyn_depth_to_maps_host(d.data(), &s, v.data(), nm.data()));
+      for (size_t i = 0; i < n; ++i) {
+        cloud_points_[k][i] = make_float3(v[4 * i], v[4 * i + 1], v[4 * i + 2]);
+        cloud_normals_[k][i] = make_float3(nm[4 * i], nm[4 * i + 1], nm[4 * i + 2]);
+      }
+    }
+    target_pcl_.points = cloud_points_[0].data();
+    target_pcl_.normals = cloud_normals_[0].data();
+    source_pcl_.points = cloud_points_[1].data();
+    source_pcl_.normals = cloud_normals_[1].data();
+  }
+
+  geometry::PointCloudXYZ target_pcl_, source_pcl_;
+  std::vector<float3> cloud_points_[2], cloud_normals_[2];
+  std::vector<float> depth_out_;
+  std::vector<uchar3> rgb_out_;
   dyn_session* session_ = nullptr;
   dyn_tsdf_params tsdf_{};
   solver::Properties opt_;

@@ -259,6 +259,12 @@ dyn_status dyn_raycast_maps(dyn_session* s, const float pose[16], const dyn_sens
 /* Number of allocated blocks (HashTable::GetNumAllocatedBlocks,
  * hashTable.cu:165). */
 dyn_status dyn_num_blocks(dyn_session* s, int64_t* n_out);
+
+/* HashTable::FindHashEntry (hashTable.cu:136-150) for n block coordinates
+ * (coords[3*i..]): the heap index of each block, or -1 where none is
+ * allocated.  Waits for the session's frames. */
+dyn_status dyn_find_blocks(dyn_session* s, const int32_t* coords, int64_t n,
+                           int32_t* heap_index_out);
 /* Copies every allocated block: coords_out[3*i..] = block coordinate
  * (HashEntry::position, hashTable.h:22), voxels_out[512*i..] = its voxels in
  * the reference's x-major order (VoxelBlock::at, geom_Types.h:116-119).
@@ -374,6 +380,14 @@ dyn_status dyn_bilateral_filter(const float* depth_dev, float* out_dev,
 dyn_status dyn_depth_to_maps(const float* depth_dev, const dyn_sensor* level,
                              float* vertex4_dev, float* normal4_dev,
                              void* stream);
+
+/* The same maps for a depth image in host memory (rgbdImage's own buffers,
+ * as the reference's managed images are): depth_host and the float4 maps
+ * are rows*cols host arrays; vertex4_host may be NULL.  The device buffers
+ * are taken and released inside the call, on the calling thread's default
+ * stream; synchronous. */
+dyn_status dyn_depth_to_maps_host(const float* depth_host, const dyn_sensor* level,
+                                  float* vertex4_host, float* normal4_host);
 
 /* The 6x6 normal equations of one ICP iteration (buildNLSKernel,
  * gnSolver.cu:26-196): for source pixels (depth, normals, intensity) and a

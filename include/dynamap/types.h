@@ -11,10 +11,38 @@
 
 #include <cmath>
 #include <cstdint>
+#include <ostream>
 #include <stdexcept>
 #include <string>
 
 #include "../dynamap.h"
+
+// The CUDA vector types the reference's interfaces name (float3, int3,
+// uchar3): CUDA's own when its headers are on the include path, else
+// layout-compatible host structs (the library needs no CUDA headers).
+#if defined(__has_include)
+#if __has_include(<vector_types.h>) && __has_include(<vector_functions.h>)
+#include <vector_types.h>
+#include <vector_functions.h>
+#define DYNAMAP_CUDA_VECTOR_TYPES 1
+#endif
+#endif
+#ifndef DYNAMAP_CUDA_VECTOR_TYPES
+struct float3 {
+  float x, y, z;
+};
+struct int3 {
+  int x, y, z;
+};
+struct uchar3 {
+  unsigned char x, y, z;
+};
+inline float3 make_float3(float x, float y, float z) { return float3{x, y, z}; }
+inline int3 make_int3(int x, int y, int z) { return int3{x, y, z}; }
+inline uchar3 make_uchar3(unsigned char x, unsigned char y, unsigned char z) {
+  return uchar3{x, y, z};
+}
+#endif
 
 namespace DynaMap {
 
@@ -75,6 +103,7 @@ struct Matrix4f {
     for (int i = 0; i < 16; ++i) data_[i] = (i % 5 == 0) ? 1.0f : 0.0f;
   }
   static Matrix4f Identity() { return Matrix4f(); }
+  void setIdentity() { *this = Matrix4f(); }
   float& operator()(int r, int c) { return data_[c * 4 + r]; }
   float operator()(int r, int c) const { return data_[c * 4 + r]; }
   float* data() { return data_; }
@@ -88,6 +117,15 @@ struct Matrix4f {
     return m;
   }
 };
+
+// Eigen's stream form: four rows, entries separated by spaces
+inline std::ostream& operator<<(std::ostream& os, const Matrix4f& m) {
+  for (int r = 0; r < 4; ++r) {
+    for (int c = 0; c < 4; ++c) os << (c ? " " : "") << m(r, c);
+    if (r < 3) os << "\n";
+  }
+  return os;
+}
 
 typedef double Vector6d[6];
 

@@ -20,14 +20,13 @@
 namespace DynaMap {
 namespace geometry {
 
-struct float3_ {
-  float x = 0.0f, y = 0.0f, z = 0.0f;
-};
+// the reference's float3 (CUDA's, or the host stand-in of dynamap/types.h)
+typedef float3 float3_;
 
 struct Vertex {
-  float3_ position;
-  float3_ normal;
-  float3_ color;  // 0..1
+  float3_ position{0.0f, 0.0f, 0.0f};
+  float3_ normal{0.0f, 0.0f, 0.0f};
+  float3_ color{0.0f, 0.0f, 0.0f};  // 0..1
 };
 
 struct Triangle {

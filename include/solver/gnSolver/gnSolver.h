@@ -12,10 +12,13 @@
 #pragma once
 
 #include <cstdint>
+#include <utility>
 #include <vector>
 
 #include "../../dynamap.h"
 #include "../../dynamap/types.h"
+#include "../../geometry/geom_Types.h"
+#include "../../image/sensor/rgbdImage.h"
 
 namespace DynaMap {
 namespace solver {
@@ -104,6 +107,33 @@ class gnSolver {
                                source_rgb, p.entries, prev_increment, &lastStats));
     pose = Matrix4f::from_row_major(p.entries);
     iterationNum = lastStats.icp_iterations[2];
+  }
+
+  // gnSolver.h:72-76, the reference's own signature: the images' depth
+  // (metres) and colour; the clouds, where their arrays are given, receive
+  // the full-resolution vertex and normal maps of the two images, as the
+  // reference's solve leaves them (the solver itself derives the pyramid's
+  // maps from the depths on the device).
+  void solve(Matrix4f& pose, Vector6d& prev_increment, rgbdImage& targetImage,
+             rgbdImage& sourceImage, geometry::PointCloudXYZ& targetCloud,
+             geometry::PointCloudXYZ& sourceCloud) {
+    const size_t n = (size_t)sensor_.rows * sensor_.cols;
+    if (!targetImage.depth || !sourceImage.depth || targetImage.size() != n ||
+        sourceImage.size() != n)
+      dyn_throw("gnSolver::solve", DYN_ERR_INVALID_ARG);
+    float4x4 p = pose.to_row_major();
+    const bool col = OptProp.colorWeight != 0.0f && targetImage.rgb && sourceImage.rgb;
+    dyn_throw("gnSolver::solve",
+              dyn_solver_solve(session_, targetImage.depth, col ? targetImage.rgbBytes() : nullptr,
+                               sourceImage.depth, col ? sourceImage.rgbBytes() : nullptr,
+                               p.entries, prev_increment, &lastStats));
+    pose = Matrix4f::from_row_major(p.entries);
+    iterationNum = lastStats.icp_iterations[2];
+    for (auto c : {std::make_pair(&targetImage, &targetCloud),
+                    std::make_pair(&sourceImage, &sourceCloud)}) {
+      if (c.second->points) c.first->getPointCloudXYZ(*c.second);
+      if (c.second->normals) c.first->getNormalsfromVertices(*c.second);
+    }
   }
 
  private:

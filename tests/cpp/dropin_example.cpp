@@ -53,9 +53,9 @@ int main(int argc, char** argv) {
   const float* g = &poses[(size_t)16 * (n - 1)];
   double dt = 0;
   for (int r = 0; r < 3; ++r) dt += (P(r, 3) - g[r * 4 + 3]) * (P(r, 3) - g[r * 4 + 3]);
-  std::vector<float> d = b.GenerateDepth(cols, rows);
+  const float* d = b.GenerateDepth(cols, rows);
   int hits = 0;
-  for (float z : d) hits += (z > 0 && z < tp.maxSensorDepth);
+  for (int i = 0; i < rows * cols; ++i) hits += (d[i] > 0 && d[i] < tp.maxSensorDepth);
   std::printf("frames %d blocks %d trans_err %.5f raycast_hits %d\n", n, b.lastStats.blocks_total,
               std::sqrt(dt), hits);
   return (std::sqrt(dt) < 0.03 && hits > rows * cols / 10) ? 0 : 1;

@@ -26,6 +26,8 @@ struct HostVolume {
   std::vector<dyn_voxel> voxels;
   std::vector<unsigned> vox16;
   std::vector<uchar4> colors;
+  std::vector<int> nonsat;
+  std::vector<unsigned char> freecell;
   dyn::Counters cnt{};
   dyn::PoseState ps{};
 
@@ -44,6 +46,10 @@ struct HostVolume {
     v.vox16 = fp16 ? vox16.data() : nullptr;
     v.colors = fp16 ? colors.data() : nullptr;
     v.fp16 = fp16 ? 1 : 0;
+    nonsat.assign(num_blocks, 0);
+    freecell.assign(num_blocks, 0);
+    v.nonsat = nonsat.data();
+    v.freecell = freecell.data();
     v.cnt = &cnt;
     v.t.vs = vs;
     v.t.bsm = 8.0f * vs;
@@ -53,6 +59,8 @@ struct HostVolume {
     v.t.bucket_size = bsz;
     v.t.num_blocks = num_blocks;
     v.t.max_w = 255;
+    v.t.sat_lo = (float)((double)trunc * (1.0 - 1e-6));
+    v.t.free_ok = v.t.sat_lo >= vs ? 1 : 0;
   }
   int n() const { return std::min(cnt.nalloc, v.t.num_blocks); }
 };
@@ -188,9 +196,21 @@ int64_t emu_remove(void* h, int mode, int last, int max_age, const int32_t* del,
   if (H.v.voxels) std::memset(H.v.voxels + from, 0, sizeof(dyn_voxel) * tail);
   if (H.v.vox16) std::memset(H.v.vox16 + from, 0, sizeof(unsigned) * tail);
   if (H.v.colors) std::memset(H.v.colors + from, 0, sizeof(uchar4) * tail);
+  std::fill(H.nonsat.begin() + L, H.nonsat.begin() + n, 0);
+  std::fill(H.freecell.begin() + L, H.freecell.begin() + n, 0);
   H.cnt.nalloc = L;
   return dead;
 }
+
+// The free-space summaries of heap indices [0, n): counts, then flags.
+void emu_summaries(void* h, int32_t* nonsat, uint8_t* freecell) {
+  HostVolume& H = *(HostVolume*)h;
+  const int n = H.n();
+  std::copy(H.nonsat.begin(), H.nonsat.begin() + n, nonsat);
+  std::copy(H.freecell.begin(), H.freecell.begin() + n, freecell);
+}
+// Set block p's flag (a stand-in for the per-frame free-cell pass).
+void emu_set_free(void* h, int p, int value) { ((HostVolume*)h)->freecell[p] = (unsigned char)value; }
 
 // A lookup through the library's find_block: heap index or -1.
 int emu_find(void* h, int x, int y, int z) {

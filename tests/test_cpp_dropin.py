@@ -26,8 +26,8 @@ def test_dropin_headers_compile_and_link(tmp_path):
     compile_example(str(tmp_path / "dropin"))
     # every header is self-contained
     for h in ("builder/builder.h", "geometry/tsdf/tsdf.h", "solver/gnSolver/gnSolver.h",
-              "image/sensor/rgbdImage.h", "dynamap/types.h", "dynamap/pose_io.h", "utils/dataSet.h", "geometry/mesh/mesh.h",
-              "dynamap.h"):
+              "image/sensor/rgbdImage.h", "dynamap/types.h", "dynamap/pose_io.h", "utils/dataSet.h",
+              "geometry/mesh/mesh.h", "geometry/geom_Types.h", "dynamap.h"):
         src = tmp_path / "inc.cpp"
         src.write_text(f'#include "{h}"\nint main() {{ return 0; }}\n')
         subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-I", os.path.join(ROOT, "include"),
@@ -72,3 +72,44 @@ def test_mesh_save_to_file_and_volume_calls_compile(tmp_path):
     v = np.array([[float(a) for a in ln.split()[1:]] for ln in lines[:6]], np.float32)
     assert all(ln.startswith("v ") for ln in lines[:6])
     np.testing.assert_allclose(v.reshape(-1), tri, rtol=1e-5, atol=1e-6)
+
+
+IDIOM = os.path.join(ROOT, "tests", "cpp", "reference_idiom.cpp")
+
+
+def compile_idiom(out, extra=()):
+    cxx = shutil.which("g++")
+    if cxx is None:
+        pytest.skip("no C++ compiler")
+    subprocess.run([cxx, "-std=c++17", "-O1", "-Wall", "-Werror", "-I",
+                    os.path.join(ROOT, "include"), *extra, IDIOM, "-L", LIBDIR, "-ldynamap_b200",
+                    f"-Wl,-rpath,{LIBDIR}", "-lz", "-o", out], check=True)
+
+
+def test_reference_idiom_compiles(tmp_path):
+    """The reference's calls as its driver and builder write them
+    (dynaMap.cpp:180-301, builder.cu:70-139): gnSolver::solve on rgbdImage
+    frames and point clouds, tsdfVolume::init(const tsdfProperties&),
+    rgbdImage's clouds, HashTable's calls, builder's clouds -- against
+    include/ alone, and with CUDA's own vector types on the include path."""
+    compile_idiom(str(tmp_path / "idiom"))
+    cuda_inc = "/usr/local/cuda/include"
+    if os.path.isdir(cuda_inc):
+        compile_idiom(str(tmp_path / "idiom_cuda"), ("-I", cuda_inc))
+
+
+@pytest.mark.gpu
+@pytest.mark.first_b200_run
+def test_reference_idiom_runs(tmp_path, gpu_lib):
+    from test_dataset import make_tum
+    root = tmp_path / "seq"
+    root.mkdir()
+    seq, p = make_tum(root, n=8)
+    s = p["sensor"]
+    exe = str(tmp_path / "idiom")
+    compile_idiom(exe)
+    r = subprocess.run([exe, str(root)] + [str(s[k]) for k in ("rows", "cols", "fx", "fy", "cx",
+                                                                 "cy", "depth_scaler")],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "FAILED" not in r.stdout

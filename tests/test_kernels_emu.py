@@ -48,6 +48,8 @@ def build_emu(outdir, tile=None):
     L.emu_remove.restype = i64
     L.emu_remove.argtypes = [vp, i32, i32, i32, vp, i64, vp, vp, i64]
     L.emu_find.argtypes = [vp, i32, i32, i32]
+    L.emu_summaries.argtypes = [vp, vp, vp]
+    L.emu_set_free.argtypes = [vp, i32, i32]
     return L
 
 
@@ -219,6 +221,74 @@ def test_upload_places_a_repeated_key_once(emu):
     assert list(vol.upload(twice, np.concatenate([vox, vox[:1]]))) == [3, 1, 0, 0]
     c, _ = vol.download()
     assert sorted(map(tuple, c.tolist())) == sorted(map(tuple, coords.tolist()))
+
+
+def _nonsat_of(vox8, trunc, fp16):
+    """Observed voxels that are not saturated, per block, as the volume
+    stores them (FP32: sdf >= trunc (1 - 1e-6); mixed: f16 sdf/trunc == 1)."""
+    w = vox8[..., 3]
+    sdf = vox8[..., 4:].copy().view(np.float32)[..., 0]
+    if fp16:
+        h = (sdf / np.float32(trunc)).astype(np.float16)
+        sat = h == np.float16(1.0)
+    else:
+        sat = sdf >= np.float32(trunc * (1.0 - 1e-6))
+    return ((w != 0) & ~sat).sum(axis=1)
+
+
+@pytest.mark.parametrize("fp16", [False, True])
+def test_free_space_summaries_follow_upload_and_eviction(emu, fp16):
+    """The raycast's free-space summaries (VolumeDev::nonsat / freecell):
+    the upload counts each block's observed non-saturated voxels and clears
+    the free-cell flags of the lower neighbours of a block that holds any;
+    eviction moves both with the blocks and zeroes them above the new heap
+    top."""
+    trunc = 0.04
+    coords = np.array([[x, y, z] for x in range(3) for y in range(3) for z in range(2)], np.int32)
+    rng = np.random.default_rng(5)
+    n = len(coords)
+    vox = np.zeros((n, 512, 8), np.uint8)
+    sdf = np.full((n, 512), np.float32(trunc), np.float32)
+    w = rng.integers(0, 3, size=(n, 512)).astype(np.uint8)
+    surf = rng.random(n) < 0.4  # blocks with some near-surface voxels
+    for i in np.nonzero(surf)[0]:
+        k = rng.choice(512, 20, replace=False)
+        sdf[i, k] = rng.uniform(-trunc, trunc * 0.9, size=20).astype(np.float32)
+        w[i, k] = 3
+    vox[..., 3] = w
+    vox[..., 4:] = sdf.view(np.uint8).reshape(n, 512, 4)
+    vol = EmuVolume(emu, 0.01, trunc, 64, 8, 64, fp16)
+    # every block's flag set first, as a frame might have left them
+    assert list(vol.upload(coords[~surf], vox[~surf])) == [int((~surf).sum()), 0, 0, 0]
+    m0 = int((~surf).sum())
+    for p in range(m0):
+        emu.emu_set_free(vol.h, p, 1)
+    assert list(vol.upload(coords[surf], vox[surf])) == [int(surf.sum()), 0, 0, 0]
+
+    def summaries():
+        c, v = vol.download()
+        ns = np.zeros(len(c), np.int32)
+        fc = np.zeros(len(c), np.uint8)
+        emu.emu_summaries(vol.h, ns.ctypes.data, fc.ctypes.data)
+        return c, v, ns, fc
+
+    c, v, ns, fc = summaries()
+    np.testing.assert_array_equal(ns, _nonsat_of(v, trunc, fp16))
+    busy = {tuple(x) for x, k in zip(c.tolist(), ns) if k}
+    for x, f in zip(c.tolist(), fc):
+        reads_busy = any((x[0] + (q & 1), x[1] + ((q >> 1) & 1), x[2] + ((q >> 2) & 1)) in busy
+                         for q in range(8))
+        if reads_busy:
+            assert f == 0, x  # never free where a cell reads a non-saturated voxel
+    assert fc.sum() > 0  # some flags survive (blocks with no busy upper neighbour)
+    # evict a third: the survivors keep their summaries under their new index
+    before = {tuple(x): (k, f) for x, k, f in zip(c.tolist(), ns, fc)}
+    k, _, _ = vol.remove(1, coords=c[::3])
+    assert k == len(c[::3])
+    c2, v2, ns2, fc2 = summaries()
+    for x, k_, f in zip(c2.tolist(), ns2, fc2):
+        assert (k_, f) == before[tuple(x)]
+    np.testing.assert_array_equal(ns2, _nonsat_of(v2, trunc, fp16))
 
 
 def test_mesh_kernels_reproduce_the_reference_vertices(emu, oracle):
