@@ -39,14 +39,6 @@ struct DTsdf {
   int dda_cap;       // DDA step bound (3*ceil((dmax+trunc)/bsm)+8)
   int band;          // allocation rays start a truncation distance before the surface
   int rc_cap;        // raycast step bound (ceil(dmax/min(vs,trunc))+4)
-  // Free-space summaries for the raycast (tsdf.cu): an FP32 voxel counts as
-  // saturated when observed with sdf >= sat_lo (the truncation distance to
-  // within 1e-6 relative: merged free-space values round to within an ulp
-  // or two of it); a mixed voxel when its f16 value is exactly 1.  free_ok:
-  // sat_lo >= vs, so a saturated sample never ends a march (the summaries
-  // are kept only then).
-  float sat_lo;
-  int free_ok;
 };
 
 // Hash entry: 16 bytes, one vector load per slot.  key packs the block

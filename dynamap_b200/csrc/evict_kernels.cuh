@@ -214,7 +214,7 @@ __global__ void upload_kernel(VolumeDev v, const PoseState* __restrict__ ps,
         const size_t i = (size_t)ptr * kBlockVox + j;
         if (!v.fp16) {
           v.voxels[i] = o;
-          ns += o.weight != 0 && !(o.sdf >= v.t.sat_lo);
+          ns += o.weight != 0 && !(o.sdf >= v.sat_lo);
         } else {
           const __half h = __float2half_rn(o.sdf / v.t.trunc);
           v.vox16[i] = (unsigned)__half_as_ushort(h) | ((unsigned)o.weight << 16);

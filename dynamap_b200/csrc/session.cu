@@ -464,7 +464,8 @@ size_t session_bytes(const dyn_tsdf_params& t, const dyn_sensor& s, int precisio
   else
     b += sizeof(dyn_voxel) * (size_t)t.num_blocks * kBlockVox;
   b += sizeof(int2) * (size_t)t.num_blocks;  // visible list
-  b += (sizeof(int) + 1) * (size_t)t.num_blocks;  // free-space summaries
+  if (precision != DYN_PRECISION_FP32)
+    b += (sizeof(int) + 1) * (size_t)t.num_blocks;  // free-space summaries
   b += n * (2 + 3 + 4 + 4 + 4 + 3);  // inputs, raw, filtered, ray depth, target rgb
   if (precision == DYN_PRECISION_MIXED_BAND)
     b += 4 * (size_t)((s.rows + 7) / 8) * ((s.cols + 7) / 8) + 256;  // ray-start bound
@@ -561,6 +562,8 @@ dyn_status alloc_device_buffers(dyn_session* s) {
   DYN_TRY(s->dalloc(&s->d_icp, sizeof(IcpState)));
   DYN_TRY(s->dalloc(&s->d_pose, sizeof(PoseState)));
   s->vol.t = dtsdf(*tsdf, precision);
+  s->vol.sat_lo = (float)((double)tsdf->truncation_distance * (1.0 - 1e-6));
+  s->vol.free_ok = (double)s->vol.sat_lo >= (double)tsdf->voxel_size ? 1 : 0;
   DYN_TRY(s->dalloc(&s->vol.entries, sizeof(Entry) * (size_t)tsdf->num_buckets * tsdf->bucket_size));
   DYN_TRY(s->dalloc(&s->vol.block_keys, sizeof(unsigned long long) * (size_t)tsdf->num_blocks));
   const size_t nvox = (size_t)tsdf->num_blocks * kBlockVox;
@@ -574,8 +577,12 @@ dyn_status alloc_device_buffers(dyn_session* s) {
   } else {
     DYN_TRY(s->dalloc(&s->vol.voxels, sizeof(dyn_voxel) * nvox));
   }
-  DYN_TRY(s->dalloc(&s->vol.nonsat, sizeof(int) * (size_t)tsdf->num_blocks));
-  DYN_TRY(s->dalloc(&s->vol.freecell, (size_t)tsdf->num_blocks));
+  s->vol.nonsat = nullptr;
+  s->vol.freecell = nullptr;
+  if (s->vol.fp16) {  // the mixed forms' raycast steps through free cells
+    DYN_TRY(s->dalloc(&s->vol.nonsat, sizeof(int) * (size_t)tsdf->num_blocks));
+    DYN_TRY(s->dalloc(&s->vol.freecell, (size_t)tsdf->num_blocks));
+  }
   DYN_TRY(s->dalloc(&s->vol.cnt, sizeof(Counters)));
   DYN_TRY(s->dalloc(&s->d_gvis, sizeof(int2) * (size_t)tsdf->num_blocks));
   s->rb_tx = ((int)s->sensor.cols + 7) / 8;

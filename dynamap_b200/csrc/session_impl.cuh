@@ -75,8 +75,6 @@ inline DTsdf dtsdf(const dyn_tsdf_params& p, int precision) {
   double step = std::min((double)p.voxel_size, (double)p.truncation_distance);
   t.rc_cap = (int)std::ceil((double)p.max_sensor_depth / step) + 4;
   t.band = precision == DYN_PRECISION_MIXED_BAND ? 1 : 0;
-  t.sat_lo = (float)((double)p.truncation_distance * (1.0 - 1e-6));
-  t.free_ok = (double)t.sat_lo >= (double)p.voxel_size ? 1 : 0;
   return t;
 }
 

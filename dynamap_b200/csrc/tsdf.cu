@@ -498,8 +498,7 @@ __device__ inline int integrate_voxel(const VolumeDev& v, const float* __restric
   out.x = (unsigned)r0 | ((unsigned)r1 << 8) | ((unsigned)r2 << 16) | ((unsigned)nw << 24);
   out.y = __float_as_uint(nsdf);
   *reinterpret_cast<uint2*>(vox) = out;
-  const bool was = w == 0 || osdf >= t.sat_lo, now = nsdf >= t.sat_lo;
-  return (int)was - (int)now;
+  return 0;  // the FP32 form keeps no free-space summaries
 }
 
 // the batch-wide visible list: each item (session, block) by one CTA
@@ -531,10 +530,14 @@ __global__ void __launch_bounds__(kBlockVox)
     else
       d = integrate_voxel<true, false>(S.vol, S.raw, S.sdist, rgb, S.ls[0], invT, item.y,
                                        threadIdx.x);
-    // the block's non-saturated count follows its voxels exactly (one CTA
-    // per visible block, so the owner thread updates it alone)
-    const int up = __syncthreads_count(d > 0), down = __syncthreads_count(d < 0);
-    if (threadIdx.x == 0 && up != down && S.vol.nonsat) S.vol.nonsat[item.y] += up - down;
+    // the block's non-saturated count follows its voxels exactly: each warp
+    // adds its voxels' changes (mixed sessions only; most warps change
+    // nothing, and no barrier holds the CTA's warps together)
+    if (S.vol.nonsat) {
+      const unsigned up = __ballot_sync(0xffffffffu, d > 0), dn = __ballot_sync(0xffffffffu, d < 0);
+      const int net = __popc(up) - __popc(dn);
+      if ((threadIdx.x & 31) == 0 && net != 0) atomicAdd(S.vol.nonsat + item.y, net);
+    }
   }
 }
 
@@ -558,7 +561,7 @@ __global__ void fused_free_cells_kernel(const SessDev* __restrict__ tab,
     const unsigned long long key = v.block_keys[item.y];
     const int x = key_x(key), y = key_y(key), z = key_z(key);
     const bool own = v.nonsat[item.y] == 0;
-    bool free = own && v.t.free_ok;
+    bool free = own && v.free_ok;
 #pragma unroll
     for (int k = 1; k < 8; ++k) {
       const int dx = k & 1, dy = (k >> 1) & 1, dz = (k >> 2) & 1;
@@ -585,7 +588,10 @@ struct VoxelSample {
 struct BlockCache {
   int x, y, z;
   int ptr;
-  int free;  // the block's free-cell flag (cell_block_free)
+};
+// the cache of the mixed march's cell blocks, with the block's free-cell flag
+struct FreeCache : BlockCache {
+  int free;
 };
 
 // voxel_index, blk_of and loc_of (WorldToGlobalVoxelHashing / WorldToBlock /
@@ -603,8 +609,19 @@ __device__ inline int block_ptr(const VolumeDev& v, int bx, int by, int bz, Bloc
   }
   return bc.ptr;
 }
+__device__ inline uint2 load_voxel(const VolumeDev& v, int ptr, int lin) {
+  if (ptr < 0) return make_uint2(0u, 0u);
+  return __ldg(reinterpret_cast<const uint2*>(v.voxels + (size_t)ptr * kBlockVox + lin));
+}
 __device__ inline int lin_of(int gx, int gy, int gz) {
   return (loc_of(gx) << 6) | (loc_of(gy) << 3) | loc_of(gz);
+}
+
+__device__ inline uint2 get_voxel(const VolumeDev& v, F3 pos, float inv_vs, BlockCache& bc) {
+  const float vs = v.t.vs;
+  int gx = voxel_index(pos.x, vs, inv_vs), gy = voxel_index(pos.y, vs, inv_vs),
+      gz = voxel_index(pos.z, vs, inv_vs);
+  return load_voxel(v, block_ptr(v, blk_of(gx), blk_of(gy), blk_of(gz), bc), lin_of(gx, gy, gz));
 }
 
 __device__ inline int vw(uint2 r) { return (int)(r.x >> 24); }
@@ -638,21 +655,146 @@ __device__ inline int corner_block(const CellBlocks& cb, bool cx, bool cy, bool 
             : (ky ? (kz ? cb.pyz : cb.py) : (kz ? cb.pz : cb.p0));
 }
 
-// ------------------------------------------------------------ the march
+// tsdfVolume::GetInterpolatedVoxel, tsdf.cu:47-175.  The eight corners are
+// pos_dual + {0, vs} per axis, so each axis has two coordinate values: they
+// are resolved once (six index computations instead of twenty-four) and
+// combined per corner; every corner still gets exactly the reference's
+// float coordinate.  When the 2x2x2 corners lie in one block (the common
+// case) the block is resolved once.  Corners are summed in the reference's
+// order.  COLOR false skips the colour sums (the marching loop only reads
+// sdf and weight).
+template <bool COLOR>
+__device__ inline VoxelSample get_interpolated(const VolumeDev& v, F3 position, float inv_vs,
+                                               BlockCache& bc) {
+  VoxelSample out;
+  uint2 v0 = get_voxel(v, position, inv_vs, bc);
+  out.w = vw(v0);
+  if (out.w == 0) {
+    out.sdf = vsdf(v0);
+    out.r = (float)(v0.x & 0xff);
+    out.g = (float)((v0.x >> 8) & 0xff);
+    out.b = (float)((v0.x >> 16) & 0xff);
+    return out;
+  }
+  const float vs = v.t.vs;
+  F3 pos_dual = position - f3(vs / 2.0f, vs / 2.0f, vs / 2.0f);
+  const float inv = 1.0f / vs;
+  F3 vp = position * inv;
+  F3 wt = f3(vp.x - floorf(vp.x), vp.y - floorf(vp.y), vp.z - floorf(vp.z));
+  int gx[2], gy[2], gz[2];
+  gx[0] = voxel_index(pos_dual.x + 0.0f, vs, inv_vs);
+  gx[1] = voxel_index(pos_dual.x + vs, vs, inv_vs);
+  gy[0] = voxel_index(pos_dual.y + 0.0f, vs, inv_vs);
+  gy[1] = voxel_index(pos_dual.y + vs, vs, inv_vs);
+  gz[0] = voxel_index(pos_dual.z + 0.0f, vs, inv_vs);
+  gz[1] = voxel_index(pos_dual.z + vs, vs, inv_vs);
+  // the high corners lie in the next block along an axis where they cross
+  const bool cx = blk_of(gx[1]) != blk_of(gx[0]), cy = blk_of(gy[1]) != blk_of(gy[0]),
+             cz = blk_of(gz[1]) != blk_of(gz[0]);
+  CellBlocks cells;
+  cell_blocks(v, blk_of(gx[0]), blk_of(gy[0]), blk_of(gz[0]), cx, cy, cz, bc, cells);
+  float dist = 0.0f;
+  float cr = 0.0f, cg = 0.0f, cb = 0.0f;
+  const int off[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1},
+                         {1, 1, 0}, {0, 1, 1}, {1, 0, 1}, {1, 1, 1}};
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const int ox = off[k][0], oy = off[k][1], oz = off[k][2];
+    const int ptr = corner_block(cells, cx, cy, cz, ox, oy, oz);
+    uint2 vv = load_voxel(v, ptr, lin_of(gx[ox], gy[oy], gz[oz]));
+    uint2 src = (vw(vv) == 0) ? v0 : vv;
+    float a = ox ? wt.x : 1.0f - wt.x;
+    float b = oy ? wt.y : 1.0f - wt.y;
+    float c = oz ? wt.z : 1.0f - wt.z;
+    float coef = a * b * c;
+    dist += coef * vsdf(src);
+    if (COLOR) {
+      cr = cr + (float)(src.x & 0xff) * coef;
+      cg = cg + (float)((src.x >> 8) & 0xff) * coef;
+      cb = cb + (float)((src.x >> 16) & 0xff) * coef;
+    }
+  }
+  out.sdf = dist;
+  out.r = cr;
+  out.g = cg;
+  out.b = cb;
+  return out;
+}
+
 constexpr int kRayTX = 16, kRayTY = 16;
 
-// tsdfVolume::GenerateDepthKernel / GenerateRgbKernel (tsdf.cu:471-526)
-// with GetInterpolatedVoxel (tsdf.cu:47-175), in voxel units: the sample at
-// depth z is q = o + z * d (o the camera centre, d the pixel's ray direction
-// per unit depth, both divided by the voxel size) by fused multiply-adds.
-// The reference's step rule is kept: from 0, step by the interpolated sdf
-// where the sample's voxel (floor(q + 0.5), the reference's rounding of
-// p / vs up to ties) is observed, by the truncation distance where it is
-// not, until the sdf drops under a voxel or the depth passes
-// max_sensor_depth.  The trilinear cell is floor(q) .. floor(q) + 1 with
-// weights q - floor(q) (the reference's rounded p - vs/2 and p + vs/2 and
-// its weights from p / vs); unobserved corners take the centre voxel's
-// value.  Two shortcuts give what the full sample would give:
+
+// tsdfVolume raycast (tsdf.cu:471-526) of pixel (x, y) from camera pose T:
+// march from 0 by the interpolated sdf (a truncation where unobserved) until
+// the sdf drops under a voxel or the depth passes max_sensor_depth; then the
+// interpolated colour at the hit.  Beyond the near distance, samples before
+// skip_to or after skip_far (the tile's ray depth bounds: no allocated block
+// there) step by the truncation without a lookup -- what the lookup would
+// have returned.  Returns true when the march hit the step cap.
+__device__ inline bool raycast_exact_px(const VolumeDev& v, const DSensor& s, const M4f& T, int x,
+                                        int y, float skip_to, float skip_far,
+                                        float* __restrict__ depth_out,
+                                        uint8_t* __restrict__ rgb_out) {
+  const int i = y * s.cols + x;
+  const DTsdf& t = v.t;
+  const float inv_vs = 1.0f / t.vs;
+  // getPoint3d (utils.h:104-112) with the pixel's (u - cx), (v - cy) hoisted
+  const float ax = (float)x - s.cx, ay = (float)y - s.cy;
+  BlockCache bc;
+  bc.x = bc.y = bc.z = 0x7fffffff;
+  bc.ptr = -1;
+  float cur = 0.0f;
+  int steps = 0;
+  bool over = false;
+  const float znear = ray_near(t);
+  while (cur < t.dmax) {
+    if (steps++ >= t.rc_cap) {
+      over = true;
+      break;
+    }
+    if (cur >= znear && (cur < skip_to || cur > skip_far)) {  // no allocated block here
+      cur += t.trunc;
+      continue;
+    }
+    F3 pc = f3(ax * cur / s.fx, ay * cur / s.fy, cur);
+    F3 point = xform(T, pc);
+    VoxelSample vx = get_interpolated<false>(v, point, inv_vs, bc);
+    if (vx.w == 0) cur += t.trunc;
+    else cur += vx.sdf;
+    if (vx.w != 0 && vx.sdf < t.vs) break;
+  }
+  depth_out[i] = cur;
+  if (rgb_out) {
+    uint8_t r = 0, g = 0, b = 0;
+    if (cur < t.dmax) {
+      F3 point = xform(T, point3d(i, cur, s));
+      VoxelSample vx = get_interpolated<true>(v, point, inv_vs, bc);
+      r = (uint8_t)vx.r;
+      g = (uint8_t)vx.g;
+      b = (uint8_t)vx.b;
+    }
+    rgb_out[3 * (size_t)i] = r;
+    rgb_out[3 * (size_t)i + 1] = g;
+    rgb_out[3 * (size_t)i + 2] = b;
+  }
+  return over;
+}
+
+
+// ------------------------------------------------------------ mixed-precision raycast
+// The mixed forms' march: tsdfVolume::GenerateDepthKernel /
+// GenerateRgbKernel (tsdf.cu:471-526) with GetInterpolatedVoxel
+// (tsdf.cu:47-175) in voxel units: the sample at depth z is q = o + z * d
+// (o the camera centre, d the pixel's ray direction per unit depth, both
+// divided by the voxel size) by fused multiply-adds.  The reference's step
+// rule is kept: from 0, step by the interpolated sdf where the sample's
+// voxel (floor(q + 0.5), the reference's rounding of p / vs up to ties) is
+// observed, by the truncation distance where it is not, until the sdf drops
+// under a voxel or the depth passes max_sensor_depth.  The trilinear cell
+// is floor(q) .. floor(q) + 1 with weights q - floor(q) (the reference's
+// rounded p - vs/2 and p + vs/2 and its weights from p / vs); unobserved
+// corners take the centre voxel's value.  Two shortcuts give what the full
+// sample would give:
 //  * beyond the near distance, a sample before the tile's near bound or
 //    after its far bound (no allocated block there) steps by the truncation
 //    without a lookup;
@@ -660,27 +802,17 @@ constexpr int kRayTX = 16, kRayTY = 16;
 //    read is unobserved or saturated, VolumeDev::freecell) steps by the
 //    truncation distance without reading voxels: the reference's step there
 //    is the truncation (unobserved centre) or the interpolation of
-//    saturated values, which is the truncation to within 1e-6 relative, and
-//    never ends the march (free_ok).
-// Voxel values: FP32 form sdf in metres; mixed form f16 sdf / truncation
-// (scaled back by the truncation after the sum).
+//    saturated values (f16 value exactly 1), which is the truncation up to
+//    the rounding of the weights, and never ends the march (free_ok).
+// The FP32 drop-in keeps raycast_exact_px: its targets decide the tracked
+// poses, whose bar against the reference (1e-4 m / 1e-4 rad per frame)
+// holds only with the reference's own rounding in the march -- with this
+// march in the FP32 form, tracked poses left that bar after six to nine
+// frames on the parity sequences, through the solver's discrete
+// convergence test (an extra or a missing iteration moves a pose by up to
+// the 1e-3 increment threshold).
 template <bool FP16>
 struct Vox;
-template <>
-struct Vox<false> {
-  using raw_t = uint2;
-  static __device__ raw_t load(const VolumeDev& v, int ptr, int lin) {
-    if (ptr < 0) return make_uint2(0u, 0u);
-    return __ldg(reinterpret_cast<const uint2*>(v.voxels + (size_t)ptr * kBlockVox + lin));
-  }
-  static __device__ int w(raw_t r) { return (int)(r.x >> 24); }
-  static __device__ float val(raw_t r) { return __uint_as_float(r.y); }
-  static __device__ float unit(const DTsdf&) { return 1.0f; }
-  static __device__ uchar4 color(const VolumeDev&, raw_t r, int, int) {
-    return make_uchar4(r.x & 0xff, (r.x >> 8) & 0xff, (r.x >> 16) & 0xff, 0);
-  }
-  static constexpr bool kHasColor = true;
-};
 template <>
 struct Vox<true> {
   using raw_t = unsigned;
@@ -696,7 +828,6 @@ struct Vox<true> {
     return (v.colors && ptr >= 0) ? v.colors[(size_t)ptr * kBlockVox + lin]
                                   : make_uchar4(0, 0, 0, 0);
   }
-  static constexpr bool kHasColor = false;  // colour lives in v.colors
 };
 
 // The interpolated sample at q (voxel units) whose centre voxel raw0 (heap
@@ -750,7 +881,7 @@ __device__ inline VoxelSample interp(const VolumeDev& v, F3 q, typename Vox<FP16
 
 // The block of a cell's low corner through the ray's cache, with its
 // free-cell flag (0 where no flags are kept).
-__device__ inline int cell_block_free(const VolumeDev& v, int bx, int by, int bz, BlockCache& bc,
+__device__ inline int cell_block_free(const VolumeDev& v, int bx, int by, int bz, FreeCache& bc,
                                       int* free) {
   if (bx != bc.x || by != bc.y || bz != bc.z) {
     bc.x = bx;
@@ -779,10 +910,11 @@ __device__ inline bool raycast_px(const VolumeDev& v, const DSensor& s, const M4
   const F3 d = f3((T.m[0] * axf + T.m[1] * ayf + T.m[2]) * inv_vs,
                   (T.m[4] * axf + T.m[5] * ayf + T.m[6]) * inv_vs,
                   (T.m[8] * axf + T.m[9] * ayf + T.m[10]) * inv_vs);
-  BlockCache bc, bc0;  // the cell's low-corner block (with its flag); the centre voxel's block
+  FreeCache bc;   // the cell's low-corner block, with its flag
+  BlockCache bc0;  // the centre voxel's block where it is another
   bc.x = bc.y = bc.z = bc0.x = bc0.y = bc0.z = 0x7fffffff;
   bc.ptr = bc0.ptr = -1;
-  bc.free = bc0.free = 0;
+  bc.free = 0;
   float cur = 0.0f;
   int steps = 0;
   bool over = false;
@@ -806,7 +938,9 @@ __device__ inline bool raycast_px(const VolumeDev& v, const DSensor& s, const M4
     }
     const int gx = (int)flx + (q.x - flx >= 0.5f), gy = (int)fly + (q.y - fly >= 0.5f),
               gz = (int)flz + (q.z - flz >= 0.5f);
-    const int ptr = block_ptr(v, blk_of(gx), blk_of(gy), blk_of(gz), bc0);
+    // the centre voxel's block: mostly the cell's own, already resolved
+    const int ptr = (blk_of(gx) == bc.x && blk_of(gy) == bc.y && blk_of(gz) == bc.z)
+                        ? bc.ptr : block_ptr(v, blk_of(gx), blk_of(gy), blk_of(gz), bc0);
     const int lin = lin_of(gx, gy, gz);
     const typename V::raw_t raw = V::load(v, ptr, lin);
     if (V::w(raw) == 0) {
@@ -876,7 +1010,8 @@ __device__ inline void raycast_tile(const VolumeDev& v, const DSensor& s,
       skip_to = fminf(__uint_as_float(B.near8[f]), __uint_as_float(B.near64[c]));
       skip_far = fmaxf(__uint_as_float(B.far8[f]), __uint_as_float(B.far64[c]));
     }
-    const bool o = raycast_px<MIXED>(v, s, T, x, y, skip_to, skip_far, depth_out, rgb_out);
+    const bool o = MIXED ? raycast_px<true>(v, s, T, x, y, skip_to, skip_far, depth_out, rgb_out)
+                         : raycast_exact_px(v, s, T, x, y, skip_to, skip_far, depth_out, rgb_out);
     if (o) atomicAdd(&over, 1);
   }
   __syncthreads();

@@ -14,18 +14,25 @@ struct VolumeDev {
   dyn_voxel* voxels;              // FP32 form: num_blocks * 512, x-major per block
   unsigned* vox16;                // mixed form: {f16 sdf | u16 weight << 16} per voxel
   uchar4* colors;                 // mixed form: r,g,b per voxel (null: no colour kept)
-  // Free-space summaries per heap index (null: not kept): nonsat = voxels
-  // that are observed and not saturated (t.sat_lo), kept exact by the
-  // integration; freecell = 1 when every voxel a trilinear cell keyed in the
-  // block can read (the block and its seven upper neighbours, missing
-  // neighbours included) is unobserved or saturated, so the raycast's
-  // interpolated sdf there is the truncation distance.  freecell may be 0
-  // where it could be 1, never the reverse.
-  int* nonsat;
-  unsigned char* freecell;
   int fp16;                       // 1: mixed-precision voxels (vox16 [+ colors])
   Counters* cnt;
   DTsdf t;
+  // Free-space summaries per heap index, kept for the mixed forms (null in
+  // the FP32 form, whose raycast evaluates every sample): nonsat = voxels
+  // that are observed and not saturated, kept exact by the integration;
+  // freecell = 1 when every voxel a trilinear cell keyed in the block can
+  // read (the block and its seven upper neighbours, missing neighbours
+  // included) is unobserved or saturated, so the raycast's interpolated sdf
+  // there is the truncation distance.  freecell may be 0 where it could be
+  // 1, never the reverse.  A mixed voxel is saturated when its f16 value is
+  // exactly 1 (free space); an FP32 voxel (the upload's count, for a volume
+  // that keeps summaries) when sdf >= sat_lo, the truncation distance to
+  // within 1e-6 relative.  free_ok: sat_lo >= vs, so a saturated sample
+  // never ends a march (flags are set only then).
+  int* nonsat;
+  unsigned char* freecell;
+  float sat_lo;
+  int free_ok;
 };
 
 void launch_volume_clear(const VolumeDev& v, cudaStream_t st);

@@ -59,8 +59,8 @@ struct HostVolume {
     v.t.bucket_size = bsz;
     v.t.num_blocks = num_blocks;
     v.t.max_w = 255;
-    v.t.sat_lo = (float)((double)trunc * (1.0 - 1e-6));
-    v.t.free_ok = v.t.sat_lo >= vs ? 1 : 0;
+    v.sat_lo = (float)((double)trunc * (1.0 - 1e-6));
+    v.free_ok = v.sat_lo >= vs ? 1 : 0;
   }
   int n() const { return std::min(cnt.nalloc, v.t.num_blocks); }
 };

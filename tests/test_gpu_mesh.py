@@ -32,7 +32,7 @@ def mesh_host(tmp_path_factory):
 
 def small_rgb():
     p = configs.preset("cfg2")
-    p["tsdf"].update(num_blocks=1 << 15, num_buckets=1 << 16)
+    p["tsdf"].update(num_blocks=1 << 16, num_buckets=1 << 16)
     p["sensor"].update(rows=120, cols=160, fx=131.25, fy=131.25, cx=79.5, cy=59.5)
     return p
 
