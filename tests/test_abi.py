@@ -150,7 +150,8 @@ def test_session_bytes_follow_the_voxel_form():
     abi.check("bytes", lib.dyn_session_bytes(C.byref(t), C.byref(s), 1, C.byref(n16)))
     vox = t.num_blocks * 512
     # FP32 voxels are 8 bytes; the mixed bound counts 4 + 4 (colour kept)
-    assert n32.value - n16.value == 0
+    # plus the raycast's free-space summaries (5 bytes per block)
+    assert n16.value - n32.value == 5 * t.num_blocks
     assert n32.value > vox * 8
     assert lib.dyn_session_bytes(C.byref(t), C.byref(s), 0, None) == 1
 
