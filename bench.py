@@ -327,6 +327,14 @@ def config_block(args, p):
                   f"{t['num_buckets'] * t['bucket_size'] * 16 / 2**20:.0f} MiB) exceeds the 126 MB L2"}
 
 
+_T0 = time.perf_counter()
+
+
+def note(what: str) -> None:
+    """Progress of the run on stderr (the JSON line stays alone on stdout)."""
+    print(f"[bench {time.perf_counter() - _T0:7.1f} s] {what}", file=sys.stderr, flush=True)
+
+
 def run_ours(args):
     import numpy as np
 
@@ -336,6 +344,7 @@ def run_ours(args):
     nframes = args.warmup + args.steps
     workers = max(1, min(32, ((os.cpu_count() or 2) - 1) // max(world, 1)))
     depth, rgb, poses = make_frames(args.config, args.seed + rank, nframes, workers)
+    note("frames rendered")
 
     import torch
     from dynamap_b200 import abi, configs
@@ -371,6 +380,7 @@ def run_ours(args):
         abi.check("stream", lib.dyn_session_stream(m.h, C.byref(ptr)))
         return torch.cuda.ExternalStream(ptr.value, device=torch.device("cuda", local))
 
+    note("pass A: device throughput")
     # ---- pass A: device throughput --------------------------------------
     with Session(t, g, b, s, precision=prec, device=local) as m:
         m.set_pose(poses[0])
@@ -424,6 +434,7 @@ def run_ours(args):
                                "vs_fp32": elapsed_a / el}
         barrier()
 
+    note("pass B: latency and stages")
     # ---- pass B: per-frame latency and stage times ------------------------
     lat_dev, lat_host, stats = [], [], []
     with Session(t, g, b, s, precision=prec, device=local) as m:
@@ -448,6 +459,7 @@ def run_ours(args):
         stage_ms = {abi.STAGES[k]: ms[k] / max(nfr.value, 1) for k in range(len(abi.STAGES))}
     barrier()
 
+    note("pass C: end to end")
     # ---- pass C: end to end through the host API ---------------------------
     pin_d = torch.from_numpy(depth).pin_memory()
     pin_c = torch.from_numpy(rgb).pin_memory() if has_rgb else None
@@ -463,8 +475,13 @@ def run_ours(args):
         h0 = time.perf_counter()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for i in range(args.warmup, nframes):
-            m.process(d_np[i], c_np[i] if has_rgb else None, strict=False)
+        # two frames in flight: frame k+1 is submitted (its copy overlapping
+        # frame k's work) before frame k's result is read
+        m.submit(d_np[args.warmup], c_np[args.warmup] if has_rgb else None)
+        for i in range(args.warmup + 1, nframes):
+            m.submit(d_np[i], c_np[i] if has_rgb else None)
+            m.result(strict=False)
+        m.result(strict=False)
         e1.record(stream)
         torch.cuda.synchronize()
         elapsed_c_host = time.perf_counter() - h0
@@ -475,11 +492,13 @@ def run_ours(args):
     # shortened serving run
     batched = serving = None
     if args.batched and prec == abi.PRECISION_FP32:
+        note("batched block")
         del d_dev, c_dev, pin_d, pin_c
         torch.cuda.empty_cache()
         batched = measure_batched(args, ranks, local, args.sessions, args.steps, args.warmup,
                                   ["mixed", "band"], e2e=True)
     if args.serving and prec == abi.PRECISION_FP32:
+        note("serving block")
         serving = measure_serving(args, ranks, local, args.embed_serve_seconds, "band")
 
     if rank != 0:
@@ -511,6 +530,7 @@ def run_ours(args):
     # tracking accuracy against the ground truth
     gt = poses[args.warmup:nframes]
     ate = float(np.sqrt(np.mean([np.sum((a[:3, 3] - b_[:3, 3]) ** 2) for a, b_ in zip(track, gt)])))
+    note("cpu baseline and FP64 accuracy")
     cpu = cpu_baseline(args.config, depth, rgb, poses, seconds=args.cpu_seconds) \
         if not args.no_cpu else None
     acc = accuracy_vs_fp64(p, depth, rgb, poses, args.fp64_frames, local) \

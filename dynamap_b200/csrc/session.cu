@@ -63,13 +63,20 @@ void release(dyn_session* s) {
     for (auto& m : s->batch->ss)
       if (m == s) m = nullptr;
   }
+  if (s->copy_stream) cudaStreamSynchronize(s->copy_stream);
   if (s->stream) cudaStreamSynchronize(s->stream);
   if (s->exec) cudaGraphExecDestroy(s->exec);
+  if (s->exec_1) cudaGraphExecDestroy(s->exec_1);
   for (void* p : s->allocs) cudaFree(p);
-  if (s->h_depth) cudaFreeHost(s->h_depth);
-  if (s->h_rgb) cudaFreeHost(s->h_rgb);
-  if (s->h_res) cudaFreeHost(s->h_res);
+  for (void* p : {(void*)s->h_depth, (void*)s->h_rgb, (void*)s->h_res, (void*)s->h_depth_1,
+                  (void*)s->h_rgb_1, (void*)s->h_res_1, (void*)s->h_res_aux})
+    if (p) cudaFreeHost(p);
   if (s->h2d_done) cudaEventDestroy(s->h2d_done);
+  for (int k = 0; k < 2; ++k) {
+    if (s->ev_h2d[k]) cudaEventDestroy(s->ev_h2d[k]);
+    if (s->ev_done[k]) cudaEventDestroy(s->ev_done[k]);
+  }
+  if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
   for (int k = 0; k < DYN_NUM_STAGES; ++k)
     if (s->ev[k]) cudaEventDestroy(s->ev[k]);
   if (s->stream) cudaStreamDestroy(s->stream);
@@ -362,6 +369,8 @@ dyn_status copy_frame_in(dyn_session* s, const uint16_t* depth, const uint8_t* r
 }
 
 dyn_status upload_frame(dyn_session* s, const uint16_t* depth, const uint8_t* rgb) {
+  // no pipelined copy may still read slot 0's staging buffers
+  DYN_CUDA(cudaStreamSynchronize(s->copy_stream));
   // the staging buffers may still feed the previous frame's copies
   DYN_CUDA(cudaEventSynchronize(s->h2d_done));
   dyn_status r = copy_frame_in(s, depth, rgb, s->stream);
@@ -378,13 +387,102 @@ Marks session_marks(dyn_session* s) {
   return m;
 }
 
-dyn_status launch_frame(dyn_session* s) {
-  if (!s->exec) {
-    dyn_status r = capture_frame(s->d_sd, s->shape, s->d_res, s->h_res, s->stream,
-                                 session_marks(s), &s->exec, &s->kernels_per_frame);
+// ---- frames through the session's graphs, up to two in flight
+struct SlotIO {
+  uint16_t* d_u16;
+  uint8_t* d_rgb;
+  int* d_flag;
+  int* flag_host;
+  uint16_t** h_depth;
+  uint8_t** h_rgb;
+  ResultBlock* h_res;
+  cudaGraphExec_t* exec;
+  SessDev* d_sd;
+};
+SlotIO slot_io(dyn_session* s, int k) {
+  if (k == 0)
+    return {s->d_u16, s->d_rgb, s->d_rgb_flag, &s->rgb_flag_host, &s->h_depth, &s->h_rgb,
+            s->h_res, &s->exec, s->d_sd};
+  return {s->d_u16_1, s->d_rgb_1, s->d_rgb_flag_1, &s->rgb_flag_host_1, &s->h_depth_1,
+          &s->h_rgb_1, s->h_res_1, &s->exec_1, s->d_sd_1};
+}
+
+// The frame's inputs into slot k on the copy stream: host pointers (pinned
+// ones read directly, others through the slot's pinned staging) or device
+// pointers.
+dyn_status stage_slot(dyn_session* s, int k, const uint16_t* depth, const uint8_t* rgb,
+                      bool device_src) {
+  SlotIO io = slot_io(s, k);
+  cudaStream_t cs = s->copy_stream;
+  const size_t nd = s->npx * sizeof(uint16_t), nc = s->npx * 3;
+  // the slot's staging may still feed its last copy; its device inputs may
+  // still be read by the frame two back
+  DYN_CUDA(cudaEventSynchronize(s->ev_h2d[k]));
+  DYN_CUDA(cudaStreamWaitEvent(cs, s->ev_done[k], 0));
+  auto put = [&](void* dst, const void* src, size_t n, void** stage) -> dyn_status {
+    if (device_src) {
+      DYN_CUDA(cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToDevice, cs));
+    } else if (is_pinned(src)) {
+      DYN_CUDA(cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, cs));
+    } else {
+      if (!*stage) {
+        if (cudaMallocHost(stage, n) != cudaSuccess) {
+          cudaGetLastError();
+          return DYN_ERR_OOM;
+        }
+      }
+      std::memcpy(*stage, src, n);
+      DYN_CUDA(cudaMemcpyAsync(dst, *stage, n, cudaMemcpyHostToDevice, cs));
+    }
+    return DYN_OK;
+  };
+  DYN_TRY(put(io.d_u16, depth, nd, reinterpret_cast<void**>(io.h_depth)));
+  if (rgb) DYN_TRY(put(io.d_rgb, rgb, nc, reinterpret_cast<void**>(io.h_rgb)));
+  const int v = rgb ? 1 : 0;
+  if (*io.flag_host != v) {
+    DYN_CUDA(cudaMemsetAsync(io.d_flag, v, sizeof(int), cs));
+    *io.flag_host = v;
+  }
+  DYN_CUDA(cudaEventRecord(s->ev_h2d[k], cs));
+  return DYN_OK;
+}
+
+// Slot k's frame graph on the session stream once its inputs are in.
+dyn_status launch_slot(dyn_session* s, int k) {
+  SlotIO io = slot_io(s, k);
+  if (!*io.exec) {
+    dyn_status r = capture_frame(io.d_sd, s->shape, s->d_res, io.h_res, s->stream,
+                                 session_marks(s), io.exec, &s->kernels_per_frame);
     if (r != DYN_OK) return r;
   }
-  DYN_CUDA(cudaGraphLaunch(s->exec, s->stream));
+  DYN_CUDA(cudaStreamWaitEvent(s->stream, s->ev_h2d[k], 0));
+  DYN_CUDA(cudaGraphLaunch(*io.exec, s->stream));
+  DYN_CUDA(cudaEventRecord(s->ev_done[k], s->stream));
+  return DYN_OK;
+}
+
+// One frame: optional pose hint (stream-ordered after the frames in
+// flight), inputs into the next slot, the graph.  With two frames in
+// flight the older one's result is given up (its slot is reused).
+dyn_status submit_frame(dyn_session* s, const uint16_t* depth, const uint8_t* rgb,
+                        bool device_src, const float* hint) {
+  if (s->n_inflight == 2) {
+    s->inflight[0] = s->inflight[1];
+    s->n_inflight = 1;
+  }
+  if (hint) {
+    double H[16];
+    for (int k = 0; k < 16; ++k) H[k] = (double)hint[k];
+    // pageable source: staged before the call returns
+    DYN_CUDA(cudaMemcpyAsync(s->d_pose_in, H, sizeof(H), cudaMemcpyHostToDevice, s->stream));
+    launch_pose_hint(s->d_pose, s->d_icp, s->d_pose_in, s->gp.compose_left, s->stream);
+    DYN_CUDA(cudaGetLastError());
+  }
+  const int k = s->next_slot;
+  DYN_TRY(stage_slot(s, k, depth, rgb, device_src));
+  DYN_TRY(launch_slot(s, k));
+  s->inflight[s->n_inflight++] = k;
+  s->next_slot = k ^ 1;
   s->pending = true;
   s->frames++;
   return DYN_OK;
@@ -447,6 +545,7 @@ dyn_status reset_state(dyn_session* s, bool sync = true) {
   if (sync) DYN_CUDA(cudaStreamSynchronize(st));
   s->frames = 0;
   s->pending = false;
+  s->n_inflight = 0;
   return DYN_OK;
 }
 
@@ -593,6 +692,11 @@ dyn_status alloc_device_buffers(dyn_session* s) {
   DYN_TRY(s->dalloc(&s->d_res, sizeof(ResultBlock)));
   DYN_TRY(s->dalloc(&s->d_btab, sizeof(BilateralTable)));
   DYN_TRY(s->dalloc(&s->d_sd, sizeof(SessDev)));
+  // the second input slot of pipelined frames
+  DYN_TRY(s->dalloc(&s->d_u16_1, s->npx * 2));
+  DYN_TRY(s->dalloc(&s->d_rgb_1, s->npx * 3));
+  DYN_TRY(s->dalloc(&s->d_rgb_flag_1, sizeof(int)));
+  DYN_TRY(s->dalloc(&s->d_sd_1, sizeof(SessDev)));
   return DYN_OK;
 }
 
@@ -657,15 +761,23 @@ dyn_status create_session(const dyn_tsdf_params* tsdf, const dyn_gn_params* gn,
       return r;              \
     }                        \
   } while (0)
-  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreateWithFlags(&s->h2d_done, cudaEventDisableTiming) != cudaSuccess) {
+  bool ok = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreateWithFlags(&s->h2d_done, cudaEventDisableTiming) == cudaSuccess;
+  for (int k = 0; k < 2 && ok; ++k)
+    ok = cudaEventCreateWithFlags(&s->ev_h2d[k], cudaEventDisableTiming) == cudaSuccess &&
+         cudaEventCreateWithFlags(&s->ev_done[k], cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) {
+    cudaGetLastError();
     release(s);
     return DYN_ERR_CUDA;
   }
   TRY(alloc_device_buffers(s));
   if (mem.host_staging) {
     TRY(ensure_staging(s));
-    if (cudaMallocHost(&s->h_res, sizeof(ResultBlock)) != cudaSuccess) {
+    if (cudaMallocHost(&s->h_res, sizeof(ResultBlock)) != cudaSuccess ||
+        cudaMallocHost(&s->h_res_1, sizeof(ResultBlock)) != cudaSuccess ||
+        cudaMallocHost(&s->h_res_aux, sizeof(ResultBlock)) != cudaSuccess) {
       cudaGetLastError();
       release(s);
       return DYN_ERR_OOM;
@@ -680,14 +792,22 @@ dyn_status create_session(const dyn_tsdf_params* tsdf, const dyn_gn_params* gn,
     cudaMemsetAsync(s->d_sint[l], 0, m * 4, s->stream);
   }
   cudaMemsetAsync(s->d_rgb_flag, 0, sizeof(int), s->stream);
+  cudaMemsetAsync(s->d_rgb_flag_1, 0, sizeof(int), s->stream);
   s->rgb_flag_host = 0;
+  s->rgb_flag_host_1 = 0;
   fill_sessdev(s);
+  s->hsd_1 = s->hsd;  // slot 1: its own inputs, everything else shared
+  s->hsd_1.u16 = s->d_u16_1;
+  s->hsd_1.rgb = s->d_rgb_1;
+  s->hsd_1.rgb_flag = s->d_rgb_flag_1;
   dyn_session* self = s;
   s->shape = make_shape(&self, 1, s->d_gvis, s->d_gcount, tsdf->num_blocks);
   if (cudaMemcpyAsync(s->d_btab, &s->btab, sizeof(BilateralTable), cudaMemcpyHostToDevice,
                       s->stream) != cudaSuccess ||
       cudaMemcpyAsync(s->d_sd, &s->hsd, sizeof(SessDev), cudaMemcpyHostToDevice, s->stream) !=
-          cudaSuccess) {
+          cudaSuccess ||
+      cudaMemcpyAsync(s->d_sd_1, &s->hsd_1, sizeof(SessDev), cudaMemcpyHostToDevice,
+                      s->stream) != cudaSuccess) {
     release(s);
     return DYN_ERR_CUDA;
   }
@@ -777,49 +897,39 @@ dyn_status dyn_session_set_pose(dyn_session* s, const float pose[16]) {
 dyn_status dyn_frame_submit(dyn_session* s, const uint16_t* depth_host, const uint8_t* rgb_host) {
   if (!s || !depth_host || s->batch || s->owner_stream) return DYN_ERR_INVALID_ARG;
   DeviceGuard dg(s->device);
-  dyn_status r = upload_frame(s, depth_host, rgb_host);
-  if (r != DYN_OK) return r;
-  return launch_frame(s);
+  return submit_frame(s, depth_host, rgb_host, false, nullptr);
 }
 
 dyn_status dyn_frame_submit_hint(dyn_session* s, const uint16_t* depth_host,
                                  const uint8_t* rgb_host, const float pose_hint[16]) {
   if (!s || !depth_host || s->batch || s->owner_stream) return DYN_ERR_INVALID_ARG;
-  if (!pose_hint) return dyn_frame_submit(s, depth_host, rgb_host);
   DeviceGuard dg(s->device);
-  double H[16];
-  for (int k = 0; k < 16; ++k) H[k] = (double)pose_hint[k];
-  // pageable source: staged before the call returns; stream-ordered after
-  // the previous frame (whose pose the hint is taken relative to)
-  DYN_CUDA(cudaMemcpyAsync(s->d_pose_in, H, sizeof(H), cudaMemcpyHostToDevice, s->stream));
-  launch_pose_hint(s->d_pose, s->d_icp, s->d_pose_in, s->gp.compose_left, s->stream);
-  DYN_CUDA(cudaGetLastError());
-  dyn_status r = upload_frame(s, depth_host, rgb_host);
-  if (r != DYN_OK) return r;
-  return launch_frame(s);
+  return submit_frame(s, depth_host, rgb_host, false, pose_hint);
 }
 
 dyn_status dyn_frame_submit_device(dyn_session* s, const uint16_t* depth_dev, const uint8_t* rgb_dev) {
   if (!s || !depth_dev || s->batch || s->owner_stream) return DYN_ERR_INVALID_ARG;
   DeviceGuard dg(s->device);
-  DYN_CUDA(cudaMemcpyAsync(s->d_u16, depth_dev, s->npx * 2, cudaMemcpyDeviceToDevice, s->stream));
-  if (rgb_dev)
-    DYN_CUDA(cudaMemcpyAsync(s->d_rgb, rgb_dev, s->npx * 3, cudaMemcpyDeviceToDevice, s->stream));
-  DYN_TRY(set_rgb_flag(s, rgb_dev != nullptr, s->stream));
-  return launch_frame(s);
+  return submit_frame(s, depth_dev, rgb_dev, true, nullptr);
 }
 
 dyn_status dyn_frame_result(dyn_session* s, float pose_out[16], dyn_frame_stats* stats) {
   if (!s) return DYN_ERR_INVALID_ARG;
-  if (!s->pending) return DYN_ERR_NOT_READY;
+  if (s->n_inflight == 0) return DYN_ERR_NOT_READY;
   DeviceGuard dg(s->device);
-  DYN_CUDA(cudaStreamSynchronize(s->stream));
-  s->pending = false;
-  if (s->profile) add_stage_times(s->ev, s->stage_ms, &s->prof_frames);
+  const int k = s->inflight[0];
+  DYN_CUDA(cudaEventSynchronize(s->ev_done[k]));
+  s->inflight[0] = s->inflight[1];
+  s->n_inflight--;
+  s->pending = s->n_inflight > 0;
+  // stage events are re-recorded by every frame: read them only when no
+  // later frame is in flight
+  if (s->profile && s->n_inflight == 0) add_stage_times(s->ev, s->stage_ms, &s->prof_frames);
+  const ResultBlock& res = *slot_io(s, k).h_res;
   if (pose_out)
-    for (int k = 0; k < 16; ++k) pose_out[k] = (float)s->h_res->pose.pose[k];
-  if (stats) fill_stats(s, *s->h_res, stats);
-  return counters_status(s->h_res->cnt);
+    for (int j = 0; j < 16; ++j) pose_out[j] = (float)res.pose.pose[j];
+  if (stats) fill_stats(s, res, stats);
+  return counters_status(res.cnt);
 }
 
 dyn_status dyn_integrate_with_pose(dyn_session* s, const uint16_t* depth_host,
@@ -835,12 +945,12 @@ dyn_status dyn_integrate_with_pose(dyn_session* s, const uint16_t* depth_host,
   bump_frame_kernel<<<1, 32, 0, s->stream>>>(s->d_pose);
   enqueue_map_update(s->d_sd, s->shape, s->stream, none);
   gather_results_kernel<<<1, 128, 0, s->stream>>>(s->d_sd, 1, nullptr, s->d_res);
-  DYN_CUDA(cudaMemcpyAsync(s->h_res, s->d_res, sizeof(ResultBlock), cudaMemcpyDeviceToHost,
+  DYN_CUDA(cudaMemcpyAsync(s->h_res_aux, s->d_res, sizeof(ResultBlock), cudaMemcpyDeviceToHost,
                            s->stream));
   DYN_CUDA(cudaStreamSynchronize(s->stream));
   DYN_CUDA(cudaGetLastError());
   s->frames++;
-  return counters_status(s->h_res->cnt);
+  return counters_status(s->h_res_aux->cnt);
 }
 
 dyn_status dyn_solver_solve(dyn_session* s, const float* target_depth_host,
@@ -885,13 +995,14 @@ dyn_status dyn_solver_solve(dyn_session* s, const float* target_depth_host,
   enqueue_icp(s->d_sd, s->shape, st);
   fused_pose_finalize(s->d_sd, s->shape, 0, st);
   gather_results_kernel<<<1, 128, 0, st>>>(s->d_sd, 1, nullptr, s->d_res);
-  DYN_CUDA(cudaMemcpyAsync(s->h_res, s->d_res, sizeof(ResultBlock), cudaMemcpyDeviceToHost, st));
+  DYN_CUDA(cudaMemcpyAsync(s->h_res_aux, s->d_res, sizeof(ResultBlock), cudaMemcpyDeviceToHost,
+                           st));
   DYN_CUDA(cudaStreamSynchronize(st));
   DYN_CUDA(cudaGetLastError());
-  for (int k = 0; k < 16; ++k) pose_inout[k] = (float)s->h_res->pose.pose[k];
+  for (int k = 0; k < 16; ++k) pose_inout[k] = (float)s->h_res_aux->pose.pose[k];
   if (increment_out)
-    for (int k = 0; k < 6; ++k) increment_out[k] = s->h_res->pose.last_inc[k];
-  if (stats) fill_stats(s, *s->h_res, stats);
+    for (int k = 0; k < 6; ++k) increment_out[k] = s->h_res_aux->pose.last_inc[k];
+  if (stats) fill_stats(s, *s->h_res_aux, stats);
   return DYN_OK;
 }
 
@@ -1098,10 +1209,11 @@ dyn_status dyn_session_profile(dyn_session* s, int32_t enable) {
   if (en && !s->ev[0])
     for (int k = 0; k < DYN_NUM_STAGES; ++k) DYN_CUDA(cudaEventCreate(&s->ev[k]));
   if (en != s->profile) {
-    if (s->exec) {
-      cudaGraphExecDestroy(s->exec);
-      s->exec = nullptr;
-    }
+    for (cudaGraphExec_t* e : {&s->exec, &s->exec_1})
+      if (*e) {
+        cudaGraphExecDestroy(*e);
+        *e = nullptr;
+      }
     s->profile = en;
   }
   return DYN_OK;

@@ -168,7 +168,32 @@ struct dyn_session {
   int kernels_per_frame = 0;
   bool debug_maps = false;
   int frames = 0;
-  bool pending = false;
+  bool pending = false;  // a frame submitted whose result has not been read
+  // Two frames in flight (dyn_frame_submit before the previous frame's
+  // dyn_frame_result): input slot 0 is d_u16 / d_rgb / d_rgb_flag with
+  // h_depth / h_rgb, h_res, exec and d_sd above; slot 1 has its own.  A
+  // frame's host->device copy runs on copy_stream and overlaps the previous
+  // frame's graph on 'stream'; ev_h2d[k] marks slot k's copy done (the
+  // graph waits for it, the next copy into slot k's staging waits for it),
+  // ev_done[k] slot k's graph done (the next copy into slot k's device
+  // buffers waits for it).  Results are read in submission order.
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_h2d[2] = {};
+  cudaEvent_t ev_done[2] = {};
+  uint16_t* d_u16_1 = nullptr;
+  uint8_t* d_rgb_1 = nullptr;
+  int* d_rgb_flag_1 = nullptr;
+  int rgb_flag_host_1 = -1;
+  SessDev* d_sd_1 = nullptr;
+  SessDev hsd_1;
+  uint16_t* h_depth_1 = nullptr;
+  uint8_t* h_rgb_1 = nullptr;
+  ResultBlock* h_res_1 = nullptr;
+  cudaGraphExec_t exec_1 = nullptr;
+  ResultBlock* h_res_aux = nullptr;  // results of the calls outside the frame graphs
+  int inflight[2] = {0, 0};          // slots of the frames in flight, oldest first
+  int n_inflight = 0;
+  int next_slot = 0;
 
   // device memory: cudaMalloc per buffer, or carved from a region a server
   // reserved (region != null), or only counted (measure)

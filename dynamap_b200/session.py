@@ -121,9 +121,14 @@ class Session:
 
     # ---- frames
     def submit(self, depth: np.ndarray, rgb: np.ndarray | None = None, pose_hint=None) -> None:
+        """One frame (dyn_frame_submit).  Up to two frames may be in flight:
+        submit frame k+1 before reading frame k's result and its copy to the
+        device overlaps frame k's work; results come back in order."""
         d = np.ascontiguousarray(depth, np.uint16)
         r = None if rgb is None else np.ascontiguousarray(rgb, np.uint8)
-        self._keep = (d, r)
+        # page-locked inputs are read by the copy after the call returns:
+        # keep the last two frames' arrays alive
+        self._keep = (getattr(self, "_keep", (None,))[-1], (d, r))
         if pose_hint is None:
             abi.check("dyn_frame_submit", self.lib.dyn_frame_submit(self.h, _ptr(d), _ptr(r)))
         else:

@@ -198,9 +198,15 @@ dyn_status dyn_session_set_pose(dyn_session* s, const float pose[16]);
 
 /* builder::buildModelLS (builder.cu:70-139) for one frame: track against
  * the model (or the previous frame in mode 0), integrate, raycast the
- * target for the next frame.  Enqueued on the session's stream; returns
- * before the GPU finishes.  Host buffers are copied before return
- * (they may be reused immediately). */
+ * target for the next frame.  Enqueued; returns before the GPU finishes.
+ * Pageable host buffers are copied before return (they may be reused at
+ * once); page-locked ones (cudaHostAlloc / cudaHostRegister) are read by
+ * the device copy after return and must stay unchanged until the frame's
+ * dyn_frame_result.  Two frames may be in flight: submitting frame k+1
+ * before reading frame k's result overlaps frame k+1's host->device copy
+ * (on the session's copy stream, into a second input slot) with frame k's
+ * work; dyn_frame_result returns results in submission order.  A third
+ * submit gives up the oldest unread result. */
 dyn_status dyn_frame_submit(dyn_session* s, const uint16_t* depth_host,
                             const uint8_t* rgb_host /* nullable */);
 /* Same, with the frame already resident on the device. */
@@ -214,7 +220,8 @@ dyn_status dyn_frame_submit_device(dyn_session* s, const uint16_t* depth_dev,
 dyn_status dyn_frame_submit_hint(dyn_session* s, const uint16_t* depth_host,
                                  const uint8_t* rgb_host /* nullable */,
                                  const float pose_hint[16] /* nullable */);
-/* Waits for the last submitted frame; returns its pose and counters. */
+/* Waits for the oldest frame in flight; returns its pose and counters
+ * (DYN_ERR_NOT_READY when no frame is in flight). */
 dyn_status dyn_frame_result(dyn_session* s, float pose_out[16],
                             dyn_frame_stats* stats /* nullable */);
 

@@ -1,0 +1,435 @@
+// nodeHandler/nodeHandler.h -- the streaming front end: RGB-D streams in,
+// one pose per frame out, through the serving loop (dyn_server).
+//
+// It takes the place of the reference's ROS node
+// (include/nodeHandler/nodeHandler.h:50-90, nodeHandler.cpp): there each
+// synchronised depth + colour message pair reaches kinect_callback
+// (nodeHandler.cpp:170), which converts the images and runs the mapper, and
+// tf_publisher (:139-153) broadcasts the estimated camera pose.  ROS is not
+// part of this build, so a stream is fed in-process: kinect_callback may be
+// called from any thread (a camera driver's, a decoder's, one of the
+// replayers below) and copies the frame into the stream's queue; one
+// serving thread steps the server whenever frames wait -- all streams'
+// waiting frames fused into one launch per stage (continuous batching) --
+// and hands each result to the pose callback, in each stream's frame order.
+// Every frame is processed; a stream has at most one frame on the device at
+// a time, so its results equal the same frames stepped alone.
+//
+// Sources: TumReplayer replays a TUM-layout directory (utils::dataSet) at a
+// frame rate; PipeReader reads frames from a file descriptor (a pipe from a
+// capture process) in a small binary format (see PipeReader).
+//
+// Header-only over the C ABI of dynamap.h; needs C++17 and threads.
+#pragma once
+
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstdint>
+#include <cstring>
+#include <deque>
+#include <functional>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include <unistd.h>
+
+#include "../builder/builder.h"
+#include "../dynamap.h"
+#include "../dynamap/types.h"
+#include "../utils/dataSet.h"
+
+namespace DynaMap {
+
+class DynaMapNodeHandler {
+ public:
+  // one stream: the builder's init arguments (builder.h:51-54) plus the
+  // voxel form and the first pose
+  struct StreamConfig {
+    tsdf::tsdfProperties tsdf;
+    solver::Properties solver;
+    rgbdSensor sensor;
+    gaussianKernal kernel;
+    int mode = 1;  // 0 frame-to-frame, 1 frame-to-model
+    int precision = DYN_PRECISION_FP32;
+    Matrix4f pose0;
+    bool bilateral = true;
+  };
+  // tf_publisher's role: the frame's time stamp, its camera pose and the
+  // frame's statistics (status: the frame's dyn_status, e.g. a full heap)
+  using PoseCallback = std::function<void(int stream, double stamp, const Matrix4f& pose,
+                                          const dyn_frame_stats& stats, dyn_status status)>;
+
+  explicit DynaMapNodeHandler(size_t budget_bytes = 0, int device = 0, int max_sessions = 64) {
+    dyn_server_params p;
+    p.budget_bytes = budget_bytes;
+    p.max_sessions = max_sessions;
+    p.device = device;
+    dyn_throw("DynaMapNodeHandler", dyn_server_create(&p, &server_));
+  }
+  DynaMapNodeHandler(const DynaMapNodeHandler&) = delete;
+  DynaMapNodeHandler& operator=(const DynaMapNodeHandler&) = delete;
+  virtual ~DynaMapNodeHandler() {
+    shutdown();
+    if (server_) dyn_server_destroy(server_);
+  }
+
+  void setPoseCallback(PoseCallback cb) {
+    std::lock_guard<std::mutex> lk(mu_);
+    on_pose_ = std::move(cb);
+  }
+
+  // Admits a stream; returns its id.  Throws when the budget or the slots
+  // are exhausted (DYN_ERR_BUDGET_EXCEEDED: add it after another stream
+  // has been removed).
+  int addStream(const StreamConfig& c) {
+    std::lock_guard<std::mutex> lk(server_mu_);
+    dyn_tsdf_params t = c.tsdf.to_c();
+    dyn_gn_params g = c.solver.to_c(c.mode);
+    dyn_bilateral_params b;
+    b.diameter = c.kernel.diameter;
+    b.sigma_i = c.kernel.sigmaI;
+    b.sigma_s = c.kernel.sigmaS;
+    b.enabled = c.bilateral ? 1 : 0;
+    dyn_sensor s = c.sensor.to_c();
+    float4x4 p0 = c.pose0.to_row_major();
+    int32_t slot = -1;
+    dyn_throw("DynaMapNodeHandler::addStream",
+              dyn_server_admit(server_, &t, &g, &b, &s, c.precision, p0.entries, &slot));
+    std::lock_guard<std::mutex> lk2(mu_);
+    auto st = std::make_shared<Stream>();
+    st->slot = slot;
+    st->npx = (size_t)c.sensor.rows * c.sensor.cols;
+    st->scaler = c.sensor.depthScaler;
+    const int id = next_id_++;
+    streams_[id] = st;
+    return id;
+  }
+
+  // nodeHandler.cpp:170: one frame of a stream (uint16 depth in sensor
+  // units, rows*cols; RGB triplets or null).  The frame is copied; the call
+  // returns at once.
+  void kinect_callback(int stream, const uint16_t* depth, const uint8_t* rgb, double stamp) {
+    std::unique_lock<std::mutex> lk(mu_);
+    auto it = streams_.find(stream);
+    if (it == streams_.end() || it->second->closing)
+      dyn_throw("DynaMapNodeHandler::kinect_callback", DYN_ERR_INVALID_ARG);
+    Stream& s = *it->second;
+    Frame f;
+    f.stamp = stamp;
+    f.depth.assign(depth, depth + s.npx);
+    if (rgb) f.rgb.assign(rgb, rgb + 3 * s.npx);
+    s.queue.push_back(std::move(f));
+    ++queued_;
+    cv_.notify_all();
+  }
+  // the reference's own input: depth in metres (TYPE_32FC1), turned into
+  // sensor units (rounded depth * depthScaler, 0 where not positive)
+  void kinect_callback(int stream, const float* depth_m, const uint8_t* rgb, double stamp) {
+    size_t n = 0;
+    float scaler = 1.0f;
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      auto it = streams_.find(stream);
+      if (it == streams_.end()) dyn_throw("DynaMapNodeHandler::kinect_callback", DYN_ERR_INVALID_ARG);
+      n = it->second->npx;
+      scaler = it->second->scaler;
+    }
+    std::vector<uint16_t> u(n);
+    for (size_t i = 0; i < n; ++i) {
+      const float v = depth_m[i] * scaler;
+      u[i] = (depth_m[i] > 0.0f && v < 65535.5f) ? (uint16_t)(v + 0.5f) : (uint16_t)0;
+    }
+    kinect_callback(stream, u.data(), rgb, stamp);
+  }
+
+  // Stops taking frames for the stream; it is released once its queued
+  // frames have been processed.
+  void removeStream(int stream) {
+    std::lock_guard<std::mutex> lk(mu_);
+    auto it = streams_.find(stream);
+    if (it != streams_.end()) it->second->closing = true;
+    cv_.notify_all();
+  }
+
+  // Starts the serving thread (ros::spin's role).
+  void spin() {
+    if (worker_.joinable()) return;
+    running_ = true;
+    worker_ = std::thread([this] { serve(); });
+  }
+  // Waits until every queued frame has been processed and reported.
+  void waitIdle() {
+    std::unique_lock<std::mutex> lk(mu_);
+    idle_cv_.wait(lk, [this] { return queued_ == 0 || !running_; });
+  }
+  void shutdown() {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      running_ = false;
+    }
+    cv_.notify_all();
+    if (worker_.joinable()) worker_.join();
+    idle_cv_.notify_all();
+  }
+  // frames processed, steps run (several frames share a step)
+  int64_t framesDone() const { return frames_done_; }
+  int64_t steps() const { return steps_; }
+  dyn_server* server() const { return server_; }
+  // the session behind a stream (raycast, mesh, download), only while the
+  // stream is idle
+  dyn_session* session(int stream) {
+    std::lock_guard<std::mutex> slk(server_mu_);  // server first, as everywhere
+    std::lock_guard<std::mutex> lk(mu_);
+    auto it = streams_.find(stream);
+    if (it == streams_.end()) return nullptr;
+    dyn_session* out = nullptr;
+    dyn_server_session(server_, it->second->slot, &out);
+    return out;
+  }
+
+ private:
+  struct Frame {
+    double stamp = 0.0;
+    std::vector<uint16_t> depth;
+    std::vector<uint8_t> rgb;
+  };
+  struct Stream {
+    int32_t slot = -1;
+    size_t npx = 0;
+    float scaler = 1.0f;
+    std::deque<Frame> queue;
+    bool in_flight = false;  // a frame pushed and stepped, result not yet read
+    double stamp = 0.0;      // that frame's
+    bool closing = false;
+  };
+
+  // One pass: push the next frame of every stream without a frame on the
+  // device, step once, then report the results that are ready.
+  struct Refused {
+    int id;
+    double stamp;
+    dyn_status status;
+  };
+  void serve() {
+    std::vector<std::pair<int, std::shared_ptr<Stream>>> ready;
+    std::vector<Refused> refused;
+    while (true) {
+      ready.clear();
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait_for(lk, std::chrono::milliseconds(1), [this] {
+          if (!running_) return true;
+          for (auto& kv : streams_)
+            if (!kv.second->in_flight && !kv.second->queue.empty()) return true;
+          return in_flight_ > 0;
+        });
+        if (!running_ && in_flight_ == 0) break;
+        for (auto& kv : streams_) ready.push_back(kv);
+      }
+      int pushed = 0;
+      {
+        std::lock_guard<std::mutex> slk(server_mu_);
+        for (auto& [id, s] : ready) {
+          Frame f;
+          {
+            std::lock_guard<std::mutex> lk(mu_);
+            if (s->in_flight || s->queue.empty()) continue;
+            f = std::move(s->queue.front());
+            s->queue.pop_front();
+          }
+          const dyn_status r = dyn_server_push(server_, s->slot, f.depth.data(),
+                                               f.rgb.empty() ? nullptr : f.rgb.data());
+          if (r == DYN_ERR_NOT_READY) {  // not stepped yet: put it back
+            std::lock_guard<std::mutex> lk(mu_);
+            s->queue.push_front(std::move(f));
+            continue;
+          }
+          if (r != DYN_OK) {  // refused (a malformed frame): reported below, dropped
+            refused.push_back({id, f.stamp, r});
+            continue;
+          }
+          std::lock_guard<std::mutex> lk(mu_);
+          s->in_flight = true;
+          s->stamp = f.stamp;
+          ++in_flight_;
+          ++pushed;
+        }
+        if (pushed) {
+          int32_t n = 0;
+          dyn_throw("DynaMapNodeHandler: step", dyn_server_step(server_, &n));
+          ++steps_;
+        }
+      }
+      for (const Refused& x : refused) report(x.id, x.stamp, nullptr, nullptr, x.status);
+      refused.clear();
+      // results, in each stream's order (one frame per stream in flight)
+      for (auto& [id, s] : ready) {
+        bool fl;
+        {
+          std::lock_guard<std::mutex> lk(mu_);
+          fl = s->in_flight;
+        }
+        if (!fl) continue;
+        float pose[16];
+        dyn_frame_stats st;
+        dyn_status r;
+        {
+          std::lock_guard<std::mutex> slk(server_mu_);
+          int32_t done = 0;
+          dyn_throw("DynaMapNodeHandler: poll", dyn_server_poll(server_, s->slot, &done));
+          if (!done) continue;
+          r = dyn_server_result(server_, s->slot, pose, &st);
+        }
+        {
+          std::lock_guard<std::mutex> lk(mu_);
+          s->in_flight = false;
+          --in_flight_;
+        }
+        report(id, s->stamp, pose, &st, r);
+      }
+      // streams that were removed and have nothing left
+      std::lock_guard<std::mutex> slk(server_mu_);
+      std::lock_guard<std::mutex> lk(mu_);
+      for (auto it = streams_.begin(); it != streams_.end();) {
+        Stream& s = *it->second;
+        if (s.closing && s.queue.empty() && !s.in_flight) {
+          dyn_server_release(server_, s.slot);
+          it = streams_.erase(it);
+        } else {
+          ++it;
+        }
+      }
+    }
+  }
+
+  // the pose callback for one handed-over frame (pose null: the frame was
+  // refused), then the frame counts as done
+  void report(int id, double stamp, const float* pose, const dyn_frame_stats* st, dyn_status r) {
+    PoseCallback cb;
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      cb = on_pose_;
+    }
+    dyn_frame_stats none{};
+    if (cb)
+      cb(id, stamp, pose ? Matrix4f::from_row_major(pose) : Matrix4f(), st ? *st : none, r);
+    std::lock_guard<std::mutex> lk(mu_);
+    --queued_;
+    ++frames_done_;
+    if (queued_ == 0) idle_cv_.notify_all();
+  }
+
+  dyn_server* server_ = nullptr;
+  std::mutex mu_;         // streams, queues, counters, callback
+  std::mutex server_mu_;  // calls on the server (not thread-safe)
+  std::condition_variable cv_, idle_cv_;
+  std::map<int, std::shared_ptr<Stream>> streams_;
+  PoseCallback on_pose_;
+  std::thread worker_;
+  bool running_ = false;
+  int next_id_ = 0;
+  int64_t queued_ = 0;  // frames handed over and not yet reported
+  int in_flight_ = 0;
+  std::atomic<int64_t> frames_done_{0}, steps_{0};
+};
+
+// Replays a TUM-layout directory into a stream at 'rate_hz' frames per
+// second (0: as fast as the stream takes them), stamps from the files.
+class TumReplayer {
+ public:
+  TumReplayer(DynaMapNodeHandler& h, int stream, std::string dir, double rate_hz)
+      : h_(h), stream_(stream), dir_(std::move(dir)), rate_(rate_hz) {}
+  ~TumReplayer() { join(); }
+  void start() {
+    th_ = std::thread([this] {
+      utils::dataSet ds(dir_);
+      const auto t0 = std::chrono::steady_clock::now();
+      for (size_t k = 0; k < ds.size(); ++k) {
+        if (rate_ > 0)
+          std::this_thread::sleep_until(t0 + std::chrono::duration<double>((double)k / rate_));
+        ds.invokeNextFrame();
+        h_.kinect_callback(stream_, ds.image.depth.data(),
+                           ds.image.rgb.empty() ? nullptr : ds.image.rgb.data(), ds.stamp);
+        ++sent_;
+      }
+    });
+  }
+  void join() {
+    if (th_.joinable()) th_.join();
+  }
+  int sent() const { return sent_; }
+
+ private:
+  DynaMapNodeHandler& h_;
+  int stream_;
+  std::string dir_;
+  double rate_;
+  std::thread th_;
+  std::atomic<int> sent_{0};
+};
+
+// Frames from a file descriptor (a pipe): per frame a 32-byte header
+//   char magic[4] = "DYNF"; uint32 rows, cols, flags (bit 0: RGB follows);
+//   double stamp; uint64 reserved (0)
+// then rows*cols uint16 depth (sensor units, little-endian) and, with
+// bit 0, rows*cols*3 bytes RGB.  End of file ends the stream.
+class PipeReader {
+ public:
+  PipeReader(DynaMapNodeHandler& h, int stream, int fd, uint32_t rows, uint32_t cols)
+      : h_(h), stream_(stream), fd_(fd), rows_(rows), cols_(cols) {}
+  ~PipeReader() { join(); }
+  void start() {
+    th_ = std::thread([this] {
+      const size_t n = (size_t)rows_ * cols_;
+      std::vector<uint16_t> d(n);
+      std::vector<uint8_t> c(3 * n);
+      while (true) {
+        unsigned char hdr[32];
+        if (!read_all(hdr, sizeof hdr)) break;
+        uint32_t rows, cols, flags;
+        double stamp;
+        std::memcpy(&rows, hdr + 4, 4);
+        std::memcpy(&cols, hdr + 8, 4);
+        std::memcpy(&flags, hdr + 12, 4);
+        std::memcpy(&stamp, hdr + 16, 8);
+        if (std::memcmp(hdr, "DYNF", 4) != 0 || rows != rows_ || cols != cols_) {
+          bad_ = true;
+          break;
+        }
+        if (!read_all(d.data(), 2 * n)) break;
+        if ((flags & 1) && !read_all(c.data(), 3 * n)) break;
+        h_.kinect_callback(stream_, d.data(), (flags & 1) ? c.data() : nullptr, stamp);
+        ++sent_;
+      }
+    });
+  }
+  void join() {
+    if (th_.joinable()) th_.join();
+  }
+  int sent() const { return sent_; }
+  bool malformed() const { return bad_; }
+
+ private:
+  bool read_all(void* p, size_t n) {
+    char* q = static_cast<char*>(p);
+    while (n > 0) {
+      const ssize_t r = ::read(fd_, q, n);
+      if (r <= 0) return false;
+      q += r;
+      n -= (size_t)r;
+    }
+    return true;
+  }
+  DynaMapNodeHandler& h_;
+  int stream_, fd_;
+  uint32_t rows_, cols_;
+  std::thread th_;
+  std::atomic<int> sent_{0};
+  std::atomic<bool> bad_{false};
+};
+
+}  // namespace DynaMap

@@ -1,0 +1,101 @@
+// Streams through the front end (include/nodeHandler/nodeHandler.h): one
+// served session per line of a spec file, each fed by a TUM-layout
+// directory replayed at a frame rate or by frames on standard input.
+//   stream_example SPEC OUT
+// SPEC, one stream per line:
+//   SOURCE rows cols fx fy cx cy scaler voxel buckets blocks trunc maxdepth
+//   colour_weight precision rate_hz p00 .. p33 (first pose, row-major)
+// SOURCE: a directory, or "-" for frames on standard input (the pipe
+// format of PipeReader).  OUT, one line per frame as the pose callback
+// reports it: "stream stamp status it0 it1 it2 p00 .. p33".
+#include <cstdio>
+#include <fstream>
+#include <memory>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "nodeHandler/nodeHandler.h"
+
+using namespace DynaMap;
+
+int main(int argc, char** argv) {
+  if (argc != 3) return 2;
+  std::ifstream spec(argv[1]);
+  std::vector<std::string> sources;
+  std::vector<DynaMapNodeHandler::StreamConfig> cfgs;
+  std::vector<double> rates;
+  std::string line;
+  while (std::getline(spec, line)) {
+    if (line.empty()) continue;
+    std::istringstream ss(line);
+    std::string src;
+    DynaMapNodeHandler::StreamConfig c;
+    int log2b = 0;
+    float pose[16];
+    double rate = 0;
+    ss >> src >> c.sensor.rows >> c.sensor.cols >> c.sensor.f.x >> c.sensor.f.y >> c.sensor.c.x >>
+        c.sensor.c.y >> c.sensor.depthScaler >> c.tsdf.voxelSize >> log2b >> c.tsdf.numBlocks >>
+        c.tsdf.truncationDistance >> c.tsdf.maxSensorDepth >> c.solver.colorWeight >>
+        c.precision >> rate;
+    for (float& v : pose) ss >> v;
+    if (!ss) return 2;
+    c.tsdf.numBuckets = 1 << log2b;
+    c.tsdf.bucketSize = 10;
+    c.tsdf.minSensorDepth = 0.15f;
+    c.solver.lvlIterationNum[0] = 10;
+    c.solver.lvlIterationNum[1] = 5;
+    c.solver.lvlIterationNum[2] = 4;
+    c.solver.icpMaxDepth = c.tsdf.maxSensorDepth;
+    c.solver.huberConstant = 0.3f;
+    c.pose0 = Matrix4f::from_row_major(pose);
+    sources.push_back(src);
+    cfgs.push_back(c);
+    rates.push_back(rate);
+  }
+  std::FILE* out = std::fopen(argv[2], "w");
+  if (!out) return 2;
+  std::mutex out_mu;
+  DynaMapNodeHandler node(size_t(24) << 30);
+  node.setPoseCallback([&](int stream, double stamp, const Matrix4f& P, const dyn_frame_stats& st,
+                           dyn_status status) {
+    std::lock_guard<std::mutex> lk(out_mu);
+    std::fprintf(out, "%d %.6f %d %d %d %d", stream, stamp, (int)status, st.icp_iterations[0],
+                 st.icp_iterations[1], st.icp_iterations[2]);
+    for (int r = 0; r < 4; ++r)
+      for (int k = 0; k < 4; ++k) std::fprintf(out, " %.9g", P(r, k));
+    std::fprintf(out, "\n");
+  });
+  std::vector<int> ids;
+  for (auto& c : cfgs) ids.push_back(node.addStream(c));
+  node.spin();
+  std::vector<std::unique_ptr<TumReplayer>> replay;
+  std::unique_ptr<PipeReader> pipe;
+  for (size_t i = 0; i < sources.size(); ++i) {
+    if (sources[i] == "-") {
+      pipe.reset(new PipeReader(node, ids[i], 0, cfgs[i].sensor.rows, cfgs[i].sensor.cols));
+      pipe->start();
+    } else {
+      replay.emplace_back(new TumReplayer(node, ids[i], sources[i], rates[i]));
+      replay.back()->start();
+    }
+  }
+  int sent = 0;
+  for (auto& r : replay) {
+    r->join();
+    sent += r->sent();
+  }
+  if (pipe) {
+    pipe->join();
+    sent += pipe->sent();
+    if (pipe->malformed()) return 3;
+  }
+  node.waitIdle();
+  for (int id : ids) node.removeStream(id);
+  node.shutdown();
+  std::fclose(out);
+  std::printf("frames %d done %lld steps %lld\n", sent, (long long)node.framesDone(),
+              (long long)node.steps());
+  return node.framesDone() == sent ? 0 : 1;
+}

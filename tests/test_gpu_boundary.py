@@ -4,7 +4,7 @@ maps (dyn_raycast_maps) and tracking from a pose hint
 import numpy as np
 import pytest
 
-from dynamap_b200 import configs
+from dynamap_b200 import abi, configs
 from dynamap_b200.session import Session
 
 pytestmark = pytest.mark.gpu
@@ -61,3 +61,42 @@ def test_pose_hint(gpu_lib):
             # the true pose as the hint: tracking stays at the truth
             h = hinted.process(seq.depth[k], pose_hint=gt[k])[0]
             assert np.linalg.norm(h[:3, 3] - gt[k][:3, 3]) < 1e-2
+
+
+def test_two_frames_in_flight_give_the_sequential_results(gpu_lib):
+    """dyn_frame_submit of frame k+1 before frame k's dyn_frame_result (the
+    copy of k+1 overlapping frame k's work, through the second input slot):
+    every frame's pose and statistics equal those of one frame at a time,
+    from pageable and from page-locked frames, and device frames too."""
+    import torch
+    p = small()
+    p["sensor"].update(rows=120, cols=160, fx=131.25, fy=131.25, cx=79.5, cy=59.5)
+    seq = configs.sequence(p, seed=35, n_frames=9)
+    t, g, b, s = configs.structs(p)
+    with Session(t, g, b, s) as m:
+        m.set_pose(seq.poses[0])
+        ref = [m.process(seq.depth[k]) for k in range(len(seq.depth))]
+    pinned = torch.from_numpy(seq.depth).pin_memory().numpy()
+    dev = torch.from_numpy(seq.depth).cuda()
+    nb = seq.depth.shape[1] * seq.depth.shape[2] * 2
+    for source in ("pageable", "pinned", "device"):
+        with Session(t, g, b, s) as m:
+            m.set_pose(seq.poses[0])
+            got = []
+
+            def submit(k):
+                if source == "device":
+                    m.submit_device(dev.data_ptr() + k * nb)
+                else:
+                    m.submit((seq.depth if source == "pageable" else pinned)[k])
+            submit(0)
+            for k in range(1, len(seq.depth)):
+                submit(k)
+                got.append(m.result())
+            got.append(m.result())
+            with pytest.raises(abi.DynError):
+                m.result()  # nothing in flight
+        for k, ((pa, sa), (pb, sb)) in enumerate(zip(ref, got)):
+            np.testing.assert_array_equal(pa, pb, err_msg=f"{source} frame {k}")
+            assert list(sa.icp_iterations) == list(sb.icp_iterations)
+            assert sa.blocks_total == sb.blocks_total

@@ -1,0 +1,123 @@
+"""The streaming front end (include/nodeHandler/nodeHandler.h, the
+counterpart of the reference's ROS node, nodeHandler.cpp:170): RGB-D
+streams replayed from TUM-layout directories at 30 Hz and one fed through a
+pipe go into one server; every frame is reported once, in each stream's
+order, and each stream's poses and iteration counts equal the same frames
+through a lone Session (the server fuses the streams' frames into shared
+launches; a session's results do not depend on its batch)."""
+import os
+import shutil
+import struct
+import subprocess
+
+import numpy as np
+import pytest
+
+from dynamap_b200 import abi, configs
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+SRC = os.path.join(ROOT, "tests", "cpp", "stream_example.cpp")
+LIBDIR = os.path.join(ROOT, "dynamap_b200")
+
+
+def compile_stream(out):
+    cxx = shutil.which("g++")
+    if cxx is None:
+        pytest.skip("no C++ compiler")
+    subprocess.run([cxx, "-std=c++17", "-O2", "-Wall", "-Werror", "-I",
+                    os.path.join(ROOT, "include"), SRC, "-L", LIBDIR, "-ldynamap_b200",
+                    f"-Wl,-rpath,{LIBDIR}", "-lz", "-pthread", "-o", out], check=True)
+
+
+def test_front_end_compiles(tmp_path):
+    compile_stream(str(tmp_path / "stream"))
+
+
+def spec_line(source, p, precision, rate, pose0):
+    s, t, g = p["sensor"], p["tsdf"], p["gn"]
+    vals = [source, s["rows"], s["cols"], s["fx"], s["fy"], s["cx"], s["cy"], s["depth_scaler"],
+            t["voxel_size"], int(np.log2(t["num_buckets"])), t["num_blocks"],
+            t["truncation_distance"], t["max_sensor_depth"], g["color_weight"], precision, rate]
+    vals += ["%.9g" % v for v in np.asarray(pose0, np.float32).reshape(16)]
+    return " ".join(str(v) for v in vals)
+
+
+def stream_preset(p, color_weight):
+    """The parameters stream_example gives a stream (its fixed ICP schedule,
+    bilateral filter and depth window)."""
+    p = {k: (dict(v) if isinstance(v, dict) else v) for k, v in p.items()}
+    p["tsdf"].update(bucket_size=10, block_size=8, max_sdf_weight=64, min_sensor_depth=0.15)
+    p["gn"].update(lvl_iteration_num=[10, 5, 4], lvl_scale=[4, 2, 1], color_weight=color_weight,
+                   icp_min_depth=0.15, icp_max_depth=p["tsdf"]["max_sensor_depth"], mode=1,
+                   compose_left=0, huber_constant=0.3)
+    p["bilateral"] = dict(diameter=8, sigma_i=10.0, sigma_s=1.0, enabled=1)
+    return p
+
+
+def pipe_frames(depth, stamps):
+    out = bytearray()
+    rows, cols = depth.shape[1:]
+    for d, st in zip(depth, stamps):
+        out += b"DYNF" + struct.pack("<IIIdQ", rows, cols, 0, st, 0)
+        out += np.ascontiguousarray(d, np.uint16).tobytes()
+    return bytes(out)
+
+
+@pytest.mark.gpu
+@pytest.mark.first_b200_run
+def test_streams_through_the_server_equal_lone_sessions(tmp_path, gpu_lib):
+    from dynamap_b200.session import Session
+    from test_dataset import make_tum
+    n = 8
+    dirs, seqs, presets, precs = [], [], [], []
+    for k, (seed, prec) in enumerate(((31, abi.PRECISION_FP32), (32, abi.PRECISION_MIXED))):
+        root = tmp_path / f"seq{k}"
+        root.mkdir()
+        seq, p = make_tum(root, n=n, seed=seed)
+        p["tsdf"].update(num_buckets=1 << 18, num_blocks=1 << 16)
+        dirs.append(str(root))
+        seqs.append(seq)
+        presets.append(stream_preset(p, 0.1))
+        precs.append(prec)
+    # the pipe stream: 320x240 depth only
+    pp = configs.preset("cfg1")
+    pp["tsdf"].update(num_buckets=1 << 18, num_blocks=1 << 16)
+    pseq = configs.sequence(pp, seed=33, n_frames=n)
+    pstamps = [100.0 + 0.0333 * k for k in range(n)]
+    presets.append(stream_preset(pp, 0.0))
+    precs.append(abi.PRECISION_FP32)
+    spec = tmp_path / "spec.txt"
+    lines = [spec_line(dirs[0], presets[0], precs[0], 30.0, seqs[0].poses[0]),
+             spec_line(dirs[1], presets[1], precs[1], 30.0, seqs[1].poses[0]),
+             spec_line("-", presets[2], precs[2], 0.0, pseq.poses[0])]
+    spec.write_text("\n".join(lines) + "\n")
+    exe = str(tmp_path / "stream")
+    compile_stream(exe)
+    out = tmp_path / "poses.txt"
+    r = subprocess.run([exe, str(spec), str(out)], input=pipe_frames(pseq.depth, pstamps),
+                       capture_output=True, timeout=300)
+    assert r.returncode == 0, r.stdout.decode() + r.stderr.decode()
+    rows = [ln.split() for ln in out.read_text().splitlines()]
+    got = {}
+    for row in rows:
+        got.setdefault(int(row[0]), []).append(row)
+    assert sorted(got) == [0, 1, 2] and all(len(v) == n for v in got.values())
+    frames = [(seqs[0].depth, seqs[0].rgb, seqs[0].poses[0]),
+              (seqs[1].depth, seqs[1].rgb, seqs[1].poses[0]),
+              (pseq.depth, None, pseq.poses[0])]
+    for sid in range(3):
+        rs = got[sid]
+        stamps = [float(x[1]) for x in rs]
+        assert stamps == sorted(stamps)  # each stream in frame order
+        assert all(int(x[2]) == 0 for x in rs)
+        t, g, b, s = configs.structs(presets[sid])
+        depth, rgb, pose0 = frames[sid]
+        with Session(t, g, b, s, precision=precs[sid]) as m:
+            m.set_pose(pose0)
+            for k in range(n):
+                pose, st = m.process(depth[k], None if rgb is None else rgb[k])
+                want = np.array([float(v) for v in rs[k][6:22]], np.float32).reshape(4, 4)
+                np.testing.assert_array_equal(want, pose, err_msg=f"stream {sid} frame {k}")
+                assert [int(v) for v in rs[k][3:6]] == list(st.icp_iterations)
+    # the pipe stream's stamps came through
+    np.testing.assert_allclose(sorted(float(x[1]) for x in got[2]), pstamps, atol=1e-6)
