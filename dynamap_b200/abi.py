@@ -19,6 +19,7 @@ STATUS = {0: "ok", 1: "invalid argument", 2: "out of device memory",
 DYN_ERR_BUDGET_EXCEEDED = 3
 DYN_ERR_HASH_FULL = 4
 DYN_ERR_HEAP_EXHAUSTED = 5
+DYN_ERR_TIMEOUT = 7
 DYN_ERR_NOT_READY = 9
 DYN_ERR_NO_DEVICE = 10
 STAGES = ["ingest", "bilateral", "source_maps", "icp", "allocate", "visible", "integrate",
@@ -121,6 +122,7 @@ SIGNATURES = {
     "dyn_raycast": (C.c_int, [_vp, P(C.c_float), P(Sensor), _vp, _vp]),
     "dyn_num_blocks": (C.c_int, [_vp, P(C.c_int64)]),
     "dyn_find_blocks": (C.c_int, [_vp, _vp, C.c_int64, _vp]),
+    "dyn_barrier_selftest": (C.c_int, [C.c_int32, C.c_int32, C.c_int32]),
     "dyn_download_blocks": (C.c_int, [_vp, _vp, _vp, C.c_int64, P(C.c_int64)]),
     "dyn_extract_mesh": (C.c_int, [_vp, P(C.c_float), P(C.c_float), _vp, C.c_int64,
                                    P(C.c_int64)]),

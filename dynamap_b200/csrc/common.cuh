@@ -61,6 +61,7 @@ struct Counters {
   int raycast_overruns;
   int visible;
   int unique_probed;
+  int icp_timeout;     // the persistent ICP's grid barrier gave up (bounded wait)
 };
 
 struct F3 {

@@ -5,14 +5,21 @@
 // gnSolver::solve (:317-438).  The reference adds 42 FP32 atomics per
 // correspondence into one 6x6 system and round-trips to the host (Eigen LDLT)
 // every iteration.  Here each thread accumulates its pixels' 21 upper-
-// triangle JtJ terms, 6 Jtr terms, r^2 and a count in registers, the block
-// reduces them with warp shuffles, and the last block to finish (ticket
-// counter) sums the block partials in FP64 in block order -- a fixed
-// reduction order, so results are run-to-run deterministic -- and then runs
-// the GN update (scale by 1/max(A), damping, 6x6 LDL^T, convergence test) and
-// the SE(3) exponential for the next iteration, in FP64, with no host
-// round trip.
+// triangle JtJ terms, 6 Jtr terms, r^2 and a count in registers (FP64 sums
+// of the FP32 terms; compensated FP32 sums in the mixed form), the block
+// reduces them with warp shuffles into a partial per pixel tile, and the
+// tiles' partials are summed in FP64 in tile order -- a fixed reduction
+// order, so results are run-to-run deterministic and do not depend on the
+// grid -- before the GN update (scale by 1/max(A), damping, 6x6 LDL^T,
+// convergence test) and the SE(3) exponential for the next iteration, in
+// FP64, with no host round trip.  Per frame this runs either as one chained
+// launch per iteration (the last block to finish a level's tiles updates
+// the solver) or as one persistent cooperative launch for all levels and
+// iterations (below); both give the same bits.
 #include "icp.cuh"
+
+#include <algorithm>
+#include <mutex>
 
 #include "sessdev.cuh"
 
@@ -25,9 +32,14 @@ __device__ inline bool normal_ok(float4 n) {
   return !(n.x == 0.0f && n.y == 0.0f && n.z == 0.0f);
 }
 
+// Per-thread sums of the per-pixel terms.  The FP32 form adds each pixel's
+// FP32 terms in FP64 (as the oracle does), so that its normal equations
+// differ from the oracle's only by the order of FP64 additions; the mixed
+// form keeps FP32 sums with Kahan compensation.
 struct Acc {
-  float v[kIcpVals];
-  float c[kIcpVals];  // Kahan compensation (used when kahan != 0)
+  double d[kIcpVals];  // FP64 sums (kahan == 0)
+  float v[kIcpVals];   // compensated FP32 sums (kahan != 0)
+  float c[kIcpVals];   // their compensation
 };
 
 template <bool KAHAN>
@@ -38,7 +50,7 @@ __device__ inline void acc_add(Acc& a, int k, float x) {
     a.c[k] = __fsub_rn(__fsub_rn(t, a.v[k]), y);
     a.v[k] = t;
   } else {
-    a.v[k] += x;
+    a.d[k] += (double)x;
   }
 }
 
@@ -112,8 +124,7 @@ __device__ inline void block_reduce(const Acc& a, bool kahan, double* red /*[8][
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int k = 0; k < kIcpVals; ++k) {
-    double v = (double)a.v[k];
-    if (kahan) v -= (double)a.c[k];
+    double v = kahan ? (double)a.v[k] - (double)a.c[k] : a.d[k];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if (lane == 0) red[warp * kIcpVals + k] = v;
@@ -309,12 +320,14 @@ __device__ void inverse4f(const float* e, float* out) {
 // summed system 'acc' (upper triangle row by row, then the 6 right-hand
 // sides): scale by 1 / max(A), add reg * max(scaled A) / it to the
 // diagonal, solve, accumulate.  The maxima run over all 36 entries in
-// row-major order, as over the full symmetric matrix.  Updates inc/prev;
-// returns true when converged.
+// row-major order, as over the full symmetric matrix.  Updates inc/prev
+// (the solver state's, in global or shared memory); returns true when
+// converged.
 __device__ __forceinline__ double sym_at(const double (&a)[21], int i, int j) {
   return i >= j ? a[tri(i, j)] : a[tri(j, i)];
 }
-__device__ bool gn_update(const double* acc, const IcpParams& P, int it, IcpState* st) {
+__device__ bool gn_update(const double* acc, const IcpParams& P, int it, double* st_inc,
+                          double* st_prev) {
   double a[21], b[6];
   {  // acc holds the upper triangle row by row
 #pragma unroll
@@ -347,31 +360,78 @@ __device__ bool gn_update(const double* acc, const IcpParams& P, int it, IcpStat
   double inc[6], ch = 0.0;
 #pragma unroll
   for (int k = 0; k < 6; ++k) {
-    inc[k] = st->inc[k] + d[k];
-    st->inc[k] = inc[k];
-    double c = inc[k] - st->prev[k];
+    inc[k] = st_inc[k] + d[k];
+    st_inc[k] = inc[k];
+    double c = inc[k] - st_prev[k];
     ch += c * c;
   }
   bool conv = fabs(sqrt(ch)) <= (double)P.min_inc;
   if (!conv) {
 #pragma unroll
-    for (int k = 0; k < 6; ++k) st->prev[k] = inc[k];
+    for (int k = 0; k < 6; ++k) st_prev[k] = inc[k];
   }
   return conv;
 }
 
-// Blocks of a level's reduction: about four pixels per thread (fewer
-// partial sums to combine than one pixel per thread), at most kIcpMaxBlocks.
+// Blocks of a level's chained reduction: one per tile, at most
+// kIcpMaxBlocks (a block then takes several tiles).
 inline __host__ __device__ int icp_grid(int n) {
-  int g = (n + 4 * kIcpThreads - 1) / (4 * kIcpThreads);
+  int g = icp_tiles(n);
   if (g > kIcpMaxBlocks) g = kIcpMaxBlocks;
   if (g < 1) g = 1;
   return g;
 }
 
+// The partial sums of tile 'tile' of level L into row[0..28]: each thread
+// accumulates its four pixels (tile * kIcpTile + threadIdx.x + m * 256) in
+// FP32, the block adds them in FP64 in a fixed order.  Every thread of the
+// block calls it; 'red' is the block's shared scratch.
+template <bool KAHAN>
+__device__ inline void tile_partial(const IcpLevel& L, const IcpParams& P, const M4f& T,
+                                    int tile, double* red, double* __restrict__ row) {
+  Acc a;
+#pragma unroll
+  for (int k = 0; k < kIcpVals; ++k) {
+    a.v[k] = a.c[k] = 0.0f;
+    a.d[k] = 0.0;
+  }
+  const int n = L.s.rows * L.s.cols;
+  const int base = tile * kIcpTile + (int)threadIdx.x;
+#pragma unroll
+  for (int m = 0; m < kIcpTile / kIcpThreads; ++m) {
+    const int idx = base + m * kIcpThreads;
+    if (idx < n) pixel_terms<KAHAN>(L, P, T, idx, a);
+  }
+  block_reduce(a, KAHAN, red);
+  if (threadIdx.x < kIcpVals) row[threadIdx.x] = red[threadIdx.x];
+  __syncthreads();  // red is reused by the next tile
+}
+
+// The level's total (tiles in index order), the iteration's statistics, the
+// GN update and the next transform, for a solver state held at st_* (global
+// memory in the chained kernels, shared memory in the persistent one).
+// tot[] must be shared; the update runs on thread 0.
+__device__ inline void level_update(const double* __restrict__ partials, int ntiles,
+                                    const IcpParams& P, int pl, int it, double* tot, double* red,
+                                    double* st_inc, double* st_prev, float* st_T,
+                                    int* st_converged, int* st_iters, int* st_inliers,
+                                    float* st_rms) {
+  final_reduce(partials, ntiles, tot, red);
+  if (threadIdx.x == 0) {
+    st_iters[pl] = it;
+    st_inliers[pl] = (int)tot[28];
+    st_rms[pl] = tot[28] > 0 ? (float)sqrt(tot[27] / tot[28]) : 0.0f;
+    const bool conv = gn_update(tot, P, it, st_inc, st_prev);
+    *st_converged = conv ? 1 : 0;
+    double Td[16];
+    se3_exp(st_inc, Td);
+    for (int k = 0; k < 16; ++k) st_T[k] = (float)Td[k];
+  }
+}
+
 // One GN iteration of level slot pl, iteration it (1-based), block 'bid' of
-// 'nb' blocks: the block's partial sums, then -- in the last block to finish
-// -- the FP64 total and the GN update (gnSolver.cu:379-415).
+// 'nb' blocks: the partial sums of the block's tiles, then -- in the last
+// block to finish -- the FP64 total and the GN update (gnSolver.cu:379-415).
 template <bool KAHAN>
 __device__ inline void icp_iteration_body(const IcpLevel& L, const IcpParams& P, int pl, int it,
                                           IcpState* st, double* __restrict__ partials, int bid,
@@ -387,14 +447,9 @@ __device__ inline void icp_iteration_body(const IcpLevel& L, const IcpParams& P,
   __syncthreads();
   if (skip) return;
   const M4f T = Ts;
-  Acc a;
-#pragma unroll
-  for (int k = 0; k < kIcpVals; ++k) a.v[k] = a.c[k] = 0.0f;
-  const int n = L.s.rows * L.s.cols;
-  for (int idx = bid * kIcpThreads + threadIdx.x; idx < n; idx += nb * kIcpThreads)
-    pixel_terms<KAHAN>(L, P, T, idx, a);
-  block_reduce(a, KAHAN, red);
-  if (threadIdx.x < kIcpVals) partials[(size_t)bid * kIcpVals + threadIdx.x] = red[threadIdx.x];
+  const int ntiles = icp_tiles(L.s.rows * L.s.cols);
+  for (int tile = bid; tile < ntiles; tile += nb)
+    tile_partial<KAHAN>(L, P, T, tile, red, partials + (size_t)tile * kIcpVals);
   __threadfence();
   __shared__ unsigned int ticket;
   if (threadIdx.x == 0) ticket = atomicAdd(&st->ticket, 1u);
@@ -402,25 +457,9 @@ __device__ inline void icp_iteration_body(const IcpLevel& L, const IcpParams& P,
   if (ticket != (unsigned)nb - 1) return;
   __threadfence();
   __shared__ double tot[kIcpVals];
-  final_reduce(partials, nb, tot, red);
-  if (threadIdx.x == 0) {
-    st->ticket = 0;
-    st->iters[pl] = it;
-    st->inliers[pl] = (int)tot[28];
-    st->rms[pl] = tot[28] > 0 ? (float)sqrt(tot[27] / tot[28]) : 0.0f;
-    bool conv = gn_update(tot, P, it, st);
-    st->converged = conv ? 1 : 0;
-    double Td[16];
-    se3_exp(st->inc, Td);
-    for (int k = 0; k < 16; ++k) st->T[k] = (float)Td[k];
-  }
-}
-
-template <bool KAHAN>
-__global__ void __launch_bounds__(kIcpThreads)
-    icp_iteration_kernel(IcpLevel L, IcpParams P, int pl, int it, IcpState* st,
-                         double* __restrict__ partials) {
-  icp_iteration_body<KAHAN>(L, P, pl, it, st, partials, blockIdx.x, gridDim.x);
+  level_update(partials, ntiles, P, pl, it, tot, red, st->inc, st->prev, st->T, &st->converged,
+               st->iters, st->inliers, st->rms);
+  if (threadIdx.x == 0) st->ticket = 0;
 }
 
 // Programmatic dependent launch: an iteration kernel launched with the
@@ -435,16 +474,7 @@ __device__ inline void release_successor() {
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
-// Every session of the frame in one launch (blockIdx.z); a session uses
-// only the blocks of its own grid, so its reduction is the same as alone.
-// One instantiation per summation kind; sessions of the other kind return.
-template <bool KAHAN>
-__global__ void __launch_bounds__(kIcpThreads, 2)
-    fused_icp_iteration_kernel(const SessDev* __restrict__ tab, int pl, int it) {
-  const SessDev& S = tab[blockIdx.z];
-  if ((S.icpp.kahan != 0) != KAHAN) return;
-  if (it >= S.slot_iters[pl]) return;  // the reference runs iterations 1 .. N-1
-  const int l = S.slot_level[pl];
+__device__ inline IcpLevel level_of(const SessDev& S, int l) {
   IcpLevel L;
   L.sd = S.sdep[l];
   L.sn = S.snrm[l];
@@ -453,6 +483,19 @@ __global__ void __launch_bounds__(kIcpThreads, 2)
   L.tn = S.tnrm[l];
   L.ti = S.tint[l];
   L.s = S.ls[l];
+  return L;
+}
+
+// Every session of the frame in one launch (blockIdx.z); a session uses
+// only the blocks of its own grid.  One instantiation per summation kind;
+// sessions of the other kind return.
+template <bool KAHAN>
+__global__ void __launch_bounds__(kIcpThreads, 2)
+    fused_icp_iteration_kernel(const SessDev* __restrict__ tab, int pl, int it) {
+  const SessDev& S = tab[blockIdx.z];
+  if ((S.icpp.kahan != 0) != KAHAN) return;
+  if (it >= S.slot_iters[pl]) return;  // the reference runs iterations 1 .. N-1
+  const IcpLevel L = level_of(S, S.slot_level[pl]);
   const int nb = icp_grid(L.s.rows * L.s.cols);
   if ((int)blockIdx.x >= nb) return;
   wait_predecessor();  // the solver state and partials of the previous iteration
@@ -460,7 +503,170 @@ __global__ void __launch_bounds__(kIcpThreads, 2)
   icp_iteration_body<KAHAN>(L, S.icpp, pl, it, S.icp, S.partials, blockIdx.x, nb);
 }
 
+// ---- the persistent form: one launch walks every level and iteration
+//
+// A cooperative launch (all blocks resident at once) over the table: each
+// session owns a run of blocks (icp_share: about its share of the tiles),
+// every block keeps its session's solver state in shared memory, and one
+// grid-wide barrier per iteration separates the tiles' partial sums from
+// their use: after it, every block of the session adds the partials (the
+// same sums, in the same order, so every block holds the same state) and
+// runs the GN update itself -- no second barrier.  Iterations alternate
+// between two rows of partials, so a block may start the next iteration's
+// tiles while another still reads this one's.  The results are those of the
+// chained kernels bit for bit (the same tiles, summed in the same order).
+
+// Current value of the GPU's nanosecond timer.
+__device__ inline unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Grid-wide barrier number k of a launch whose arrival counter 'bar' starts
+// at 0: complete when the counter reaches target = k * gridDim.x.  The wait
+// is bounded: after kBarrierWaitNs (or once *abort is raised) the block
+// gives up, raises *abort and returns false.
+constexpr unsigned long long kBarrierWaitNs = 500000000ull;  // half a second
+__device__ inline bool grid_barrier(unsigned* bar, unsigned target, int* abort) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();  // this block's partial sums before its arrival
+    atomicAdd(bar, 1u);
+    const unsigned long long t0 = global_ns();
+    int good = 1;
+    while (*(volatile unsigned*)bar < target) {
+      if (*(volatile int*)abort || global_ns() - t0 > kBarrierWaitNs) {
+        good = 0;
+        break;
+      }
+      __nanosleep(64);
+    }
+    if (!good) atomicExch(abort, 1);
+    __threadfence();  // the other blocks' partial sums after the arrivals
+    ok = good;
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+// Blocks of a session in a persistent launch of 'budget' blocks over a table
+// whose sessions have sum_tiles level-0 tiles in all.
+__host__ __device__ inline int icp_share(int tiles, long long sum_tiles, int budget) {
+  long long b = (long long)budget * tiles / (sum_tiles > 0 ? sum_tiles : 1);
+  if (b > tiles) b = tiles;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+__global__ void __launch_bounds__(kIcpThreads, 2)
+    fused_icp_persistent_kernel(const SessDev* __restrict__ tab, int n, int budget,
+                                int it0, int it1, int it2, unsigned* __restrict__ bar,
+                                int* __restrict__ abort) {
+  // this block's session and its index among the session's blocks
+  __shared__ int z_s, local_s, nblk_s;
+  if (threadIdx.x == 0) {
+    long long sum = 0;
+    for (int j = 0; j < n; ++j) sum += icp_tiles(tab[j].npx);
+    int first = 0, z = n - 1, nb = 1;
+    for (int j = 0; j < n; ++j) {
+      nb = icp_share(icp_tiles(tab[j].npx), sum, budget);
+      if ((int)blockIdx.x < first + nb) {
+        z = j;
+        break;
+      }
+      first += nb;
+    }
+    z_s = z;
+    local_s = (int)blockIdx.x - first;
+    nblk_s = nb;
+  }
+  __syncthreads();
+  const SessDev& S = tab[z_s];
+  const int local = local_s, nblk = nblk_s;
+  const bool own = local >= 0 && local < nblk;  // spare blocks only pass the barriers
+  // the session's solver state, one copy per block
+  __shared__ double red[(kIcpThreads / 32) * kIcpVals];
+  __shared__ double tot[kIcpVals];
+  __shared__ double inc[6], prev[6];
+  __shared__ float Tf[16];
+  __shared__ int conv, have, iters[3], inliers[3];
+  __shared__ float rms[3];
+  if (threadIdx.x < 6) {
+    inc[threadIdx.x] = S.icp->inc[threadIdx.x];
+    prev[threadIdx.x] = S.icp->prev[threadIdx.x];
+  }
+  if (threadIdx.x < 16) Tf[threadIdx.x] = S.icp->T[threadIdx.x];
+  if (threadIdx.x < 3) {
+    iters[threadIdx.x] = S.icp->iters[threadIdx.x];
+    inliers[threadIdx.x] = S.icp->inliers[threadIdx.x];
+    rms[threadIdx.x] = S.icp->rms[threadIdx.x];
+  }
+  if (threadIdx.x == 0) {
+    conv = S.icp->converged;
+    have = S.icp->have_target;
+  }
+  __syncthreads();
+  const int maxit[3] = {it0, it1, it2};
+  const size_t row = (size_t)icp_tiles(S.npx) * kIcpVals;
+  unsigned nbar = 0;
+  int parity = 0;
+  for (int pl = 0; pl < 3; ++pl)
+    for (int it = 1; it < maxit[pl]; ++it) {
+      const bool active = own && it < S.slot_iters[pl] && have && !(it > 1 && conv);
+      const IcpLevel L = level_of(S, S.slot_level[pl]);
+      const int ntiles = icp_tiles(L.s.rows * L.s.cols);
+      double* part = S.partials + (size_t)parity * row;
+      if (active) {
+        M4f T;
+#pragma unroll
+        for (int k = 0; k < 16; ++k) T.m[k] = Tf[k];
+        for (int tile = local; tile < ntiles; tile += nblk) {
+          if (S.icpp.kahan) tile_partial<true>(L, S.icpp, T, tile, red, part + (size_t)tile * kIcpVals);
+          else tile_partial<false>(L, S.icpp, T, tile, red, part + (size_t)tile * kIcpVals);
+        }
+      }
+      ++nbar;
+      if (!grid_barrier(bar, nbar * gridDim.x, abort)) {
+        if (threadIdx.x == 0) atomicExch(&S.vol.cnt->icp_timeout, 1);
+        return;
+      }
+      if (active) {
+        level_update(part, ntiles, S.icpp, pl, it, tot, red, inc, prev, Tf, &conv, iters, inliers,
+                     rms);
+        __syncthreads();
+      }
+      parity ^= 1;
+    }
+  // the session's first block hands the state on (pose finalisation)
+  if (own && local == 0) {
+    if (threadIdx.x < 6) {
+      S.icp->inc[threadIdx.x] = inc[threadIdx.x];
+      S.icp->prev[threadIdx.x] = prev[threadIdx.x];
+    }
+    if (threadIdx.x < 16) S.icp->T[threadIdx.x] = Tf[threadIdx.x];
+    if (threadIdx.x < 3) {
+      S.icp->iters[threadIdx.x] = iters[threadIdx.x];
+      S.icp->inliers[threadIdx.x] = inliers[threadIdx.x];
+      S.icp->rms[threadIdx.x] = rms[threadIdx.x];
+    }
+    if (threadIdx.x == 0) {
+      S.icp->converged = conv;
+      S.icp->ticket = 0;
+    }
+  }
+}
+
+// A barrier self-test: 'blocks' blocks wait at barrier 1 for blocks + missing
+// arrivals (missing > 0: a wait that cannot complete, which must end in the
+// bounded timeout).
+__global__ void barrier_selftest_kernel(unsigned* bar, unsigned target, int* abort) {
+  grid_barrier(bar, target, abort);
+}
+
 // Normal equations only (stage entry point): no solver state.
+template <bool KAHAN>
 __global__ void __launch_bounds__(kIcpThreads)
     icp_reduce_kernel(IcpLevel L, IcpParams P, const float* __restrict__ Tdev,
                       double* __restrict__ partials, unsigned int* ticket_ctr,
@@ -472,14 +678,15 @@ __global__ void __launch_bounds__(kIcpThreads)
   const M4f T = Ts;
   Acc a;
 #pragma unroll
-  for (int k = 0; k < kIcpVals; ++k) a.v[k] = a.c[k] = 0.0f;
+  for (int k = 0; k < kIcpVals; ++k) {
+    a.v[k] = a.c[k] = 0.0f;
+    a.d[k] = 0.0;
+  }
   const int n = L.s.rows * L.s.cols;
   for (int idx = blockIdx.x * kIcpThreads + threadIdx.x; idx < n;
-       idx += gridDim.x * kIcpThreads) {
-    if (P.kahan) pixel_terms<true>(L, P, T, idx, a);
-    else pixel_terms<false>(L, P, T, idx, a);
-  }
-  block_reduce(a, P.kahan != 0, red);
+       idx += gridDim.x * kIcpThreads)
+    pixel_terms<KAHAN>(L, P, T, idx, a);
+  block_reduce(a, KAHAN, red);
   if (threadIdx.x < kIcpVals) partials[(size_t)blockIdx.x * kIcpVals + threadIdx.x] = red[threadIdx.x];
   __threadfence();
   __shared__ unsigned int ticket;
@@ -626,13 +833,89 @@ __global__ void pose_set_kernel(PoseState* ps, const double* pose) {
 
 size_t icp_scratch_bytes() { return sizeof(double) * (size_t)kIcpMaxBlocks * kIcpVals; }
 
-void launch_icp_iteration(const IcpLevel& L, const IcpParams& P, int pl, int it, IcpState* st,
-                          double* partials, cudaStream_t stream) {
-  int g = icp_grid(L.s.rows * L.s.cols);
-  if (P.kahan)
-    icp_iteration_kernel<true><<<g, kIcpThreads, 0, stream>>>(L, P, pl, it, st, partials);
-  else
-    icp_iteration_kernel<false><<<g, kIcpThreads, 0, stream>>>(L, P, pl, it, st, partials);
+size_t icp_frame_scratch_bytes(size_t npx) {
+  const size_t rows = 2 * (size_t)icp_tiles((int)npx) * kIcpVals * sizeof(double);
+  return rows > icp_scratch_bytes() ? rows : icp_scratch_bytes();
+}
+
+int icp_persistent_capacity(int device) {
+  static std::mutex mu;
+  static int cap[64] = {};
+  if (device < 0 || device >= 64) return 0;
+  std::lock_guard<std::mutex> lk(mu);
+  if (cap[device] == 0) {
+    int coop = 0, sms = 0, per_sm = 0;
+    if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fused_icp_persistent_kernel,
+                                                      kIcpThreads, 0) != cudaSuccess) {
+      cudaGetLastError();
+      coop = 0;
+    }
+    cap[device] = coop ? std::max(1, per_sm * sms) : -1;
+  }
+  return cap[device] > 0 ? cap[device] : 0;
+}
+
+int icp_persistent_grid(const int* npx, int n, int budget) {
+  if (budget <= 0 || n <= 0) return 0;
+  long long sum = 0;
+  for (int j = 0; j < n; ++j) sum += icp_tiles(npx[j]);
+  long long g = 0;
+  for (int j = 0; j < n; ++j) g += icp_share(icp_tiles(npx[j]), sum, budget);
+  return g <= budget ? (int)g : 0;
+}
+
+void fused_icp_persistent(const SessDev* tab, const BatchShape& b, cudaStream_t st) {
+  // the barrier's arrival counter and abort flag start at zero every frame
+  cudaMemsetAsync(b.icp_bar, 0, 2 * sizeof(unsigned), st);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(b.icp_grid);
+  cfg.blockDim = dim3(kIcpThreads);
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, fused_icp_persistent_kernel, tab, b.n, b.icp_budget,
+                     b.max_slot_iters[0], b.max_slot_iters[1], b.max_slot_iters[2], b.icp_bar,
+                     reinterpret_cast<int*>(b.icp_bar + 1));
+}
+
+dyn_status icp_barrier_selftest(int blocks, int missing, unsigned* bar_dev, cudaStream_t st) {
+  if (blocks < 1 || missing < 0) return DYN_ERR_INVALID_ARG;
+  int dev = 0, sms = 0, per_sm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, barrier_selftest_kernel, 32, 0) !=
+          cudaSuccess) {
+    cudaGetLastError();
+    return DYN_ERR_CUDA;
+  }
+  if (blocks > per_sm * sms) return DYN_ERR_INVALID_ARG;  // not all resident at once
+  if (cudaMemsetAsync(bar_dev, 0, 2 * sizeof(unsigned), st) != cudaSuccess) return DYN_ERR_CUDA;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(blocks);
+  cfg.blockDim = dim3(32);
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, barrier_selftest_kernel, bar_dev,
+                                           (unsigned)(blocks + missing),
+                                           reinterpret_cast<int*>(bar_dev + 1));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return e == cudaErrorCooperativeLaunchTooLarge ? DYN_ERR_INVALID_ARG : DYN_ERR_CUDA;
+  }
+  unsigned h[2] = {0, 0};
+  if (cudaMemcpyAsync(h, bar_dev, sizeof(h), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return DYN_ERR_CUDA;
+  return h[1] ? DYN_ERR_TIMEOUT : DYN_OK;
 }
 
 void launch_pose_finalize(const IcpParams& P, IcpState* st, PoseState* ps, cudaStream_t stream) {
@@ -652,13 +935,21 @@ void launch_icp_reduce_only(const IcpLevel& L, const IcpParams& P, const float* 
                             double* partials, unsigned int* ticket, double* out_dev,
                             cudaStream_t stream) {
   int g = icp_grid(L.s.rows * L.s.cols);
-  icp_reduce_kernel<<<g, kIcpThreads, 0, stream>>>(L, P, T_dev, partials, ticket, out_dev);
+  if (P.kahan)
+    icp_reduce_kernel<true><<<g, kIcpThreads, 0, stream>>>(L, P, T_dev, partials, ticket, out_dev);
+  else
+    icp_reduce_kernel<false><<<g, kIcpThreads, 0, stream>>>(L, P, T_dev, partials, ticket, out_dev);
 }
 
 void launch_icp_reduce_grid(const IcpLevel& L, const IcpParams& P, const float* T_dev,
                             double* partials, unsigned int* ticket, double* out_dev, int grid,
                             cudaStream_t stream) {
-  icp_reduce_kernel<<<grid, kIcpThreads, 0, stream>>>(L, P, T_dev, partials, ticket, out_dev);
+  if (P.kahan)
+    icp_reduce_kernel<true><<<grid, kIcpThreads, 0, stream>>>(L, P, T_dev, partials, ticket,
+                                                               out_dev);
+  else
+    icp_reduce_kernel<false><<<grid, kIcpThreads, 0, stream>>>(L, P, T_dev, partials, ticket,
+                                                                out_dev);
 }
 
 // 'chained': launched with programmatic stream serialization, so that the

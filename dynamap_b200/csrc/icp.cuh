@@ -50,14 +50,34 @@ struct IcpParams {
 constexpr int kIcpThreads = 256;
 constexpr int kIcpMaxBlocks = 148 * 8;
 constexpr int kIcpVals = 29;
+// The per-frame ICP sums its normal equations per pixel tile: tile j holds
+// pixels [j * kIcpTile, (j + 1) * kIcpTile) of a level, four per thread,
+// and its partial sums are the same whichever block computes them; the
+// level's total adds the tiles in index order.  So the result does not
+// depend on how many blocks work on a level, nor on the sessions that share
+// the launch.
+constexpr int kIcpTile = 4 * kIcpThreads;
+inline __host__ __device__ int icp_tiles(int npx) { return (npx + kIcpTile - 1) / kIcpTile; }
 
 // Scratch a reduction needs: per-block partial sums (kIcpMaxBlocks*29 doubles).
 size_t icp_scratch_bytes();
+// Scratch of the per-frame ICP of a session whose largest level has npx
+// pixels: two rows of per-tile partial sums (iterations alternate rows) and
+// at least icp_scratch_bytes().
+size_t icp_frame_scratch_bytes(size_t npx);
 
-// One GN iteration of level slot 'pl' (iteration 'it', 1-based): reduce the
-// normal equations into 'partials', the last block solves and updates 'st'.
-void launch_icp_iteration(const IcpLevel& L, const IcpParams& P, int pl, int it,
-                          IcpState* st, double* partials, cudaStream_t stream);
+// The persistent ICP (one cooperative launch per frame): the blocks that can
+// be resident at once on 'device' (0: cooperative launches unavailable),
+// and the grid of a table whose sessions' largest levels have npx[j]
+// pixels, within 'budget' blocks (0: the table does not fit; the chained
+// kernels run it, with the same results).
+int icp_persistent_capacity(int device);
+int icp_persistent_grid(const int* npx, int n, int budget);
+// A bounded grid barrier run alone: 'blocks' blocks wait for blocks +
+// missing arrivals (bar_dev: two words).  DYN_OK when it completes,
+// DYN_ERR_TIMEOUT when the bounded wait ran out, DYN_ERR_INVALID_ARG when
+// the blocks cannot all be resident.
+dyn_status icp_barrier_selftest(int blocks, int missing, unsigned* bar_dev, cudaStream_t st);
 // After the last level: guards, pose composition, float pose + inverse, reset
 // of the solver state.  Runs with one thread.
 void launch_pose_finalize(const IcpParams& P, IcpState* st, PoseState* ps,

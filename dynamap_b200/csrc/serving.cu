@@ -87,6 +87,7 @@ dyn_status dyn_batch_create(dyn_session* const* sessions, int32_t n, dyn_batch**
   if (r == DYN_OK) r = dalloc((void**)&b->d_map, sizeof(int) * (size_t)n);
   if (r == DYN_OK) r = dalloc((void**)&b->d_gvis, sizeof(int2) * (size_t)cap);
   if (r == DYN_OK) r = dalloc((void**)&b->d_gcount, sizeof(int) * kMaxGroups);
+  if (r == DYN_OK) r = dalloc((void**)&b->d_icp_bar, 2 * sizeof(unsigned) * kMaxGroups);
   if (r == DYN_OK) r = dalloc((void**)&b->d_res, sizeof(ResultBlock) * (size_t)n);
   for (int g = 1; g < k && r == DYN_OK; ++g)
     if (cudaStreamCreateWithFlags(&b->groups.st[g], cudaStreamNonBlocking) != cudaSuccess ||
@@ -129,6 +130,10 @@ dyn_status dyn_batch_create(dyn_session* const* sessions, int32_t n, dyn_batch**
     G.map[g] = b->d_map + start[g];
     G.shape[g] = make_shape(sorted.data() + start[g], n_g, b->d_gvis + voff, b->d_gcount + g,
                             (int)cap_g);
+    // the groups' persistent ICP launches may run at once: each takes its
+    // share of the resident blocks
+    set_icp_persistent(G.shape[g], sorted.data() + start[g], n_g, b->d_icp_bar + 2 * g,
+                       icp_persistent_capacity(b->device) / k);
     voff += cap_g;
   }
   FrameGroups& one = b->single;
@@ -137,6 +142,7 @@ dyn_status dyn_batch_create(dyn_session* const* sessions, int32_t n, dyn_batch**
   one.tab[0] = b->d_tab;
   one.map[0] = b->d_map;
   one.shape[0] = make_shape(sorted.data(), n, b->d_gvis, b->d_gcount, (int)cap);
+  set_icp_persistent(one.shape[0], sorted.data(), n, b->d_icp_bar, icp_persistent_capacity(b->device));
   b->shape = one.shape[0];
   for (int i = 0; i < n; ++i) sessions[i]->batch = b;
   *out = b;
@@ -450,6 +456,7 @@ struct dyn_server {
   int64_t frames = 0;
   int2* d_gvis = nullptr;
   int* d_gcount = nullptr;
+  unsigned* d_icp_bar = nullptr;  // the persistent ICP's barrier words
   int64_t gvis_cap = 0;
   ResultBlock* d_res = nullptr;
   ResultBlock* h_res = nullptr;  // pinned, one entry per slot
@@ -479,6 +486,7 @@ void release(dyn_server* sv) {
   cudaFree(sv->d_arena);
   cudaFree(sv->d_gvis);
   cudaFree(sv->d_gcount);
+  cudaFree(sv->d_icp_bar);
   cudaFree(sv->d_res);
   if (sv->h_res) cudaFreeHost(sv->h_res);
   if (sv->stream) cudaStreamDestroy(sv->stream);
@@ -521,6 +529,7 @@ dyn_status dyn_server_create(const dyn_server_params* p, dyn_server** out) {
   bool ok = cudaMalloc(&sv->d_arena, sv->budget ? sv->budget : 256) == cudaSuccess &&
             cudaStreamCreateWithFlags(&sv->stream, cudaStreamNonBlocking) == cudaSuccess &&
             cudaMalloc(&sv->d_gcount, 256) == cudaSuccess &&
+            cudaMalloc(&sv->d_icp_bar, 256) == cudaSuccess &&
             cudaMalloc(&sv->d_res, sizeof(ResultBlock) * (size_t)cap) == cudaSuccess &&
             cudaMallocHost(&sv->h_res, sizeof(ResultBlock) * (size_t)cap) == cudaSuccess;
   for (StepBuf& r : sv->ring)
@@ -677,7 +686,8 @@ dyn_status dyn_server_step(dyn_server* sv, int32_t* n_out) {
     DYN_TRY(set_rgb_flag(s, sl.queued_rgb, st));
     DYN_CUDA(cudaEventRecord(s->h2d_done, st));
   }
-  const BatchShape b = make_shape(sv->act.data(), n, sv->d_gvis, sv->d_gcount, (int)cap);
+  BatchShape b = make_shape(sv->act.data(), n, sv->d_gvis, sv->d_gcount, (int)cap);
+  set_icp_persistent(b, sv->act.data(), n, sv->d_icp_bar, icp_persistent_capacity(sv->device));
   enqueue_frame(rb.d_tab, b, rb.d_map, sv->d_res, sv->h_res, sv->capacity, st, Marks());
   DYN_CUDA(cudaGetLastError());
   DYN_CUDA(cudaEventRecord(rb.done, st));

@@ -89,6 +89,12 @@ struct BatchShape {
   int2* gvis;              // batch-wide visible list (session, heap index)
   int* gcount;             // its length (device)
   int gvis_cap;
+  // the persistent ICP: blocks of the cooperative launch (0: the chained
+  // kernels instead), the budget its sessions' shares are taken from, and
+  // the barrier's arrival counter and abort flag (two words, device)
+  int icp_grid;
+  int icp_budget;
+  unsigned* icp_bar;
 };
 
 // image.cu
@@ -100,6 +106,7 @@ void fused_target_prepare(const SessDev* tab, const BatchShape& b, cudaStream_t 
 void fused_icp_iteration(const SessDev* tab, const BatchShape& b, int slot, int it, bool chained,
                          cudaStream_t st);
 void fused_pose_finalize(const SessDev* tab, const BatchShape& b, int bump, cudaStream_t st);
+void fused_icp_persistent(const SessDev* tab, const BatchShape& b, cudaStream_t st);
 // tsdf.cu
 void fused_reset_counters(const SessDev* tab, const BatchShape& b, cudaStream_t st);
 void fused_allocate(const SessDev* tab, const BatchShape& b, cudaStream_t st);

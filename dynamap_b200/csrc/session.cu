@@ -16,6 +16,7 @@
 // table of its members, one launch per stage for all of them and the whole
 // frame as one graph.
 #include <cstdio>
+#include <cstdlib>
 #include <mutex>
 #include <new>
 
@@ -141,6 +142,10 @@ void enqueue_source(const SessDev* tab, const BatchShape& b, cudaStream_t st, co
 // of each level slot; every launch after the first overlaps its
 // predecessor's tail (programmatic dependent launch).
 void enqueue_icp(const SessDev* tab, const BatchShape& b, cudaStream_t st) {
+  if (b.icp_grid > 0) {  // one persistent launch for every level and iteration
+    fused_icp_persistent(tab, b, st);
+    return;
+  }
   bool chained = false;
   for (int pl = 0; pl < 3; ++pl)
     for (int it = 1; it < b.max_slot_iters[pl]; ++it) {
@@ -271,6 +276,22 @@ BatchShape make_shape(dyn_session* const* ss, int n, int2* gvis, int* gcount, in
     b.fp16_mask |= s->vol.fp16 ? 2 : 1;
   }
   return b;
+}
+
+// The persistent ICP for a table of sessions: its grid within 'budget'
+// blocks (0: chained kernels) and its barrier words.  DYN_ICP_CHAINED=1 in
+// the environment keeps every table on the chained kernels (the same
+// results; for comparisons).
+void set_icp_persistent(BatchShape& b, dyn_session* const* ss, int n, unsigned* bar, int budget) {
+  static const bool chained_only = [] {
+    const char* e = std::getenv("DYN_ICP_CHAINED");
+    return e && e[0] == '1';
+  }();
+  std::vector<int> npx((size_t)n);
+  for (int i = 0; i < n; ++i) npx[i] = (int)ss[i]->npx;
+  b.icp_budget = budget;
+  b.icp_grid = (chained_only || !bar) ? 0 : icp_persistent_grid(npx.data(), n, budget);
+  b.icp_bar = bar;
 }
 
 // The session's descriptor (device buffers, sensor levels, parameters).
@@ -503,6 +524,7 @@ void add_stage_times(cudaEvent_t* ev, double* ms_acc, int64_t* frames) {
 }
 
 dyn_status counters_status(const Counters& c) {
+  if (c.icp_timeout) return DYN_ERR_TIMEOUT;
   if (c.heap_exhausted) return DYN_ERR_HEAP_EXHAUSTED;
   if (c.bucket_full) return DYN_ERR_HASH_FULL;
   return DYN_OK;
@@ -563,13 +585,13 @@ size_t session_bytes(const dyn_tsdf_params& t, const dyn_sensor& s, int precisio
   else
     b += sizeof(dyn_voxel) * (size_t)t.num_blocks * kBlockVox;
   b += sizeof(int2) * (size_t)t.num_blocks;  // visible list
-  if (precision != DYN_PRECISION_FP32)
+  if (precision == DYN_PRECISION_MIXED)
     b += (sizeof(int) + 1) * (size_t)t.num_blocks;  // free-space summaries
   b += n * (2 + 3 + 4 + 4 + 4 + 3);  // inputs, raw, filtered, ray depth, target rgb
   if (precision == DYN_PRECISION_MIXED_BAND)
     b += 4 * (size_t)((s.rows + 7) / 8) * ((s.cols + 7) / 8) + 256;  // ray-start bound
   b += 2 * n * (4 + 16 + 16 + 4) * 4 / 3;  // source + target pyramids
-  b += icp_scratch_bytes() + sizeof(SessDev) + sizeof(BilateralTable) + sizeof(ResultBlock) +
+  b += icp_frame_scratch_bytes(n) + sizeof(SessDev) + sizeof(BilateralTable) + sizeof(ResultBlock) +
        8192;
   return b;
 }
@@ -657,7 +679,8 @@ dyn_status alloc_device_buffers(dyn_session* s) {
   }
   DYN_TRY(s->dalloc(&s->d_pose_override, 64));
   DYN_TRY(s->dalloc(&s->d_pose_in, 128));
-  DYN_TRY(s->dalloc(&s->d_partials, icp_scratch_bytes()));
+  DYN_TRY(s->dalloc(&s->d_partials, icp_frame_scratch_bytes(s->npx)));
+  DYN_TRY(s->dalloc(&s->d_icp_bar, 2 * sizeof(unsigned)));
   DYN_TRY(s->dalloc(&s->d_icp, sizeof(IcpState)));
   DYN_TRY(s->dalloc(&s->d_pose, sizeof(PoseState)));
   s->vol.t = dtsdf(*tsdf, precision);
@@ -678,7 +701,7 @@ dyn_status alloc_device_buffers(dyn_session* s) {
   }
   s->vol.nonsat = nullptr;
   s->vol.freecell = nullptr;
-  if (s->vol.fp16) {  // the mixed forms' raycast steps through free cells
+  if (s->vol.fp16 && !s->vol.t.band) {  // the mixed form's raycast steps through free cells
     DYN_TRY(s->dalloc(&s->vol.nonsat, sizeof(int) * (size_t)tsdf->num_blocks));
     DYN_TRY(s->dalloc(&s->vol.freecell, (size_t)tsdf->num_blocks));
   }
@@ -802,6 +825,7 @@ dyn_status create_session(const dyn_tsdf_params* tsdf, const dyn_gn_params* gn,
   s->hsd_1.rgb_flag = s->d_rgb_flag_1;
   dyn_session* self = s;
   s->shape = make_shape(&self, 1, s->d_gvis, s->d_gcount, tsdf->num_blocks);
+  set_icp_persistent(s->shape, &self, 1, s->d_icp_bar, icp_persistent_capacity(device));
   if (cudaMemcpyAsync(s->d_btab, &s->btab, sizeof(BilateralTable), cudaMemcpyHostToDevice,
                       s->stream) != cudaSuccess ||
       cudaMemcpyAsync(s->d_sd, &s->hsd, sizeof(SessDev), cudaMemcpyHostToDevice, s->stream) !=
@@ -1350,6 +1374,29 @@ dyn_status dyn_icp_normal_equations(const float* src_depth_dev, const float* src
   DYN_CUDA(cudaMemcpyAsync(out_host, sc.out, sizeof(double) * kIcpVals, cudaMemcpyDeviceToHost, st));
   DYN_CUDA(cudaStreamSynchronize(st));
   return DYN_OK;
+}
+
+dyn_status dyn_barrier_selftest(int32_t device, int32_t blocks, int32_t missing) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return DYN_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= ndev || blocks < 1 || missing < 0) return DYN_ERR_INVALID_ARG;
+  DeviceGuard dg(device);
+  unsigned* bar = nullptr;
+  cudaStream_t st = nullptr;
+  if (cudaMalloc(&bar, 2 * sizeof(unsigned)) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    if (bar) cudaFree(bar);
+    return DYN_ERR_OOM;
+  }
+  const dyn_status r = icp_barrier_selftest(blocks, missing, bar, st);
+  cudaStreamSynchronize(st);
+  cudaStreamDestroy(st);
+  cudaFree(bar);
+  return r;
 }
 
 dyn_status dyn_sessions_submit(dyn_session* const* sessions, int32_t n,

@@ -137,6 +137,7 @@ struct dyn_session {
   float* d_pose_override = nullptr;
   double* d_pose_in = nullptr;
   double* d_partials = nullptr;
+  unsigned* d_icp_bar = nullptr;  // the persistent ICP's barrier words
   IcpState* d_icp = nullptr;
   PoseState* d_pose = nullptr;
   VolumeDev vol;
@@ -273,6 +274,7 @@ struct dyn_batch {
   SessDev* d_tab = nullptr;
   int2* d_gvis = nullptr;
   int* d_gcount = nullptr;
+  unsigned* d_icp_bar = nullptr;  // two words per group (persistent ICP barrier)
   ResultBlock* d_res = nullptr;
   ResultBlock* h_res = nullptr;  // pinned, n entries
   BatchShape shape;
@@ -330,6 +332,9 @@ dyn_status quiesce(dyn_session* s);
 // The launch shape of a table of sessions (the largest member bounds every
 // grid).
 BatchShape make_shape(dyn_session* const* ss, int n, int2* gvis, int* gcount, int gvis_cap);
+// The persistent ICP of a table: its grid within 'budget' blocks (0 when it
+// does not fit: the chained kernels, same results) and its barrier words.
+void set_icp_persistent(BatchShape& b, dyn_session* const* ss, int n, unsigned* bar, int budget);
 // Marks whether this frame of 's' carries RGB (stream-ordered).
 dyn_status set_rgb_flag(dyn_session* s, bool has_rgb, cudaStream_t st);
 // Host frame into the session's device input buffers on 'st'.

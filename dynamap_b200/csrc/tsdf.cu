@@ -930,11 +930,13 @@ __device__ inline bool raycast_px(const VolumeDev& v, const DSensor& s, const M4
     }
     const F3 q = f3(__fmaf_rn(cur, d.x, o.x), __fmaf_rn(cur, d.y, o.y), __fmaf_rn(cur, d.z, o.z));
     const float flx = floorf(q.x), fly = floorf(q.y), flz = floorf(q.z);
-    int free;
-    cell_block_free(v, (int)flx >> 3, (int)fly >> 3, (int)flz >> 3, bc, &free);
-    if (free) {  // the interpolated sdf is the truncation distance
-      cur += t.trunc;
-      continue;
+    if (v.freecell) {
+      int free;
+      cell_block_free(v, (int)flx >> 3, (int)fly >> 3, (int)flz >> 3, bc, &free);
+      if (free) {  // the interpolated sdf is the truncation distance
+        cur += t.trunc;
+        continue;
+      }
     }
     const int gx = (int)flx + (q.x - flx >= 0.5f), gy = (int)fly + (q.y - fly >= 0.5f),
               gz = (int)flz + (q.z - flz >= 0.5f);
@@ -1081,6 +1083,7 @@ __global__ void fused_reset_counters_kernel(const SessDev* __restrict__ tab,
   c->raycast_overruns = 0;
   c->visible = 0;
   c->unique_probed = 0;
+  c->icp_timeout = 0;
 }
 
 __global__ void clear_entries_kernel(Entry* e, size_t n) {

@@ -17,8 +17,9 @@ struct VolumeDev {
   int fp16;                       // 1: mixed-precision voxels (vox16 [+ colors])
   Counters* cnt;
   DTsdf t;
-  // Free-space summaries per heap index, kept for the mixed forms (null in
-  // the FP32 form, whose raycast evaluates every sample): nonsat = voxels
+  // Free-space summaries per heap index, kept for the mixed form (null in
+  // the FP32 form, whose raycast evaluates every sample, and with band
+  // allocation, which allocates no free space to step through): nonsat = voxels
   // that are observed and not saturated, kept exact by the integration;
   // freecell = 1 when every voxel a trilinear cell keyed in the block can
   // read (the block and its seven upper neighbours, missing neighbours

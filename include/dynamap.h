@@ -437,6 +437,18 @@ dyn_status dyn_icp_normal_equations_noalloc(
     const dyn_sensor* level, const dyn_gn_params* gn, const float T[16],
     double out_host[29], void* stream);
 
+/* The bounded grid-wide barrier of the persistent ICP (one cooperative
+ * launch per frame walks every level and iteration; its blocks meet at one
+ * barrier per iteration), run alone on 'device': 'blocks' blocks, all
+ * resident at once, wait for blocks + missing arrivals.  DYN_OK when the
+ * barrier completes; DYN_ERR_TIMEOUT when its bounded wait (half a second)
+ * runs out, as it must when missing > 0 -- the blocks give up and return,
+ * the device stays usable; DYN_ERR_INVALID_ARG when the blocks cannot all
+ * be resident (refused before anything runs).  A frame whose ICP barrier
+ * timed out reports DYN_ERR_TIMEOUT.  For tests of that failure path; no
+ * counterpart in the reference. */
+dyn_status dyn_barrier_selftest(int32_t device, int32_t blocks, int32_t missing);
+
 /* ---- multi-session stepping ---------------------------------------------
  * No counterpart in the reference (its builder drives one stream).
  *
