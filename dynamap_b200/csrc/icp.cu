@@ -118,31 +118,82 @@ __device__ inline void pixel_terms(const IcpLevel& L, const IcpParams& P, const 
   acc_add<KAHAN>(a, 28, 1.0f);
 }
 
-// Block sum of the 29 accumulators in double, fixed order; result in
-// red[0..28] (shared) after the call.
-__device__ inline void block_reduce(const Acc& a, bool kahan, double* red /*[8][29]*/) {
+// ---- block and tile sums
+// The FP32 form adds in FP64 throughout.  The mixed form keeps the normal
+// equations in FP32 up to the solve: a compensated pair (s, c) -- value
+// s + c, c the rounding error carried along -- is added with Knuth's
+// two-sum at every step (thread, warp shuffles, warps of a block, tiles),
+// and only the level's total becomes FP64 for the 6x6 solve.  A pair is
+// stored in a double-sized slot as two floats.
+__device__ inline void two_sum(float a, float b, float& s, float& e) {
+  s = __fadd_rn(a, b);
+  const float ap = __fsub_rn(s, b), bp = __fsub_rn(s, ap);
+  e = __fadd_rn(__fsub_rn(a, ap), __fsub_rn(b, bp));
+}
+__device__ inline void pair_add(float& s, float& c, float s2, float c2) {
+  float e;
+  two_sum(s, s2, s, e);
+  c = __fadd_rn(__fadd_rn(c, c2), e);
+}
+__device__ inline double pack_pair(float s, float c) {
+  return __longlong_as_double((long long)(((unsigned long long)__float_as_uint(c) << 32) |
+                                          (unsigned long long)__float_as_uint(s)));
+}
+__device__ inline void unpack_pair(double d, float& s, float& c) {
+  const unsigned long long u = (unsigned long long)__double_as_longlong(d);
+  s = __uint_as_float((unsigned)(u & 0xffffffffull));
+  c = __uint_as_float((unsigned)(u >> 32));
+}
+
+// Block sum of the 29 accumulators in a fixed order; result in red[0..28]
+// (shared) after the call: FP64 values, or packed compensated pairs (KAHAN).
+template <bool KAHAN>
+__device__ inline void block_reduce(const Acc& a, double* red /*[8][29]*/) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int k = 0; k < kIcpVals; ++k) {
-    double v = kahan ? (double)a.v[k] - (double)a.c[k] : a.d[k];
+    if (KAHAN) {
+      float sv = a.v[k], sc = -a.c[k];  // Kahan's c is the negated error
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (lane == 0) red[warp * kIcpVals + k] = v;
+      for (int o = 16; o > 0; o >>= 1) {
+        const float s2 = __shfl_xor_sync(0xffffffffu, sv, o);
+        const float c2 = __shfl_xor_sync(0xffffffffu, sc, o);
+        pair_add(sv, sc, s2, c2);
+      }
+      if (lane == 0) red[warp * kIcpVals + k] = pack_pair(sv, sc);
+    } else {
+      double v = a.d[k];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) red[warp * kIcpVals + k] = v;
+    }
   }
   __syncthreads();
   if (threadIdx.x < kIcpVals) {
-    double s = 0.0;
-    for (int w = 0; w < kIcpThreads / 32; ++w) s += red[w * kIcpVals + threadIdx.x];
-    red[threadIdx.x] = s;  // row 0 reused: each thread rewrites its own column
+    if (KAHAN) {
+      float sv = 0.0f, sc = 0.0f;
+      for (int w = 0; w < kIcpThreads / 32; ++w) {
+        float s2, c2;
+        unpack_pair(red[w * kIcpVals + threadIdx.x], s2, c2);
+        pair_add(sv, sc, s2, c2);
+      }
+      red[threadIdx.x] = pack_pair(sv, sc);  // row 0 reused: each thread its own column
+    } else {
+      double sum = 0.0;
+      for (int w = 0; w < kIcpThreads / 32; ++w) sum += red[w * kIcpVals + threadIdx.x];
+      red[threadIdx.x] = sum;
+    }
   }
   __syncthreads();
 }
 
-// Sum of the per-block partials in FP64, in a fixed order: thread (g, k)
-// of 8 x 29 sums value k of blocks g, g + 8, g + 16, ... (all 29 values'
-// loads in flight at once, coalesced along k), then thread k adds the 8
-// group sums in group order.  'scratch' is 8 x 29 doubles of shared memory;
-// out[29] in shared memory.
+// Sum of the per-tile (or per-block) partials in a fixed order: thread
+// (g, k) of 8 x 29 sums value k of rows g, g + 8, g + 16, ... (all 29
+// values' loads in flight at once, coalesced along k), then thread k adds
+// the 8 group sums in group order.  'scratch' is 8 x 29 doubles of shared
+// memory; out[29] (shared) receives FP64 values (a compensated pair's
+// s + c in the KAHAN form).
+template <bool KAHAN>
 __device__ inline void final_reduce(const double* __restrict__ partials, int nblocks,
                                     double* out, double* scratch) {
   constexpr int kGroups = kIcpThreads / 32;  // 8: scratch is the block-reduce array
@@ -150,17 +201,39 @@ __device__ inline void final_reduce(const double* __restrict__ partials, int nbl
   const int t = threadIdx.x;
   if (t < kGroups * kIcpVals) {
     const int g = t / kIcpVals, k = t - g * kIcpVals;
-    double s = 0.0;
+    if (KAHAN) {
+      float sv = 0.0f, sc = 0.0f;
 #pragma unroll 4
-    for (int b = g; b < nblocks; b += kGroups) s += __ldcg(partials + (size_t)b * kIcpVals + k);
-    scratch[g * kIcpVals + k] = s;
+      for (int b = g; b < nblocks; b += kGroups) {
+        float s2, c2;
+        unpack_pair(__ldcg(partials + (size_t)b * kIcpVals + k), s2, c2);
+        pair_add(sv, sc, s2, c2);
+      }
+      scratch[g * kIcpVals + k] = pack_pair(sv, sc);
+    } else {
+      double sum = 0.0;
+#pragma unroll 4
+      for (int b = g; b < nblocks; b += kGroups) sum += __ldcg(partials + (size_t)b * kIcpVals + k);
+      scratch[g * kIcpVals + k] = sum;
+    }
   }
   __syncthreads();
   if (t < kIcpVals) {
-    double s = 0.0;
+    if (KAHAN) {
+      float sv = 0.0f, sc = 0.0f;
 #pragma unroll
-    for (int g = 0; g < kGroups; ++g) s += scratch[g * kIcpVals + t];
-    out[t] = s;
+      for (int g = 0; g < kGroups; ++g) {
+        float s2, c2;
+        unpack_pair(scratch[g * kIcpVals + t], s2, c2);
+        pair_add(sv, sc, s2, c2);
+      }
+      out[t] = (double)sv + (double)sc;  // FP64 from here on: the 6x6 solve
+    } else {
+      double sum = 0.0;
+#pragma unroll
+      for (int g = 0; g < kGroups; ++g) sum += scratch[g * kIcpVals + t];
+      out[t] = sum;
+    }
   }
   __syncthreads();
 }
@@ -402,7 +475,7 @@ __device__ inline void tile_partial(const IcpLevel& L, const IcpParams& P, const
     const int idx = base + m * kIcpThreads;
     if (idx < n) pixel_terms<KAHAN>(L, P, T, idx, a);
   }
-  block_reduce(a, KAHAN, red);
+  block_reduce<KAHAN>(a, red);
   if (threadIdx.x < kIcpVals) row[threadIdx.x] = red[threadIdx.x];
   __syncthreads();  // red is reused by the next tile
 }
@@ -411,12 +484,13 @@ __device__ inline void tile_partial(const IcpLevel& L, const IcpParams& P, const
 // GN update and the next transform, for a solver state held at st_* (global
 // memory in the chained kernels, shared memory in the persistent one).
 // tot[] must be shared; the update runs on thread 0.
+template <bool KAHAN>
 __device__ inline void level_update(const double* __restrict__ partials, int ntiles,
                                     const IcpParams& P, int pl, int it, double* tot, double* red,
                                     double* st_inc, double* st_prev, float* st_T,
                                     int* st_converged, int* st_iters, int* st_inliers,
                                     float* st_rms) {
-  final_reduce(partials, ntiles, tot, red);
+  final_reduce<KAHAN>(partials, ntiles, tot, red);
   if (threadIdx.x == 0) {
     st_iters[pl] = it;
     st_inliers[pl] = (int)tot[28];
@@ -457,8 +531,8 @@ __device__ inline void icp_iteration_body(const IcpLevel& L, const IcpParams& P,
   if (ticket != (unsigned)nb - 1) return;
   __threadfence();
   __shared__ double tot[kIcpVals];
-  level_update(partials, ntiles, P, pl, it, tot, red, st->inc, st->prev, st->T, &st->converged,
-               st->iters, st->inliers, st->rms);
+  level_update<KAHAN>(partials, ntiles, P, pl, it, tot, red, st->inc, st->prev, st->T,
+                      &st->converged, st->iters, st->inliers, st->rms);
   if (threadIdx.x == 0) st->ticket = 0;
 }
 
@@ -633,8 +707,12 @@ __global__ void __launch_bounds__(kIcpThreads, 2)
         return;
       }
       if (active) {
-        level_update(part, ntiles, S.icpp, pl, it, tot, red, inc, prev, Tf, &conv, iters, inliers,
-                     rms);
+        if (S.icpp.kahan)
+          level_update<true>(part, ntiles, S.icpp, pl, it, tot, red, inc, prev, Tf, &conv, iters,
+                             inliers, rms);
+        else
+          level_update<false>(part, ntiles, S.icpp, pl, it, tot, red, inc, prev, Tf, &conv, iters,
+                              inliers, rms);
         __syncthreads();
       }
       parity ^= 1;
@@ -686,7 +764,7 @@ __global__ void __launch_bounds__(kIcpThreads)
   for (int idx = blockIdx.x * kIcpThreads + threadIdx.x; idx < n;
        idx += gridDim.x * kIcpThreads)
     pixel_terms<KAHAN>(L, P, T, idx, a);
-  block_reduce(a, KAHAN, red);
+  block_reduce<KAHAN>(a, red);
   if (threadIdx.x < kIcpVals) partials[(size_t)blockIdx.x * kIcpVals + threadIdx.x] = red[threadIdx.x];
   __threadfence();
   __shared__ unsigned int ticket;
@@ -695,7 +773,7 @@ __global__ void __launch_bounds__(kIcpThreads)
   if (ticket != gridDim.x - 1) return;
   __threadfence();
   __shared__ double tot[kIcpVals];
-  final_reduce(partials, gridDim.x, tot, red);
+  final_reduce<KAHAN>(partials, gridDim.x, tot, red);
   if (threadIdx.x < kIcpVals) out[threadIdx.x] = tot[threadIdx.x];
   if (threadIdx.x == 0) *ticket_ctr = 0;
 }
