@@ -19,6 +19,16 @@
 // frame rate; PipeReader reads frames from a file descriptor (a pipe from a
 // capture process) in a small binary format (see PipeReader).
 //
+// A stream's block pool is fixed when it is admitted.  With an eviction
+// policy (StreamConfig::evict) the front end keeps it from filling: after a
+// frame whose map holds more than highWater of the pool, the blocks the
+// allocation has not touched for more than maxAge frames move to a host
+// store (dyn_evict_blocks, the reference's unused HashTable::DeleteBlock
+// applied by age); before each frame, stored blocks that the camera at its
+// last pose can see -- within the sensor's range and image, widened by a
+// margin -- go back (dyn_upload_blocks), so a revisited place keeps what
+// was fused into it.
+//
 // Header-only over the C ABI of dynamap.h; needs C++17 and threads.
 #pragma once
 
@@ -29,10 +39,12 @@
 #include <cstring>
 #include <deque>
 #include <functional>
+#include <cmath>
 #include <map>
 #include <memory>
 #include <mutex>
 #include <thread>
+#include <unordered_map>
 #include <vector>
 
 #include <unistd.h>
@@ -57,6 +69,15 @@ class DynaMapNodeHandler {
     int precision = DYN_PRECISION_FP32;
     Matrix4f pose0;
     bool bilateral = true;
+    struct EvictPolicy {
+      bool enabled = false;
+      float highWater = 0.85f;  // share of the pool that triggers an eviction
+      int maxAge = 4;           // blocks untouched for more frames leave
+      float margin = 0.1f;      // metres the upload's view test is widened by
+    } evict;
+  };
+  struct StreamCounts {
+    int64_t evictions = 0, evicted = 0, uploaded = 0, stored = 0;
   };
   // tf_publisher's role: the frame's time stamp, its camera pose and the
   // frame's statistics (status: the frame's dyn_status, e.g. a full heap)
@@ -104,6 +125,8 @@ class DynaMapNodeHandler {
     st->slot = slot;
     st->npx = (size_t)c.sensor.rows * c.sensor.cols;
     st->scaler = c.sensor.depthScaler;
+    st->cfg = c;
+    st->pose = c.pose0;
     const int id = next_id_++;
     streams_[id] = st;
     return id;
@@ -175,6 +198,12 @@ class DynaMapNodeHandler {
     if (worker_.joinable()) worker_.join();
     idle_cv_.notify_all();
   }
+  // eviction and upload counts of a stream (its host store's blocks)
+  StreamCounts counts(int stream) {
+    std::lock_guard<std::mutex> lk(mu_);
+    auto it = streams_.find(stream);
+    return it == streams_.end() ? StreamCounts() : it->second->counts;
+  }
   // frames processed, steps run (several frames share a step)
   int64_t framesDone() const { return frames_done_; }
   int64_t steps() const { return steps_; }
@@ -205,7 +234,84 @@ class DynaMapNodeHandler {
     bool in_flight = false;  // a frame pushed and stepped, result not yet read
     double stamp = 0.0;      // that frame's
     bool closing = false;
+    StreamConfig cfg;
+    Matrix4f pose;           // after the last reported frame
+    // evicted blocks: packed coordinate -> 512 voxels
+    std::unordered_map<uint64_t, std::vector<dyn_voxel>> store;
+    StreamCounts counts;
   };
+  static uint64_t block_key(int x, int y, int z) {
+    const uint64_t m = (1ull << 21) - 1;
+    return (((uint64_t)x & m) << 42) | (((uint64_t)y & m) << 21) | ((uint64_t)z & m);
+  }
+  static int key_part(uint64_t k, int shift) {
+    return (int)((int64_t)(((k >> shift) & ((1ull << 21) - 1)) << 43) >> 43);
+  }
+
+  // Stored blocks the camera at the stream's last pose can see go back into
+  // its volume (server lock held; the stream has no frame on the device).
+  void upload_visible(Stream& s) {
+    if (!s.cfg.evict.enabled || s.store.empty()) return;
+    const float bs = s.cfg.tsdf.voxelSize * (float)s.cfg.tsdf.blockSize;
+    const float r = bs * 0.8660254f + s.cfg.evict.margin;  // half diagonal + margin
+    const rgbdSensor& sn = s.cfg.sensor;
+    const Matrix4f& P = s.pose;
+    std::vector<int32_t> coords;
+    std::vector<dyn_voxel> vox;
+    std::vector<uint64_t> taken;
+    for (const auto& kv : s.store) {
+      const int x = key_part(kv.first, 42), y = key_part(kv.first, 21), z = key_part(kv.first, 0);
+      const float c[3] = {((float)x + 0.5f) * bs, ((float)y + 0.5f) * bs, ((float)z + 0.5f) * bs};
+      float q[3];  // R^T (c - t)
+      for (int i = 0; i < 3; ++i)
+        q[i] = P(0, i) * (c[0] - P(0, 3)) + P(1, i) * (c[1] - P(1, 3)) + P(2, i) * (c[2] - P(2, 3));
+      if (q[2] < -r || q[2] > s.cfg.tsdf.maxSensorDepth + r) continue;
+      bool in = q[2] <= r;  // around the camera: always
+      if (!in) {
+        const float u = sn.f.x * q[0] / q[2] + sn.c.x, v = sn.f.y * q[1] / q[2] + sn.c.y;
+        const float pu = sn.f.x * r / q[2], pv = sn.f.y * r / q[2];
+        in = u >= -pu && u <= (float)sn.cols + pu && v >= -pv && v <= (float)sn.rows + pv;
+      }
+      if (!in) continue;
+      coords.insert(coords.end(), {x, y, z});
+      vox.insert(vox.end(), kv.second.begin(), kv.second.end());
+      taken.push_back(kv.first);
+    }
+    if (taken.empty()) return;
+    dyn_session* sess = nullptr;
+    dyn_server_session(server_, s.slot, &sess);
+    int64_t counts[4] = {0, 0, 0, 0};
+    if (sess && dyn_upload_blocks(sess, coords.data(), vox.data(), (int64_t)taken.size(), counts) ==
+                    DYN_OK) {
+      for (uint64_t k : taken) s.store.erase(k);
+      std::lock_guard<std::mutex> lk(mu_);
+      s.counts.uploaded += counts[0];
+      s.counts.stored = (int64_t)s.store.size();
+    }
+  }
+
+  // After a frame: the pool past its high-water mark sends the blocks the
+  // allocation has not touched for maxAge frames to the host store.
+  void evict_old(Stream& s, const dyn_frame_stats& st) {
+    const auto& e = s.cfg.evict;
+    if (!e.enabled || (double)st.blocks_total <= (double)e.highWater * s.cfg.tsdf.numBlocks) return;
+    dyn_session* sess = nullptr;
+    dyn_server_session(server_, s.slot, &sess);
+    if (!sess) return;
+    const int64_t cap = st.blocks_total;
+    std::vector<int32_t> coords((size_t)cap * 3);
+    std::vector<dyn_voxel> vox((size_t)cap * 512);
+    int64_t n = 0;
+    if (dyn_evict_blocks(sess, e.maxAge, coords.data(), vox.data(), cap, &n) != DYN_OK) return;
+    const int64_t m = n < cap ? n : cap;
+    for (int64_t i = 0; i < m; ++i)
+      s.store[block_key(coords[3 * i], coords[3 * i + 1], coords[3 * i + 2])] =
+          std::vector<dyn_voxel>(vox.begin() + i * 512, vox.begin() + (i + 1) * 512);
+    std::lock_guard<std::mutex> lk(mu_);
+    s.counts.evictions++;
+    s.counts.evicted += m;
+    s.counts.stored = (int64_t)s.store.size();
+  }
 
   // One pass: push the next frame of every stream without a frame on the
   // device, step once, then report the results that are ready.
@@ -241,6 +347,7 @@ class DynaMapNodeHandler {
             f = std::move(s->queue.front());
             s->queue.pop_front();
           }
+          upload_visible(*s);
           const dyn_status r = dyn_server_push(server_, s->slot, f.depth.data(),
                                                f.rgb.empty() ? nullptr : f.rgb.data());
           if (r == DYN_ERR_NOT_READY) {  // not stepped yet: put it back
@@ -283,6 +390,8 @@ class DynaMapNodeHandler {
           dyn_throw("DynaMapNodeHandler: poll", dyn_server_poll(server_, s->slot, &done));
           if (!done) continue;
           r = dyn_server_result(server_, s->slot, pose, &st);
+          s->pose = Matrix4f::from_row_major(pose);
+          evict_old(*s, st);
         }
         {
           std::lock_guard<std::mutex> lk(mu_);

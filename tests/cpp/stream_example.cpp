@@ -1,14 +1,17 @@
 // Streams through the front end (include/nodeHandler/nodeHandler.h): one
 // served session per line of a spec file, each fed by a TUM-layout
 // directory replayed at a frame rate or by frames on standard input.
-//   stream_example SPEC OUT
+//   stream_example SPEC OUT [--evict HIGH_WATER MAX_AGE MARGIN]
 // SPEC, one stream per line:
 //   SOURCE rows cols fx fy cx cy scaler voxel buckets blocks trunc maxdepth
 //   colour_weight precision rate_hz p00 .. p33 (first pose, row-major)
 // SOURCE: a directory, or "-" for frames on standard input (the pipe
 // format of PipeReader).  OUT, one line per frame as the pose callback
-// reports it: "stream stamp status it0 it1 it2 p00 .. p33".
+// reports it: "stream stamp status it0 it1 it2 p00 .. p33".  With --evict
+// every stream gets the front end's eviction policy, and stdout ends with
+// one line per stream: "counts stream evictions evicted uploaded stored".
 #include <cstdio>
+#include <cstdlib>
 #include <fstream>
 #include <memory>
 #include <mutex>
@@ -21,7 +24,14 @@
 using namespace DynaMap;
 
 int main(int argc, char** argv) {
-  if (argc != 3) return 2;
+  if (argc != 3 && argc != 7) return 2;
+  DynaMapNodeHandler::StreamConfig::EvictPolicy ev;
+  if (argc == 7) {
+    ev.enabled = true;
+    ev.highWater = (float)std::atof(argv[4]);
+    ev.maxAge = std::atoi(argv[5]);
+    ev.margin = (float)std::atof(argv[6]);
+  }
   std::ifstream spec(argv[1]);
   std::vector<std::string> sources;
   std::vector<DynaMapNodeHandler::StreamConfig> cfgs;
@@ -50,6 +60,7 @@ int main(int argc, char** argv) {
     c.solver.icpMaxDepth = c.tsdf.maxSensorDepth;
     c.solver.huberConstant = 0.3f;
     c.pose0 = Matrix4f::from_row_major(pose);
+    c.evict = ev;
     sources.push_back(src);
     cfgs.push_back(c);
     rates.push_back(rate);
@@ -92,10 +103,17 @@ int main(int argc, char** argv) {
     if (pipe->malformed()) return 3;
   }
   node.waitIdle();
+  std::vector<DynaMapNodeHandler::StreamCounts> counts;
+  for (int id : ids) counts.push_back(node.counts(id));
   for (int id : ids) node.removeStream(id);
   node.shutdown();
   std::fclose(out);
   std::printf("frames %d done %lld steps %lld\n", sent, (long long)node.framesDone(),
               (long long)node.steps());
+  if (ev.enabled)
+    for (size_t i = 0; i < ids.size(); ++i)
+      std::printf("counts %d %lld %lld %lld %lld\n", ids[i], (long long)counts[i].evictions,
+                  (long long)counts[i].evicted, (long long)counts[i].uploaded,
+                  (long long)counts[i].stored);
   return node.framesDone() == sent ? 0 : 1;
 }

@@ -121,3 +121,72 @@ def test_streams_through_the_server_equal_lone_sessions(tmp_path, gpu_lib):
                 assert [int(v) for v in rs[k][3:6]] == list(st.icp_iterations)
     # the pipe stream's stamps came through
     np.testing.assert_allclose(sorted(float(x[1]) for x in got[2]), pstamps, atol=1e-6)
+
+
+def write_tum_order(root, seq, order, t0=1305031102.0):
+    """A TUM-layout directory whose k-th frame is frame order[k] of seq."""
+    import cv2
+    from dynamap_b200 import trajectory
+    os.makedirs(root / "depth")
+    os.makedirs(root / "rgb")
+    rows, gt = [], []
+    for k, i in enumerate(order):
+        td = t0 + 0.0333 * k
+        dn, rn = "depth/%.6f.png" % td, "rgb/%.6f.png" % (td + 0.004)
+        assert cv2.imwrite(str(root / dn), seq.depth[i].astype(np.uint16))
+        assert cv2.imwrite(str(root / rn), np.ascontiguousarray(seq.rgb[i][:, :, ::-1]))
+        rows.append((td, dn, td + 0.004, rn))
+        gt.append(trajectory.tum_line(td + 0.002, seq.poses[i]))
+    (root / "association.txt").write_text("".join("%.6f %s %.6f %s\n" % r for r in rows))
+    (root / "groundtruth.txt").write_text("\n".join(gt) + "\n")
+
+
+@pytest.mark.gpu
+@pytest.mark.first_b200_run
+def test_eviction_keeps_a_small_pool_from_filling(tmp_path, gpu_lib):
+    """A 160x120 RGB stream that moves 3 cm / 2 deg per frame for 12 frames
+    and comes back: its map outgrows a 46,000-block pool on the way out (one
+    frame allocates about 40,000 blocks with free-space carving).  Without a
+    policy frames report the heap exhausted; with eviction (above 90 % of
+    the pool, blocks untouched for more than 2 frames) every frame succeeds,
+    blocks go to the host and come back when the camera returns, and the
+    trajectory stays within 5 mm of a session whose pool holds everything."""
+    from dynamap_b200.session import Session
+    p = configs.preset("cfg2")
+    p["sensor"].update(rows=120, cols=160, fx=131.25, fy=131.25, cx=79.5, cy=59.5)
+    p["seq"].update(trans=0.03, rot=2.0)
+    p["tsdf"].update(num_buckets=1 << 18, num_blocks=46000)
+    seq = configs.sequence(p, seed=31, n_frames=12)
+    order = list(range(12)) + list(range(10, -1, -1))
+    root = tmp_path / "seq"
+    root.mkdir()
+    write_tum_order(root, seq, order)
+    pp = stream_preset(p, 0.1)
+    spec = tmp_path / "spec.txt"
+    spec.write_text(spec_line(str(root), pp, abi.PRECISION_FP32, 0.0, seq.poses[0]) + "\n")
+    exe = str(tmp_path / "stream")
+    compile_stream(exe)
+    runs = {}
+    for name, extra in (("plain", []), ("evict", ["--evict", "0.9", "2", "0.1"])):
+        out = tmp_path / f"{name}.txt"
+        r = subprocess.run([exe, str(spec), str(out)] + extra, capture_output=True, text=True,
+                           timeout=300)
+        assert r.returncode == 0, r.stdout + r.stderr
+        runs[name] = ([ln.split() for ln in out.read_text().splitlines()], r.stdout)
+    plain_status = [int(x[2]) for x in runs["plain"][0]]
+    assert abi.DYN_ERR_HEAP_EXHAUSTED in plain_status
+    rows, stdout = runs["evict"]
+    assert len(rows) == len(order) and all(int(x[2]) == 0 for x in rows), [x[2] for x in rows]
+    c = [ln.split() for ln in stdout.splitlines() if ln.startswith("counts")][0]
+    evictions, evicted, uploaded = int(c[2]), int(c[3]), int(c[4])
+    assert evictions > 0 and evicted > 0 and uploaded > 0, c
+    # the same frames through a session whose pool holds the whole map
+    big = dict(pp)
+    big["tsdf"] = dict(pp["tsdf"], num_blocks=1 << 17)
+    t, g, b, s = configs.structs(big)
+    with Session(t, g, b, s) as m:
+        m.set_pose(seq.poses[0])
+        ref = [m.process(seq.depth[i], seq.rgb[i])[0] for i in order]
+    got = [np.array([float(v) for v in x[6:22]], np.float32).reshape(4, 4) for x in rows]
+    diff = max(float(np.linalg.norm(a[:3, 3] - r_[:3, 3])) for a, r_ in zip(got, ref))
+    assert diff < 5e-3, diff
