@@ -831,9 +831,11 @@ def run_large(args):
     e0.record(ts)
     vis = np.zeros(n)
     stats = None
+    exhausted = np.zeros(n, np.int64)  # frames that found the block pool full
     for k in range(args.warmup, nframes):
         _, stats, _ = step(k)
         vis += np.array([st.blocks_visible for st in stats], np.float64)
+        exhausted += np.array([st.heap_exhausted > 0 for st in stats], np.int64)
     torch.cuda.synchronize()
     e1.record(ts)
     torch.cuda.synchronize()
@@ -876,7 +878,7 @@ def run_large(args):
         "data": "synthetic: seeded room scene (8 x 8 x 3 m, walls, 40 primitives) and "
                 "cube scenes, Perlin albedo RGB",
         "config": {"workload": "cfg5: one 1280x720 RGB-D session (room, 4 mm voxels, 2^23 "
-                               "buckets x 10, 2^21 blocks, 8 m range) batched with eight "
+                               "buckets x 10, 2^22 blocks, 8 m range) batched with eight "
                                f"640x480 RGB-D sessions (cfg2), {args.precision}, one frame "
                                "of every session per step",
                    "precision": args.precision, "sessions_per_gpu": n,
@@ -884,6 +886,8 @@ def run_large(args):
         "stage_ms_per_step": stage_ms,
         "hbm_fraction": frac,
         "large_session": {"blocks_total": int(big_blocks),
+                          "pool_blocks": int(t0s.num_blocks),
+                          "frames_heap_exhausted": int(exhausted[0]),
                           "voxels": int(big_blocks) * 512,
                           "hash_load_factor": big_blocks / (t0s.num_buckets * t0s.bucket_size),
                           "visible_per_frame": float(vis[0])},

@@ -49,14 +49,14 @@ PRESETS = {
         seq=dict(n_frames=500, trans=0.01, rot=1.0, rgb=True, kind="cube"),
     ),
     # Large-scene stress: 1280x720 depth + RGB through the 8 x 8 x 3 m room
-    # (walls, 40 primitives), 4 mm voxels, 2^23 buckets, 2^21 blocks,
+    # (walls, 40 primitives), 4 mm voxels, 2^23 buckets, 2^22 blocks,
     # ranges to 8 m; run in the mixed form with band allocation, batched with
     # eight 640x480 sessions (cfg2 sensor, cube scenes).
     "cfg5": dict(
         sensor=dict(rows=720, cols=1280, fx=910.0, fy=910.0, cx=639.5, cy=359.5,
                     depth_scaler=1000.0),
         tsdf=dict(voxel_size=0.004, num_buckets=1 << 23, bucket_size=10,
-                  num_blocks=1 << 21, block_size=8, max_sdf_weight=64,
+                  num_blocks=1 << 22, block_size=8, max_sdf_weight=64,
                   truncation_distance=0.016, max_sensor_depth=8.0,
                   min_sensor_depth=0.15),
         gn=_gn([10, 5, 4], color_weight=0.1, dmax=8.0),

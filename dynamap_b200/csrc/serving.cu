@@ -141,6 +141,8 @@ dyn_status dyn_batch_create(dyn_session* const* sessions, int32_t n, dyn_batch**
   one.st[0] = b->stream;
   one.tab[0] = b->d_tab;
   one.map[0] = b->d_map;
+  b->sorted = sorted;
+  b->gstart.assign(start.begin(), start.end());
   one.shape[0] = make_shape(sorted.data(), n, b->d_gvis, b->d_gcount, (int)cap);
   set_icp_persistent(one.shape[0], sorted.data(), n, b->d_icp_bar, icp_persistent_capacity(b->device));
   b->shape = one.shape[0];
@@ -164,17 +166,30 @@ static dyn_status batch_ready(dyn_batch* b) {
 // Autotuner candidates: launch shapes that change no result (integration
 // CTAs, raycast tile), so they can be timed on live frames.
 struct TuneCandidate {
-  int integrate_ctas, ray_tile;
+  int integrate_ctas;
+  int ray_tile;
+  int icp;  // 0: persistent ICP on the group's full share of the resident
+            // blocks, 1: on half of it, 2: the chained kernels
 };
-constexpr TuneCandidate kTune[] = {{148 * 8, 0}, {148 * 4, 0}, {148 * 16, 0},
-                                   {148 * 8, 1}, {148 * 4, 1}, {148 * 16, 1},
-                                   {148 * 8, 2}, {148 * 4, 2}, {148 * 16, 2}};
+// Phase 1: the integration grid x the raycast tile (persistent ICP); phase
+// 2: the ICP's shape with phase 1's best.  Every candidate gives the same
+// results (the batch test steps through all of them).
+constexpr TuneCandidate kTune[] = {{148 * 8, 0, 0}, {148 * 4, 0, 0}, {148 * 16, 0, 0},
+                                   {148 * 8, 1, 0}, {148 * 4, 1, 0}, {148 * 16, 1, 0},
+                                   {148 * 8, 2, 0}, {148 * 4, 2, 0}, {148 * 16, 2, 0}};
 constexpr int kNumTune = (int)(sizeof(kTune) / sizeof(kTune[0]));
+constexpr int kNumIcpShapes = 3;
 
 static void apply_shape(dyn_batch* b, const TuneCandidate& c) {
-  for (int g = 0; g < b->groups.k; ++g) {
-    b->groups.shape[g].integrate_ctas = c.integrate_ctas;
-    b->groups.shape[g].ray_tile = c.ray_tile;
+  const int cap = icp_persistent_capacity(b->device);
+  const int k = b->groups.k;
+  for (int g = 0; g < k; ++g) {
+    BatchShape& sh = b->groups.shape[g];
+    sh.integrate_ctas = c.integrate_ctas;
+    sh.ray_tile = c.ray_tile;
+    const int budget = c.icp == 2 ? 0 : (c.icp == 1 ? cap / k / 2 : cap / k);
+    set_icp_persistent(sh, b->sorted.data() + b->gstart[g], b->gstart[g + 1] - b->gstart[g],
+                       sh.icp_bar, budget);
   }
   b->single.shape[0].integrate_ctas = c.integrate_ctas;
   b->single.shape[0].ray_tile = c.ray_tile;
@@ -182,6 +197,15 @@ static void apply_shape(dyn_batch* b, const TuneCandidate& c) {
     cudaGraphExecDestroy(b->exec);
     b->exec = nullptr;
   }
+}
+
+// The candidate measured in position i of the run: phase 1's shapes, then
+// the ICP shapes 1 and 2 with phase 1's best.
+static TuneCandidate tune_candidate(const dyn_batch* b, int i) {
+  if (i < kNumTune) return kTune[i];
+  TuneCandidate c = kTune[b->tune_best1];
+  c.icp = 1 + (i - kNumTune);
+  return c;
 }
 
 // Reads the last timed frame and moves through the candidates: each runs
@@ -196,15 +220,24 @@ static dyn_status tune_step(dyn_batch* b) {
     if (b->tune_count > 0) b->tune_ms[b->tune_idx] += ms;
     if (++b->tune_count >= b->tune_frames) {
       b->tune_count = 0;
-      if (++b->tune_idx == kNumTune) {
+      ++b->tune_idx;
+      if (b->tune_idx == kNumTune) {  // phase 1 done: its best, then the ICP shapes
         int best = 0;
         for (int i = 1; i < kNumTune; ++i)
           if (b->tune_ms[i] < b->tune_ms[best]) best = i;
+        b->tune_best1 = best;
+      }
+      if (b->tune_idx == kNumTune + kNumIcpShapes - 1) {
+        int best = 0;
+        for (int i = 1; i < b->tune_idx; ++i)
+          if (b->tune_ms[i] < b->tune_ms[best]) best = i;
         b->tune_best = best;
-        apply_shape(b, kTune[best]);
+        const TuneCandidate c = tune_candidate(b, best);
+        b->tune_icp = c.icp;
+        apply_shape(b, c);
         return DYN_OK;
       }
-      apply_shape(b, kTune[b->tune_idx]);
+      apply_shape(b, tune_candidate(b, b->tune_idx));
     }
   }
   return DYN_OK;
@@ -344,7 +377,8 @@ dyn_status dyn_batch_autotune(dyn_batch* b, int32_t frames_per_candidate) {
   b->tune_count = 0;
   b->tune_best = -1;
   b->tune_pending = false;
-  b->tune_ms.assign(kNumTune, 0.0f);
+  b->tune_ms.assign(kNumTune + kNumIcpShapes - 1, 0.0f);
+  b->tune_best1 = -1;
   apply_shape(b, kTune[0]);  // the default shape, measured first
   return DYN_OK;
 }

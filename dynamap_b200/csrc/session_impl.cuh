@@ -293,6 +293,12 @@ struct dyn_batch {
   bool tune_pending = false;
   cudaEvent_t tune_ev[2] = {nullptr, nullptr};
   std::vector<float> tune_ms;
+  int tune_best1 = -1;          // phase 1's best candidate
+  int tune_icp = 0;             // the ICP shape kept (0 persistent, 1 half budget, 2 chained)
+  // members in table order and the first member of each group (for the
+  // ICP's launch shape)
+  std::vector<dyn_session*> sorted;
+  std::vector<int> gstart;
   bool pending = false;
 };
 
