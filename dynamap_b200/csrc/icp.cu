@@ -57,31 +57,80 @@ __device__ inline void acc_add(Acc& a, int k, float x) {
 // Per-pixel terms of buildNLSKernel (gnSolver.cu:55-194) for source pixel
 // idx; the reference's unchecked projection is bounded (z > 0, inside the
 // image) and photometric gradient taps outside the image read the centre.
-template <bool KAHAN>
-__device__ inline void pixel_terms(const IcpLevel& L, const IcpParams& P, const M4f& T,
-                                   int idx, Acc& a) {
-  const DSensor& s = L.s;
-  float d = L.sd[idx];
-  if (d < P.dmin || d > P.dmax) return;
-  float4 sn4 = L.sn[idx];
-  if (!normal_ok(sn4)) return;
-  F3 p = xform(T, point3d(idx, d, s));
-  if (!(p.z > 0.0f)) return;
+// Three steps, so that a thread can issue the loads of several pixels
+// before it waits on any: the source pixel's depth and normal, its
+// projection into the target, the target's depth, normal and intensities.
+struct PixSrc {
+  float d;
+  float4 n;
+};
+struct PixProj {
+  F3 p;        // source point in the target frame
+  float4 sn;   // source normal
+  int index;   // target pixel
   int px, py;
-  if (!project(p, s, &px, &py)) return;
-  if (px < 0 || py < 0 || px >= s.cols || py >= s.rows) return;
-  int index = py * s.cols + px;
-  float td = L.td[index];
-  if (td < P.dmin || td > P.dmax) return;
-  float4 n4 = L.tn[index];
-  if (!normal_ok(n4)) return;
-  F3 n = f3(n4.x, n4.y, n4.z);
-  float cosT = dot3(n, f3(sn4.x, sn4.y, sn4.z));
-  F3 q = point3d(index, td, s);
+};
+struct PixTgt {
+  float td;
+  float4 tn;
+  float ic, il, iu, si;  // photometric taps (colour weight != 0)
+};
+
+__device__ inline PixSrc load_src(const IcpLevel& L, int idx) {
+  PixSrc a;
+  a.d = L.sd[idx];
+  a.n = L.sn[idx];
+  return a;
+}
+
+__device__ inline bool project_src(const IcpLevel& L, const IcpParams& P, const M4f& T, int idx,
+                                   const PixSrc& a, PixProj& q) {
+  const DSensor& s = L.s;
+  if (a.d < P.dmin || a.d > P.dmax) return false;
+  if (!normal_ok(a.n)) return false;
+  F3 p = xform(T, point3d(idx, a.d, s));
+  if (!(p.z > 0.0f)) return false;
+  int px, py;
+  if (!project(p, s, &px, &py)) return false;
+  if (px < 0 || py < 0 || px >= s.cols || py >= s.rows) return false;
+  q.p = p;
+  q.sn = a.n;
+  q.index = py * s.cols + px;
+  q.px = px;
+  q.py = py;
+  return true;
+}
+
+__device__ inline PixTgt load_tgt(const IcpLevel& L, const IcpParams& P, const PixProj& q,
+                                  int idx) {
+  PixTgt t;
+  t.td = L.td[q.index];
+  t.tn = L.tn[q.index];
+  if (P.cw != 0.0f) {
+    const int il = q.px >= 1 ? q.index - 1 : q.index;
+    const int iu = q.py >= 1 ? q.index - L.s.cols : q.index;
+    t.ic = L.ti[q.index];
+    t.il = L.ti[il];
+    t.iu = L.ti[iu];
+    t.si = L.si[idx];
+  }
+  return t;
+}
+
+template <bool KAHAN>
+__device__ inline void accumulate(const IcpLevel& L, const IcpParams& P, const PixProj& q,
+                                  const PixTgt& t, Acc& a) {
+  const DSensor& s = L.s;
+  if (t.td < P.dmin || t.td > P.dmax) return;
+  if (!normal_ok(t.tn)) return;
+  const F3 p = q.p;
+  F3 n = f3(t.tn.x, t.tn.y, t.tn.z);
+  float cosT = dot3(n, f3(q.sn.x, q.sn.y, q.sn.z));
+  F3 qq = point3d(q.index, t.td, s);
   if (!(fabsf(cosT) > P.cos_thr)) return;
   F3 c = cross3(p, n);
   float cn[6] = {c.x, c.y, c.z, n.x, n.y, n.z};
-  F3 pq = p - q;
+  F3 pq = p - qq;
   float b[6];
 #pragma unroll
   for (int k = 0; k < 6; ++k)
@@ -89,14 +138,11 @@ __device__ inline void pixel_terms(const IcpLevel& L, const IcpParams& P, const 
   float r = dot3(pq, n);
   if (P.cw != 0.0f) {
     // gnSolver.cu:137-190: J_c = grad(I_t)(1x3) * [-p^ | I](3x6)
-    int il = px >= 1 ? index - 1 : index;
-    int iu = py >= 1 ? index - s.cols : index;
-    float ic = L.ti[index];
-    float gx = (ic - L.ti[il]) / 2.0f;
-    float gy = (ic - L.ti[iu]) / 2.0f;
+    float gx = (t.ic - t.il) / 2.0f;
+    float gy = (t.ic - t.iu) / 2.0f;
     float Jc[6] = {gx * 0.0f + gy * (-p.z), gx * p.z + gy * 0.0f, gx * (-p.y) + gy * p.x,
                    gx, gy, 0.0f};
-    float e = ic - L.si[idx];
+    float e = t.ic - t.si;
     float w1 = 1.0f - P.cw;
     int u = 0;
 #pragma unroll
@@ -116,6 +162,33 @@ __device__ inline void pixel_terms(const IcpLevel& L, const IcpParams& P, const 
   }
   acc_add<KAHAN>(a, 27, r * r);
   acc_add<KAHAN>(a, 28, 1.0f);
+}
+
+template <bool KAHAN>
+__device__ inline void pixel_terms(const IcpLevel& L, const IcpParams& P, const M4f& T,
+                                   int idx, Acc& a) {
+  PixProj q;
+  if (!project_src(L, P, T, idx, load_src(L, idx), q)) return;
+  accumulate<KAHAN>(L, P, q, load_tgt(L, P, q, idx), a);
+}
+
+// Two pixels with their loads issued together (source, then target), then
+// added in order: the same sums as pixel_terms on i0, then on i1.
+template <bool KAHAN>
+__device__ inline void pixel_pair(const IcpLevel& L, const IcpParams& P, const M4f& T, int i0,
+                                  int i1, int n, Acc& a) {
+  const bool v0 = i0 < n, v1 = i1 < n;
+  PixSrc a0, a1;
+  if (v0) a0 = load_src(L, i0);
+  if (v1) a1 = load_src(L, i1);
+  PixProj q0, q1;
+  const bool ok0 = v0 && project_src(L, P, T, i0, a0, q0);
+  const bool ok1 = v1 && project_src(L, P, T, i1, a1, q1);
+  PixTgt t0, t1;
+  if (ok0) t0 = load_tgt(L, P, q0, i0);
+  if (ok1) t1 = load_tgt(L, P, q1, i1);
+  if (ok0) accumulate<KAHAN>(L, P, q0, t0, a);
+  if (ok1) accumulate<KAHAN>(L, P, q1, t1, a);
 }
 
 // ---- block and tile sums
@@ -147,26 +220,54 @@ __device__ inline void unpack_pair(double d, float& s, float& c) {
 
 // Block sum of the 29 accumulators in a fixed order; result in red[0..28]
 // (shared) after the call: FP64 values, or packed compensated pairs (KAHAN).
+// The warp sum is a halving exchange over 32 slots (values 29..31 zero):
+// at offset o every lane keeps the half of its remaining slots that its
+// bit o selects, sends the other half to lane ^ o and adds what that lane
+// sent; after offsets 16, 8, 4, 2, 1 lane l holds the warp's total of value
+// l.  31 exchanges per lane instead of 29 x 5 for a butterfly per value.
 template <bool KAHAN>
 __device__ inline void block_reduce(const Acc& a, double* red /*[8][29]*/) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (KAHAN) {
+    float s[32], c[32];
 #pragma unroll
-  for (int k = 0; k < kIcpVals; ++k) {
-    if (KAHAN) {
-      float sv = a.v[k], sc = -a.c[k];  // Kahan's c is the negated error
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const float s2 = __shfl_xor_sync(0xffffffffu, sv, o);
-        const float c2 = __shfl_xor_sync(0xffffffffu, sc, o);
-        pair_add(sv, sc, s2, c2);
-      }
-      if (lane == 0) red[warp * kIcpVals + k] = pack_pair(sv, sc);
-    } else {
-      double v = a.d[k];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-      if (lane == 0) red[warp * kIcpVals + k] = v;
+    for (int k = 0; k < kIcpVals; ++k) {
+      s[k] = a.v[k];
+      c[k] = -a.c[k];  // Kahan's c is the negated error
     }
+#pragma unroll
+    for (int k = kIcpVals; k < 32; ++k) s[k] = c[k] = 0.0f;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const bool up = (lane & o) != 0;
+#pragma unroll
+      for (int k = 0; k < o; ++k) {
+        const float ks = up ? s[k + o] : s[k], kc = up ? c[k + o] : c[k];
+        const float gs = up ? s[k] : s[k + o], gc = up ? c[k] : c[k + o];
+        const float rs = __shfl_xor_sync(0xffffffffu, gs, o);
+        const float rc = __shfl_xor_sync(0xffffffffu, gc, o);
+        s[k] = ks;
+        c[k] = kc;
+        pair_add(s[k], c[k], rs, rc);
+      }
+    }
+    if (lane < kIcpVals) red[warp * kIcpVals + lane] = pack_pair(s[0], c[0]);
+  } else {
+    double s[32];
+#pragma unroll
+    for (int k = 0; k < kIcpVals; ++k) s[k] = a.d[k];
+#pragma unroll
+    for (int k = kIcpVals; k < 32; ++k) s[k] = 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const bool up = (lane & o) != 0;
+#pragma unroll
+      for (int k = 0; k < o; ++k) {
+        const double keep = up ? s[k + o] : s[k], give = up ? s[k] : s[k + o];
+        s[k] = keep + __shfl_xor_sync(0xffffffffu, give, o);
+      }
+    }
+    if (lane < kIcpVals) red[warp * kIcpVals + lane] = s[0];
   }
   __syncthreads();
   if (threadIdx.x < kIcpVals) {
@@ -470,11 +571,10 @@ __device__ inline void tile_partial(const IcpLevel& L, const IcpParams& P, const
   }
   const int n = L.s.rows * L.s.cols;
   const int base = tile * kIcpTile + (int)threadIdx.x;
+  static_assert(kIcpTile / kIcpThreads % 2 == 0, "pixels go in pairs");
 #pragma unroll
-  for (int m = 0; m < kIcpTile / kIcpThreads; ++m) {
-    const int idx = base + m * kIcpThreads;
-    if (idx < n) pixel_terms<KAHAN>(L, P, T, idx, a);
-  }
+  for (int m = 0; m < kIcpTile / kIcpThreads; m += 2)
+    pixel_pair<KAHAN>(L, P, T, base + m * kIcpThreads, base + (m + 1) * kIcpThreads, n, a);
   block_reduce<KAHAN>(a, red);
   if (threadIdx.x < kIcpVals) row[threadIdx.x] = red[threadIdx.x];
   __syncthreads();  // red is reused by the next tile
@@ -520,10 +620,10 @@ __device__ inline void icp_iteration_body(const IcpLevel& L, const IcpParams& P,
   if (threadIdx.x < 16) Ts.m[threadIdx.x] = st->T[threadIdx.x];
   __syncthreads();
   if (skip) return;
-  const M4f T = Ts;
+  // the transform stays in shared memory (registers go to the sums)
   const int ntiles = icp_tiles(L.s.rows * L.s.cols);
   for (int tile = bid; tile < ntiles; tile += nb)
-    tile_partial<KAHAN>(L, P, T, tile, red, partials + (size_t)tile * kIcpVals);
+    tile_partial<KAHAN>(L, P, Ts, tile, red, partials + (size_t)tile * kIcpVals);
   __threadfence();
   __shared__ unsigned int ticket;
   if (threadIdx.x == 0) ticket = atomicAdd(&st->ticket, 1u);
@@ -569,9 +669,11 @@ __global__ void __launch_bounds__(kIcpThreads, 2)
   const SessDev& S = tab[blockIdx.z];
   if ((S.icpp.kahan != 0) != KAHAN) return;
   if (it >= S.slot_iters[pl]) return;  // the reference runs iterations 1 .. N-1
-  const IcpLevel L = level_of(S, S.slot_level[pl]);
-  const int nb = icp_grid(L.s.rows * L.s.cols);
+  const int l = S.slot_level[pl];
+  const int nb = icp_grid(S.ls[l].rows * S.ls[l].cols);
   if ((int)blockIdx.x >= nb) return;
+  __shared__ IcpLevel L;  // shared: registers go to the sums
+  if (threadIdx.x == 0) L = level_of(S, l);
   wait_predecessor();  // the solver state and partials of the previous iteration
   release_successor();
   icp_iteration_body<KAHAN>(L, S.icpp, pl, it, S.icp, S.partials, blockIdx.x, nb);
@@ -597,28 +699,60 @@ __device__ inline unsigned long long global_ns() {
   return t;
 }
 
-// Grid-wide barrier number k of a launch whose arrival counter 'bar' starts
-// at 0: complete when the counter reaches target = k * gridDim.x.  The wait
-// is bounded: after kBarrierWaitNs (or once *abort is raised) the block
-// gives up, raises *abort and returns false.
+// Grid-wide barrier number k (1, 2, ...) of a launch of 'nb' blocks (the
+// grid) whose barrier words (kIcpBarWords, zero at launch) are 'bar'.
+// Arrivals and releases are spread over kIcpBarSpread counters and flags,
+// each on its own 128-byte line: block b adds one to counter
+// b % kIcpBarSpread; block 0 alone polls the counters until each holds k
+// times its blocks, then writes k to every release flag; block b polls flag
+// b % kIcpBarSpread.  So no line takes
+// more than a few dozen blocks' polls beside the arrivals it counts.  Every
+// wait is bounded: after kBarrierWaitNs (or once the abort word is raised)
+// the block gives up, raises the abort word and returns false.
 constexpr unsigned long long kBarrierWaitNs = 500000000ull;  // half a second
-__device__ inline bool grid_barrier(unsigned* bar, unsigned target, int* abort) {
+__device__ inline unsigned* bar_counter(unsigned* bar, int i) { return bar + 32 * i; }
+__device__ inline unsigned* bar_flag(unsigned* bar, int i) {
+  return bar + 32 * (kIcpBarSpread + i);
+}
+__device__ inline int* bar_abort(unsigned* bar) {
+  return reinterpret_cast<int*>(bar + 32 * (2 * kIcpBarSpread));
+}
+__device__ inline bool grid_barrier(unsigned* bar, unsigned k, unsigned nb) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
+    const unsigned me = blockIdx.x;
+    int* abort = bar_abort(bar);
     __threadfence();  // this block's partial sums before its arrival
-    atomicAdd(bar, 1u);
+    atomicAdd(bar_counter(bar, (int)(me % kIcpBarSpread)), 1u);
     const unsigned long long t0 = global_ns();
     int good = 1;
-    while (*(volatile unsigned*)bar < target) {
-      if (*(volatile int*)abort || global_ns() - t0 > kBarrierWaitNs) {
-        good = 0;
-        break;
+    if (me == 0) {
+      for (int i = 0; i < kIcpBarSpread && good; ++i) {
+        const unsigned want = k * ((nb + kIcpBarSpread - 1 - (unsigned)i) / kIcpBarSpread);
+        while (*(volatile unsigned*)bar_counter(bar, i) < want) {
+          if (*(volatile int*)abort || global_ns() - t0 > kBarrierWaitNs) {
+            good = 0;
+            break;
+          }
+          __nanosleep(32);
+        }
       }
-      __nanosleep(64);
+      __threadfence();  // the arrivals' partial sums before the release
+      if (good)
+        for (int i = 0; i < kIcpBarSpread; ++i) *(volatile unsigned*)bar_flag(bar, i) = k;
+    } else {
+      volatile unsigned* flag = bar_flag(bar, (int)(me % kIcpBarSpread));
+      while (*flag < k) {
+        if (*(volatile int*)abort || global_ns() - t0 > kBarrierWaitNs) {
+          good = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
     }
     if (!good) atomicExch(abort, 1);
-    __threadfence();  // the other blocks' partial sums after the arrivals
+    __threadfence();  // the other blocks' partial sums after the release
     ok = good;
   }
   __syncthreads();
@@ -634,17 +768,21 @@ __host__ __device__ inline int icp_share(int tiles, long long sum_tiles, int bud
   return (int)b;
 }
 
+// One instantiation per summation kind: a table whose sessions sum both
+// ways gets one launch per kind, each over that kind's sessions only.
+template <bool KAHAN>
 __global__ void __launch_bounds__(kIcpThreads, 2)
     fused_icp_persistent_kernel(const SessDev* __restrict__ tab, int n, int budget,
-                                int it0, int it1, int it2, unsigned* __restrict__ bar,
-                                int* __restrict__ abort) {
+                                int it0, int it1, int it2, unsigned* __restrict__ bar) {
   // this block's session and its index among the session's blocks
   __shared__ int z_s, local_s, nblk_s;
   if (threadIdx.x == 0) {
     long long sum = 0;
-    for (int j = 0; j < n; ++j) sum += icp_tiles(tab[j].npx);
+    for (int j = 0; j < n; ++j)
+      if ((tab[j].icpp.kahan != 0) == KAHAN) sum += icp_tiles(tab[j].npx);
     int first = 0, z = n - 1, nb = 1;
     for (int j = 0; j < n; ++j) {
+      if ((tab[j].icpp.kahan != 0) != KAHAN) continue;
       nb = icp_share(icp_tiles(tab[j].npx), sum, budget);
       if ((int)blockIdx.x < first + nb) {
         z = j;
@@ -664,7 +802,9 @@ __global__ void __launch_bounds__(kIcpThreads, 2)
   __shared__ double red[(kIcpThreads / 32) * kIcpVals];
   __shared__ double tot[kIcpVals];
   __shared__ double inc[6], prev[6];
-  __shared__ float Tf[16];
+  __shared__ M4f Tm;                      // the transform of the iteration
+  __shared__ IcpLevel Ls;                 // the iteration's level
+  float* const Tf = Tm.m;
   __shared__ int conv, have, iters[3], inliers[3];
   __shared__ float rms[3];
   if (threadIdx.x < 6) {
@@ -688,31 +828,29 @@ __global__ void __launch_bounds__(kIcpThreads, 2)
   int parity = 0;
   for (int pl = 0; pl < 3; ++pl)
     for (int it = 1; it < maxit[pl]; ++it) {
-      const bool active = own && it < S.slot_iters[pl] && have && !(it > 1 && conv);
-      const IcpLevel L = level_of(S, S.slot_level[pl]);
-      const int ntiles = icp_tiles(L.s.rows * L.s.cols);
+      const bool sess_active = it < S.slot_iters[pl] && have && !(it > 1 && conv);
+      // a lone session's blocks all hold its state: once it has converged
+      // (or has no target) they skip the level's remaining barriers together
+      if (n == 1 && !sess_active) continue;
+      const bool active = own && sess_active;
+      const int l = S.slot_level[pl];
+      const int ntiles = icp_tiles(S.ls[l].rows * S.ls[l].cols);
       double* part = S.partials + (size_t)parity * row;
       if (active) {
-        M4f T;
-#pragma unroll
-        for (int k = 0; k < 16; ++k) T.m[k] = Tf[k];
-        for (int tile = local; tile < ntiles; tile += nblk) {
-          if (S.icpp.kahan) tile_partial<true>(L, S.icpp, T, tile, red, part + (size_t)tile * kIcpVals);
-          else tile_partial<false>(L, S.icpp, T, tile, red, part + (size_t)tile * kIcpVals);
-        }
+        // level and transform stay in shared memory (registers go to the sums)
+        if (threadIdx.x == 0) Ls = level_of(S, l);
+        __syncthreads();
+        for (int tile = local; tile < ntiles; tile += nblk)
+          tile_partial<KAHAN>(Ls, S.icpp, Tm, tile, red, part + (size_t)tile * kIcpVals);
       }
       ++nbar;
-      if (!grid_barrier(bar, nbar * gridDim.x, abort)) {
+      if (!grid_barrier(bar, nbar, gridDim.x)) {
         if (threadIdx.x == 0) atomicExch(&S.vol.cnt->icp_timeout, 1);
         return;
       }
       if (active) {
-        if (S.icpp.kahan)
-          level_update<true>(part, ntiles, S.icpp, pl, it, tot, red, inc, prev, Tf, &conv, iters,
-                             inliers, rms);
-        else
-          level_update<false>(part, ntiles, S.icpp, pl, it, tot, red, inc, prev, Tf, &conv, iters,
-                              inliers, rms);
+        level_update<KAHAN>(part, ntiles, S.icpp, pl, it, tot, red, inc, prev, Tf, &conv, iters,
+                            inliers, rms);
         __syncthreads();
       }
       parity ^= 1;
@@ -736,11 +874,11 @@ __global__ void __launch_bounds__(kIcpThreads, 2)
   }
 }
 
-// A barrier self-test: 'blocks' blocks wait at barrier 1 for blocks + missing
-// arrivals (missing > 0: a wait that cannot complete, which must end in the
-// bounded timeout).
-__global__ void barrier_selftest_kernel(unsigned* bar, unsigned target, int* abort) {
-  grid_barrier(bar, target, abort);
+// A barrier self-test: the launch's blocks meet at barrier 1 expecting
+// 'expect' blocks (more than were launched: a wait that cannot complete,
+// which must end in the bounded timeout).
+__global__ void barrier_selftest_kernel(unsigned* bar, unsigned expect) {
+  grid_barrier(bar, 1u, expect);
 }
 
 // Normal equations only (stage entry point): no solver state.
@@ -922,33 +1060,47 @@ int icp_persistent_capacity(int device) {
   if (device < 0 || device >= 64) return 0;
   std::lock_guard<std::mutex> lk(mu);
   if (cap[device] == 0) {
-    int coop = 0, sms = 0, per_sm = 0;
+    int coop = 0, sms = 0, per_sm = 0, per_k = 0;
     if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fused_icp_persistent_kernel,
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fused_icp_persistent_kernel<false>,
+                                                      kIcpThreads, 0) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_k, fused_icp_persistent_kernel<true>,
                                                       kIcpThreads, 0) != cudaSuccess) {
       cudaGetLastError();
       coop = 0;
     }
+    per_sm = std::min(per_sm, per_k);
     cap[device] = coop ? std::max(1, per_sm * sms) : -1;
   }
   return cap[device] > 0 ? cap[device] : 0;
 }
 
-int icp_persistent_grid(const int* npx, int n, int budget) {
+int icp_persistent_grid(const int* npx, const int* kahan, int n, int budget, int* grid_k) {
+  grid_k[0] = grid_k[1] = 0;
   if (budget <= 0 || n <= 0) return 0;
-  long long sum = 0;
-  for (int j = 0; j < n; ++j) sum += icp_tiles(npx[j]);
-  long long g = 0;
-  for (int j = 0; j < n; ++j) g += icp_share(icp_tiles(npx[j]), sum, budget);
-  return g <= budget ? (int)g : 0;
+  for (int kind = 0; kind < 2; ++kind) {
+    long long sum = 0;
+    for (int j = 0; j < n; ++j)
+      if ((kahan[j] != 0) == (kind == 1)) sum += icp_tiles(npx[j]);
+    long long g = 0;
+    for (int j = 0; j < n; ++j)
+      if ((kahan[j] != 0) == (kind == 1)) g += icp_share(icp_tiles(npx[j]), sum, budget);
+    if (g > budget) {
+      grid_k[0] = grid_k[1] = 0;
+      return 0;
+    }
+    grid_k[kind] = (int)g;
+  }
+  return grid_k[0] + grid_k[1];
 }
 
-void fused_icp_persistent(const SessDev* tab, const BatchShape& b, cudaStream_t st) {
-  // the barrier's arrival counter and abort flag start at zero every frame
-  cudaMemsetAsync(b.icp_bar, 0, 2 * sizeof(unsigned), st);
+template <bool KAHAN>
+static void launch_persistent(const SessDev* tab, const BatchShape& b, cudaStream_t st) {
+  // the barrier's counters, flags and abort word start at zero every launch
+  cudaMemsetAsync(b.icp_bar, 0, kIcpBarWords * sizeof(unsigned), st);
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(b.icp_grid);
+  cfg.gridDim = dim3(b.icp_grid_k[KAHAN ? 1 : 0]);
   cfg.blockDim = dim3(kIcpThreads);
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
@@ -956,9 +1108,13 @@ void fused_icp_persistent(const SessDev* tab, const BatchShape& b, cudaStream_t 
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  cudaLaunchKernelEx(&cfg, fused_icp_persistent_kernel, tab, b.n, b.icp_budget,
-                     b.max_slot_iters[0], b.max_slot_iters[1], b.max_slot_iters[2], b.icp_bar,
-                     reinterpret_cast<int*>(b.icp_bar + 1));
+  cudaLaunchKernelEx(&cfg, fused_icp_persistent_kernel<KAHAN>, tab, b.n, b.icp_budget,
+                     b.max_slot_iters[0], b.max_slot_iters[1], b.max_slot_iters[2], b.icp_bar);
+}
+
+void fused_icp_persistent(const SessDev* tab, const BatchShape& b, cudaStream_t st) {
+  if (b.icp_grid_k[0] > 0) launch_persistent<false>(tab, b, st);
+  if (b.icp_grid_k[1] > 0) launch_persistent<true>(tab, b, st);
 }
 
 dyn_status icp_barrier_selftest(int blocks, int missing, unsigned* bar_dev, cudaStream_t st) {
@@ -972,7 +1128,8 @@ dyn_status icp_barrier_selftest(int blocks, int missing, unsigned* bar_dev, cuda
     return DYN_ERR_CUDA;
   }
   if (blocks > per_sm * sms) return DYN_ERR_INVALID_ARG;  // not all resident at once
-  if (cudaMemsetAsync(bar_dev, 0, 2 * sizeof(unsigned), st) != cudaSuccess) return DYN_ERR_CUDA;
+  if (cudaMemsetAsync(bar_dev, 0, kIcpBarWords * sizeof(unsigned), st) != cudaSuccess)
+    return DYN_ERR_CUDA;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(blocks);
   cfg.blockDim = dim3(32);
@@ -982,18 +1139,18 @@ dyn_status icp_barrier_selftest(int blocks, int missing, unsigned* bar_dev, cuda
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  const cudaError_t e = cudaLaunchKernelEx(&cfg, barrier_selftest_kernel, bar_dev,
-                                           (unsigned)(blocks + missing),
-                                           reinterpret_cast<int*>(bar_dev + 1));
+  const cudaError_t e =
+      cudaLaunchKernelEx(&cfg, barrier_selftest_kernel, bar_dev, (unsigned)(blocks + missing));
   if (e != cudaSuccess) {
     cudaGetLastError();
     return e == cudaErrorCooperativeLaunchTooLarge ? DYN_ERR_INVALID_ARG : DYN_ERR_CUDA;
   }
-  unsigned h[2] = {0, 0};
-  if (cudaMemcpyAsync(h, bar_dev, sizeof(h), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+  int abort_h = 0;
+  if (cudaMemcpyAsync(&abort_h, bar_dev + 32 * (2 * kIcpBarSpread), sizeof(int),
+                      cudaMemcpyDeviceToHost, st) != cudaSuccess ||
       cudaStreamSynchronize(st) != cudaSuccess)
     return DYN_ERR_CUDA;
-  return h[1] ? DYN_ERR_TIMEOUT : DYN_OK;
+  return abort_h ? DYN_ERR_TIMEOUT : DYN_OK;
 }
 
 void launch_pose_finalize(const IcpParams& P, IcpState* st, PoseState* ps, cudaStream_t stream) {

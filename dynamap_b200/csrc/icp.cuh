@@ -66,15 +66,22 @@ size_t icp_scratch_bytes();
 // at least icp_scratch_bytes().
 size_t icp_frame_scratch_bytes(size_t npx);
 
-// The persistent ICP (one cooperative launch per frame): the blocks that can
-// be resident at once on 'device' (0: cooperative launches unavailable),
-// and the grid of a table whose sessions' largest levels have npx[j]
-// pixels, within 'budget' blocks (0: the table does not fit; the chained
-// kernels run it, with the same results).
+// The persistent ICP (one cooperative launch per frame and summation kind):
+// the blocks that can be resident at once on 'device' (0: cooperative
+// launches unavailable), and the grids of a table whose sessions' largest
+// levels have npx[j] pixels and sum plainly (kahan[j] == 0) or with
+// compensation: grid_k[kind] blocks within 'budget' each (0: no session of
+// that kind).  Returns their total, or 0 when a kind does not fit (the
+// chained kernels run the table, with the same results).
 int icp_persistent_capacity(int device);
-int icp_persistent_grid(const int* npx, int n, int budget);
+int icp_persistent_grid(const int* npx, const int* kahan, int n, int budget, int* grid_k);
+// The persistent ICP's grid barrier words (a launch's arrival counters,
+// release flags and abort word, each on its own 128-byte line): a launch's
+// barrier buffer holds kIcpBarWords unsigned words.
+constexpr int kIcpBarSpread = 8;
+constexpr int kIcpBarWords = (2 * kIcpBarSpread + 1) * 32;
 // A bounded grid barrier run alone: 'blocks' blocks wait for blocks +
-// missing arrivals (bar_dev: two words).  DYN_OK when it completes,
+// missing arrivals (bar_dev: kIcpBarWords words).  DYN_OK when it completes,
 // DYN_ERR_TIMEOUT when the bounded wait ran out, DYN_ERR_INVALID_ARG when
 // the blocks cannot all be resident.
 dyn_status icp_barrier_selftest(int blocks, int missing, unsigned* bar_dev, cudaStream_t st);

@@ -18,6 +18,22 @@ extern "C" {
 
 // ---------------------------------------------------------------- batches
 
+// Resident blocks of group g's persistent ICP out of 'cap': in proportion
+// to the group's level-0 pixel tiles among all groups' (at least one).
+static int group_budget(const std::vector<dyn_session*>& sorted, const std::vector<int>& start,
+                        int g, int cap) {
+  long long all = 0, mine = 0;
+  const int k = (int)start.size() - 1;
+  for (int h = 0; h < k; ++h)
+    for (int j = start[h]; j < start[h + 1]; ++j) {
+      const long long t = icp_tiles((int)sorted[j]->npx);
+      all += t;
+      if (h == g) mine += t;
+    }
+  if (all <= 0) return 0;
+  return std::max(1, (int)((long long)cap * mine / all));
+}
+
 dyn_status dyn_batch_create(dyn_session* const* sessions, int32_t n, dyn_batch** out) {
   if (!out) return DYN_ERR_INVALID_ARG;
   *out = nullptr;
@@ -87,7 +103,7 @@ dyn_status dyn_batch_create(dyn_session* const* sessions, int32_t n, dyn_batch**
   if (r == DYN_OK) r = dalloc((void**)&b->d_map, sizeof(int) * (size_t)n);
   if (r == DYN_OK) r = dalloc((void**)&b->d_gvis, sizeof(int2) * (size_t)cap);
   if (r == DYN_OK) r = dalloc((void**)&b->d_gcount, sizeof(int) * kMaxGroups);
-  if (r == DYN_OK) r = dalloc((void**)&b->d_icp_bar, 2 * sizeof(unsigned) * kMaxGroups);
+  if (r == DYN_OK) r = dalloc((void**)&b->d_icp_bar, kIcpBarWords * sizeof(unsigned) * kMaxGroups);
   if (r == DYN_OK) r = dalloc((void**)&b->d_res, sizeof(ResultBlock) * (size_t)n);
   for (int g = 1; g < k && r == DYN_OK; ++g)
     if (cudaStreamCreateWithFlags(&b->groups.st[g], cudaStreamNonBlocking) != cudaSuccess ||
@@ -130,10 +146,10 @@ dyn_status dyn_batch_create(dyn_session* const* sessions, int32_t n, dyn_batch**
     G.map[g] = b->d_map + start[g];
     G.shape[g] = make_shape(sorted.data() + start[g], n_g, b->d_gvis + voff, b->d_gcount + g,
                             (int)cap_g);
-    // the groups' persistent ICP launches may run at once: each takes its
-    // share of the resident blocks
-    set_icp_persistent(G.shape[g], sorted.data() + start[g], n_g, b->d_icp_bar + 2 * g,
-                       icp_persistent_capacity(b->device) / k);
+    // the groups' persistent ICP launches may run at once: each takes a
+    // share of the resident blocks in proportion to its pixel tiles
+    set_icp_persistent(G.shape[g], sorted.data() + start[g], n_g, b->d_icp_bar + kIcpBarWords * g,
+                       group_budget(sorted, start, g, icp_persistent_capacity(b->device)));
     voff += cap_g;
   }
   FrameGroups& one = b->single;
@@ -187,7 +203,8 @@ static void apply_shape(dyn_batch* b, const TuneCandidate& c) {
     BatchShape& sh = b->groups.shape[g];
     sh.integrate_ctas = c.integrate_ctas;
     sh.ray_tile = c.ray_tile;
-    const int budget = c.icp == 2 ? 0 : (c.icp == 1 ? cap / k / 2 : cap / k);
+    const int share = group_budget(b->sorted, b->gstart, g, cap);
+    const int budget = c.icp == 2 ? 0 : (c.icp == 1 ? share / 2 : share);
     set_icp_persistent(sh, b->sorted.data() + b->gstart[g], b->gstart[g + 1] - b->gstart[g],
                        sh.icp_bar, budget);
   }
@@ -563,7 +580,7 @@ dyn_status dyn_server_create(const dyn_server_params* p, dyn_server** out) {
   bool ok = cudaMalloc(&sv->d_arena, sv->budget ? sv->budget : 256) == cudaSuccess &&
             cudaStreamCreateWithFlags(&sv->stream, cudaStreamNonBlocking) == cudaSuccess &&
             cudaMalloc(&sv->d_gcount, 256) == cudaSuccess &&
-            cudaMalloc(&sv->d_icp_bar, 256) == cudaSuccess &&
+            cudaMalloc(&sv->d_icp_bar, kIcpBarWords * sizeof(unsigned)) == cudaSuccess &&
             cudaMalloc(&sv->d_res, sizeof(ResultBlock) * (size_t)cap) == cudaSuccess &&
             cudaMallocHost(&sv->h_res, sizeof(ResultBlock) * (size_t)cap) == cudaSuccess;
   for (StepBuf& r : sv->ring)

@@ -89,10 +89,12 @@ struct BatchShape {
   int2* gvis;              // batch-wide visible list (session, heap index)
   int* gcount;             // its length (device)
   int gvis_cap;
-  // the persistent ICP: blocks of the cooperative launch (0: the chained
-  // kernels instead), the budget its sessions' shares are taken from, and
-  // the barrier's arrival counter and abort flag (two words, device)
+  // the persistent ICP: blocks of its cooperative launches (0: the chained
+  // kernels instead) in all and per summation kind (plain, compensated),
+  // the budget each launch's shares are taken from, and the barrier's
+  // counters, flags and abort word (kIcpBarWords, device)
   int icp_grid;
+  int icp_grid_k[2];
   int icp_budget;
   unsigned* icp_bar;
 };

@@ -287,10 +287,16 @@ void set_icp_persistent(BatchShape& b, dyn_session* const* ss, int n, unsigned* 
     const char* e = std::getenv("DYN_ICP_CHAINED");
     return e && e[0] == '1';
   }();
-  std::vector<int> npx((size_t)n);
-  for (int i = 0; i < n; ++i) npx[i] = (int)ss[i]->npx;
+  std::vector<int> npx((size_t)n), kahan((size_t)n);
+  for (int i = 0; i < n; ++i) {
+    npx[i] = (int)ss[i]->npx;
+    kahan[i] = ss[i]->icp_params().kahan;
+  }
   b.icp_budget = budget;
-  b.icp_grid = (chained_only || !bar) ? 0 : icp_persistent_grid(npx.data(), n, budget);
+  b.icp_grid_k[0] = b.icp_grid_k[1] = 0;
+  b.icp_grid = (chained_only || !bar)
+                   ? 0
+                   : icp_persistent_grid(npx.data(), kahan.data(), n, budget, b.icp_grid_k);
   b.icp_bar = bar;
 }
 
@@ -680,7 +686,7 @@ dyn_status alloc_device_buffers(dyn_session* s) {
   DYN_TRY(s->dalloc(&s->d_pose_override, 64));
   DYN_TRY(s->dalloc(&s->d_pose_in, 128));
   DYN_TRY(s->dalloc(&s->d_partials, icp_frame_scratch_bytes(s->npx)));
-  DYN_TRY(s->dalloc(&s->d_icp_bar, 2 * sizeof(unsigned)));
+  DYN_TRY(s->dalloc(&s->d_icp_bar, kIcpBarWords * sizeof(unsigned)));
   DYN_TRY(s->dalloc(&s->d_icp, sizeof(IcpState)));
   DYN_TRY(s->dalloc(&s->d_pose, sizeof(PoseState)));
   s->vol.t = dtsdf(*tsdf, precision);
@@ -1386,7 +1392,7 @@ dyn_status dyn_barrier_selftest(int32_t device, int32_t blocks, int32_t missing)
   DeviceGuard dg(device);
   unsigned* bar = nullptr;
   cudaStream_t st = nullptr;
-  if (cudaMalloc(&bar, 2 * sizeof(unsigned)) != cudaSuccess ||
+  if (cudaMalloc(&bar, kIcpBarWords * sizeof(unsigned)) != cudaSuccess ||
       cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
     cudaGetLastError();
     if (bar) cudaFree(bar);

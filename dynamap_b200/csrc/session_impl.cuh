@@ -274,7 +274,7 @@ struct dyn_batch {
   SessDev* d_tab = nullptr;
   int2* d_gvis = nullptr;
   int* d_gcount = nullptr;
-  unsigned* d_icp_bar = nullptr;  // two words per group (persistent ICP barrier)
+  unsigned* d_icp_bar = nullptr;  // kIcpBarWords per group (persistent ICP barrier)
   ResultBlock* d_res = nullptr;
   ResultBlock* h_res = nullptr;  // pinned, n entries
   BatchShape shape;
