@@ -238,6 +238,32 @@ __global__ void fused_ingest_kernel(const SessDev* __restrict__ tab) {
   S.sdist[i] = norm3(point3d_uv(i - y * s0.cols, y, d, s0));
 }
 
+// The free-space tile map of a depth-only frame of a carving session (one
+// thread per fine tile; its value also enters its coarse tile's minimum).
+__global__ void fused_free_tiles_kernel(const SessDev* __restrict__ tab) {
+  const SessDev& S = tab[blockIdx.z];
+  if (!S.ftile || S.vol.t.band || *S.rgb_flag) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= S.rb_tx * S.rb_ty) return;
+  const DSensor& s = S.ls[0];
+  const DTsdf& t = S.vol.t;
+  const int tx = i % S.rb_tx, ty = i / S.rb_tx;
+  const int x0 = tx * kRbTile, y0 = ty * kRbTile;
+  const int x1 = min(x0 + kRbTile, s.cols), y1 = min(y0 + kRbTile, s.rows);
+  float mn = 3.0e38f;
+  bool ok = true;
+  for (int y = y0; y < y1; ++y)
+    for (int x = x0; x < x1; ++x) {
+      const float d = S.raw[y * s.cols + x];
+      if (!(d >= t.dmin && d <= t.dmax)) ok = false;
+      else mn = fminf(mn, S.sdist[y * s.cols + x] - t.trunc);
+    }
+  const unsigned v = __float_as_uint(ok ? fmaxf(mn, 0.0f) : 0.0f);
+  S.ftile[i] = v;
+  const int cx = (S.rb_tx + kRbCoarse - 1) / kRbCoarse;
+  atomicMin(S.ftile + S.rb_tx * S.rb_ty + (ty / kRbCoarse) * cx + tx / kRbCoarse, v);
+}
+
 __global__ void fused_bilateral_kernel(const SessDev* __restrict__ tab) {
   extern __shared__ float tile[];
   const SessDev& S = tab[blockIdx.z];
@@ -365,6 +391,7 @@ void launch_copy_f(const float* src, float* dst, size_t n, cudaStream_t st) {
 // ---- fused stages
 void fused_ingest(const SessDev* tab, const BatchShape& b, cudaStream_t st) {
   fused_ingest_kernel<<<dim3(nblk(b.max_npx, 256), 1, b.n), 256, 0, st>>>(tab);
+  fused_free_tiles_kernel<<<dim3(nblk(b.max_rb_tiles, 128), 1, b.n), 128, 0, st>>>(tab);
 }
 
 void fused_bilateral(const SessDev* tab, const BatchShape& b, cudaStream_t st) {

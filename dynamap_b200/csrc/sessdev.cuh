@@ -24,6 +24,17 @@ inline __host__ __device__ int ray_bounds_words(int tiles_x, int tiles_y) {
   return 2 * tiles_x * tiles_y + 2 * cx * cy;
 }
 
+// The visible list's session index carries this bit for free-space blocks
+// (every voxel takes the free-space update; see fused_visible_kernel).
+constexpr int kVisFree = 1 << 30;
+// Free-space tile map of a depth-only frame: per fine 8x8-pixel tile, then
+// per coarse tile, the least (sdist - truncation) over its pixels as float
+// bits, 0 where a pixel's depth is outside the sensor range (negative
+// values count as 0).
+inline __host__ __device__ int free_tile_words(int tiles_x, int tiles_y) {
+  return ray_bounds_words(tiles_x, tiles_y) / 2;
+}
+
 struct SessDev {
   DSensor ls[kLevels];  // level sensors (scale 1, 2, 4, 8)
   int nlev;             // levels in use
@@ -51,6 +62,7 @@ struct SessDev {
   float* tint[kLevels];
   float* ray;
   uint8_t* trgb;
+  unsigned* ftile;      // free-space tile map, free_tile_words(rb_tx, rb_ty) words
   unsigned* rbound;     // ray depth bounds (float bits), ray_bounds_words(rb_tx,
   int rb_tx, rb_ty;     // rb_ty) words; rb_tx x rb_ty fine tiles
   const BilateralTable* btab;  // device copy

@@ -331,6 +331,7 @@ void fill_sessdev(dyn_session* s) {
   d.ray = s->d_ray;
   d.trgb = s->d_trgb;
   d.rbound = s->d_rbound;
+  d.ftile = s->d_ftile;
   d.rb_tx = s->rb_tx;
   d.rb_ty = s->rb_ty;
   d.btab = s->d_btab;
@@ -594,8 +595,10 @@ size_t session_bytes(const dyn_tsdf_params& t, const dyn_sensor& s, int precisio
   if (precision == DYN_PRECISION_MIXED)
     b += (sizeof(int) + 1) * (size_t)t.num_blocks;  // free-space summaries
   b += n * (2 + 3 + 4 + 4 + 4 + 3);  // inputs, raw, filtered, ray depth, target rgb
-  if (precision == DYN_PRECISION_MIXED_BAND)
-    b += 4 * (size_t)((s.rows + 7) / 8) * ((s.cols + 7) / 8) + 256;  // ray-start bound
+  {  // ray depth bounds and the free-space tile map
+    const int tx = ((int)s.cols + 7) / 8, ty = ((int)s.rows + 7) / 8;
+    b += 4 * (size_t)(ray_bounds_words(tx, ty) + free_tile_words(tx, ty)) + 512;
+  }
   b += 2 * n * (4 + 16 + 16 + 4) * 4 / 3;  // source + target pyramids
   b += icp_frame_scratch_bytes(n) + sizeof(SessDev) + sizeof(BilateralTable) + sizeof(ResultBlock) +
        8192;
@@ -716,6 +719,7 @@ dyn_status alloc_device_buffers(dyn_session* s) {
   s->rb_tx = ((int)s->sensor.cols + 7) / 8;
   s->rb_ty = ((int)s->sensor.rows + 7) / 8;
   DYN_TRY(s->dalloc(&s->d_rbound, sizeof(unsigned) * (size_t)ray_bounds_words(s->rb_tx, s->rb_ty)));
+  DYN_TRY(s->dalloc(&s->d_ftile, sizeof(unsigned) * (size_t)free_tile_words(s->rb_tx, s->rb_ty)));
   DYN_TRY(s->dalloc(&s->d_gcount, sizeof(int)));
   DYN_TRY(s->dalloc(&s->d_rgb_flag, sizeof(int)));
   DYN_TRY(s->dalloc(&s->d_res, sizeof(ResultBlock)));

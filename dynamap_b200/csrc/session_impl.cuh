@@ -148,6 +148,7 @@ struct dyn_session {
   int* d_rgb_flag = nullptr;   // nonzero: the current frame carries RGB
   int rgb_flag_host = -1;      // last value written (-1: unknown)
   unsigned* d_rbound = nullptr;  // ray depth bounds per 8x8 pixel tile (near, then far)
+  unsigned* d_ftile = nullptr;   // free-space tile map (depth-only frames)
   int rb_tx = 0, rb_ty = 0;
   int2* d_gvis = nullptr;      // visible list of the table of one
   int* d_gcount = nullptr;

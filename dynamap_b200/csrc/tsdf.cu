@@ -267,7 +267,7 @@ __device__ inline float ray_near(const DTsdf& t) { return t.bsm; }
 
 __device__ inline void bound_block(unsigned long long key, const DTsdf& t, const DSensor& s,
                                    const M4f& invT, unsigned* __restrict__ rb, int tiles_x,
-                                   int tiles_y) {
+                                   int tiles_y, bool near, bool far) {
   const float vs = t.vs;
   const float znear = ray_near(t);
   const float lo[3] = {((float)key_x(key) * 8.0f - 1.5f) * vs,
@@ -322,8 +322,9 @@ __device__ inline void bound_block(unsigned long long key, const DTsdf& t, const
   // rectangle spans more than 16 tiles (one close to the camera) goes to
   // the coarse level instead, so that no thread walks hundreds of tiles;
   // the coarse bounds of such blocks are loose only near the camera.
-  // Carving sessions keep the near bound at 0: their blocks start at the
-  // camera.
+  // Carving sessions' blocks start at the camera: their near bound comes
+  // from the blocks that hold observed non-saturated voxels (mixed form,
+  // fused_surface_bound_kernel) or stays 0 (FP32 form).
   const unsigned zb = __float_as_uint(fmaxf(zmin, 0.0f)), ze = __float_as_uint(zmax);
   RayBounds B = ray_bounds(rb, tiles_x, tiles_y);
   unsigned *nb = B.near8, *fb = B.far8;
@@ -339,13 +340,71 @@ __device__ inline void bound_block(unsigned long long key, const DTsdf& t, const
   }
   for (int ty = y0; ty <= y1; ++ty)
     for (int tx = x0; tx <= x1; ++tx) {
-      if (t.band) atomicMin(nb + ty * tw + tx, zb);
-      atomicMax(fb + ty * tw + tx, ze);
+      if (near) atomicMin(nb + ty * tw + tx, zb);
+      if (far) atomicMax(fb + ty * tw + tx, ze);
     }
 }
 
+// Free-space blocks of a depth-only frame.  A voxel whose point is nearer
+// than (sdist - truncation) of its pixel takes IntegrateScanKernel's
+// free-space branch (sdf = truncation).  A visible block is a free-space
+// block when that holds for every voxel: the block's voxel points (the box
+// of corners origin .. origin + 7 voxels) lie in front of the camera and
+// project inside the image (a pixel of margin around the corners'
+// projections), and the farthest corner (with 1e-5 relative + 1e-5 m of
+// margin) is nearer than the free-space tile map's least (sdist -
+// truncation) over the tiles that rectangle touches -- which is 0 wherever
+// a pixel's depth is outside the sensor range.  The per-voxel arithmetic
+// rounds far below these margins, so its test takes the free-space branch
+// for every voxel of such a block, and integration skips the per-voxel
+// projection (colours are zero: no RGB).  Blocks whose rectangle covers
+// more than 16 coarse tiles (close to the camera) take the per-voxel test.
+__device__ inline bool free_space_block(unsigned long long key, const DTsdf& t, const DSensor& s,
+                                        const M4f& invT, const unsigned* __restrict__ ftile,
+                                        int tiles_x, int tiles_y) {
+  const float vs = t.vs, e = 7.0f * vs;
+  const float ox = (float)key_x(key) * vs * (float)kBlockSize,
+              oy = (float)key_y(key) * vs * (float)kBlockSize,
+              oz = (float)key_z(key) * vs * (float)kBlockSize;
+  float u0 = 3.0e38f, u1 = -3.0e38f, v0 = 3.0e38f, v1 = -3.0e38f, dm = 0.0f;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const F3 c = xform(invT, f3(ox + ((k & 1) ? e : 0.0f), oy + ((k & 2) ? e : 0.0f),
+                                oz + ((k & 4) ? e : 0.0f)));
+    if (!(c.z > 0.01f)) return false;
+    const float u = s.fx * c.x / c.z + s.cx, w = s.fy * c.y / c.z + s.cy;
+    u0 = fminf(u0, u);
+    u1 = fmaxf(u1, u);
+    v0 = fminf(v0, w);
+    v1 = fmaxf(v1, w);
+    dm = fmaxf(dm, norm3(c));
+  }
+  if (!(u0 >= 1.0f && v0 >= 1.0f && u1 <= (float)(s.cols - 2) && v1 <= (float)(s.rows - 2)))
+    return false;
+  const int x0 = (int)floorf(u0) - 1, x1 = (int)ceilf(u1) + 1;
+  const int y0 = (int)floorf(v0) - 1, y1 = (int)ceilf(v1) + 1;
+  if (x0 < 0 || y0 < 0 || x1 >= s.cols || y1 >= s.rows) return false;
+  int tx0 = x0 / kRbTile, tx1 = x1 / kRbTile, ty0 = y0 / kRbTile, ty1 = y1 / kRbTile;
+  const unsigned* m = ftile;
+  int tw = tiles_x;
+  if ((tx1 - tx0 + 1) * (ty1 - ty0 + 1) > 16) {
+    m = ftile + tiles_x * tiles_y;
+    tw = (tiles_x + kRbCoarse - 1) / kRbCoarse;
+    tx0 /= kRbCoarse;
+    tx1 /= kRbCoarse;
+    ty0 /= kRbCoarse;
+    ty1 /= kRbCoarse;
+    if ((tx1 - tx0 + 1) * (ty1 - ty0 + 1) > 16) return false;
+  }
+  unsigned mn = 0xffffffffu;
+  for (int ty = ty0; ty <= ty1; ++ty)
+    for (int tx = tx0; tx <= tx1; ++tx) mn = min(mn, __ldg(m + ty * tw + tx));
+  return dm * (1.0f + 1e-5f) + 1e-5f < __uint_as_float(mn);
+}
+
 // Every session's visible blocks appended to one batch-wide list of
-// (session, heap index), so integration balances across sessions.
+// (session, heap index), so integration balances across sessions; the
+// session index carries kVisFree for free-space blocks.
 __global__ void fused_visible_kernel(const SessDev* __restrict__ tab, int2* __restrict__ gvis,
                                      int* __restrict__ gcount) {
   const SessDev& S = tab[blockIdx.z];
@@ -363,8 +422,11 @@ __global__ void fused_visible_kernel(const SessDev* __restrict__ tab, int2* __re
       const unsigned long long key = v.block_keys[i];
       vis = block_visible(key, v.t, S.ls[0], invT);
       // every allocated block (visible or not) enters the ray-start bound
-      if (S.rbound) bound_block(key, v.t, S.ls[0], invT, S.rbound, S.rb_tx, S.rb_ty);
+      if (S.rbound) bound_block(key, v.t, S.ls[0], invT, S.rbound, S.rb_tx, S.rb_ty, v.t.band, true);
     }
+    bool fr = false;
+    if (vis && S.ftile && !v.t.band && !*S.rgb_flag)
+      fr = free_space_block(v.block_keys[i], v.t, S.ls[0], invT, S.ftile, S.rb_tx, S.rb_ty);
     unsigned m = __ballot_sync(0xffffffffu, vis);
     int off = 0;
     if (lane == 0 && m) {
@@ -372,8 +434,32 @@ __global__ void fused_visible_kernel(const SessDev* __restrict__ tab, int2* __re
       off = atomicAdd(gcount, __popc(m));
     }
     off = __shfl_sync(0xffffffffu, off, 0);
-    if (vis) gvis[off + __popc(m & ((1u << lane) - 1))] = make_int2((int)blockIdx.z, i);
+    if (vis)
+      gvis[off + __popc(m & ((1u << lane) - 1))] =
+          make_int2((int)blockIdx.z | (fr ? kVisFree : 0), i);
   }
+}
+
+// The near ray bound of mixed carving sessions, after integration.  A
+// sample whose cell and centre voxel lie only in blocks without observed
+// non-saturated voxels (unallocated, unobserved or saturated: f16 value 1)
+// steps the truncation distance, or the interpolation of saturated values
+// -- the truncation up to the rounding of the weights, never ending the
+// march (free_ok) -- as the free-cell shortcut does; so the near bound of a
+// tile is the nearest depth of the boxes of the blocks that hold such
+// voxels (VolumeDev::nonsat > 0), widened as bound_block widens every box.
+__global__ void fused_surface_bound_kernel(const SessDev* __restrict__ tab) {
+  const SessDev& S = tab[blockIdx.z];
+  const VolumeDev& v = S.vol;
+  if (!S.rbound || !v.nonsat || !v.free_ok || v.t.band) return;
+  __shared__ M4f invT;
+  if (threadIdx.x < 16) invT.m[threadIdx.x] = S.pose->invf[threadIdx.x];
+  __syncthreads();
+  int n = v.cnt->nalloc;
+  if (n > v.t.num_blocks) n = v.t.num_blocks;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    if (v.nonsat[i] > 0)
+      bound_block(v.block_keys[i], v.t, S.ls[0], invT, S.rbound, S.rb_tx, S.rb_ty, true, false);
 }
 
 // ------------------------------------------------------------ integration
@@ -394,13 +480,14 @@ __device__ inline float norm3_fast(F3 v) {
   return q > 0.0f ? q * rsqrtf(q) : 0.0f;
 }
 
-// Returns the change of the block's count of observed, non-saturated voxels
-// (-1, 0 or +1) that this voxel's update makes (0 when it is not updated).
-template <bool FP16, bool FAST>
-__device__ inline int integrate_voxel(const VolumeDev& v, const float* __restrict__ depth,
-                                       const float* __restrict__ sdist,
-                                       const uint8_t* __restrict__ rgb, const DSensor& s,
-                                       const M4f& invT, int ptr, int lin) {
+// Whether this frame updates voxel 'lin' of block 'ptr', and with which
+// sdf and colour (the per-voxel test of IntegrateScanKernel).
+template <bool FAST>
+__device__ inline bool observe_voxel(const VolumeDev& v, const float* __restrict__ depth,
+                                     const float* __restrict__ sdist,
+                                     const uint8_t* __restrict__ rgb, const DSensor& s,
+                                     const M4f& invT, int ptr, int lin, float& sdf, uint8_t& c0,
+                                     uint8_t& c1, uint8_t& c2) {
   const DTsdf& t = v.t;
   const float vs = t.vs;
   const int bx = lin >> 6, by = (lin >> 3) & 7, bz = lin & 7;
@@ -417,42 +504,51 @@ __device__ inline int integrate_voxel(const VolumeDev& v, const float* __restric
   float sd, vd, d;
   if (FAST) {
     vp = xform_fma(invT, vp);
-    if (!(vp.z > 0.0f)) return 0;
+    if (!(vp.z > 0.0f)) return false;
     const float rz = __fdividef(1.0f, vp.z);
     const float xf = __fmaf_rn(s.fx * vp.x, rz, s.cx), yf = __fmaf_rn(s.fy * vp.y, rz, s.cy);
-    if (!(fabsf(xf) < 2e9f) || !(fabsf(yf) < 2e9f)) return 0;
+    if (!(fabsf(xf) < 2e9f) || !(fabsf(yf) < 2e9f)) return false;
     px = (int)roundf(xf);
     py = (int)roundf(yf);
-    if (!(px >= 0 && py >= 0 && px < s.cols && py < s.rows)) return 0;
+    if (!(px >= 0 && py >= 0 && px < s.cols && py < s.rows)) return false;
     d = __ldg(depth + py * s.cols + px);
-    if (d < t.dmin) return 0;
-    if (d > t.dmax) return 0;
+    if (d < t.dmin) return false;
+    if (d > t.dmax) return false;
     const F3 p3 = f3(__fdividef(((float)px - s.cx) * d, s.fx),
                      __fdividef(((float)py - s.cy) * d, s.fy), d);
     sd = norm3_fast(p3);
     vd = norm3_fast(vp);
   } else {
     vp = xform(invT, vp);
-    if (!project(vp, s, &px, &py)) return 0;
-    if (!(px >= 0 && py >= 0 && px < s.cols && py < s.rows)) return 0;
+    if (!project(vp, s, &px, &py)) return false;
+    if (!(px >= 0 && py >= 0 && px < s.cols && py < s.rows)) return false;
     d = __ldg(depth + py * s.cols + px);
-    if (d < t.dmin) return 0;
-    if (d > t.dmax) return 0;
+    if (d < t.dmin) return false;
+    if (d > t.dmax) return false;
     sd = __ldg(sdist + py * s.cols + px);  // norm3(point3d_uv(px, py, d, s))
     vd = norm3(vp);
   }
   const int idx = py * s.cols + px;
-  float sdf;
   if (vd > sd - t.trunc && vd < sd + t.trunc && d < t.dmax) sdf = sd - vd;
   else if (vd < sd - t.trunc) sdf = t.trunc;
-  else return 0;
-  uint8_t c0 = 0, c1 = 0, c2 = 0;
+  else return false;
+  c0 = c1 = c2 = 0;
   if (rgb) {
     c0 = __ldg(rgb + 3 * (size_t)idx);
     c1 = __ldg(rgb + 3 * (size_t)idx + 1);
     c2 = __ldg(rgb + 3 * (size_t)idx + 2);
   }
-  const size_t vi = (size_t)ptr * kBlockVox + lin;
+  return true;
+}
+
+// Voxel::mergeVoxel (geom_Types.h:79-103) of one observation into voxel vi.
+// Returns the change of the block's count of observed, non-saturated voxels
+// (-1, 0 or +1) that the update makes (FP16 form; the FP32 form keeps no
+// free-space summaries and returns 0).
+template <bool FP16>
+__device__ inline int merge_voxel(const VolumeDev& v, size_t vi, float sdf, bool has_rgb,
+                                  uint8_t c0, uint8_t c1, uint8_t c2) {
+  const DTsdf& t = v.t;
   if (FP16) {
     // mixed form: the same FP32 merge, stored as f16 sdf / truncation
     // (|value| <= 1, free space exactly 1) and a u16 weight
@@ -487,7 +583,7 @@ __device__ inline int integrate_voxel(const VolumeDev& v, const float* __restric
   float nsdf = (osdf * fw + sdf * 1.0f) / (fw + 1.0f);
   // colour merge (geom_Types.h:87-91); a zero colour merged with a zero
   // colour stays exactly zero, so depth-only frames skip the divisions
-  if (rgb || (raw.x & 0x00ffffffu)) {
+  if (has_rgb || (raw.x & 0x00ffffffu)) {
     r0 = (uint8_t)(((float)r0 * fw + (float)c0 * 1.0f) / (fw + 1.0f));
     r1 = (uint8_t)(((float)r1 * fw + (float)c1 * 1.0f) / (fw + 1.0f));
     r2 = (uint8_t)(((float)r2 * fw + (float)c2 * 1.0f) / (fw + 1.0f));
@@ -498,7 +594,21 @@ __device__ inline int integrate_voxel(const VolumeDev& v, const float* __restric
   out.x = (unsigned)r0 | ((unsigned)r1 << 8) | ((unsigned)r2 << 16) | ((unsigned)nw << 24);
   out.y = __float_as_uint(nsdf);
   *reinterpret_cast<uint2*>(vox) = out;
-  return 0;  // the FP32 form keeps no free-space summaries
+  return 0;
+}
+
+// IntegrateScanKernel voxel loop (tsdf.cu:301-341) + Voxel::mergeVoxel for
+// voxel 'lin' of block 'ptr': the nonsat change (merge_voxel), 0 when the
+// voxel is not updated.
+template <bool FP16, bool FAST>
+__device__ inline int integrate_voxel(const VolumeDev& v, const float* __restrict__ depth,
+                                       const float* __restrict__ sdist,
+                                       const uint8_t* __restrict__ rgb, const DSensor& s,
+                                       const M4f& invT, int ptr, int lin) {
+  float sdf;
+  uint8_t c0, c1, c2;
+  if (!observe_voxel<FAST>(v, depth, sdist, rgb, s, invT, ptr, lin, sdf, c0, c1, c2)) return 0;
+  return merge_voxel<FP16>(v, (size_t)ptr * kBlockVox + lin, sdf, rgb != nullptr, c0, c1, c2);
 }
 
 // the batch-wide visible list: each item (session, block) by one CTA
@@ -511,7 +621,8 @@ __global__ void __launch_bounds__(kBlockVox)
   if (threadIdx.x == 0) cur_s = -1;
   __syncthreads();
   for (int b = blockIdx.x; b < n; b += gridDim.x) {
-    const int2 item = gvis[b];
+    const int2 entry = gvis[b];
+    const int2 item = make_int2(entry.x & ~kVisFree, entry.y);
     if (item.x != cur_s) {  // uniform across the CTA
       __syncthreads();
       if (threadIdx.x < 16) invT.m[threadIdx.x] = tab[item.x].pose->invf[threadIdx.x];
@@ -521,7 +632,11 @@ __global__ void __launch_bounds__(kBlockVox)
     const SessDev& S = tab[item.x];
     const uint8_t* rgb = *S.rgb_flag ? S.rgb : nullptr;
     int d;
-    if (!S.vol.fp16)
+    if (entry.x & kVisFree) {  // a free-space block: every voxel's sdf is the truncation
+      const size_t vi = (size_t)item.y * kBlockVox + threadIdx.x;
+      d = S.vol.fp16 ? merge_voxel<true>(S.vol, vi, S.vol.t.trunc, false, 0, 0, 0)
+                     : merge_voxel<false>(S.vol, vi, S.vol.t.trunc, false, 0, 0, 0);
+    } else if (!S.vol.fp16)
       d = integrate_voxel<false, false>(S.vol, S.raw, S.sdist, rgb, S.ls[0], invT, item.y,
                                         threadIdx.x);
     else if (S.vol.t.band)
@@ -555,7 +670,8 @@ __global__ void fused_free_cells_kernel(const SessDev* __restrict__ tab,
                                         const int* __restrict__ gcount) {
   const int n = *gcount;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const int2 item = gvis[i];
+    const int2 entry = gvis[i];
+    const int2 item = make_int2(entry.x & ~kVisFree, entry.y);
     const VolumeDev& v = tab[item.x].vol;
     if (!v.freecell) continue;
     const unsigned long long key = v.block_keys[item.y];
@@ -1062,7 +1178,8 @@ __global__ void fused_reset_counters_kernel(const SessDev* __restrict__ tab,
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (S.rbound) {
     // near: no block (3.4e38), or 0 where unused; far: no block (0)
-    const unsigned nb = S.vol.t.band ? 0x7f7f7f7fu : 0u;
+    const bool near_used = S.vol.t.band || (S.vol.nonsat && S.vol.free_ok);
+    const unsigned nb = near_used ? 0x7f7f7f7fu : 0u;
     const RayBounds B = ray_bounds(S.rbound, S.rb_tx, S.rb_ty);
     if (i < S.rb_tx * S.rb_ty) {
       B.near8[i] = nb;
@@ -1073,6 +1190,8 @@ __global__ void fused_reset_counters_kernel(const SessDev* __restrict__ tab,
       B.far64[i] = 0u;
     }
   }
+  if (S.ftile && i < ((S.rb_tx + kRbCoarse - 1) / kRbCoarse) * ((S.rb_ty + kRbCoarse - 1) / kRbCoarse))
+    S.ftile[S.rb_tx * S.rb_ty + i] = 0x7f7f7f7fu;  // coarse free-space tiles: min of none
   if (i != 0) return;
   if (blockIdx.z == 0) *gcount = 0;
   Counters* c = S.vol.cnt;
@@ -1177,6 +1296,13 @@ void fused_integrate(const SessDev* tab, const BatchShape& b, cudaStream_t st) {
 
 void fused_free_cells(const SessDev* tab, const BatchShape& b, cudaStream_t st) {
   fused_free_cells_kernel<<<148 * 2, 256, 0, st>>>(tab, b.gvis, b.gcount);
+  if (b.fp16_mask & 2) {  // mixed sessions: the near ray bound from their summaries
+    int cap = 592 / b.n;
+    if (cap < 8) cap = 8;
+    int g = nblk(b.max_blocks, 256);
+    if (g > cap) g = cap;
+    fused_surface_bound_kernel<<<dim3(g, 1, b.n), 256, 0, st>>>(tab);
+  }
 }
 
 void fused_raycast(const SessDev* tab, const BatchShape& b, cudaStream_t st) {
