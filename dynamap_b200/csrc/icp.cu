@@ -353,8 +353,12 @@ __host__ __device__ constexpr int tri(int i, int j) { return i * (i + 1) / 2 + j
 // D[j] = A[j][j] - sum_k L[j][k]^2 D[k] and L[i][j] = (A[i][j] - sum_k
 // L[i][k] L[j][k] D[k]) / D[j], each sum in increasing k; then forward
 // substitution, division by D, back substitution.  L overwrites the strict
-// lower triangle of a, D its diagonal.  Returns false on a zero pivot.
+// lower triangle of a, D its diagonal.  Each pivot's reciprocal is taken
+// once and multiplies (one FP64 division per column instead of one per
+// entry: the one-thread solve sits between every two ICP iterations).
+// Returns false on a zero pivot.
 __device__ __forceinline__ bool ldlt6(double (&a)[21], const double (&b)[6], double (&x)[6]) {
+  double rd[6];  // 1 / D[j]
   // triangular bounds are written as guards on fixed-length loops, so that
   // every loop has a constant trip count and unrolls completely
 #pragma unroll
@@ -365,6 +369,7 @@ __device__ __forceinline__ bool ldlt6(double (&a)[21], const double (&b)[6], dou
       if (k < j) s -= a[tri(j, k)] * a[tri(j, k)] * a[tri(k, k)];
     a[tri(j, j)] = s;
     if (!(fabs(s) > 0.0)) return false;
+    rd[j] = 1.0 / s;
 #pragma unroll
     for (int i = 0; i < 6; ++i) {
       if (i <= j) continue;
@@ -372,7 +377,7 @@ __device__ __forceinline__ bool ldlt6(double (&a)[21], const double (&b)[6], dou
 #pragma unroll
       for (int k = 0; k < 6; ++k)
         if (k < j) t -= a[tri(i, k)] * a[tri(j, k)] * a[tri(k, k)];
-      a[tri(i, j)] = t / s;
+      a[tri(i, j)] = t * rd[j];
     }
   }
   double y[6];
@@ -385,7 +390,7 @@ __device__ __forceinline__ bool ldlt6(double (&a)[21], const double (&b)[6], dou
     y[i] = t;
   }
 #pragma unroll
-  for (int i = 0; i < 6; ++i) y[i] /= a[tri(i, i)];
+  for (int i = 0; i < 6; ++i) y[i] *= rd[i];
 #pragma unroll
   for (int i = 5; i >= 0; --i) {
     double t = y[i];
@@ -497,8 +502,16 @@ __device__ void inverse4f(const float* e, float* out) {
 // row-major order, as over the full symmetric matrix.  Updates inc/prev
 // (the solver state's, in global or shared memory); returns true when
 // converged.
-__device__ __forceinline__ double sym_at(const double (&a)[21], int i, int j) {
-  return i >= j ? a[tri(i, j)] : a[tri(j, i)];
+__device__ __forceinline__ double max21(const double (&a)[21]) {
+  double m[11];
+#pragma unroll
+  for (int k = 0; k < 10; ++k) m[k] = fmax(a[2 * k], a[2 * k + 1]);
+  m[10] = a[20];
+#pragma unroll
+  for (int w = 1; w < 11; w *= 2)
+#pragma unroll
+    for (int k = 0; k + w < 11; k += 2 * w) m[k] = fmax(m[k], m[k + w]);
+  return m[0];
 }
 __device__ bool gn_update(const double* acc, const IcpParams& P, int it, double* st_inc,
                           double* st_prev) {
@@ -512,17 +525,15 @@ __device__ bool gn_update(const double* acc, const IcpParams& P, int it, double*
   }
 #pragma unroll
   for (int k = 0; k < 6; ++k) b[k] = acc[21 + k];
-  double mx = a[0];
-#pragma unroll
-  for (int k = 1; k < 36; ++k) mx = fmax(mx, sym_at(a, k / 6, k % 6));
+  // the maxima over all 36 entries are the maxima over the 21 stored ones
+  // (fmax ignores NaNs in any order), taken as a tree
+  const double mx = max21(a);
   const double scaling = 1.0 / mx;
 #pragma unroll
   for (int k = 0; k < 6; ++k) b[k] *= scaling;
 #pragma unroll
   for (int k = 0; k < 21; ++k) a[k] *= scaling;
-  double mx2 = a[0];
-#pragma unroll
-  for (int k = 1; k < 36; ++k) mx2 = fmax(mx2, sym_at(a, k / 6, k % 6));
+  const double mx2 = max21(a);
   const double alpha = (double)P.reg * mx2;
 #pragma unroll
   for (int k = 0; k < 6; ++k) a[tri(k, k)] += alpha / (double)it;
@@ -557,7 +568,7 @@ inline __host__ __device__ int icp_grid(int n) {
 }
 
 // The partial sums of tile 'tile' of level L into row[0..28]: each thread
-// accumulates its four pixels (tile * kIcpTile + threadIdx.x + m * 256) in
+// accumulates its pixels (tile * tile_px + threadIdx.x + m * 256) in
 // FP32, the block adds them in FP64 in a fixed order.  Every thread of the
 // block calls it; 'red' is the block's shared scratch.
 template <bool KAHAN>
@@ -570,11 +581,14 @@ __device__ inline void tile_partial(const IcpLevel& L, const IcpParams& P, const
     a.d[k] = 0.0;
   }
   const int n = L.s.rows * L.s.cols;
-  const int base = tile * kIcpTile + (int)threadIdx.x;
-  static_assert(kIcpTile / kIcpThreads % 2 == 0, "pixels go in pairs");
-#pragma unroll
-  for (int m = 0; m < kIcpTile / kIcpThreads; m += 2)
-    pixel_pair<KAHAN>(L, P, T, base + m * kIcpThreads, base + (m + 1) * kIcpThreads, n, a);
+  const int tpx = icp_tile_px(n);
+  const int base = tile * tpx + (int)threadIdx.x;
+  if (tpx == kIcpThreads) {
+    if (base < n) pixel_terms<KAHAN>(L, P, T, base, a);
+  } else {
+    for (int m = 0; m < tpx / kIcpThreads; m += 2)
+      pixel_pair<KAHAN>(L, P, T, base + m * kIcpThreads, base + (m + 1) * kIcpThreads, n, a);
+  }
   block_reduce<KAHAN>(a, red);
   if (threadIdx.x < kIcpVals) row[threadIdx.x] = red[threadIdx.x];
   __syncthreads();  // red is reused by the next tile
@@ -703,9 +717,9 @@ __device__ inline unsigned long long global_ns() {
 // grid) whose barrier words (kIcpBarWords, zero at launch) are 'bar'.
 // Arrivals and releases are spread over kIcpBarSpread counters and flags,
 // each on its own 128-byte line: block b adds one to counter
-// b % kIcpBarSpread; block 0 alone polls the counters until each holds k
-// times its blocks, then writes k to every release flag; block b polls flag
-// b % kIcpBarSpread.  So no line takes
+// b % kIcpBarSpread; block 0 alone polls the counters (one thread each)
+// until each holds k times its blocks, then writes k to every release
+// flag; block b polls flag b % kIcpBarSpread.  So no line takes
 // more than a few dozen blocks' polls beside the arrivals it counts.  Every
 // wait is bounded: after kBarrierWaitNs (or once the abort word is raised)
 // the block gives up, raises the abort word and returns false.
@@ -719,37 +733,47 @@ __device__ inline int* bar_abort(unsigned* bar) {
 }
 __device__ inline bool grid_barrier(unsigned* bar, unsigned k, unsigned nb) {
   __shared__ int ok;
+  const unsigned me = blockIdx.x;
+  int* abort = bar_abort(bar);
   __syncthreads();
   if (threadIdx.x == 0) {
-    const unsigned me = blockIdx.x;
-    int* abort = bar_abort(bar);
     __threadfence();  // this block's partial sums before its arrival
     atomicAdd(bar_counter(bar, (int)(me % kIcpBarSpread)), 1u);
-    const unsigned long long t0 = global_ns();
+  }
+  if (me == 0) {  // block 0: threads 0 .. kIcpBarSpread-1 poll one counter each
     int good = 1;
-    if (me == 0) {
-      for (int i = 0; i < kIcpBarSpread && good; ++i) {
-        const unsigned want = k * ((nb + kIcpBarSpread - 1 - (unsigned)i) / kIcpBarSpread);
-        while (*(volatile unsigned*)bar_counter(bar, i) < want) {
-          if (*(volatile int*)abort || global_ns() - t0 > kBarrierWaitNs) {
-            good = 0;
-            break;
-          }
-          __nanosleep(32);
-        }
-      }
-      __threadfence();  // the arrivals' partial sums before the release
-      if (good)
-        for (int i = 0; i < kIcpBarSpread; ++i) *(volatile unsigned*)bar_flag(bar, i) = k;
-    } else {
-      volatile unsigned* flag = bar_flag(bar, (int)(me % kIcpBarSpread));
-      while (*flag < k) {
+    if (threadIdx.x < kIcpBarSpread) {
+      const unsigned want =
+          k * ((nb + kIcpBarSpread - 1 - threadIdx.x) / kIcpBarSpread);
+      volatile unsigned* c = bar_counter(bar, (int)threadIdx.x);
+      const unsigned long long t0 = global_ns();
+      while (*c < want) {
         if (*(volatile int*)abort || global_ns() - t0 > kBarrierWaitNs) {
           good = 0;
           break;
         }
-        __nanosleep(64);
+        __nanosleep(32);
       }
+      __threadfence();  // the arrivals' partial sums before the release
+    }
+    good = __syncthreads_and(good);
+    if (threadIdx.x == 0) {
+      if (good)
+        for (int i = 0; i < kIcpBarSpread; ++i) *(volatile unsigned*)bar_flag(bar, i) = k;
+      else
+        atomicExch(abort, 1);
+      ok = good;
+    }
+  } else if (threadIdx.x == 0) {
+    volatile unsigned* flag = bar_flag(bar, (int)(me % kIcpBarSpread));
+    const unsigned long long t0 = global_ns();
+    int good = 1;
+    while (*flag < k) {
+      if (*(volatile int*)abort || global_ns() - t0 > kBarrierWaitNs) {
+        good = 0;
+        break;
+      }
+      __nanosleep(64);
     }
     if (!good) atomicExch(abort, 1);
     __threadfence();  // the other blocks' partial sums after the release

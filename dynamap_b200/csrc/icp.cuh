@@ -51,13 +51,20 @@ constexpr int kIcpThreads = 256;
 constexpr int kIcpMaxBlocks = 148 * 8;
 constexpr int kIcpVals = 29;
 // The per-frame ICP sums its normal equations per pixel tile: tile j holds
-// pixels [j * kIcpTile, (j + 1) * kIcpTile) of a level, four per thread,
-// and its partial sums are the same whichever block computes them; the
-// level's total adds the tiles in index order.  So the result does not
-// depend on how many blocks work on a level, nor on the sessions that share
-// the launch.
-constexpr int kIcpTile = 4 * kIcpThreads;
-inline __host__ __device__ int icp_tiles(int npx) { return (npx + kIcpTile - 1) / kIcpTile; }
+// pixels [j * t, (j + 1) * t) of a level of n pixels, t = icp_tile_px(n)
+// (256, 512 or 1024 pixels: one, two or four per thread, smaller tiles on
+// the coarse levels so that more blocks share their short work), and its
+// partial sums are the same whichever block computes them; the level's
+// total adds the tiles in index order.  So the result does not depend on
+// how many blocks work on a level, nor on the sessions that share the
+// launch.  A level never has more tiles than the session's finest one.
+inline __host__ __device__ int icp_tile_px(int npx) {
+  return npx <= 8192 ? kIcpThreads : (npx <= 65536 ? 2 * kIcpThreads : 4 * kIcpThreads);
+}
+inline __host__ __device__ int icp_tiles(int npx) {
+  const int t = icp_tile_px(npx);
+  return (npx + t - 1) / t;
+}
 
 // Scratch a reduction needs: per-block partial sums (kIcpMaxBlocks*29 doubles).
 size_t icp_scratch_bytes();
