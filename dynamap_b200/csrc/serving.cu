@@ -496,6 +496,7 @@ struct dyn_server {
   int device = 0;
   size_t budget = 0, used = 0;
   char* d_arena = nullptr;  // the budget, reserved at creation
+  size_t sessions_off = 0;  // the sessions' part of it (after the visible list)
   Arena arena;
   int capacity = 0;
   std::vector<ServerSlot> slots;
@@ -505,10 +506,14 @@ struct dyn_server {
   int64_t steps = 0;
   int64_t steps_done = 0;  // steps known to have completed (in order)
   int64_t frames = 0;
-  int2* d_gvis = nullptr;
+  int2* d_gvis = nullptr;  // the start of the budget: one entry per block admissible
   int* d_gcount = nullptr;
   unsigned* d_icp_bar = nullptr;  // the persistent ICP's barrier words
   int64_t gvis_cap = 0;
+  // streams and events lent to admitted sessions (created ahead of the
+  // serving loop: stream creation can block for tens of milliseconds while
+  // the device is busy)
+  std::vector<std::pair<cudaStream_t, cudaEvent_t>> pool;
   ResultBlock* d_res = nullptr;
   ResultBlock* h_res = nullptr;  // pinned, one entry per slot
   std::vector<dyn_session*> act;
@@ -525,6 +530,7 @@ void release(dyn_server* sv) {
   for (ServerSlot& sl : sv->slots)
     if (sl.s) {
       sl.s->owner_stream = nullptr;
+      sv->pool.emplace_back(sl.s->stream, sl.s->h2d_done);
       dyn_session_destroy(sl.s);
     }
   for (StepBuf& r : sv->ring) {
@@ -534,8 +540,11 @@ void release(dyn_server* sv) {
     if (r.h_map) cudaFreeHost(r.h_map);
     if (r.done) cudaEventDestroy(r.done);
   }
+  for (auto& pe : sv->pool) {
+    cudaStreamDestroy(pe.first);
+    cudaEventDestroy(pe.second);
+  }
   cudaFree(sv->d_arena);
-  cudaFree(sv->d_gvis);
   cudaFree(sv->d_gcount);
   cudaFree(sv->d_icp_bar);
   cudaFree(sv->d_res);
@@ -543,6 +552,32 @@ void release(dyn_server* sv) {
   if (sv->stream) cudaStreamDestroy(sv->stream);
   cudaSetDevice(prev);
   delete sv;
+}
+
+// Device bytes every admitted block costs at least (its voxels in the
+// smallest form, its heap key and its entry in the session's visible list),
+// which bounds the blocks of all admitted sessions by the budget.
+constexpr size_t kMinBlockBytes = 4 * kBlockVox + sizeof(unsigned long long) + sizeof(int2);
+// Pooled stream/event pairs made at creation (more are made on demand).
+constexpr int kServerStreamPool = 64;
+
+dyn_status pool_make(cudaStream_t* st, cudaEvent_t* ev) {
+  *st = nullptr;
+  *ev = nullptr;
+  if (cudaStreamCreateWithFlags(st, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(ev, cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    if (*st) cudaStreamDestroy(*st);
+    return DYN_ERR_CUDA;
+  }
+  return DYN_OK;
+}
+dyn_status pool_take(dyn_server* sv, cudaStream_t* st, cudaEvent_t* ev) {
+  if (sv->pool.empty()) return pool_make(st, ev);
+  *st = sv->pool.back().first;
+  *ev = sv->pool.back().second;
+  sv->pool.pop_back();
+  return DYN_OK;
 }
 
 dyn_status check_slot(dyn_server* sv, int32_t slot) {
@@ -577,7 +612,15 @@ dyn_status dyn_server_create(const dyn_server_params* p, dyn_server** out) {
     return DYN_ERR_CUDA;
   }
   sv->budget = (p->budget_bytes ? p->budget_bytes : free_b / 10 * 9) / 256 * 256;
-  bool ok = cudaMalloc(&sv->d_arena, sv->budget ? sv->budget : 256) == cudaSuccess &&
+  // the batch visible list comes first in the budget, sized for every block
+  // the rest of the budget can hold, so a step never has to grow it
+  sv->gvis_cap = (int64_t)(sv->budget / kMinBlockBytes) + 1;
+  sv->sessions_off = ((size_t)sv->gvis_cap * sizeof(int2) + 255) / 256 * 256;
+  if (sv->sessions_off >= sv->budget) {
+    delete sv;
+    return DYN_ERR_BUDGET_EXCEEDED;
+  }
+  bool ok = cudaMalloc(&sv->d_arena, sv->budget) == cudaSuccess &&
             cudaStreamCreateWithFlags(&sv->stream, cudaStreamNonBlocking) == cudaSuccess &&
             cudaMalloc(&sv->d_gcount, 256) == cudaSuccess &&
             cudaMalloc(&sv->d_icp_bar, kIcpBarWords * sizeof(unsigned)) == cudaSuccess &&
@@ -594,8 +637,19 @@ dyn_status dyn_server_create(const dyn_server_params* p, dyn_server** out) {
     release(sv);
     return DYN_ERR_OOM;
   }
+  sv->d_gvis = reinterpret_cast<int2*>(sv->d_arena);
+  for (int i = 0; i < std::min(cap, kServerStreamPool) && ok; ++i) {
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev = nullptr;
+    ok = pool_make(&st, &ev) == DYN_OK;
+    if (ok) sv->pool.emplace_back(st, ev);
+  }
+  if (!ok) {
+    release(sv);
+    return DYN_ERR_CUDA;
+  }
   std::memset(sv->h_res, 0, sizeof(ResultBlock) * (size_t)cap);
-  sv->arena.init(sv->d_arena, sv->budget);
+  sv->arena.init(sv->d_arena + sv->sessions_off, sv->budget - sv->sessions_off);
   *out = sv;
   return DYN_OK;
 }
@@ -624,18 +678,24 @@ dyn_status dyn_server_admit(dyn_server* sv, const dyn_tsdf_params* tsdf, const d
   // locked frames need none); initialisation enqueued on the session's
   // stream, which the server's stream waits for
   SessionMemory mem;
-  mem.region = sv->d_arena + off;
+  mem.region = sv->d_arena + sv->sessions_off + off;
   mem.region_size = bytes;
   mem.host_staging = false;
   mem.sync = false;
+  dyn_status r = pool_take(sv, &mem.stream, &mem.h2d_done);
+  if (r != DYN_OK) {
+    sv->arena.give(off, bytes);
+    return r;
+  }
   dyn_session* s = nullptr;
-  dyn_status r = create_session(tsdf, gn, bil, sensor, precision, sv->device, mem, &s);
+  r = create_session(tsdf, gn, bil, sensor, precision, sv->device, mem, &s);
   if (r == DYN_OK && pose0) r = set_pose_async(s, pose0);
   if (r == DYN_OK && (cudaEventRecord(s->h2d_done, s->stream) != cudaSuccess ||
                       cudaStreamWaitEvent(sv->stream, s->h2d_done, 0) != cudaSuccess))
     r = DYN_ERR_CUDA;
   if (r != DYN_OK) {
     if (s) dyn_session_destroy(s);
+    sv->pool.emplace_back(mem.stream, mem.h2d_done);
     sv->arena.give(off, bytes);
     return r;
   }
@@ -659,7 +719,9 @@ dyn_status dyn_server_release(dyn_server* sv, int32_t slot) {
   if (sl.last_step >= 0 && sl.last_step >= sv->steps - kServerRing)
     DYN_CUDA(cudaEventSynchronize(sv->ring[sl.last_ring].done));
   sl.s->owner_stream = nullptr;
+  const std::pair<cudaStream_t, cudaEvent_t> lent(sl.s->stream, sl.s->h2d_done);
   dyn_session_destroy(sl.s);  // its device buffers are the region: nothing freed
+  sv->pool.push_back(lent);   // (the destroy synchronised the stream)
   sv->arena.give(sl.offset, sl.bytes);
   sv->used -= sl.bytes;
   sl = ServerSlot();
@@ -710,17 +772,9 @@ dyn_status dyn_server_step(dyn_server* sv, int32_t* n_out) {
   }
   const int n = (int)sv->act.size();
   if (n == 0) return DYN_OK;
-  if (cap > sv->gvis_cap) {
-    // grow the batch visible list (at least doubling: the wait for the
-    // steps in flight and the reallocation happen a few times per run)
-    const int64_t want = std::max(cap, 2 * sv->gvis_cap);
-    DYN_CUDA(cudaStreamSynchronize(sv->stream));
-    cudaFree(sv->d_gvis);
-    sv->d_gvis = nullptr;
-    sv->gvis_cap = 0;
-    DYN_CUDA(cudaMalloc(&sv->d_gvis, sizeof(int2) * (size_t)want));
-    sv->gvis_cap = want;
-  }
+  // the admitted sessions' blocks fit the list by construction (each block
+  // costs at least kMinBlockBytes of the budget)
+  if (cap > sv->gvis_cap) return DYN_ERR_BUDGET_EXCEEDED;
   cudaStream_t st = sv->stream;
   DYN_CUDA(cudaMemcpyAsync(rb.d_tab, rb.h_tab, sizeof(SessDev) * (size_t)n,
                            cudaMemcpyHostToDevice, st));

@@ -72,7 +72,7 @@ void release(dyn_session* s) {
   for (void* p : {(void*)s->h_depth, (void*)s->h_rgb, (void*)s->h_res, (void*)s->h_depth_1,
                   (void*)s->h_rgb_1, (void*)s->h_res_1, (void*)s->h_res_aux})
     if (p) cudaFreeHost(p);
-  if (s->h2d_done) cudaEventDestroy(s->h2d_done);
+  if (s->h2d_done && !s->borrowed_stream) cudaEventDestroy(s->h2d_done);
   for (int k = 0; k < 2; ++k) {
     if (s->ev_h2d[k]) cudaEventDestroy(s->ev_h2d[k]);
     if (s->ev_done[k]) cudaEventDestroy(s->ev_done[k]);
@@ -80,7 +80,7 @@ void release(dyn_session* s) {
   if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
   for (int k = 0; k < DYN_NUM_STAGES; ++k)
     if (s->ev[k]) cudaEventDestroy(s->ev[k]);
-  if (s->stream) cudaStreamDestroy(s->stream);
+  if (s->stream && !s->borrowed_stream) cudaStreamDestroy(s->stream);
   cudaSetDevice(prev);
   delete s;
 }
@@ -398,7 +398,7 @@ dyn_status copy_frame_in(dyn_session* s, const uint16_t* depth, const uint8_t* r
 
 dyn_status upload_frame(dyn_session* s, const uint16_t* depth, const uint8_t* rgb) {
   // no pipelined copy may still read slot 0's staging buffers
-  DYN_CUDA(cudaStreamSynchronize(s->copy_stream));
+  if (s->copy_stream) DYN_CUDA(cudaStreamSynchronize(s->copy_stream));
   // the staging buffers may still feed the previous frame's copies
   DYN_CUDA(cudaEventSynchronize(s->h2d_done));
   dyn_status r = copy_frame_in(s, depth, rgb, s->stream);
@@ -794,12 +794,21 @@ dyn_status create_session(const dyn_tsdf_params* tsdf, const dyn_gn_params* gn,
       return r;              \
     }                        \
   } while (0)
-  bool ok = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) == cudaSuccess &&
-            cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking) == cudaSuccess &&
-            cudaEventCreateWithFlags(&s->h2d_done, cudaEventDisableTiming) == cudaSuccess;
-  for (int k = 0; k < 2 && ok; ++k)
-    ok = cudaEventCreateWithFlags(&s->ev_h2d[k], cudaEventDisableTiming) == cudaSuccess &&
-         cudaEventCreateWithFlags(&s->ev_done[k], cudaEventDisableTiming) == cudaSuccess;
+  bool ok = true;
+  if (mem.stream) {
+    // a server's pooled stream and event: creating streams while the
+    // device is busy can block the caller for tens of milliseconds
+    s->stream = mem.stream;
+    s->h2d_done = mem.h2d_done;
+    s->borrowed_stream = true;
+  } else {
+    ok = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) == cudaSuccess &&
+         cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking) == cudaSuccess &&
+         cudaEventCreateWithFlags(&s->h2d_done, cudaEventDisableTiming) == cudaSuccess;
+    for (int k = 0; k < 2 && ok; ++k)
+      ok = cudaEventCreateWithFlags(&s->ev_h2d[k], cudaEventDisableTiming) == cudaSuccess &&
+           cudaEventCreateWithFlags(&s->ev_done[k], cudaEventDisableTiming) == cudaSuccess;
+  }
   if (!ok) {
     cudaGetLastError();
     release(s);

@@ -156,6 +156,7 @@ struct dyn_session {
   BatchShape shape;
   dyn_batch* batch = nullptr;  // member of this batch (frames go through it)
   cudaStream_t owner_stream = nullptr;  // a server's stream when it owns the session
+  bool borrowed_stream = false;  // 'stream' and 'h2d_done' belong to the server's pool
   // host
   uint16_t* h_depth = nullptr;
   uint8_t* h_rgb = nullptr;
@@ -378,6 +379,11 @@ struct SessionMemory {
   size_t region_size = 0;
   bool host_staging = true;  // pinned staging and result buffers now (else on first use)
   bool sync = true;          // return after the initialisation has run
+  // a stream and event the session uses instead of creating its own (a
+  // server's pool); such a session has no copy stream and no second input
+  // slot events (frames reach it only through its server)
+  cudaStream_t stream = nullptr;
+  cudaEvent_t h2d_done = nullptr;
 };
 // Exact device bytes of a session with these parameters (no CUDA calls);
 // 0 when the parameters are invalid.

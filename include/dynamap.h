@@ -517,10 +517,17 @@ dyn_status dyn_batch_tuning(dyn_batch* b, int32_t* done, int32_t* integrate_ctas
  * dyn_server_result waits for the last step that processed the slot and
  * returns its latest result.  A served session takes frames only through
  * the server; its other calls (raycast, download, pose, images) wait for
- * the server's work in flight.  Calls on one server are not thread-safe. */
+ * the server's work in flight.  Calls on one server are not thread-safe.
+ * The server reserves its whole budget at creation: the first budget/258
+ * bytes hold the batch visible list (one entry for every block the rest of
+ * the budget can hold: a block costs at least 2,064 bytes), the rest is
+ * carved into sessions.  It also makes its sessions' streams ahead of time
+ * (a pool of up to 64, more on demand, reused after release), so neither
+ * admission nor a step allocates device memory or creates a stream. */
 typedef struct dyn_server dyn_server;
 typedef struct {
-  size_t budget_bytes;   /* device bytes for sessions (0: 90% of free memory) */
+  size_t budget_bytes;   /* device bytes for sessions and the batch visible list
+                            (0: 90% of free memory) */
   int32_t max_sessions;  /* slots (0: 256) */
   int32_t device;
 } dyn_server_params;
