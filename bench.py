@@ -564,6 +564,9 @@ def run_ours(args):
     ranks.close()
 
 
+TUNE_FRAMES = 3  # autotuner frames per candidate shape (the first not timed)
+
+
 def measure_batched(args, ranks, local, n_sessions, steps, warmup, precisions,
                     e2e=True, streams=False, stage_split=False):
     """The batched configuration: n_sessions independent sessions of mixed
@@ -572,6 +575,10 @@ def measure_batched(args, ranks, local, n_sessions, steps, warmup, precisions,
     per stage (dyn_batch, one CUDA graph per frame), beside the plain FP32
     per-frame path on the same GPU: the same sessions driven one frame at a
     time, each waited for before the next (the reference's per-frame loop).
+    Each fused batch runs the project's autotuner (dyn_batch_autotune) over
+    its warm-up frames: integration grid x raycast tile, then the ICP form
+    (persistent grid, half grid, chained kernels), all result-neutral; the
+    timed frames use the shape it kept.
     Returns the per-form figures: aggregate frames/s (device-resident
     frames; end to end from pinned host memory with 'e2e'), the speed-up
     over the plain path, and each session's trajectory against the plain
@@ -583,6 +590,9 @@ def measure_batched(args, ranks, local, n_sessions, steps, warmup, precisions,
     from dynamap_b200 import abi, configs
     from dynamap_b200.session import Batch, Session
     world, rank = ranks.world, ranks.rank
+    # the autotuner's candidates (9 launch shapes, then 2 more ICP forms)
+    # take TUNE_FRAMES frames each, then the kept shape's graph is captured
+    warmup = max(warmup, 11 * TUNE_FRAMES + 2)
     nframes = warmup + steps
     mix = configs.session_mix(n_sessions, nframes, base_seed=100 + 1000 * rank)
     workers = max(1, min(32, ((os.cpu_count() or 2) - 1) // max(world, 1)))
@@ -656,9 +666,11 @@ def measure_batched(args, ranks, local, n_sessions, steps, warmup, precisions,
         prec = PRECISIONS[pname]
         ss = open_sessions(prec)
         bt = Batch(ss)
+        bt.autotune(TUNE_FRAMES)
         for k in range(warmup):
             bt.submit_device([dev_frames[j].data_ptr() + k * nbytes[j] for j in range(n)])
             bt.result(strict=False)
+        tuned, tune_ctas, tune_tile = bt.tuning()
         track = [[] for _ in range(n)]
 
         def fused_device():
@@ -674,7 +686,10 @@ def measure_batched(args, ranks, local, n_sessions, steps, warmup, precisions,
         launches = bt.kernels_per_frame() * steps
         form = {"fps": total / t_dev, "ms_per_step": 1e3 * t_dev / steps,
                 "speedup_vs_plain": t_plain / t_dev, "gpu_launches": launches,
-                "clocks": clocks}
+                "clocks": clocks,
+                "autotuned": {"done": tuned, "integrate_ctas": tune_ctas,
+                              "ray_tile": ["16x16", "32x8", "8x8"][tune_tile],
+                              "frames_per_candidate": TUNE_FRAMES}}
         if stage_split:
             bt.profile(True)
             for k in range(warmup, min(nframes, warmup + 20)):
@@ -697,6 +712,7 @@ def measure_batched(args, ranks, local, n_sessions, steps, warmup, precisions,
         if e2e:
             ss = open_sessions(prec)
             bt = Batch(ss)
+            bt.autotune(TUNE_FRAMES)
             for k in range(warmup):
                 bt.submit([pinned[j][k] for j in range(n)])
                 bt.result(strict=False)

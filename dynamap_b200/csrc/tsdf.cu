@@ -807,17 +807,37 @@ __device__ inline VoxelSample get_interpolated(const VolumeDev& v, F3 position, 
   // the high corners lie in the next block along an axis where they cross
   const bool cx = blk_of(gx[1]) != blk_of(gx[0]), cy = blk_of(gy[1]) != blk_of(gy[0]),
              cz = blk_of(gz[1]) != blk_of(gz[0]);
-  CellBlocks cells;
-  cell_blocks(v, blk_of(gx[0]), blk_of(gy[0]), blk_of(gz[0]), cx, cy, cz, bc, cells);
-  float dist = 0.0f;
-  float cr = 0.0f, cg = 0.0f, cb = 0.0f;
   const int off[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1},
                          {1, 1, 0}, {0, 1, 1}, {1, 0, 1}, {1, 1, 1}};
+  // the eight corner voxels: one block and constant strides from the low
+  // corner in the common case (no axis crosses a block boundary and each
+  // high index is the low one + 1), else each corner's block and index
+  uint2 cv[8];
+  if (!(cx || cy || cz) && gx[1] - gx[0] == 1 && gy[1] - gy[0] == 1 && gz[1] - gz[0] == 1) {
+    const int p0 = block_ptr(v, blk_of(gx[0]), blk_of(gy[0]), blk_of(gz[0]), bc);
+    const uint2* base = reinterpret_cast<const uint2*>(v.voxels + (size_t)(p0 < 0 ? 0 : p0) *
+                                                                      kBlockVox +
+                                                       lin_of(gx[0], gy[0], gz[0]));
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      cv[k] = p0 < 0 ? make_uint2(0u, 0u)
+                     : __ldg(base + (off[k][0] << 6) + (off[k][1] << 3) + off[k][2]);
+  } else {
+    CellBlocks cells;
+    cell_blocks(v, blk_of(gx[0]), blk_of(gy[0]), blk_of(gz[0]), cx, cy, cz, bc, cells);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int ox = off[k][0], oy = off[k][1], oz = off[k][2];
+      cv[k] = load_voxel(v, corner_block(cells, cx, cy, cz, ox, oy, oz),
+                         lin_of(gx[ox], gy[oy], gz[oz]));
+    }
+  }
+  float dist = 0.0f;
+  float cr = 0.0f, cg = 0.0f, cb = 0.0f;
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
     const int ox = off[k][0], oy = off[k][1], oz = off[k][2];
-    const int ptr = corner_block(cells, cx, cy, cz, ox, oy, oz);
-    uint2 vv = load_voxel(v, ptr, lin_of(gx[ox], gy[oy], gz[oz]));
+    const uint2 vv = cv[k];
     uint2 src = (vw(vv) == 0) ? v0 : vv;
     float a = ox ? wt.x : 1.0f - wt.x;
     float b = oy ? wt.y : 1.0f - wt.y;
@@ -1012,8 +1032,10 @@ __device__ inline int cell_block_free(const VolumeDev& v, int bx, int by, int bz
 
 // The march of pixel (x, y) from camera pose T; the colour at the hit when
 // rgb_out is given.  skip_to / skip_far: the tile's ray depth bounds.
-// Returns true when the march hit the step cap.
-template <bool FP16>
+// Returns true when the march hit the step cap.  FREE: the session keeps
+// free-cell flags (mixed form with carving); without them (band sessions)
+// the cell's and the centre voxel's blocks share one lookup cache.
+template <bool FP16, bool FREE>
 __device__ inline bool raycast_px(const VolumeDev& v, const DSensor& s, const M4f& T, int x,
                                   int y, float skip_to, float skip_far,
                                   float* __restrict__ depth_out, uint8_t* __restrict__ rgb_out) {
@@ -1046,7 +1068,7 @@ __device__ inline bool raycast_px(const VolumeDev& v, const DSensor& s, const M4
     }
     const F3 q = f3(__fmaf_rn(cur, d.x, o.x), __fmaf_rn(cur, d.y, o.y), __fmaf_rn(cur, d.z, o.z));
     const float flx = floorf(q.x), fly = floorf(q.y), flz = floorf(q.z);
-    if (v.freecell) {
+    if (FREE) {
       int free;
       cell_block_free(v, (int)flx >> 3, (int)fly >> 3, (int)flz >> 3, bc, &free);
       if (free) {  // the interpolated sdf is the truncation distance
@@ -1057,8 +1079,10 @@ __device__ inline bool raycast_px(const VolumeDev& v, const DSensor& s, const M4
     const int gx = (int)flx + (q.x - flx >= 0.5f), gy = (int)fly + (q.y - fly >= 0.5f),
               gz = (int)flz + (q.z - flz >= 0.5f);
     // the centre voxel's block: mostly the cell's own, already resolved
-    const int ptr = (blk_of(gx) == bc.x && blk_of(gy) == bc.y && blk_of(gz) == bc.z)
-                        ? bc.ptr : block_ptr(v, blk_of(gx), blk_of(gy), blk_of(gz), bc0);
+    const int ptr = !FREE ? block_ptr(v, blk_of(gx), blk_of(gy), blk_of(gz), bc)
+                    : (blk_of(gx) == bc.x && blk_of(gy) == bc.y && blk_of(gz) == bc.z)
+                        ? bc.ptr
+                        : block_ptr(v, blk_of(gx), blk_of(gy), blk_of(gz), bc0);
     const int lin = lin_of(gx, gy, gz);
     const typename V::raw_t raw = V::load(v, ptr, lin);
     if (V::w(raw) == 0) {
@@ -1128,7 +1152,10 @@ __device__ inline void raycast_tile(const VolumeDev& v, const DSensor& s,
       skip_to = fminf(__uint_as_float(B.near8[f]), __uint_as_float(B.near64[c]));
       skip_far = fmaxf(__uint_as_float(B.far8[f]), __uint_as_float(B.far64[c]));
     }
-    const bool o = MIXED ? raycast_px<true>(v, s, T, x, y, skip_to, skip_far, depth_out, rgb_out)
+    const bool o = MIXED ? (v.freecell ? raycast_px<true, true>(v, s, T, x, y, skip_to, skip_far,
+                                                                 depth_out, rgb_out)
+                                       : raycast_px<true, false>(v, s, T, x, y, skip_to,
+                                                                  skip_far, depth_out, rgb_out))
                          : raycast_exact_px(v, s, T, x, y, skip_to, skip_far, depth_out, rgb_out);
     if (o) atomicAdd(&over, 1);
   }
