@@ -526,7 +526,13 @@ def run_ours(args):
         roof = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": hbm, "unit": "GB/s",
                 "frac": ach / hbm, "peak_source": f"{peak_kind} hbm_gbs",
                 "algorithmic_bytes_per_launch": alg, "launch_ms": stage_ms[dom],
-                "traffic": traffic}
+                "traffic": traffic,
+                "traffic_source": (None if traffic is None else
+                                   "derived: dram__bytes_read.sum + dram__bytes_write.sum per "
+                                   "launch from the ncu capture summarised in profiles/"
+                                   f"{dom if prec == abi.PRECISION_FP32 else dom + '_mixed'}"
+                                   "_kernel.md, scaled by this run's visible blocks; not "
+                                   "measured in this run")}
     # tracking accuracy against the ground truth
     gt = poses[args.warmup:nframes]
     ate = float(np.sqrt(np.mean([np.sum((a[:3, 3] - b_[:3, 3]) ** 2) for a, b_ in zip(track, gt)])))
