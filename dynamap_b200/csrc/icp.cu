@@ -34,25 +34,15 @@ __device__ inline bool normal_ok(float4 n) {
 
 // Per-thread sums of the per-pixel terms.  The FP32 form adds each pixel's
 // FP32 terms in FP64 (as the oracle does), so that its normal equations
-// differ from the oracle's only by the order of FP64 additions; the mixed
-// form keeps FP32 sums with Kahan compensation.
+// differ from the oracle's only by the order of FP64 additions.  The mixed
+// form (KAHAN) sums a thread's few pixels in FP32 by fused multiply-adds;
+// from the warp sums on, its sums are compensated pairs (block_reduce).
 struct Acc {
   double d[kIcpVals];  // FP64 sums (kahan == 0)
-  float v[kIcpVals];   // compensated FP32 sums (kahan != 0)
-  float c[kIcpVals];   // their compensation
+  float v[kIcpVals];   // FP32 sums (kahan != 0)
 };
 
-template <bool KAHAN>
-__device__ inline void acc_add(Acc& a, int k, float x) {
-  if (KAHAN) {
-    float y = __fsub_rn(x, a.c[k]);
-    float t = __fadd_rn(a.v[k], y);
-    a.c[k] = __fsub_rn(__fsub_rn(t, a.v[k]), y);
-    a.v[k] = t;
-  } else {
-    a.d[k] += (double)x;
-  }
-}
+__device__ inline void acc_add(Acc& a, int k, float x) { a.d[k] += (double)x; }
 
 // Per-pixel terms of buildNLSKernel (gnSolver.cu:55-194) for source pixel
 // idx; the reference's unchecked projection is bounded (z > 0, inside the
@@ -83,12 +73,29 @@ __device__ inline PixSrc load_src(const IcpLevel& L, int idx) {
   return a;
 }
 
+// Pixel (u, v) of index idx in an image of 'cols' columns, exactly: a
+// reciprocal estimate of the row (relative error a few 2^-24, so under one
+// row off for images of up to 2^26 pixels) corrected by one step.
+__device__ inline void pixel_uv(int idx, int cols, int& u, int& v) {
+  v = __float2int_rz(__int2float_rn(idx) * __fdividef(1.0f, (float)cols));
+  u = idx - v * cols;
+  if (u < 0) {
+    --v;
+    u += cols;
+  } else if (u >= cols) {
+    ++v;
+    u -= cols;
+  }
+}
+
 __device__ inline bool project_src(const IcpLevel& L, const IcpParams& P, const M4f& T, int idx,
                                    const PixSrc& a, PixProj& q) {
   const DSensor& s = L.s;
   if (a.d < P.dmin || a.d > P.dmax) return false;
   if (!normal_ok(a.n)) return false;
-  F3 p = xform(T, point3d(idx, a.d, s));
+  int u, v;
+  pixel_uv(idx, s.cols, u, v);
+  F3 p = xform(T, point3d_uv(u, v, a.d, s));
   if (!(p.z > 0.0f)) return false;
   int px, py;
   if (!project(p, s, &px, &py)) return false;
@@ -117,6 +124,47 @@ __device__ inline PixTgt load_tgt(const IcpLevel& L, const IcpParams& P, const P
   return t;
 }
 
+// The mixed form's terms of one pixel (the same terms as below, by fused
+// multiply-adds: b_k = cn_k (pq . n), the reference's three-product sum in
+// exact arithmetic) added into FP32 per-thread sums.
+__device__ inline void accumulate_mixed(const IcpParams& P, const F3 p, const F3 n, const F3 pq,
+                                        const PixTgt& t, Acc& a) {
+  const F3 c = cross3(p, n);
+  const float cn[6] = {c.x, c.y, c.z, n.x, n.y, n.z};
+  const float r = __fmaf_rn(pq.x, n.x, __fmaf_rn(pq.y, n.y, __fmul_rn(pq.z, n.z)));
+  if (P.cw != 0.0f) {
+    const float gx = (t.ic - t.il) * 0.5f, gy = (t.ic - t.iu) * 0.5f;
+    const float Jc[6] = {-gy * p.z, gx * p.z, __fmaf_rn(gy, p.x, -gx * p.y), gx, gy, 0.0f};
+    const float e = t.ic - t.si;
+    const float w1 = 1.0f - P.cw;
+    float wcn[6], cj[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+      wcn[i] = w1 * cn[i];
+      cj[i] = P.cw * Jc[i];
+    }
+    int u = 0;
+#pragma unroll
+    for (int i = 0; i < 6; ++i)
+#pragma unroll
+      for (int j = i; j < 6; ++j, ++u)
+        a.v[u] = __fmaf_rn(wcn[i], cn[j], __fmaf_rn(cj[i], Jc[j], a.v[u]));
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+      a.v[21 + k] = __fmaf_rn(-wcn[k], r, __fmaf_rn(-cj[k], e, a.v[21 + k]));
+  } else {
+    int u = 0;
+#pragma unroll
+    for (int i = 0; i < 6; ++i)
+#pragma unroll
+      for (int j = i; j < 6; ++j, ++u) a.v[u] = __fmaf_rn(cn[i], cn[j], a.v[u]);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) a.v[21 + k] = __fmaf_rn(-cn[k], r, a.v[21 + k]);
+  }
+  a.v[27] = __fmaf_rn(r, r, a.v[27]);
+  a.v[28] = __fadd_rn(a.v[28], 1.0f);
+}
+
 template <bool KAHAN>
 __device__ inline void accumulate(const IcpLevel& L, const IcpParams& P, const PixProj& q,
                                   const PixTgt& t, Acc& a) {
@@ -126,11 +174,15 @@ __device__ inline void accumulate(const IcpLevel& L, const IcpParams& P, const P
   const F3 p = q.p;
   F3 n = f3(t.tn.x, t.tn.y, t.tn.z);
   float cosT = dot3(n, f3(q.sn.x, q.sn.y, q.sn.z));
-  F3 qq = point3d(q.index, t.td, s);
+  F3 qq = point3d_uv(q.px, q.py, t.td, s);
   if (!(fabsf(cosT) > P.cos_thr)) return;
+  F3 pq = p - qq;
+  if (KAHAN) {
+    accumulate_mixed(P, p, n, pq, t, a);
+    return;
+  }
   F3 c = cross3(p, n);
   float cn[6] = {c.x, c.y, c.z, n.x, n.y, n.z};
-  F3 pq = p - qq;
   float b[6];
 #pragma unroll
   for (int k = 0; k < 6; ++k)
@@ -148,20 +200,20 @@ __device__ inline void accumulate(const IcpLevel& L, const IcpParams& P, const P
 #pragma unroll
     for (int i = 0; i < 6; ++i)
 #pragma unroll
-      for (int j = i; j < 6; ++j) acc_add<KAHAN>(a, u++, w1 * (cn[i] * cn[j]) + (P.cw * Jc[i]) * Jc[j]);
+      for (int j = i; j < 6; ++j) acc_add(a, u++, w1 * (cn[i] * cn[j]) + (P.cw * Jc[i]) * Jc[j]);
 #pragma unroll
-    for (int k = 0; k < 6; ++k) acc_add<KAHAN>(a, 21 + k, -(w1 * b[k] + (P.cw * Jc[k]) * e));
+    for (int k = 0; k < 6; ++k) acc_add(a, 21 + k, -(w1 * b[k] + (P.cw * Jc[k]) * e));
   } else {
     int u = 0;
 #pragma unroll
     for (int i = 0; i < 6; ++i)
 #pragma unroll
-      for (int j = i; j < 6; ++j) acc_add<KAHAN>(a, u++, cn[i] * cn[j]);
+      for (int j = i; j < 6; ++j) acc_add(a, u++, cn[i] * cn[j]);
 #pragma unroll
-    for (int k = 0; k < 6; ++k) acc_add<KAHAN>(a, 21 + k, -b[k]);
+    for (int k = 0; k < 6; ++k) acc_add(a, 21 + k, -b[k]);
   }
-  acc_add<KAHAN>(a, 27, r * r);
-  acc_add<KAHAN>(a, 28, 1.0f);
+  acc_add(a, 27, r * r);
+  acc_add(a, 28, 1.0f);
 }
 
 template <bool KAHAN>
@@ -233,7 +285,7 @@ __device__ inline void block_reduce(const Acc& a, double* red /*[8][29]*/) {
 #pragma unroll
     for (int k = 0; k < kIcpVals; ++k) {
       s[k] = a.v[k];
-      c[k] = -a.c[k];  // Kahan's c is the negated error
+      c[k] = 0.0f;
     }
 #pragma unroll
     for (int k = kIcpVals; k < 32; ++k) s[k] = c[k] = 0.0f;
@@ -577,7 +629,7 @@ __device__ inline void tile_partial(const IcpLevel& L, const IcpParams& P, const
   Acc a;
 #pragma unroll
   for (int k = 0; k < kIcpVals; ++k) {
-    a.v[k] = a.c[k] = 0.0f;
+    a.v[k] = 0.0f;
     a.d[k] = 0.0;
   }
   const int n = L.s.rows * L.s.cols;
@@ -919,7 +971,7 @@ __global__ void __launch_bounds__(kIcpThreads)
   Acc a;
 #pragma unroll
   for (int k = 0; k < kIcpVals; ++k) {
-    a.v[k] = a.c[k] = 0.0f;
+    a.v[k] = 0.0f;
     a.d[k] = 0.0;
   }
   const int n = L.s.rows * L.s.cols;

@@ -163,7 +163,7 @@ __global__ void downsample_intensity_kernel(const float* __restrict__ src, int r
 // row/image.
 __device__ inline void maps_px(const float* __restrict__ depth, float4* __restrict__ normal,
                                float4* __restrict__ vertex, const DSensor& s, int i) {
-  int y = i / s.cols, x = i - (i / s.cols) * s.cols;
+  const int y = i / s.cols, x = i - y * s.cols;
   float d = depth[i];
   float4 nrm = make_float4(0.f, 0.f, 0.f, 0.f);
   if (!(d > 0.0f)) {
@@ -171,14 +171,14 @@ __device__ inline void maps_px(const float* __restrict__ depth, float4* __restri
     if (vertex) vertex[i] = nrm;
     return;
   }
-  F3 p = point3d(i, d, s);
+  F3 p = point3d_uv(x, y, d, s);
   if (vertex) vertex[i] = make_float4(p.x, p.y, p.z, 1.0f);
   if (x - 2 >= 0 && x + 2 < s.cols && y - 1 >= 0 && y + 1 < s.rows) {
     int il = i - 2, ir = i + 2, iu = i - s.cols, id = i + s.cols;
     float dl = depth[il], dr = depth[ir], du = depth[iu], dd = depth[id];
     if (dl > 0.0f && dr > 0.0f && du > 0.0f && dd > 0.0f) {
-      F3 left = point3d(il, dl, s), right = point3d(ir, dr, s);
-      F3 up = point3d(iu, du, s), down = point3d(id, dd, s);
+      F3 left = point3d_uv(x - 2, y, dl, s), right = point3d_uv(x + 2, y, dr, s);
+      F3 up = point3d_uv(x, y - 1, du, s), down = point3d_uv(x, y + 1, dd, s);
       F3 c = cross3(right - left, down - up);
       float dd2 = dot3(c, c);
       if (dd2 > 0.0f) {

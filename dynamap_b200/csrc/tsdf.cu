@@ -122,7 +122,7 @@ __device__ inline void allocate_tile(const float* __restrict__ depth, const DSen
     const int i = y * s.cols + x;
     const float d = depth[i];
     if (!(d < t.dmin || d > t.dmax)) {  // tsdf.cu:442-444
-      F3 point = xform(T, point3d(i, d, s));
+      F3 point = xform(T, point3d_uv(x, y, d, s));
       if (!(point.x == 0 && point.y == 0 && point.z == 0)) {
         F3 start_pt = f3(T.m[3], T.m[7], T.m[11]);
         // band allocation: the ray starts a truncation distance before the
@@ -903,7 +903,7 @@ __device__ inline bool raycast_exact_px(const VolumeDev& v, const DSensor& s, co
   if (rgb_out) {
     uint8_t r = 0, g = 0, b = 0;
     if (cur < t.dmax) {
-      F3 point = xform(T, point3d(i, cur, s));
+      F3 point = xform(T, point3d_uv(x, y, cur, s));
       VoxelSample vx = get_interpolated<true>(v, point, inv_vs, bc);
       r = (uint8_t)vx.r;
       g = (uint8_t)vx.g;
