@@ -88,6 +88,28 @@ __device__ inline void pixel_uv(int idx, int cols, int& u, int& v) {
   }
 }
 
+// getPoint3d and Project (utils.h:104-119) by fused multiply-adds and
+// approximate division: the mixed form's projective association.
+__device__ inline F3 point3d_fast(int u, int v, float d, const DSensor& s) {
+  return f3(__fdividef(((float)u - s.cx) * d, s.fx), __fdividef(((float)v - s.cy) * d, s.fy), d);
+}
+__device__ inline bool project_fast(F3 p, const DSensor& s, int* px, int* py) {
+  const float rz = __fdividef(1.0f, p.z);
+  const float x = __fmaf_rn(s.fx * p.x, rz, s.cx), y = __fmaf_rn(s.fy * p.y, rz, s.cy);
+  if (!(fabsf(x) < 2e9f) || !(fabsf(y) < 2e9f)) return false;
+  *px = (int)roundf(x);
+  *py = (int)roundf(y);
+  return true;
+}
+__device__ inline F3 xform_fma_icp(const M4f& T, F3 v) {
+  return f3(__fmaf_rn(T.m[0], v.x, __fmaf_rn(T.m[1], v.y, __fmaf_rn(T.m[2], v.z, T.m[3]))),
+            __fmaf_rn(T.m[4], v.x, __fmaf_rn(T.m[5], v.y, __fmaf_rn(T.m[6], v.z, T.m[7]))),
+            __fmaf_rn(T.m[8], v.x, __fmaf_rn(T.m[9], v.y, __fmaf_rn(T.m[10], v.z, T.m[11]))));
+}
+
+// FAST: the mixed form (fused multiply-adds, approximate division); else
+// the reference's expressions with IEEE rounding.
+template <bool FAST>
 __device__ inline bool project_src(const IcpLevel& L, const IcpParams& P, const M4f& T, int idx,
                                    const PixSrc& a, PixProj& q) {
   const DSensor& s = L.s;
@@ -95,10 +117,10 @@ __device__ inline bool project_src(const IcpLevel& L, const IcpParams& P, const 
   if (!normal_ok(a.n)) return false;
   int u, v;
   pixel_uv(idx, s.cols, u, v);
-  F3 p = xform(T, point3d_uv(u, v, a.d, s));
+  F3 p = FAST ? xform_fma_icp(T, point3d_fast(u, v, a.d, s)) : xform(T, point3d_uv(u, v, a.d, s));
   if (!(p.z > 0.0f)) return false;
   int px, py;
-  if (!project(p, s, &px, &py)) return false;
+  if (!(FAST ? project_fast(p, s, &px, &py) : project(p, s, &px, &py))) return false;
   if (px < 0 || py < 0 || px >= s.cols || py >= s.rows) return false;
   q.p = p;
   q.sn = a.n;
@@ -174,7 +196,7 @@ __device__ inline void accumulate(const IcpLevel& L, const IcpParams& P, const P
   const F3 p = q.p;
   F3 n = f3(t.tn.x, t.tn.y, t.tn.z);
   float cosT = dot3(n, f3(q.sn.x, q.sn.y, q.sn.z));
-  F3 qq = point3d_uv(q.px, q.py, t.td, s);
+  F3 qq = KAHAN ? point3d_fast(q.px, q.py, t.td, s) : point3d_uv(q.px, q.py, t.td, s);
   if (!(fabsf(cosT) > P.cos_thr)) return;
   F3 pq = p - qq;
   if (KAHAN) {
@@ -220,7 +242,7 @@ template <bool KAHAN>
 __device__ inline void pixel_terms(const IcpLevel& L, const IcpParams& P, const M4f& T,
                                    int idx, Acc& a) {
   PixProj q;
-  if (!project_src(L, P, T, idx, load_src(L, idx), q)) return;
+  if (!project_src<KAHAN>(L, P, T, idx, load_src(L, idx), q)) return;
   accumulate<KAHAN>(L, P, q, load_tgt(L, P, q, idx), a);
 }
 
@@ -234,8 +256,8 @@ __device__ inline void pixel_pair(const IcpLevel& L, const IcpParams& P, const M
   if (v0) a0 = load_src(L, i0);
   if (v1) a1 = load_src(L, i1);
   PixProj q0, q1;
-  const bool ok0 = v0 && project_src(L, P, T, i0, a0, q0);
-  const bool ok1 = v1 && project_src(L, P, T, i1, a1, q1);
+  const bool ok0 = v0 && project_src<KAHAN>(L, P, T, i0, a0, q0);
+  const bool ok1 = v1 && project_src<KAHAN>(L, P, T, i1, a1, q1);
   PixTgt t0, t1;
   if (ok0) t0 = load_tgt(L, P, q0, i0);
   if (ok1) t1 = load_tgt(L, P, q1, i1);
