@@ -99,7 +99,6 @@ def test_reference_idiom_compiles(tmp_path):
 
 
 @pytest.mark.gpu
-@pytest.mark.first_b200_run
 def test_reference_idiom_runs(tmp_path, gpu_lib):
     from test_dataset import make_tum
     root = tmp_path / "seq"

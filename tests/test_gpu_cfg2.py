@@ -19,7 +19,7 @@ import pytest
 from dynamap_b200 import abi, configs
 from dynamap_b200.session import Session
 
-pytestmark = [pytest.mark.gpu, pytest.mark.first_b200_run]
+pytestmark = pytest.mark.gpu
 
 
 def cfg2(rows=480, cols=640):

@@ -14,7 +14,7 @@ import pytest
 
 from dynamap_b200 import abi, configs
 
-pytestmark = [pytest.mark.gpu, pytest.mark.first_b200_run]
+pytestmark = pytest.mark.gpu
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 

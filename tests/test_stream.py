@@ -64,7 +64,6 @@ def pipe_frames(depth, stamps):
 
 
 @pytest.mark.gpu
-@pytest.mark.first_b200_run
 def test_streams_through_the_server_equal_lone_sessions(tmp_path, gpu_lib):
     from dynamap_b200.session import Session
     from test_dataset import make_tum
@@ -142,7 +141,6 @@ def write_tum_order(root, seq, order, t0=1305031102.0):
 
 
 @pytest.mark.gpu
-@pytest.mark.first_b200_run
 def test_eviction_keeps_a_small_pool_from_filling(tmp_path, gpu_lib):
     """A 160x120 RGB stream that moves 3 cm / 2 deg per frame for 12 frames
     and comes back: its map (about 57,000 blocks with free-space carving)
