@@ -151,6 +151,27 @@ __device__ inline int voxel_index(float p, float vs, float inv_vs) {
   const float sg = (float)((p > 0.0f) - (p < 0.0f));
   return (int)(p / vs + sg * 0.5f);
 }
+// voxel_index of p and of p1 = fl(p + vs), the two corners of a trilinear
+// cell along one axis.  When p's fast path applies (t is at least 16 ulps
+// from every integer, so the exact p / vs + sign * 0.5 is at least 12 ulps
+// away) and p and p1 take the same sign branch with t outside (-1, 0], the
+// exact value for p1 is the one for p plus 1 + delta with |delta| below 2
+// ulps (the rounding of p + vs and of the reference's quotient and sum),
+// so its truncation is the truncation of t plus 1.  Otherwise both indices
+// are computed on their own.
+__device__ inline void voxel_index_pair(float p, float p1, float vs, float inv_vs, int& g0,
+                                        int& g1) {
+  const float t = __fadd_rn(__fmul_rn(p, inv_vs), copysignf(0.5f, p));
+  const float n = rintf(t);
+  if (fabsf(t - n) > __fmaf_rn(fabsf(t), 1.9073486328125e-6f, 1.9073486328125e-6f) &&
+      (p > 0.0f || (p1 < 0.0f && t < -1.0f))) {
+    g0 = (int)t;
+    g1 = g0 + 1;
+    return;
+  }
+  g0 = voxel_index(p, vs, inv_vs);
+  g1 = voxel_index(p1, vs, inv_vs);
+}
 // WorldToBlock / WorldToLocalVoxel (tsdf.cu:195-225) for block size 8: the
 // reference's floor division and non-negative remainder are g >> 3, g & 7.
 __device__ inline int blk_of(int g) { return g >> 3; }

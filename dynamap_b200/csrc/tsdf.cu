@@ -798,12 +798,9 @@ __device__ inline VoxelSample get_interpolated(const VolumeDev& v, F3 position, 
   F3 vp = position * inv;
   F3 wt = f3(vp.x - floorf(vp.x), vp.y - floorf(vp.y), vp.z - floorf(vp.z));
   int gx[2], gy[2], gz[2];
-  gx[0] = voxel_index(pos_dual.x + 0.0f, vs, inv_vs);
-  gx[1] = voxel_index(pos_dual.x + vs, vs, inv_vs);
-  gy[0] = voxel_index(pos_dual.y + 0.0f, vs, inv_vs);
-  gy[1] = voxel_index(pos_dual.y + vs, vs, inv_vs);
-  gz[0] = voxel_index(pos_dual.z + 0.0f, vs, inv_vs);
-  gz[1] = voxel_index(pos_dual.z + vs, vs, inv_vs);
+  voxel_index_pair(pos_dual.x + 0.0f, pos_dual.x + vs, vs, inv_vs, gx[0], gx[1]);
+  voxel_index_pair(pos_dual.y + 0.0f, pos_dual.y + vs, vs, inv_vs, gy[0], gy[1]);
+  voxel_index_pair(pos_dual.z + 0.0f, pos_dual.z + vs, vs, inv_vs, gz[0], gz[1]);
   // the high corners lie in the next block along an axis where they cross
   const bool cx = blk_of(gx[1]) != blk_of(gx[0]), cy = blk_of(gy[1]) != blk_of(gy[0]),
              cz = blk_of(gz[1]) != blk_of(gz[0]);
