@@ -29,9 +29,20 @@
 // margin -- go back (dyn_upload_blocks), so a revisited place keeps what
 // was fused into it.
 //
+// Streams beyond the HBM budget (setParking(true)): a stream that does not
+// fit when it is added starts parked, and a parked stream with a frame
+// waiting is admitted in place of the admitted stream idle the longest (no
+// frame queued or on the device), which is parked: its blocks go to host
+// memory (dyn_download_blocks) and its slot and device bytes are released.
+// A resumed stream gets a new session at its last pose with its blocks
+// uploaded back (dyn_upload_blocks); its first frame is integrated at that
+// pose without tracking (the new session has no target yet), the frames
+// after it track against the restored map.
+//
 // Header-only over the C ABI of dynamap.h; needs C++17 and threads.
 #pragma once
 
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
@@ -78,6 +89,8 @@ class DynaMapNodeHandler {
   };
   struct StreamCounts {
     int64_t evictions = 0, evicted = 0, uploaded = 0, stored = 0;
+    int64_t parks = 0, resumes = 0;  // times parked / resumed (setParking)
+    int64_t restored = 0;            // blocks uploaded back at resumes
   };
   // tf_publisher's role: the frame's time stamp, its camera pose and the
   // frame's statistics (status: the frame's dyn_status, e.g. a full heap)
@@ -103,26 +116,27 @@ class DynaMapNodeHandler {
     on_pose_ = std::move(cb);
   }
 
+  // Streams beyond the budget are parked and resumed in turn instead of
+  // refused (see the header comment).  Off by default.
+  void setParking(bool on) {
+    std::lock_guard<std::mutex> lk(server_mu_);
+    parking_ = on;
+  }
+
   // Admits a stream; returns its id.  Throws when the budget or the slots
   // are exhausted (DYN_ERR_BUDGET_EXCEEDED: add it after another stream
-  // has been removed).
+  // has been removed), unless parking is on: then the stream starts
+  // parked and is admitted when it has a frame.
   int addStream(const StreamConfig& c) {
     std::lock_guard<std::mutex> lk(server_mu_);
-    dyn_tsdf_params t = c.tsdf.to_c();
-    dyn_gn_params g = c.solver.to_c(c.mode);
-    dyn_bilateral_params b;
-    b.diameter = c.kernel.diameter;
-    b.sigma_i = c.kernel.sigmaI;
-    b.sigma_s = c.kernel.sigmaS;
-    b.enabled = c.bilateral ? 1 : 0;
-    dyn_sensor s = c.sensor.to_c();
-    float4x4 p0 = c.pose0.to_row_major();
     int32_t slot = -1;
-    dyn_throw("DynaMapNodeHandler::addStream",
-              dyn_server_admit(server_, &t, &g, &b, &s, c.precision, p0.entries, &slot));
+    const dyn_status r = admit(c, c.pose0, &slot);
+    if (!(r == DYN_ERR_BUDGET_EXCEEDED && parking_))
+      dyn_throw("DynaMapNodeHandler::addStream", r);
     std::lock_guard<std::mutex> lk2(mu_);
     auto st = std::make_shared<Stream>();
     st->slot = slot;
+    st->last_active = steps_;
     st->npx = (size_t)c.sensor.rows * c.sensor.cols;
     st->scaler = c.sensor.depthScaler;
     st->cfg = c;
@@ -214,7 +228,7 @@ class DynaMapNodeHandler {
     std::lock_guard<std::mutex> slk(server_mu_);  // server first, as everywhere
     std::lock_guard<std::mutex> lk(mu_);
     auto it = streams_.find(stream);
-    if (it == streams_.end()) return nullptr;
+    if (it == streams_.end() || it->second->slot < 0) return nullptr;
     dyn_session* out = nullptr;
     dyn_server_session(server_, it->second->slot, &out);
     return out;
@@ -227,7 +241,7 @@ class DynaMapNodeHandler {
     std::vector<uint8_t> rgb;
   };
   struct Stream {
-    int32_t slot = -1;
+    int32_t slot = -1;  // -1 while parked
     size_t npx = 0;
     float scaler = 1.0f;
     std::deque<Frame> queue;
@@ -239,7 +253,82 @@ class DynaMapNodeHandler {
     // evicted blocks: packed coordinate -> 512 voxels
     std::unordered_map<uint64_t, std::vector<dyn_voxel>> store;
     StreamCounts counts;
+    // while parked: the blocks its session held (coordinates, 512 voxels each)
+    std::vector<int32_t> park_coords;
+    std::vector<dyn_voxel> park_vox;
+    int64_t last_active = 0;  // the step of its last admission or result
   };
+
+  dyn_status admit(const StreamConfig& c, const Matrix4f& pose, int32_t* slot) {
+    dyn_tsdf_params t = c.tsdf.to_c();
+    dyn_gn_params g = c.solver.to_c(c.mode);
+    dyn_bilateral_params b;
+    b.diameter = c.kernel.diameter;
+    b.sigma_i = c.kernel.sigmaI;
+    b.sigma_s = c.kernel.sigmaS;
+    b.enabled = c.bilateral ? 1 : 0;
+    dyn_sensor s = c.sensor.to_c();
+    float4x4 p0 = pose.to_row_major();
+    return dyn_server_admit(server_, &t, &g, &b, &s, c.precision, p0.entries, slot);
+  }
+
+  // Parks an idle stream: its blocks to host memory, its slot released
+  // (server lock held; the stream has no frame on the device).
+  bool park(Stream& v) {
+    dyn_session* sess = nullptr;
+    if (dyn_server_session(server_, v.slot, &sess) != DYN_OK || !sess) return false;
+    int64_t n = 0, got = 0;
+    if (dyn_num_blocks(sess, &n) != DYN_OK) return false;
+    v.park_coords.resize((size_t)n * 3);
+    v.park_vox.resize((size_t)n * 512);
+    if (n > 0 && dyn_download_blocks(sess, v.park_coords.data(), v.park_vox.data(), n, &got) !=
+                     DYN_OK)
+      return false;
+    v.park_coords.resize((size_t)std::min(got, n) * 3);
+    v.park_vox.resize((size_t)std::min(got, n) * 512);
+    if (dyn_server_release(server_, v.slot) != DYN_OK) return false;
+    std::lock_guard<std::mutex> lk(mu_);
+    v.slot = -1;
+    v.counts.parks++;
+    return true;
+  }
+
+  // Admits a parked stream that has a frame waiting, parking the admitted
+  // streams idle the longest while the budget does not hold it (server
+  // lock held).  False when no idle stream is left to park.
+  bool resume(Stream& s) {
+    int32_t slot = -1;
+    while (true) {
+      const dyn_status r = admit(s.cfg, s.pose, &slot);
+      if (r == DYN_OK) break;
+      if (r != DYN_ERR_BUDGET_EXCEEDED) return false;
+      Stream* victim = nullptr;
+      {
+        std::lock_guard<std::mutex> lk(mu_);
+        for (auto& kv : streams_) {
+          Stream& v = *kv.second;
+          if (&v == &s || v.slot < 0 || v.in_flight || !v.queue.empty()) continue;
+          if (!victim || v.last_active < victim->last_active) victim = &v;
+        }
+      }
+      if (!victim || !park(*victim)) return false;
+    }
+    const int64_t n = (int64_t)s.park_coords.size() / 3;
+    int64_t counts[4] = {0, 0, 0, 0};
+    if (n > 0) {
+      dyn_session* sess = nullptr;
+      dyn_server_session(server_, slot, &sess);
+      if (sess) dyn_upload_blocks(sess, s.park_coords.data(), s.park_vox.data(), n, counts);
+    }
+    std::vector<int32_t>().swap(s.park_coords);
+    std::vector<dyn_voxel>().swap(s.park_vox);
+    std::lock_guard<std::mutex> lk(mu_);
+    s.slot = slot;
+    s.last_active = steps_;
+    s.counts.resumes++;
+    s.counts.restored += counts[0];
+    return true;
+  }
   static uint64_t block_key(int x, int y, int z) {
     const uint64_t m = (1ull << 21) - 1;
     return (((uint64_t)x & m) << 42) | (((uint64_t)y & m) << 21) | ((uint64_t)z & m);
@@ -341,9 +430,15 @@ class DynaMapNodeHandler {
         std::lock_guard<std::mutex> slk(server_mu_);
         for (auto& [id, s] : ready) {
           Frame f;
+          bool parked;
           {
             std::lock_guard<std::mutex> lk(mu_);
             if (s->in_flight || s->queue.empty()) continue;
+            parked = s->slot < 0;
+          }
+          if (parked && !resume(*s)) continue;  // waits for an idle stream
+          {
+            std::lock_guard<std::mutex> lk(mu_);
             f = std::move(s->queue.front());
             s->queue.pop_front();
           }
@@ -391,6 +486,7 @@ class DynaMapNodeHandler {
           if (!done) continue;
           r = dyn_server_result(server_, s->slot, pose, &st);
           s->pose = Matrix4f::from_row_major(pose);
+          s->last_active = steps_;
           evict_old(*s, st);
         }
         {
@@ -406,7 +502,7 @@ class DynaMapNodeHandler {
       for (auto it = streams_.begin(); it != streams_.end();) {
         Stream& s = *it->second;
         if (s.closing && s.queue.empty() && !s.in_flight) {
-          dyn_server_release(server_, s.slot);
+          if (s.slot >= 0) dyn_server_release(server_, s.slot);
           it = streams_.erase(it);
         } else {
           ++it;
@@ -441,6 +537,7 @@ class DynaMapNodeHandler {
   std::thread worker_;
   bool running_ = false;
   int next_id_ = 0;
+  bool parking_ = false;
   int64_t queued_ = 0;  // frames handed over and not yet reported
   int in_flight_ = 0;
   std::atomic<int64_t> frames_done_{0}, steps_{0};

@@ -191,3 +191,67 @@ def test_eviction_keeps_a_small_pool_from_filling(tmp_path, gpu_lib):
     got = [np.array([float(v) for v in x[6:22]], np.float32).reshape(4, 4) for x in rows]
     diff = max(float(np.linalg.norm(a[:3, 3] - r_[:3, 3])) for a, r_ in zip(got, ref))
     assert diff < 5e-3, diff
+
+
+@pytest.mark.gpu
+def test_streams_beyond_the_budget_take_turns(tmp_path, gpu_lib):
+    """Two 160x120 RGB streams under a budget that holds one session, with
+    parking on: stream A replays frames 0-7 of its sequence, then stream B
+    its 8 frames, then A frames 8-15.  B starts parked; its first frame
+    parks A (A's blocks to host memory, its slot released) and admits B;
+    A's return parks B and resumes A with its blocks uploaded back.  Every
+    frame succeeds; A's frames before the first park equal a run whose
+    budget holds both streams bit for bit; A's first frame after the resume
+    holds at least the blocks it had before it was parked; and A's poses
+    after the resume (the first of its frames integrated at its last pose
+    without tracking) stay within 3 cm of the run that never parks."""
+    from dynamap_b200.session import Server
+    p = configs.preset("cfg2")
+    p["sensor"].update(rows=120, cols=160, fx=131.25, fy=131.25, cx=79.5, cy=59.5)
+    p["tsdf"].update(num_buckets=1 << 16, num_blocks=1 << 15)
+    seq_a = configs.sequence(p, seed=41, n_frames=16)
+    seq_b = configs.sequence(p, seed=42, n_frames=8)
+    write_tum_order(tmp_path / "a1", seq_a, range(8))
+    write_tum_order(tmp_path / "a2", seq_a, range(8, 16), t0=1305031102.0 + 0.0333 * 8)
+    write_tum_order(tmp_path / "b", seq_b, range(8), t0=1305031202.0)
+    pp = stream_preset(p, 0.1)
+    with Server(budget_bytes=4 << 30) as sv:
+        slot = sv.admit(*configs.structs(pp), precision=abi.PRECISION_FP32)
+        need = sv.usage()["used_bytes"]
+        sv.release(slot)
+    budget = int(need * 1.01) + (1 << 20)  # one session (and the visible list), not two
+    spec = tmp_path / "spec.txt"
+    spec.write_text(
+        spec_line(f"{tmp_path / 'a1'},{tmp_path / 'a2'}", pp, abi.PRECISION_FP32, 0.0,
+                  seq_a.poses[0]) + "\n" +
+        spec_line(str(tmp_path / "b"), pp, abi.PRECISION_FP32, 0.0, seq_b.poses[0]) + "\n")
+    exe = str(tmp_path / "stream")
+    compile_stream(exe)
+    runs = {}
+    for name, extra in (("park", ["--park", str(budget), "--sequential"]),
+                        ("roomy", ["--park", str(8 << 30), "--sequential"])):
+        out = tmp_path / f"{name}.txt"
+        r = subprocess.run([exe, str(spec), str(out)] + extra, capture_output=True, text=True,
+                           timeout=300)
+        assert r.returncode == 0, r.stdout + r.stderr
+        rows = [ln.split() for ln in out.read_text().splitlines()]
+        counts = {int(c[1]): [int(v) for v in c[2:]] for c in
+                  (ln.split() for ln in r.stdout.splitlines() if ln.startswith("counts"))}
+        runs[name] = (rows, counts)
+    rows, counts = runs["park"]
+    assert len(rows) == 24 and all(int(x[2]) == 0 for x in rows), [x[2] for x in rows]
+    a = [x for x in rows if x[0] == "0"]
+    b = [x for x in rows if x[0] == "1"]
+    assert len(a) == 16 and len(b) == 8
+    # counts: evictions evicted uploaded stored parks resumes restored
+    assert counts[0][4] == 1 and counts[0][5] == 1 and counts[0][6] > 0, counts
+    assert counts[1][4] == 1 and counts[1][5] == 1, counts
+    assert runs["roomy"][1][0][4] == 0 and runs["roomy"][1][1][4] == 0, runs["roomy"][1]
+    assert int(a[8][22]) >= int(a[7][22]), (a[7][22], a[8][22])
+    ref = [x for x in runs["roomy"][0] if x[0] == "0"]
+    pose = lambda x: np.array([float(v) for v in x[6:22]], np.float32).reshape(4, 4)
+    for k in range(8):
+        np.testing.assert_array_equal(pose(a[k]), pose(ref[k]), err_msg=f"frame {k}")
+    diff = max(float(np.linalg.norm(pose(a[k])[:3, 3] - pose(ref[k])[:3, 3]))
+               for k in range(8, 16))
+    assert diff < 0.03, diff
