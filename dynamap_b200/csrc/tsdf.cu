@@ -482,19 +482,41 @@ __device__ inline float norm3_fast(F3 v) {
 
 // Whether this frame updates voxel 'lin' of block 'ptr', and with which
 // sdf and colour (the per-voxel test of IntegrateScanKernel).
+// The world position of a block's first voxel (its key times the block's
+// extent, as the reference computes it per voxel).
+__device__ inline F3 block_origin(const VolumeDev& v, int ptr) {
+  const float vs = v.t.vs;
+  const unsigned long long key = v.block_keys[ptr];
+  return f3((float)key_x(key) * vs * (float)kBlockSize, (float)key_y(key) * vs * (float)kBlockSize,
+            (float)key_z(key) * vs * (float)kBlockSize);
+}
+
+// Voxel::mergeVoxelColor (geom_Types.h:87-91) of an observation of weight 1
+// into a channel of weight w: the byte of (old * w + obs) / (w + 1) in
+// FP32.  The numerator is an integer below 2^24 (exact in FP32), and the
+// rounded quotient truncates to the floor of the exact one: below an
+// integer k <= 255 the quotient is at least 1 / (w + 1) >= 2^-16 away,
+// more than the half ulp (at most 2^-17) it would take to round up to k.
+// So the integer quotient gives the same byte; it comes from an estimate
+// by the reciprocal rcp_d of w + 1 (relative error a few 2^-24, under one
+// unit off) corrected by one step.
+__device__ inline uint8_t colour_merge(unsigned old, unsigned obs, unsigned w, float rcp_d) {
+  const int n = (int)(old * w + obs), d = (int)w + 1;
+  int q = __float2int_rz(__int2float_rn(n) * rcp_d);
+  const int r = n - q * d;
+  q += (int)(r >= d) - (int)(r < 0);
+  return (uint8_t)q;
+}
+
 template <bool FAST>
 __device__ inline bool observe_voxel(const VolumeDev& v, const float* __restrict__ depth,
                                      const float* __restrict__ sdist,
                                      const uint8_t* __restrict__ rgb, const DSensor& s,
-                                     const M4f& invT, int ptr, int lin, float& sdf, uint8_t& c0,
-                                     uint8_t& c1, uint8_t& c2) {
+                                     const M4f& invT, F3 position, int lin, float& sdf,
+                                     uint8_t& c0, uint8_t& c1, uint8_t& c2) {
   const DTsdf& t = v.t;
   const float vs = t.vs;
   const int bx = lin >> 6, by = (lin >> 3) & 7, bz = lin & 7;
-  const unsigned long long key = v.block_keys[ptr];
-  F3 position = f3((float)key_x(key) * vs * (float)kBlockSize,
-                   (float)key_y(key) * vs * (float)kBlockSize,
-                   (float)key_z(key) * vs * (float)kBlockSize);
   F3 vp = f3(position.x + (float)bx * vs, position.y + (float)by * vs,
              position.z + (float)bz * vs);
   // pixel, depth gate and band decide which voxels a frame updates: IEEE
@@ -565,9 +587,10 @@ __device__ inline int merge_voxel(const VolumeDev& v, size_t vi, float sdf, bool
     if (v.colors) {
       uchar4 c = v.colors[vi];
       // colour exactly as the FP32 form (truncated to bytes)
-      c.x = (uint8_t)(((float)c.x * fw + (float)c0 * 1.0f) / (fw + 1.0f));
-      c.y = (uint8_t)(((float)c.y * fw + (float)c1 * 1.0f) / (fw + 1.0f));
-      c.z = (uint8_t)(((float)c.z * fw + (float)c2 * 1.0f) / (fw + 1.0f));
+      const float rd = __fdividef(1.0f, fw + 1.0f);
+      c.x = colour_merge(c.x, c0, (unsigned)w, rd);
+      c.y = colour_merge(c.y, c1, (unsigned)w, rd);
+      c.z = colour_merge(c.z, c2, (unsigned)w, rd);
       v.colors[vi] = c;
     }
     // saturated: f16 value exactly 1 (free space); unobserved before
@@ -584,9 +607,10 @@ __device__ inline int merge_voxel(const VolumeDev& v, size_t vi, float sdf, bool
   // colour merge (geom_Types.h:87-91); a zero colour merged with a zero
   // colour stays exactly zero, so depth-only frames skip the divisions
   if (has_rgb || (raw.x & 0x00ffffffu)) {
-    r0 = (uint8_t)(((float)r0 * fw + (float)c0 * 1.0f) / (fw + 1.0f));
-    r1 = (uint8_t)(((float)r1 * fw + (float)c1 * 1.0f) / (fw + 1.0f));
-    r2 = (uint8_t)(((float)r2 * fw + (float)c2 * 1.0f) / (fw + 1.0f));
+    const float rd = __fdividef(1.0f, fw + 1.0f);
+    r0 = colour_merge(r0, c0, w, rd);
+    r1 = colour_merge(r1, c1, w, rd);
+    r2 = colour_merge(r2, c2, w, rd);
   }
   int nw = (uint8_t)(w + 1);
   if (nw > t.max_w) nw = t.max_w;
@@ -604,10 +628,10 @@ template <bool FP16, bool FAST>
 __device__ inline int integrate_voxel(const VolumeDev& v, const float* __restrict__ depth,
                                        const float* __restrict__ sdist,
                                        const uint8_t* __restrict__ rgb, const DSensor& s,
-                                       const M4f& invT, int ptr, int lin) {
+                                       const M4f& invT, F3 origin, int ptr, int lin) {
   float sdf;
   uint8_t c0, c1, c2;
-  if (!observe_voxel<FAST>(v, depth, sdist, rgb, s, invT, ptr, lin, sdf, c0, c1, c2)) return 0;
+  if (!observe_voxel<FAST>(v, depth, sdist, rgb, s, invT, origin, lin, sdf, c0, c1, c2)) return 0;
   return merge_voxel<FP16>(v, (size_t)ptr * kBlockVox + lin, sdf, rgb != nullptr, c0, c1, c2);
 }
 
@@ -617,10 +641,12 @@ __global__ void __launch_bounds__(kBlockVox)
                            const int* __restrict__ gcount) {
   __shared__ M4f invT;
   __shared__ int cur_s;
+  __shared__ float org[2][3];  // the block's origin, by iteration parity
   const int n = *gcount;
   if (threadIdx.x == 0) cur_s = -1;
   __syncthreads();
-  for (int b = blockIdx.x; b < n; b += gridDim.x) {
+  int par = 0;
+  for (int b = blockIdx.x; b < n; b += gridDim.x, par ^= 1) {
     const int2 entry = gvis[b];
     const int2 item = make_int2(entry.x & ~kVisFree, entry.y);
     if (item.x != cur_s) {  // uniform across the CTA
@@ -630,6 +656,17 @@ __global__ void __launch_bounds__(kBlockVox)
       __syncthreads();
     }
     const SessDev& S = tab[item.x];
+    // one thread computes the block's origin (the same expression every
+    // voxel would evaluate); the barrier also keeps every thread within one
+    // iteration of the others, so the other parity's slot is free
+    if (threadIdx.x == 0 && !(entry.x & kVisFree)) {
+      const F3 o = block_origin(S.vol, item.y);
+      org[par][0] = o.x;
+      org[par][1] = o.y;
+      org[par][2] = o.z;
+    }
+    __syncthreads();
+    const F3 origin = f3(org[par][0], org[par][1], org[par][2]);
     const uint8_t* rgb = *S.rgb_flag ? S.rgb : nullptr;
     int d;
     if (entry.x & kVisFree) {  // a free-space block: every voxel's sdf is the truncation
@@ -637,14 +674,14 @@ __global__ void __launch_bounds__(kBlockVox)
       d = S.vol.fp16 ? merge_voxel<true>(S.vol, vi, S.vol.t.trunc, false, 0, 0, 0)
                      : merge_voxel<false>(S.vol, vi, S.vol.t.trunc, false, 0, 0, 0);
     } else if (!S.vol.fp16)
-      d = integrate_voxel<false, false>(S.vol, S.raw, S.sdist, rgb, S.ls[0], invT, item.y,
-                                        threadIdx.x);
+      d = integrate_voxel<false, false>(S.vol, S.raw, S.sdist, rgb, S.ls[0], invT, origin,
+                                        item.y, threadIdx.x);
     else if (S.vol.t.band)
-      d = integrate_voxel<true, true>(S.vol, S.raw, S.sdist, rgb, S.ls[0], invT, item.y,
-                                      threadIdx.x);
+      d = integrate_voxel<true, true>(S.vol, S.raw, S.sdist, rgb, S.ls[0], invT, origin,
+                                      item.y, threadIdx.x);
     else
-      d = integrate_voxel<true, false>(S.vol, S.raw, S.sdist, rgb, S.ls[0], invT, item.y,
-                                       threadIdx.x);
+      d = integrate_voxel<true, false>(S.vol, S.raw, S.sdist, rgb, S.ls[0], invT, origin,
+                                       item.y, threadIdx.x);
     // the block's non-saturated count follows its voxels exactly: each warp
     // adds its voxels' changes (mixed sessions only; most warps change
     // nothing, and no barrier holds the CTA's warps together)
