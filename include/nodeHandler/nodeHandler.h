@@ -426,6 +426,7 @@ class DynaMapNodeHandler {
         for (auto& kv : streams_) ready.push_back(kv);
       }
       int pushed = 0;
+      bool waiting_parked = false;  // a parked stream found no idle stream to replace
       {
         std::lock_guard<std::mutex> slk(server_mu_);
         for (auto& [id, s] : ready) {
@@ -436,7 +437,10 @@ class DynaMapNodeHandler {
             if (s->in_flight || s->queue.empty()) continue;
             parked = s->slot < 0;
           }
-          if (parked && !resume(*s)) continue;  // waits for an idle stream
+          if (parked && !resume(*s)) {  // waits for an idle stream
+            waiting_parked = true;
+            continue;
+          }
           {
             std::lock_guard<std::mutex> lk(mu_);
             f = std::move(s->queue.front());
@@ -465,6 +469,16 @@ class DynaMapNodeHandler {
           dyn_throw("DynaMapNodeHandler: step", dyn_server_step(server_, &n));
           ++steps_;
         }
+      }
+      // nothing to step while a parked stream waits: back off instead of
+      // spinning (its wake-up condition stays true until a stream idles)
+      if (!pushed && waiting_parked) {
+        bool none;
+        {
+          std::lock_guard<std::mutex> lk(mu_);
+          none = in_flight_ == 0;
+        }
+        if (none) std::this_thread::sleep_for(std::chrono::microseconds(200));
       }
       for (const Refused& x : refused) report(x.id, x.stamp, nullptr, nullptr, x.status);
       refused.clear();
