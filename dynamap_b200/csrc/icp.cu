@@ -659,6 +659,9 @@ __device__ inline void tile_partial(const IcpLevel& L, const IcpParams& P, const
   const int base = tile * tpx + (int)threadIdx.x;
   if (tpx == kIcpThreads) {
     if (base < n) pixel_terms<KAHAN>(L, P, T, base, a);
+  } else if (!KAHAN) {  // FP64 sums hold most registers: one pixel at a time
+    for (int m = 0; m < tpx / kIcpThreads; ++m)
+      if (base + m * kIcpThreads < n) pixel_terms<KAHAN>(L, P, T, base + m * kIcpThreads, a);
   } else {
     for (int m = 0; m < tpx / kIcpThreads; m += 2)
       pixel_pair<KAHAN>(L, P, T, base + m * kIcpThreads, base + (m + 1) * kIcpThreads, n, a);
