@@ -795,6 +795,7 @@ def run_batched(args):
         "step_ms": {"frame_of_all_sessions": f["ms_per_step"]},
         "stage_ms_per_step": f.get("stage_ms_per_step"),
         "streams_e2e_fps": f.get("streams_e2e_fps"),
+        "autotuned": f.get("autotuned"),
         "gpu_launches": f["gpu_launches"],
         "clocks": f["clocks"],
         "e2e": f["e2e"],
