@@ -255,3 +255,27 @@ def test_streams_beyond_the_budget_take_turns(tmp_path, gpu_lib):
     diff = max(float(np.linalg.norm(pose(a[k])[:3, 3] - pose(ref[k])[:3, 3]))
                for k in range(8, 16))
     assert diff < 0.03, diff
+
+
+def test_parking_policy_against_a_stand_in_server(tmp_path):
+    """The front end's parking policy (setParking) without a GPU: the C ABI's
+    serving calls answered by tests/cpp/fake_server.cpp, a budget for one
+    session, two streams taking turns (tests/cpp/park_fake.cpp checks the
+    frames, poses, restored blocks and the park / resume / admission
+    counts)."""
+    cxx = shutil.which("g++")
+    if cxx is None:
+        pytest.skip("no C++ compiler")
+    lib = tmp_path / "libfakedyn.so"
+    exe = tmp_path / "park_fake"
+    inc = os.path.join(ROOT, "include")
+    subprocess.run([cxx, "-std=c++17", "-O2", "-Wall", "-Werror", "-fPIC", "-shared", "-I", inc,
+                    os.path.join(ROOT, "tests", "cpp", "fake_server.cpp"), "-o", str(lib)],
+                   check=True)
+    subprocess.run([cxx, "-std=c++17", "-O2", "-Wall", "-Werror", "-I", inc,
+                    os.path.join(ROOT, "tests", "cpp", "park_fake.cpp"), "-L", str(tmp_path),
+                    "-lfakedyn", f"-Wl,-rpath,{tmp_path}", "-pthread", "-o", str(exe)],
+                   check=True)
+    for _ in range(3):
+        r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+        assert r.returncode == 0 and "ok" in r.stdout, r.stdout + r.stderr
