@@ -257,6 +257,11 @@ class DynaMapNodeHandler {
     std::vector<int32_t> park_coords;
     std::vector<dyn_voxel> park_vox;
     int64_t last_active = 0;  // the step of its last admission or result
+    // host buffers the eviction hands blocks out into, grown when the map
+    // outgrows them and kept (not cleared) between evictions
+    std::vector<int32_t> evict_coords;
+    std::unique_ptr<dyn_voxel[]> evict_vox;
+    int64_t evict_cap = 0;
   };
 
   dyn_status admit(const StreamConfig& c, const Matrix4f& pose, int32_t* slot) {
@@ -387,15 +392,23 @@ class DynaMapNodeHandler {
     dyn_session* sess = nullptr;
     dyn_server_session(server_, s.slot, &sess);
     if (!sess) return;
+    // every allocated block may leave, so the buffers hold them all
     const int64_t cap = st.blocks_total;
-    std::vector<int32_t> coords((size_t)cap * 3);
-    std::vector<dyn_voxel> vox((size_t)cap * 512);
+    if (cap > s.evict_cap) {
+      s.evict_coords.resize((size_t)cap * 3);
+      s.evict_vox.reset(new dyn_voxel[(size_t)cap * 512]);
+      s.evict_cap = cap;
+    }
+    const int32_t* coords = s.evict_coords.data();
+    const dyn_voxel* vox = s.evict_vox.get();
     int64_t n = 0;
-    if (dyn_evict_blocks(sess, e.maxAge, coords.data(), vox.data(), cap, &n) != DYN_OK) return;
+    if (dyn_evict_blocks(sess, e.maxAge, s.evict_coords.data(), s.evict_vox.get(), cap, &n) !=
+        DYN_OK)
+      return;
     const int64_t m = n < cap ? n : cap;
     for (int64_t i = 0; i < m; ++i)
       s.store[block_key(coords[3 * i], coords[3 * i + 1], coords[3 * i + 2])] =
-          std::vector<dyn_voxel>(vox.begin() + i * 512, vox.begin() + (i + 1) * 512);
+          std::vector<dyn_voxel>(vox + i * 512, vox + (i + 1) * 512);
     std::lock_guard<std::mutex> lk(mu_);
     s.counts.evictions++;
     s.counts.evicted += m;

@@ -9,6 +9,8 @@
 //    with every voxel's sdf = k and moves the pose 0.01 m along x from the
 //    last pose (the first frame of a session keeps its first pose);
 //  * blocks download and upload as coordinates plus 512 voxels.
+//  * dyn_evict_blocks removes the blocks of frames more than max_age before
+//    the last processed one.
 // Every call is counted in fake_calls() for the test driver.
 #include <cstdint>
 #include <cstring>
@@ -24,6 +26,7 @@ struct dyn_session {
   float pose[16];
   int frames = 0;
   int pending = -1;  // the pushed frame's first depth pixel, -1 when none
+  int last_k = 0;    // the last processed frame's
   int64_t bytes = 0;
 };
 
@@ -117,6 +120,7 @@ dyn_status dyn_server_step(dyn_server* sv, int32_t* n_out) {
       s->blocks[std::make_tuple(k, s->id, z)] = v;
     }
     s->frames++;
+    s->last_k = k;
     s->pending = -2;  // processed, result not read
     ++n;
   }
@@ -187,9 +191,26 @@ dyn_status dyn_upload_blocks(dyn_session* s, const int32_t* coords, const dyn_vo
   return DYN_OK;
 }
 
-dyn_status dyn_evict_blocks(dyn_session*, int32_t, int32_t*, dyn_voxel*, int64_t,
-                            int64_t* n_out) {
-  *n_out = 0;
+// blocks of frames more than max_age frames before the last one leave
+dyn_status dyn_evict_blocks(dyn_session* s, int32_t max_age, int32_t* coords_out,
+                            dyn_voxel* voxels_out, int64_t capacity, int64_t* n_out) {
+  int64_t i = 0;
+  for (auto it = s->blocks.begin(); it != s->blocks.end();) {
+    if (std::get<0>(it->first) >= s->last_k - max_age) {
+      ++it;
+      continue;
+    }
+    if (i < capacity) {
+      coords_out[3 * i] = std::get<0>(it->first);
+      coords_out[3 * i + 1] = std::get<1>(it->first);
+      coords_out[3 * i + 2] = std::get<2>(it->first);
+      std::memcpy(voxels_out + 512 * i, it->second.data(), 512 * sizeof(dyn_voxel));
+    }
+    ++i;
+    it = s->blocks.erase(it);
+  }
+  *n_out = i;
+  g_calls[5]++;
   return DYN_OK;
 }
 

@@ -2,7 +2,8 @@
 // (DynaMapNodeHandler::setParking), against the stand-in server of
 // fake_server.cpp: a budget that holds one session, stream A fed frames
 // 1-5, then stream B frames 1-5, then A frames 6-10, then B again while A
-// keeps a frame queued.  Prints "ok" and returns 0 when every check holds,
+// keeps a frame queued; then the eviction policy on a stream whose map
+// outgrows its pool.  Prints "ok" and returns 0 when every check holds,
 // else prints what failed and returns 1.
 #include <cstdio>
 #include <map>
@@ -100,6 +101,40 @@ int main() {
   // (and A's removal, if the serving thread ran once more before shutdown)
   std::printf("admissions %lld releases %lld\n", (long long)calls[0], (long long)calls[1]);
   CHECK(calls[0] == 5 && calls[1] >= 4);
+
+  // the eviction policy on a stream whose map outgrows 60 % of a 10-block
+  // pool: blocks of frames more than one frame old go to the host store;
+  // every evicted block is stored or was uploaded back, and eviction
+  // repeats as the map grows (its buffers reused)
+  {
+    DynaMapNodeHandler ev(1 << 20, 0, 8);
+    DynaMapNodeHandler::StreamConfig e = c;
+    e.tsdf.numBlocks = 10;
+    e.evict.enabled = true;
+    e.evict.highWater = 0.6f;
+    e.evict.maxAge = 1;
+    int done = 0;
+    ev.setPoseCallback([&](int, double, const Matrix4f&, const dyn_frame_stats&,
+                           dyn_status status) {
+      if (status == DYN_OK) ++done;
+    });
+    const int id = ev.addStream(e);
+    ev.spin();
+    for (int k = 1; k <= 12; ++k) {
+      uint16_t depth[4] = {(uint16_t)k, 0, 0, 0};
+      ev.kinect_callback(id, depth, nullptr, (double)k);
+      ev.waitIdle();
+    }
+    const auto ce = ev.counts(id);
+    ev.removeStream(id);
+    ev.shutdown();
+    std::printf("evictions %lld evicted %lld uploaded %lld stored %lld\n",
+                (long long)ce.evictions, (long long)ce.evicted, (long long)ce.uploaded,
+                (long long)ce.stored);
+    CHECK(done == 12);
+    CHECK(ce.evictions >= 5 && ce.evicted >= 15);
+    CHECK(ce.stored + ce.uploaded == ce.evicted);
+  }
   if (failures) return 1;
   std::printf("ok\n");
   return 0;

@@ -258,22 +258,29 @@ def test_streams_beyond_the_budget_take_turns(tmp_path, gpu_lib):
 
 
 def test_parking_policy_against_a_stand_in_server(tmp_path):
-    """The front end's parking policy (setParking) without a GPU: the C ABI's
-    serving calls answered by tests/cpp/fake_server.cpp, a budget for one
-    session, two streams taking turns (tests/cpp/park_fake.cpp checks the
-    frames, poses, restored blocks and the park / resume / admission
-    counts)."""
+    """The front end's parking and eviction policies without a GPU: the C
+    ABI's serving calls answered by tests/cpp/fake_server.cpp (built, like
+    the driver, with AddressSanitizer and UBSan where the compiler has
+    them); tests/cpp/park_fake.cpp runs two streams taking turns under a
+    budget for one session (frames, poses, restored blocks, park / resume /
+    admission counts) and a stream whose map outgrows its pool (eviction
+    counts: every evicted block stored or uploaded back)."""
     cxx = shutil.which("g++")
     if cxx is None:
         pytest.skip("no C++ compiler")
     lib = tmp_path / "libfakedyn.so"
     exe = tmp_path / "park_fake"
     inc = os.path.join(ROOT, "include")
-    subprocess.run([cxx, "-std=c++17", "-O2", "-Wall", "-Werror", "-fPIC", "-shared", "-I", inc,
-                    os.path.join(ROOT, "tests", "cpp", "fake_server.cpp"), "-o", str(lib)],
+    san = ["-O1", "-g", "-fsanitize=address,undefined"]
+    probe = subprocess.run([cxx, "-x", "c++", "-", "-o", str(tmp_path / "probe")] + san,
+                           input="int main(){return 0;}", text=True, capture_output=True)
+    if probe.returncode != 0:
+        san = ["-O2"]
+    subprocess.run([cxx, "-std=c++17", "-Wall", "-Werror", "-fPIC", "-shared", "-I", inc] + san +
+                   [os.path.join(ROOT, "tests", "cpp", "fake_server.cpp"), "-o", str(lib)],
                    check=True)
-    subprocess.run([cxx, "-std=c++17", "-O2", "-Wall", "-Werror", "-I", inc,
-                    os.path.join(ROOT, "tests", "cpp", "park_fake.cpp"), "-L", str(tmp_path),
+    subprocess.run([cxx, "-std=c++17", "-Wall", "-Werror", "-I", inc] + san +
+                   [os.path.join(ROOT, "tests", "cpp", "park_fake.cpp"), "-L", str(tmp_path),
                     "-lfakedyn", f"-Wl,-rpath,{tmp_path}", "-pthread", "-o", str(exe)],
                    check=True)
     for _ in range(3):
