@@ -9,7 +9,10 @@ FP32 expressions with numpy (IEEE single precision, round to nearest):
 * corner indices (csrc/common.cuh voxel_index_pair): where the fast path
   of the lower corner's index applies, the upper corner's index
   (WorldToGlobalVoxelHashing of pos_dual + vs, tsdf.cu:189-193) is the
-  lower one plus one.
+  lower one plus one;
+* pixel coordinates (csrc/icp.cu pixel_uv): the row and column of a pixel
+  index from a reciprocal estimate corrected by one step equal the integer
+  division's.
 
 The GPU tests show the kernels bit-exact against the oracle on whole
 frames; these check the arithmetic argument itself on every (or many)
@@ -62,3 +65,24 @@ def test_upper_corner_index_follows_from_the_lower_one():
             assert np.array_equal(g0[fast] + 1, _ref_index(p1, vs)[fast])
             used += int(fast.sum())
     assert used > 5_000_000
+
+
+def test_pixel_coordinates_from_a_reciprocal_estimate():
+    """pixel_uv (csrc/icp.cu): the row of pixel index idx as the truncated
+    product of idx and an approximate reciprocal of the column count, then
+    one correction step, equals idx / cols and idx % cols for images of up
+    to 8192 x 8192 pixels and reciprocals a few ulps off."""
+    rng = np.random.default_rng(5)
+    for rows, cols in ((120, 160), (240, 320), (480, 640), (720, 1280), (60, 80), (30, 40),
+                       (8192, 8192), (8192, 7), (3, 8191)):
+        n = rows * cols
+        idx = np.arange(n, dtype=np.int64) if n <= 2_000_000 else \
+            np.concatenate([rng.integers(0, n, 2_000_000), np.arange(n - 100_000, n)])
+        for k in (-4, -1, 0, 1, 4):
+            rc = (f(1.0) / f(cols)).astype(np.float32)
+            rc = f(float(rc) * (1.0 + k * 2.0 ** -23))
+            v = np.trunc((idx.astype(np.float32) * rc).astype(np.float32)).astype(np.int64)
+            u = idx - v * cols
+            v = np.where(u < 0, v - 1, np.where(u >= cols, v + 1, v))
+            u = idx - v * cols
+            assert np.array_equal(v, idx // cols) and np.array_equal(u, idx % cols), (rows, cols, k)
