@@ -117,7 +117,7 @@ typedef struct dyn_bilateral_params {
 
 typedef enum dyn_precision {
   DYN_PRECISION_FP32 = 0,   /* 8-byte voxels {r,g,b,w,f32 sdf}: the drop-in */
-  DYN_PRECISION_MIXED = 1,  /* f16 sdf + u16 weight, Kahan-f32 normal eqns */
+  DYN_PRECISION_MIXED = 1,  /* f16 sdf + u16 weight, compensated-f32 normal eqns */
   /* DYN_PRECISION_MIXED, and each depth ray allocates only the blocks
    * within the truncation band of its surface point (the reference
    * allocates every block from the camera to the surface,
